@@ -1,0 +1,235 @@
+/*
+ * tarang_gpu.h — C ABI of the B200 pseudo-spectral time-step path of Tarang-4.0.
+ *
+ * The reference has no FFI layer: its "operator API" is the C++ class interface that the
+ * solver drivers call (trunk/src/IFluid/Ifluid_main.cc:258-301, IMHD/IMHD_main.cc,
+ * RBslip/RB_slip_main.cc:365-400).  Each entry point below replaces one of those calls; the
+ * C++ mirror classes in tarang_b200.hpp (CVF, RVF, IncVF, IncFluid, ...) keep the reference
+ * method names and call these functions.
+ *
+ * Conventions
+ *  - Every function returns an int status: TG_OK (0) or a negative TG_ERR_* code.  The last
+ *    error text of a context is available from tg_last_error().
+ *  - Host buffers are caller-owned.  Device state is owned by the context.
+ *  - Fields cross the boundary in the reference layout: complex<double> interleaved (re, im),
+ *    row-major [l1][l2][l3] with l3 in [0, N3/2]; real space uses the same buffer as
+ *    N1 x N2 x (N3+2) doubles with the last two reals of each row as zeroed padding
+ *    (lib/four/four_tr.cc:299-302).  n_doubles = 2 * N1 * N2 * (N3/2+1).
+ *  - A context is externally synchronised (like the reference's single-threaded rank):
+ *    different contexts may be used from different threads.  All work of a context is
+ *    queued on its stream; calls that return data to the host synchronise that stream.
+ */
+#ifndef TARANG_GPU_H
+#define TARANG_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TG_ABI_VERSION 1
+
+/* status codes */
+#define TG_OK 0
+#define TG_ERR_ARG (-1)         /* invalid argument or unsupported size */
+#define TG_ERR_OOM (-2)         /* device allocation failed / request over the HBM budget */
+#define TG_ERR_NONFINITE (-3)   /* total energy is NaN or Inf (Ifluid_main.cc:282-286) */
+#define TG_ERR_CUDA (-4)        /* a CUDA runtime call failed */
+#define TG_ERR_UNSUPPORTED (-5) /* combination not implemented */
+#define TG_ERR_TIMEOUT (-6)     /* a bounded wait ran out */
+#define TG_ERR_STATE (-7)       /* call out of order (e.g. Time_advance before Compute_nlin) */
+#define TG_ERR_BUSY (-8)        /* serving: no slot or no memory free right now */
+
+/* basis_type (string_switches[1] in the reference) */
+#define TG_FOUR 0
+#define TG_SCFT 1
+/* program kind (prog_para.d: INC_FLUID, INC_MHD, INC_SCALAR, RB_SLIP) */
+#define TG_FLUID 0
+#define TG_MHD 1
+#define TG_SCALAR 2
+#define TG_RB 3
+/* arithmetic form */
+#define TG_FP64 0
+#define TG_FP32_MIXED 1 /* FP32 transforms and products, FP64 RK state/projection/reductions */
+/* integ_scheme */
+#define TG_RK4 4
+/* force_field_proc (compute_force_main.cc:43-124) */
+#define TG_FORCE_DECAY 0
+#define TG_FORCE_ENERGY_SUPPLY 1
+#define TG_FORCE_RB 51
+
+/* field ids (dense, reference layout) */
+#define TG_V1 0 /* U.V1..V3 */
+#define TG_V2 1
+#define TG_V3 2
+#define TG_W1 3 /* W.V1..V3 (B field of MHD) */
+#define TG_W2 4
+#define TG_W3 5
+#define TG_T 6 /* T.F (scalar / temperature) */
+#define TG_NLIN1 7 /* U.nlin1..3 */
+#define TG_NLIN2 8
+#define TG_NLIN3 9
+#define TG_WNLIN1 10
+#define TG_WNLIN2 11
+#define TG_WNLIN3 12
+#define TG_TNLIN 13
+#define TG_PRESSURE 14 /* NLIN's CSF F: the pressure */
+#define TG_FORCE1 15   /* U.Force1..3 */
+#define TG_FORCE2 16
+#define TG_FORCE3 17
+#define TG_WORK0 24 /* TG_WORK0 .. TG_WORK0+7: free dense work fields for the transforms */
+#define TG_NWORK 8
+#define TG_NFIELDS 32
+
+/* energy-transfer kinds (compute_flux.cc, compute_shell_tr.cc) */
+#define TG_ET_UU 0 /* U< -> U> (fluid, and U->U of MHD) */
+#define TG_ET_BB 1 /* B< -> B> */
+#define TG_ET_UB 2 /* U< -> B> */
+#define TG_ET_BU 3 /* B< -> U> */
+#define TG_ET_TT 4 /* T< -> T> (scalar) */
+
+typedef struct tg_config {
+  int N[3];           /* N1, N2, N3 (N3 even) */
+  int basis;          /* TG_FOUR / TG_SCFT */
+  int physics;        /* TG_FLUID / TG_MHD / TG_SCALAR / TG_RB */
+  int precision;      /* TG_FP64 / TG_FP32_MIXED */
+  int dealias;        /* 1: alias_switch "DEALIAS" (2/3 rule), 0: "ALIAS" */
+  int scheme;         /* TG_RK4 */
+  double kfactor[3];  /* 2 pi / L per axis (Ifluid_main.cc:159-161) */
+  double nu;          /* dissipation_coefficient of U */
+  double eta;         /* dissipation_coefficient of B (MHD) */
+  double kappa;       /* diffusion_coefficient of T */
+  double dt;          /* Tdt: the upper bound of Get_dt (compute_dt.cc:47-59) */
+  int force_kind;     /* TG_FORCE_* */
+  double force_para[4]; /* energy supply: inner radius, outer radius, epsilon, eps_h/(k eps) */
+  int n_shells;       /* energy transfer: no_shells (= no_spheres), scheme 0 radii */
+  double rb_ra, rb_pr;  /* Rayleigh and Prandtl numbers (RB, PRLARGE + ULARGE) */
+  int device;         /* CUDA device ordinal */
+  void* stream;       /* cudaStream_t to queue on; NULL: the context creates one */
+} tg_config;
+
+typedef struct tg_ctx tg_ctx;
+
+/* defaults: FOUR fluid FP64 DEALIAS RK4, kfactor 1, decay forcing, 12 shells, device 0 */
+void tg_config_default(tg_config* cfg);
+
+int tg_ctx_create(const tg_config* cfg, tg_ctx** out);
+int tg_ctx_destroy(tg_ctx* ctx);
+const char* tg_last_error(const tg_ctx* ctx);
+int tg_synchronize(tg_ctx* ctx);
+/* bytes of device memory the context holds */
+int tg_device_bytes(const tg_ctx* ctx, size_t* bytes);
+
+/* Field I/O in the reference layout (Read_data_MPI / Write_data_MPI array_basic.cc:294-858
+ * without the MPI gather).  With dealias on, uploads of solver fields keep the 2/3 support
+ * only (the reference dealiases every initial condition, init_cond_*.cc). */
+int tg_field_upload(tg_ctx* ctx, int field, const double* host, size_t n_doubles);
+int tg_field_download(tg_ctx* ctx, int field, double* host, size_t n_doubles);
+int tg_field_copy(tg_ctx* ctx, int dst_field, int src_field);
+
+/* Forward_transform_array / Inverse_transform_array (universal_tr.cc:66-146) on a work field,
+ * in place.  parity: 0 cos/even, 1 sin/odd (SCFT only; ignored for FOUR). */
+int tg_forward_transform(tg_ctx* ctx, int field, int parity);
+int tg_inverse_transform(tg_ctx* ctx, int field, int parity);
+
+/* IncFluid::Compute_force() (compute_force_main.cc:43-124) */
+int tg_compute_force(tg_ctx* ctx);
+/* IncVF::Compute_nlin() / (W) / (T)  (compute_nlin.cc:58-108, compute_nlin_VF_MHD.cc:72-164,
+ * compute_nlin_SF.cc:65-263); nlin is dealiased */
+int tg_compute_nlin(tg_ctx* ctx);
+/* IncFluid::Add_force() (add_force.cc:47-84): nlin -= Force */
+int tg_add_force(tg_ctx* ctx);
+/* IncVF::Compute_pressure() (compute_pressure.cc:54-62) */
+int tg_compute_pressure(tg_ctx* ctx);
+/* IncFluid::Compute_rhs() (compute_rhs.cc:52-149) */
+int tg_compute_rhs(tg_ctx* ctx);
+/* IncFluid::Get_dt() (compute_dt.cc:47-108); also sets the dt Time_advance uses */
+int tg_get_dt(tg_ctx* ctx, double* dt);
+/* IncFluid::Time_advance() RK4 (time_advance.cc:100-155): precondition as in the reference,
+ * nlin = N(u) - f and pressure computed for the current field. */
+int tg_time_advance(tg_ctx* ctx);
+/* n iterations of the loop body Ifluid_main.cc:261-286 (force, nlin, add force, pressure,
+ * Get_dt, Time_advance, energy).  energies (may be NULL) receives the total energy after each
+ * step (n doubles; for MHD the sum U + B).  Returns TG_ERR_NONFINITE if an energy is NaN/Inf. */
+int tg_step(tg_ctx* ctx, int n, double* energies);
+/* elapsed simulated time and step count since creation */
+int tg_time(const tg_ctx* ctx, double* t, long long* steps);
+
+/* CV_Compute_totalenergy_diss (Cvf.cc:385-397) of group 0 = U, 1 = B, 2 = T (T: CSF energy) */
+int tg_energy(tg_ctx* ctx, int group, double* energy, double* dissipation);
+/* CV_Compute_shell_spectrum (Cvf.cc:419-449): ek = [3][n] per component (group T: [1][n]),
+ * dissk = [n] (may be NULL).  n must be >= kmax_outside + 1. */
+int tg_shell_spectrum(tg_ctx* ctx, int group, double* ek, double* dissk, int n);
+/* shell radii of the energy transfer (EnergyTr.cc:136-160): n_shells + 1 doubles */
+int tg_et_radii(tg_ctx* ctx, double* radii, int n);
+/* Compute_flux (compute_flux.cc:52-304): flux[s], s = 0..n_shells (index 0 unused) */
+int tg_flux(tg_ctx* ctx, int kind, double* flux, int n);
+/* Compute_shell_tr (compute_shell_tr.cc:59-281): (n_shells+1) x (n_shells+1) row-major */
+int tg_shell_to_shell(tg_ctx* ctx, int kind, double* tr, int n);
+/* Get_Nusselt_no (nusselt.cc:53-89), RB only */
+int tg_nusselt(tg_ctx* ctx, double* nusselt);
+
+/* ------------------------------------------------------------------------------------------
+ * Profiling (no counterpart in the reference, whose only timing is time(0) around main,
+ * src/main.cc:95-151): per-launch CUDA events on the context's stream.  While enabled, steps
+ * run eagerly (no graph replay).  Stats aggregate by kernel name; algorithmic bytes are the
+ * bytes a launch must read and write on the stored (2/3-dealiased) support.
+ * ---------------------------------------------------------------------------------------- */
+typedef struct tg_kernel_stat {
+  char name[48];
+  int launches;
+  double total_ms;
+  double bytes_per_launch;
+} tg_kernel_stat;
+
+int tg_profile_enable(tg_ctx* ctx, int enable);
+/* synchronises; fills up to max stats, sets *n; clears the records */
+int tg_profile_read(tg_ctx* ctx, tg_kernel_stat* out, int max, int* n);
+
+/* ------------------------------------------------------------------------------------------
+ * Serving: a persistent request loop that admits independent solves by HBM budget, keeps
+ * their spectral state resident and advances same-shape requests together.
+ * ---------------------------------------------------------------------------------------- */
+typedef struct tg_server tg_server;
+
+typedef struct tg_server_config {
+  size_t hbm_budget_bytes; /* admission budget */
+  int max_batch;           /* most requests of one shape advanced together */
+  int device;
+  int use_graphs;          /* 1: replay one captured CUDA graph per shape and batch size */
+} tg_server_config;
+
+typedef struct tg_request {
+  tg_config cfg;        /* shape, physics, precision, coefficients */
+  int n_steps;          /* RK4 steps to run */
+  const double* init;   /* initial fields, reference layout, concatenated per state field
+                           (fluid 3, MHD 6, scalar/RB 4); copied at submit */
+  size_t n_doubles;     /* length of init */
+} tg_request;
+
+typedef struct tg_request_status {
+  int state;            /* 0 queued, 1 running, 2 done, 3 failed */
+  int error;            /* TG_ERR_* when failed */
+  int steps_done;
+  double submit_s, start_s, finish_s; /* server clock (seconds) */
+  double final_energy;
+} tg_request_status;
+
+int tg_server_create(const tg_server_config* cfg, tg_server** out);
+int tg_server_destroy(tg_server* srv);
+int tg_server_submit(tg_server* srv, const tg_request* req, long long* id);
+/* one scheduling round: admit what fits, advance every resident batch by one step */
+int tg_server_pump(tg_server* srv, int* n_active);
+/* pump until every submitted request is done or failed (bounded by max_rounds; 0 = no bound) */
+int tg_server_drain(tg_server* srv, long long max_rounds);
+int tg_server_poll(tg_server* srv, long long id, tg_request_status* st);
+/* final state of a finished request, reference layout, same packing as tg_request.init */
+int tg_server_result(tg_server* srv, long long id, double* host, size_t n_doubles);
+double tg_server_clock(tg_server* srv);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TARANG_GPU_H */

@@ -1,0 +1,842 @@
+"""CPU oracle: an FP64 restatement of Tarang-4.0's pseudo-spectral time-step path.
+
+TEST INFRASTRUCTURE ONLY.  This module is the checker for the CUDA path: only
+``tests/``, ``__graft_entry__.smoke()`` and the ``cpu_baseline`` / ``--impl
+reference`` legs of ``bench.py`` may import it.  The product (the C-ABI library
+``tarang_b200/libtarang_gpu.so`` and its Python mirror) never calls it.
+
+Parity status.  The reference (C++, blitz++, FFTW3-MPI, MPI) cannot be built on
+this image, so the oracle restates its algorithms and is pinned by
+  * the one known answer in the reference's own tests
+    (``trunk/test/test-fftw/out1.d``: an unnormalised C2R->R2C round trip of a
+    unit delta at (0,0,2) on a 4^3 grid returns 64 = N^3,
+    produced by ``trunk/test/test-fftw/main_mpi.cc:93-118``), and
+  * analytic known answers (single modes, Taylor-Green, Beltrami flow,
+    exact viscous decay, energy conservation of the inviscid nonlinear term,
+    antisymmetry of the shell-to-shell transfer),
+  all checked in ``tests/test_oracle_*.py``.  Every other value is "parity
+  unpinned by the reference's own tests" and is pinned by those identities.
+
+Transforms use ``scipy.fft`` (pocketfft), whose unnormalised r2c/c2r and
+DCT/DST-II/III definitions are the published definitions FFTW uses for
+``fftw_plan_dft_r2c``/``c2r`` and REDFT10/RODFT10/REDFT01/RODFT01.
+
+Array layout (the reference's): spectral fields are complex128 arrays of shape
+(N1, N2, N3//2+1) indexed (l1, l2, l3); real-space fields are float64 arrays of
+shape (N1, N2, N3) indexed (x, y, z).  Wavenumbers follow
+``lib/four/four_inline.h:88-129`` (index <= N/2 counts as positive).
+
+File:line citations are relative to the reference project root (``trunk/``).
+"""
+
+from __future__ import annotations
+
+import math
+import os
+
+import numpy as np
+import scipy.fft as sfft
+
+_WORKERS = int(os.environ.get("TARANG_ORACLE_WORKERS", os.cpu_count() or 1))
+
+MYEPS = 1e-15      # lib/basis_basicfn/extern_def_vars.h:81
+MYEPS2 = 1e-5      # lib/basis_basicfn/extern_def_vars.h:82
+INF_RADIUS = 1e4   # lib/basis_basicfn/extern_def_vars.h (INF_RADIUS used as the last sphere)
+
+
+# --------------------------------------------------------------------------------------
+# Wavenumber helpers  (lib/four/four_inline.h, lib/scft/scft_inline.h)
+# --------------------------------------------------------------------------------------
+
+def kx_four(N1):
+    """Get_kx_FOUR  lib/four/four_inline.h:88-92 (single rank: local_N1_start = 0)."""
+    l = np.arange(N1)
+    return np.where(l <= N1 // 2, l, l - N1)
+
+
+def ky_four(N2):
+    """Get_ky3D_FOUR  lib/four/four_inline.h:129."""
+    l = np.arange(N2)
+    return np.where(l <= N2 // 2, l, l - N2)
+
+
+def kz_four(N3):
+    return np.arange(N3 // 2 + 1)
+
+
+def kx_scft(N1):
+    """Get_kx_SCFT  lib/scft/scft_inline.h:86 (kx = m >= 0)."""
+    return np.arange(N1)
+
+
+def kvec(N, kfactor, basis="FOUR"):
+    """Broadcastable (Kx, Ky, Kz) grids of actual wavenumbers (globalvar_waveno_switch = 0)."""
+    N1, N2, N3 = N
+    kx = (kx_four(N1) if basis == "FOUR" else kx_scft(N1)).astype(np.float64) * kfactor[0]
+    ky = ky_four(N2).astype(np.float64) * kfactor[1]
+    kz = kz_four(N3).astype(np.float64) * kfactor[2]
+    return kx[:, None, None], ky[None, :, None], kz[None, None, :]
+
+
+def kmag(N, kfactor, basis="FOUR"):
+    """Kmagnitude_FOUR  lib/four/four_inline.h:155-166; Kmagnitude_SCFT scft_inline.h:128-139."""
+    Kx, Ky, Kz = kvec(N, kfactor, basis)
+    return np.sqrt(Kx * Kx + Ky * Ky + Kz * Kz)
+
+
+def ksqr(N, kfactor, basis="FOUR"):
+    Kx, Ky, Kz = kvec(N, kfactor, basis)
+    return Kx * Kx + Ky * Ky + Kz * Kz
+
+
+def max_radius_inside(N, kfactor, alias="DEALIAS", basis="FOUR"):
+    """Max_radius_inside_(de)aliased_FOUR  lib/four/four_inline.h:190-257 (SCFT: scft_inline.h)."""
+    N1, N2, N3 = N
+    if basis == "FOUR":
+        d = 3 if alias == "DEALIAS" else 2
+        kmag_ = min((N1 // d) * kfactor[0], (N2 // d) * kfactor[1])
+        if N3 > 2:
+            kmag_ = min(kmag_, (N3 // d) * kfactor[2])
+        return int(kmag_)
+    # SCFT: x extent is N1 (dealiased 2N1/3), y/z as FOUR
+    if alias == "DEALIAS":
+        kmag_ = min((2 * N1 // 3) * kfactor[0], (N2 // 3) * kfactor[1])
+        if N3 > 2:
+            kmag_ = min(kmag_, (N3 // 3) * kfactor[2])
+    else:
+        kmag_ = min(N1 * kfactor[0], (N2 // 2) * kfactor[1])
+        if N3 > 2:
+            kmag_ = min(kmag_, (N3 // 2) * kfactor[2])
+    return int(kmag_)
+
+
+def min_radius_outside(N, kfactor, alias="DEALIAS", basis="FOUR"):
+    """Min_radius_outside_(de)aliased_FOUR  lib/four/four_inline.h:172-228."""
+    N1, N2, N3 = N
+    if basis == "FOUR":
+        d = 3 if alias == "DEALIAS" else 2
+        return int(math.ceil(math.sqrt(((N1 // d) * kfactor[0]) ** 2 + ((N2 // d) * kfactor[1]) ** 2
+                                       + ((N3 // d) * kfactor[2]) ** 2)))
+    if alias == "DEALIAS":
+        return int(math.ceil(math.sqrt(((2 * N1 // 3) * kfactor[0]) ** 2 + ((N2 // 3) * kfactor[1]) ** 2
+                                       + ((N3 // 3) * kfactor[2]) ** 2)))
+    return int(math.ceil(math.sqrt((N1 * kfactor[0]) ** 2 + ((N2 // 2) * kfactor[1]) ** 2
+                                   + ((N3 // 2) * kfactor[2]) ** 2)))
+
+
+def approx_number_modes_in_shell(N, radius, kfactor, basis="FOUR"):
+    """Approx_number_modes_in_shell_FOUR  lib/four/four_inline.h:276-306 (3-D branch).
+    SCFT (scft_inline.h:242) uses the same hemisphere area for the 3-D case."""
+    return (2 * math.pi * radius * radius) / (kfactor[0] * kfactor[1] * kfactor[2])
+
+
+def multiplicity_four(N):
+    """Multiplicity_factor_FOUR  lib/four/four_inline.h:347-365 as a (N1,N2,N3/2+1) array."""
+    N1, N2, N3 = N
+    kx = kx_four(N1)[:, None, None]
+    ky = ky_four(N2)[None, :, None]
+    l3 = kz_four(N3)[None, None, :]
+    f = np.where(l3 > 0, 1.0, 0.5)
+    dbl = (kx == N1 // 2) | ((ky == N2 // 2) & (N2 > 1))
+    return np.broadcast_to(np.where(dbl, 2 * f, f), (N1, N2, N3 // 2 + 1)).copy()
+
+
+def multiplicity_scft(N):
+    """Multiplicity_factor_SCFT  lib/scft/scft_inline.h:313-335."""
+    N1, N2, N3 = N
+    m = kx_scft(N1)[:, None, None]
+    ky = ky_four(N2)[None, :, None]
+    l3 = kz_four(N3)[None, None, :]
+    f = np.where(l3 > 0, np.where(m > 0, 2.0, 1.0), np.where(m > 0, 1.0, 0.5))
+    dbl = (ky == N2 // 2) & (N2 > 1)
+    return np.broadcast_to(np.where(dbl, 2 * f, f), (N1, N2, N3 // 2 + 1)).copy()
+
+
+def multiplicity(N, basis="FOUR"):
+    return multiplicity_four(N) if basis == "FOUR" else multiplicity_scft(N)
+
+
+# --------------------------------------------------------------------------------------
+# Dealiasing and reality condition  (lib/fields/universal/universal_misc.cc)
+# --------------------------------------------------------------------------------------
+
+def dealias_keep_mask(N, basis="FOUR"):
+    """Boolean mask of modes that Dealias_array keeps  (universal_misc.cc:118-159)."""
+    N1, N2, N3 = N
+    keep = np.ones((N1, N2, N3 // 2 + 1), dtype=bool)
+    if N1 >= 3:
+        if basis == "FOUR":
+            kx = kx_four(N1)
+            keep[np.abs(kx) >= N1 // 3, :, :] = False
+        else:
+            kx = kx_scft(N1)
+            keep[np.abs(kx) >= 2 * N1 // 3, :, :] = False
+    if N2 >= 3:
+        keep[:, N2 // 3: 2 * N2 // 3 + 2, :] = False   # Range(N2/3, 2N2/3+1) inclusive
+    if N3 >= 3:
+        keep[:, :, N3 // 3: N3 // 2 + 1] = False       # Range(N3/3, N3/2) inclusive
+    return keep
+
+
+def dealias(A, basis="FOUR"):
+    """Dealias_array  universal_misc.cc:118-159 (returns a new array)."""
+    return np.where(dealias_keep_mask(A.shape[:2] + ((A.shape[2] - 1) * 2,), basis), A, 0)
+
+
+def satisfy_reality(A, basis="FOUR"):
+    """Satisfy_reality_array  universal_misc.cc:51-109: for kz = 0 and kz = N3/2 planes set
+    A(kx, ky<0) = conj(A(-kx, -ky)) and A(kx<0, 0) = conj(A(-kx, 0)), from a snapshot."""
+    A = A.copy()
+    N1, N2 = A.shape[0], A.shape[1]
+    N3h = A.shape[2] - 1
+    for l3 in (0, N3h):
+        plane = A[:, :, l3].copy()
+        if basis == "FOUR":
+            kx = kx_four(N1)
+            conj_nx = np.where(-kx >= 0, -kx, -kx + N1)
+            for ly in range(N2 // 2 + 1, N2):
+                pos_iy = -(ly - N2)
+                A[:, ly, l3] = np.conj(plane[conj_nx, pos_iy])
+            for lx in range(N1):
+                if kx[lx] < 0:
+                    A[lx, 0, l3] = np.conj(plane[-kx[lx], 0])
+        else:
+            for ly in range(N2 // 2 + 1, N2):
+                pos_iy = -(ly - N2)
+                A[:, ly, l3] = np.conj(A[:, pos_iy, l3])
+    return A
+
+
+# --------------------------------------------------------------------------------------
+# FOUR transforms  (lib/four/four_tr.cc)
+# --------------------------------------------------------------------------------------
+
+def forward_four(real):
+    """ArrayFFT_FOUR  four_tr.cc:199-209: zero-pad, r2c (sign -1), then Norm_FOUR 1/(N1N2N3)
+    (four_tr.cc:306-309).  Input real (N1,N2,N3) -> spectrum (N1,N2,N3/2+1)."""
+    N1, N2, N3 = real.shape
+    return sfft.rfftn(real, axes=(0, 1, 2), workers=_WORKERS) / (N1 * N2 * N3)
+
+
+def inverse_four(spec, N3=None):
+    """ArrayIFFT_FOUR  four_tr.cc:229-295: unnormalised c2c(y), c2c(x), c2r(z).  The c2r along
+    z uses only the real parts of the kz = 0 and kz = N3/2 entries (FFTW/pocketfft c2r rule)."""
+    N1, N2, M1 = spec.shape
+    if N3 is None:
+        N3 = 2 * (M1 - 1)
+    return sfft.irfftn(spec, s=(N1, N2, N3), axes=(0, 1, 2), workers=_WORKERS) * (N1 * N2 * N3)
+
+
+def xderiv_four(A, kfactor):
+    """Xderiv_FOUR  four_tr.cc:314-323: B = i kx A."""
+    N = (A.shape[0], A.shape[1], 2 * (A.shape[2] - 1))
+    Kx, _, _ = kvec(N, kfactor)
+    return 1j * Kx * A
+
+
+def yderiv_four(A, kfactor):
+    """Yderiv_FOUR  four_tr.cc:329-343."""
+    N = (A.shape[0], A.shape[1], 2 * (A.shape[2] - 1))
+    _, Ky, _ = kvec(N, kfactor)
+    return 1j * Ky * A
+
+
+def zderiv_four(A, kfactor):
+    """Zderiv_FOUR  four_tr.cc:348-353."""
+    N = (A.shape[0], A.shape[1], 2 * (A.shape[2] - 1))
+    _, _, Kz = kvec(N, kfactor)
+    return 1j * Kz * A
+
+
+# --------------------------------------------------------------------------------------
+# SCFT transforms  (lib/scft/scft_tr.cc): axis 0 (x) is sin/cos on the half-sample grid
+# --------------------------------------------------------------------------------------
+
+def forward_scft(real, parity):
+    """ArraySFT_SCFT (parity 1) / ArrayCFT_SCFT (parity 0)  scft_tr.cc:230-431.
+    RODFT10 / REDFT10 along x, r2c over (y, z), Norm_SCFT 1/(2 N1 N2 N3) (scft_tr.cc:89-92);
+    the sine coefficients are shifted one slot right (ArrayShiftRight_SCFT scft_tr.cc:153-184):
+    slot m <-> sin(m pi x), slot 0 = 0, the last DST-II coefficient is dropped."""
+    N1, N2, N3 = real.shape
+    if parity == 1:
+        t = sfft.dst(real, type=2, axis=0, norm=None, workers=_WORKERS)
+    else:
+        t = sfft.dct(real, type=2, axis=0, norm=None, workers=_WORKERS)
+    s = sfft.rfftn(t, axes=(1, 2), workers=_WORKERS) / (2.0 * N1 * N2 * N3)
+    if parity == 1:
+        out = np.zeros_like(s)
+        out[1:] = s[:-1]
+        return out
+    return s
+
+
+def inverse_scft(spec, parity, N3=None):
+    """ArrayISFT_SCFT (parity 1) / ArrayICFT_SCFT (parity 0)  scft_tr.cc:440-639: shift left
+    (sine), unnormalised c2r over (y, z), then RODFT01 / REDFT01 along x."""
+    N1, N2, M1 = spec.shape
+    if N3 is None:
+        N3 = 2 * (M1 - 1)
+    if parity == 1:
+        s = np.zeros_like(spec)
+        s[:-1] = spec[1:]
+    else:
+        s = spec
+    r = sfft.irfftn(s, s=(N2, N3), axes=(1, 2), workers=_WORKERS) * (N2 * N3)
+    if parity == 1:
+        return sfft.dst(r, type=3, axis=0, norm=None, workers=_WORKERS)
+    return sfft.dct(r, type=3, axis=0, norm=None, workers=_WORKERS)
+
+
+def xderiv_scft(A, kfactor, parity):
+    """Xderiv_Sin_SCFT (+kx, sin -> cos) / Xderiv_Cos_SCFT (-kx, cos -> sin)  scft_tr.cc:649-672.
+    parity follows universal_tr.cc:186-210: parity 1 = the input is a sine series."""
+    N = (A.shape[0], A.shape[1], 2 * (A.shape[2] - 1))
+    Kx, _, _ = kvec(N, kfactor, "SCFT")
+    return (Kx * A) if parity == 1 else (-Kx * A)
+
+
+def forward(real, basis="FOUR", parity=0):
+    """Forward_transform_array  universal_tr.cc:66-86."""
+    return forward_four(real) if basis == "FOUR" else forward_scft(real, parity)
+
+
+def inverse(spec, basis="FOUR", parity=0, N3=None):
+    """Inverse_transform_array  universal_tr.cc:126-146."""
+    return inverse_four(spec, N3) if basis == "FOUR" else inverse_scft(spec, parity, N3)
+
+
+def xderiv(A, kfactor, basis="FOUR", parity=0):
+    return xderiv_four(A, kfactor) if basis == "FOUR" else xderiv_scft(A, kfactor, parity)
+
+
+yderiv = lambda A, kfactor, basis="FOUR", parity=0: yderiv_four(A, kfactor)   # noqa: E731  Fourier in y
+zderiv = lambda A, kfactor, basis="FOUR", parity=0: zderiv_four(A, kfactor)   # noqa: E731  Fourier in z
+
+
+# --------------------------------------------------------------------------------------
+# Energies and spectra  (lib/four/four_energy.cc, lib/scft/scft_energy.cc)
+# --------------------------------------------------------------------------------------
+
+def total_energy_four(A, B=None):
+    """Get_local_energy_FOUR  four_energy.cc:48-86 (and the cross form :108-168), 1 rank:
+    sum over stored modes + the unstored ky = -N2/2 and kx = -N1/2 planes, kz = 0 halved,
+    origin excluded."""
+    if B is None:
+        B = A
+    N1, N2 = A.shape[0], A.shape[1]
+    P = np.real(A * np.conj(B))
+    t = P.sum()
+    if N2 > 1:
+        t += P[:, N2 // 2, :].sum()
+    t += P[N1 // 2, :, :].sum()
+    t -= P[:, :, 0].sum() / 2
+    if N2 > 1:
+        t -= P[:, N2 // 2, 0].sum() / 2
+    t -= P[N1 // 2, :, 0].sum() / 2
+    t -= P[0, 0, 0] / 2
+    return float(t)
+
+
+def total_energy_scft(A, B=None):
+    """Get_total_energy_SCFT  scft_energy.cc:51-104: per ky plane 2 sum|A|^2 - sum|A(m,ky,0)|^2
+    - sum|A(0,ky,kz)|^2 + |A(0,ky,0)|^2/2 (weights 2/1/1/half = Multiplicity_factor_SCFT), the
+    ky = N2/2 plane counted twice, minus |A(0,0,0)|^2/2 (origin excluded)."""
+    if B is None:
+        B = A
+    N = (A.shape[0], A.shape[1], 2 * (A.shape[2] - 1))
+    mult = multiplicity_scft(N)
+    P = np.real(A * np.conj(B))
+    t = (mult * P).sum() - mult[0, 0, 0] * P[0, 0, 0]
+    return float(t)
+
+
+def total_energy(A, basis="FOUR", B=None):
+    return total_energy_four(A, B) if basis == "FOUR" else total_energy_scft(A, B)
+
+
+def total_Sn(A, n, kfactor, alias="DEALIAS", basis="FOUR"):
+    """Get_local_Sn_FOUR  four_energy.cc:179-211: sum mult K^n |A|^2 over K <= kmax_outside;
+    for n = 0 the origin is subtracted."""
+    N = (A.shape[0], A.shape[1], 2 * (A.shape[2] - 1))
+    K = kmag(N, kfactor, basis)
+    kkmax = min_radius_outside(N, kfactor, alias, basis)
+    mult = multiplicity(N, basis)
+    w = np.where(K <= kkmax, mult * (K ** n if n != 0 else 1.0), 0.0)
+    s = float((w * np.abs(A) ** 2).sum())
+    if n == 0:
+        s -= mult[0, 0, 0] * abs(A[0, 0, 0]) ** 2
+    return s
+
+
+def shell_spectrum(A, n, kfactor, alias="DEALIAS", basis="FOUR", B=None):
+    """Compute_shell_spectrum_FOUR  four_energy.cc:244-338 (cross form :341-436):
+    Sk(ceil|K|) += mult K^n Re(A B*) for ceil|K| <= kkmax; shells (kmax_inside, kmax] rescaled
+    by Approx_number_modes_in_shell / count when count >= 1.  Length kmax_outside + 1."""
+    if B is None:
+        B = A
+    N = (A.shape[0], A.shape[1], 2 * (A.shape[2] - 1))
+    K = kmag(N, kfactor, basis)
+    kkmax = min_radius_outside(N, kfactor, alias, basis)
+    kin = max_radius_inside(N, kfactor, alias, basis)
+    mult = multiplicity(N, basis)
+    idx = np.ceil(K).astype(np.int64)
+    sel = idx <= kkmax
+    val = mult * (K ** n if n != 0 else 1.0) * np.real(A * np.conj(B))
+    Sk = np.bincount(idx[sel], weights=val[sel], minlength=kkmax + 1)[: kkmax + 1]
+    cnt = np.bincount(idx[sel], weights=np.broadcast_to(mult, K.shape)[sel], minlength=kkmax + 1)[: kkmax + 1]
+    for i in range(kin + 1, kkmax + 1):
+        if cnt[i] >= 1:
+            Sk[i] = Sk[i] * approx_number_modes_in_shell(N, i, kfactor, basis) / cnt[i]
+    return Sk
+
+
+# --------------------------------------------------------------------------------------
+# Field operations used by the solver
+# --------------------------------------------------------------------------------------
+
+def divide_ksqr(A, kfactor, basis="FOUR"):
+    """Array_divide_ksqr_FOUR  four_basic.cc:220-245 (A(0,0,0) = 0)."""
+    N = (A.shape[0], A.shape[1], 2 * (A.shape[2] - 1))
+    K2 = ksqr(N, kfactor, basis)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        out = A / K2
+    out[0, 0, 0] = 0.0
+    return out
+
+
+def exp_ksqr(A, factor, kfactor, basis="FOUR"):
+    """Array_exp_ksqr_FOUR  four_basic.cc:312-337: A *= exp(factor K^2)."""
+    N = (A.shape[0], A.shape[1], 2 * (A.shape[2] - 1))
+    return A * np.exp(factor * ksqr(N, kfactor, basis))
+
+
+# --------------------------------------------------------------------------------------
+# Nonlinear terms  (lib/IncFlow/nlin_calc)
+# --------------------------------------------------------------------------------------
+
+def nlin_fluid(V, kfactor, basis="FOUR", alias="DEALIAS"):
+    """IncVF::Compute_nlin()  compute_nlin.cc:58-108 (normal order):
+    nlin_i = D_j F(u_i u_j) with the diagonal products first (RSprod.cc:52-57, Nlin.cc:85-94),
+    then the off-diagonal products u1u2, u2u3, u3u1 (RSprod.cc:70-77) and their derivatives
+    (Derivative_RSprod_VV RSprod.cc:94-105); then Dealias_nlin (dealias.cc:113-119)."""
+    N1, N2 = V[0].shape[0], V[0].shape[1]
+    N3 = 2 * (V[0].shape[2] - 1)
+    par_inv = (1, 0, 0)
+    ur = [inverse(V[i], basis, par_inv[i], N3) for i in range(3)]
+    nl = [forward(ur[i] * ur[i], basis, 0) for i in range(3)]
+    nl[0] = xderiv(nl[0], kfactor, basis, 0)
+    nl[1] = yderiv(nl[1], kfactor)
+    nl[2] = zderiv(nl[2], kfactor)
+    p12 = forward(ur[0] * ur[1], basis, 1)   # RV_Forward_transform_RSprod Rvf.cc:179-186: SFT, CFT, SFT
+    p23 = forward(ur[1] * ur[2], basis, 0)
+    p31 = forward(ur[2] * ur[0], basis, 1)
+    nl[0] = nl[0] + yderiv(p12, kfactor) + zderiv(p31, kfactor)
+    nl[1] = nl[1] + xderiv(p12, kfactor, basis, 1) + zderiv(p23, kfactor)
+    nl[2] = nl[2] + xderiv(p31, kfactor, basis, 1) + yderiv(p23, kfactor)
+    if alias == "DEALIAS":
+        nl = [dealias(a, basis) for a in nl]
+    return nl
+
+
+def nlin_mhd(V, W, kfactor, basis="FOUR", alias="DEALIAS"):
+    """IncVF::Compute_nlin(IncVF& W)  compute_nlin_VF_MHD.cc:72-164 with Elsasser variables
+    (elsasser.cc:53-130): Zp = U + B, Zm = U - B;  Zp.nlin_i = D_j F(Zm_j Zp_i),
+    Zm.nlin_i = D_j F(Zp_j Zm_i) (RSprod.cc:117-194); U.nlin = (Zp.nlin + Zm.nlin)/2,
+    B.nlin = (Zp.nlin - Zm.nlin)/2; Dealias_nlin(W).  Returns (U.nlin, B.nlin)."""
+    N3 = 2 * (V[0].shape[2] - 1)
+    Zp = [V[i] + W[i] for i in range(3)]
+    Zm = [V[i] - W[i] for i in range(3)]
+    par_inv = (1, 0, 0)
+    zp = [inverse(Zp[i], basis, par_inv[i], N3) for i in range(3)]
+    zm = [inverse(Zm[i], basis, par_inv[i], N3) for i in range(3)]
+    d = [forward(zp[i] * zm[i], basis, 0) for i in range(3)]
+    d[0] = xderiv(d[0], kfactor, basis, 0)
+    d[1] = yderiv(d[1], kfactor)
+    d[2] = zderiv(d[2], kfactor)
+    n = list(d)
+    nw = list(d)
+    v1 = forward(zp[0] * zm[1], basis, 1)
+    w1 = forward(zm[0] * zp[1], basis, 1)
+    v2 = forward(zp[1] * zm[2], basis, 0)
+    w2 = forward(zm[1] * zp[2], basis, 0)
+    v3 = forward(zp[2] * zm[0], basis, 1)
+    w3 = forward(zm[2] * zp[0], basis, 1)
+    # Derivative_RSprod_VV(W) RSprod.cc:170-193
+    n[0] = n[0] + yderiv(v1, kfactor) + zderiv(w3, kfactor)
+    n[1] = n[1] + xderiv(w1, kfactor, basis, 1) + zderiv(v2, kfactor)
+    n[2] = n[2] + xderiv(v3, kfactor, basis, 1) + yderiv(w2, kfactor)
+    nw[0] = nw[0] + yderiv(w1, kfactor) + zderiv(v3, kfactor)
+    nw[1] = nw[1] + xderiv(v1, kfactor, basis, 1) + zderiv(w2, kfactor)
+    nw[2] = nw[2] + xderiv(w3, kfactor, basis, 1) + yderiv(v2, kfactor)
+    un = [0.5 * (n[i] + nw[i]) for i in range(3)]
+    bn = [0.5 * (n[i] - nw[i]) for i in range(3)]
+    if alias == "DEALIAS":
+        un = [dealias(a, basis) for a in un]
+        bn = [dealias(a, basis) for a in bn]
+    return un, bn
+
+
+def nlin_scalar(V, F, kfactor, basis="FOUR", alias="DEALIAS", dealias_T=True):
+    """Scalar part of IncVF::Compute_nlin(IncSF& T)  compute_nlin_SF.cc:65-263:
+    T.nlin = D_j F(u_j theta) with SCFT parities (x: sin*sin -> cos; y, z: sin*cos -> sin)."""
+    N3 = 2 * (V[0].shape[2] - 1)
+    par_inv = (1, 0, 0)
+    ur = [inverse(V[i], basis, par_inv[i], N3) for i in range(3)]
+    tr = inverse(F, basis, 1, N3)
+    a = forward(ur[0] * tr, basis, 0)
+    b = forward(ur[1] * tr, basis, 1)
+    c = forward(ur[2] * tr, basis, 1)
+    tn = xderiv(a, kfactor, basis, 0) + yderiv(b, kfactor) + zderiv(c, kfactor)
+    if alias == "DEALIAS" and dealias_T:
+        tn = dealias(tn, basis)
+    return tn
+
+
+# --------------------------------------------------------------------------------------
+# Pressure projection and right-hand side
+# --------------------------------------------------------------------------------------
+
+def pressure(nl, kfactor, basis="FOUR", alias="DEALIAS"):
+    """Compute_pressure  compute_pressure.cc:54-62: F = Xderiv(nlin1, parity 1) + Yderiv(nlin2)
+    + Zderiv(nlin3) (compute_divergence.cc:55-65), F /= K^2 (F(0) = 0), dealias F."""
+    p = xderiv(nl[0], kfactor, basis, 1) + yderiv(nl[1], kfactor) + zderiv(nl[2], kfactor)
+    p = divide_ksqr(p, kfactor, basis)
+    if alias == "DEALIAS":
+        p = dealias(p, basis)
+    return p
+
+
+def rhs_from_nlin(nl, p, kfactor, basis="FOUR"):
+    """Compute_rhs  compute_rhs.cc:52-60 with Add_pressure_gradient add_pressure_grad.cc:48-61:
+    nlin_i += D_i p (parity 0), then nlin = -nlin."""
+    g = [xderiv(p, kfactor, basis, 0), yderiv(p, kfactor), zderiv(p, kfactor)]
+    return [-(nl[i] + g[i]) for i in range(3)]
+
+
+# --------------------------------------------------------------------------------------
+# Forcing  (lib/IncFluid/force)
+# --------------------------------------------------------------------------------------
+
+def number_modes_in_shell(N, inner, outer, kfactor, basis="FOUR"):
+    """Get_local_number_modes_in_shell_FOUR  four_basic.cc:48-90: modes with
+    inner <= |K| < outer (note: half-open the other way to the forcing loop), kz = 0 counted
+    once, kz > 0 twice."""
+    kxm = int(math.ceil(outer / kfactor[0]))
+    kym = int(math.ceil(outer / kfactor[1]))
+    kzm = int(math.ceil(outer / kfactor[2]))
+    cnt = 0
+    kxr = range(-kxm, kxm + 1) if basis == "FOUR" else range(0, kxm + 1)
+    for kx in kxr:
+        for ky in range(-kym, kym + 1):
+            for kz in range(0, kzm + 1):
+                km = math.sqrt((kx * kfactor[0]) ** 2 + (ky * kfactor[1]) ** 2 + (kz * kfactor[2]) ** 2)
+                if inner <= km < outer:
+                    cnt += 1 if kz == 0 else 2
+    return cnt
+
+
+def force_const_energy_supply(V, N, kfactor, inner, outer, eps, eps_h=0.0):
+    """Compute_force_const_energy_helicity_supply  compute_force_ek_hk_supply.cc:51-157 with
+    Force_alpha_beta  force_alpha_beta.cc:60-121 (FOUR) and Satisfy_reality_array on F.
+    F = alpha u + beta omega on inner < |K| <= outer; alpha = temp(1 - s h)/(1 - s^2),
+    beta = temp (h - s)/(1 - s^2), temp = eps/(nf 2 E_k), s = H_k/(k E_k); vorticity is used
+    only when beta > MYEPS."""
+    N1, N2, N3 = N
+    nf = number_modes_in_shell(N, inner, outer, kfactor)
+    e_per_mode = eps / nf
+    F = [np.zeros_like(V[0]) for _ in range(3)]
+    kxm = int(math.ceil(outer / kfactor[0]))
+    kym = int(math.ceil(outer / kfactor[1]))
+    kzm = int(math.ceil(outer / kfactor[2]))
+    for kx in range(-kxm, kxm + 1):
+        for ky in range(-kym, kym + 1):
+            for kz in range(0, kzm + 1):
+                lx = kx if kx >= 0 else kx + N1
+                ly = ky if ky >= 0 else ky + N2
+                lz = kz
+                km = math.sqrt((kx * kfactor[0]) ** 2 + (ky * kfactor[1]) ** 2 + (kz * kfactor[2]) ** 2)
+                if not (inner < km <= outer):
+                    continue
+                v = np.array([V[0][lx, ly, lz], V[1][lx, ly, lz], V[2][lx, ly, lz]])
+                Ek = float(np.sum(np.abs(v) ** 2)) / 2.0        # CV_Modal_energy (Cvf.cc:595-600)
+                if Ek <= MYEPS:
+                    continue
+                kk = np.array([kx * kfactor[0], ky * kfactor[1], kz * kfactor[2]])
+                vr, vi = v.real, v.imag
+                Hk = float(np.dot(kk, np.cross(vr, vi)))       # Get_Modal_helicity_FOUR four_basic.cc:136-155
+                temp = e_per_mode / (2 * Ek)
+                sk = Hk / (km * Ek)
+                if abs(sk * sk - 1) > MYEPS2:
+                    alpha = temp * (1 - sk * eps_h) / (1 - sk * sk)
+                    beta = temp * (eps_h - sk) / (1 - sk * sk)
+                else:
+                    alpha = temp / 2
+                    beta = alpha / (sk * km)
+                vort = np.zeros(3, dtype=np.complex128)
+                if beta > MYEPS:                                 # Compute_Modal_vorticity_FOUR four_basic.cc:166-186
+                    vort = 1j * np.array([kk[1] * v[2] - kk[2] * v[1],
+                                          kk[2] * v[0] - kk[0] * v[2],
+                                          kk[0] * v[1] - kk[1] * v[0]])
+                for c in range(3):
+                    F[c][lx, ly, lz] = alpha * v[c] + beta * vort[c]
+    F = [satisfy_reality(f) for f in F]
+    return F
+
+
+# --------------------------------------------------------------------------------------
+# Integrating-factor RK4  (lib/IncFluid/time_advance)
+# --------------------------------------------------------------------------------------
+
+def get_dt(E, N, kfactor, Tdt, alias="DEALIAS", basis="FOUR"):
+    """IncFluid::Get_dt  compute_dt.cc:47-59: min(dx / (sqrt(E) 20), Tdt), dx = 2 pi / kmax_inside."""
+    kmax = max_radius_inside(N, kfactor, alias, basis)
+    dx = 2 * math.pi / kmax
+    dt = dx / (math.sqrt(E) * 20) if E > 0 else float("inf")
+    return min(dt, Tdt)
+
+
+class FluidSolver:
+    """The fluid loop iteration of Ifluid_main.cc:258-301 with IncFluid::Time_advance (RK4)
+    time_advance.cc:100-155, Single_time_step single_time_step.cc:54-86 and Compute_RK4_parts
+    single_time_step.cc:440-444, Compute_force_TO_rhs single_time_step.cc:351-365."""
+
+    def __init__(self, N, kfactor, nu, Tdt, basis="FOUR", alias="DEALIAS", force=None):
+        self.N = tuple(N)
+        self.kfactor = tuple(kfactor)
+        self.nu = nu
+        self.Tdt = Tdt
+        self.basis = basis
+        self.alias = alias
+        self.force = force   # None (decay) or dict(inner, outer, eps, eps_h)
+
+    # Compute_force(); Compute_nlin(); Add_force(); Compute_pressure(); Compute_rhs()
+    def rhs(self, V):
+        if self.force is not None:
+            F = force_const_energy_supply(V, self.N, self.kfactor, **self.force)
+        else:
+            F = None
+        nl = nlin_fluid(V, self.kfactor, self.basis, self.alias)
+        if F is not None:
+            nl = [nl[i] - F[i] for i in range(3)]
+        p = pressure(nl, self.kfactor, self.basis, self.alias)
+        return rhs_from_nlin(nl, p, self.kfactor, self.basis), F
+
+    def E(self, V, a, dt):
+        return [exp_ksqr(v, -self.nu * a * dt, self.kfactor, self.basis) for v in V]
+
+    def step(self, V):
+        """One loop iteration; returns (V_new, dt)."""
+        E0 = sum(total_energy(v, self.basis) for v in V)
+        dt = get_dt(E0, self.N, self.kfactor, self.Tdt, self.alias, self.basis)
+        u0 = [v.copy() for v in V]
+        # stage 1: Single_time_step(dt, 1/2, 1/2, 1/2): V += dt/2 N; V *= E(1/2)
+        r, _ = self.rhs(u0)
+        u = [u0[i] + (dt / 2) * r[i] for i in range(3)]
+        u = self.E(u, 0.5, dt)
+        r = self.E(r, 1.0, dt)
+        tot = [(dt / 6) * r[i] for i in range(3)]
+        # stage 2: Single_time_step(dt, 1/2, 0, 1/2): V = E(1/2) u0 + dt/2 N
+        r, _ = self.rhs(u)
+        u = self.E(u0, 0.5, dt)
+        u = [u[i] + (dt / 2) * r[i] for i in range(3)]
+        r = self.E(r, 0.5, dt)
+        tot = [tot[i] + (dt / 3) * r[i] for i in range(3)]
+        # stage 3: Single_time_step(dt, 1, 1/2, 1): V = E(1/2)(E(1/2) u0 + dt N)
+        r, _ = self.rhs(u)
+        u = self.E(u0, 0.5, dt)
+        u = [u[i] + dt * r[i] for i in range(3)]
+        u = self.E(u, 0.5, dt)
+        r = self.E(r, 0.5, dt)
+        tot = [tot[i] + (dt / 3) * r[i] for i in range(3)]
+        # stage 4
+        r, _ = self.rhs(u)
+        tot = [tot[i] + (dt / 6) * r[i] for i in range(3)]
+        u = self.E(u0, 1.0, dt)
+        u = [u[i] + tot[i] for i in range(3)]
+        if self.alias == "DEALIAS":
+            u = [dealias(a, self.basis) for a in u]
+        return u, dt
+
+
+class MHDSolver(FluidSolver):
+    """The MHD loop of src/IMHD/IMHD_main.cc with Time_advance(IncVF& W)
+    time_advance_VF_MHD.cc:59-182: the same IF-RK4 with nu for U and eta for B; only U.nlin is
+    projected (Compute_pressure uses U's nlin), W.nlin -> -W.nlin (compute_rhs.cc:111-119)."""
+
+    def __init__(self, N, kfactor, nu, eta, Tdt, basis="FOUR", alias="DEALIAS"):
+        super().__init__(N, kfactor, nu, Tdt, basis, alias, None)
+        self.eta = eta
+
+    def rhs2(self, V, W):
+        un, bn = nlin_mhd(V, W, self.kfactor, self.basis, self.alias)
+        p = pressure(un, self.kfactor, self.basis, self.alias)
+        ru = rhs_from_nlin(un, p, self.kfactor, self.basis)
+        rb = [-b for b in bn]
+        return ru, rb
+
+    def Eb(self, V, a, dt):
+        return [exp_ksqr(v, -self.eta * a * dt, self.kfactor, self.basis) for v in V]
+
+    def step2(self, V, W):
+        E0 = sum(total_energy(v, self.basis) for v in V) + sum(total_energy(w, self.basis) for w in W)
+        kmax = max_radius_inside(self.N, self.kfactor, self.alias, self.basis)
+        dx = 2 * math.pi / kmax
+        dt = dx / (math.sqrt(E0) * 20)
+        B0sqr = sum(float(np.real(w[0, 0, 0])) ** 2 for w in W)
+        if B0sqr > MYEPS:
+            dt = min(dt, dx / (math.sqrt(B0sqr) * 20))
+        dt = min(dt, self.Tdt)
+        u0 = [v.copy() for v in V]
+        b0 = [w.copy() for w in W]
+        ru, rb = self.rhs2(u0, b0)
+        u = self.E([u0[i] + (dt / 2) * ru[i] for i in range(3)], 0.5, dt)
+        b = self.Eb([b0[i] + (dt / 2) * rb[i] for i in range(3)], 0.5, dt)
+        totu = [(dt / 6) * x for x in self.E(ru, 1.0, dt)]
+        totb = [(dt / 6) * x for x in self.Eb(rb, 1.0, dt)]
+        ru, rb = self.rhs2(u, b)
+        u = [x + (dt / 2) * y for x, y in zip(self.E(u0, 0.5, dt), ru)]
+        b = [x + (dt / 2) * y for x, y in zip(self.Eb(b0, 0.5, dt), rb)]
+        totu = [t + (dt / 3) * x for t, x in zip(totu, self.E(ru, 0.5, dt))]
+        totb = [t + (dt / 3) * x for t, x in zip(totb, self.Eb(rb, 0.5, dt))]
+        ru, rb = self.rhs2(u, b)
+        u = self.E([x + dt * y for x, y in zip(self.E(u0, 0.5, dt), ru)], 0.5, dt)
+        b = self.Eb([x + dt * y for x, y in zip(self.Eb(b0, 0.5, dt), rb)], 0.5, dt)
+        totu = [t + (dt / 3) * x for t, x in zip(totu, self.E(ru, 0.5, dt))]
+        totb = [t + (dt / 3) * x for t, x in zip(totb, self.Eb(rb, 0.5, dt))]
+        ru, rb = self.rhs2(u, b)
+        totu = [t + (dt / 6) * x for t, x in zip(totu, ru)]
+        totb = [t + (dt / 6) * x for t, x in zip(totb, rb)]
+        u = [x + t for x, t in zip(self.E(u0, 1.0, dt), totu)]
+        b = [x + t for x, t in zip(self.Eb(b0, 1.0, dt), totb)]
+        if self.alias == "DEALIAS":
+            u = [dealias(a, self.basis) for a in u]
+            b = [dealias(a, self.basis) for a in b]
+        return u, b, dt
+
+
+# --------------------------------------------------------------------------------------
+# Energy transfer: flux and shell-to-shell  (lib/IncFlow/EnergyTrdir, lib/four/four_ET.cc)
+# --------------------------------------------------------------------------------------
+
+def et_radii(N, kfactor, no_shells, alias="DEALIAS", basis="FOUR"):
+    """EnergyTr::EnergyTr shell radii, scheme 0  EnergyTr.cc:136-160:
+    R = {0, 2, 4, 8, 8 * 2^(s (i - 3)) for i = 4..S-3, R_in/2, R_in, INF}, s = log2(R_in/16)/(S-5)."""
+    S = no_shells
+    R_in = 1.0 * max_radius_inside(N, kfactor, alias, basis)
+    R = np.zeros(S + 1)
+    R[0], R[1], R[2], R[3] = 0.0, 2.0, 4.0, 8.0
+    R[S - 2] = R_in / 2
+    R[S - 1] = R_in
+    R[S] = INF_RADIUS
+    if S > 6:
+        s = math.log2(R_in / 16.0) / (S - 5)
+        for i in range(4, S - 2):
+            R[i] = 8 * 2.0 ** (s * (i - 3))
+    return R
+
+
+def fill_array_shell(A, inner, outer, kfactor, basis="FOUR"):
+    """Fill_array_shell  universal_ET.cc:45-65: B = A on inner < |K| <= outer, else 0."""
+    N = (A.shape[0], A.shape[1], 2 * (A.shape[2] - 1))
+    K = kmag(N, kfactor, basis)
+    return np.where((K > inner) & (K <= outer), A, 0)
+
+
+def et_nlin(V, G, kfactor, basis="FOUR"):
+    """IncVF::EnergyTr_Compute_nlin()  ET_compute_nlin.cc:85-120 with the ET products
+    (ET_RSprod.cc:49-169): N_i = D_j F(V_j G_i); not projected, not dealiased."""
+    N3 = 2 * (V[0].shape[2] - 1)
+    par_inv = (1, 0, 0)
+    vr = [inverse(V[i], basis, par_inv[i], N3) for i in range(3)]
+    gr = [inverse(G[i], basis, par_inv[i], N3) for i in range(3)]
+    n = [forward(vr[i] * gr[i], basis, 0) for i in range(3)]
+    n[0] = xderiv(n[0], kfactor, basis, 0)
+    n[1] = yderiv(n[1], kfactor)
+    n[2] = zderiv(n[2], kfactor)
+    v1 = forward(vr[0] * gr[1], basis, 1)   # V1r = V1 G2
+    g1 = forward(gr[0] * vr[1], basis, 1)   # G1  = G1 V2
+    v2 = forward(vr[1] * gr[2], basis, 0)   # V2r = V2 G3
+    g2 = forward(gr[1] * vr[2], basis, 0)   # G2  = G2 V3
+    v3 = forward(vr[2] * gr[0], basis, 1)   # V3r = V3 G1
+    g3 = forward(gr[2] * vr[0], basis, 1)   # G3  = G3 V1
+    # Derivative_RSprod_VV_ET  ET_RSprod.cc:155-168
+    n[0] = n[0] + yderiv(g1, kfactor) + zderiv(v3, kfactor)
+    n[1] = n[1] + xderiv(v1, kfactor, basis, 1) + zderiv(g2, kfactor)
+    n[2] = n[2] + xderiv(g3, kfactor, basis, 1) + yderiv(v2, kfactor)
+    return n
+
+
+def shell_mult_single(A, B, inner, outer, kfactor, basis="FOUR"):
+    """Shell_mult_single_FOUR  four_ET.cc:49-106: sum_{inner<|K|<=outer} 2 mult Re(A B*)."""
+    N = (A.shape[0], A.shape[1], 2 * (A.shape[2] - 1))
+    K = kmag(N, kfactor, basis)
+    mult = multiplicity(N, basis)
+    sel = (K > inner) & (K <= outer)
+    return float((2 * mult * np.real(A * np.conj(B)))[sel].sum())
+
+
+def shell_index(K, R):
+    """Get_shell_index  basis_basicfn.cc:288-299: first index with K <= R[index]."""
+    return np.searchsorted(R, K, side="left")
+
+
+def shell_mult_all(As, Bs, R, kfactor, alias="DEALIAS", basis="FOUR"):
+    """Shell_mult_all_FOUR (vector form)  four_ET.cc:181-256: for |K| <= kmax_inside,
+    result[shell_index(|K|)] += 2 mult Re(sum_i A_i B_i*).  Length S+1."""
+    A0 = As[0]
+    N = (A0.shape[0], A0.shape[1], 2 * (A0.shape[2] - 1))
+    K = kmag(N, kfactor, basis)
+    kin = max_radius_inside(N, kfactor, alias, basis)
+    mult = multiplicity(N, basis)
+    val = 2 * mult * sum(np.real(a * np.conj(b)) for a, b in zip(As, Bs))
+    sel = K <= kin
+    idx = shell_index(K[sel], R)
+    return np.bincount(idx, weights=val[sel], minlength=len(R))[: len(R)]
+
+
+def compute_flux(V, kfactor, no_shells, alias="DEALIAS", basis="FOUR"):
+    """IncVF::Compute_flux()  compute_flux.cc:52-69: for sphere s = 1..S, G = u on
+    0 < |K| <= R_s, flux(s) = -sum_{|K| > R_s} 2 mult Re(N(G) . u*).  Length S+1, [0] = 0."""
+    N = (V[0].shape[0], V[0].shape[1], 2 * (V[0].shape[2] - 1))
+    R = et_radii(N, kfactor, no_shells, alias, basis)
+    flux = np.zeros(no_shells + 1)
+    for s in range(1, no_shells + 1):
+        G = [fill_array_shell(v, 0.0, R[s], kfactor, basis) for v in V]
+        n = et_nlin(V, G, kfactor, basis)
+        flux[s] = -sum(shell_mult_single(n[i], V[i], R[s], INF_RADIUS, kfactor, basis) for i in range(3))
+    return flux
+
+
+def compute_shell_tr(V, kfactor, no_shells, alias="DEALIAS", basis="FOUR"):
+    """IncVF::Compute_shell_tr()  compute_shell_tr.cc:59-79: row n (1..S-1) = -Shell_mult_all of
+    N(u^(n)) against u, giver shell n = (R_{n-1}, R_n].  Shape (S+1, S+1)."""
+    N = (V[0].shape[0], V[0].shape[1], 2 * (V[0].shape[2] - 1))
+    R = et_radii(N, kfactor, no_shells, alias, basis)
+    T = np.zeros((no_shells + 1, no_shells + 1))
+    for n_ in range(1, no_shells):
+        G = [fill_array_shell(v, R[n_ - 1], R[n_], kfactor, basis) for v in V]
+        n = et_nlin(V, G, kfactor, basis)
+        T[n_, :] = -shell_mult_all(n, V, R, kfactor, alias, basis)
+    return T
+
+
+# --------------------------------------------------------------------------------------
+# Convenience: the reference's packed real layout (N1, N2, N3/2+1) complex <-> (N1, N2, N3)
+# --------------------------------------------------------------------------------------
+
+def pack_real(real):
+    """Real (N1,N2,N3) -> the reference's in-place layout: complex (N1,N2,N3/2+1) whose slot l3
+    holds (x[2 l3], x[2 l3 + 1]); the last slot is the zeroed padding (four_tr.cc:299-302)."""
+    N1, N2, N3 = real.shape
+    out = np.zeros((N1, N2, N3 // 2 + 1), dtype=np.complex128)
+    out[:, :, : N3 // 2] = real[:, :, 0::2] + 1j * real[:, :, 1::2]
+    return out
+
+
+def unpack_real(packed):
+    N1, N2, M1 = packed.shape
+    N3 = 2 * (M1 - 1)
+    out = np.empty((N1, N2, N3))
+    out[:, :, 0::2] = packed[:, :, : N3 // 2].real
+    out[:, :, 1::2] = packed[:, :, : N3 // 2].imag
+    return out

@@ -1,0 +1,68 @@
+// Common device/host helpers for the Tarang B200 hot path: a POD complex type whose layout
+// matches the reference's complex<double> (two reals, real part first), error plumbing and
+// the axis maps that describe which wavenumbers of an axis are stored.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+
+namespace tg {
+
+template <typename R>
+struct __align__(2 * sizeof(R)) cx {
+  R x, y;
+};
+
+template <typename R>
+__host__ __device__ __forceinline__ cx<R> mkc(R a, R b) {
+  cx<R> c;
+  c.x = a;
+  c.y = b;
+  return c;
+}
+template <typename R>
+__host__ __device__ __forceinline__ cx<R> operator+(cx<R> a, cx<R> b) { return mkc<R>(a.x + b.x, a.y + b.y); }
+template <typename R>
+__host__ __device__ __forceinline__ cx<R> operator-(cx<R> a, cx<R> b) { return mkc<R>(a.x - b.x, a.y - b.y); }
+template <typename R>
+__host__ __device__ __forceinline__ cx<R> operator*(cx<R> a, cx<R> b) {
+  return mkc<R>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <typename R>
+__host__ __device__ __forceinline__ cx<R> operator*(R s, cx<R> a) { return mkc<R>(s * a.x, s * a.y); }
+template <typename R>
+__host__ __device__ __forceinline__ cx<R> conjc(cx<R> a) { return mkc<R>(a.x, -a.y); }
+// multiply by (dir * i): dir = +1 -> i*a, dir = -1 -> -i*a
+template <int DIR, typename R>
+__host__ __device__ __forceinline__ cx<R> mul_i(cx<R> a) {
+  return DIR > 0 ? mkc<R>(-a.y, a.x) : mkc<R>(a.y, -a.x);
+}
+// i * a
+template <typename R>
+__host__ __device__ __forceinline__ cx<R> ione(cx<R> a) { return mkc<R>(-a.y, a.x); }
+// pointwise product of two packed-real values (Array_real_mult: re*re, im*im)
+template <typename R>
+__host__ __device__ __forceinline__ cx<R> rmul(cx<R> a, cx<R> b) { return mkc<R>(a.x * b.x, a.y * b.y); }
+
+template <typename Rd, typename Rs>
+__host__ __device__ __forceinline__ cx<Rd> cvt(cx<Rs> a) { return mkc<Rd>((Rd)a.x, (Rd)a.y); }
+
+// Which FFT indices of an axis of length L are stored: [0, lo) and [L - hi, L), in that order,
+// as rows 0 .. lo+hi-1.  A full axis has lo = L, hi = 0.
+struct AxisMap {
+  int L, lo, hi;
+};
+
+__host__ __device__ __forceinline__ int amap_row(const AxisMap& m, int n) {
+  if (n < m.lo) return n;
+  int off = m.L - m.hi;
+  if (n >= off) return n - off + m.lo;
+  return -1;
+}
+__host__ __device__ __forceinline__ int amap_index(const AxisMap& m, int r) {
+  return r < m.lo ? r : r - m.lo + (m.L - m.hi);
+}
+__host__ __device__ __forceinline__ int amap_count(const AxisMap& m) { return m.lo + m.hi; }
+
+}  // namespace tg

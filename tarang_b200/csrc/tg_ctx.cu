@@ -1,0 +1,1169 @@
+// Solver context: geometry, device buffers, the nonlinear-term pipeline, the fused RK4 step
+// and the C ABI entry points of include/tarang_gpu.h (except energy transfer and serving).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "tg_ctx.h"
+
+using namespace tg;
+
+namespace tg {
+
+int set_err(tg_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+int cuda_err(tg_ctx* c, cudaError_t e, const char* where) {
+  if (e == cudaSuccess) return TG_OK;
+  std::string m = std::string(where) + ": " + cudaGetErrorString(e);
+  if (e == cudaErrorMemoryAllocation) return set_err(c, TG_ERR_OOM, m);
+  return set_err(c, TG_ERR_CUDA, m);
+}
+
+}  // namespace tg
+
+#define TG_CK(call)                                        \
+  do {                                                     \
+    cudaError_t _e = (call);                               \
+    if (_e != cudaSuccess) return cuda_err(c, _e, #call);  \
+  } while (0)
+
+namespace {
+
+// Device table exp(-2 pi i m / L), m in [0, L), evaluated in long double and rounded.
+int make_twiddles(tg_ctx* c, int L) {
+  if (L <= 0 || c->tw.count(L)) return TG_OK;
+  std::vector<cx<double>> h(L);
+  const long double two_pi = 6.283185307179586476925286766559005768L;
+  for (int m = 0; m < L; ++m) {
+    const long double ang = two_pi * (long double)m / (long double)L;
+    h[m].x = (double)cosl(ang);
+    h[m].y = (double)(-sinl(ang));
+  }
+  cx<double>* d = nullptr;
+  TG_CK(cudaMalloc(&d, sizeof(cx<double>) * L));
+  c->bytes += sizeof(cx<double>) * L;
+  TG_CK(cudaMemcpy(d, h.data(), sizeof(cx<double>) * L, cudaMemcpyHostToDevice));
+  c->tw[L] = d;
+  return TG_OK;
+}
+
+int dalloc(tg_ctx* c, void** p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(c, TG_ERR_OOM, "device allocation of " + std::to_string(bytes) + " bytes failed");
+  }
+  c->bytes += bytes;
+  e = cudaMemsetAsync(*p, 0, bytes, c->st);
+  if (e != cudaSuccess) return cuda_err(c, e, "cudaMemsetAsync");
+  return TG_OK;
+}
+
+// Stored wavenumbers of one axis under the 2/3 rule (Dealias_array universal_misc.cc:118-159)
+void keep_axis(int N, int axis, int basis, int dealias, int& lo, int& hi) {
+  lo = N;
+  hi = 0;
+  if (!dealias || N < 3) return;
+  if (axis == 0) {
+    if (basis == TG_FOUR) {
+      lo = N / 3;          // kx = 0 .. N/3-1
+      hi = N / 3 - 1;      // kx = -(N/3-1) .. -1
+    } else {
+      lo = 2 * N / 3;      // m = 0 .. 2N/3-1
+      hi = 0;
+    }
+  } else {
+    lo = N / 3;                      // l2 = 0 .. N/3-1
+    hi = N - (2 * N / 3 + 2);        // l2 = 2N/3+2 .. N-1
+    if (hi < 0) hi = 0;
+  }
+  if (hi < 0) hi = 0;
+}
+
+AxisMap full_map(int L) { return AxisMap{L, L, 0}; }
+
+// ------------------------------------------------------------------ profiling scopes
+cudaEvent_t prof_event(tg_ctx* c) {
+  if (!c->ev_pool.empty()) {
+    cudaEvent_t e = c->ev_pool.back();
+    c->ev_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+struct Prof {
+  tg_ctx* c;
+  long idx = -1;
+  Prof(tg_ctx* c_, const char* name, double bytes) : c(c_) {
+    if (!c->prof) return;
+    tg_ctx::ProfRec r{name, prof_event(c), prof_event(c), bytes};
+    cudaEventRecord(r.a, c->st);
+    c->prof_recs.push_back(r);
+    idx = (long)c->prof_recs.size() - 1;
+  }
+  ~Prof() {
+    if (idx >= 0) cudaEventRecord(c->prof_recs[idx].b, c->st);
+  }
+};
+
+// elements on the stored support of each pipeline stage layout (kz counted to nkz)
+double el_compact(const tg_ctx* c) { return (double)c->g.nkx * c->g.nky * c->g.nkz; }
+double el_xstage(const tg_ctx* c) { return (double)c->N1 * c->g.nky * c->g.nkz; }
+double el_ystage(const tg_ctx* c) { return (double)c->N1 * c->N2 * c->g.nkz; }
+
+int max_radius_inside(const tg_ctx* c) {
+  // Max_radius_inside_(de)aliased_FOUR four_inline.h:190-257
+  const int d = c->cfg.dealias ? 3 : 2;
+  const double* kf = c->cfg.kfactor;
+  double km;
+  if (c->basis == TG_FOUR) {
+    km = std::min((c->N1 / d) * kf[0], (c->N2 / d) * kf[1]);
+    if (c->N3 > 2) km = std::min(km, (c->N3 / d) * kf[2]);
+  } else {
+    const int nx = c->cfg.dealias ? (2 * c->N1 / 3) : c->N1;
+    km = std::min(nx * kf[0], (c->N2 / d) * kf[1]);
+    if (c->N3 > 2) km = std::min(km, (c->N3 / d) * kf[2]);
+  }
+  return (int)km;
+}
+
+// ------------------------------------------------------------------ pipeline
+// X-inverse, Y-inverse, fused z-pass (c2r, products, r2c), Y-forward, X-forward.
+// inputs: compact fields of precision inprec.  MHD: in[0..2] = U, in[3..5] = B, the x-pass
+// forms z+ = U + B (fields 0..2) and z- = U - B (fields 3..5).
+int run_pipeline(tg_ctx* c, const void* const* in, int inprec) {
+  if (!c->pipeline_ok) return set_err(c, TG_ERR_UNSUPPORTED, "nonlinear term needs N3/2 a power of two in [4, 256]");
+  const Geo& g = c->g;
+  const int nin = c->nin, np = c->nprod;
+  // x inverse
+  {
+    AxisLaunch l;
+    l.L = c->N1;
+    l.dir = +1;
+    l.pin = inprec;
+    l.pout = c->tprec;
+    l.pwork = c->tprec;
+    l.nbatch = 1;
+    l.nfields = nin;
+    l.a.sb = 0;
+    l.a.sr = (long long)g.nky * g.kzp;
+    l.a.db = 0;
+    l.a.dr = (long long)g.nky * g.kzp;
+    l.a.ncols = g.nky * g.kzp;
+    l.a.in = g.ax;
+    l.a.out = full_map(c->N1);
+    l.a.scale = 1.0;
+    l.a.tw = c->tw[c->N1];
+    for (int f = 0; f < nin; ++f) {
+      l.ps.dst[f] = c->WX[f];
+      if (c->phys == TG_MHD) {
+        l.ps.src[f] = in[f % 3];
+        l.ps.src2[f] = in[3 + f % 3];
+        l.a.comb[f] = f < 3 ? +1 : -1;
+      } else {
+        l.ps.src[f] = in[f];
+        l.a.comb[f] = 0;
+      }
+    }
+    const double insz = inprec == F64 ? 16.0 : 8.0;
+    Prof pr(c, "x_inverse", c->nstate * el_compact(c) * insz + nin * el_xstage(c) * c->tsz);
+    TG_CK(launch_axis(l, c->st));
+  }
+  // y inverse
+  {
+    AxisLaunch l;
+    l.L = c->N2;
+    l.dir = +1;
+    l.pin = l.pout = l.pwork = c->tprec;
+    l.nbatch = c->N1;
+    l.nfields = nin;
+    l.a.sb = (long long)g.nky * g.kzp;
+    l.a.sr = g.kzp;
+    l.a.db = (long long)c->N2 * g.kzp;
+    l.a.dr = g.kzp;
+    l.a.ncols = g.kzp;
+    l.a.in = g.ay;
+    l.a.out = full_map(c->N2);
+    l.a.scale = 1.0;
+    l.a.tw = c->tw[c->N2];
+    for (int f = 0; f < nin; ++f) {
+      l.ps.src[f] = c->WX[f];
+      l.ps.dst[f] = c->WY[f];
+    }
+    Prof pr(c, "y_inverse", nin * (el_xstage(c) + el_ystage(c)) * c->tsz);
+    TG_CK(launch_axis(l, c->st));
+  }
+  // z: inverse, products, forward
+  {
+    ZProdLaunch l;
+    l.M = c->Mz;
+    l.nin = nin;
+    l.nprod = np;
+    l.pin = l.pout = l.pwork = c->tprec;
+    l.a.nrows = (long long)c->N1 * c->N2;
+    l.a.ss = g.kzp;
+    l.a.ds = g.kzp;
+    l.a.nin = g.nkz;
+    l.a.nout = g.nkz;
+    l.a.nfill = g.kzp;
+    l.a.pad = 0;
+    l.a.scale = 1.0 / ((double)c->N1 * c->N2 * c->N3);
+    l.a.twM = c->tw[c->Mz];
+    l.a.twN = c->tw[c->N3];
+    for (int f = 0; f < nin; ++f) l.ps.src[f] = c->WY[f];
+    for (int q = 0; q < np; ++q) l.ps.dst[q] = c->PP[q];
+    l.pp = c->pairs;
+    Prof pr(c, "z_products", (nin + np) * el_ystage(c) * c->tsz);
+    TG_CK(launch_zprod(l, c->st));
+  }
+  // y forward
+  {
+    AxisLaunch l;
+    l.L = c->N2;
+    l.dir = -1;
+    l.pin = l.pout = l.pwork = c->tprec;
+    l.nbatch = c->N1;
+    l.nfields = np;
+    l.a.sb = (long long)c->N2 * g.kzp;
+    l.a.sr = g.kzp;
+    l.a.db = (long long)g.nky * g.kzp;
+    l.a.dr = g.kzp;
+    l.a.ncols = g.kzp;
+    l.a.in = full_map(c->N2);
+    l.a.out = g.ay;
+    l.a.scale = 1.0;
+    l.a.tw = c->tw[c->N2];
+    for (int q = 0; q < np; ++q) {
+      l.ps.src[q] = c->PP[q];
+      l.ps.dst[q] = c->PY[q];
+    }
+    Prof pr(c, "y_forward", np * (el_ystage(c) + el_xstage(c)) * c->tsz);
+    TG_CK(launch_axis(l, c->st));
+  }
+  // x forward
+  {
+    AxisLaunch l;
+    l.L = c->N1;
+    l.dir = -1;
+    l.pin = l.pout = l.pwork = c->tprec;
+    l.nbatch = 1;
+    l.nfields = np;
+    l.a.sb = 0;
+    l.a.sr = (long long)g.nky * g.kzp;
+    l.a.db = 0;
+    l.a.dr = (long long)g.nky * g.kzp;
+    l.a.ncols = g.nky * g.kzp;
+    l.a.in = full_map(c->N1);
+    l.a.out = g.ax;
+    l.a.scale = 1.0;
+    l.a.tw = c->tw[c->N1];
+    for (int q = 0; q < np; ++q) {
+      l.ps.src[q] = c->PY[q];
+      l.ps.dst[q] = c->PX[q];
+    }
+    Prof pr(c, "x_forward", np * (el_xstage(c) + el_compact(c)) * c->tsz);
+    TG_CK(launch_axis(l, c->st));
+  }
+  return TG_OK;
+}
+
+int run_force(tg_ctx* c, const void* const* U, int uprec) {
+  if (!c->force_on) return TG_OK;
+  ForceArgs f{};
+  f.g = c->g;
+  for (int i = 0; i < 3; ++i) f.U[i] = U[i];
+  f.uprec = uprec;
+  f.fx = c->fx;
+  f.fy = c->fy;
+  f.fz = c->fz;
+  f.inner = c->cfg.force_para[0];
+  f.outer = c->cfg.force_para[1];
+  f.e_per_mode = c->nf_modes > 0 ? c->cfg.force_para[2] / c->nf_modes : 0.0;
+  f.eps_h = c->cfg.force_para[3];
+  f.FB = c->FB;
+  Prof pr(c, "force", 0.0);
+  TG_CK(launch_force_supply(f, c->st));
+  return TG_OK;
+}
+
+RKArgs rk_args(tg_ctx* c, int stage) {
+  RKArgs a{};
+  a.g = c->g;
+  a.stage = stage;
+  a.nstate = c->nstate;
+  for (int i = 0; i < 6; ++i) {
+    a.nu[i] = c->nu_of[i];
+    a.U0[i] = c->U0[i];
+    a.TOT[i] = c->TOT[i];
+    a.US[i] = c->US[i];
+    a.RHS[i] = c->NL[i];
+  }
+  for (int q = 0; q < 9; ++q) a.PX[q] = c->PX[q];
+  a.dt = c->scal;
+  a.FB = c->force_on ? c->FB : nullptr;
+  a.fx = c->fx;
+  a.fy = c->fy;
+  a.fz = c->fz;
+  a.part = (stage == 4) ? c->part : nullptr;
+  return a;
+}
+
+int run_finalize(tg_ctx* c, int dt_mode, bool ring) {
+  FinalizeArgs f{};
+  f.part = c->part;
+  f.nblocks = c->npart_blocks;
+  f.nslots = 8;
+  f.out = c->red_out;
+  f.scal = c->scal;
+  f.ering = ring ? c->ering : nullptr;
+  f.ering_pos = c->ering_pos;
+  f.dt_mode = dt_mode;
+  f.dx = c->dx_cfl;
+  f.Tdt = c->cfg.dt;
+  f.mhd = (c->phys == TG_MHD);
+  if (f.mhd) {
+    // mean field B0 = real(B(0,0,0)) (compute_dt.cc:86-93): compact index 0 is the origin
+    for (int i = 0; i < 3; ++i) f.B0[i] = c->U0[3 + i];
+  }
+  Prof pr(c, "finalize", 0.0);
+  TG_CK(launch_finalize(f, c->st));
+  return TG_OK;
+}
+
+// energy partials of the master state into slots (U: 0,1; B: 2,3; T: 4,5) + finalize
+int run_energy(tg_ctx* c, int dt_mode) {
+  TG_CK(cudaMemsetAsync(c->part, 0, sizeof(double) * 8 * (size_t)c->npart_blocks, c->st));
+  int nb = 0;
+  const cx<double>* F[3] = {c->U0[0], c->U0[1], c->U0[2]};
+  TG_CK(launch_energy_partials(c->g, F, 3, c->part, 0, 8, c->st, &nb));
+  if (c->phys == TG_MHD) {
+    const cx<double>* B[3] = {c->U0[3], c->U0[4], c->U0[5]};
+    TG_CK(launch_energy_partials(c->g, B, 3, c->part, 2, 8, c->st, &nb));
+  } else if (c->phys == TG_SCALAR || c->phys == TG_RB) {
+    const cx<double>* T[1] = {c->U0[3]};
+    TG_CK(launch_energy_partials(c->g, T, 1, c->part, 4, 8, c->st, &nb));
+  }
+  return run_finalize(c, dt_mode, false);
+}
+
+int ensure_dt(tg_ctx* c) {
+  if (c->energy_valid) return TG_OK;
+  int rc = run_energy(c, 2);
+  if (rc) return rc;
+  c->energy_valid = true;
+  return TG_OK;
+}
+
+// stages 2..4 (or 1..4) of the RK4 step on the fused path; `ring` records the step's energy
+int run_stages(tg_ctx* c, int first_stage, bool ring) {
+  for (int stage = first_stage; stage <= 4; ++stage) {
+    const void* in[6];
+    int inprec;
+    if (stage == 1) {
+      for (int i = 0; i < c->nstate; ++i) in[i] = c->U0[i];
+      inprec = F64;
+    } else {
+      for (int i = 0; i < c->nstate; ++i) in[i] = c->US[i];
+      inprec = c->tprec;
+    }
+    int rc = run_force(c, in, inprec);
+    if (rc) return rc;
+    rc = run_pipeline(c, in, inprec);
+    if (rc) return rc;
+    RKArgs a = rk_args(c, stage);
+    {
+      const double ns = c->nstate, e = el_compact(c);
+      const double rd = c->nprod * e * c->tsz + ns * e * 16 + (stage > 1 ? ns * e * 16 : 0);
+      const double wr = (stage < 4) ? ns * e * (c->tsz + 16) : ns * e * 16;
+      Prof pr(c, "rk_stage", rd + wr);
+      TG_CK(launch_rk(a, c->phys, c->tprec, c->tprec, 0, c->st, nullptr));
+    }
+  }
+  return run_finalize(c, 1, ring);
+}
+
+int enqueue_step(tg_ctx* c) { return run_stages(c, 1, true); }
+
+int field_state_index(const tg_ctx* c, int field) {
+  if (field >= TG_V1 && field <= TG_V3) return field - TG_V1;
+  if (field >= TG_W1 && field <= TG_W3 && c->phys == TG_MHD) return 3 + field - TG_W1;
+  if (field == TG_T && (c->phys == TG_SCALAR || c->phys == TG_RB)) return 3;
+  return -1;
+}
+int field_nl_index(const tg_ctx* c, int field) {
+  if (field >= TG_NLIN1 && field <= TG_NLIN3) return field - TG_NLIN1;
+  if (field >= TG_WNLIN1 && field <= TG_WNLIN3 && c->phys == TG_MHD) return 3 + field - TG_WNLIN1;
+  if (field == TG_TNLIN && (c->phys == TG_SCALAR || c->phys == TG_RB)) return 3;
+  return -1;
+}
+
+int ensure_dense(tg_ctx* c, int field) {
+  if (c->dense[field]) return TG_OK;
+  void* p = nullptr;
+  int rc = dalloc(c, &p, sizeof(cx<double>) * (size_t)c->D);
+  if (rc) return rc;
+  c->dense[field] = (cx<double>*)p;
+  return TG_OK;
+}
+int ensure_staging(tg_ctx* c) {
+  if (c->staging) return TG_OK;
+  void* p = nullptr;
+  int rc = dalloc(c, &p, sizeof(cx<double>) * (size_t)c->D);
+  if (rc) return rc;
+  c->staging = (cx<double>*)p;
+  return TG_OK;
+}
+
+// dense FOUR transforms of a work field, in place (ArrayFFT_FOUR / ArrayIFFT_FOUR)
+int dense_transform(tg_ctx* c, cx<double>* f, int forward) {
+  const int wp = (c->prec == TG_FP64) ? F64 : F32;
+  const long long M3 = c->M3;
+  if (forward) {
+    ZLaunch z;
+    z.M = c->Mz;
+    z.kind = 1;
+    z.pin = F64;
+    z.pout = F64;
+    z.pwork = wp;
+    z.a.nrows = (long long)c->N1 * c->N2;
+    z.a.ss = M3;
+    z.a.ds = M3;
+    z.a.nout = (int)M3;
+    z.a.nfill = (int)M3;
+    z.a.scale = 1.0 / ((double)c->N1 * c->N2 * c->N3);
+    z.a.twM = c->tw[c->Mz];
+    z.a.twN = c->tw[c->N3];
+    z.ps.src[0] = f;
+    z.ps.dst[0] = f;
+    TG_CK(launch_z(z, c->st));
+  }
+  for (int pass = 0; pass < 2; ++pass) {
+    // inverse: x then y; forward: y then x
+    const bool xpass = forward ? (pass == 1) : (pass == 0);
+    AxisLaunch l;
+    l.dir = forward ? -1 : +1;
+    l.pin = F64;
+    l.pout = F64;
+    l.pwork = wp;
+    l.nfields = 1;
+    l.a.scale = 1.0;
+    l.ps.src[0] = f;
+    l.ps.dst[0] = f;
+    if (xpass) {
+      l.L = c->N1;
+      l.nbatch = 1;
+      l.a.sb = l.a.db = 0;
+      l.a.sr = l.a.dr = (long long)c->N2 * M3;
+      l.a.ncols = (int)(c->N2 * M3);
+      l.a.in = l.a.out = full_map(c->N1);
+      l.a.tw = c->tw[c->N1];
+    } else {
+      l.L = c->N2;
+      l.nbatch = c->N1;
+      l.a.sb = l.a.db = (long long)c->N2 * M3;
+      l.a.sr = l.a.dr = M3;
+      l.a.ncols = (int)M3;
+      l.a.in = l.a.out = full_map(c->N2);
+      l.a.tw = c->tw[c->N2];
+    }
+    TG_CK(launch_axis(l, c->st));
+  }
+  if (!forward) {
+    ZLaunch z;
+    z.M = c->Mz;
+    z.kind = 0;
+    z.pin = F64;
+    z.pout = F64;
+    z.pwork = wp;
+    z.a.nrows = (long long)c->N1 * c->N2;
+    z.a.ss = M3;
+    z.a.ds = M3;
+    z.a.nin = (int)M3;
+    z.a.pad = 1;
+    z.a.scale = 1.0;
+    z.a.twM = c->tw[c->Mz];
+    z.a.twN = c->tw[c->N3];
+    z.ps.src[0] = f;
+    z.ps.dst[0] = f;
+    TG_CK(launch_z(z, c->st));
+  }
+  return TG_OK;
+}
+
+void free_ctx(tg_ctx* c) {
+  if (!c) return;
+  if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+  auto fr = [](void* p) {
+    if (p) cudaFree(p);
+  };
+  for (auto& kv : c->tw) fr(kv.second);
+  for (int i = 0; i < 6; ++i) {
+    fr(c->U0[i]);
+    fr(c->TOT[i]);
+    fr(c->US[i]);
+    fr(c->NL[i]);
+    fr(c->WX[i]);
+    fr(c->WY[i]);
+  }
+  for (int i = 0; i < 9; ++i) {
+    fr(c->PP[i]);
+    fr(c->PY[i]);
+    fr(c->PX[i]);
+  }
+  fr(c->PR);
+  fr(c->FB);
+  fr(c->scal);
+  fr(c->red_out);
+  fr(c->part);
+  fr(c->ering);
+  fr(c->ering_pos);
+  fr(c->diag);
+  for (int i = 0; i < TG_NFIELDS; ++i) fr(c->dense[i]);
+  fr(c->staging);
+  for (auto& r : c->prof_recs) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  for (auto e : c->ev_pool) cudaEventDestroy(e);
+  if (c->h_pinned) cudaFreeHost(c->h_pinned);
+  if (c->own_stream && c->st) cudaStreamDestroy(c->st);
+  delete c;
+}
+
+// Get_number_modes_in_shell_FOUR (four_basic.cc:48-105): inner <= |K| < outer, kz = 0 once,
+// kz > 0 twice
+int count_force_modes(const tg_config& cfg) {
+  const double inner = cfg.force_para[0], outer = cfg.force_para[1];
+  const int kxm = (int)std::ceil(outer / cfg.kfactor[0]);
+  const int kym = (int)std::ceil(outer / cfg.kfactor[1]);
+  const int kzm = (int)std::ceil(outer / cfg.kfactor[2]);
+  int cnt = 0;
+  for (int kx = -kxm; kx <= kxm; ++kx)
+    for (int ky = -kym; ky <= kym; ++ky)
+      for (int kz = 0; kz <= kzm; ++kz) {
+        const double a = kx * cfg.kfactor[0], b = ky * cfg.kfactor[1], d = kz * cfg.kfactor[2];
+        const double km = std::sqrt(a * a + b * b + d * d);
+        if (km >= inner && km < outer) cnt += (kz == 0) ? 1 : 2;
+      }
+  return cnt;
+}
+
+}  // namespace
+
+// =====================================================================================
+// C ABI
+// =====================================================================================
+extern "C" {
+
+void tg_config_default(tg_config* cfg) {
+  if (!cfg) return;
+  std::memset(cfg, 0, sizeof(*cfg));
+  cfg->N[0] = cfg->N[1] = cfg->N[2] = 64;
+  cfg->basis = TG_FOUR;
+  cfg->physics = TG_FLUID;
+  cfg->precision = TG_FP64;
+  cfg->dealias = 1;
+  cfg->scheme = TG_RK4;
+  cfg->kfactor[0] = cfg->kfactor[1] = cfg->kfactor[2] = 1.0;
+  cfg->nu = 0.01;
+  cfg->eta = 0.01;
+  cfg->kappa = 0.01;
+  cfg->dt = 1e-3;
+  cfg->force_kind = TG_FORCE_DECAY;
+  cfg->n_shells = 12;
+  cfg->device = 0;
+  cfg->stream = nullptr;
+}
+
+const char* tg_last_error(const tg_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int tg_ctx_create(const tg_config* cfg, tg_ctx** out) {
+  if (!cfg || !out) return TG_ERR_ARG;
+  *out = nullptr;
+  const int N1 = cfg->N[0], N2 = cfg->N[1], N3 = cfg->N[2];
+  if (N1 < 2 || N2 < 2 || N3 < 4 || (N3 & 1)) return TG_ERR_ARG;
+  if (cfg->basis != TG_FOUR) return TG_ERR_UNSUPPORTED;
+  if (cfg->physics != TG_FLUID && cfg->physics != TG_MHD && cfg->physics != TG_SCALAR) return TG_ERR_UNSUPPORTED;
+  if (cfg->precision != TG_FP64 && cfg->precision != TG_FP32_MIXED) return TG_ERR_ARG;
+  if (cfg->scheme != TG_RK4) return TG_ERR_UNSUPPORTED;
+  if (cfg->force_kind != TG_FORCE_DECAY && cfg->force_kind != TG_FORCE_ENERGY_SUPPLY) return TG_ERR_UNSUPPORTED;
+  if (cfg->force_kind == TG_FORCE_ENERGY_SUPPLY && cfg->physics != TG_FLUID) return TG_ERR_UNSUPPORTED;
+  for (int i = 0; i < 3; ++i)
+    if (!(cfg->kfactor[i] > 0)) return TG_ERR_ARG;
+  if (!(cfg->dt > 0)) return TG_ERR_ARG;
+  // the fused product z-pass needs N3/2 in {4..256} (a power of two); other grids get the
+  // transform API only.  The x and y passes take any length.
+  const int Mz = N3 / 2;
+  const bool pipeline_ok = is_pow2(Mz) && Mz >= 4 && Mz <= 256;
+
+  tg_ctx* c = new tg_ctx();
+  c->cfg = *cfg;
+  c->dev = cfg->device;
+  cudaError_t e = cudaSetDevice(c->dev);
+  if (e != cudaSuccess) {
+    delete c;
+    return TG_ERR_CUDA;
+  }
+  if (cfg->stream) {
+    c->st = (cudaStream_t)cfg->stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) {
+      delete c;
+      return TG_ERR_CUDA;
+    }
+    c->own_stream = true;
+  }
+  c->pipeline_ok = pipeline_ok;
+  c->N1 = N1;
+  c->N2 = N2;
+  c->N3 = N3;
+  c->M3 = N3 / 2 + 1;
+  c->Mz = Mz;
+  c->phys = cfg->physics;
+  c->basis = cfg->basis;
+  c->prec = cfg->precision;
+  c->tprec = (c->prec == TG_FP64) ? F64 : F32;
+  c->tsz = (c->tprec == F64) ? sizeof(cx<double>) : sizeof(cx<float>);
+  int lo, hi;
+  Geo& g = c->g;
+  g.N1 = N1;
+  g.N2 = N2;
+  g.N3 = N3;
+  keep_axis(N1, 0, c->basis, cfg->dealias, lo, hi);
+  g.ax = AxisMap{N1, lo, hi};
+  keep_axis(N2, 1, c->basis, cfg->dealias, lo, hi);
+  g.ay = AxisMap{N2, lo, hi};
+  g.nkx = amap_count(g.ax);
+  g.nky = amap_count(g.ay);
+  g.nkz = (cfg->dealias && N3 >= 3) ? N3 / 3 : N3 / 2 + 1;
+  g.kzp = (g.nkz + 7) / 8 * 8;
+  g.S = (long long)g.nkx * g.nky * g.kzp;
+  g.kf0 = cfg->kfactor[0];
+  g.kf1 = cfg->kfactor[1];
+  g.kf2 = cfg->kfactor[2];
+  g.basis = c->basis;
+  c->S = g.S;
+  c->D = (long long)N1 * N2 * c->M3;
+
+  // physics layout of the pipeline
+  ProdPairs& pp = c->pairs;
+  if (c->phys == TG_FLUID) {
+    c->nstate = 3;
+    c->nin = 3;
+    c->nprod = 6;
+    const signed char A[6] = {0, 1, 2, 0, 1, 2}, B[6] = {0, 1, 2, 1, 2, 0};
+    for (int q = 0; q < 6; ++q) {
+      pp.a[q] = A[q];
+      pp.b[q] = B[q];
+    }
+    for (int i = 0; i < 3; ++i) c->nu_of[i] = cfg->nu;
+  } else if (c->phys == TG_MHD) {
+    c->nstate = 6;
+    c->nin = 6;
+    c->nprod = 9;
+    // inputs 0..2 = z+, 3..5 = z-
+    const signed char A[9] = {0, 1, 2, 0, 3, 1, 4, 2, 5}, B[9] = {3, 4, 5, 4, 1, 5, 2, 3, 0};
+    for (int q = 0; q < 9; ++q) {
+      pp.a[q] = A[q];
+      pp.b[q] = B[q];
+    }
+    for (int i = 0; i < 3; ++i) {
+      c->nu_of[i] = cfg->nu;
+      c->nu_of[3 + i] = cfg->eta;
+    }
+  } else {
+    c->nstate = 4;
+    c->nin = 4;
+    c->nprod = 9;
+    const signed char A[9] = {0, 1, 2, 0, 1, 2, 0, 1, 2}, B[9] = {0, 1, 2, 1, 2, 0, 3, 3, 3};
+    for (int q = 0; q < 9; ++q) {
+      pp.a[q] = A[q];
+      pp.b[q] = B[q];
+    }
+    for (int i = 0; i < 3; ++i) c->nu_of[i] = cfg->nu;
+    c->nu_of[3] = cfg->kappa;
+  }
+
+  int rc = TG_OK;
+  auto fail = [&](int code) {
+    std::string m = c->err;
+    free_ctx(c);
+    return code;
+  };
+  for (int L : {N1, N2, Mz, N3}) {
+    rc = make_twiddles(c, L);
+    if (rc) return fail(rc);
+  }
+  const size_t Sd = sizeof(cx<double>) * (size_t)g.S;
+  const size_t St = c->tsz * (size_t)g.S;
+  const size_t WXb = c->tsz * (size_t)N1 * g.nky * g.kzp;
+  const size_t WYb = c->tsz * (size_t)N1 * N2 * g.kzp;
+  for (int i = 0; i < c->nstate; ++i) {
+    if ((rc = dalloc(c, (void**)&c->U0[i], Sd))) return fail(rc);
+    if ((rc = dalloc(c, (void**)&c->TOT[i], Sd))) return fail(rc);
+    if ((rc = dalloc(c, &c->US[i], St))) return fail(rc);
+    if ((rc = dalloc(c, (void**)&c->NL[i], Sd))) return fail(rc);
+  }
+  if ((rc = dalloc(c, (void**)&c->PR, Sd))) return fail(rc);
+  for (int i = 0; i < c->nin; ++i) {
+    if ((rc = dalloc(c, &c->WX[i], WXb))) return fail(rc);
+    if ((rc = dalloc(c, &c->WY[i], WYb))) return fail(rc);
+  }
+  for (int q = 0; q < c->nprod; ++q) {
+    if ((rc = dalloc(c, &c->PP[q], WYb))) return fail(rc);
+    if ((rc = dalloc(c, &c->PY[q], WXb))) return fail(rc);
+    if ((rc = dalloc(c, &c->PX[q], St))) return fail(rc);
+  }
+  c->npart_blocks = (int)((g.S + 255) / 256);
+  if ((rc = dalloc(c, (void**)&c->part, sizeof(double) * 8 * (size_t)c->npart_blocks))) return fail(rc);
+  if ((rc = dalloc(c, (void**)&c->scal, sizeof(double) * 8))) return fail(rc);
+  if ((rc = dalloc(c, (void**)&c->red_out, sizeof(double) * 8))) return fail(rc);
+  c->ering_cap = 1 << 16;
+  if ((rc = dalloc(c, (void**)&c->ering, sizeof(double) * c->ering_cap))) return fail(rc);
+  if ((rc = dalloc(c, (void**)&c->ering_pos, sizeof(int) * 4))) return fail(rc);
+  if (cudaMallocHost(&c->h_pinned, sizeof(double) * 1024) != cudaSuccess) return fail(TG_ERR_OOM);
+  {
+    double init[8] = {cfg->dt, 0, 0, 0, 0, 0, 0, 0};
+    e = cudaMemcpyAsync(c->scal, init, sizeof(init), cudaMemcpyHostToDevice, c->st);
+    if (e != cudaSuccess) return fail(cuda_err(c, e, "init scalars"));
+  }
+  c->dx_cfl = 2 * M_PI / std::max(1, max_radius_inside(c));
+  if (cfg->force_kind == TG_FORCE_ENERGY_SUPPLY) {
+    c->force_on = 1;
+    const double outer = cfg->force_para[1];
+    c->fx = (int)std::ceil(outer / cfg->kfactor[0]);
+    c->fy = (int)std::ceil(outer / cfg->kfactor[1]);
+    c->fz = (int)std::ceil(outer / cfg->kfactor[2]);
+    c->fbox = (2 * c->fx + 1) * (2 * c->fy + 1) * (c->fz + 1);
+    c->nf_modes = count_force_modes(*cfg);
+    if (c->nf_modes <= 0) return fail(set_err(c, TG_ERR_ARG, "forcing shell holds no modes"));
+    if ((rc = dalloc(c, (void**)&c->FB, sizeof(cx<double>) * 3 * (size_t)c->fbox))) return fail(rc);
+  }
+  e = cudaStreamSynchronize(c->st);
+  if (e != cudaSuccess) return fail(cuda_err(c, e, "create"));
+  *out = c;
+  return TG_OK;
+}
+
+int tg_ctx_destroy(tg_ctx* c) {
+  if (!c) return TG_ERR_ARG;
+  cudaSetDevice(c->dev);
+  cudaStreamSynchronize(c->st);
+  free_ctx(c);
+  return TG_OK;
+}
+
+int tg_synchronize(tg_ctx* c) {
+  if (!c) return TG_ERR_ARG;
+  TG_CK(cudaStreamSynchronize(c->st));
+  return TG_OK;
+}
+
+int tg_device_bytes(const tg_ctx* c, size_t* bytes) {
+  if (!c || !bytes) return TG_ERR_ARG;
+  *bytes = c->bytes;
+  return TG_OK;
+}
+
+int tg_field_upload(tg_ctx* c, int field, const double* host, size_t n) {
+  if (!c || !host || field < 0 || field >= TG_NFIELDS) return TG_ERR_ARG;
+  if (n != 2 * (size_t)c->D) return set_err(c, TG_ERR_ARG, "upload: n_doubles must be 2*N1*N2*(N3/2+1)");
+  cudaSetDevice(c->dev);
+  const int si = field_state_index(c, field);
+  const int ni = field_nl_index(c, field);
+  if (field >= TG_WORK0 && field < TG_WORK0 + TG_NWORK) {
+    int rc = ensure_dense(c, field);
+    if (rc) return rc;
+    TG_CK(cudaMemcpyAsync(c->dense[field], host, sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
+    TG_CK(cudaStreamSynchronize(c->st));
+    return TG_OK;
+  }
+  cx<double>* target = nullptr;
+  if (si >= 0) target = c->U0[si];
+  else if (ni >= 0) target = c->NL[ni];
+  else if (field == TG_PRESSURE) target = c->PR;
+  else return set_err(c, TG_ERR_ARG, "upload: field not stored by this context");
+  int rc = ensure_staging(c);
+  if (rc) return rc;
+  TG_CK(cudaMemcpyAsync(c->staging, host, sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
+  TG_CK(launch_dense_to_compact(c->g, c->staging, target, 0, c->st));
+  TG_CK(cudaStreamSynchronize(c->st));
+  if (si >= 0) {
+    c->energy_valid = false;
+    c->have_nlin = c->have_pressure = c->have_force = false;
+  }
+  return TG_OK;
+}
+
+int tg_field_download(tg_ctx* c, int field, double* host, size_t n) {
+  if (!c || !host || field < 0 || field >= TG_NFIELDS) return TG_ERR_ARG;
+  if (n != 2 * (size_t)c->D) return set_err(c, TG_ERR_ARG, "download: n_doubles must be 2*N1*N2*(N3/2+1)");
+  cudaSetDevice(c->dev);
+  if (field >= TG_WORK0 && field < TG_WORK0 + TG_NWORK) {
+    if (!c->dense[field]) return set_err(c, TG_ERR_STATE, "download: work field never written");
+    TG_CK(cudaMemcpyAsync(host, c->dense[field], sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
+    TG_CK(cudaStreamSynchronize(c->st));
+    return TG_OK;
+  }
+  if (field >= TG_FORCE1 && field <= TG_FORCE3) {
+    std::memset(host, 0, sizeof(double) * n);
+    if (!c->force_on || !c->have_force) return TG_OK;
+    std::vector<cx<double>> box((size_t)c->fbox);
+    const int comp = field - TG_FORCE1;
+    TG_CK(cudaMemcpyAsync(box.data(), c->FB + (size_t)comp * c->fbox, sizeof(cx<double>) * c->fbox,
+                          cudaMemcpyDeviceToHost, c->st));
+    TG_CK(cudaStreamSynchronize(c->st));
+    const int ny = 2 * c->fy + 1, nz = c->fz + 1;
+    for (int p = 0; p < c->fbox; ++p) {
+      const int kz = p % nz, ky = (p / nz) % ny - c->fy, kx = p / (nz * ny) - c->fx;
+      const int lx = kx >= 0 ? kx : kx + c->N1, ly = ky >= 0 ? ky : ky + c->N2;
+      if (lx < 0 || lx >= c->N1 || ly < 0 || ly >= c->N2 || kz >= c->M3) continue;
+      const size_t o = (((size_t)lx * c->N2 + ly) * c->M3 + kz) * 2;
+      host[o] = box[p].x;
+      host[o + 1] = box[p].y;
+    }
+    return TG_OK;
+  }
+  const void* src = nullptr;
+  int sp = 0;
+  const int si = field_state_index(c, field);
+  const int ni = field_nl_index(c, field);
+  if (si >= 0) src = c->U0[si];
+  else if (ni >= 0) src = c->NL[ni];
+  else if (field == TG_PRESSURE) src = c->PR;
+  else return set_err(c, TG_ERR_ARG, "download: field not stored by this context");
+  int rc = ensure_staging(c);
+  if (rc) return rc;
+  TG_CK(launch_compact_to_dense(c->g, src, sp, c->staging, c->st));
+  TG_CK(cudaMemcpyAsync(host, c->staging, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
+  TG_CK(cudaStreamSynchronize(c->st));
+  return TG_OK;
+}
+
+int tg_field_copy(tg_ctx* c, int dst, int src) {
+  if (!c || dst < 0 || dst >= TG_NFIELDS || src < 0 || src >= TG_NFIELDS) return TG_ERR_ARG;
+  cudaSetDevice(c->dev);
+  const bool dwork = dst >= TG_WORK0 && dst < TG_WORK0 + TG_NWORK;
+  const bool swork = src >= TG_WORK0 && src < TG_WORK0 + TG_NWORK;
+  auto compact_of = [&](int f) -> cx<double>* {
+    int si = field_state_index(c, f), ni = field_nl_index(c, f);
+    if (si >= 0) return c->U0[si];
+    if (ni >= 0) return c->NL[ni];
+    if (f == TG_PRESSURE) return c->PR;
+    return nullptr;
+  };
+  if (dwork) {
+    int rc = ensure_dense(c, dst);
+    if (rc) return rc;
+    if (swork) {
+      if (!c->dense[src]) return set_err(c, TG_ERR_STATE, "copy: source work field never written");
+      TG_CK(cudaMemcpyAsync(c->dense[dst], c->dense[src], sizeof(cx<double>) * c->D, cudaMemcpyDeviceToDevice, c->st));
+    } else {
+      cx<double>* s = compact_of(src);
+      if (!s) return TG_ERR_ARG;
+      TG_CK(launch_compact_to_dense(c->g, s, 0, c->dense[dst], c->st));
+    }
+    return TG_OK;
+  }
+  cx<double>* d = compact_of(dst);
+  if (!d) return TG_ERR_ARG;
+  if (swork) {
+    if (!c->dense[src]) return set_err(c, TG_ERR_STATE, "copy: source work field never written");
+    TG_CK(launch_dense_to_compact(c->g, c->dense[src], d, 0, c->st));
+  } else {
+    cx<double>* s = compact_of(src);
+    if (!s) return TG_ERR_ARG;
+    TG_CK(cudaMemcpyAsync(d, s, sizeof(cx<double>) * c->S, cudaMemcpyDeviceToDevice, c->st));
+  }
+  if (field_state_index(c, dst) >= 0) {
+    c->energy_valid = false;
+    c->have_nlin = c->have_pressure = c->have_force = false;
+  }
+  return TG_OK;
+}
+
+int tg_forward_transform(tg_ctx* c, int field, int parity) {
+  (void)parity;
+  if (!c || field < TG_WORK0 || field >= TG_WORK0 + TG_NWORK) return TG_ERR_ARG;
+  cudaSetDevice(c->dev);
+  if (!c->dense[field]) return set_err(c, TG_ERR_STATE, "transform: work field never written");
+  return dense_transform(c, c->dense[field], 1);
+}
+
+int tg_inverse_transform(tg_ctx* c, int field, int parity) {
+  (void)parity;
+  if (!c || field < TG_WORK0 || field >= TG_WORK0 + TG_NWORK) return TG_ERR_ARG;
+  cudaSetDevice(c->dev);
+  if (!c->dense[field]) return set_err(c, TG_ERR_STATE, "transform: work field never written");
+  return dense_transform(c, c->dense[field], 0);
+}
+
+int tg_compute_force(tg_ctx* c) {
+  if (!c) return TG_ERR_ARG;
+  cudaSetDevice(c->dev);
+  if (c->force_on) {
+    const void* in[3] = {c->U0[0], c->U0[1], c->U0[2]};
+    int rc = run_force(c, in, F64);
+    if (rc) return rc;
+  }
+  c->have_force = true;
+  return TG_OK;
+}
+
+int tg_compute_nlin(tg_ctx* c) {
+  if (!c) return TG_ERR_ARG;
+  cudaSetDevice(c->dev);
+  const void* in[6];
+  for (int i = 0; i < c->nstate; ++i) in[i] = c->U0[i];
+  int rc = run_pipeline(c, in, F64);
+  if (rc) return rc;
+  TG_CK(launch_assemble_nlin(c->g, c->phys, c->tprec, (const void* const*)c->PX, c->NL, c->st));
+  c->have_nlin = true;
+  c->have_pressure = false;
+  return TG_OK;
+}
+
+int tg_add_force(tg_ctx* c) {
+  if (!c) return TG_ERR_ARG;
+  if (!c->have_nlin) return set_err(c, TG_ERR_STATE, "Add_force before Compute_nlin");
+  cudaSetDevice(c->dev);
+  if (c->force_on) {
+    if (!c->have_force) return set_err(c, TG_ERR_STATE, "Add_force before Compute_force");
+    TG_CK(launch_sub_force_box(c->g, 3, c->FB, c->fx, c->fy, c->fz, c->NL, c->st));
+  }
+  return TG_OK;
+}
+
+int tg_compute_pressure(tg_ctx* c) {
+  if (!c) return TG_ERR_ARG;
+  if (!c->have_nlin) return set_err(c, TG_ERR_STATE, "Compute_pressure before Compute_nlin");
+  cudaSetDevice(c->dev);
+  TG_CK(launch_pressure(c->g, c->NL, c->PR, c->st));
+  c->have_pressure = true;
+  return TG_OK;
+}
+
+int tg_compute_rhs(tg_ctx* c) {
+  if (!c) return TG_ERR_ARG;
+  if (!c->have_nlin || !c->have_pressure) return set_err(c, TG_ERR_STATE, "Compute_rhs before Compute_pressure");
+  cudaSetDevice(c->dev);
+  TG_CK(launch_rhs_from_nlin(c->g, c->phys, c->NL, c->PR, c->st));
+  return TG_OK;
+}
+
+int tg_get_dt(tg_ctx* c, double* dt) {
+  if (!c) return TG_ERR_ARG;
+  cudaSetDevice(c->dev);
+  int rc = run_energy(c, 2);
+  if (rc) return rc;
+  c->energy_valid = true;
+  if (dt) {
+    TG_CK(cudaMemcpyAsync(c->h_pinned, c->scal, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    TG_CK(cudaStreamSynchronize(c->st));
+    *dt = c->h_pinned[0];
+  }
+  return TG_OK;
+}
+
+int tg_time_advance(tg_ctx* c) {
+  if (!c) return TG_ERR_ARG;
+  if (!c->have_nlin || !c->have_pressure) return set_err(c, TG_ERR_STATE, "Time_advance needs Compute_nlin and Compute_pressure");
+  cudaSetDevice(c->dev);
+  int rc = ensure_dt(c);
+  if (rc) return rc;
+  // stage 1 from the caller's nlin and pressure (Compute_rhs inside Time_advance)
+  TG_CK(launch_rhs_from_nlin(c->g, c->phys, c->NL, c->PR, c->st));
+  RKArgs a = rk_args(c, 1);
+  TG_CK(launch_rk(a, c->phys, c->tprec, c->tprec, 1, c->st, nullptr));
+  rc = run_stages(c, 2, false);
+  if (rc) return rc;
+  c->have_nlin = c->have_pressure = c->have_force = false;
+  return TG_OK;
+}
+
+int tg_step(tg_ctx* c, int n, double* energies) {
+  if (!c || n < 0) return TG_ERR_ARG;
+  if (n == 0) return TG_OK;
+  cudaSetDevice(c->dev);
+  int rc = ensure_dt(c);
+  if (rc) return rc;
+  int done = 0;
+  while (done < n) {
+    const int chunk = std::min(n - done, c->ering_cap);
+    TG_CK(cudaMemsetAsync(c->ering_pos, 0, sizeof(int), c->st));
+    for (int i = 0; i < chunk; ++i) {
+      if (c->graphs && !c->prof && c->eager_steps >= 1) {
+        if (!c->step_graph) {
+          cudaGraph_t gr = nullptr;
+          TG_CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+          rc = enqueue_step(c);
+          cudaError_t e2 = cudaStreamEndCapture(c->st, &gr);
+          if (rc) {
+            if (gr) cudaGraphDestroy(gr);
+            return rc;
+          }
+          if (e2 != cudaSuccess) return cuda_err(c, e2, "cudaStreamEndCapture");
+          cudaError_t e3 = cudaGraphInstantiate(&c->step_graph, gr, 0);
+          cudaGraphDestroy(gr);
+          if (e3 != cudaSuccess) return cuda_err(c, e3, "cudaGraphInstantiate");
+        }
+        TG_CK(cudaGraphLaunch(c->step_graph, c->st));
+      } else {
+        rc = enqueue_step(c);
+        if (rc) return rc;
+        c->eager_steps++;
+      }
+    }
+    if (energies) {
+      TG_CK(cudaMemcpyAsync(energies + done, c->ering, sizeof(double) * chunk, cudaMemcpyDeviceToHost, c->st));
+    }
+    TG_CK(cudaMemcpyAsync(c->h_pinned, c->scal, sizeof(double) * 8, cudaMemcpyDeviceToHost, c->st));
+    TG_CK(cudaStreamSynchronize(c->st));
+    done += chunk;
+    if (c->h_pinned[3] != 0.0) return set_err(c, TG_ERR_NONFINITE, "ERROR: Numerical Overflow (total energy is not finite)");
+  }
+  c->have_nlin = c->have_pressure = c->have_force = false;
+  return TG_OK;
+}
+
+int tg_time(const tg_ctx* c, double* t, long long* steps) {
+  if (!c) return TG_ERR_ARG;
+  double h[8];
+  tg_ctx* cc = const_cast<tg_ctx*>(c);
+  cudaSetDevice(c->dev);
+  cudaError_t e = cudaMemcpyAsync(h, c->scal, sizeof(h), cudaMemcpyDeviceToHost, c->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+  if (e != cudaSuccess) return cuda_err(cc, e, "tg_time");
+  if (t) *t = h[1];
+  if (steps) *steps = (long long)h[2];
+  return TG_OK;
+}
+
+int tg_energy(tg_ctx* c, int group, double* energy, double* diss) {
+  if (!c) return TG_ERR_ARG;
+  if (group < 0 || group > 2) return TG_ERR_ARG;
+  if (group == 1 && c->phys != TG_MHD) return TG_ERR_ARG;
+  if (group == 2 && c->phys != TG_SCALAR && c->phys != TG_RB) return TG_ERR_ARG;
+  cudaSetDevice(c->dev);
+  int rc = run_energy(c, 0);
+  if (rc) return rc;
+  TG_CK(cudaMemcpyAsync(c->h_pinned, c->red_out, sizeof(double) * 8, cudaMemcpyDeviceToHost, c->st));
+  TG_CK(cudaStreamSynchronize(c->st));
+  const int s = group * 2;
+  // CV_total_energy and CV_total_dissipation = 2 sum mult K^2 |u|^2 (Cvf.cc:385-397)
+  if (energy) *energy = c->h_pinned[s];
+  if (diss) *diss = 2.0 * c->h_pinned[s + 1];
+  return TG_OK;
+}
+
+int tg_shell_spectrum(tg_ctx* c, int group, double* ek, double* dissk, int n) {
+  if (!c || !ek) return TG_ERR_ARG;
+  if (group < 0 || group > 2) return TG_ERR_ARG;
+  if (group == 1 && c->phys != TG_MHD) return TG_ERR_ARG;
+  if (group == 2 && c->phys != TG_SCALAR && c->phys != TG_RB) return TG_ERR_ARG;
+  cudaSetDevice(c->dev);
+  // Min_radius_outside / Max_radius_inside (four_inline.h:172-257)
+  const int d = c->cfg.dealias ? 3 : 2;
+  const double* kf = c->cfg.kfactor;
+  const double a0 = (c->N1 / d) * kf[0], a1 = (c->N2 / d) * kf[1], a2 = (c->N3 / d) * kf[2];
+  const int kkmax = (int)std::ceil(std::sqrt(a0 * a0 + a1 * a1 + a2 * a2));
+  const int kin = max_radius_inside(c);
+  const int nbins = kkmax + 1;
+  if (n < nbins) return set_err(c, TG_ERR_ARG, "shell spectrum: n < kmax_outside + 1");
+  const int nf = (group == 2) ? 1 : 3;
+  const cx<double>* F[3];
+  for (int i = 0; i < nf; ++i) F[i] = c->U0[(group == 0 ? 0 : 3) + i];
+  // scratch: [nf*nbins] ek, [nbins] cnt, [nbins] diss, [nbins] cnt2
+  const size_t need = (size_t)(nf + 3) * nbins;
+  if (c->diag_cap < need) {
+    if (c->diag) cudaFree(c->diag);
+    c->diag = nullptr;
+    c->diag_cap = 0;
+    int rc = dalloc(c, (void**)&c->diag, sizeof(double) * need);
+    if (rc) return rc;
+    c->diag_cap = need;
+  }
+  double* dbuf = c->diag;
+  TG_CK(cudaMemsetAsync(dbuf, 0, sizeof(double) * need, c->st));
+  TG_CK(launch_shell_spectrum(c->g, F, nf, 0.0, dbuf, dbuf + (size_t)nf * nbins, nbins, c->st));
+  // dissipation spectrum: sum over components of K^2-weighted, times 2 (Cvf.cc:430-448)
+  double* dk = dbuf + (size_t)(nf + 1) * nbins;
+  double* dcnt = dk + nbins;
+  {
+    // accumulate all components into one row by summing separate passes
+    for (int i = 0; i < nf; ++i) {
+      const cx<double>* Fi[1] = {F[i]};
+      TG_CK(launch_shell_spectrum(c->g, Fi, 1, 2.0, dk, dcnt, nbins, c->st));
+    }
+  }
+  std::vector<double> h(need);
+  TG_CK(cudaMemcpyAsync(h.data(), dbuf, sizeof(double) * need, cudaMemcpyDeviceToHost, c->st));
+  TG_CK(cudaStreamSynchronize(c->st));
+  const double* cnt = h.data() + (size_t)nf * nbins;
+  const double approx_fac = 2 * M_PI / (kf[0] * kf[1] * kf[2]);
+  for (int i = 0; i < nf; ++i)
+    for (int b = 0; b < n; ++b) ek[(size_t)i * n + b] = 0.0;
+  if (dissk)
+    for (int b = 0; b < n; ++b) dissk[b] = 0.0;
+  for (int b = 0; b < nbins; ++b) {
+    // partial shells (kmax_inside, kmax] rescaled (four_energy.cc:324-336)
+    const bool resc = (b > kin) && (cnt[b] >= 1);
+    const double f = resc ? approx_fac * b * b / cnt[b] : 1.0;
+    for (int i = 0; i < nf; ++i) ek[(size_t)i * n + b] = h[(size_t)i * nbins + b] * f;
+    if (dissk) dissk[b] = 2.0 * h[(size_t)(nf + 1) * nbins + b] * f;
+  }
+  return TG_OK;
+}
+
+int tg_profile_enable(tg_ctx* c, int enable) {
+  if (!c) return TG_ERR_ARG;
+  c->prof = enable != 0;
+  return TG_OK;
+}
+
+int tg_profile_read(tg_ctx* c, tg_kernel_stat* out, int max, int* n) {
+  if (!c || (max > 0 && !out)) return TG_ERR_ARG;
+  cudaSetDevice(c->dev);
+  TG_CK(cudaStreamSynchronize(c->st));
+  std::vector<tg_kernel_stat> agg;
+  for (auto& r : c->prof_recs) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, r.a, r.b);
+    size_t k = 0;
+    for (; k < agg.size(); ++k)
+      if (std::strncmp(agg[k].name, r.name, sizeof(agg[k].name)) == 0) break;
+    if (k == agg.size()) {
+      tg_kernel_stat st{};
+      std::strncpy(st.name, r.name, sizeof(st.name) - 1);
+      agg.push_back(st);
+    }
+    agg[k].launches += 1;
+    agg[k].total_ms += ms;
+    agg[k].bytes_per_launch += r.bytes;
+    c->ev_pool.push_back(r.a);
+    c->ev_pool.push_back(r.b);
+  }
+  c->prof_recs.clear();
+  for (auto& a : agg)
+    if (a.launches) a.bytes_per_launch /= a.launches;
+  const int m = std::min<int>(max, (int)agg.size());
+  for (int i = 0; i < m; ++i) out[i] = agg[i];
+  if (n) *n = (int)agg.size();
+  return TG_OK;
+}
+
+int tg_nusselt(tg_ctx* c, double* nu) {
+  (void)nu;
+  if (!c) return TG_ERR_ARG;
+  return set_err(c, TG_ERR_UNSUPPORTED, "Nusselt number needs the RB (SCFT) physics");
+}
+
+}  // extern "C"

@@ -1,0 +1,96 @@
+// Internal definition of a solver context (the device-side state of one IncFluid/IncVF/IncSF
+// set of objects in the reference).
+#pragma once
+
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/tarang_gpu.h"
+#include "tg_fft_launch.h"
+#include "tg_spectral.cuh"
+
+struct tg_ctx {
+  tg_config cfg{};
+  std::string err;
+  int dev = 0;
+  cudaStream_t st = nullptr;
+  bool own_stream = false;
+
+  // geometry
+  int N1 = 0, N2 = 0, N3 = 0, M3 = 0, Mz = 0;
+  int phys = 0, basis = 0, prec = 0;
+  int tprec = 0;            // transform precision (tg::F64 / tg::F32)
+  size_t tsz = 16;          // bytes per complex at transform precision
+  tg::Geo g{};
+  long long S = 0;          // compact elements per field
+  long long D = 0;          // dense elements per field
+  int nstate = 3, nin = 3, nprod = 6;
+  tg::ProdPairs pairs{};
+  double nu_of[6] = {0, 0, 0, 0, 0, 0};
+
+  // twiddle tables: length -> exp(-2 pi i m / L)
+  std::map<int, tg::cx<double>*> tw;
+
+  // compact solver state
+  tg::cx<double>* U0[6] = {};
+  tg::cx<double>* TOT[6] = {};
+  void* US[6] = {};
+  tg::cx<double>* NL[6] = {};
+  tg::cx<double>* PR = nullptr;
+  // pipeline intermediates (transform precision)
+  void* WX[6] = {};
+  void* WY[6] = {};
+  void* PP[9] = {};
+  void* PY[9] = {};
+  void* PX[9] = {};
+
+  // forcing box
+  int force_on = 0;
+  int fx = 0, fy = 0, fz = 0, fbox = 0;
+  int nf_modes = 0;
+  tg::cx<double>* FB = nullptr;
+
+  // scalars and reductions
+  double* scal = nullptr;   // [0] dt, [1] t_now, [2] steps, [3] nonfinite
+  double* red_out = nullptr;  // [8]
+  double* part = nullptr;   // [nblocks][8]
+  int npart_blocks = 0;
+  double* ering = nullptr;  // energy per step of the current tg_step call
+  int* ering_pos = nullptr;
+  int ering_cap = 0;
+  double* h_pinned = nullptr;  // small pinned host buffer
+  double* diag = nullptr;      // diagnostics scratch (spectra, transfer tables)
+  size_t diag_cap = 0;
+  double dx_cfl = 0;
+
+  // dense fields (reference layout, FP64), allocated on demand
+  tg::cx<double>* dense[TG_NFIELDS] = {};
+  tg::cx<double>* staging = nullptr;
+
+  // status
+  bool energy_valid = false;  // scal[0] holds Get_dt of the current state
+  bool have_nlin = false, have_pressure = false, have_force = false;
+  size_t bytes = 0;
+
+  // profiling: per-launch events on st
+  struct ProfRec {
+    const char* name;
+    cudaEvent_t a, b;
+    double bytes;
+  };
+  bool prof = false;
+  std::vector<ProfRec> prof_recs;
+  std::vector<cudaEvent_t> ev_pool;
+
+  // graph of one fused step
+  cudaGraphExec_t step_graph = nullptr;
+  bool graphs = true;
+  bool pipeline_ok = true;
+  int eager_steps = 0;
+};
+
+namespace tg {
+int set_err(tg_ctx* c, int code, const std::string& msg);
+int cuda_err(tg_ctx* c, cudaError_t e, const char* where);
+}  // namespace tg

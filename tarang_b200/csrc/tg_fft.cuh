@@ -1,0 +1,449 @@
+// FFT pass kernels of the 3-D pseudo-spectral transforms.
+//
+// A 3-D FOUR transform of a (N1, N2, N3/2+1) complex field is three passes:
+//   x-pass : batched c2c along axis 1 (row stride N2*(N3/2+1)),   kernel k_axis_c2c
+//   y-pass : batched c2c along axis 2 (row stride N3/2+1),         kernel k_axis_c2c
+//   z-pass : c2r / r2c along the contiguous axis 3 via a length-N3/2 complex FFT,
+//            kernels k_z_c2r / k_z_r2c, or k_z_prod which fuses the inverse of several
+//            fields, their pointwise real-space products and the forward of every product.
+// Each pass reads and writes HBM once.  Inside a block the FFT of length L = R1*R2 is a
+// two-step (four-step) FFT: a radix-R1 register DFT per thread, a twiddle, one transpose
+// through shared memory, and a radix-R2 register DFT.  Axis maps (AxisMap) let a pass read
+// only the stored (2/3-dealiased) wavenumbers and write only the ones that are kept, so the
+// solver's fields live in a compact layout and the zero 1/3 band is neither read nor written.
+#pragma once
+
+#include "tg_common.cuh"
+#include "tg_dft.cuh"
+
+namespace tg {
+
+constexpr int kMaxPtr = 12;
+
+struct PtrSet {
+  const void* src[kMaxPtr];
+  void* dst[kMaxPtr];
+  const void* src2[kMaxPtr];  // optional second source: input = src + comb * src2
+};
+
+struct AxisArgs {
+  long long sb, sr;   // source: element stride between batches, between rows (FFT index)
+  long long db, dr;   // destination strides
+  int ncols;          // contiguous columns per batch processed
+  AxisMap in, out;    // stored rows on input and output
+  double scale;       // output scale
+  const cx<double>* tw;  // exp(-2 pi i m / L), m in [0, L)
+  int comb[kMaxPtr];  // per field: 0, or +1 / -1 to read src + comb * src2 (Elsasser z+-)
+};
+
+// ------------------------------------------------------------------------------------------
+// strided-axis c2c, power-of-two L = R1 * R2 (R1 >= R2), 256 threads, W = 256/R1 columns
+// ------------------------------------------------------------------------------------------
+template <typename Ri, typename Ro, typename Rw, int R1, int R2, int DIR>
+__global__ void __launch_bounds__(256) k_axis_c2c(AxisArgs a, PtrSet ps) {
+  constexpr int L = R1 * R2;
+  constexpr int W = 256 / R1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cx<Rw>* tw = reinterpret_cast<cx<Rw>*>(smem_raw);
+  cx<Rw>* ex = tw + L;
+  const int tid = threadIdx.x;
+  const int f = blockIdx.z;
+  const cx<Ri>* src = reinterpret_cast<const cx<Ri>*>(ps.src[f]) + (long long)blockIdx.y * a.sb;
+  cx<Ro>* dst = reinterpret_cast<cx<Ro>*>(ps.dst[f]) + (long long)blockIdx.y * a.db;
+  const int comb = a.comb[f];
+  const cx<Ri>* src2 = comb ? reinterpret_cast<const cx<Ri>*>(ps.src2[f]) + (long long)blockIdx.y * a.sb : src;
+  for (int i = tid; i < L; i += 256) tw[i] = cvt<Rw>(a.tw[i]);
+  const int w = tid % W;
+  const int col = blockIdx.x * W + w;
+  const bool ok = col < a.ncols;
+  __syncthreads();
+  {
+    const int n2 = tid / W;
+    if (n2 < R2) {
+      cx<Rw> v[R1];
+#pragma unroll
+      for (int n1 = 0; n1 < R1; ++n1) {
+        const int r = amap_row(a.in, R2 * n1 + n2);
+        v[n1] = mkc<Rw>(0, 0);
+        if (ok && r >= 0) {
+          const long long o = (long long)r * a.sr + col;
+          v[n1] = cvt<Rw>(src[o]);
+          if (comb > 0) v[n1] = v[n1] + cvt<Rw>(src2[o]);
+          else if (comb < 0) v[n1] = v[n1] - cvt<Rw>(src2[o]);
+        }
+      }
+      DFT<R1, DIR, Rw>::run(v);
+#pragma unroll
+      for (int k1 = 0; k1 < R1; ++k1) {
+        cx<Rw> t = tw[(n2 * k1) & (L - 1)];
+        if (DIR > 0) t.y = -t.y;
+        ex[(k1 * R2 + n2) * W + w] = v[k1] * t;
+      }
+    }
+  }
+  __syncthreads();
+  {
+    const int k1 = tid / W;
+    cx<Rw> v[R2];
+#pragma unroll
+    for (int n2 = 0; n2 < R2; ++n2) v[n2] = ex[(k1 * R2 + n2) * W + w];
+    DFT<R2, DIR, Rw>::run(v);
+    const Rw sc = (Rw)a.scale;
+#pragma unroll
+    for (int k2 = 0; k2 < R2; ++k2) {
+      const int r = amap_row(a.out, k1 + R1 * k2);
+      if (ok && r >= 0) dst[(long long)r * a.dr + col] = cvt<Ro>(sc * v[k2]);
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// strided-axis direct DFT for any L (used for lengths that are not a power of two)
+// block = 256 threads, 8 columns, tile [L][8] in shared memory
+// ------------------------------------------------------------------------------------------
+template <typename Ri, typename Ro, typename Rw, int DIR>
+__global__ void __launch_bounds__(256) k_axis_dft(AxisArgs a, PtrSet ps, int L) {
+  constexpr int W = 8;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cx<Rw>* tw = reinterpret_cast<cx<Rw>*>(smem_raw);
+  cx<Rw>* tile = tw + L;
+  const int tid = threadIdx.x;
+  const int f = blockIdx.z;
+  const cx<Ri>* src = reinterpret_cast<const cx<Ri>*>(ps.src[f]) + (long long)blockIdx.y * a.sb;
+  cx<Ro>* dst = reinterpret_cast<cx<Ro>*>(ps.dst[f]) + (long long)blockIdx.y * a.db;
+  const int comb = a.comb[f];
+  const cx<Ri>* src2 = comb ? reinterpret_cast<const cx<Ri>*>(ps.src2[f]) + (long long)blockIdx.y * a.sb : src;
+  const int c0 = blockIdx.x * W;
+  for (int i = tid; i < L; i += 256) {
+    cx<Rw> t = cvt<Rw>(a.tw[i]);
+    if (DIR > 0) t.y = -t.y;
+    tw[i] = t;
+  }
+  for (int i = tid; i < L * W; i += 256) {
+    const int n = i / W, w = i % W;
+    const int r = amap_row(a.in, n);
+    const int col = c0 + w;
+    cx<Rw> v = mkc<Rw>(0, 0);
+    if (col < a.ncols && r >= 0) {
+      const long long o = (long long)r * a.sr + col;
+      v = cvt<Rw>(src[o]);
+      if (comb > 0) v = v + cvt<Rw>(src2[o]);
+      else if (comb < 0) v = v - cvt<Rw>(src2[o]);
+    }
+    tile[i] = v;
+  }
+  __syncthreads();
+  const Rw sc = (Rw)a.scale;
+  for (int i = tid; i < L * W; i += 256) {
+    const int k = i / W, w = i % W;
+    const int r = amap_row(a.out, k);
+    const int col = c0 + w;
+    if (col >= a.ncols || r < 0) continue;
+    cx<Rw> acc = mkc<Rw>(0, 0);
+    int m = 0;
+    for (int n = 0; n < L; ++n) {
+      acc = acc + tile[n * W + w] * tw[m];
+      m += k;
+      if (m >= L) m -= L;
+    }
+    dst[(long long)r * a.dr + col] = cvt<Ro>(sc * acc);
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// z-pass (contiguous axis) c2r / r2c.  Rows hold N3/2+1 spectral values of which the first
+// `nin` are stored (the rest are zero); the real row of N3 = 2M values is packed as M complex
+// (x[2m] + i x[2m+1]), the reference's in-place layout, followed by a zero padding slot.
+// ------------------------------------------------------------------------------------------
+struct ZArgs {
+  long long nrows;
+  long long ss, ds;     // row strides (complex elements)
+  int nin, nout;        // stored spectral entries on input (c2r) / output (r2c)
+  int nfill;            // r2c: entries [nout, nfill) of each output row are written as zero
+  int pad;              // c2r: write a zero to slot M of each output row
+  double scale;
+  const cx<double>* twM;  // exp(-2 pi i m / M), m in [0, M)
+  const cx<double>* twN;  // exp(-2 pi i k / N), k in [0, N), N = 2M
+};
+
+// c2r pre-twiddle: Z[k] = (X[k] + conj(X[M-k])) + i e^{+i pi k/M} (X[k] - conj(X[M-k])); the
+// imaginary parts of X[0] and X[M] are ignored (the c2r rule of FFTW and pocketfft).
+template <typename Rw, typename Ri>
+__device__ __forceinline__ cx<Rw> c2r_pre(const cx<Ri>* row, int k, int M, int nin, const cx<Rw>* twN) {
+  cx<Rw> a = (k < nin) ? cvt<Rw>(row[k]) : mkc<Rw>(0, 0);
+  const int km = M - k;
+  cx<Rw> b = (km < nin) ? cvt<Rw>(row[km]) : mkc<Rw>(0, 0);
+  if (k == 0) {
+    a.y = 0;
+    b.y = 0;
+  }
+  b.y = -b.y;
+  cx<Rw> h = twN[k];
+  h.y = -h.y;  // e^{+i pi k / M}
+  return (a + b) + ione(h * (a - b));
+}
+
+// r2c post-twiddle: X[k] = (Z[k] + conj(Z[M-k]))/2 - (i/2) e^{-i pi k/M} (Z[k] - conj(Z[M-k]))
+template <typename Rw>
+__device__ __forceinline__ cx<Rw> r2c_post(const cx<Rw>* zrow, int k, int M, const cx<Rw>* twN) {
+  const cx<Rw> zk = zrow[k & (M - 1)];
+  cx<Rw> zm = zrow[(M - k) & (M - 1)];
+  zm.y = -zm.y;
+  const cx<Rw> s = zk + zm;
+  const cx<Rw> d = twN[k] * (zk - zm);
+  return mkc<Rw>((Rw)0.5 * (s.x + d.y), (Rw)0.5 * (s.y - d.x));
+}
+
+template <typename Ri, typename Ro, typename Rw, int R1, int R2>
+__global__ void __launch_bounds__(256) k_z_c2r(ZArgs a, PtrSet ps) {
+  constexpr int M = R1 * R2;
+  constexpr int T = R1;
+  constexpr int ROWS = 256 / T;
+  constexpr int EXP = R2 + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cx<Rw>* twM = reinterpret_cast<cx<Rw>*>(smem_raw);
+  cx<Rw>* twN = twM + M;
+  cx<Rw>* ex = twN + 2 * M;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < M; i += 256) twM[i] = cvt<Rw>(a.twM[i]);
+  for (int i = tid; i < 2 * M; i += 256) twN[i] = cvt<Rw>(a.twN[i]);
+  const int f = blockIdx.z;
+  const int rl = tid / T, t = tid % T;
+  const long long row = (long long)blockIdx.x * ROWS + rl;
+  const bool ok = row < a.nrows;
+  const cx<Ri>* src = reinterpret_cast<const cx<Ri>*>(ps.src[f]) + row * a.ss;
+  cx<Ro>* dst = reinterpret_cast<cx<Ro>*>(ps.dst[f]) + row * a.ds;
+  cx<Rw>* exr = ex + rl * R1 * EXP;
+  __syncthreads();
+  if (t < R2) {
+    cx<Rw> v[R1];
+#pragma unroll
+    for (int n1 = 0; n1 < R1; ++n1)
+      v[n1] = ok ? c2r_pre<Rw>(src, R2 * n1 + t, M, a.nin, twN) : mkc<Rw>(0, 0);
+    DFT<R1, +1, Rw>::run(v);
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+      cx<Rw> w = twM[(t * k1) & (M - 1)];
+      w.y = -w.y;
+      exr[k1 * EXP + t] = v[k1] * w;
+    }
+  }
+  __syncthreads();
+  {
+    const int k1 = t;
+    cx<Rw> v[R2];
+#pragma unroll
+    for (int n2 = 0; n2 < R2; ++n2) v[n2] = exr[k1 * EXP + n2];
+    DFT<R2, +1, Rw>::run(v);
+    const Rw sc = (Rw)a.scale;
+    if (ok) {
+#pragma unroll
+      for (int k2 = 0; k2 < R2; ++k2) dst[k1 + R1 * k2] = cvt<Ro>(sc * v[k2]);
+      if (a.pad && k1 == 0) dst[M] = mkc<Ro>(0, 0);
+    }
+  }
+}
+
+template <typename Ri, typename Ro, typename Rw, int R1, int R2>
+__global__ void __launch_bounds__(256) k_z_r2c(ZArgs a, PtrSet ps) {
+  constexpr int M = R1 * R2;
+  constexpr int T = R1;
+  constexpr int ROWS = 256 / T;
+  constexpr int EXP = R2 + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cx<Rw>* twM = reinterpret_cast<cx<Rw>*>(smem_raw);
+  cx<Rw>* twN = twM + M;
+  cx<Rw>* ex = twN + 2 * M;
+  cx<Rw>* zb = ex + ROWS * R1 * EXP;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < M; i += 256) twM[i] = cvt<Rw>(a.twM[i]);
+  for (int i = tid; i < 2 * M; i += 256) twN[i] = cvt<Rw>(a.twN[i]);
+  const int f = blockIdx.z;
+  const int rl = tid / T, t = tid % T;
+  const long long row = (long long)blockIdx.x * ROWS + rl;
+  const bool ok = row < a.nrows;
+  const cx<Ri>* src = reinterpret_cast<const cx<Ri>*>(ps.src[f]) + row * a.ss;
+  cx<Ro>* dst = reinterpret_cast<cx<Ro>*>(ps.dst[f]) + row * a.ds;
+  cx<Rw>* exr = ex + rl * R1 * EXP;
+  cx<Rw>* zr = zb + rl * M;
+  __syncthreads();
+  if (t < R2) {
+    cx<Rw> v[R1];
+#pragma unroll
+    for (int n1 = 0; n1 < R1; ++n1) v[n1] = ok ? cvt<Rw>(src[R2 * n1 + t]) : mkc<Rw>(0, 0);
+    DFT<R1, -1, Rw>::run(v);
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) exr[k1 * EXP + t] = v[k1] * twM[(t * k1) & (M - 1)];
+  }
+  __syncthreads();
+  {
+    const int k1 = t;
+    cx<Rw> v[R2];
+#pragma unroll
+    for (int n2 = 0; n2 < R2; ++n2) v[n2] = exr[k1 * EXP + n2];
+    DFT<R2, -1, Rw>::run(v);
+#pragma unroll
+    for (int k2 = 0; k2 < R2; ++k2) zr[k1 + R1 * k2] = v[k2];
+  }
+  __syncthreads();
+  if (ok) {
+    const Rw sc = (Rw)a.scale;
+    for (int k = t; k < a.nout; k += T) dst[k] = cvt<Ro>(sc * r2c_post<Rw>(zr, k, M, twN));
+    for (int k = a.nout + t; k < a.nfill; k += T) dst[k] = mkc<Ro>(0, 0);
+  }
+}
+
+// direct z-pass DFTs for any even N3 (N3/2 not a power of two); one row per block
+template <typename Ri, typename Ro, typename Rw>
+__global__ void __launch_bounds__(128) k_z_c2r_dft(ZArgs a, PtrSet ps, int M) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int N = 2 * M;
+  cx<Rw>* twN = reinterpret_cast<cx<Rw>*>(smem_raw);
+  cx<Rw>* X = twN + N;
+  const int f = blockIdx.z;
+  const long long row = blockIdx.x;
+  const cx<Ri>* src = reinterpret_cast<const cx<Ri>*>(ps.src[f]) + row * a.ss;
+  cx<Ro>* dst = reinterpret_cast<cx<Ro>*>(ps.dst[f]) + row * a.ds;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) twN[i] = cvt<Rw>(a.twN[i]);
+  for (int k = threadIdx.x; k <= M; k += blockDim.x) X[k] = (k < a.nin) ? cvt<Rw>(src[k]) : mkc<Rw>(0, 0);
+  __syncthreads();
+  const Rw sc = (Rw)a.scale;
+  for (int n = threadIdx.x; n < N; n += blockDim.x) {
+    // x[n] = Re X0 + Re XM (-1)^n + 2 sum_{k=1}^{M-1} Re(X_k e^{+2 pi i k n / N})
+    Rw acc = X[0].x + ((n & 1) ? -X[M].x : X[M].x);
+    int m = 0;
+    for (int k = 1; k < M; ++k) {
+      m += n;
+      if (m >= N) m -= N;
+      const cx<Rw> w = twN[m];  // e^{-i theta}; Re(X e^{+i theta}) = X.x w.x + X.y w.y
+      acc += (Rw)2 * (X[k].x * w.x + X[k].y * w.y);
+    }
+    reinterpret_cast<Ro*>(dst)[n] = (Ro)(sc * acc);
+  }
+  if (a.pad && threadIdx.x == 0) dst[M] = mkc<Ro>(0, 0);
+}
+
+template <typename Ri, typename Ro, typename Rw>
+__global__ void __launch_bounds__(128) k_z_r2c_dft(ZArgs a, PtrSet ps, int M) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int N = 2 * M;
+  cx<Rw>* twN = reinterpret_cast<cx<Rw>*>(smem_raw);
+  Rw* x = reinterpret_cast<Rw*>(twN + N);
+  const int f = blockIdx.z;
+  const long long row = blockIdx.x;
+  const Ri* src = reinterpret_cast<const Ri*>(reinterpret_cast<const cx<Ri>*>(ps.src[f]) + row * a.ss);
+  cx<Ro>* dst = reinterpret_cast<cx<Ro>*>(ps.dst[f]) + row * a.ds;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) twN[i] = cvt<Rw>(a.twN[i]);
+  for (int i = threadIdx.x; i < N; i += blockDim.x) x[i] = (Rw)src[i];
+  __syncthreads();
+  const Rw sc = (Rw)a.scale;
+  for (int k = threadIdx.x; k < a.nout; k += blockDim.x) {
+    cx<Rw> acc = mkc<Rw>(0, 0);
+    int m = 0;
+    for (int n = 0; n < N; ++n) {
+      acc = acc + x[n] * twN[m];
+      m += k;
+      if (m >= N) m -= N;
+    }
+    dst[k] = cvt<Ro>(sc * acc);
+  }
+  for (int k = a.nout + threadIdx.x; k < a.nfill; k += blockDim.x) dst[k] = mkc<Ro>(0, 0);
+}
+
+// ------------------------------------------------------------------------------------------
+// Fused z-pass of the nonlinear term: inverse (c2r) of NIN fields, NPROD pointwise real-space
+// products (pairs of inputs), forward (r2c) of every product with scale 1/(N1 N2 N3).
+// Between the inverse and the forward FFT each thread keeps the same positions
+// m = k1 + R1 k2, which are exactly the inputs of the forward FFT's first step with the radix
+// roles swapped, so the products are formed without another exchange.
+// ------------------------------------------------------------------------------------------
+struct ProdPairs {
+  signed char a[12], b[12];
+};
+
+template <typename Ri, typename Ro, typename Rw, int R1, int R2, int NIN, int NPROD>
+__global__ void __launch_bounds__(256 / ((R1 * R2 >= 128) ? 2 : 1))
+    k_z_prod(ZArgs a, PtrSet ps, ProdPairs pp) {
+  constexpr int M = R1 * R2;
+  constexpr int T = R1;
+  constexpr int ROWS = (256 / ((M >= 128) ? 2 : 1)) / T;
+  constexpr int EXA = R2 + 1;   // inverse exchange pitch
+  constexpr int EXB = R1 + 1;   // forward exchange pitch
+  constexpr int EXS = (R1 * EXA > R2 * EXB) ? R1 * EXA : R2 * EXB;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cx<Rw>* twM = reinterpret_cast<cx<Rw>*>(smem_raw);
+  cx<Rw>* twN = twM + M;
+  cx<Rw>* ex = twN + 2 * M;
+  cx<Rw>* zb = ex + ROWS * EXS;
+  cx<Rw>* rs = zb + ROWS * M;  // [NIN][ROWS][M]
+  const int tid = threadIdx.x;
+  for (int i = tid; i < M; i += blockDim.x) twM[i] = cvt<Rw>(a.twM[i]);
+  for (int i = tid; i < 2 * M; i += blockDim.x) twN[i] = cvt<Rw>(a.twN[i]);
+  const int rl = tid / T, t = tid % T;
+  const long long row = (long long)blockIdx.x * ROWS + rl;
+  const bool ok = row < a.nrows;
+  cx<Rw>* exr = ex + rl * EXS;
+  cx<Rw>* zr = zb + rl * M;
+  __syncthreads();
+#pragma unroll 1
+  for (int c = 0; c < NIN; ++c) {
+    const cx<Ri>* src = reinterpret_cast<const cx<Ri>*>(ps.src[c]) + row * a.ss;
+    if (t < R2) {
+      cx<Rw> v[R1];
+#pragma unroll
+      for (int n1 = 0; n1 < R1; ++n1)
+        v[n1] = ok ? c2r_pre<Rw>(src, R2 * n1 + t, M, a.nin, twN) : mkc<Rw>(0, 0);
+      DFT<R1, +1, Rw>::run(v);
+#pragma unroll
+      for (int k1 = 0; k1 < R1; ++k1) {
+        cx<Rw> w = twM[(t * k1) & (M - 1)];
+        w.y = -w.y;
+        exr[k1 * EXA + t] = v[k1] * w;
+      }
+    }
+    __syncthreads();
+    {
+      cx<Rw> v[R2];
+#pragma unroll
+      for (int n2 = 0; n2 < R2; ++n2) v[n2] = exr[t * EXA + n2];
+      DFT<R2, +1, Rw>::run(v);
+      cx<Rw>* rsr = rs + ((long long)c * ROWS + rl) * M;
+#pragma unroll
+      for (int k2 = 0; k2 < R2; ++k2) rsr[t + R1 * k2] = v[k2];
+    }
+    __syncthreads();
+  }
+  const Rw sc = (Rw)a.scale;
+#pragma unroll 1
+  for (int q = 0; q < NPROD; ++q) {
+    const cx<Rw>* ra = rs + ((long long)pp.a[q] * ROWS + rl) * M;
+    const cx<Rw>* rb = rs + ((long long)pp.b[q] * ROWS + rl) * M;
+    {
+      // forward step 1: radix R2 over k2 for this thread's n2' = t
+      cx<Rw> v[R2];
+#pragma unroll
+      for (int k2 = 0; k2 < R2; ++k2) v[k2] = rmul(ra[t + R1 * k2], rb[t + R1 * k2]);
+      DFT<R2, -1, Rw>::run(v);
+#pragma unroll
+      for (int k1p = 0; k1p < R2; ++k1p) exr[k1p * EXB + t] = v[k1p] * twM[(t * k1p) & (M - 1)];
+    }
+    __syncthreads();
+    if (t < R2) {
+      cx<Rw> v[R1];
+#pragma unroll
+      for (int n2p = 0; n2p < R1; ++n2p) v[n2p] = exr[t * EXB + n2p];
+      DFT<R1, -1, Rw>::run(v);
+#pragma unroll
+      for (int k2p = 0; k2p < R1; ++k2p) zr[t + R2 * k2p] = v[k2p];
+    }
+    __syncthreads();
+    if (ok) {
+      cx<Ro>* dst = reinterpret_cast<cx<Ro>*>(ps.dst[q]) + row * a.ds;
+      for (int k = t; k < a.nout; k += T) dst[k] = cvt<Ro>(sc * r2c_post<Rw>(zr, k, M, twN));
+      for (int k = a.nout + t; k < a.nfill; k += T) dst[k] = mkc<Ro>(0, 0);
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace tg

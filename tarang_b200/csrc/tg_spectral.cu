@@ -1,0 +1,613 @@
+// Mode-space kernels of the time step (see tg_spectral.cuh).
+#include "tg_spectral.cuh"
+
+namespace tg {
+
+namespace {
+
+constexpr int TPB = 256;
+
+template <typename R>
+__device__ __forceinline__ cx<double> ldc(const void* p, long long i) {
+  return cvt<double>(reinterpret_cast<const cx<R>*>(p)[i]);
+}
+template <typename R>
+__device__ __forceinline__ void stc(void* p, long long i, cx<double> v) {
+  reinterpret_cast<cx<R>*>(p)[i] = cvt<R>(v);
+}
+
+__device__ __forceinline__ cx<double> kdot(double kx, double ky, double kz, cx<double> a, cx<double> b, cx<double> c) {
+  return mkc<double>(kx * a.x + ky * b.x + kz * c.x, kx * a.y + ky * b.y + kz * c.y);
+}
+// i (kx a + ky b + kz c)
+__device__ __forceinline__ cx<double> ikdot(double kx, double ky, double kz, cx<double> a, cx<double> b, cx<double> c) {
+  return ione(kdot(kx, ky, kz, a, b, c));
+}
+
+// block sum of NV doubles; thread 0 of the block gets the totals in v
+template <int NV>
+__device__ __forceinline__ void block_sum(double* v) {
+  __shared__ double red[TPB / 32][NV];
+#pragma unroll
+  for (int j = 0; j < NV; ++j) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[j] += __shfl_down_sync(0xffffffffu, v[j], o);
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) {
+#pragma unroll
+    for (int j = 0; j < NV; ++j) red[wid][j] = v[j];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+      double s = 0;
+      for (int w = 0; w < TPB / 32; ++w) s += red[w][j];
+      v[j] = s;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ layout conversion
+template <typename R>
+__global__ void k_dense_to_compact(Geo g, const cx<double>* __restrict__ dense, cx<R>* __restrict__ comp) {
+  const long long idx = (long long)blockIdx.x * TPB + threadIdx.x;
+  if (idx >= g.S) return;
+  int r1, r2, l3;
+  compact_mode(g, idx, r1, r2, l3);
+  cx<double> v = mkc<double>(0, 0);
+  if (l3 < g.nkz) {
+    const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
+    const int M3 = g.N3 / 2 + 1;
+    v = dense[((long long)l1 * g.N2 + l2) * M3 + l3];
+  }
+  comp[idx] = cvt<R>(v);
+}
+
+template <typename R>
+__global__ void k_compact_to_dense(Geo g, const cx<R>* __restrict__ comp, cx<double>* __restrict__ dense) {
+  const int M3 = g.N3 / 2 + 1;
+  const long long D = (long long)g.N1 * g.N2 * M3;
+  const long long idx = (long long)blockIdx.x * TPB + threadIdx.x;
+  if (idx >= D) return;
+  const int l3 = (int)(idx % M3);
+  const long long rr = idx / M3;
+  const int l2 = (int)(rr % g.N2), l1 = (int)(rr / g.N2);
+  const int r1 = amap_row(g.ax, l1), r2 = amap_row(g.ay, l2);
+  cx<double> v = mkc<double>(0, 0);
+  if (r1 >= 0 && r2 >= 0 && l3 < g.nkz) v = cvt<double>(comp[((long long)r1 * g.nky + r2) * g.kzp + l3]);
+  dense[idx] = v;
+}
+
+// ------------------------------------------------------------------ nonlinear-term assembly
+// Product order of the z-pass (see tg_ctx.cu):
+//  fluid : 0 u1u1, 1 u2u2, 2 u3u3, 3 u1u2, 4 u2u3, 5 u3u1        (RSprod.cc:52-105)
+//  MHD   : 0 zp1zm1, 1 zp2zm2, 2 zp3zm3, 3 zp1zm2 (v1), 4 zm1zp2 (w1), 5 zp2zm3 (v2),
+//          6 zm2zp3 (w2), 7 zp3zm1 (v3), 8 zm3zp1 (w3)              (RSprod.cc:117-194)
+//  scalar: fluid 0..5, then 6 u1 th, 7 u2 th, 8 u3 th               (compute_nlin_SF.cc)
+template <typename Rp, int PHYS>
+__device__ __forceinline__ void assemble(const void* const* PX, long long idx, double kx, double ky, double kz,
+                                         cx<double>* n) {
+  if constexpr (PHYS == PH_FLUID || PHYS == PH_SCALAR || PHYS == PH_RB) {
+    const cx<double> p0 = ldc<Rp>(PX[0], idx), p1 = ldc<Rp>(PX[1], idx), p2 = ldc<Rp>(PX[2], idx);
+    const cx<double> p3 = ldc<Rp>(PX[3], idx), p4 = ldc<Rp>(PX[4], idx), p5 = ldc<Rp>(PX[5], idx);
+    n[0] = ikdot(kx, ky, kz, p0, p3, p5);
+    n[1] = ikdot(kx, ky, kz, p3, p1, p4);
+    n[2] = ikdot(kx, ky, kz, p5, p4, p2);
+    if constexpr (PHYS != PH_FLUID) {
+      const cx<double> p6 = ldc<Rp>(PX[6], idx), p7 = ldc<Rp>(PX[7], idx), p8 = ldc<Rp>(PX[8], idx);
+      n[3] = ikdot(kx, ky, kz, p6, p7, p8);
+    }
+  } else {
+    cx<double> p[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) p[q] = ldc<Rp>(PX[q], idx);
+    // Zp.nlin (n) and Zm.nlin (nw)
+    const cx<double> n0 = ikdot(kx, ky, kz, p[0], p[3], p[8]);
+    const cx<double> n1 = ikdot(kx, ky, kz, p[4], p[1], p[5]);
+    const cx<double> n2 = ikdot(kx, ky, kz, p[7], p[6], p[2]);
+    const cx<double> w0 = ikdot(kx, ky, kz, p[0], p[4], p[7]);
+    const cx<double> w1 = ikdot(kx, ky, kz, p[3], p[1], p[6]);
+    const cx<double> w2 = ikdot(kx, ky, kz, p[8], p[5], p[2]);
+    // Elsasser_to_UB_nlin (elsasser.cc:118-130)
+    n[0] = 0.5 * (n0 + w0);
+    n[1] = 0.5 * (n1 + w1);
+    n[2] = 0.5 * (n2 + w2);
+    n[3] = 0.5 * (n0 - w0);
+    n[4] = 0.5 * (n1 - w1);
+    n[5] = 0.5 * (n2 - w2);
+  }
+}
+
+template <int PHYS>
+struct NState {
+  static constexpr int v = (PHYS == PH_FLUID) ? 3 : (PHYS == PH_MHD ? 6 : 4);
+};
+
+// rhs = -[nlin - f + i k p] with p = i k.(nlin - f)/K^2 on the velocity (Compute_pressure,
+// Add_pressure_gradient, Compute_rhs); other fields rhs = -(nlin - f).
+__device__ __forceinline__ void project_rhs(cx<double>* r, int ns, double kx, double ky, double kz, double K2) {
+  const cx<double> kN = kdot(kx, ky, kz, r[0], r[1], r[2]);
+  if (K2 > 0) {
+    const double inv = 1.0 / K2;
+    r[0] = mkc<double>(-(r[0].x - kx * inv * kN.x), -(r[0].y - kx * inv * kN.y));
+    r[1] = mkc<double>(-(r[1].x - ky * inv * kN.x), -(r[1].y - ky * inv * kN.y));
+    r[2] = mkc<double>(-(r[2].x - kz * inv * kN.x), -(r[2].y - kz * inv * kN.y));
+  } else {
+    r[0] = mkc<double>(-r[0].x, -r[0].y);
+    r[1] = mkc<double>(-r[1].x, -r[1].y);
+    r[2] = mkc<double>(-r[2].x, -r[2].y);
+  }
+  for (int c = 3; c < ns; ++c) r[c] = mkc<double>(-r[c].x, -r[c].y);
+}
+
+// ------------------------------------------------------------------ RK4 stage kernel
+// IncFluid::Time_advance RK4 (time_advance.cc:100-155) with E(a) = exp(-nu a dt K^2):
+//  stage 1: u1 = E(1/2)(u0 + dt/2 N0),        tot  = dt/6 E(1) N0
+//  stage 2: u2 = E(1/2) u0 + dt/2 N1,         tot += dt/3 E(1/2) N1
+//  stage 3: u3 = E(1/2)(E(1/2) u0 + dt N2),   tot += dt/3 E(1/2) N2
+//  stage 4: u  = E(1) u0 + tot + dt/6 N3   (then the energy of u for the NaN check / Get_dt)
+template <typename Rp, typename Rs, int PHYS, int SRC>
+__global__ void __launch_bounds__(TPB) k_rk(RKArgs a) {
+  constexpr int NS = NState<PHYS>::v;
+  const Geo& g = a.g;
+  const long long idx = (long long)blockIdx.x * TPB + threadIdx.x;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  if (idx < g.S) {
+    int r1, r2, l3;
+    compact_mode(g, idx, r1, r2, l3);
+    if (l3 < g.nkz) {
+      const int kxi = geo_kx(g, r1), kyi = geo_ky(g, r2);
+      const double kx = kxi * g.kf0, ky = kyi * g.kf1, kz = l3 * g.kf2;
+      const double K2 = kx * kx + ky * ky + kz * kz;
+      cx<double> r[NS];
+      if constexpr (SRC == 0) {
+        assemble<Rp, PHYS>(a.PX, idx, kx, ky, kz, r);
+        if (a.FB != nullptr && kxi >= -a.fx && kxi <= a.fx && kyi >= -a.fy && kyi <= a.fy && l3 <= a.fz) {
+          const int box = (2 * a.fx + 1) * (2 * a.fy + 1) * (a.fz + 1);
+          const int p = ((kxi + a.fx) * (2 * a.fy + 1) + (kyi + a.fy)) * (a.fz + 1) + l3;
+#pragma unroll
+          for (int c = 0; c < NS; ++c) r[c] = r[c] - a.FB[(long long)c * box + p];
+        }
+        project_rhs(r, NS, kx, ky, kz, K2);
+      } else {
+#pragma unroll
+        for (int c = 0; c < NS; ++c) r[c] = a.RHS[c][idx];
+      }
+      const double dt = *a.dt;
+      const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
+#pragma unroll
+      for (int c = 0; c < NS; ++c) {
+        const double eh = exp(-a.nu[c] * 0.5 * dt * K2);
+        const cx<double> u0 = a.U0[c][idx];
+        const cx<double> rc = r[c];
+        if (a.stage == 1) {
+          const double e1 = exp(-a.nu[c] * dt * K2);
+          stc<Rs>(a.US[c], idx, eh * (u0 + (0.5 * dt) * rc));
+          a.TOT[c][idx] = (dt / 6.0) * (e1 * rc);
+        } else if (a.stage == 2) {
+          stc<Rs>(a.US[c], idx, eh * u0 + (0.5 * dt) * rc);
+          a.TOT[c][idx] = a.TOT[c][idx] + (dt / 3.0) * (eh * rc);
+        } else if (a.stage == 3) {
+          stc<Rs>(a.US[c], idx, eh * (eh * u0 + dt * rc));
+          a.TOT[c][idx] = a.TOT[c][idx] + (dt / 3.0) * (eh * rc);
+        } else {
+          const double e1 = exp(-a.nu[c] * dt * K2);
+          const cx<double> tot = a.TOT[c][idx] + (dt / 6.0) * rc;
+          const cx<double> u = e1 * u0 + tot;
+          a.U0[c][idx] = u;
+          const double m2 = u.x * u.x + u.y * u.y;
+          const int grp = (PHYS == PH_MHD) ? (c / 3) * 2 : (c < 3 ? 0 : 4);
+          acc[grp] += energy_weight_four(l1, l2, l3, g.N1, g.N2) * m2;
+          acc[grp + 1] += mult_four(l1, l2, l3, g.N1, g.N2) * K2 * m2;
+        }
+      }
+    }
+  }
+  if (a.stage == 4 && a.part != nullptr) {
+    block_sum<6>(acc);
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int j = 0; j < 6; ++j) a.part[(long long)blockIdx.x * 8 + j] = acc[j];
+    }
+  }
+}
+
+template <typename Rp, typename Rs, int PHYS>
+cudaError_t run_rk_src(const RKArgs& a, int src, cudaStream_t s, int nblk) {
+  if (src == 0) k_rk<Rp, Rs, PHYS, 0><<<nblk, TPB, 0, s>>>(a);
+  else k_rk<Rp, Rs, PHYS, 1><<<nblk, TPB, 0, s>>>(a);
+  return cudaGetLastError();
+}
+template <typename Rp, typename Rs>
+cudaError_t run_rk_phys(const RKArgs& a, int phys, int src, cudaStream_t s, int nblk) {
+  switch (phys) {
+    case PH_FLUID: return run_rk_src<Rp, Rs, PH_FLUID>(a, src, s, nblk);
+    case PH_MHD: return run_rk_src<Rp, Rs, PH_MHD>(a, src, s, nblk);
+    case PH_SCALAR: return run_rk_src<Rp, Rs, PH_SCALAR>(a, src, s, nblk);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// ------------------------------------------------------------------ forcing
+// Compute_force_const_energy_helicity_supply (compute_force_ek_hk_supply.cc:51-157) with
+// Force_alpha_beta (force_alpha_beta.cc:60-121) and the reality condition of the force
+// (Satisfy_reality_array universal_misc.cc:51-109).  One block.
+template <typename Ru>
+__global__ void __launch_bounds__(TPB) k_force_supply(ForceArgs a) {
+  const Geo& g = a.g;
+  const int ny = 2 * a.fy + 1, nz = a.fz + 1;
+  const int box = (2 * a.fx + 1) * ny * nz;
+  for (int p = threadIdx.x; p < box; p += TPB) {
+    const int kz = p % nz;
+    const int ky = (p / nz) % ny - a.fy;
+    const int kx = p / (nz * ny) - a.fx;
+    cx<double> F[3] = {mkc<double>(0, 0), mkc<double>(0, 0), mkc<double>(0, 0)};
+    const double kkx = kx * g.kf0, kky = ky * g.kf1, kkz = kz * g.kf2;
+    const double km = sqrt(kkx * kkx + kky * kky + kkz * kkz);
+    if (km > a.inner && km <= a.outer) {
+      const int lx = kx >= 0 ? kx : kx + g.N1;
+      const int ly = ky >= 0 ? ky : ky + g.N2;
+      const int r1 = (lx >= 0 && lx < g.N1) ? amap_row(g.ax, lx) : -1;
+      const int r2 = (ly >= 0 && ly < g.N2) ? amap_row(g.ay, ly) : -1;
+      cx<double> v[3] = {mkc<double>(0, 0), mkc<double>(0, 0), mkc<double>(0, 0)};
+      if (r1 >= 0 && r2 >= 0 && kz < g.nkz) {
+        const long long i = ((long long)r1 * g.nky + r2) * g.kzp + kz;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) v[c] = ldc<Ru>(a.U[c], i);
+      }
+      const double Ek = 0.5 * (v[0].x * v[0].x + v[0].y * v[0].y + v[1].x * v[1].x + v[1].y * v[1].y +
+                               v[2].x * v[2].x + v[2].y * v[2].y);
+      if (Ek > 1e-15) {
+        // modal helicity k . (Vr x Vi)  (Get_Modal_helicity_FOUR four_basic.cc:136-155)
+        const double cx_ = v[1].x * v[2].y - v[2].x * v[1].y;
+        const double cy_ = v[2].x * v[0].y - v[0].x * v[2].y;
+        const double cz_ = v[0].x * v[1].y - v[1].x * v[0].y;
+        const double Hk = kkx * cx_ + kky * cy_ + kkz * cz_;
+        const double temp = a.e_per_mode / (2 * Ek);
+        const double sk = Hk / (km * Ek);
+        double alpha, beta;
+        if (fabs(sk * sk - 1) > 1e-5) {
+          alpha = temp * (1 - sk * a.eps_h) / (1 - sk * sk);
+          beta = temp * (a.eps_h - sk) / (1 - sk * sk);
+        } else {
+          alpha = temp / 2;
+          beta = alpha / (sk * km);
+        }
+        cx<double> w[3] = {mkc<double>(0, 0), mkc<double>(0, 0), mkc<double>(0, 0)};
+        if (beta > 1e-15) {
+          // vorticity i K x V (Compute_Modal_vorticity_FOUR four_basic.cc:166-186)
+          w[0] = ione(kky * v[2] - kkz * v[1]);
+          w[1] = ione(kkz * v[0] - kkx * v[2]);
+          w[2] = ione(kkx * v[1] - kky * v[0]);
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) F[c] = alpha * v[c] + beta * w[c];
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) a.FB[(long long)c * box + p] = F[c];
+  }
+  __syncthreads();
+  // reality condition on the kz = 0 plane: F(kx, ky<0) = conj F(-kx, -ky); F(kx<0, 0) = conj F(-kx, 0)
+  for (int p = threadIdx.x; p < box; p += TPB) {
+    const int kz = p % nz;
+    const int ky = (p / nz) % ny - a.fy;
+    const int kx = p / (nz * ny) - a.fx;
+    if (kz != 0) continue;
+    if (!(ky < 0 || (ky == 0 && kx < 0))) continue;
+    const int mx = -kx, my = -ky;
+    if (mx < -a.fx || mx > a.fx || my < -a.fy || my > a.fy) continue;
+    const int pm = ((mx + a.fx) * ny + (my + a.fy)) * nz;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) a.FB[(long long)c * box + p] = conjc(a.FB[(long long)c * box + pm]);
+  }
+}
+
+// ------------------------------------------------------------------ fine-grained API kernels
+template <typename Rp, int PHYS>
+__global__ void k_assemble(Geo g, const void* const* PXd, cx<double>* const* NLd) {
+  constexpr int NS = NState<PHYS>::v;
+  const long long idx = (long long)blockIdx.x * TPB + threadIdx.x;
+  if (idx >= g.S) return;
+  int r1, r2, l3;
+  compact_mode(g, idx, r1, r2, l3);
+  cx<double> n[NS];
+  if (l3 < g.nkz) {
+    const double kx = geo_kx(g, r1) * g.kf0, ky = geo_ky(g, r2) * g.kf1, kz = l3 * g.kf2;
+    assemble<Rp, PHYS>(PXd, idx, kx, ky, kz, n);
+  } else {
+#pragma unroll
+    for (int c = 0; c < NS; ++c) n[c] = mkc<double>(0, 0);
+  }
+#pragma unroll
+  for (int c = 0; c < NS; ++c) NLd[c][idx] = n[c];
+}
+
+struct PtrArr6 {
+  cx<double>* p[6];
+  const void* q[9];
+};
+
+template <typename Rp, int PHYS>
+__global__ void k_assemble_v(Geo g, PtrArr6 pa) {
+  constexpr int NS = NState<PHYS>::v;
+  const long long idx = (long long)blockIdx.x * TPB + threadIdx.x;
+  if (idx >= g.S) return;
+  int r1, r2, l3;
+  compact_mode(g, idx, r1, r2, l3);
+  cx<double> n[NS];
+  if (l3 < g.nkz) {
+    const double kx = geo_kx(g, r1) * g.kf0, ky = geo_ky(g, r2) * g.kf1, kz = l3 * g.kf2;
+    assemble<Rp, PHYS>(pa.q, idx, kx, ky, kz, n);
+  } else {
+#pragma unroll
+    for (int c = 0; c < NS; ++c) n[c] = mkc<double>(0, 0);
+  }
+#pragma unroll
+  for (int c = 0; c < NS; ++c) pa.p[c][idx] = n[c];
+}
+
+__global__ void k_sub_force_box(Geo g, int ncomp, const cx<double>* FB, int fx, int fy, int fz, PtrArr6 pa) {
+  const int ny = 2 * fy + 1, nz = fz + 1;
+  const int box = (2 * fx + 1) * ny * nz;
+  const int p = blockIdx.x * TPB + threadIdx.x;
+  if (p >= box) return;
+  const int kz = p % nz;
+  const int ky = (p / nz) % ny - fy;
+  const int kx = p / (nz * ny) - fx;
+  const int lx = kx >= 0 ? kx : kx + g.N1;
+  const int ly = ky >= 0 ? ky : ky + g.N2;
+  if (lx < 0 || lx >= g.N1 || ly < 0 || ly >= g.N2 || kz >= g.nkz) return;
+  const int r1 = amap_row(g.ax, lx), r2 = amap_row(g.ay, ly);
+  if (r1 < 0 || r2 < 0) return;
+  const long long i = ((long long)r1 * g.nky + r2) * g.kzp + kz;
+  for (int c = 0; c < ncomp; ++c) pa.p[c][i] = pa.p[c][i] - FB[(long long)c * box + p];
+}
+
+__global__ void k_pressure(Geo g, PtrArr6 pa, cx<double>* PR) {
+  const long long idx = (long long)blockIdx.x * TPB + threadIdx.x;
+  if (idx >= g.S) return;
+  int r1, r2, l3;
+  compact_mode(g, idx, r1, r2, l3);
+  cx<double> p = mkc<double>(0, 0);
+  if (l3 < g.nkz) {
+    const double kx = geo_kx(g, r1) * g.kf0, ky = geo_ky(g, r2) * g.kf1, kz = l3 * g.kf2;
+    const double K2 = kx * kx + ky * ky + kz * kz;
+    // Compute_divergence_nlin then CS_divide_ksqr (A(0,0,0) = 0)
+    if (K2 > 0) p = (1.0 / K2) * ikdot(kx, ky, kz, pa.p[0][idx], pa.p[1][idx], pa.p[2][idx]);
+  }
+  PR[idx] = p;
+}
+
+__global__ void k_rhs_from_nlin(Geo g, int ns, PtrArr6 pa, const cx<double>* PR) {
+  const long long idx = (long long)blockIdx.x * TPB + threadIdx.x;
+  if (idx >= g.S) return;
+  int r1, r2, l3;
+  compact_mode(g, idx, r1, r2, l3);
+  if (l3 >= g.nkz) return;
+  const double kx = geo_kx(g, r1) * g.kf0, ky = geo_ky(g, r2) * g.kf1, kz = l3 * g.kf2;
+  const cx<double> p = PR[idx];
+  // Add_pressure_gradient: nlin_i += i k_i p; Compute_rhs: nlin = -nlin
+  const cx<double> g0 = ione(kx * p), g1 = ione(ky * p), g2 = ione(kz * p);
+  pa.p[0][idx] = mkc<double>(0, 0) - (pa.p[0][idx] + g0);
+  pa.p[1][idx] = mkc<double>(0, 0) - (pa.p[1][idx] + g1);
+  pa.p[2][idx] = mkc<double>(0, 0) - (pa.p[2][idx] + g2);
+  for (int c = 3; c < ns; ++c) pa.p[c][idx] = mkc<double>(0, 0) - pa.p[c][idx];
+}
+
+// ------------------------------------------------------------------ reductions
+__global__ void __launch_bounds__(TPB) k_energy_partials(Geo g, PtrArr6 pa, int nf, double* part, int slot, int nslots) {
+  const long long idx = (long long)blockIdx.x * TPB + threadIdx.x;
+  double acc[2] = {0, 0};
+  if (idx < g.S) {
+    int r1, r2, l3;
+    compact_mode(g, idx, r1, r2, l3);
+    if (l3 < g.nkz) {
+      const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
+      const double kx = geo_kx(g, r1) * g.kf0, ky = geo_ky(g, r2) * g.kf1, kz = l3 * g.kf2;
+      const double K2 = kx * kx + ky * ky + kz * kz;
+      double w, m;
+      if (g.basis == 0) {
+        w = energy_weight_four(l1, l2, l3, g.N1, g.N2);
+        m = mult_four(l1, l2, l3, g.N1, g.N2);
+      } else {
+        m = mult_scft(l1, l2, l3, g.N2);
+        w = (l1 == 0 && l2 == 0 && l3 == 0) ? m - 0.5 : m;
+      }
+      for (int c = 0; c < nf; ++c) {
+        const cx<double> u = pa.p[c][idx];
+        const double m2 = u.x * u.x + u.y * u.y;
+        acc[0] += w * m2;
+        acc[1] += m * K2 * m2;
+      }
+    }
+  }
+  block_sum<2>(acc);
+  if (threadIdx.x == 0) {
+    part[(long long)blockIdx.x * nslots + slot] = acc[0];
+    part[(long long)blockIdx.x * nslots + slot + 1] = acc[1];
+  }
+}
+
+__global__ void __launch_bounds__(TPB) k_finalize(FinalizeArgs a) {
+  __shared__ double red[TPB];
+  for (int j = 0; j < a.nslots; ++j) {
+    double s = 0;
+    for (int b = threadIdx.x; b < a.nblocks; b += TPB) s += a.part[(long long)b * a.nslots + j];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = TPB / 2; o > 0; o >>= 1) {
+      if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) a.out[j] = red[0];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && a.dt_mode == 1) {
+    // time advanced by the step that just ended, then Get_dt for the next step
+    a.scal[1] += a.scal[0];
+    a.scal[2] += 1.0;
+    double E = a.out[0] + (a.mhd ? a.out[2] : 0.0);
+    if (!(E == E) || E > 1e300 || E < -1e300) a.scal[3] = 1.0;
+    if (a.ering != nullptr) {
+      const int pos = *a.ering_pos;
+      a.ering[pos] = E;
+      *a.ering_pos = pos + 1;
+    }
+    double dt = (E > 0) ? a.dx / (sqrt(E) * 20.0) : a.Tdt;
+    if (a.mhd && a.B0[0] != nullptr) {
+      const double b0 = a.B0[0][0].x, b1 = a.B0[1][0].x, b2 = a.B0[2][0].x;
+      const double B0sqr = b0 * b0 + b1 * b1 + b2 * b2;
+      if (B0sqr > 1e-15) dt = fmin(dt, a.dx / (sqrt(B0sqr) * 20.0));
+    }
+    a.scal[0] = fmin(dt, a.Tdt);
+  } else if (threadIdx.x == 0 && a.dt_mode == 2) {
+    // Get_dt only (no time advance)
+    double E = a.out[0] + (a.mhd ? a.out[2] : 0.0);
+    double dt = (E > 0) ? a.dx / (sqrt(E) * 20.0) : a.Tdt;
+    if (a.mhd && a.B0[0] != nullptr) {
+      const double b0 = a.B0[0][0].x, b1 = a.B0[1][0].x, b2 = a.B0[2][0].x;
+      const double B0sqr = b0 * b0 + b1 * b1 + b2 * b2;
+      if (B0sqr > 1e-15) dt = fmin(dt, a.dx / (sqrt(B0sqr) * 20.0));
+    }
+    a.scal[0] = fmin(dt, a.Tdt);
+  }
+}
+
+__global__ void __launch_bounds__(TPB) k_shell_spectrum(Geo g, PtrArr6 pa, int nf, double n_pow, double* ek, double* cnt, int nbins) {
+  extern __shared__ double sh[];  // [(nf + 1) * nbins]
+  for (int i = threadIdx.x; i < (nf + 1) * nbins; i += TPB) sh[i] = 0;
+  __syncthreads();
+  const long long stride = (long long)gridDim.x * TPB;
+  for (long long idx = (long long)blockIdx.x * TPB + threadIdx.x; idx < g.S; idx += stride) {
+    int r1, r2, l3;
+    compact_mode(g, idx, r1, r2, l3);
+    if (l3 >= g.nkz) continue;
+    const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
+    const double kx = geo_kx(g, r1) * g.kf0, ky = geo_ky(g, r2) * g.kf1, kz = l3 * g.kf2;
+    const double K = sqrt(kx * kx + ky * ky + kz * kz);
+    const int bin = (int)ceil(K);
+    if (bin >= nbins) continue;
+    const double m = (g.basis == 0) ? mult_four(l1, l2, l3, g.N1, g.N2) : mult_scft(l1, l2, l3, g.N2);
+    const double kp = (n_pow == 0.0) ? 1.0 : pow(K, n_pow);
+    for (int c = 0; c < nf; ++c) {
+      const cx<double> u = pa.p[c][idx];
+      atomicAdd(&sh[c * nbins + bin], m * kp * (u.x * u.x + u.y * u.y));
+    }
+    atomicAdd(&sh[nf * nbins + bin], m);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nf * nbins; i += TPB)
+    if (sh[i] != 0) atomicAdd(&ek[i], sh[i]);
+  for (int i = threadIdx.x; i < nbins; i += TPB)
+    if (sh[nf * nbins + i] != 0) atomicAdd(&cnt[i], sh[nf * nbins + i]);
+}
+
+inline int nblk(long long n) { return (int)((n + TPB - 1) / TPB); }
+
+}  // namespace
+
+cudaError_t launch_dense_to_compact(const Geo& g, const cx<double>* dense, void* compact, int cprec, cudaStream_t s) {
+  if (cprec == 0) k_dense_to_compact<double><<<nblk(g.S), TPB, 0, s>>>(g, dense, (cx<double>*)compact);
+  else k_dense_to_compact<float><<<nblk(g.S), TPB, 0, s>>>(g, dense, (cx<float>*)compact);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_compact_to_dense(const Geo& g, const void* compact, int cprec, cx<double>* dense, cudaStream_t s) {
+  const long long D = (long long)g.N1 * g.N2 * (g.N3 / 2 + 1);
+  if (cprec == 0) k_compact_to_dense<double><<<nblk(D), TPB, 0, s>>>(g, (const cx<double>*)compact, dense);
+  else k_compact_to_dense<float><<<nblk(D), TPB, 0, s>>>(g, (const cx<float>*)compact, dense);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rk(const RKArgs& a, int phys, int pprec, int sprec, int src, cudaStream_t s, int* nblocks) {
+  const int nb = nblk(a.g.S);
+  if (nblocks) *nblocks = nb;
+  if (pprec == 0 && sprec == 0) return run_rk_phys<double, double>(a, phys, src, s, nb);
+  if (pprec == 1 && sprec == 1) return run_rk_phys<float, float>(a, phys, src, s, nb);
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_force_supply(const ForceArgs& a, cudaStream_t s) {
+  if (a.uprec == 0) k_force_supply<double><<<1, TPB, 0, s>>>(a);
+  else k_force_supply<float><<<1, TPB, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_assemble_nlin(const Geo& g, int phys, int pprec, const void* const* PX, cx<double>* const* NL, cudaStream_t s) {
+  PtrArr6 pa{};
+  const int ns = phys == PH_FLUID ? 3 : (phys == PH_MHD ? 6 : 4);
+  const int np = phys == PH_FLUID ? 6 : 9;
+  for (int c = 0; c < ns; ++c) pa.p[c] = NL[c];
+  for (int q = 0; q < np; ++q) pa.q[q] = PX[q];
+  const int nb = nblk(g.S);
+#define TG_ASM(RP)                                                         \
+  switch (phys) {                                                          \
+    case PH_FLUID: k_assemble_v<RP, PH_FLUID><<<nb, TPB, 0, s>>>(g, pa); break; \
+    case PH_MHD: k_assemble_v<RP, PH_MHD><<<nb, TPB, 0, s>>>(g, pa); break;     \
+    default: k_assemble_v<RP, PH_SCALAR><<<nb, TPB, 0, s>>>(g, pa); break;      \
+  }
+  if (pprec == 0) {
+    TG_ASM(double)
+  } else {
+    TG_ASM(float)
+  }
+#undef TG_ASM
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sub_force_box(const Geo& g, int ncomp, const cx<double>* FB, int fx, int fy, int fz, cx<double>* const* NL, cudaStream_t s) {
+  PtrArr6 pa{};
+  for (int c = 0; c < ncomp; ++c) pa.p[c] = NL[c];
+  const int box = (2 * fx + 1) * (2 * fy + 1) * (fz + 1);
+  k_sub_force_box<<<(box + TPB - 1) / TPB, TPB, 0, s>>>(g, ncomp, FB, fx, fy, fz, pa);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pressure(const Geo& g, const cx<double>* const* NL, cx<double>* PR, cudaStream_t s) {
+  PtrArr6 pa{};
+  for (int c = 0; c < 3; ++c) pa.p[c] = const_cast<cx<double>*>(NL[c]);
+  k_pressure<<<nblk(g.S), TPB, 0, s>>>(g, pa, PR);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rhs_from_nlin(const Geo& g, int phys, cx<double>* const* NL, const cx<double>* PR, cudaStream_t s) {
+  PtrArr6 pa{};
+  const int ns = phys == PH_FLUID ? 3 : (phys == PH_MHD ? 6 : 4);
+  for (int c = 0; c < ns; ++c) pa.p[c] = NL[c];
+  k_rhs_from_nlin<<<nblk(g.S), TPB, 0, s>>>(g, ns, pa, PR);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_energy_partials(const Geo& g, const cx<double>* const* F, int nf, double* part, int slot, int nslots, cudaStream_t s, int* nblocks) {
+  PtrArr6 pa{};
+  for (int c = 0; c < nf; ++c) pa.p[c] = const_cast<cx<double>*>(F[c]);
+  const int nb = nblk(g.S);
+  if (nblocks) *nblocks = nb;
+  k_energy_partials<<<nb, TPB, 0, s>>>(g, pa, nf, part, slot, nslots);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_finalize(const FinalizeArgs& a, cudaStream_t s) {
+  k_finalize<<<1, TPB, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_shell_spectrum(const Geo& g, const cx<double>* const* F, int nf, double n_pow, double* ek, double* cnt, int nbins, cudaStream_t s) {
+  PtrArr6 pa{};
+  for (int c = 0; c < nf; ++c) pa.p[c] = const_cast<cx<double>*>(F[c]);
+  const size_t smem = (size_t)(nf + 1) * nbins * sizeof(double);
+  if (smem > 200 * 1024) return cudaErrorInvalidValue;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_shell_spectrum, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  int nb = nblk(g.S);
+  if (nb > 148 * 8) nb = 148 * 8;
+  k_shell_spectrum<<<nb, TPB, smem, s>>>(g, pa, nf, n_pow, ek, cnt, nbins);
+  return cudaGetLastError();
+}
+
+}  // namespace tg

@@ -1,0 +1,248 @@
+"""Python mirror of Tarang's field/solver class API over the C ABI (include/tarang_gpu.h).
+
+Method names follow the reference (lib/IncFluid/IncFluid.h, lib/IncFlow/IncVF.h,
+lib/fields/Cvf.h) so that a driver written against the reference reads the same:
+
+    U = IncFluid(N=(64, 64, 64), nu=0.01, dt=1e-3)
+    U.set_V([v1, v2, v3])                     # spectral fields, (N1, N2, N3/2+1) complex128
+    for it in range(100):                     # Ifluid_main.cc:258-301
+        U.Compute_force(); U.Compute_nlin(); U.Add_force(); U.Compute_pressure()
+        U.Tdt = U.Get_dt(); U.Time_advance()
+        E, D = U.CV_Compute_totalenergy_diss()
+
+``IncFluid.step(n)`` runs the same loop body n times in one call (one CUDA graph per step).
+Every call goes to the CUDA library; there is no CPU path.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+
+_BASIS = {"FOUR": L.TG_FOUR, "SCFT": L.TG_SCFT}
+_PHYS = {"FLUID": L.TG_FLUID, "INC_FLUID": L.TG_FLUID, "MHD": L.TG_MHD, "INC_MHD": L.TG_MHD,
+         "SCALAR": L.TG_SCALAR, "INC_SCALAR": L.TG_SCALAR, "RB": L.TG_RB, "RB_SLIP": L.TG_RB}
+_PREC = {"FP64": L.TG_FP64, "FP32": L.TG_FP32_MIXED, "FP32_MIXED": L.TG_FP32_MIXED}
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def make_config(N, basis="FOUR", physics="FLUID", precision="FP64", dealias=True,
+                kfactor=(1.0, 1.0, 1.0), nu=0.01, eta=None, kappa=None, dt=1e-3,
+                force=None, n_shells=12, device=0, Ra=0.0, Pr=0.0, stream=None) -> L.tg_config:
+    lib = L.load()
+    cfg = L.tg_config()
+    lib.tg_config_default(C.byref(cfg))
+    cfg.N[:] = [int(n) for n in N]
+    cfg.basis = _BASIS[basis] if isinstance(basis, str) else int(basis)
+    cfg.physics = _PHYS[physics] if isinstance(physics, str) else int(physics)
+    cfg.precision = _PREC[precision] if isinstance(precision, str) else int(precision)
+    cfg.dealias = 1 if dealias else 0
+    cfg.scheme = L.TG_RK4
+    cfg.kfactor[:] = [float(k) for k in kfactor]
+    cfg.nu = float(nu)
+    cfg.eta = float(nu if eta is None else eta)
+    cfg.kappa = float(nu if kappa is None else kappa)
+    cfg.dt = float(dt)
+    if force is None or force == "decay":
+        cfg.force_kind = L.TG_FORCE_DECAY
+    else:
+        cfg.force_kind = L.TG_FORCE_ENERGY_SUPPLY
+        p = [force.get("inner"), force.get("outer"), force.get("eps"), force.get("eps_h", 0.0)]
+        cfg.force_para[:] = [float(x) for x in p]
+    cfg.n_shells = int(n_shells)
+    cfg.rb_ra = float(Ra)
+    cfg.rb_pr = float(Pr)
+    cfg.device = int(device)
+    cfg.stream = C.c_void_p(int(stream)) if stream else None
+    return cfg
+
+
+class IncFluid:
+    """Solver context: the reference's IncFluid U (with IncVF W for MHD, IncSF T for scalars)."""
+
+    def __init__(self, N, **kw):
+        self.lib = L.load()
+        self.N = tuple(int(n) for n in N)
+        self.cfg = make_config(self.N, **kw)
+        self.kw = kw
+        h = C.c_void_p()
+        rc = self.lib.tg_ctx_create(C.byref(self.cfg), C.byref(h))
+        if rc != L.TG_OK:
+            raise L.TarangError(rc, "tg_ctx_create failed")
+        self.h = h
+        self.shape = (self.N[0], self.N[1], self.N[2] // 2 + 1)
+        self.ndoubles = 2 * self.shape[0] * self.shape[1] * self.shape[2]
+        self.Tdt = self.cfg.dt
+
+    # ------------------------------------------------------------------ lifetime
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.tg_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, rc, what):
+        if rc != L.TG_OK:
+            msg = self.lib.tg_last_error(self.h)
+            raise L.TarangError(rc, f"{what}: {msg.decode() if msg else ''}")
+        return rc
+
+    # ------------------------------------------------------------------ fields
+    def upload(self, field: int, arr: np.ndarray):
+        a = np.ascontiguousarray(arr, dtype=np.complex128)
+        if a.shape != self.shape:
+            raise ValueError(f"field shape {a.shape} != {self.shape}")
+        self._ck(self.lib.tg_field_upload(self.h, field, _dptr(a.view(np.float64)), self.ndoubles), "upload")
+
+    def download(self, field: int) -> np.ndarray:
+        out = np.empty(self.shape, dtype=np.complex128)
+        self._ck(self.lib.tg_field_download(self.h, field, _dptr(out.view(np.float64)), self.ndoubles), "download")
+        return out
+
+    def set_V(self, V):
+        for i, v in enumerate(V):
+            self.upload(L.TG_V1 + i, v)
+
+    def get_V(self):
+        return [self.download(L.TG_V1 + i) for i in range(3)]
+
+    def set_W(self, W):
+        for i, w in enumerate(W):
+            self.upload(L.TG_W1 + i, w)
+
+    def get_W(self):
+        return [self.download(L.TG_W1 + i) for i in range(3)]
+
+    def set_T(self, T):
+        self.upload(L.TG_T, T)
+
+    def get_T(self):
+        return self.download(L.TG_T)
+
+    def get_nlin(self):
+        return [self.download(L.TG_NLIN1 + i) for i in range(3)]
+
+    def get_Wnlin(self):
+        return [self.download(L.TG_WNLIN1 + i) for i in range(3)]
+
+    def get_Tnlin(self):
+        return self.download(L.TG_TNLIN)
+
+    def get_pressure(self):
+        return self.download(L.TG_PRESSURE)
+
+    def get_force(self):
+        return [self.download(L.TG_FORCE1 + i) for i in range(3)]
+
+    # ------------------------------------------------------------------ transforms
+    def Forward_transform_array(self, real_packed: np.ndarray, parity: int = 0, slot: int = 0) -> np.ndarray:
+        """universal_tr.cc:66-86 on a work field: real data in the reference's in-place layout."""
+        f = L.TG_WORK0 + slot
+        self.upload(f, real_packed)
+        self._ck(self.lib.tg_forward_transform(self.h, f, parity), "forward")
+        return self.download(f)
+
+    def Inverse_transform_array(self, spec: np.ndarray, parity: int = 0, slot: int = 0) -> np.ndarray:
+        """universal_tr.cc:126-146 on a work field; returns the packed real layout."""
+        f = L.TG_WORK0 + slot
+        self.upload(f, spec)
+        self._ck(self.lib.tg_inverse_transform(self.h, f, parity), "inverse")
+        return self.download(f)
+
+    # ------------------------------------------------------------------ solver calls
+    def Compute_force(self):
+        self._ck(self.lib.tg_compute_force(self.h), "Compute_force")
+
+    def Compute_nlin(self):
+        self._ck(self.lib.tg_compute_nlin(self.h), "Compute_nlin")
+
+    def Add_force(self):
+        self._ck(self.lib.tg_add_force(self.h), "Add_force")
+
+    def Compute_pressure(self):
+        self._ck(self.lib.tg_compute_pressure(self.h), "Compute_pressure")
+
+    def Compute_rhs(self):
+        self._ck(self.lib.tg_compute_rhs(self.h), "Compute_rhs")
+
+    def Get_dt(self) -> float:
+        dt = C.c_double()
+        self._ck(self.lib.tg_get_dt(self.h, C.byref(dt)), "Get_dt")
+        self.Tdt = dt.value
+        return dt.value
+
+    def Time_advance(self):
+        self._ck(self.lib.tg_time_advance(self.h), "Time_advance")
+
+    def step(self, n: int = 1, energies: bool = True):
+        """n iterations of the loop body Ifluid_main.cc:261-286; returns E after each step."""
+        e = np.empty(max(n, 1), dtype=np.float64)
+        rc = self.lib.tg_step(self.h, int(n), _dptr(e) if energies else None)
+        self._ck(rc, "step")
+        return e[:n]
+
+    def synchronize(self):
+        self._ck(self.lib.tg_synchronize(self.h), "synchronize")
+
+    def time(self):
+        t = C.c_double()
+        s = C.c_longlong()
+        self._ck(self.lib.tg_time(self.h, C.byref(t), C.byref(s)), "time")
+        return t.value, s.value
+
+    def device_bytes(self) -> int:
+        b = C.c_size_t()
+        self._ck(self.lib.tg_device_bytes(self.h, C.byref(b)), "device_bytes")
+        return b.value
+
+    # ------------------------------------------------------------------ diagnostics
+    def CV_Compute_totalenergy_diss(self, group: int = 0):
+        E = C.c_double()
+        D = C.c_double()
+        self._ck(self.lib.tg_energy(self.h, group, C.byref(E), C.byref(D)), "energy")
+        return E.value, D.value
+
+    def kmax_outside(self) -> int:
+        import math
+        d = 3 if self.cfg.dealias else 2
+        kf = self.cfg.kfactor
+        N = self.N
+        return int(math.ceil(math.sqrt(((N[0] // d) * kf[0]) ** 2 + ((N[1] // d) * kf[1]) ** 2
+                                       + ((N[2] // d) * kf[2]) ** 2)))
+
+    def CV_Compute_shell_spectrum(self, group: int = 0):
+        n = self.kmax_outside() + 1
+        nc = 1 if group == 2 else 3
+        ek = np.zeros(nc * n)
+        dk = np.zeros(n)
+        self._ck(self.lib.tg_shell_spectrum(self.h, group, _dptr(ek), _dptr(dk), n), "shell spectrum")
+        return ek.reshape(nc, n), dk
+
+    def ET_radii(self):
+        S = self.cfg.n_shells
+        r = np.zeros(S + 1)
+        self._ck(self.lib.tg_et_radii(self.h, _dptr(r), S + 1), "et radii")
+        return r
+
+    def Compute_flux(self, kind: int = L.TG_ET_UU):
+        S = self.cfg.n_shells
+        f = np.zeros(S + 1)
+        self._ck(self.lib.tg_flux(self.h, kind, _dptr(f), S + 1), "flux")
+        return f
+
+    def Compute_shell_tr(self, kind: int = L.TG_ET_UU):
+        S = self.cfg.n_shells
+        t = np.zeros((S + 1) * (S + 1))
+        self._ck(self.lib.tg_shell_to_shell(self.h, kind, _dptr(t), S + 1), "shell_tr")
+        return t.reshape(S + 1, S + 1)
