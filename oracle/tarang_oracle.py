@@ -776,8 +776,13 @@ def shell_mult_single(A, B, inner, outer, kfactor, basis="FOUR"):
 
 
 def shell_index(K, R):
-    """Get_shell_index  basis_basicfn.cc:288-299: first index with K <= R[index]."""
-    return np.searchsorted(R, K, side="left")
+    """Get_shell_index  basis_basicfn.cc:288-299: the first index (linear scan) with
+    K <= R[index].  The radii need not be sorted (scheme 0 with R_in <= 16)."""
+    K = np.asarray(K)
+    out = np.full(K.shape, len(R), dtype=np.int64)
+    for i in range(len(R) - 1, -1, -1):
+        out = np.where(K <= R[i], i, out)
+    return out
 
 
 def shell_mult_all(As, Bs, R, kfactor, alias="DEALIAS", basis="FOUR"):
@@ -817,6 +822,38 @@ def compute_shell_tr(V, kfactor, no_shells, alias="DEALIAS", basis="FOUR"):
         G = [fill_array_shell(v, R[n_ - 1], R[n_], kfactor, basis) for v in V]
         n = et_nlin(V, G, kfactor, basis)
         T[n_, :] = -shell_mult_all(n, V, R, kfactor, alias, basis)
+    return T
+
+
+def compute_flux_generic(H, F, Rf, sign, kfactor, no_shells, alias="DEALIAS", basis="FOUR"):
+    """The flux loops of IncVF::Compute_flux(IncVF& W)  compute_flux.cc:140-215 in one form:
+    for sphere s, G = F on 0 < |K| <= R_s, N = D_j F(H_j G_i) (EnergyTr_Compute_nlin with helper
+    H), flux(s) = sign * sum_{|K| > R_s} 2 mult Re(N . Rf*).
+      U->U: (H, F, Rf, sign) = (U, U, U, -1)   flux_self            (:52-69)
+      B->B: (U, B, B, -1)                      W.flux_self          (:168-181)
+      U->B: (B, U, B, +1)                      flux_VF_in_out       (:150-163)
+      B->U: (U, B, U, +1)                      W.flux_VF_in_out     (:187-201)"""
+    N = (H[0].shape[0], H[0].shape[1], 2 * (H[0].shape[2] - 1))
+    R = et_radii(N, kfactor, no_shells, alias, basis)
+    flux = np.zeros(no_shells + 1)
+    for s in range(1, no_shells + 1):
+        G = [fill_array_shell(f, 0.0, R[s], kfactor, basis) for f in F]
+        n = et_nlin(H, G, kfactor, basis)
+        flux[s] = sign * sum(shell_mult_single(n[i], Rf[i], R[s], INF_RADIUS, kfactor, basis) for i in range(3))
+    return flux
+
+
+def compute_shell_tr_generic(H, F, Rf, sign, kfactor, no_shells, alias="DEALIAS", basis="FOUR"):
+    """The shell-to-shell loops of IncVF::Compute_shell_tr(IncVF& W)  compute_shell_tr.cc:156-200:
+    row n = sign * Shell_mult_all(D_j F(H_j F^(n)_i), Rf).
+      U->U: (U, U, U, -1); B->B: (U, B, B, -1) (:163-175); U->B: (B, U, B, +1) (:182-197)."""
+    N = (H[0].shape[0], H[0].shape[1], 2 * (H[0].shape[2] - 1))
+    R = et_radii(N, kfactor, no_shells, alias, basis)
+    T = np.zeros((no_shells + 1, no_shells + 1))
+    for n_ in range(1, no_shells):
+        G = [fill_array_shell(f, R[n_ - 1], R[n_], kfactor, basis) for f in F]
+        n = et_nlin(H, G, kfactor, basis)
+        T[n_, :] = sign * shell_mult_all(n, Rf, R, kfactor, alias, basis)
     return T
 
 

@@ -24,6 +24,19 @@ int cuda_err(tg_ctx* c, cudaError_t e, const char* where) {
   return set_err(c, TG_ERR_CUDA, m);
 }
 
+int dalloc_ctx(tg_ctx* c, void** p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return set_err(c, TG_ERR_OOM, "device allocation of " + std::to_string(bytes) + " bytes failed");
+  }
+  c->bytes += bytes;
+  e = cudaMemsetAsync(*p, 0, bytes, c->st);
+  if (e != cudaSuccess) return cuda_err(c, e, "cudaMemsetAsync");
+  return TG_OK;
+}
+
 }  // namespace tg
 
 #define TG_CK(call)                                        \
@@ -87,38 +100,6 @@ void keep_axis(int N, int axis, int basis, int dealias, int& lo, int& hi) {
 
 AxisMap full_map(int L) { return AxisMap{L, L, 0}; }
 
-// ------------------------------------------------------------------ profiling scopes
-cudaEvent_t prof_event(tg_ctx* c) {
-  if (!c->ev_pool.empty()) {
-    cudaEvent_t e = c->ev_pool.back();
-    c->ev_pool.pop_back();
-    return e;
-  }
-  cudaEvent_t e = nullptr;
-  cudaEventCreate(&e);
-  return e;
-}
-
-struct Prof {
-  tg_ctx* c;
-  long idx = -1;
-  Prof(tg_ctx* c_, const char* name, double bytes) : c(c_) {
-    if (!c->prof) return;
-    tg_ctx::ProfRec r{name, prof_event(c), prof_event(c), bytes};
-    cudaEventRecord(r.a, c->st);
-    c->prof_recs.push_back(r);
-    idx = (long)c->prof_recs.size() - 1;
-  }
-  ~Prof() {
-    if (idx >= 0) cudaEventRecord(c->prof_recs[idx].b, c->st);
-  }
-};
-
-// elements on the stored support of each pipeline stage layout (kz counted to nkz)
-double el_compact(const tg_ctx* c) { return (double)c->g.nkx * c->g.nky * c->g.nkz; }
-double el_xstage(const tg_ctx* c) { return (double)c->N1 * c->g.nky * c->g.nkz; }
-double el_ystage(const tg_ctx* c) { return (double)c->N1 * c->N2 * c->g.nkz; }
-
 int max_radius_inside(const tg_ctx* c) {
   // Max_radius_inside_(de)aliased_FOUR four_inline.h:190-257
   const int d = c->cfg.dealias ? 3 : 2;
@@ -140,139 +121,21 @@ int max_radius_inside(const tg_ctx* c) {
 // inputs: compact fields of precision inprec.  MHD: in[0..2] = U, in[3..5] = B, the x-pass
 // forms z+ = U + B (fields 0..2) and z- = U - B (fields 3..5).
 int run_pipeline(tg_ctx* c, const void* const* in, int inprec) {
-  if (!c->pipeline_ok) return set_err(c, TG_ERR_UNSUPPORTED, "nonlinear term needs N3/2 a power of two in [4, 256]");
-  const Geo& g = c->g;
-  const int nin = c->nin, np = c->nprod;
-  // x inverse
-  {
-    AxisLaunch l;
-    l.L = c->N1;
-    l.dir = +1;
-    l.pin = inprec;
-    l.pout = c->tprec;
-    l.pwork = c->tprec;
-    l.nbatch = 1;
-    l.nfields = nin;
-    l.a.sb = 0;
-    l.a.sr = (long long)g.nky * g.kzp;
-    l.a.db = 0;
-    l.a.dr = (long long)g.nky * g.kzp;
-    l.a.ncols = g.nky * g.kzp;
-    l.a.in = g.ax;
-    l.a.out = full_map(c->N1);
-    l.a.scale = 1.0;
-    l.a.tw = c->tw[c->N1];
-    for (int f = 0; f < nin; ++f) {
-      l.ps.dst[f] = c->WX[f];
-      if (c->phys == TG_MHD) {
-        l.ps.src[f] = in[f % 3];
-        l.ps.src2[f] = in[3 + f % 3];
-        l.a.comb[f] = f < 3 ? +1 : -1;
-      } else {
-        l.ps.src[f] = in[f];
-        l.a.comb[f] = 0;
-      }
+  const void* src[6];
+  const void* src2[6] = {};
+  int comb[6] = {0, 0, 0, 0, 0, 0};
+  for (int f = 0; f < c->nin; ++f) {
+    if (c->phys == TG_MHD) {
+      src[f] = in[f % 3];
+      src2[f] = in[3 + f % 3];
+      comb[f] = f < 3 ? +1 : -1;
+    } else {
+      src[f] = in[f];
     }
-    const double insz = inprec == F64 ? 16.0 : 8.0;
-    Prof pr(c, "x_inverse", c->nstate * el_compact(c) * insz + nin * el_xstage(c) * c->tsz);
-    TG_CK(launch_axis(l, c->st));
   }
-  // y inverse
-  {
-    AxisLaunch l;
-    l.L = c->N2;
-    l.dir = +1;
-    l.pin = l.pout = l.pwork = c->tprec;
-    l.nbatch = c->N1;
-    l.nfields = nin;
-    l.a.sb = (long long)g.nky * g.kzp;
-    l.a.sr = g.kzp;
-    l.a.db = (long long)c->N2 * g.kzp;
-    l.a.dr = g.kzp;
-    l.a.ncols = g.kzp;
-    l.a.in = g.ay;
-    l.a.out = full_map(c->N2);
-    l.a.scale = 1.0;
-    l.a.tw = c->tw[c->N2];
-    for (int f = 0; f < nin; ++f) {
-      l.ps.src[f] = c->WX[f];
-      l.ps.dst[f] = c->WY[f];
-    }
-    Prof pr(c, "y_inverse", nin * (el_xstage(c) + el_ystage(c)) * c->tsz);
-    TG_CK(launch_axis(l, c->st));
-  }
-  // z: inverse, products, forward
-  {
-    ZProdLaunch l;
-    l.M = c->Mz;
-    l.nin = nin;
-    l.nprod = np;
-    l.pin = l.pout = l.pwork = c->tprec;
-    l.a.nrows = (long long)c->N1 * c->N2;
-    l.a.ss = g.kzp;
-    l.a.ds = g.kzp;
-    l.a.nin = g.nkz;
-    l.a.nout = g.nkz;
-    l.a.nfill = g.kzp;
-    l.a.pad = 0;
-    l.a.scale = 1.0 / ((double)c->N1 * c->N2 * c->N3);
-    l.a.twM = c->tw[c->Mz];
-    l.a.twN = c->tw[c->N3];
-    for (int f = 0; f < nin; ++f) l.ps.src[f] = c->WY[f];
-    for (int q = 0; q < np; ++q) l.ps.dst[q] = c->PP[q];
-    l.pp = c->pairs;
-    Prof pr(c, "z_products", (nin + np) * el_ystage(c) * c->tsz);
-    TG_CK(launch_zprod(l, c->st));
-  }
-  // y forward
-  {
-    AxisLaunch l;
-    l.L = c->N2;
-    l.dir = -1;
-    l.pin = l.pout = l.pwork = c->tprec;
-    l.nbatch = c->N1;
-    l.nfields = np;
-    l.a.sb = (long long)c->N2 * g.kzp;
-    l.a.sr = g.kzp;
-    l.a.db = (long long)g.nky * g.kzp;
-    l.a.dr = g.kzp;
-    l.a.ncols = g.kzp;
-    l.a.in = full_map(c->N2);
-    l.a.out = g.ay;
-    l.a.scale = 1.0;
-    l.a.tw = c->tw[c->N2];
-    for (int q = 0; q < np; ++q) {
-      l.ps.src[q] = c->PP[q];
-      l.ps.dst[q] = c->PY[q];
-    }
-    Prof pr(c, "y_forward", np * (el_ystage(c) + el_xstage(c)) * c->tsz);
-    TG_CK(launch_axis(l, c->st));
-  }
-  // x forward
-  {
-    AxisLaunch l;
-    l.L = c->N1;
-    l.dir = -1;
-    l.pin = l.pout = l.pwork = c->tprec;
-    l.nbatch = 1;
-    l.nfields = np;
-    l.a.sb = 0;
-    l.a.sr = (long long)g.nky * g.kzp;
-    l.a.db = 0;
-    l.a.dr = (long long)g.nky * g.kzp;
-    l.a.ncols = g.nky * g.kzp;
-    l.a.in = full_map(c->N1);
-    l.a.out = g.ax;
-    l.a.scale = 1.0;
-    l.a.tw = c->tw[c->N1];
-    for (int q = 0; q < np; ++q) {
-      l.ps.src[q] = c->PY[q];
-      l.ps.dst[q] = c->PX[q];
-    }
-    Prof pr(c, "x_forward", np * (el_xstage(c) + el_compact(c)) * c->tsz);
-    TG_CK(launch_axis(l, c->st));
-  }
-  return TG_OK;
+  int rc = pipe_inverse_xy(c, c->nin, src, src2, comb, inprec, c->nstate, c->WX, c->WY);
+  if (rc) return rc;
+  return pipe_products_forward(c, c->nin, c->WY, c->nprod, c->pairs, c->PP, c->PY, c->PX);
 }
 
 int run_force(tg_ctx* c, const void* const* U, int uprec) {
@@ -289,7 +152,7 @@ int run_force(tg_ctx* c, const void* const* U, int uprec) {
   f.e_per_mode = c->nf_modes > 0 ? c->cfg.force_para[2] / c->nf_modes : 0.0;
   f.eps_h = c->cfg.force_para[3];
   f.FB = c->FB;
-  Prof pr(c, "force", 0.0);
+  ProfScope pr(c, "force", 0.0);
   TG_CK(launch_force_supply(f, c->st));
   return TG_OK;
 }
@@ -333,7 +196,7 @@ int run_finalize(tg_ctx* c, int dt_mode, bool ring) {
     // mean field B0 = real(B(0,0,0)) (compute_dt.cc:86-93): compact index 0 is the origin
     for (int i = 0; i < 3; ++i) f.B0[i] = c->U0[3 + i];
   }
-  Prof pr(c, "finalize", 0.0);
+  ProfScope pr(c, "finalize", 0.0);
   TG_CK(launch_finalize(f, c->st));
   return TG_OK;
 }
@@ -383,7 +246,7 @@ int run_stages(tg_ctx* c, int first_stage, bool ring) {
       const double ns = c->nstate, e = el_compact(c);
       const double rd = c->nprod * e * c->tsz + ns * e * 16 + (stage > 1 ? ns * e * 16 : 0);
       const double wr = (stage < 4) ? ns * e * (c->tsz + 16) : ns * e * 16;
-      Prof pr(c, "rk_stage", rd + wr);
+      ProfScope pr(c, "rk_stage", rd + wr);
       TG_CK(launch_rk(a, c->phys, c->tprec, c->tprec, 0, c->st, nullptr));
     }
   }
@@ -526,6 +389,8 @@ void free_ctx(tg_ctx* c) {
   fr(c->ering);
   fr(c->ering_pos);
   fr(c->diag);
+  for (int i = 0; i < 3; ++i) fr(c->etG[i]);
+  for (int i = 0; i < c->n_et_own; ++i) fr(c->et_own[i]);
   for (int i = 0; i < TG_NFIELDS; ++i) fr(c->dense[i]);
   fr(c->staging);
   for (auto& r : c->prof_recs) {
@@ -722,7 +587,7 @@ int tg_ctx_create(const tg_config* cfg, tg_ctx** out) {
     if ((rc = dalloc(c, &c->PY[q], WXb))) return fail(rc);
     if ((rc = dalloc(c, &c->PX[q], St))) return fail(rc);
   }
-  c->npart_blocks = (int)((g.S + 255) / 256);
+  c->npart_blocks = reduction_blocks(g.S);
   if ((rc = dalloc(c, (void**)&c->part, sizeof(double) * 8 * (size_t)c->npart_blocks))) return fail(rc);
   if ((rc = dalloc(c, (void**)&c->scal, sizeof(double) * 8))) return fail(rc);
   if ((rc = dalloc(c, (void**)&c->red_out, sizeof(double) * 8))) return fail(rc);

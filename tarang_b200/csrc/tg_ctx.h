@@ -62,6 +62,16 @@ struct tg_ctx {
   double* h_pinned = nullptr;  // small pinned host buffer
   double* diag = nullptr;      // diagnostics scratch (spectra, transfer tables)
   size_t diag_cap = 0;
+
+  // energy-transfer buffers (pipeline buffers reused where the physics already has them)
+  bool et_ready = false;
+  tg::cx<double>* etG[3] = {};
+  void* etWY[6] = {};
+  void* etPP[9] = {};
+  void* etPY[9] = {};
+  void* etPX[9] = {};
+  void* et_own[32] = {};
+  int n_et_own = 0;
   double dx_cfl = 0;
 
   // dense fields (reference layout, FP64), allocated on demand
@@ -93,4 +103,24 @@ struct tg_ctx {
 namespace tg {
 int set_err(tg_ctx* c, int code, const std::string& msg);
 int cuda_err(tg_ctx* c, cudaError_t e, const char* where);
+
+// per-launch CUDA events while profiling is enabled (tg_profile_enable)
+struct ProfScope {
+  tg_ctx* c;
+  long idx = -1;
+  ProfScope(tg_ctx* c_, const char* name, double bytes);
+  ~ProfScope();
+};
+double el_compact(const tg_ctx* c);
+double el_xstage(const tg_ctx* c);
+double el_ystage(const tg_ctx* c);
+
+// x- and y-inverse passes of nf compact fields (field f read as in[f] + comb[f] * in2[f]);
+// nread = number of distinct compact fields read (for the byte count)
+int pipe_inverse_xy(tg_ctx* c, int nf, const void* const* in, const void* const* in2, const int* comb,
+                    int inprec, int nread, void* const* WX, void* const* WY);
+// fused z-pass products (pairs pp of the nin inputs), then y- and x-forward passes into PX
+int pipe_products_forward(tg_ctx* c, int nin, const void* const* WY, int nprod, const ProdPairs& pp,
+                          void* const* PP, void* const* PY, void* const* PX);
+int dalloc_ctx(tg_ctx* c, void** p, size_t bytes);
 }  // namespace tg

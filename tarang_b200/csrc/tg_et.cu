@@ -1,4 +1,20 @@
 // Energy transfer diagnostics: shell radii, flux Pi(R) and shell-to-shell transfer.
+//
+// The reference evaluates the energy-transfer nonlinearity N_i = D_j F(H_j G_i)
+// (IncVF::EnergyTr_Compute_nlin, ET_compute_nlin.cc:85-251) once per sphere for the flux
+// (compute_flux.cc:52-304, G = field inside sphere s) and once per shell for the
+// shell-to-shell transfer (compute_shell_tr.cc:59-281, G = field in shell n): 2S-1
+// evaluations of 15 transforms each.  N is linear in G, and every sphere and every shell is a
+// union of the annuli (rho[a-1], rho[a]] between consecutive sorted distinct radii, so here N
+// is evaluated once per giver annulus g (3 inverse + 9 forward transforms, the helper H
+// inverse-transformed once) and contracted in FP64 against the receiver field into a
+// histogram T[g][a] over receiver annuli.  Then
+//   flux(s)       = sign * sum_{rho[g] <= R_s} sum_{rho[a-1] >= R_s} T[g][a]   (Prod_out_sphere_nlinV)
+//   shell_tr(n,m) = sign * sum_{g in shell n} sum_{a: Get_shell_index = m, rho[a] <= R_in} T[g][a]
+//                                                     (Shell_mult_all_FOUR four_ET.cc:181-256)
+// Get_shell_index (basis_basicfn.cc:288-299) is constant on an annulus.  With monotonic radii
+// (R_in > 16) the annuli are the S shells themselves.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -34,6 +50,235 @@ std::vector<double> et_radii(const tg_ctx* c) {
 
 }  // namespace tg
 
+namespace {
+
+constexpr int TPB = 256;
+constexpr int kMaxShells = 63;
+
+// sorted distinct radii rho[0] = 0 < rho[1] < ... < rho[A]; annulus a = (rho[a-1], rho[a]]
+struct Radii {
+  double r[kMaxShells + 1];
+  int S;  // number of annuli A
+};
+
+// G = F on lo < |K| <= hi, else 0  (Fill_array_shell universal_ET.cc:45-65)
+__global__ void k_fill_shell(Geo g, const cx<double>* F0, const cx<double>* F1, const cx<double>* F2,
+                             cx<double>* G0, cx<double>* G1, cx<double>* G2, double lo, double hi) {
+  const long long idx = (long long)blockIdx.x * TPB + threadIdx.x;
+  if (idx >= g.S) return;
+  int r1, r2, l3;
+  compact_mode(g, idx, r1, r2, l3);
+  const double kx = geo_kx(g, r1) * g.kf0, ky = geo_ky(g, r2) * g.kf1, kz = l3 * g.kf2;
+  const double K = sqrt(kx * kx + ky * ky + kz * kz);
+  const bool in = (l3 < g.nkz) && (K > lo) && (K <= hi);
+  const cx<double> z = mkc<double>(0, 0);
+  G0[idx] = in ? F0[idx] : z;
+  G1[idx] = in ? F1[idx] : z;
+  G2[idx] = in ? F2[idx] : z;
+}
+
+struct ContractArgs {
+  Geo g;
+  const void* PX[9];      // P(i, j) = F(H_j G_i), q = 3 i + j
+  const cx<double>* R[2][3];  // receiver fields
+  int nrec;
+  Radii rad;
+  double* hist;           // [nrec][S+1]
+};
+
+// N_i = i k_j P(i, j); hist[r][shell(|K|)] += 2 mult Re(sum_i N_i conj(R_i))
+template <typename Rp>
+__global__ void __launch_bounds__(TPB) k_et_contract(ContractArgs a) {
+  __shared__ double sh[2 * (kMaxShells + 1)];
+  const int nb = a.rad.S + 1;
+  for (int i = threadIdx.x; i < a.nrec * nb; i += TPB) sh[i] = 0;
+  __syncthreads();
+  const Geo& g = a.g;
+  const long long stride = (long long)gridDim.x * TPB;
+  for (long long idx = (long long)blockIdx.x * TPB + threadIdx.x; idx < g.S; idx += stride) {
+    int r1, r2, l3;
+    compact_mode(g, idx, r1, r2, l3);
+    if (l3 >= g.nkz) continue;
+    const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
+    const double kx = geo_kx(g, r1) * g.kf0, ky = geo_ky(g, r2) * g.kf1, kz = l3 * g.kf2;
+    const double K = sqrt(kx * kx + ky * ky + kz * kz);
+    int bin = 0;  // receiver annulus: first rho >= |K|
+    while (bin < a.rad.S && K > a.rad.r[bin]) ++bin;
+    cx<double> N[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const cx<double> p0 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 0])[idx]);
+      const cx<double> p1 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 1])[idx]);
+      const cx<double> p2 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 2])[idx]);
+      const cx<double> s = mkc<double>(kx * p0.x + ky * p1.x + kz * p2.x, kx * p0.y + ky * p1.y + kz * p2.y);
+      N[i] = ione(s);
+    }
+    const double m = mult_four(l1, l2, l3, g.N1, g.N2);
+    for (int r = 0; r < a.nrec; ++r) {
+      double v = 0;
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const cx<double> b = a.R[r][i][idx];
+        v += N[i].x * b.x + N[i].y * b.y;
+      }
+      atomicAdd(&sh[r * nb + bin], 2.0 * m * v);
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < a.nrec * nb; i += TPB)
+    if (sh[i] != 0) atomicAdd(&a.hist[i], sh[i]);
+}
+
+struct KindSpec {
+  int H, F;      // field groups: 0 = U (state 0..2), 1 = B (state 3..5)
+  int R;         // receiver group
+  double sign;
+};
+
+bool kind_spec(const tg_ctx* c, int kind, KindSpec& k) {
+  switch (kind) {
+    case TG_ET_UU: k = {0, 0, 0, -1.0}; return true;
+    case TG_ET_BB: k = {0, 1, 1, -1.0}; break;   // W.flux_self: U.grad W< against W>
+    case TG_ET_UB: k = {1, 0, 1, +1.0}; break;   // flux_VF_in_out: W.grad U< against W>
+    case TG_ET_BU: k = {0, 1, 0, +1.0}; break;   // W.flux_VF_in_out: U.grad W< against U>
+    default: return false;
+  }
+  return c->phys == TG_MHD;
+}
+
+int ensure_et_buffers(tg_ctx* c) {
+  if (c->et_ready) return TG_OK;
+  const Geo& g = c->g;
+  const size_t Sd = sizeof(cx<double>) * (size_t)g.S;
+  const size_t St = c->tsz * (size_t)g.S;
+  const size_t WXb = c->tsz * (size_t)c->N1 * g.nky * g.kzp;
+  const size_t WYb = c->tsz * (size_t)c->N1 * c->N2 * g.kzp;
+  for (int i = 0; i < 3; ++i) {
+    int rc = dalloc_ctx(c, (void**)&c->etG[i], Sd);
+    if (rc) return rc;
+  }
+  for (int i = 0; i < 6; ++i) {
+    if (i < c->nin) {
+      c->etWY[i] = c->WY[i];
+    } else {
+      int rc = dalloc_ctx(c, &c->etWY[i], WYb);
+      if (rc) return rc;
+      c->et_own[c->n_et_own++] = c->etWY[i];
+    }
+  }
+  for (int q = 0; q < 9; ++q) {
+    if (q < c->nprod) {
+      c->etPP[q] = c->PP[q];
+      c->etPY[q] = c->PY[q];
+      c->etPX[q] = c->PX[q];
+    } else {
+      int rc = dalloc_ctx(c, &c->etPP[q], WYb);
+      if (!rc) rc = dalloc_ctx(c, &c->etPY[q], WXb);
+      if (!rc) rc = dalloc_ctx(c, &c->etPX[q], St);
+      if (rc) return rc;
+      c->et_own[c->n_et_own++] = c->etPP[q];
+      c->et_own[c->n_et_own++] = c->etPY[q];
+      c->et_own[c->n_et_own++] = c->etPX[q];
+    }
+  }
+  c->et_ready = true;
+  return TG_OK;
+}
+
+// Sorted distinct radii of the transfer shells (the reference's radii need not be monotonic
+// when R_in <= 16: EnergyTr.cc:118-126 only warns).
+std::vector<double> et_annuli(const tg_ctx* c) {
+  std::vector<double> R = et_radii(c);
+  std::vector<double> rho(R.begin(), R.end());
+  std::sort(rho.begin(), rho.end());
+  rho.erase(std::unique(rho.begin(), rho.end()), rho.end());
+  if (rho.empty() || rho[0] != 0.0) rho.insert(rho.begin(), 0.0);
+  return rho;
+}
+
+// T[r][g][a]: giver annulus g = 1..A (field F inside (rho[g-1], rho[g]]), receiver annulus
+// a = 0..A, receivers r of the given (H, F) pair
+int et_tables(tg_ctx* c, int Hg, int Fg, const int* Rg, int nrec, const std::vector<double>& rho,
+              std::vector<double>& T) {
+  const int A = (int)rho.size() - 1;
+  if (A < 1 || A > kMaxShells) return set_err(c, TG_ERR_ARG, "energy transfer needs 6 <= n_shells <= 63");
+  int rc = ensure_et_buffers(c);
+  if (rc) return rc;
+  const Geo& g = c->g;
+  Radii rad{};
+  rad.S = A;
+  for (int i = 0; i <= A; ++i) rad.r[i] = rho[i];
+  const int nb = A + 1;
+  const size_t need = (size_t)nrec * (A + 1) * nb;
+  if (c->diag_cap < need) {
+    if (c->diag) cudaFree(c->diag);
+    c->diag = nullptr;
+    c->diag_cap = 0;
+    rc = dalloc_ctx(c, (void**)&c->diag, sizeof(double) * need);
+    if (rc) return rc;
+    c->diag_cap = need;
+  }
+  cudaError_t e = cudaMemsetAsync(c->diag, 0, sizeof(double) * need, c->st);
+  if (e != cudaSuccess) return cuda_err(c, e, "memset");
+  // helper H: inverse x, y once (into etWY[0..2])
+  const void* H[3] = {c->U0[3 * Hg + 0], c->U0[3 * Hg + 1], c->U0[3 * Hg + 2]};
+  rc = pipe_inverse_xy(c, 3, H, nullptr, nullptr, F64, 3, c->WX, c->etWY);
+  if (rc) return rc;
+  ProdPairs pp{};
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      pp.a[3 * i + j] = (signed char)(3 + i);  // G_i
+      pp.b[3 * i + j] = (signed char)j;        // H_j
+    }
+  const int nblk = (int)std::min<long long>((g.S + TPB - 1) / TPB, 148LL * 8);
+  for (int n = 1; n <= A; ++n) {
+    k_fill_shell<<<(int)((g.S + TPB - 1) / TPB), TPB, 0, c->st>>>(
+        g, c->U0[3 * Fg + 0], c->U0[3 * Fg + 1], c->U0[3 * Fg + 2], c->etG[0], c->etG[1], c->etG[2], rho[n - 1], rho[n]);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_err(c, e, "fill shell");
+    const void* G[3] = {c->etG[0], c->etG[1], c->etG[2]};
+    rc = pipe_inverse_xy(c, 3, G, nullptr, nullptr, F64, 3, c->WX, c->etWY + 3);
+    if (rc) return rc;
+    rc = pipe_products_forward(c, 6, c->etWY, 9, pp, c->etPP, c->etPY, c->etPX);
+    if (rc) return rc;
+    ContractArgs a{};
+    a.g = g;
+    for (int q = 0; q < 9; ++q) a.PX[q] = c->etPX[q];
+    for (int r = 0; r < nrec; ++r)
+      for (int i = 0; i < 3; ++i) a.R[r][i] = c->U0[3 * Rg[r] + i];
+    a.nrec = nrec;
+    a.rad = rad;
+    a.hist = c->diag + (size_t)n * nrec * nb;  // layout [g][r][a]
+    {
+      ProfScope pr(c, "et_contract", 0.0);
+      if (c->tprec == F64) k_et_contract<double><<<nblk, TPB, 0, c->st>>>(a);
+      else k_et_contract<float><<<nblk, TPB, 0, c->st>>>(a);
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_err(c, e, "et contract");
+  }
+  std::vector<double> h(need);
+  e = cudaMemcpyAsync(h.data(), c->diag, sizeof(double) * need, cudaMemcpyDeviceToHost, c->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+  if (e != cudaSuccess) return cuda_err(c, e, "et tables");
+  T.assign((size_t)nrec * (A + 1) * nb, 0.0);
+  for (int n = 1; n <= A; ++n)
+    for (int r = 0; r < nrec; ++r)
+      for (int m = 0; m < nb; ++m) T[((size_t)r * (A + 1) + n) * nb + m] = h[((size_t)n * nrec + r) * nb + m];
+  return TG_OK;
+}
+
+int et_table_kind(tg_ctx* c, int kind, std::vector<double>& T, std::vector<double>& rho, double& sign) {
+  KindSpec k{};
+  if (!kind_spec(c, kind, k)) return set_err(c, TG_ERR_ARG, "energy-transfer kind not available for this physics");
+  sign = k.sign;
+  rho = et_annuli(c);
+  int Rg[1] = {k.R};
+  return et_tables(c, k.H, k.F, Rg, 1, rho, T);
+}
+
+}  // namespace
+
 extern "C" {
 
 int tg_et_radii(tg_ctx* c, double* radii, int n) {
@@ -47,19 +292,62 @@ int tg_et_radii(tg_ctx* c, double* radii, int n) {
 }
 
 int tg_flux(tg_ctx* c, int kind, double* flux, int n) {
-  (void)kind;
-  (void)flux;
-  (void)n;
-  if (!c) return TG_ERR_ARG;
-  return set_err(c, TG_ERR_UNSUPPORTED, "flux not built yet");
+  if (!c || !flux) return TG_ERR_ARG;
+  const int S = c->cfg.n_shells;
+  if (S < 6 || n < S + 1) return TG_ERR_ARG;
+  cudaSetDevice(c->dev);
+  std::vector<double> T, rho;
+  double sign = 1;
+  int rc = et_table_kind(c, kind, T, rho, sign);
+  if (rc) return rc;
+  const std::vector<double> R = et_radii(c);
+  const int A = (int)rho.size() - 1, nb = A + 1;
+  for (int s = 0; s < n; ++s) flux[s] = 0;
+  // flux(s): givers inside 0 < |K| <= R_s, receivers |K| > R_s (Prod_out_sphere_nlinV)
+  for (int s = 1; s <= S; ++s) {
+    double acc = 0;
+    for (int g = 1; g <= A; ++g) {
+      if (rho[g] > R[s]) continue;
+      for (int a = 1; a <= A; ++a)
+        if (rho[a - 1] >= R[s]) acc += T[(size_t)g * nb + a];
+    }
+    flux[s] = sign * acc;
+  }
+  return TG_OK;
 }
 
 int tg_shell_to_shell(tg_ctx* c, int kind, double* tr, int n) {
-  (void)kind;
-  (void)tr;
-  (void)n;
-  if (!c) return TG_ERR_ARG;
-  return set_err(c, TG_ERR_UNSUPPORTED, "shell-to-shell not built yet");
+  if (!c || !tr) return TG_ERR_ARG;
+  const int S = c->cfg.n_shells;
+  if (S < 6 || n < S + 1) return TG_ERR_ARG;
+  cudaSetDevice(c->dev);
+  std::vector<double> T, rho;
+  double sign = 1;
+  int rc = et_table_kind(c, kind, T, rho, sign);
+  if (rc) return rc;
+  const std::vector<double> R = et_radii(c);
+  const int A = (int)rho.size() - 1, nb = A + 1;
+  const double Rin = R[S - 1];
+  // receiver bin of an annulus: Get_shell_index (first i with R[i] >= |K|) is constant on it
+  std::vector<int> bin(nb, S);
+  for (int a = 0; a <= A; ++a) {
+    int i = 0;
+    while (i <= S && !(rho[a] <= R[i])) ++i;
+    bin[a] = i;
+  }
+  for (int i = 0; i < n * n; ++i) tr[i] = 0;
+  // rows n = 1..S-1 (compute_shell_tr.cc: shell_from_index < no_shells), receivers |K| <= R_in
+  for (int sh = 1; sh < S; ++sh) {
+    const double lo = R[sh - 1], hi = R[sh];
+    for (int g = 1; g <= A; ++g) {
+      if (!(rho[g - 1] >= lo && rho[g] <= hi)) continue;
+      for (int a = 0; a <= A; ++a) {
+        if (rho[a] > Rin || bin[a] >= n) continue;
+        tr[(size_t)sh * n + bin[a]] += sign * T[(size_t)g * nb + a];
+      }
+    }
+  }
+  return TG_OK;
 }
 
 }  // extern "C"

@@ -446,4 +446,135 @@ __global__ void __launch_bounds__(256 / ((R1 * R2 >= 128) ? 2 : 1))
   }
 }
 
+// ------------------------------------------------------------------------------------------
+// Warp-per-row fused z-pass for M = N3/2 = 32 E (E in {1, 2, 4, 8}).
+//
+// Lane l holds the entries n = l + 32 j (j < E) of a row.  Inverse length-M DFT:
+//   radix-E DFT over j in registers, twiddle e^{+2 pi i l k1 / M}, then a 32-point DFT across
+//   lanes as five radix-2 decimation-in-frequency shuffle stages -> lane l, register k1 holds
+//   z[k1 + E bitrev5(l)].
+// The products are pointwise, so the permuted order is harmless, and the forward DFT is the
+// exact adjoint network (decimation-in-time stages in reverse order, conjugate twiddles, then
+// the forward radix-E DFT), which takes the permuted order and returns X[l + 32 j] in natural
+// order.  No shared-memory transposes and no block barriers; the real-space values of the NIN
+// inputs are parked in warp-private shared memory, each lane reading back only its own slots.
+// ------------------------------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ cx<R> shfl_xor_c(cx<R> v, int m) {
+  return mkc<R>(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
+}
+template <typename R>
+__device__ __forceinline__ cx<R> shfl_c(cx<R> v, int src) {
+  return mkc<R>(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+
+// inverse 32-point DFT across lanes, DIF; tws[s] = e^{+2 pi i (l mod h) / (2h)}, h = 16 >> s
+template <typename R, int E>
+__device__ __forceinline__ void lane_dif32(cx<R> (&v)[E], const cx<R> (&tws)[5], int lane) {
+#pragma unroll
+  for (int s = 0; s < 5; ++s) {
+    const int h = 16 >> s;
+    const bool upper = (lane & h) != 0;
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+      const cx<R> p = shfl_xor_c(v[k], h);
+      v[k] = upper ? (p - v[k]) * tws[s] : v[k] + p;
+    }
+  }
+}
+
+// forward 32-point DFT across lanes: the adjoint of lane_dif32 (DIT, stages h = 1 .. 16)
+template <typename R, int E>
+__device__ __forceinline__ void lane_dit32_fwd(cx<R> (&v)[E], const cx<R> (&tws)[5], int lane) {
+#pragma unroll
+  for (int s = 4; s >= 0; --s) {
+    const int h = 16 >> s;
+    const bool upper = (lane & h) != 0;
+    const cx<R> wc = conjc(tws[s]);
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+      const cx<R> p = shfl_xor_c(v[k], h);
+      const cx<R> t = wc * (upper ? v[k] : p);
+      v[k] = upper ? p - t : v[k] + t;
+    }
+  }
+}
+
+template <typename Ri, typename Ro, typename Rw, int E, int NIN, int NPROD, int WPB>
+__global__ void __launch_bounds__(32 * WPB) k_z_prod_warp(ZArgs a, PtrSet ps, ProdPairs pp) {
+  constexpr int M = 32 * E;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  cx<Rw>* rs = reinterpret_cast<cx<Rw>*>(smem_raw) + (size_t)wib * NIN * E * 32;
+  // per-lane twiddles from twN[k] = e^{-i pi k / M}, k < 2M
+  cx<Rw> hw[E], tw1[E], tws[5];
+#pragma unroll
+  for (int j = 0; j < E; ++j) hw[j] = cvt<Rw>(a.twN[lane + 32 * j]);
+#pragma unroll
+  for (int k1 = 0; k1 < E; ++k1) tw1[k1] = conjc(cvt<Rw>(a.twN[(2 * lane * k1) % (2 * M)]));
+#pragma unroll
+  for (int s = 0; s < 5; ++s) {
+    const int h = 16 >> s;
+    tws[s] = conjc(cvt<Rw>(a.twN[(lane & (h - 1)) * (M / h)]));
+  }
+  const Rw sc = (Rw)a.scale;
+  const long long nwarps = (long long)gridDim.x * WPB;
+  for (long long row = (long long)blockIdx.x * WPB + wib; row < a.nrows; row += nwarps) {
+    // ---- inverse (c2r) of every input
+#pragma unroll 1
+    for (int c = 0; c < NIN; ++c) {
+      const cx<Ri>* src = reinterpret_cast<const cx<Ri>*>(ps.src[c]) + row * a.ss;
+      cx<Rw> v[E];
+#pragma unroll
+      for (int j = 0; j < E; ++j) {
+        const int k = lane + 32 * j;
+        cx<Rw> xa = (k < a.nin) ? cvt<Rw>(src[k]) : mkc<Rw>(0, 0);
+        const int km = M - k;
+        cx<Rw> xb = (km < a.nin) ? cvt<Rw>(src[km]) : mkc<Rw>(0, 0);
+        if (k == 0) {
+          xa.y = 0;
+          xb.y = 0;
+        }
+        xb.y = -xb.y;
+        v[j] = (xa + xb) + ione(conjc(hw[j]) * (xa - xb));
+      }
+      DFT<E, +1, Rw>::run(v);
+#pragma unroll
+      for (int k1 = 1; k1 < E; ++k1) v[k1] = v[k1] * tw1[k1];
+      lane_dif32<Rw, E>(v, tws, lane);
+#pragma unroll
+      for (int k1 = 0; k1 < E; ++k1) rs[(c * E + k1) * 32 + lane] = v[k1];
+    }
+    // ---- products and forward (r2c)
+#pragma unroll 1
+    for (int q = 0; q < NPROD; ++q) {
+      const int pa = pp.a[q], pb = pp.b[q];
+      cx<Rw> v[E];
+#pragma unroll
+      for (int k1 = 0; k1 < E; ++k1) v[k1] = rmul(rs[(pa * E + k1) * 32 + lane], rs[(pb * E + k1) * 32 + lane]);
+      lane_dit32_fwd<Rw, E>(v, tws, lane);
+#pragma unroll
+      for (int k1 = 1; k1 < E; ++k1) v[k1] = v[k1] * conjc(tw1[k1]);
+      DFT<E, -1, Rw>::run(v);
+      cx<Ro>* dst = reinterpret_cast<cx<Ro>*>(ps.dst[q]) + row * a.ds;
+      const int pl = (32 - lane) & 31;
+#pragma unroll
+      for (int j = 0; j < E; ++j) {
+        // Z[M - k] for k = lane + 32 j: lane (32 - l) & 31, register E-1-j (own register
+        // (E - j) mod E on lane 0)
+        cx<Rw> zm = shfl_c(v[E - 1 - j], pl);
+        if (lane == 0) zm = v[(E - j) % E];
+        zm.y = -zm.y;
+        const cx<Rw> s = v[j] + zm;
+        const cx<Rw> d = hw[j] * (v[j] - zm);
+        const int k = lane + 32 * j;
+        if (k < a.nout) dst[k] = cvt<Ro>(mkc<Rw>(sc * (Rw)0.5 * (s.x + d.y), sc * (Rw)0.5 * (s.y - d.x)));
+      }
+      if (lane == 0 && a.nout > M) dst[M] = cvt<Ro>(mkc<Rw>(sc * (v[0].x - v[0].y), (Rw)0));
+      for (int k = a.nout + lane; k < a.nfill; k += 32) dst[k] = mkc<Ro>(0, 0);
+    }
+  }
+}
+
 }  // namespace tg

@@ -94,16 +94,33 @@ cudaError_t run_zprod_fast(const ZProdLaunch& l, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+template <typename Ri, typename Ro, typename Rw, int E, int NIN, int NPROD>
+cudaError_t run_zprod_warp(const ZProdLaunch& l, cudaStream_t s) {
+  constexpr int WPB = 4;
+  const size_t smem = (size_t)WPB * NIN * E * 32 * sizeof(cx<Rw>);
+  auto kern = k_z_prod_warp<Ri, Ro, Rw, E, NIN, NPROD, WPB>;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  long long blocks = (l.a.nrows + WPB - 1) / WPB;
+  if (blocks > 148LL * 32) blocks = 148LL * 32;
+  kern<<<(unsigned)blocks, 32 * WPB, smem, s>>>(l.a, l.ps, l.pp);
+  return cudaGetLastError();
+}
+
 template <typename Ri, typename Ro, typename Rw, int NIN, int NPROD>
 cudaError_t run_zprod_m(const ZProdLaunch& l, cudaStream_t s) {
   switch (l.M) {
     case 4: return run_zprod_fast<Ri, Ro, Rw, 2, 2, NIN, NPROD>(l, s);
     case 8: return run_zprod_fast<Ri, Ro, Rw, 4, 2, NIN, NPROD>(l, s);
     case 16: return run_zprod_fast<Ri, Ro, Rw, 4, 4, NIN, NPROD>(l, s);
-    case 32: return run_zprod_fast<Ri, Ro, Rw, 8, 4, NIN, NPROD>(l, s);
-    case 64: return run_zprod_fast<Ri, Ro, Rw, 8, 8, NIN, NPROD>(l, s);
-    case 128: return run_zprod_fast<Ri, Ro, Rw, 16, 8, NIN, NPROD>(l, s);
-    case 256: return run_zprod_fast<Ri, Ro, Rw, 16, 16, NIN, NPROD>(l, s);
+    case 32: return run_zprod_warp<Ri, Ro, Rw, 1, NIN, NPROD>(l, s);
+    case 64: return run_zprod_warp<Ri, Ro, Rw, 2, NIN, NPROD>(l, s);
+    case 128: return run_zprod_warp<Ri, Ro, Rw, 4, NIN, NPROD>(l, s);
+    case 256: return run_zprod_warp<Ri, Ro, Rw, 8, NIN, NPROD>(l, s);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -152,9 +152,9 @@ template <typename Rp, typename Rs, int PHYS, int SRC>
 __global__ void __launch_bounds__(TPB) k_rk(RKArgs a) {
   constexpr int NS = NState<PHYS>::v;
   const Geo& g = a.g;
-  const long long idx = (long long)blockIdx.x * TPB + threadIdx.x;
   double acc[6] = {0, 0, 0, 0, 0, 0};
-  if (idx < g.S) {
+  const long long stride = (long long)gridDim.x * TPB;
+  for (long long idx = (long long)blockIdx.x * TPB + threadIdx.x; idx < g.S; idx += stride) {
     int r1, r2, l3;
     compact_mode(g, idx, r1, r2, l3);
     if (l3 < g.nkz) {
@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(TPB) k_rk(RKArgs a) {
           const int box = (2 * a.fx + 1) * (2 * a.fy + 1) * (a.fz + 1);
           const int p = ((kxi + a.fx) * (2 * a.fy + 1) + (kyi + a.fy)) * (a.fz + 1) + l3;
 #pragma unroll
-          for (int c = 0; c < NS; ++c) r[c] = r[c] - a.FB[(long long)c * box + p];
+          for (int c = 0; c < 3; ++c) r[c] = r[c] - a.FB[(long long)c * box + p];
         }
         project_rhs(r, NS, kx, ky, kz, K2);
       } else {
@@ -399,9 +399,9 @@ __global__ void k_rhs_from_nlin(Geo g, int ns, PtrArr6 pa, const cx<double>* PR)
 
 // ------------------------------------------------------------------ reductions
 __global__ void __launch_bounds__(TPB) k_energy_partials(Geo g, PtrArr6 pa, int nf, double* part, int slot, int nslots) {
-  const long long idx = (long long)blockIdx.x * TPB + threadIdx.x;
   double acc[2] = {0, 0};
-  if (idx < g.S) {
+  const long long stride = (long long)gridDim.x * TPB;
+  for (long long idx = (long long)blockIdx.x * TPB + threadIdx.x; idx < g.S; idx += stride) {
     int r1, r2, l3;
     compact_mode(g, idx, r1, r2, l3);
     if (l3 < g.nkz) {
@@ -506,8 +506,11 @@ __global__ void __launch_bounds__(TPB) k_shell_spectrum(Geo g, PtrArr6 pa, int n
 }
 
 inline int nblk(long long n) { return (int)((n + TPB - 1) / TPB); }
+inline int nred(long long n) { return nblk(n) < 148 * 8 ? nblk(n) : 148 * 8; }
 
 }  // namespace
+
+int reduction_blocks(long long S) { return nred(S); }
 
 cudaError_t launch_dense_to_compact(const Geo& g, const cx<double>* dense, void* compact, int cprec, cudaStream_t s) {
   if (cprec == 0) k_dense_to_compact<double><<<nblk(g.S), TPB, 0, s>>>(g, dense, (cx<double>*)compact);
@@ -523,7 +526,7 @@ cudaError_t launch_compact_to_dense(const Geo& g, const void* compact, int cprec
 }
 
 cudaError_t launch_rk(const RKArgs& a, int phys, int pprec, int sprec, int src, cudaStream_t s, int* nblocks) {
-  const int nb = nblk(a.g.S);
+  const int nb = nred(a.g.S);
   if (nblocks) *nblocks = nb;
   if (pprec == 0 && sprec == 0) return run_rk_phys<double, double>(a, phys, src, s, nb);
   if (pprec == 1 && sprec == 1) return run_rk_phys<float, float>(a, phys, src, s, nb);
@@ -584,7 +587,7 @@ cudaError_t launch_rhs_from_nlin(const Geo& g, int phys, cx<double>* const* NL, 
 cudaError_t launch_energy_partials(const Geo& g, const cx<double>* const* F, int nf, double* part, int slot, int nslots, cudaStream_t s, int* nblocks) {
   PtrArr6 pa{};
   for (int c = 0; c < nf; ++c) pa.p[c] = const_cast<cx<double>*>(F[c]);
-  const int nb = nblk(g.S);
+  const int nb = nred(g.S);
   if (nblocks) *nblocks = nb;
   k_energy_partials<<<nb, TPB, 0, s>>>(g, pa, nf, part, slot, nslots);
   return cudaGetLastError();

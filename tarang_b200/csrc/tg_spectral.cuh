@@ -85,6 +85,7 @@ struct ForceArgs {
 };
 
 // launchers (tg_spectral.cu)
+int reduction_blocks(long long S);  // grid of the reducing kernels (RK stage 4, energy partials)
 cudaError_t launch_dense_to_compact(const Geo& g, const cx<double>* dense, void* compact, int cprec, cudaStream_t s);
 cudaError_t launch_compact_to_dense(const Geo& g, const void* compact, int cprec, cx<double>* dense, cudaStream_t s);
 cudaError_t launch_rk(const RKArgs& a, int phys, int pprec, int sprec, int src, cudaStream_t s, int* nblocks);
