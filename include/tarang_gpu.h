@@ -171,6 +171,34 @@ int tg_shell_to_shell(tg_ctx* ctx, int kind, double* tr, int n);
 int tg_nusselt(tg_ctx* ctx, double* nusselt);
 
 /* ------------------------------------------------------------------------------------------
+ * Allocation-free energy reduction.  No counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory: an in-situ diagnostic called from inside
+ * another code's time loop, where the host application owns all device memory through its own
+ * pool and does not allow cudaMalloc (it synchronises the device and can fail part-way through
+ * a long run).  Such a caller holds its spectral fields in its own device buffers and needs
+ * the energy and dissipation of those fields without a tg_ctx.
+ *
+ * Computes, for each of n_fields consecutive fields at d_fields (device memory, reference
+ * layout, 2*N1*N2*(N3/2+1) doubles each), the FOUR total energy (Get_total_energy_FOUR) and
+ * dissipation 2*sum mult K^2 |A|^2 (Get_total_Sn_FOUR with n = 2, Cvf.cc:385-397), and writes
+ * d_out[2f] = energy of field f, d_out[2f+1] = dissipation of field f (device memory,
+ * 2*n_fields doubles).  The same numbers tg_energy returns for a context's fields.
+ *
+ * No cudaMalloc/cudaFree or allocating library call: the per-block partial sums live in a
+ * fixed device array of 8 x 1184 x 2 doubles (151,552 bytes) that every GPU loading this library
+ * holds until exit.  Limit: 1 <= n_fields <= TG_NOALLOC_MAX_FIELDS; anything beyond returns
+ * TG_ERR_ARG.  The first call on a device looks up that array's device address (with the
+ * caller's current device) and caches it: make that first call before any stream capture.
+ * Work is queued on `stream` (cudaStream_t; NULL = default stream) and the call returns
+ * without waiting.  Every call shares the array and it keeps the last call's partials; calls
+ * that overlap on the GPU (different streams, or concurrent host threads) race on it.
+ * ---------------------------------------------------------------------------------------- */
+#define TG_NOALLOC_MAX_FIELDS 8
+int tg_energy_noalloc(const double* d_fields, int n_fields, const int N[3], const double kfactor[3],
+                      int dealias, double* d_out, void* stream);
+
+/* ------------------------------------------------------------------------------------------
  * Profiling (no counterpart in the reference, whose only timing is time(0) around main,
  * src/main.cc:95-151): per-launch CUDA events on the context's stream.  While enabled, steps
  * run eagerly (no graph replay).  Stats aggregate by kernel name; algorithmic bytes are the

@@ -140,6 +140,7 @@ SIGNATURES = {
     "tg_flux": (C.c_int, [_VP, C.c_int, _DP, C.c_int]),
     "tg_shell_to_shell": (C.c_int, [_VP, C.c_int, _DP, C.c_int]),
     "tg_nusselt": (C.c_int, [_VP, _DP]),
+    "tg_energy_noalloc": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_int, _VP, _VP]),
     "tg_profile_enable": (C.c_int, [_VP, C.c_int]),
     "tg_profile_read": (C.c_int, [_VP, C.POINTER(tg_kernel_stat), C.c_int, C.POINTER(C.c_int)]),
     "tg_server_create": (C.c_int, [C.POINTER(tg_server_config), C.POINTER(_VP)]),
