@@ -125,9 +125,11 @@ def min_radius_outside(N, kfactor, alias="DEALIAS", basis="FOUR"):
 
 
 def approx_number_modes_in_shell(N, radius, kfactor, basis="FOUR"):
-    """Approx_number_modes_in_shell_FOUR  lib/four/four_inline.h:276-306 (3-D branch).
-    SCFT (scft_inline.h:242) uses the same hemisphere area for the 3-D case."""
-    return (2 * math.pi * radius * radius) / (kfactor[0] * kfactor[1] * kfactor[2])
+    """Approx_number_modes_in_shell_FOUR  four_inline.h:276-306 (3-D: hemisphere, 2 pi r^2);
+    Approx_number_modes_in_shell_SCFT  scft_inline.h:242-260 (3-D: quarter sphere, pi r^2)."""
+    if basis == "FOUR":
+        return (2 * math.pi * radius * radius) / (kfactor[0] * kfactor[1] * kfactor[2])
+    return (math.pi * radius * radius) / (kfactor[0] * kfactor[1] * kfactor[2])
 
 
 def multiplicity_four(N):
@@ -361,7 +363,10 @@ def total_Sn(A, n, kfactor, alias="DEALIAS", basis="FOUR"):
     K = kmag(N, kfactor, basis)
     kkmax = min_radius_outside(N, kfactor, alias, basis)
     mult = multiplicity(N, basis)
-    w = np.where(K <= kkmax, mult * (K ** n if n != 0 else 1.0), 0.0)
+    # Get_local_Sn_SCFT (scft_energy.cc:187) has `if (kkmag <= kkmax);` -- the empty statement
+    # makes the sum run over every mode
+    inside = (K <= kkmax) if basis == "FOUR" else np.ones_like(K, dtype=bool)
+    w = np.where(inside, mult * (K ** n if n != 0 else 1.0), 0.0)
     s = float((w * np.abs(A) ** 2).sum())
     if n == 0:
         s -= mult[0, 0, 0] * abs(A[0, 0, 0]) ** 2
@@ -383,7 +388,9 @@ def shell_spectrum(A, n, kfactor, alias="DEALIAS", basis="FOUR", B=None):
     sel = idx <= kkmax
     val = mult * (K ** n if n != 0 else 1.0) * np.real(A * np.conj(B))
     Sk = np.bincount(idx[sel], weights=val[sel], minlength=kkmax + 1)[: kkmax + 1]
-    cnt = np.bincount(idx[sel], weights=np.broadcast_to(mult, K.shape)[sel], minlength=kkmax + 1)[: kkmax + 1]
+    # SCFT counts factor/2 (Compute_local_shell_spectrum_SCFT scft_energy.cc:279)
+    cmult = mult if basis == "FOUR" else mult / 2
+    cnt = np.bincount(idx[sel], weights=np.broadcast_to(cmult, K.shape)[sel], minlength=kkmax + 1)[: kkmax + 1]
     for i in range(kin + 1, kkmax + 1):
         if cnt[i] >= 1:
             Sk[i] = Sk[i] * approx_number_modes_in_shell(N, i, kfactor, basis) / cnt[i]
@@ -712,6 +719,77 @@ class MHDSolver(FluidSolver):
             u = [dealias(a, self.basis) for a in u]
             b = [dealias(a, self.basis) for a in b]
         return u, b, dt
+
+
+class RBSolver:
+    """Rayleigh-Benard convection (RB_SLIP, Pr_switch PRLARGE, RB_Uscaling ULARGE):
+    src/RBslip/RB_slip_main.cc:236-240 (nu = sqrt(Pr/Ra), kappa = 1/sqrt(Pr Ra)) and the loop
+    :365-400; Compute_force_RB compute_force_RB.cc:51-105 (Force1 = theta, T.Force =
+    temperature_grad * u1); Compute_nlin(T) -> Compute_nlin_scalar compute_nlin_SF.cc:80-177 with
+    Dealias_nlin(T); IF-RK4 of time_advance_SF.cc for u (nu) and theta (kappa); Get_dt(T) = Get_dt().
+    Fields: V = [u1 (sin), u2 (cos), u3 (cos)], T = theta (sin) in the SCFT basis."""
+
+    def __init__(self, N, kfactor, Ra, Pr, Tdt, basis="SCFT", alias="DEALIAS", temperature_grad=1.0):
+        self.N = tuple(N)
+        self.kfactor = tuple(kfactor)
+        self.nu = math.sqrt(Pr / Ra)
+        self.kappa = 1.0 / math.sqrt(Pr * Ra)
+        self.Ra, self.Pr = Ra, Pr
+        self.Tdt = Tdt
+        self.basis = basis
+        self.alias = alias
+        self.tg = temperature_grad
+
+    def rhs(self, V, T):
+        nl = nlin_fluid(V, self.kfactor, self.basis, self.alias)
+        tn = nlin_scalar(V, T, self.kfactor, self.basis, self.alias, dealias_T=True)
+        F1 = T
+        TF = self.tg * V[0]
+        if self.alias == "DEALIAS":     # Dealias_force(T)
+            F1 = dealias(F1, self.basis)
+            TF = dealias(TF, self.basis)
+        nl = [nl[0] - F1, nl[1], nl[2]]
+        tn = tn - TF
+        p = pressure(nl, self.kfactor, self.basis, self.alias)
+        return rhs_from_nlin(nl, p, self.kfactor, self.basis), -tn
+
+    def E(self, V, coef, a, dt):
+        return [exp_ksqr(v, -coef * a * dt, self.kfactor, self.basis) for v in V]
+
+    def step(self, V, T):
+        E0 = sum(total_energy(v, self.basis) for v in V)
+        dt = get_dt(E0, self.N, self.kfactor, self.Tdt, self.alias, self.basis)
+        u0 = [v.copy() for v in V]
+        t0 = T.copy()
+        nu, ka = self.nu, self.kappa
+        ru, rt = self.rhs(u0, t0)
+        u = self.E([u0[i] + (dt / 2) * ru[i] for i in range(3)], nu, 0.5, dt)
+        t = self.E([t0 + (dt / 2) * rt], ka, 0.5, dt)[0]
+        totu = [(dt / 6) * x for x in self.E(ru, nu, 1.0, dt)]
+        tott = (dt / 6) * self.E([rt], ka, 1.0, dt)[0]
+        ru, rt = self.rhs(u, t)
+        u = [x + (dt / 2) * y for x, y in zip(self.E(u0, nu, 0.5, dt), ru)]
+        t = self.E([t0], ka, 0.5, dt)[0] + (dt / 2) * rt
+        totu = [a + (dt / 3) * x for a, x in zip(totu, self.E(ru, nu, 0.5, dt))]
+        tott = tott + (dt / 3) * self.E([rt], ka, 0.5, dt)[0]
+        ru, rt = self.rhs(u, t)
+        u = self.E([x + dt * y for x, y in zip(self.E(u0, nu, 0.5, dt), ru)], nu, 0.5, dt)
+        t = self.E([self.E([t0], ka, 0.5, dt)[0] + dt * rt], ka, 0.5, dt)[0]
+        totu = [a + (dt / 3) * x for a, x in zip(totu, self.E(ru, nu, 0.5, dt))]
+        tott = tott + (dt / 3) * self.E([rt], ka, 0.5, dt)[0]
+        ru, rt = self.rhs(u, t)
+        totu = [a + (dt / 6) * x for a, x in zip(totu, ru)]
+        tott = tott + (dt / 6) * rt
+        u = [x + a for x, a in zip(self.E(u0, nu, 1.0, dt), totu)]
+        t = self.E([t0], ka, 1.0, dt)[0] + tott
+        if self.alias == "DEALIAS":
+            u = [dealias(a, self.basis) for a in u]
+            t = dealias(t, self.basis)
+        return u, t, dt
+
+    def nusselt(self, V, T):
+        """Get_Nusselt_no  nusselt.cc:53-89, PRLARGE + ULARGE: 1 + 2 sqrt(Ra Pr) <u1, theta>."""
+        return 1 + 2 * math.sqrt(self.Ra * self.Pr) * total_energy(V[0], self.basis, T)
 
 
 # --------------------------------------------------------------------------------------

@@ -176,6 +176,8 @@ RKArgs rk_args(tg_ctx* c, int stage) {
   a.fy = c->fy;
   a.fz = c->fz;
   a.part = (stage == 4) ? c->part : nullptr;
+  a.rb_buoy_u = c->rb_fu;
+  a.rb_buoy_t = c->rb_ft;
   return a;
 }
 
@@ -242,6 +244,8 @@ int run_stages(tg_ctx* c, int first_stage, bool ring) {
     rc = run_pipeline(c, in, inprec);
     if (rc) return rc;
     RKArgs a = rk_args(c, stage);
+    for (int i = 0; i < c->nstate; ++i) a.IN[i] = in[i];
+    a.inprec = (inprec == F64) ? 0 : 1;
     {
       const double ns = c->nstate, e = el_compact(c);
       const double rd = c->nprod * e * c->tsz + ns * e * 16 + (stage > 1 ? ns * e * 16 : 0);
@@ -285,8 +289,9 @@ int ensure_staging(tg_ctx* c) {
   return TG_OK;
 }
 
-// dense FOUR transforms of a work field, in place (ArrayFFT_FOUR / ArrayIFFT_FOUR)
-int dense_transform(tg_ctx* c, cx<double>* f, int forward) {
+// dense transforms of a work field, in place: FOUR (ArrayFFT_FOUR / ArrayIFFT_FOUR) or SCFT with
+// parity 0 cos / 1 sin along x (ArrayCFT/SFT_SCFT, ArrayICFT/ISFT_SCFT)
+int dense_transform(tg_ctx* c, cx<double>* f, int forward, int parity) {
   const int wp = (c->prec == TG_FP64) ? F64 : F32;
   const long long M3 = c->M3;
   if (forward) {
@@ -337,7 +342,15 @@ int dense_transform(tg_ctx* c, cx<double>* f, int forward) {
       l.a.in = l.a.out = full_map(c->N2);
       l.a.tw = c->tw[c->N2];
     }
-    TG_CK(launch_axis(l, c->st));
+    if (xpass && c->basis == TG_SCFT) {
+      R2RArgs r{};
+      r.kind[0] = forward ? (parity ? 1 : 0) : (parity ? 3 : 2);
+      r.trig = c->trigx;
+      if (forward) l.a.scale = 0.5;  // Norm_SCFT 1/(2 N1 N2 N3)
+      TG_CK(launch_r2r(l, r, c->st));
+    } else {
+      TG_CK(launch_axis(l, c->st));
+    }
   }
   if (!forward) {
     ZLaunch z;
@@ -383,6 +396,7 @@ void free_ctx(tg_ctx* c) {
   }
   fr(c->PR);
   fr(c->FB);
+  fr(c->trigx);
   fr(c->scal);
   fr(c->red_out);
   fr(c->part);
@@ -455,11 +469,16 @@ int tg_ctx_create(const tg_config* cfg, tg_ctx** out) {
   *out = nullptr;
   const int N1 = cfg->N[0], N2 = cfg->N[1], N3 = cfg->N[2];
   if (N1 < 2 || N2 < 2 || N3 < 4 || (N3 & 1)) return TG_ERR_ARG;
-  if (cfg->basis != TG_FOUR) return TG_ERR_UNSUPPORTED;
-  if (cfg->physics != TG_FLUID && cfg->physics != TG_MHD && cfg->physics != TG_SCALAR) return TG_ERR_UNSUPPORTED;
+  if (cfg->basis != TG_FOUR && cfg->basis != TG_SCFT) return TG_ERR_ARG;
+  if (cfg->physics < TG_FLUID || cfg->physics > TG_RB) return TG_ERR_ARG;
+  if (cfg->basis == TG_SCFT && cfg->physics == TG_MHD) return TG_ERR_UNSUPPORTED;
+  if (cfg->physics == TG_RB && !(cfg->rb_ra > 0 && cfg->rb_pr > 0)) return TG_ERR_ARG;
   if (cfg->precision != TG_FP64 && cfg->precision != TG_FP32_MIXED) return TG_ERR_ARG;
   if (cfg->scheme != TG_RK4) return TG_ERR_UNSUPPORTED;
-  if (cfg->force_kind != TG_FORCE_DECAY && cfg->force_kind != TG_FORCE_ENERGY_SUPPLY) return TG_ERR_UNSUPPORTED;
+  if (cfg->force_kind != TG_FORCE_DECAY && cfg->force_kind != TG_FORCE_ENERGY_SUPPLY && cfg->force_kind != TG_FORCE_RB)
+    return TG_ERR_UNSUPPORTED;
+  if (cfg->force_kind == TG_FORCE_RB && cfg->physics != TG_RB) return TG_ERR_ARG;
+  if (cfg->force_kind == TG_FORCE_ENERGY_SUPPLY && cfg->basis != TG_FOUR) return TG_ERR_UNSUPPORTED;
   if (cfg->force_kind == TG_FORCE_ENERGY_SUPPLY && cfg->physics != TG_FLUID) return TG_ERR_UNSUPPORTED;
   for (int i = 0; i < 3; ++i)
     if (!(cfg->kfactor[i] > 0)) return TG_ERR_ARG;
@@ -555,6 +574,16 @@ int tg_ctx_create(const tg_config* cfg, tg_ctx** out) {
     }
     for (int i = 0; i < 3; ++i) c->nu_of[i] = cfg->nu;
     c->nu_of[3] = cfg->kappa;
+    if (c->phys == TG_RB) {
+      // PRLARGE + ULARGE (RB_slip_main.cc:236-240): nu = sqrt(Pr/Ra), kappa = 1/sqrt(Pr Ra);
+      // Compute_force_RB: Force1 = theta, T.Force = temperature_grad (+1) u1
+      const double nu = std::sqrt(cfg->rb_pr / cfg->rb_ra), ka = 1.0 / std::sqrt(cfg->rb_pr * cfg->rb_ra);
+      for (int i = 0; i < 3; ++i) c->nu_of[i] = nu;
+      c->nu_of[3] = ka;
+      const double on = (cfg->force_kind == TG_FORCE_RB) ? 1.0 : 0.0;
+      c->rb_fu = on;
+      c->rb_ft = on;
+    }
   }
 
   int rc = TG_OK;
@@ -563,6 +592,27 @@ int tg_ctx_create(const tg_config* cfg, tg_ctx** out) {
     free_ctx(c);
     return code;
   };
+  // SCFT x-pass kinds by field parity: u1, theta sine; u2, u3 cosine (Rvf.cc:135-186,
+  // compute_nlin_SF.cc:80-115); products u1u1, u2u2, u3u3, u2u3, u1 theta cos; u1u2, u3u1,
+  // u2 theta, u3 theta sin
+  {
+    const int inv[6] = {3, 2, 2, 3, 0, 0};
+    const int fwd[9] = {0, 0, 0, 1, 0, 1, 0, 1, 1};
+    for (int i = 0; i < 6; ++i) c->xinv_kind[i] = inv[i];
+    for (int q = 0; q < 9; ++q) c->xfwd_kind[q] = fwd[q];
+  }
+  if (c->basis == TG_SCFT) {
+    std::vector<cx<double>> h(4 * (size_t)N1);
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int j = 0; j < 4 * N1; ++j) {
+      const long double ang = pi * (long double)j / (2.0L * N1);
+      h[j].x = (double)cosl(ang);
+      h[j].y = (double)sinl(ang);
+    }
+    if ((rc = dalloc(c, (void**)&c->trigx, sizeof(cx<double>) * h.size()))) return fail(rc);
+    e = cudaMemcpy(c->trigx, h.data(), sizeof(cx<double>) * h.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail(cuda_err(c, e, "trig table"));
+  }
   for (int L : {N1, N2, Mz, N3}) {
     rc = make_twiddles(c, L);
     if (rc) return fail(rc);
@@ -756,19 +806,19 @@ int tg_field_copy(tg_ctx* c, int dst, int src) {
 }
 
 int tg_forward_transform(tg_ctx* c, int field, int parity) {
-  (void)parity;
   if (!c || field < TG_WORK0 || field >= TG_WORK0 + TG_NWORK) return TG_ERR_ARG;
   cudaSetDevice(c->dev);
   if (!c->dense[field]) return set_err(c, TG_ERR_STATE, "transform: work field never written");
-  return dense_transform(c, c->dense[field], 1);
+  if (c->basis == TG_SCFT && parity != 0 && parity != 1) return TG_ERR_ARG;
+  return dense_transform(c, c->dense[field], 1, parity);
 }
 
 int tg_inverse_transform(tg_ctx* c, int field, int parity) {
-  (void)parity;
   if (!c || field < TG_WORK0 || field >= TG_WORK0 + TG_NWORK) return TG_ERR_ARG;
   cudaSetDevice(c->dev);
   if (!c->dense[field]) return set_err(c, TG_ERR_STATE, "transform: work field never written");
-  return dense_transform(c, c->dense[field], 0);
+  if (c->basis == TG_SCFT && parity != 0 && parity != 1) return TG_ERR_ARG;
+  return dense_transform(c, c->dense[field], 0, parity);
 }
 
 int tg_compute_force(tg_ctx* c) {
@@ -803,6 +853,9 @@ int tg_add_force(tg_ctx* c) {
   if (c->force_on) {
     if (!c->have_force) return set_err(c, TG_ERR_STATE, "Add_force before Compute_force");
     TG_CK(launch_sub_force_box(c->g, 3, c->FB, c->fx, c->fy, c->fz, c->NL, c->st));
+  }
+  if (c->phys == TG_RB) {
+    TG_CK(launch_rb_sub_force(c->g, c->NL, c->U0[0], c->U0[3], c->rb_fu, c->rb_ft, c->st));
   }
   return TG_OK;
 }
@@ -938,7 +991,9 @@ int tg_shell_spectrum(tg_ctx* c, int group, double* ek, double* dissk, int n) {
   // Min_radius_outside / Max_radius_inside (four_inline.h:172-257)
   const int d = c->cfg.dealias ? 3 : 2;
   const double* kf = c->cfg.kfactor;
-  const double a0 = (c->N1 / d) * kf[0], a1 = (c->N2 / d) * kf[1], a2 = (c->N3 / d) * kf[2];
+  // SCFT: kx extent 2 N1/3 dealiased, N1 aliased (scft_inline.h:180-200)
+  const int nx = (c->basis == TG_FOUR) ? c->N1 / d : (c->cfg.dealias ? 2 * c->N1 / 3 : c->N1);
+  const double a0 = nx * kf[0], a1 = (c->N2 / d) * kf[1], a2 = (c->N3 / d) * kf[2];
   const int kkmax = (int)std::ceil(std::sqrt(a0 * a0 + a1 * a1 + a2 * a2));
   const int kin = max_radius_inside(c);
   const int nbins = kkmax + 1;
@@ -972,8 +1027,27 @@ int tg_shell_spectrum(tg_ctx* c, int group, double* ek, double* dissk, int n) {
   std::vector<double> h(need);
   TG_CK(cudaMemcpyAsync(h.data(), dbuf, sizeof(double) * need, cudaMemcpyDeviceToHost, c->st));
   TG_CK(cudaStreamSynchronize(c->st));
-  const double* cnt = h.data() + (size_t)nf * nbins;
-  const double approx_fac = 2 * M_PI / (kf[0] * kf[1] * kf[2]);
+  // Sk_count of the reference runs over every mode of its dense array, the dealiased zeros
+  // included (four_energy.cc:271-286, scft_energy.cc:266-281): geometry only, computed once
+  if ((int)c->shell_count.size() != nbins) {
+    c->shell_count.assign(nbins, 0.0);
+    for (int l1 = 0; l1 < c->N1; ++l1) {
+      const int kxi = (c->basis == TG_FOUR && l1 > c->N1 / 2) ? l1 - c->N1 : l1;
+      for (int l2 = 0; l2 < c->N2; ++l2) {
+        const int kyi = l2 <= c->N2 / 2 ? l2 : l2 - c->N2;
+        for (int l3 = 0; l3 < c->M3; ++l3) {
+          const double kx = kxi * kf[0], ky = kyi * kf[1], kz = l3 * kf[2];
+          const int b = (int)std::ceil(std::sqrt(kx * kx + ky * ky + kz * kz));
+          if (b >= nbins) continue;
+          c->shell_count[b] += (c->basis == TG_FOUR) ? mult_four(l1, l2, l3, c->N1, c->N2)
+                                                     : 0.5 * mult_scft(l1, l2, l3, c->N2);
+        }
+      }
+    }
+  }
+  const double* cnt = c->shell_count.data();
+  // Approx_number_modes_in_shell: FOUR hemisphere 2 pi r^2, SCFT quarter sphere pi r^2
+  const double approx_fac = (c->basis == TG_FOUR ? 2 * M_PI : M_PI) / (kf[0] * kf[1] * kf[2]);
   for (int i = 0; i < nf; ++i)
     for (int b = 0; b < n; ++b) ek[(size_t)i * n + b] = 0.0;
   if (dissk)
@@ -1026,9 +1100,19 @@ int tg_profile_read(tg_ctx* c, tg_kernel_stat* out, int max, int* n) {
 }
 
 int tg_nusselt(tg_ctx* c, double* nu) {
-  (void)nu;
-  if (!c) return TG_ERR_ARG;
-  return set_err(c, TG_ERR_UNSUPPORTED, "Nusselt number needs the RB (SCFT) physics");
+  if (!c || !nu) return TG_ERR_ARG;
+  if (c->phys != TG_RB) return set_err(c, TG_ERR_ARG, "Nusselt number needs the RB physics");
+  cudaSetDevice(c->dev);
+  // Get_Nusselt_no (nusselt.cc:53-89), PRLARGE + ULARGE: 1 + 2 sqrt(Ra Pr) <u1, theta>
+  int nb = 0;
+  TG_CK(launch_cross_partials(c->g, c->U0[0], c->U0[3], c->part, 0, 8, c->st, &nb));
+  std::vector<double> h((size_t)nb * 8);
+  TG_CK(cudaMemcpyAsync(h.data(), c->part, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->st));
+  TG_CK(cudaStreamSynchronize(c->st));
+  double cross = 0;
+  for (int b = 0; b < nb; ++b) cross += h[(size_t)b * 8];
+  *nu = 1.0 + 2.0 * std::sqrt(c->cfg.rb_ra * c->cfg.rb_pr) * cross;
+  return TG_OK;
 }
 
 }  // extern "C"

@@ -31,6 +31,12 @@ struct tg_ctx {
 
   // twiddle tables: length -> exp(-2 pi i m / L)
   std::map<int, tg::cx<double>*> tw;
+  // SCFT: (cos, sin)(pi j / 2 N1), j < 4 N1, and the x-pass kind of every pipeline field
+  // (0 CFT, 1 SFT forward; 2 ICFT, 3 ISFT inverse)
+  tg::cx<double>* trigx = nullptr;
+  int xinv_kind[6] = {};
+  int xfwd_kind[9] = {};
+  double rb_fu = 0, rb_ft = 0;  // RB: Force1 = rb_fu theta, T.Force = rb_ft u1
 
   // compact solver state
   tg::cx<double>* U0[6] = {};
@@ -62,6 +68,7 @@ struct tg_ctx {
   double* h_pinned = nullptr;  // small pinned host buffer
   double* diag = nullptr;      // diagnostics scratch (spectra, transfer tables)
   size_t diag_cap = 0;
+  std::vector<double> shell_count;  // Sk_count over the dense grid (geometry only)
 
   // energy-transfer buffers (pipeline buffers reused where the physics already has them)
   bool et_ready = false;

@@ -269,6 +269,7 @@ int et_tables(tg_ctx* c, int Hg, int Fg, const int* Rg, int nrec, const std::vec
 }
 
 int et_table_kind(tg_ctx* c, int kind, std::vector<double>& T, std::vector<double>& rho, double& sign) {
+  if (c->basis != TG_FOUR) return set_err(c, TG_ERR_UNSUPPORTED, "energy transfer is built for the FOUR basis");
   KindSpec k{};
   if (!kind_spec(c, kind, k)) return set_err(c, TG_ERR_ARG, "energy-transfer kind not available for this physics");
   sign = k.sign;

@@ -151,6 +151,88 @@ __global__ void __launch_bounds__(256) k_axis_dft(AxisArgs a, PtrSet ps, int L) 
 }
 
 // ------------------------------------------------------------------------------------------
+// SCFT x-pass: real-to-real transforms along axis 1 on complex columns (the real and imaginary
+// parts transform alike, as the reference's separate calls on real() and imag() do,
+// scft_tr.cc:249-259).  With t[j] = (cos, sin)(pi j / 2N), j in [0, 4N):
+//   kind 0  forward CFT  (REDFT10)             Y[k] = 2 sum_n x_n cos(pi (2n+1) k / 2N)
+//   kind 1  forward SFT  (RODFT10, shift right) Y[m] = 2 sum_n x_n sin(pi (2n+1) m / 2N)
+//           (slot m <-> DST-II index m-1; m = 0 gives 0 and index N-1 is never produced,
+//            exactly ArrayShiftRight_SCFT scft_tr.cc:153-184)
+//   kind 2  inverse ICFT (REDFT01)             y_k = X_0 + 2 sum_{m>=1} X_m cos(pi m (2k+1) / 2N)
+//   kind 3  inverse ISFT (shift left, RODFT01) y_k = 2 sum_{m>=1} X_m sin(pi m (2k+1) / 2N)
+// Block: 32 columns (one per lane) x 8 warps; the stored input rows of the tile are staged
+// in shared memory and each warp produces every eighth output row.
+// ------------------------------------------------------------------------------------------
+struct R2RArgs {
+  int kind[kMaxPtr];
+  const cx<double>* trig;  // (cos, sin)(pi j / 2N), j in [0, 4N)
+};
+
+template <typename Ri, typename Ro, typename Rw>
+__global__ void __launch_bounds__(256) k_axis_r2r(AxisArgs a, PtrSet ps, R2RArgs r, int N) {
+  constexpr int W = 32;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cx<Rw>* tr = reinterpret_cast<cx<Rw>*>(smem_raw);  // 4N
+  const int nin = amap_count(a.in);
+  cx<Rw>* tile = tr + 4 * N;                         // [nin][W]
+  const int tid = threadIdx.x, lane = tid & 31, wy = tid >> 5;
+  const int f = blockIdx.z;
+  const int kind = r.kind[f];
+  const cx<Ri>* src = reinterpret_cast<const cx<Ri>*>(ps.src[f]) + (long long)blockIdx.y * a.sb;
+  cx<Ro>* dst = reinterpret_cast<cx<Ro>*>(ps.dst[f]) + (long long)blockIdx.y * a.db;
+  const int col = blockIdx.x * W + lane;
+  const bool ok = col < a.ncols;
+  for (int i = tid; i < 4 * N; i += 256) tr[i] = cvt<Rw>(r.trig[i]);
+  for (int i = tid; i < nin * W; i += 256) {
+    const int row = i / W, w = i % W;
+    const int c2 = blockIdx.x * W + w;
+    tile[i] = (c2 < a.ncols) ? cvt<Rw>(src[(long long)row * a.sr + c2]) : mkc<Rw>(0, 0);
+  }
+  __syncthreads();
+  const int fourN = 4 * N;
+  const bool sine = (kind == 1 || kind == 3);
+  const Rw sc = (Rw)a.scale;
+  for (int ko = wy; ko < a.out.L; ko += 8) {
+    const int orow = amap_row(a.out, ko);
+    if (orow < 0) continue;
+    cx<Rw> acc = mkc<Rw>(0, 0);
+    if (kind <= 1) {
+      // forward: inputs are the N real-space points n (all stored), j = (2n+1) ko
+      const int step = 2 * ko % fourN;
+      int j = ko % fourN;
+      for (int n = 0; n < nin; ++n) {
+        const Rw t = sine ? tr[j].y : tr[j].x;
+        const cx<Rw> x = tile[n * W + lane];
+        acc.x += t * x.x;
+        acc.y += t * x.y;
+        j += step;
+        if (j >= fourN) j -= fourN;
+      }
+      acc.x *= (Rw)2;
+      acc.y *= (Rw)2;
+    } else {
+      // inverse: inputs are the stored spectral slots m, j = m (2 ko + 1)
+      const int odd = (2 * ko + 1) % fourN;
+      int j = 0;
+      for (int rr = 0; rr < nin; ++rr) {
+        const int m = amap_index(a.in, rr);
+        if (rr == 0 || rr == a.in.lo) {
+          j = (int)(((long long)m * odd) % fourN);
+        } else {
+          j += odd;
+          if (j >= fourN) j -= fourN;
+        }
+        const Rw t = (sine ? tr[j].y : tr[j].x) * ((m == 0 && !sine) ? (Rw)1 : (Rw)2);
+        const cx<Rw> x = tile[rr * W + lane];
+        acc.x += t * x.x;
+        acc.y += t * x.y;
+      }
+    }
+    if (ok) dst[(long long)orow * a.dr + col] = cvt<Ro>(sc * acc);
+  }
+}
+
+// ------------------------------------------------------------------------------------------
 // z-pass (contiguous axis) c2r / r2c.  Rows hold N3/2+1 spectral values of which the first
 // `nin` are stored (the rest are zero); the real row of N3 = 2M values is packed as M complex
 // (x[2m] + i x[2m+1]), the reference's in-place layout, followed by a zero padding slot.
@@ -468,34 +550,40 @@ __device__ __forceinline__ cx<R> shfl_c(cx<R> v, int src) {
   return mkc<R>(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
 }
 
-// inverse 32-point DFT across lanes, DIF; tws[s] = e^{+2 pi i (l mod h) / (2h)}, h = 16 >> s
+// Inverse 32-point DFT across lanes, DIF, branch-free.  Stage s pairs lanes l and l ^ h
+// (h = 16 >> s); with p the partner's value the lower lane keeps v + p and the upper lane
+// (p - v) w, w = e^{+2 pi i (l mod h) / (2h)}.  Both are (p + sg v) wl with sg = -1 / +1 and
+// wl = w / 1 on the upper / lower lane (wl[s] precomputed per lane).
 template <typename R, int E>
-__device__ __forceinline__ void lane_dif32(cx<R> (&v)[E], const cx<R> (&tws)[5], int lane) {
+__device__ __forceinline__ void lane_dif32(cx<R> (&v)[E], const cx<R> (&wl)[5], int lane) {
 #pragma unroll
   for (int s = 0; s < 5; ++s) {
     const int h = 16 >> s;
-    const bool upper = (lane & h) != 0;
+    const R sg = (lane & h) ? (R)-1 : (R)1;
 #pragma unroll
     for (int k = 0; k < E; ++k) {
       const cx<R> p = shfl_xor_c(v[k], h);
-      v[k] = upper ? (p - v[k]) * tws[s] : v[k] + p;
+      const cx<R> a = mkc<R>(fma(sg, v[k].x, p.x), fma(sg, v[k].y, p.y));
+      v[k] = a * wl[s];
     }
   }
 }
 
-// forward 32-point DFT across lanes: the adjoint of lane_dif32 (DIT, stages h = 1 .. 16)
+// Forward 32-point DFT across lanes: the adjoint of lane_dif32 (DIT, stages h = 1 .. 16).
+// The upper lane pre-multiplies by conj(w) and both lanes finish with r + sg s, where s is the
+// lane's (weighted) value and r the partner's.
 template <typename R, int E>
-__device__ __forceinline__ void lane_dit32_fwd(cx<R> (&v)[E], const cx<R> (&tws)[5], int lane) {
+__device__ __forceinline__ void lane_dit32_fwd(cx<R> (&v)[E], const cx<R> (&wl)[5], int lane) {
 #pragma unroll
   for (int s = 4; s >= 0; --s) {
     const int h = 16 >> s;
-    const bool upper = (lane & h) != 0;
-    const cx<R> wc = conjc(tws[s]);
+    const R sg = (lane & h) ? (R)-1 : (R)1;
+    const cx<R> wc = conjc(wl[s]);
 #pragma unroll
     for (int k = 0; k < E; ++k) {
-      const cx<R> p = shfl_xor_c(v[k], h);
-      const cx<R> t = wc * (upper ? v[k] : p);
-      v[k] = upper ? p - t : v[k] + t;
+      const cx<R> sv = wc * v[k];
+      const cx<R> r = shfl_xor_c(sv, h);
+      v[k] = mkc<R>(fma(sg, sv.x, r.x), fma(sg, sv.y, r.y));
     }
   }
 }
@@ -516,7 +604,8 @@ __global__ void __launch_bounds__(32 * WPB) k_z_prod_warp(ZArgs a, PtrSet ps, Pr
 #pragma unroll
   for (int s = 0; s < 5; ++s) {
     const int h = 16 >> s;
-    tws[s] = conjc(cvt<Rw>(a.twN[(lane & (h - 1)) * (M / h)]));
+    // e^{+2 pi i (l mod h) / (2h)} on the upper lane of each pair, 1 on the lower lane
+    tws[s] = (lane & h) ? conjc(cvt<Rw>(a.twN[(lane & (h - 1)) * (M / h)])) : mkc<Rw>(1, 0);
   }
   const Rw sc = (Rw)a.scale;
   const long long nwarps = (long long)gridDim.x * WPB;

@@ -56,7 +56,34 @@ cudaError_t run_axis_prec(const AxisLaunch& l, cudaStream_t s) {
   return l.dir < 0 ? run_axis_dir<Ri, Ro, Rw, -1>(l, s) : run_axis_dir<Ri, Ro, Rw, +1>(l, s);
 }
 
+template <typename Ri, typename Ro, typename Rw>
+cudaError_t run_r2r(const AxisLaunch& l, const R2RArgs& r, int N, cudaStream_t s) {
+  const int nin = amap_count(l.a.in);
+  const size_t smem = (size_t)(4 * N + (size_t)nin * 32) * sizeof(cx<Rw>);
+  auto kern = k_axis_r2r<Ri, Ro, Rw>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid((l.a.ncols + 31) / 32, l.nbatch, l.nfields);
+  kern<<<grid, 256, smem, s>>>(l.a, l.ps, r, N);
+  return cudaGetLastError();
+}
+
 }  // namespace
+
+cudaError_t launch_r2r(const AxisLaunch& l, const R2RArgs& r, cudaStream_t s) {
+  if (l.a.ncols <= 0 || l.nbatch <= 0 || l.nfields <= 0) return cudaSuccess;
+  if (l.nbatch > 65535 || l.nfields > kMaxPtr || l.L < 2 || l.L > 1024) return cudaErrorInvalidValue;
+  const int N = l.L;
+  if (l.pwork == F64) {
+    if (l.pin == F64 && l.pout == F64) return run_r2r<double, double, double>(l, r, N, s);
+    return cudaErrorInvalidValue;
+  }
+  if (l.pin == F64 && l.pout == F64) return run_r2r<double, double, float>(l, r, N, s);
+  if (l.pin == F64 && l.pout == F32) return run_r2r<double, float, float>(l, r, N, s);
+  if (l.pin == F32 && l.pout == F32) return run_r2r<float, float, float>(l, r, N, s);
+  if (l.pin == F32 && l.pout == F64) return run_r2r<float, double, float>(l, r, N, s);
+  return cudaErrorInvalidValue;
+}
 
 cudaError_t launch_axis(const AxisLaunch& l, cudaStream_t s) {
   if (l.a.ncols <= 0 || l.nbatch <= 0 || l.nfields <= 0) return cudaSuccess;

@@ -36,6 +36,8 @@ struct ZProdLaunch {
 };
 
 cudaError_t launch_axis(const AxisLaunch& l, cudaStream_t s);
+// SCFT x-pass (real-to-real, per-field kind); l.L = N1, l.dir unused
+cudaError_t launch_r2r(const AxisLaunch& l, const R2RArgs& r, cudaStream_t s);
 cudaError_t launch_z(const ZLaunch& l, cudaStream_t s);
 cudaError_t launch_zprod(const ZProdLaunch& l, cudaStream_t s);
 

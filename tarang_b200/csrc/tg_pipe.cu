@@ -69,7 +69,16 @@ int pipe_inverse_xy(tg_ctx* c, int nf, const void* const* in, const void* const*
     }
     const double insz = inprec == F64 ? 16.0 : 8.0;
     ProfScope pr(c, "x_inverse", nread * el_compact(c) * insz + nf * el_xstage(c) * c->tsz);
-    cudaError_t e = launch_axis(l, c->st);
+    cudaError_t e;
+    if (c->basis == TG_SCFT) {
+      // ISFT / ICFT along x (scft_tr.cc:440-639) on the stored sin/cos slots
+      R2RArgs r{};
+      for (int f = 0; f < nf; ++f) r.kind[f] = c->xinv_kind[f];
+      r.trig = c->trigx;
+      e = launch_r2r(l, r, c->st);
+    } else {
+      e = launch_axis(l, c->st);
+    }
     if (e != cudaSuccess) return cuda_err(c, e, "x inverse");
   }
   {
@@ -171,7 +180,18 @@ int pipe_products_forward(tg_ctx* c, int nin, const void* const* WY, int nprod, 
       l.ps.dst[q] = PX[q];
     }
     ProfScope pr(c, "x_forward", nprod * (el_xstage(c) + el_compact(c)) * c->tsz);
-    cudaError_t e = launch_axis(l, c->st);
+    cudaError_t e;
+    if (c->basis == TG_SCFT) {
+      // SFT / CFT along x with Norm_SCFT's extra 1/2 (scft_tr.cc:89-92; the z-pass applied
+      // 1/(N1 N2 N3))
+      R2RArgs r{};
+      for (int q = 0; q < nprod; ++q) r.kind[q] = c->xfwd_kind[q];
+      r.trig = c->trigx;
+      l.a.scale = 0.5;
+      e = launch_r2r(l, r, c->st);
+    } else {
+      e = launch_axis(l, c->st);
+    }
     if (e != cudaSuccess) return cuda_err(c, e, "x forward");
   }
   return TG_OK;

@@ -86,20 +86,40 @@ __global__ void k_compact_to_dense(Geo g, const cx<R>* __restrict__ comp, cx<dou
 //  MHD   : 0 zp1zm1, 1 zp2zm2, 2 zp3zm3, 3 zp1zm2 (v1), 4 zm1zp2 (w1), 5 zp2zm3 (v2),
 //          6 zm2zp3 (w2), 7 zp3zm1 (v3), 8 zm3zp1 (w3)              (RSprod.cc:117-194)
 //  scalar: fluid 0..5, then 6 u1 th, 7 u2 th, 8 u3 th               (compute_nlin_SF.cc)
+// x-derivative of a coefficient (Xderiv universal_tr.cc:186-210): FOUR i kx; SCFT a real factor
+// by the parity of the series, cos -> sin: -kx (Xderiv_Cos_SCFT), sin -> cos: +kx
+// (Xderiv_Sin_SCFT, scft_tr.cc:649-672)
+struct XDer {
+  double kx;
+  int scft;
+  __device__ __forceinline__ cx<double> cos_in(cx<double> p) const {
+    return scft ? mkc<double>(-kx * p.x, -kx * p.y) : ione(kx * p);
+  }
+  __device__ __forceinline__ cx<double> sin_in(cx<double> p) const {
+    return scft ? mkc<double>(kx * p.x, kx * p.y) : ione(kx * p);
+  }
+};
+__device__ __forceinline__ cx<double> iky_ikz(double ky, double kz, cx<double> b, cx<double> c) {
+  return ione(mkc<double>(ky * b.x + kz * c.x, ky * b.y + kz * c.y));
+}
+
 template <typename Rp, int PHYS>
-__device__ __forceinline__ void assemble(const void* const* PX, long long idx, double kx, double ky, double kz,
+__device__ __forceinline__ void assemble(const void* const* PX, long long idx, const XDer& dx, double ky, double kz,
                                          cx<double>* n) {
   if constexpr (PHYS == PH_FLUID || PHYS == PH_SCALAR || PHYS == PH_RB) {
+    // parities of the products (RV_Forward_transform_RSprod Rvf.cc:179-186): u1u1, u2u2, u3u3,
+    // u2u3 cos; u1u2, u3u1 sin; and u1 th cos, u2 th, u3 th sin (compute_nlin_SF.cc:80-115)
     const cx<double> p0 = ldc<Rp>(PX[0], idx), p1 = ldc<Rp>(PX[1], idx), p2 = ldc<Rp>(PX[2], idx);
     const cx<double> p3 = ldc<Rp>(PX[3], idx), p4 = ldc<Rp>(PX[4], idx), p5 = ldc<Rp>(PX[5], idx);
-    n[0] = ikdot(kx, ky, kz, p0, p3, p5);
-    n[1] = ikdot(kx, ky, kz, p3, p1, p4);
-    n[2] = ikdot(kx, ky, kz, p5, p4, p2);
+    n[0] = dx.cos_in(p0) + iky_ikz(ky, kz, p3, p5);
+    n[1] = dx.sin_in(p3) + iky_ikz(ky, kz, p1, p4);
+    n[2] = dx.sin_in(p5) + iky_ikz(ky, kz, p4, p2);
     if constexpr (PHYS != PH_FLUID) {
       const cx<double> p6 = ldc<Rp>(PX[6], idx), p7 = ldc<Rp>(PX[7], idx), p8 = ldc<Rp>(PX[8], idx);
-      n[3] = ikdot(kx, ky, kz, p6, p7, p8);
+      n[3] = dx.cos_in(p6) + iky_ikz(ky, kz, p7, p8);
     }
   } else {
+    const double kx = dx.kx;
     cx<double> p[9];
 #pragma unroll
     for (int q = 0; q < 9; ++q) p[q] = ldc<Rp>(PX[q], idx);
@@ -125,20 +145,19 @@ struct NState {
   static constexpr int v = (PHYS == PH_FLUID) ? 3 : (PHYS == PH_MHD ? 6 : 4);
 };
 
-// rhs = -[nlin - f + i k p] with p = i k.(nlin - f)/K^2 on the velocity (Compute_pressure,
-// Add_pressure_gradient, Compute_rhs); other fields rhs = -(nlin - f).
-__device__ __forceinline__ void project_rhs(cx<double>* r, int ns, double kx, double ky, double kz, double K2) {
-  const cx<double> kN = kdot(kx, ky, kz, r[0], r[1], r[2]);
+// rhs = -[nlin - f + grad p] with p = div(nlin - f)/K^2 on the velocity (Compute_pressure with
+// Compute_divergence_nlin: Xderiv of nlin1 with parity 1; Add_pressure_gradient: Xderiv of p
+// with parity 0; Compute_rhs); other fields rhs = -(nlin - f).
+__device__ __forceinline__ void project_rhs(cx<double>* r, int ns, const XDer& dx, double ky, double kz, double K2) {
+  cx<double> p = mkc<double>(0, 0);
   if (K2 > 0) {
-    const double inv = 1.0 / K2;
-    r[0] = mkc<double>(-(r[0].x - kx * inv * kN.x), -(r[0].y - kx * inv * kN.y));
-    r[1] = mkc<double>(-(r[1].x - ky * inv * kN.x), -(r[1].y - ky * inv * kN.y));
-    r[2] = mkc<double>(-(r[2].x - kz * inv * kN.x), -(r[2].y - kz * inv * kN.y));
-  } else {
-    r[0] = mkc<double>(-r[0].x, -r[0].y);
-    r[1] = mkc<double>(-r[1].x, -r[1].y);
-    r[2] = mkc<double>(-r[2].x, -r[2].y);
+    const cx<double> div = dx.sin_in(r[0]) + iky_ikz(ky, kz, r[1], r[2]);
+    p = (1.0 / K2) * div;
   }
+  const cx<double> g0 = dx.cos_in(p), g1 = ione(ky * p), g2 = ione(kz * p);
+  r[0] = mkc<double>(-(r[0].x + g0.x), -(r[0].y + g0.y));
+  r[1] = mkc<double>(-(r[1].x + g1.x), -(r[1].y + g1.y));
+  r[2] = mkc<double>(-(r[2].x + g2.x), -(r[2].y + g2.y));
   for (int c = 3; c < ns; ++c) r[c] = mkc<double>(-r[c].x, -r[c].y);
 }
 
@@ -163,14 +182,23 @@ __global__ void __launch_bounds__(TPB) k_rk(RKArgs a) {
       const double K2 = kx * kx + ky * ky + kz * kz;
       cx<double> r[NS];
       if constexpr (SRC == 0) {
-        assemble<Rp, PHYS>(a.PX, idx, kx, ky, kz, r);
+        const XDer dx{kx, g.basis};
+        assemble<Rp, PHYS>(a.PX, idx, dx, ky, kz, r);
         if (a.FB != nullptr && kxi >= -a.fx && kxi <= a.fx && kyi >= -a.fy && kyi <= a.fy && l3 <= a.fz) {
           const int box = (2 * a.fx + 1) * (2 * a.fy + 1) * (a.fz + 1);
           const int p = ((kxi + a.fx) * (2 * a.fy + 1) + (kyi + a.fy)) * (a.fz + 1) + l3;
 #pragma unroll
           for (int c = 0; c < 3; ++c) r[c] = r[c] - a.FB[(long long)c * box + p];
         }
-        project_rhs(r, NS, kx, ky, kz, K2);
+        if constexpr (PHYS == PH_RB) {
+          // Compute_force_RB (compute_force_RB.cc:51-105) from the stage's fields, then Add_force:
+          // nlin1 -= fu * theta, T.nlin -= ft * u1
+          const cx<double> th = a.inprec ? ldc<float>(a.IN[3], idx) : ldc<double>(a.IN[3], idx);
+          const cx<double> u1 = a.inprec ? ldc<float>(a.IN[0], idx) : ldc<double>(a.IN[0], idx);
+          r[0] = r[0] - a.rb_buoy_u * th;
+          r[3] = r[3] - a.rb_buoy_t * u1;
+        }
+        project_rhs(r, NS, dx, ky, kz, K2);
       } else {
 #pragma unroll
         for (int c = 0; c < NS; ++c) r[c] = a.RHS[c][idx];
@@ -199,8 +227,17 @@ __global__ void __launch_bounds__(TPB) k_rk(RKArgs a) {
           a.U0[c][idx] = u;
           const double m2 = u.x * u.x + u.y * u.y;
           const int grp = (PHYS == PH_MHD) ? (c / 3) * 2 : (c < 3 ? 0 : 4);
-          acc[grp] += energy_weight_four(l1, l2, l3, g.N1, g.N2) * m2;
-          acc[grp + 1] += mult_four(l1, l2, l3, g.N1, g.N2) * K2 * m2;
+          double w, m;
+          if (g.basis == 0) {
+            w = energy_weight_four(l1, l2, l3, g.N1, g.N2);
+            m = mult_four(l1, l2, l3, g.N1, g.N2);
+          } else {
+            // Get_total_energy_SCFT (scft_energy.cc:51-104): multiplicity, origin excluded
+            m = mult_scft(l1, l2, l3, g.N2);
+            w = (l1 == 0 && l2 == 0 && l3 == 0) ? m - 0.5 : m;
+          }
+          acc[grp] += w * m2;
+          acc[grp + 1] += m * K2 * m2;
         }
       }
     }
@@ -226,6 +263,7 @@ cudaError_t run_rk_phys(const RKArgs& a, int phys, int src, cudaStream_t s, int 
     case PH_FLUID: return run_rk_src<Rp, Rs, PH_FLUID>(a, src, s, nblk);
     case PH_MHD: return run_rk_src<Rp, Rs, PH_MHD>(a, src, s, nblk);
     case PH_SCALAR: return run_rk_src<Rp, Rs, PH_SCALAR>(a, src, s, nblk);
+    case PH_RB: return run_rk_src<Rp, Rs, PH_RB>(a, src, s, nblk);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -340,7 +378,7 @@ __global__ void k_assemble_v(Geo g, PtrArr6 pa) {
   cx<double> n[NS];
   if (l3 < g.nkz) {
     const double kx = geo_kx(g, r1) * g.kf0, ky = geo_ky(g, r2) * g.kf1, kz = l3 * g.kf2;
-    assemble<Rp, PHYS>(pa.q, idx, kx, ky, kz, n);
+    assemble<Rp, PHYS>(pa.q, idx, XDer{kx, g.basis}, ky, kz, n);
   } else {
 #pragma unroll
     for (int c = 0; c < NS; ++c) n[c] = mkc<double>(0, 0);
@@ -375,8 +413,9 @@ __global__ void k_pressure(Geo g, PtrArr6 pa, cx<double>* PR) {
   if (l3 < g.nkz) {
     const double kx = geo_kx(g, r1) * g.kf0, ky = geo_ky(g, r2) * g.kf1, kz = l3 * g.kf2;
     const double K2 = kx * kx + ky * ky + kz * kz;
-    // Compute_divergence_nlin then CS_divide_ksqr (A(0,0,0) = 0)
-    if (K2 > 0) p = (1.0 / K2) * ikdot(kx, ky, kz, pa.p[0][idx], pa.p[1][idx], pa.p[2][idx]);
+    // Compute_divergence_nlin (Xderiv of nlin1 with parity 1) then CS_divide_ksqr (A(0,0,0) = 0)
+    const XDer dx{kx, g.basis};
+    if (K2 > 0) p = (1.0 / K2) * (dx.sin_in(pa.p[0][idx]) + iky_ikz(ky, kz, pa.p[1][idx], pa.p[2][idx]));
   }
   PR[idx] = p;
 }
@@ -389,15 +428,48 @@ __global__ void k_rhs_from_nlin(Geo g, int ns, PtrArr6 pa, const cx<double>* PR)
   if (l3 >= g.nkz) return;
   const double kx = geo_kx(g, r1) * g.kf0, ky = geo_ky(g, r2) * g.kf1, kz = l3 * g.kf2;
   const cx<double> p = PR[idx];
-  // Add_pressure_gradient: nlin_i += i k_i p; Compute_rhs: nlin = -nlin
-  const cx<double> g0 = ione(kx * p), g1 = ione(ky * p), g2 = ione(kz * p);
+  // Add_pressure_gradient (Xderiv of p with parity 0, Yderiv, Zderiv); Compute_rhs: nlin = -nlin
+  const cx<double> g0 = XDer{kx, g.basis}.cos_in(p), g1 = ione(ky * p), g2 = ione(kz * p);
   pa.p[0][idx] = mkc<double>(0, 0) - (pa.p[0][idx] + g0);
   pa.p[1][idx] = mkc<double>(0, 0) - (pa.p[1][idx] + g1);
   pa.p[2][idx] = mkc<double>(0, 0) - (pa.p[2][idx] + g2);
   for (int c = 3; c < ns; ++c) pa.p[c][idx] = mkc<double>(0, 0) - pa.p[c][idx];
 }
 
+// Add_force(T) for RB (add_force.cc:62-68) with Compute_force_RB: nlin1 -= fu theta,
+// T.nlin -= ft u1 (theta, u1 from the master state)
+__global__ void k_rb_sub_force(Geo g, PtrArr6 pa, const cx<double>* u1, const cx<double>* th, double fu, double ft) {
+  const long long idx = (long long)blockIdx.x * TPB + threadIdx.x;
+  if (idx >= g.S) return;
+  pa.p[0][idx] = pa.p[0][idx] - fu * th[idx];
+  pa.p[3][idx] = pa.p[3][idx] - ft * u1[idx];
+}
+
 // ------------------------------------------------------------------ reductions
+// cross energy Re(A B*) with the energy weights (Get_total_energy(A, B), four_energy.cc:108-168,
+// scft_energy.cc:108-158), per block into part[b * nslots + slot]
+__global__ void __launch_bounds__(TPB) k_cross_partials(Geo g, const cx<double>* A, const cx<double>* B, double* part, int slot, int nslots) {
+  double acc[1] = {0};
+  const long long stride = (long long)gridDim.x * TPB;
+  for (long long idx = (long long)blockIdx.x * TPB + threadIdx.x; idx < g.S; idx += stride) {
+    int r1, r2, l3;
+    compact_mode(g, idx, r1, r2, l3);
+    if (l3 >= g.nkz) continue;
+    const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
+    double w;
+    if (g.basis == 0) {
+      w = energy_weight_four(l1, l2, l3, g.N1, g.N2);
+    } else {
+      const double m = mult_scft(l1, l2, l3, g.N2);
+      w = (l1 == 0 && l2 == 0 && l3 == 0) ? m - 0.5 : m;
+    }
+    const cx<double> a = A[idx], b = B[idx];
+    acc[0] += w * (a.x * b.x + a.y * b.y);
+  }
+  block_sum<1>(acc);
+  if (threadIdx.x == 0) part[(long long)blockIdx.x * nslots + slot] = acc[0];
+}
+
 __global__ void __launch_bounds__(TPB) k_energy_partials(Geo g, PtrArr6 pa, int nf, double* part, int slot, int nslots) {
   double acc[2] = {0, 0};
   const long long stride = (long long)gridDim.x * TPB;
@@ -496,7 +568,7 @@ __global__ void __launch_bounds__(TPB) k_shell_spectrum(Geo g, PtrArr6 pa, int n
       const cx<double> u = pa.p[c][idx];
       atomicAdd(&sh[c * nbins + bin], m * kp * (u.x * u.x + u.y * u.y));
     }
-    atomicAdd(&sh[nf * nbins + bin], m);
+    atomicAdd(&sh[nf * nbins + bin], g.basis == 0 ? m : 0.5 * m);  // SCFT counts factor/2 (scft_energy.cc:279)
   }
   __syncthreads();
   for (int i = threadIdx.x; i < nf * nbins; i += TPB)
@@ -581,6 +653,22 @@ cudaError_t launch_rhs_from_nlin(const Geo& g, int phys, cx<double>* const* NL, 
   const int ns = phys == PH_FLUID ? 3 : (phys == PH_MHD ? 6 : 4);
   for (int c = 0; c < ns; ++c) pa.p[c] = NL[c];
   k_rhs_from_nlin<<<nblk(g.S), TPB, 0, s>>>(g, ns, pa, PR);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rb_sub_force(const Geo& g, cx<double>* const* NL, const cx<double>* u1, const cx<double>* th,
+                                double fu, double ft, cudaStream_t s) {
+  PtrArr6 pa{};
+  for (int c = 0; c < 4; ++c) pa.p[c] = NL[c];
+  k_rb_sub_force<<<nblk(g.S), TPB, 0, s>>>(g, pa, u1, th, fu, ft);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cross_partials(const Geo& g, const cx<double>* A, const cx<double>* B, double* part, int slot,
+                                  int nslots, cudaStream_t s, int* nblocks) {
+  const int nb = nred(g.S);
+  if (nblocks) *nblocks = nb;
+  k_cross_partials<<<nb, TPB, 0, s>>>(g, A, B, part, slot, nslots);
   return cudaGetLastError();
 }
 

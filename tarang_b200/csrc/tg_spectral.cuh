@@ -72,7 +72,9 @@ struct RKArgs {
   const cx<double>* FB;    // force box [nstate][box] or null
   int fx, fy, fz;          // force box half widths (kx, ky in [-f, f], kz in [0, fz])
   double* part;            // stage 4: per-block partial sums [blocks][8]
-  double rb_buoy_u, rb_buoy_t;  // RB: rhs_u1 += rb_buoy_u * theta, rhs_T += rb_buoy_t * u1
+  double rb_buoy_u, rb_buoy_t;  // RB forces: Force1 = rb_buoy_u * theta, T.Force = rb_buoy_t * u1
+  const void* IN[6];       // the stage's input fields (the forces are computed from them)
+  int inprec;              // 0 FP64, 1 FP32
 };
 
 struct ForceArgs {
@@ -94,6 +96,10 @@ cudaError_t launch_assemble_nlin(const Geo& g, int phys, int pprec, const void* 
 cudaError_t launch_sub_force_box(const Geo& g, int ncomp, const cx<double>* FB, int fx, int fy, int fz, cx<double>* const* NL, cudaStream_t s);
 cudaError_t launch_pressure(const Geo& g, const cx<double>* const* NL, cx<double>* PR, cudaStream_t s);
 cudaError_t launch_rhs_from_nlin(const Geo& g, int phys, cx<double>* const* NL, const cx<double>* PR, cudaStream_t s);
+cudaError_t launch_rb_sub_force(const Geo& g, cx<double>* const* NL, const cx<double>* u1, const cx<double>* th,
+                                double fu, double ft, cudaStream_t s);
+cudaError_t launch_cross_partials(const Geo& g, const cx<double>* A, const cx<double>* B, double* part, int slot,
+                                  int nslots, cudaStream_t s, int* nblocks);
 // energy partials of a group of fields (FP64 compact), per block: [E, D]
 cudaError_t launch_energy_partials(const Geo& g, const cx<double>* const* F, int nf, double* part, int slot, int nslots, cudaStream_t s, int* nblocks);
 // reduce partials [nblocks][nslots] -> out[nslots] in fixed order; then the dt rule

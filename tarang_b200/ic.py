@@ -88,6 +88,35 @@ def taylor_green(N, k0=1, amp=1.0):
     return V
 
 
+def rb_perturbation(N, nmodes=8, amp=1e-3, seed=20261205):
+    """Rayleigh-Benard initial temperature deviation in the SCFT basis: modes 1 <= m <= nmodes,
+    |ky| <= nmodes, kz <= nmodes get real and imaginary parts uniform in (-amp, amp) (seeded),
+    then the SCFT reality condition on the kz = 0 plane (universal_misc.cc:93-104); the velocity
+    starts at zero.  Returns theta, shape (N1, N2, N3/2+1)."""
+    N1, N2, N3 = N
+    rng = np.random.Generator(np.random.PCG64(seed))
+    T = np.zeros((N1, N2, N3 // 2 + 1), dtype=np.complex128)
+    kys = list(range(0, nmodes + 1)) + list(range(-nmodes, 0))
+    for m in range(1, min(nmodes, N1 - 1) + 1):
+        for ky in kys:
+            ly = ky if ky >= 0 else ky + N2
+            for kz in range(0, min(nmodes, N3 // 2) + 1):
+                re, im = rng.uniform(-amp, amp, size=2)
+                T[m, ly, kz] = re + 1j * im
+    for ly in range(N2 // 2 + 1, N2):
+        T[:, ly, 0] = np.conj(T[:, N2 - ly, 0])
+    T[:, 0, 0] = T[:, 0, 0].real
+    # the reference dealiases every initial condition (SCFT 2/3 rule, universal_misc.cc:142-158)
+    keep = np.ones(T.shape, dtype=bool)
+    if N1 >= 3:
+        keep[2 * N1 // 3:] = False
+    if N2 >= 3:
+        keep[:, N2 // 3: 2 * N2 // 3 + 2] = False
+    if N3 >= 3:
+        keep[:, :, N3 // 3: N3 // 2 + 1] = False
+    return np.where(keep, T, 0)
+
+
 def random_phase_field(N, kfactor=(1.0, 1.0, 1.0), k0=4.0, energy=0.5, seed=20261202, dealias=True):
     """Seeded random-phase divergence-free field with E(k) ~ k^4 exp(-2 (k/k0)^2), total
     energy `energy` in the Get_total_energy convention.  Returns [V1, V2, V3]."""

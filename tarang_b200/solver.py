@@ -49,7 +49,9 @@ def make_config(N, basis="FOUR", physics="FLUID", precision="FP64", dealias=True
     cfg.eta = float(nu if eta is None else eta)
     cfg.kappa = float(nu if kappa is None else kappa)
     cfg.dt = float(dt)
-    if force is None or force == "decay":
+    if force is None and cfg.physics == L.TG_RB:
+        cfg.force_kind = L.TG_FORCE_RB          # Compute_force_RB (force_field_proc 51)
+    elif force is None or force == "decay":
         cfg.force_kind = L.TG_FORCE_DECAY
     else:
         cfg.force_kind = L.TG_FORCE_ENERGY_SUPPLY
@@ -218,7 +220,11 @@ class IncFluid:
         d = 3 if self.cfg.dealias else 2
         kf = self.cfg.kfactor
         N = self.N
-        return int(math.ceil(math.sqrt(((N[0] // d) * kf[0]) ** 2 + ((N[1] // d) * kf[1]) ** 2
+        if self.cfg.basis == L.TG_SCFT:   # Min_radius_outside_SCFT: kx extent 2N1/3 (N1 aliased)
+            nx = (2 * N[0] // 3) if self.cfg.dealias else N[0]
+        else:
+            nx = N[0] // d
+        return int(math.ceil(math.sqrt((nx * kf[0]) ** 2 + ((N[1] // d) * kf[1]) ** 2
                                        + ((N[2] // d) * kf[2]) ** 2)))
 
     def CV_Compute_shell_spectrum(self, group: int = 0):

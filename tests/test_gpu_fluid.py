@@ -68,6 +68,20 @@ def test_energy_dissipation_spectrum(lib):
     assert np.abs(dk - dw).max() < 1e-12 * np.abs(dw).max()
 
 
+def test_spectrum_partial_shells(lib):
+    """Energy out to the corners of the dealiased cube: the shells beyond kmax_inside are
+    rescaled by Approx_number_modes_in_shell / count, with counts over the whole grid."""
+    N = (64, 64, 64)
+    V = ic.random_phase_field(N, k0=40.0, seed=14)
+    s = make(N)
+    s.set_V(V)
+    ek, dk = s.CV_Compute_shell_spectrum()
+    for i in range(3):
+        w = o.shell_spectrum(V[i], 0, KF)
+        assert np.abs(ek[i] - w).max() < 1e-12 * np.abs(w).max()
+        assert w[25] > 1e-3 * np.abs(w).max()   # the partial shells carry energy here
+
+
 def test_get_dt(lib):
     N = (64, 64, 64)
     V = ic.random_phase_field(N, seed=5, energy=50.0)   # large energy: the CFL bound is active
