@@ -216,44 +216,84 @@ int tg_profile_enable(tg_ctx* ctx, int enable);
 int tg_profile_read(tg_ctx* ctx, tg_kernel_stat* out, int max, int* n);
 
 /* ------------------------------------------------------------------------------------------
- * Serving: a persistent request loop that admits independent solves by HBM budget, keeps
- * their spectral state resident and advances same-shape requests together.
+ * Serving (no counterpart in the reference, whose programs run one solve per process,
+ * src/main.cc:95-151): a request loop that admits independent solves by an HBM budget, keeps
+ * their spectral state resident and advances requests of the same shape together.
+ *
+ * Requests whose configurations agree on everything but the coefficients (nu, eta, kappa, Ra,
+ * Pr, dt) share a batch: one context with B slots whose kernels take the slot as a grid
+ * dimension, so one launch of each pass (and one CUDA graph per step) advances all of them.
+ * Each slot's arithmetic is the same as that of a lone context: a request's fields after n
+ * steps do not depend on what else is resident (bit for bit), and equal tg_step's.  Forced
+ * requests (TG_FORCE_ENERGY_SUPPLY) get a context of their own.
+ *
+ * One host thread drives a server; calls on one server must not overlap.
  * ---------------------------------------------------------------------------------------- */
 typedef struct tg_server tg_server;
 
 typedef struct tg_server_config {
-  size_t hbm_budget_bytes; /* admission budget */
-  int max_batch;           /* most requests of one shape advanced together */
+  size_t hbm_budget_bytes; /* admission budget: device bytes of all resident batches */
+  int max_batch;           /* most requests in one batch */
   int device;
-  int use_graphs;          /* 1: replay one captured CUDA graph per shape and batch size */
+  int use_graphs;          /* 1: replay one captured CUDA graph per batch and active count */
+  int keep_results;        /* 1: keep each finished request's fields for tg_server_result */
 } tg_server_config;
 
 typedef struct tg_request {
-  tg_config cfg;        /* shape, physics, precision, coefficients */
+  tg_config cfg;        /* shape, physics, precision, coefficients (device and stream ignored) */
   int n_steps;          /* RK4 steps to run */
   const double* init;   /* initial fields, reference layout, concatenated per state field
                            (fluid 3, MHD 6, scalar/RB 4); copied at submit */
   size_t n_doubles;     /* length of init */
 } tg_request;
 
+#define TG_REQ_QUEUED 0
+#define TG_REQ_RUNNING 1
+#define TG_REQ_DONE 2
+#define TG_REQ_FAILED 3
+
 typedef struct tg_request_status {
-  int state;            /* 0 queued, 1 running, 2 done, 3 failed */
-  int error;            /* TG_ERR_* when failed */
+  int state;            /* TG_REQ_* */
+  int error;            /* TG_ERR_* when failed: TG_ERR_OOM (does not fit the budget),
+                           TG_ERR_NONFINITE (energy not finite), TG_ERR_CUDA */
   int steps_done;
   double submit_s, start_s, finish_s; /* server clock (seconds) */
-  double final_energy;
+  double final_energy;  /* kinetic energy after the last step (MHD: kinetic + magnetic) */
+  double t_final;       /* simulated time */
 } tg_request_status;
+
+typedef struct tg_server_stats {
+  size_t bytes_resident;   /* device bytes of the resident batches */
+  size_t bytes_peak;
+  int n_batches;           /* resident batches */
+  int n_running, n_queued;
+  long long rounds;        /* pump rounds that advanced at least one batch */
+  long long request_steps; /* steps advanced, summed over requests */
+  long long graph_launches, eager_steps;
+} tg_server_stats;
+
+/* device bytes that a batch of `batch` requests of configuration cfg holds (admission cost) */
+int tg_request_bytes(const tg_config* cfg, int batch, size_t* bytes);
 
 int tg_server_create(const tg_server_config* cfg, tg_server** out);
 int tg_server_destroy(tg_server* srv);
+/* validates and copies the request; TG_ERR_ARG / TG_ERR_UNSUPPORTED for a configuration that
+ * tg_ctx_create rejects or an init of the wrong length (no id).  A request that cannot fit the
+ * budget even alone gets an id and state TG_REQ_FAILED with TG_ERR_OOM. */
 int tg_server_submit(tg_server* srv, const tg_request* req, long long* id);
-/* one scheduling round: admit what fits, advance every resident batch by one step */
+/* one scheduling round: admit queued requests that fit (first come first served, later ones
+ * may pass one that waits for room), advance every resident batch by one step (batches on
+ * their own streams, overlapping), retire finished and failed requests; *n_active = requests
+ * running or queued afterwards */
 int tg_server_pump(tg_server* srv, int* n_active);
 /* pump until every submitted request is done or failed (bounded by max_rounds; 0 = no bound) */
 int tg_server_drain(tg_server* srv, long long max_rounds);
 int tg_server_poll(tg_server* srv, long long id, tg_request_status* st);
-/* final state of a finished request, reference layout, same packing as tg_request.init */
+/* final fields of a finished request (keep_results = 1), same packing as tg_request.init */
 int tg_server_result(tg_server* srv, long long id, double* host, size_t n_doubles);
+/* drop a finished request's kept fields */
+int tg_server_release(tg_server* srv, long long id);
+int tg_server_stats_get(tg_server* srv, tg_server_stats* st);
 double tg_server_clock(tg_server* srv);
 
 #ifdef __cplusplus

@@ -41,6 +41,8 @@ TG_NFIELDS = 32
 
 TG_ET_UU, TG_ET_BB, TG_ET_UB, TG_ET_BU, TG_ET_TT = 0, 1, 2, 3, 4
 
+TG_REQ_QUEUED, TG_REQ_RUNNING, TG_REQ_DONE, TG_REQ_FAILED = 0, 1, 2, 3
+
 ERR_NAMES = {
     TG_ERR_ARG: "TG_ERR_ARG", TG_ERR_OOM: "TG_ERR_OOM", TG_ERR_NONFINITE: "TG_ERR_NONFINITE",
     TG_ERR_CUDA: "TG_ERR_CUDA", TG_ERR_UNSUPPORTED: "TG_ERR_UNSUPPORTED",
@@ -77,6 +79,7 @@ class tg_server_config(C.Structure):
         ("max_batch", C.c_int),
         ("device", C.c_int),
         ("use_graphs", C.c_int),
+        ("keep_results", C.c_int),
     ]
 
 
@@ -98,6 +101,21 @@ class tg_request_status(C.Structure):
         ("start_s", C.c_double),
         ("finish_s", C.c_double),
         ("final_energy", C.c_double),
+        ("t_final", C.c_double),
+    ]
+
+
+class tg_server_stats(C.Structure):
+    _fields_ = [
+        ("bytes_resident", C.c_size_t),
+        ("bytes_peak", C.c_size_t),
+        ("n_batches", C.c_int),
+        ("n_running", C.c_int),
+        ("n_queued", C.c_int),
+        ("rounds", C.c_longlong),
+        ("request_steps", C.c_longlong),
+        ("graph_launches", C.c_longlong),
+        ("eager_steps", C.c_longlong),
     ]
 
 
@@ -150,7 +168,10 @@ SIGNATURES = {
     "tg_server_drain": (C.c_int, [_VP, C.c_longlong]),
     "tg_server_poll": (C.c_int, [_VP, C.c_longlong, C.POINTER(tg_request_status)]),
     "tg_server_result": (C.c_int, [_VP, C.c_longlong, _DP, C.c_size_t]),
+    "tg_server_release": (C.c_int, [_VP, C.c_longlong]),
+    "tg_server_stats_get": (C.c_int, [_VP, C.POINTER(tg_server_stats)]),
     "tg_server_clock": (C.c_double, [_VP]),
+    "tg_request_bytes": (C.c_int, [C.POINTER(tg_config), C.c_int, C.POINTER(C.c_size_t)]),
 }
 
 _lib = None

@@ -178,46 +178,60 @@ RKArgs rk_args(tg_ctx* c, int stage) {
   a.part = (stage == 4) ? c->part : nullptr;
   a.rb_buoy_u = c->rb_fu;
   a.rb_buoy_t = c->rb_ft;
+  a.nact = c->nact;
+  a.nu_tab = c->nu_tab;
   return a;
 }
 
-int run_finalize(tg_ctx* c, int dt_mode, bool ring) {
+// reduce the partials of slots r0 .. r0+n-1 and apply the dt rule to each of them
+int run_finalize(tg_ctx* c, int dt_mode, bool ring, int r0 = 0, int n = -1) {
+  if (n < 0) n = c->nact;
   FinalizeArgs f{};
-  f.part = c->part;
+  f.part = c->part + (size_t)r0 * 8 * c->npart_blocks;
   f.nblocks = c->npart_blocks;
   f.nslots = 8;
-  f.out = c->red_out;
-  f.scal = c->scal;
-  f.ering = ring ? c->ering : nullptr;
+  f.out = c->red_out + (size_t)r0 * 8;
+  f.scal = c->scal + (size_t)r0 * 8;
+  f.ering = (ring && r0 == 0) ? c->ering : nullptr;
   f.ering_pos = c->ering_pos;
   f.dt_mode = dt_mode;
   f.dx = c->dx_cfl;
   f.Tdt = c->cfg.dt;
   f.mhd = (c->phys == TG_MHD);
+  f.nact = n;
+  f.S = c->S;
   if (f.mhd) {
     // mean field B0 = real(B(0,0,0)) (compute_dt.cc:86-93): compact index 0 is the origin
-    for (int i = 0; i < 3; ++i) f.B0[i] = c->U0[3 + i];
+    for (int i = 0; i < 3; ++i) f.B0[i] = c->U0[3 + i] + (size_t)r0 * c->S;
   }
   ProfScope pr(c, "finalize", 0.0);
   TG_CK(launch_finalize(f, c->st));
   return TG_OK;
 }
 
-// energy partials of the master state into slots (U: 0,1; B: 2,3; T: 4,5) + finalize
-int run_energy(tg_ctx* c, int dt_mode) {
-  TG_CK(cudaMemsetAsync(c->part, 0, sizeof(double) * 8 * (size_t)c->npart_blocks, c->st));
+}  // namespace
+
+namespace tg {
+// energy partials of the master state of slots r0 .. r0+n-1 into reduction slots (U: 0,1;
+// B: 2,3; T: 4,5), then finalize
+int run_energy_slots(tg_ctx* c, int dt_mode, int r0, int n) {
+  const size_t o = (size_t)r0 * c->S;
+  double* part = c->part + (size_t)r0 * 8 * c->npart_blocks;
+  TG_CK(cudaMemsetAsync(part, 0, sizeof(double) * 8 * (size_t)c->npart_blocks * n, c->st));
   int nb = 0;
-  const cx<double>* F[3] = {c->U0[0], c->U0[1], c->U0[2]};
-  TG_CK(launch_energy_partials(c->g, F, 3, c->part, 0, 8, c->st, &nb));
+  const cx<double>* F[3] = {c->U0[0] + o, c->U0[1] + o, c->U0[2] + o};
+  TG_CK(launch_energy_partials(c->g, F, 3, part, 0, 8, c->st, &nb, n));
   if (c->phys == TG_MHD) {
-    const cx<double>* B[3] = {c->U0[3], c->U0[4], c->U0[5]};
-    TG_CK(launch_energy_partials(c->g, B, 3, c->part, 2, 8, c->st, &nb));
+    const cx<double>* B[3] = {c->U0[3] + o, c->U0[4] + o, c->U0[5] + o};
+    TG_CK(launch_energy_partials(c->g, B, 3, part, 2, 8, c->st, &nb, n));
   } else if (c->phys == TG_SCALAR || c->phys == TG_RB) {
-    const cx<double>* T[1] = {c->U0[3]};
-    TG_CK(launch_energy_partials(c->g, T, 1, c->part, 4, 8, c->st, &nb));
+    const cx<double>* T[1] = {c->U0[3] + o};
+    TG_CK(launch_energy_partials(c->g, T, 1, part, 4, 8, c->st, &nb, n));
   }
-  return run_finalize(c, dt_mode, false);
+  return run_finalize(c, dt_mode, false, r0, n);
 }
+
+int run_energy(tg_ctx* c, int dt_mode) { return run_energy_slots(c, dt_mode, 0, c->nact); }
 
 int ensure_dt(tg_ctx* c) {
   if (c->energy_valid) return TG_OK;
@@ -257,7 +271,10 @@ int run_stages(tg_ctx* c, int first_stage, bool ring) {
   return run_finalize(c, 1, ring);
 }
 
-int enqueue_step(tg_ctx* c) { return run_stages(c, 1, true); }
+int enqueue_step(tg_ctx* c, bool ring) { return run_stages(c, 1, ring); }
+}  // namespace tg
+
+namespace {
 
 int field_state_index(const tg_ctx* c, int field) {
   if (field >= TG_V1 && field <= TG_V3) return field - TG_V1;
@@ -398,6 +415,7 @@ void free_ctx(tg_ctx* c) {
   fr(c->FB);
   fr(c->trigx);
   fr(c->scal);
+  fr(c->nu_tab);
   fr(c->red_out);
   fr(c->part);
   fr(c->ering);
@@ -464,25 +482,17 @@ void tg_config_default(tg_config* cfg) {
 
 const char* tg_last_error(const tg_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
-int tg_ctx_create(const tg_config* cfg, tg_ctx** out) {
-  if (!cfg || !out) return TG_ERR_ARG;
+}  // extern "C"
+
+namespace tg {
+int ctx_create_batch(const tg_config* cfg, int B, tg_ctx** out) {
+  if (!cfg || !out || B < 1) return TG_ERR_ARG;
   *out = nullptr;
+  {
+    const int v = validate_config(cfg);
+    if (v) return v;
+  }
   const int N1 = cfg->N[0], N2 = cfg->N[1], N3 = cfg->N[2];
-  if (N1 < 2 || N2 < 2 || N3 < 4 || (N3 & 1)) return TG_ERR_ARG;
-  if (cfg->basis != TG_FOUR && cfg->basis != TG_SCFT) return TG_ERR_ARG;
-  if (cfg->physics < TG_FLUID || cfg->physics > TG_RB) return TG_ERR_ARG;
-  if (cfg->basis == TG_SCFT && cfg->physics == TG_MHD) return TG_ERR_UNSUPPORTED;
-  if (cfg->physics == TG_RB && !(cfg->rb_ra > 0 && cfg->rb_pr > 0)) return TG_ERR_ARG;
-  if (cfg->precision != TG_FP64 && cfg->precision != TG_FP32_MIXED) return TG_ERR_ARG;
-  if (cfg->scheme != TG_RK4) return TG_ERR_UNSUPPORTED;
-  if (cfg->force_kind != TG_FORCE_DECAY && cfg->force_kind != TG_FORCE_ENERGY_SUPPLY && cfg->force_kind != TG_FORCE_RB)
-    return TG_ERR_UNSUPPORTED;
-  if (cfg->force_kind == TG_FORCE_RB && cfg->physics != TG_RB) return TG_ERR_ARG;
-  if (cfg->force_kind == TG_FORCE_ENERGY_SUPPLY && cfg->basis != TG_FOUR) return TG_ERR_UNSUPPORTED;
-  if (cfg->force_kind == TG_FORCE_ENERGY_SUPPLY && cfg->physics != TG_FLUID) return TG_ERR_UNSUPPORTED;
-  for (int i = 0; i < 3; ++i)
-    if (!(cfg->kfactor[i] > 0)) return TG_ERR_ARG;
-  if (!(cfg->dt > 0)) return TG_ERR_ARG;
   // the fused product z-pass needs N3/2 in {4..256} (a power of two); other grids get the
   // transform API only.  The x and y passes take any length.
   const int Mz = N3 / 2;
@@ -543,48 +553,39 @@ int tg_ctx_create(const tg_config* cfg, tg_ctx** out) {
     c->nstate = 3;
     c->nin = 3;
     c->nprod = 6;
-    const signed char A[6] = {0, 1, 2, 0, 1, 2}, B[6] = {0, 1, 2, 1, 2, 0};
+    const signed char PA[6] = {0, 1, 2, 0, 1, 2}, PB[6] = {0, 1, 2, 1, 2, 0};
     for (int q = 0; q < 6; ++q) {
-      pp.a[q] = A[q];
-      pp.b[q] = B[q];
+      pp.a[q] = PA[q];
+      pp.b[q] = PB[q];
     }
-    for (int i = 0; i < 3; ++i) c->nu_of[i] = cfg->nu;
   } else if (c->phys == TG_MHD) {
     c->nstate = 6;
     c->nin = 6;
     c->nprod = 9;
     // inputs 0..2 = z+, 3..5 = z-
-    const signed char A[9] = {0, 1, 2, 0, 3, 1, 4, 2, 5}, B[9] = {3, 4, 5, 4, 1, 5, 2, 3, 0};
+    const signed char PA[9] = {0, 1, 2, 0, 3, 1, 4, 2, 5}, PB[9] = {3, 4, 5, 4, 1, 5, 2, 3, 0};
     for (int q = 0; q < 9; ++q) {
-      pp.a[q] = A[q];
-      pp.b[q] = B[q];
-    }
-    for (int i = 0; i < 3; ++i) {
-      c->nu_of[i] = cfg->nu;
-      c->nu_of[3 + i] = cfg->eta;
+      pp.a[q] = PA[q];
+      pp.b[q] = PB[q];
     }
   } else {
     c->nstate = 4;
     c->nin = 4;
     c->nprod = 9;
-    const signed char A[9] = {0, 1, 2, 0, 1, 2, 0, 1, 2}, B[9] = {0, 1, 2, 1, 2, 0, 3, 3, 3};
+    const signed char PA[9] = {0, 1, 2, 0, 1, 2, 0, 1, 2}, PB[9] = {0, 1, 2, 1, 2, 0, 3, 3, 3};
     for (int q = 0; q < 9; ++q) {
-      pp.a[q] = A[q];
-      pp.b[q] = B[q];
+      pp.a[q] = PA[q];
+      pp.b[q] = PB[q];
     }
-    for (int i = 0; i < 3; ++i) c->nu_of[i] = cfg->nu;
-    c->nu_of[3] = cfg->kappa;
     if (c->phys == TG_RB) {
-      // PRLARGE + ULARGE (RB_slip_main.cc:236-240): nu = sqrt(Pr/Ra), kappa = 1/sqrt(Pr Ra);
       // Compute_force_RB: Force1 = theta, T.Force = temperature_grad (+1) u1
-      const double nu = std::sqrt(cfg->rb_pr / cfg->rb_ra), ka = 1.0 / std::sqrt(cfg->rb_pr * cfg->rb_ra);
-      for (int i = 0; i < 3; ++i) c->nu_of[i] = nu;
-      c->nu_of[3] = ka;
       const double on = (cfg->force_kind == TG_FORCE_RB) ? 1.0 : 0.0;
       c->rb_fu = on;
       c->rb_ft = on;
     }
   }
+
+  state_viscosities(cfg, c->nu_of);
 
   int rc = TG_OK;
   auto fail = [&](int code) {
@@ -617,17 +618,21 @@ int tg_ctx_create(const tg_config* cfg, tg_ctx** out) {
     rc = make_twiddles(c, L);
     if (rc) return fail(rc);
   }
-  const size_t Sd = sizeof(cx<double>) * (size_t)g.S;
-  const size_t St = c->tsz * (size_t)g.S;
-  const size_t WXb = c->tsz * (size_t)N1 * g.nky * g.kzp;
-  const size_t WYb = c->tsz * (size_t)N1 * N2 * g.kzp;
+  // a batch of B same-shape requests stores request r of every field at offset r * S
+  c->B = B;
+  c->nact = 1;
+  const size_t Sd1 = sizeof(cx<double>) * (size_t)g.S;
+  const size_t Sd = Sd1 * B;
+  const size_t St = c->tsz * (size_t)g.S * B;
+  const size_t WXb = c->tsz * (size_t)N1 * g.nky * g.kzp * B;
+  const size_t WYb = c->tsz * (size_t)N1 * N2 * g.kzp * B;
   for (int i = 0; i < c->nstate; ++i) {
     if ((rc = dalloc(c, (void**)&c->U0[i], Sd))) return fail(rc);
     if ((rc = dalloc(c, (void**)&c->TOT[i], Sd))) return fail(rc);
     if ((rc = dalloc(c, &c->US[i], St))) return fail(rc);
-    if ((rc = dalloc(c, (void**)&c->NL[i], Sd))) return fail(rc);
+    if ((rc = dalloc(c, (void**)&c->NL[i], Sd1))) return fail(rc);
   }
-  if ((rc = dalloc(c, (void**)&c->PR, Sd))) return fail(rc);
+  if ((rc = dalloc(c, (void**)&c->PR, Sd1))) return fail(rc);
   for (int i = 0; i < c->nin; ++i) {
     if ((rc = dalloc(c, &c->WX[i], WXb))) return fail(rc);
     if ((rc = dalloc(c, &c->WY[i], WYb))) return fail(rc);
@@ -638,20 +643,36 @@ int tg_ctx_create(const tg_config* cfg, tg_ctx** out) {
     if ((rc = dalloc(c, &c->PX[q], St))) return fail(rc);
   }
   c->npart_blocks = reduction_blocks(g.S);
-  if ((rc = dalloc(c, (void**)&c->part, sizeof(double) * 8 * (size_t)c->npart_blocks))) return fail(rc);
-  if ((rc = dalloc(c, (void**)&c->scal, sizeof(double) * 8))) return fail(rc);
-  if ((rc = dalloc(c, (void**)&c->red_out, sizeof(double) * 8))) return fail(rc);
+  if ((rc = dalloc(c, (void**)&c->part, sizeof(double) * 8 * (size_t)c->npart_blocks * B))) return fail(rc);
+  if ((rc = dalloc(c, (void**)&c->scal, sizeof(double) * 8 * B))) return fail(rc);
+  if ((rc = dalloc(c, (void**)&c->red_out, sizeof(double) * 8 * B))) return fail(rc);
+  if ((rc = dalloc(c, (void**)&c->nu_tab, sizeof(double) * 6 * B))) return fail(rc);
+  {
+    std::vector<double> nut((size_t)6 * B);
+    for (int r = 0; r < B; ++r)
+      for (int i = 0; i < 6; ++i) nut[(size_t)r * 6 + i] = c->nu_of[i];
+    e = cudaMemcpyAsync(c->nu_tab, nut.data(), sizeof(double) * nut.size(), cudaMemcpyHostToDevice, c->st);
+    if (e != cudaSuccess) return fail(cuda_err(c, e, "init viscosities"));
+  }
   c->ering_cap = 1 << 16;
   if ((rc = dalloc(c, (void**)&c->ering, sizeof(double) * c->ering_cap))) return fail(rc);
   if ((rc = dalloc(c, (void**)&c->ering_pos, sizeof(int) * 4))) return fail(rc);
   if (cudaMallocHost(&c->h_pinned, sizeof(double) * 1024) != cudaSuccess) return fail(TG_ERR_OOM);
   {
-    double init[8] = {cfg->dt, 0, 0, 0, 0, 0, 0, 0};
-    e = cudaMemcpyAsync(c->scal, init, sizeof(init), cudaMemcpyHostToDevice, c->st);
+    // per request: dt, t, steps, non-finite flag, Tdt
+    std::vector<double> init((size_t)8 * B, 0.0);
+    for (int r = 0; r < B; ++r) {
+      init[(size_t)r * 8 + 0] = cfg->dt;
+      init[(size_t)r * 8 + 4] = cfg->dt;
+    }
+    e = cudaMemcpyAsync(c->scal, init.data(), sizeof(double) * init.size(), cudaMemcpyHostToDevice, c->st);
+    if (e != cudaSuccess) return fail(cuda_err(c, e, "init scalars"));
+    e = cudaStreamSynchronize(c->st);
     if (e != cudaSuccess) return fail(cuda_err(c, e, "init scalars"));
   }
   c->dx_cfl = 2 * M_PI / std::max(1, max_radius_inside(c));
   if (cfg->force_kind == TG_FORCE_ENERGY_SUPPLY) {
+    if (B != 1) return fail(set_err(c, TG_ERR_UNSUPPORTED, "forced requests are not batched"));
     c->force_on = 1;
     const double outer = cfg->force_para[1];
     c->fx = (int)std::ceil(outer / cfg->kfactor[0]);
@@ -667,6 +688,101 @@ int tg_ctx_create(const tg_config* cfg, tg_ctx** out) {
   *out = c;
   return TG_OK;
 }
+
+int validate_config(const tg_config* cfg) {
+  if (!cfg) return TG_ERR_ARG;
+  const int N1 = cfg->N[0], N2 = cfg->N[1], N3 = cfg->N[2];
+  if (N1 < 2 || N2 < 2 || N3 < 4 || (N3 & 1)) return TG_ERR_ARG;
+  if (cfg->basis != TG_FOUR && cfg->basis != TG_SCFT) return TG_ERR_ARG;
+  if (cfg->physics < TG_FLUID || cfg->physics > TG_RB) return TG_ERR_ARG;
+  if (cfg->basis == TG_SCFT && cfg->physics == TG_MHD) return TG_ERR_UNSUPPORTED;
+  if (cfg->physics == TG_RB && !(cfg->rb_ra > 0 && cfg->rb_pr > 0)) return TG_ERR_ARG;
+  if (cfg->precision != TG_FP64 && cfg->precision != TG_FP32_MIXED) return TG_ERR_ARG;
+  if (cfg->scheme != TG_RK4) return TG_ERR_UNSUPPORTED;
+  if (cfg->force_kind != TG_FORCE_DECAY && cfg->force_kind != TG_FORCE_ENERGY_SUPPLY && cfg->force_kind != TG_FORCE_RB)
+    return TG_ERR_UNSUPPORTED;
+  if (cfg->force_kind == TG_FORCE_RB && cfg->physics != TG_RB) return TG_ERR_ARG;
+  if (cfg->force_kind == TG_FORCE_ENERGY_SUPPLY && cfg->basis != TG_FOUR) return TG_ERR_UNSUPPORTED;
+  if (cfg->force_kind == TG_FORCE_ENERGY_SUPPLY && cfg->physics != TG_FLUID) return TG_ERR_UNSUPPORTED;
+  for (int i = 0; i < 3; ++i)
+    if (!(cfg->kfactor[i] > 0)) return TG_ERR_ARG;
+  if (!(cfg->dt > 0)) return TG_ERR_ARG;
+  return TG_OK;
+}
+
+void state_viscosities(const tg_config* cfg, double nu[6]) {
+  for (int i = 0; i < 6; ++i) nu[i] = 0.0;
+  for (int i = 0; i < 3; ++i) nu[i] = cfg->nu;
+  if (cfg->physics == TG_MHD) {
+    for (int i = 0; i < 3; ++i) nu[3 + i] = cfg->eta;
+  } else if (cfg->physics == TG_SCALAR) {
+    nu[3] = cfg->kappa;
+  } else if (cfg->physics == TG_RB) {
+    // PRLARGE + ULARGE (RB_slip_main.cc:236-240): nu = sqrt(Pr/Ra), kappa = 1/sqrt(Pr Ra)
+    const double v = std::sqrt(cfg->rb_pr / cfg->rb_ra), ka = 1.0 / std::sqrt(cfg->rb_pr * cfg->rb_ra);
+    for (int i = 0; i < 3; ++i) nu[i] = v;
+    nu[3] = ka;
+  }
+}
+
+int ensure_staging_ctx(tg_ctx* c) { return ensure_staging(c); }
+
+// Device bytes that ctx_create_batch(cfg, B) allocates (same sizes, same order), plus the dense
+// staging field that uploads and downloads add (with_staging).  0 for a configuration that
+// ctx_create_batch rejects on its shape.
+size_t ctx_bytes_estimate(const tg_config* cfg, int B, bool with_staging) {
+  if (!cfg || B < 1) return 0;
+  const int N1 = cfg->N[0], N2 = cfg->N[1], N3 = cfg->N[2];
+  if (N1 < 2 || N2 < 2 || N3 < 4 || (N3 & 1)) return 0;
+  const int Mz = N3 / 2;
+  int lo, hi;
+  keep_axis(N1, 0, cfg->basis, cfg->dealias, lo, hi);
+  const int nkx = amap_count(AxisMap{N1, lo, hi});
+  keep_axis(N2, 1, cfg->basis, cfg->dealias, lo, hi);
+  const int nky = amap_count(AxisMap{N2, lo, hi});
+  const int nkz = (cfg->dealias && N3 >= 3) ? N3 / 3 : N3 / 2 + 1;
+  const int kzp = (nkz + 7) / 8 * 8;
+  const size_t S = (size_t)nkx * nky * kzp;
+  const size_t tsz = cfg->precision == TG_FP64 ? sizeof(cx<double>) : sizeof(cx<float>);
+  int nstate = 3, nin = 3, nprod = 6;
+  if (cfg->physics == TG_MHD) {
+    nstate = nin = 6;
+    nprod = 9;
+  } else if (cfg->physics == TG_SCALAR || cfg->physics == TG_RB) {
+    nstate = nin = 4;
+    nprod = 9;
+  }
+  size_t b = 0;
+  std::vector<int> lens;
+  for (int L : {N1, N2, Mz, N3})
+    if (std::find(lens.begin(), lens.end(), L) == lens.end()) {
+      lens.push_back(L);
+      b += sizeof(cx<double>) * (size_t)L;
+    }
+  if (cfg->basis == TG_SCFT) b += sizeof(cx<double>) * 4 * (size_t)N1;
+  const size_t Sd1 = sizeof(cx<double>) * S;
+  const size_t WXb = tsz * (size_t)N1 * nky * kzp * B;
+  const size_t WYb = tsz * (size_t)N1 * N2 * kzp * B;
+  b += (size_t)nstate * (2 * Sd1 * B + tsz * S * B + Sd1) + Sd1;
+  b += (size_t)nin * (WXb + WYb);
+  b += (size_t)nprod * (WYb + WXb + tsz * S * B);
+  b += sizeof(double) * 8 * (size_t)reduction_blocks((long long)S) * B;
+  b += sizeof(double) * (8 + 8 + 6) * (size_t)B;
+  b += sizeof(double) * (1 << 16) + sizeof(int) * 4;
+  if (cfg->force_kind == TG_FORCE_ENERGY_SUPPLY) {
+    const double outer = cfg->force_para[1];
+    const int fx = (int)std::ceil(outer / cfg->kfactor[0]), fy = (int)std::ceil(outer / cfg->kfactor[1]),
+              fz = (int)std::ceil(outer / cfg->kfactor[2]);
+    b += sizeof(cx<double>) * 3 * (size_t)(2 * fx + 1) * (2 * fy + 1) * (fz + 1);
+  }
+  if (with_staging) b += sizeof(cx<double>) * (size_t)N1 * N2 * (N3 / 2 + 1);
+  return b;
+}
+}  // namespace tg
+
+extern "C" {
+
+int tg_ctx_create(const tg_config* cfg, tg_ctx** out) { return tg::ctx_create_batch(cfg, 1, out); }
 
 int tg_ctx_destroy(tg_ctx* c) {
   if (!c) return TG_ERR_ARG;
@@ -922,7 +1038,7 @@ int tg_step(tg_ctx* c, int n, double* energies) {
         if (!c->step_graph) {
           cudaGraph_t gr = nullptr;
           TG_CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
-          rc = enqueue_step(c);
+          rc = enqueue_step(c, true);
           cudaError_t e2 = cudaStreamEndCapture(c->st, &gr);
           if (rc) {
             if (gr) cudaGraphDestroy(gr);
@@ -935,7 +1051,7 @@ int tg_step(tg_ctx* c, int n, double* energies) {
         }
         TG_CK(cudaGraphLaunch(c->step_graph, c->st));
       } else {
-        rc = enqueue_step(c);
+        rc = enqueue_step(c, true);
         if (rc) return rc;
         c->eager_steps++;
       }

@@ -28,6 +28,11 @@ struct tg_ctx {
   int nstate = 3, nin = 3, nprod = 6;
   tg::ProdPairs pairs{};
   double nu_of[6] = {0, 0, 0, 0, 0, 0};
+  // batch of same-shape requests (serving): B slots, the first nact of them advanced by a step;
+  // slot r of every state and pipeline buffer at offset r * S (or r * stage size)
+  int B = 1;
+  int nact = 1;
+  double* nu_tab = nullptr;  // [B][6] viscosity per slot and state field
 
   // twiddle tables: length -> exp(-2 pi i m / L)
   std::map<int, tg::cx<double>*> tw;
@@ -58,9 +63,9 @@ struct tg_ctx {
   tg::cx<double>* FB = nullptr;
 
   // scalars and reductions
-  double* scal = nullptr;   // [0] dt, [1] t_now, [2] steps, [3] nonfinite
-  double* red_out = nullptr;  // [8]
-  double* part = nullptr;   // [nblocks][8]
+  double* scal = nullptr;   // per slot [8]: [0] dt, [1] t_now, [2] steps, [3] nonfinite, [4] Tdt
+  double* red_out = nullptr;  // per slot [8]
+  double* part = nullptr;   // per slot [nblocks][8]
   int npart_blocks = 0;
   double* ering = nullptr;  // energy per step of the current tg_step call
   int* ering_pos = nullptr;
@@ -130,4 +135,18 @@ int pipe_inverse_xy(tg_ctx* c, int nf, const void* const* in, const void* const*
 int pipe_products_forward(tg_ctx* c, int nin, const void* const* WY, int nprod, const ProdPairs& pp,
                           void* const* PP, void* const* PY, void* const* PX);
 int dalloc_ctx(tg_ctx* c, void** p, size_t bytes);
+// a context holding B same-shape request slots (B = 1: tg_ctx_create)
+int ctx_create_batch(const tg_config* cfg, int B, tg_ctx** out);
+size_t ctx_bytes_estimate(const tg_config* cfg, int B, bool with_staging);
+int ensure_staging_ctx(tg_ctx* c);
+// TG_OK or the code tg_ctx_create returns for cfg before allocating anything
+int validate_config(const tg_config* cfg);
+// viscosity of each state field (nu, eta, kappa; RB: from Ra and Pr)
+void state_viscosities(const tg_config* cfg, double nu[6]);
+// one fused RK4 step of the first nact slots, enqueued on c->st; ring: record slot 0's energy
+int enqueue_step(tg_ctx* c, bool ring);
+// energies of the master state of all active slots, or of slots r0 .. r0+n-1; dt_mode 2 sets
+// each slot's dt by the Get_dt rule without advancing its time
+int run_energy(tg_ctx* c, int dt_mode);
+int run_energy_slots(tg_ctx* c, int dt_mode, int r0, int n);
 }  // namespace tg

@@ -50,11 +50,11 @@ int pipe_inverse_xy(tg_ctx* c, int nf, const void* const* in, const void* const*
     l.pin = inprec;
     l.pout = c->tprec;
     l.pwork = c->tprec;
-    l.nbatch = 1;
+    l.nbatch = c->nact;
     l.nfields = nf;
-    l.a.sb = 0;
+    l.a.sb = g.S;  // request stride of the batch
     l.a.sr = (long long)g.nky * g.kzp;
-    l.a.db = 0;
+    l.a.db = (long long)c->N1 * g.nky * g.kzp;
     l.a.dr = (long long)g.nky * g.kzp;
     l.a.ncols = g.nky * g.kzp;
     l.a.in = g.ax;
@@ -86,7 +86,7 @@ int pipe_inverse_xy(tg_ctx* c, int nf, const void* const* in, const void* const*
     l.L = c->N2;
     l.dir = +1;
     l.pin = l.pout = l.pwork = c->tprec;
-    l.nbatch = c->N1;
+    l.nbatch = c->nact * c->N1;
     l.nfields = nf;
     l.a.sb = (long long)g.nky * g.kzp;
     l.a.sr = g.kzp;
@@ -118,7 +118,7 @@ int pipe_products_forward(tg_ctx* c, int nin, const void* const* WY, int nprod, 
     l.nin = nin;
     l.nprod = nprod;
     l.pin = l.pout = l.pwork = c->tprec;
-    l.a.nrows = (long long)c->N1 * c->N2;
+    l.a.nrows = (long long)c->nact * c->N1 * c->N2;
     l.a.ss = g.kzp;
     l.a.ds = g.kzp;
     l.a.nin = g.nkz;
@@ -140,7 +140,7 @@ int pipe_products_forward(tg_ctx* c, int nin, const void* const* WY, int nprod, 
     l.L = c->N2;
     l.dir = -1;
     l.pin = l.pout = l.pwork = c->tprec;
-    l.nbatch = c->N1;
+    l.nbatch = c->nact * c->N1;
     l.nfields = nprod;
     l.a.sb = (long long)c->N2 * g.kzp;
     l.a.sr = g.kzp;
@@ -164,11 +164,11 @@ int pipe_products_forward(tg_ctx* c, int nin, const void* const* WY, int nprod, 
     l.L = c->N1;
     l.dir = -1;
     l.pin = l.pout = l.pwork = c->tprec;
-    l.nbatch = 1;
+    l.nbatch = c->nact;
     l.nfields = nprod;
-    l.a.sb = 0;
+    l.a.sb = (long long)c->N1 * g.nky * g.kzp;
     l.a.sr = (long long)g.nky * g.kzp;
-    l.a.db = 0;
+    l.a.db = g.S;
     l.a.dr = (long long)g.nky * g.kzp;
     l.a.ncols = g.nky * g.kzp;
     l.a.in = full_map(c->N1);

@@ -1,37 +1,522 @@
-// Serving loop (continuous batching of independent solves): see tg_server_impl below.
+// Serving loop: continuous batching of independent solves on one GPU.
+//
+// A batch is a context created with B request slots (ctx_create_batch): every state and
+// pipeline buffer holds B copies at a fixed slot stride, and every kernel of the step takes the
+// slot as a grid dimension, so one launch per pass advances the first nact slots.  Active slots
+// are kept dense (0 .. nact-1): a request that leaves hands its slot to the last one.  A step of
+// a batch with nact active slots is one CUDA graph, captured once per (batch, nact).
+//
+// Per request, the slot carries its own viscosities (nu_tab row), dt, time, step count,
+// non-finite flag and dt ceiling (scal row); the energy reduction of each slot runs in its own
+// blocks in a fixed order.  So a request's fields after n steps are the same bits whatever else
+// shares its batch, and the same as tg_step on a lone context.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
 #include "tg_ctx.h"
+
+using namespace tg;
+
+namespace {
+
+struct Req {
+  long long id = 0;
+  tg_config cfg{};
+  int n_steps = 0;
+  int nstate = 3;
+  std::vector<double> init;    // dropped at admission
+  std::vector<double> result;  // kept when keep_results
+  tg_request_status st{};
+  std::string key;
+  long long batch = -1;        // batch id while running
+};
+
+struct Batch {
+  long long id = 0;
+  std::string key;
+  tg_ctx* c = nullptr;
+  int B = 0;
+  bool solo = false;                 // forced request: one slot, never shared
+  std::vector<long long> slot_req;   // request id of active slot r
+  std::map<int, cudaGraphExec_t> graphs;  // per active count
+  bool warmed = false;               // one eager step ran (module loading outside capture)
+  double* h = nullptr;               // pinned: scal [B][8], red_out [B][8]
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+struct tg_server {
+  tg_server_config cfg{};
+  int dev = 0;
+  std::chrono::steady_clock::time_point t0;
+  long long next_id = 1, next_batch = 1;
+  std::map<long long, Req> reqs;
+  std::vector<long long> queue;        // FIFO of queued request ids
+  std::map<long long, Batch> batches;
+  size_t bytes = 0, bytes_peak = 0;
+  long long rounds = 0, request_steps = 0, graph_launches = 0, eager_steps = 0;
+  std::string err;
+};
+
+namespace {
+
+double now_s(const tg_server* s) {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - s->t0).count();
+}
+
+int state_fields(int physics) {
+  if (physics == TG_MHD) return 6;
+  if (physics == TG_SCALAR || physics == TG_RB) return 4;
+  return 3;
+}
+
+// Requests share a batch when they agree on everything that the kernels or the geometry read
+// from the context; the per-slot coefficients (viscosities, dt) may differ.
+std::string batch_key(const tg_config& c, long long id) {
+  char buf[512];
+  std::snprintf(buf, sizeof(buf), "%d,%d,%d|b%d|p%d|x%d|d%d|s%d|k%a,%a,%a|f%d", c.N[0], c.N[1], c.N[2], c.basis,
+                c.physics, c.precision, c.dealias, c.scheme, c.kfactor[0], c.kfactor[1], c.kfactor[2],
+                c.force_kind);
+  std::string k(buf);
+  if (c.force_kind == TG_FORCE_ENERGY_SUPPLY) k += "|solo" + std::to_string(id);
+  return k;
+}
+
+void destroy_batch(tg_server* s, Batch& b) {
+  if (b.c) {
+    cudaSetDevice(b.c->dev);
+    cudaStreamSynchronize(b.c->st);
+    for (auto& kv : b.graphs) cudaGraphExecDestroy(kv.second);
+    b.graphs.clear();
+    tg_ctx_destroy(b.c);
+    b.c = nullptr;
+  }
+  if (b.h) cudaFreeHost(b.h);
+  b.h = nullptr;
+  s->bytes -= b.bytes;
+  b.bytes = 0;
+}
+
+void finish_req(tg_server* s, Req& r, int state, int error) {
+  r.st.state = state;
+  r.st.error = error;
+  r.st.finish_s = now_s(s);
+  r.batch = -1;
+  std::vector<double>().swap(r.init);
+}
+
+// copy a request's fields into slot `slot` of batch b and set the slot's coefficients, time and
+// dt (Get_dt of the initial state, compute_dt.cc:47-108)
+int load_slot(tg_server* s, Batch& b, int slot, Req& r) {
+  tg_ctx* c = b.c;
+  const size_t D2 = 2 * (size_t)c->D;
+  cudaError_t e;
+  for (int i = 0; i < c->nstate; ++i) {
+    e = cudaMemcpyAsync(c->staging, r.init.data() + (size_t)i * D2, sizeof(double) * D2, cudaMemcpyHostToDevice, c->st);
+    if (e != cudaSuccess) return cuda_err(c, e, "slot upload");
+    e = launch_dense_to_compact(c->g, c->staging, c->U0[i] + (size_t)slot * c->S, 0, c->st);
+    if (e != cudaSuccess) return cuda_err(c, e, "slot upload");
+  }
+  double nu[6];
+  state_viscosities(&r.cfg, nu);
+  double* hp = b.h;  // the pinned rows are free between rounds
+  for (int i = 0; i < 6; ++i) hp[i] = nu[i];
+  const double sc[8] = {r.cfg.dt, 0, 0, 0, r.cfg.dt, 0, 0, 0};
+  for (int i = 0; i < 8; ++i) hp[8 + i] = sc[i];
+  e = cudaMemcpyAsync(c->nu_tab + (size_t)slot * 6, hp, sizeof(double) * 6, cudaMemcpyHostToDevice, c->st);
+  if (e != cudaSuccess) return cuda_err(c, e, "slot coefficients");
+  e = cudaMemcpyAsync(c->scal + (size_t)slot * 8, hp + 8, sizeof(double) * 8, cudaMemcpyHostToDevice, c->st);
+  if (e != cudaSuccess) return cuda_err(c, e, "slot scalars");
+  int rc = run_energy_slots(c, 2, slot, 1);
+  if (rc) return rc;
+  // the pinned rows are reused by the next load: wait for the copies out of them
+  e = cudaStreamSynchronize(c->st);
+  if (e != cudaSuccess) return cuda_err(c, e, "slot load");
+  std::vector<double>().swap(r.init);
+  return TG_OK;
+}
+
+// fields of slot `slot` into r.result (reference layout)
+int store_slot(tg_server* s, Batch& b, int slot, Req& r) {
+  tg_ctx* c = b.c;
+  if (!s->cfg.keep_results) return TG_OK;
+  const size_t D2 = 2 * (size_t)c->D;
+  r.result.assign(D2 * c->nstate, 0.0);
+  for (int i = 0; i < c->nstate; ++i) {
+    cudaError_t e = launch_compact_to_dense(c->g, c->U0[i] + (size_t)slot * c->S, 0, c->staging, c->st);
+    if (e != cudaSuccess) return cuda_err(c, e, "slot download");
+    e = cudaMemcpyAsync(r.result.data() + (size_t)i * D2, c->staging, sizeof(double) * D2, cudaMemcpyDeviceToHost, c->st);
+    if (e != cudaSuccess) return cuda_err(c, e, "slot download");
+  }
+  cudaError_t e = cudaStreamSynchronize(c->st);
+  if (e != cudaSuccess) return cuda_err(c, e, "slot download");
+  return TG_OK;
+}
+
+// slot `to` takes the request in slot `from` (device copies on the batch stream)
+int move_slot(Batch& b, int from, int to) {
+  tg_ctx* c = b.c;
+  const size_t Sd = sizeof(cx<double>) * (size_t)c->S;
+  cudaError_t e;
+  for (int i = 0; i < c->nstate; ++i) {
+    e = cudaMemcpyAsync(c->U0[i] + (size_t)to * c->S, c->U0[i] + (size_t)from * c->S, Sd, cudaMemcpyDeviceToDevice, c->st);
+    if (e != cudaSuccess) return cuda_err(c, e, "slot move");
+  }
+  e = cudaMemcpyAsync(c->scal + (size_t)to * 8, c->scal + (size_t)from * 8, sizeof(double) * 8, cudaMemcpyDeviceToDevice, c->st);
+  if (e != cudaSuccess) return cuda_err(c, e, "slot move");
+  e = cudaMemcpyAsync(c->red_out + (size_t)to * 8, c->red_out + (size_t)from * 8, sizeof(double) * 8, cudaMemcpyDeviceToDevice, c->st);
+  if (e != cudaSuccess) return cuda_err(c, e, "slot move");
+  e = cudaMemcpyAsync(c->nu_tab + (size_t)to * 6, c->nu_tab + (size_t)from * 6, sizeof(double) * 6, cudaMemcpyDeviceToDevice, c->st);
+  if (e != cudaSuccess) return cuda_err(c, e, "slot move");
+  return TG_OK;
+}
+
+// a new batch for request r's key: as many slots as fit in a quarter of the budget (at least
+// one) and in what is left of it, at most max_batch
+int open_batch(tg_server* s, const Req& r, long long* bid) {
+  const bool solo = r.cfg.force_kind == TG_FORCE_ENERGY_SUPPLY;
+  const size_t budget = s->cfg.hbm_budget_bytes;
+  const size_t left = budget > s->bytes ? budget - s->bytes : 0;
+  const size_t one = ctx_bytes_estimate(&r.cfg, 1, true);
+  if (one == 0 || one > left) return TG_ERR_OOM;
+  const size_t cap = std::min(left, std::max(budget / 4, one));
+  int B = 1;
+  if (!solo) {
+    B = std::max(1, s->cfg.max_batch);
+    while (B > 1 && ctx_bytes_estimate(&r.cfg, B, true) > cap) --B;
+  }
+  tg_config cc = r.cfg;
+  cc.device = s->dev;
+  cc.stream = nullptr;
+  tg_ctx* c = nullptr;
+  int rc = ctx_create_batch(&cc, B, &c);
+  if (rc) return rc;
+  rc = ensure_staging_ctx(c);
+  if (rc) {
+    tg_ctx_destroy(c);
+    return rc;
+  }
+  Batch b;
+  b.id = s->next_batch++;
+  b.key = r.key;
+  b.c = c;
+  b.B = B;
+  b.solo = solo;
+  c->graphs = s->cfg.use_graphs != 0;
+  if (cudaMallocHost(&b.h, sizeof(double) * 16 * (size_t)std::max(B, 2)) != cudaSuccess) {
+    tg_ctx_destroy(c);
+    return TG_ERR_OOM;
+  }
+  b.bytes = c->bytes;
+  s->bytes += b.bytes;
+  s->bytes_peak = std::max(s->bytes_peak, s->bytes);
+  *bid = b.id;
+  s->batches.emplace(b.id, std::move(b));
+  return TG_OK;
+}
+
+// admit queued requests in arrival order into batches with free slots or into new batches
+int admit(tg_server* s) {
+  std::vector<long long> still;
+  for (size_t qi = 0; qi < s->queue.size(); ++qi) {
+    Req& r = s->reqs[s->queue[qi]];
+    long long bid = -1;
+    for (auto& kv : s->batches) {
+      Batch& b = kv.second;
+      if (b.key == r.key && !b.solo && (int)b.slot_req.size() < b.B) {
+        bid = kv.first;
+        break;
+      }
+    }
+    if (bid < 0) {
+      int rc = open_batch(s, r, &bid);
+      if (rc == TG_ERR_OOM) {
+        if (s->batches.empty()) {
+          // nothing resident and still no room: the allocation itself failed
+          finish_req(s, r, TG_REQ_FAILED, TG_ERR_OOM);
+        } else {
+          still.push_back(r.id);  // waits for room
+        }
+        continue;
+      }
+      if (rc) {
+        finish_req(s, r, TG_REQ_FAILED, rc);
+        continue;
+      }
+    }
+    Batch& b = s->batches[bid];
+    const int slot = (int)b.slot_req.size();
+    r.st.start_s = now_s(s);
+    int rc = load_slot(s, b, slot, r);
+    if (rc) {
+      s->err = b.c->err;
+      finish_req(s, r, TG_REQ_FAILED, rc);
+      continue;
+    }
+    r.st.state = TG_REQ_RUNNING;
+    r.batch = bid;
+    if (r.n_steps == 0) {
+      rc = store_slot(s, b, slot, r);
+      finish_req(s, r, rc ? TG_REQ_FAILED : TG_REQ_DONE, rc);
+      continue;
+    }
+    b.slot_req.push_back(r.id);
+  }
+  s->queue.swap(still);
+  return TG_OK;
+}
+
+// one step of the active slots of batch b, then the slot scalars into pinned memory
+int launch_batch(tg_server* s, Batch& b) {
+  tg_ctx* c = b.c;
+  const int nact = (int)b.slot_req.size();
+  c->nact = nact;
+  cudaError_t e;
+  if (s->cfg.use_graphs && b.warmed) {
+    auto it = b.graphs.find(nact);
+    if (it == b.graphs.end()) {
+      cudaGraph_t gr = nullptr;
+      e = cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal);
+      if (e != cudaSuccess) return cuda_err(c, e, "cudaStreamBeginCapture");
+      int rc = enqueue_step(c, false);
+      cudaError_t e2 = cudaStreamEndCapture(c->st, &gr);
+      if (rc) {
+        if (gr) cudaGraphDestroy(gr);
+        return rc;
+      }
+      if (e2 != cudaSuccess) return cuda_err(c, e2, "cudaStreamEndCapture");
+      cudaGraphExec_t ex = nullptr;
+      e = cudaGraphInstantiate(&ex, gr, 0);
+      cudaGraphDestroy(gr);
+      if (e != cudaSuccess) return cuda_err(c, e, "cudaGraphInstantiate");
+      it = b.graphs.emplace(nact, ex).first;
+    }
+    e = cudaGraphLaunch(it->second, c->st);
+    if (e != cudaSuccess) return cuda_err(c, e, "cudaGraphLaunch");
+    s->graph_launches++;
+  } else {
+    int rc = enqueue_step(c, false);
+    if (rc) return rc;
+    b.warmed = true;
+    s->eager_steps++;
+  }
+  e = cudaMemcpyAsync(b.h, c->scal, sizeof(double) * 8 * nact, cudaMemcpyDeviceToHost, c->st);
+  if (e != cudaSuccess) return cuda_err(c, e, "slot scalars");
+  e = cudaMemcpyAsync(b.h + 8 * (size_t)b.B, c->red_out, sizeof(double) * 8 * nact, cudaMemcpyDeviceToHost, c->st);
+  if (e != cudaSuccess) return cuda_err(c, e, "slot energies");
+  return TG_OK;
+}
+
+// after the step: count it, retire finished and non-finite requests, keep the slots dense
+int collect_batch(tg_server* s, Batch& b, int launch_rc) {
+  tg_ctx* c = b.c;
+  cudaError_t e = cudaStreamSynchronize(c->st);
+  const int nact = (int)b.slot_req.size();
+  if (launch_rc || e != cudaSuccess) {
+    const int code = launch_rc ? launch_rc : cuda_err(c, e, "batch step");
+    s->err = c->err;
+    for (long long id : b.slot_req) finish_req(s, s->reqs[id], TG_REQ_FAILED, code);
+    b.slot_req.clear();
+    return code;
+  }
+  std::vector<int> leave;
+  for (int r = 0; r < nact; ++r) {
+    Req& q = s->reqs[b.slot_req[r]];
+    const double* sc = b.h + 8 * (size_t)r;
+    const double* ro = b.h + 8 * (size_t)b.B + 8 * (size_t)r;
+    q.st.steps_done++;
+    s->request_steps++;
+    q.st.t_final = sc[1];
+    q.st.final_energy = ro[0] + (c->phys == TG_MHD ? ro[2] : 0.0);
+    if (sc[3] != 0.0) {
+      finish_req(s, q, TG_REQ_FAILED, TG_ERR_NONFINITE);
+      leave.push_back(r);
+    } else if (q.st.steps_done >= q.n_steps) {
+      int rc = store_slot(s, b, r, q);
+      finish_req(s, q, rc ? TG_REQ_FAILED : TG_REQ_DONE, rc);
+      leave.push_back(r);
+    }
+  }
+  // fill each hole from the end, highest hole first
+  for (auto it = leave.rbegin(); it != leave.rend(); ++it) {
+    const int hole = *it;
+    const int last = (int)b.slot_req.size() - 1;
+    if (hole != last) {
+      int rc = move_slot(b, last, hole);
+      if (rc) return rc;
+      b.slot_req[hole] = b.slot_req[last];
+    }
+    b.slot_req.pop_back();
+  }
+  return TG_OK;
+}
+
+bool key_queued(const tg_server* s, const std::string& key) {
+  for (long long id : s->queue)
+    if (s->reqs.at(id).key == key) return true;
+  return false;
+}
+
+}  // namespace
 
 extern "C" {
 
+int tg_request_bytes(const tg_config* cfg, int batch, size_t* bytes) {
+  if (!cfg || !bytes || batch < 1) return TG_ERR_ARG;
+  const int v = validate_config(cfg);
+  if (v) return v;
+  *bytes = ctx_bytes_estimate(cfg, batch, true);
+  return *bytes ? TG_OK : TG_ERR_ARG;
+}
+
 int tg_server_create(const tg_server_config* cfg, tg_server** out) {
-  (void)cfg;
-  if (out) *out = nullptr;
-  return TG_ERR_UNSUPPORTED;
+  if (!cfg || !out) return TG_ERR_ARG;
+  *out = nullptr;
+  if (cfg->hbm_budget_bytes == 0 || cfg->max_batch < 1) return TG_ERR_ARG;
+  if (cudaSetDevice(cfg->device) != cudaSuccess) return TG_ERR_CUDA;
+  tg_server* s = new tg_server();
+  s->cfg = *cfg;
+  s->dev = cfg->device;
+  s->t0 = std::chrono::steady_clock::now();
+  *out = s;
+  return TG_OK;
 }
-int tg_server_destroy(tg_server* srv) { return srv ? TG_ERR_UNSUPPORTED : TG_ERR_ARG; }
-int tg_server_submit(tg_server* srv, const tg_request* req, long long* id) {
-  (void)srv; (void)req; (void)id;
-  return TG_ERR_UNSUPPORTED;
+
+int tg_server_destroy(tg_server* s) {
+  if (!s) return TG_ERR_ARG;
+  cudaSetDevice(s->dev);
+  for (auto& kv : s->batches) destroy_batch(s, kv.second);
+  delete s;
+  return TG_OK;
 }
-int tg_server_pump(tg_server* srv, int* n_active) {
-  (void)srv; (void)n_active;
-  return TG_ERR_UNSUPPORTED;
+
+int tg_server_submit(tg_server* s, const tg_request* rq, long long* id) {
+  if (!s || !rq || !id) return TG_ERR_ARG;
+  *id = -1;
+  const int v = validate_config(&rq->cfg);
+  if (v) return v;
+  const int Mz = rq->cfg.N[2] / 2;
+  if (!(Mz >= 4 && Mz <= 256 && (Mz & (Mz - 1)) == 0)) return TG_ERR_UNSUPPORTED;
+  if (rq->n_steps < 0) return TG_ERR_ARG;
+  const int ns = state_fields(rq->cfg.physics);
+  const size_t D2 = 2 * (size_t)rq->cfg.N[0] * rq->cfg.N[1] * (rq->cfg.N[2] / 2 + 1);
+  if (!rq->init || rq->n_doubles != D2 * ns) return TG_ERR_ARG;
+  Req r;
+  r.id = s->next_id++;
+  r.cfg = rq->cfg;
+  r.n_steps = rq->n_steps;
+  r.nstate = ns;
+  r.key = batch_key(r.cfg, r.id);
+  r.st.state = TG_REQ_QUEUED;
+  r.st.submit_s = now_s(s);
+  if (ctx_bytes_estimate(&r.cfg, 1, true) > s->cfg.hbm_budget_bytes) {
+    r.st.state = TG_REQ_FAILED;
+    r.st.error = TG_ERR_OOM;
+    r.st.finish_s = r.st.submit_s;
+  } else {
+    r.init.assign(rq->init, rq->init + rq->n_doubles);
+    s->queue.push_back(r.id);
+  }
+  *id = r.id;
+  s->reqs.emplace(r.id, std::move(r));
+  return TG_OK;
 }
-int tg_server_drain(tg_server* srv, long long max_rounds) {
-  (void)srv; (void)max_rounds;
-  return TG_ERR_UNSUPPORTED;
+
+int tg_server_pump(tg_server* s, int* n_active) {
+  if (!s) return TG_ERR_ARG;
+  cudaSetDevice(s->dev);
+  int rc = admit(s);
+  if (rc) return rc;
+  std::vector<std::pair<long long, int>> launched;
+  for (auto& kv : s->batches) {
+    Batch& b = kv.second;
+    if (b.slot_req.empty()) continue;
+    launched.emplace_back(kv.first, launch_batch(s, b));
+  }
+  int first_err = TG_OK;
+  for (auto& lb : launched) {
+    const int r2 = collect_batch(s, s->batches[lb.first], lb.second);
+    if (r2 && !first_err) first_err = r2;
+  }
+  if (!launched.empty()) s->rounds++;
+  // release empty batches that no queued request will use
+  for (auto it = s->batches.begin(); it != s->batches.end();) {
+    if (it->second.slot_req.empty() && !key_queued(s, it->second.key)) {
+      destroy_batch(s, it->second);
+      it = s->batches.erase(it);
+    } else {
+      ++it;
+    }
+  }
+  if (n_active) {
+    int n = (int)s->queue.size();
+    for (auto& kv : s->batches) n += (int)kv.second.slot_req.size();
+    *n_active = n;
+  }
+  return first_err;
 }
-int tg_server_poll(tg_server* srv, long long id, tg_request_status* st) {
-  (void)srv; (void)id; (void)st;
-  return TG_ERR_UNSUPPORTED;
+
+int tg_server_drain(tg_server* s, long long max_rounds) {
+  if (!s) return TG_ERR_ARG;
+  int first_err = TG_OK;
+  for (long long i = 0; max_rounds <= 0 || i < max_rounds; ++i) {
+    int n = 0;
+    const int rc = tg_server_pump(s, &n);
+    if (rc && !first_err) first_err = rc;
+    if (n == 0) return first_err;
+  }
+  return first_err ? first_err : TG_ERR_TIMEOUT;
 }
-int tg_server_result(tg_server* srv, long long id, double* host, size_t n) {
-  (void)srv; (void)id; (void)host; (void)n;
-  return TG_ERR_UNSUPPORTED;
+
+int tg_server_poll(tg_server* s, long long id, tg_request_status* st) {
+  if (!s || !st) return TG_ERR_ARG;
+  auto it = s->reqs.find(id);
+  if (it == s->reqs.end()) return TG_ERR_ARG;
+  *st = it->second.st;
+  return TG_OK;
 }
-double tg_server_clock(tg_server* srv) {
-  (void)srv;
-  return 0.0;
+
+int tg_server_result(tg_server* s, long long id, double* host, size_t n) {
+  if (!s || !host) return TG_ERR_ARG;
+  auto it = s->reqs.find(id);
+  if (it == s->reqs.end()) return TG_ERR_ARG;
+  const Req& r = it->second;
+  if (r.st.state != TG_REQ_DONE || r.result.empty()) return TG_ERR_STATE;
+  if (n != r.result.size()) return TG_ERR_ARG;
+  std::memcpy(host, r.result.data(), sizeof(double) * n);
+  return TG_OK;
 }
+
+int tg_server_release(tg_server* s, long long id) {
+  if (!s) return TG_ERR_ARG;
+  auto it = s->reqs.find(id);
+  if (it == s->reqs.end()) return TG_ERR_ARG;
+  std::vector<double>().swap(it->second.result);
+  return TG_OK;
+}
+
+int tg_server_stats_get(tg_server* s, tg_server_stats* st) {
+  if (!s || !st) return TG_ERR_ARG;
+  std::memset(st, 0, sizeof(*st));
+  st->bytes_resident = s->bytes;
+  st->bytes_peak = s->bytes_peak;
+  st->n_batches = (int)s->batches.size();
+  for (auto& kv : s->batches) st->n_running += (int)kv.second.slot_req.size();
+  st->n_queued = (int)s->queue.size();
+  st->rounds = s->rounds;
+  st->request_steps = s->request_steps;
+  st->graph_launches = s->graph_launches;
+  st->eager_steps = s->eager_steps;
+  return TG_OK;
+}
+
+double tg_server_clock(tg_server* s) { return s ? now_s(s) : 0.0; }
 
 }  // extern "C"

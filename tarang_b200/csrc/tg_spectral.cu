@@ -178,12 +178,13 @@ __global__ void __launch_bounds__(TPB) k_rk(RKArgs a) {
     compact_mode(g, idx, r1, r2, l3);
     if (l3 < g.nkz) {
       const int kxi = geo_kx(g, r1), kyi = geo_ky(g, r2);
+      const long long gi = (long long)blockIdx.y * g.S + idx;  // request blockIdx.y of the batch
       const double kx = kxi * g.kf0, ky = kyi * g.kf1, kz = l3 * g.kf2;
       const double K2 = kx * kx + ky * ky + kz * kz;
       cx<double> r[NS];
       if constexpr (SRC == 0) {
         const XDer dx{kx, g.basis};
-        assemble<Rp, PHYS>(a.PX, idx, dx, ky, kz, r);
+        assemble<Rp, PHYS>(a.PX, gi, dx, ky, kz, r);
         if (a.FB != nullptr && kxi >= -a.fx && kxi <= a.fx && kyi >= -a.fy && kyi <= a.fy && l3 <= a.fz) {
           const int box = (2 * a.fx + 1) * (2 * a.fy + 1) * (a.fz + 1);
           const int p = ((kxi + a.fx) * (2 * a.fy + 1) + (kyi + a.fy)) * (a.fz + 1) + l3;
@@ -193,38 +194,39 @@ __global__ void __launch_bounds__(TPB) k_rk(RKArgs a) {
         if constexpr (PHYS == PH_RB) {
           // Compute_force_RB (compute_force_RB.cc:51-105) from the stage's fields, then Add_force:
           // nlin1 -= fu * theta, T.nlin -= ft * u1
-          const cx<double> th = a.inprec ? ldc<float>(a.IN[3], idx) : ldc<double>(a.IN[3], idx);
-          const cx<double> u1 = a.inprec ? ldc<float>(a.IN[0], idx) : ldc<double>(a.IN[0], idx);
+          const cx<double> th = a.inprec ? ldc<float>(a.IN[3], gi) : ldc<double>(a.IN[3], gi);
+          const cx<double> u1 = a.inprec ? ldc<float>(a.IN[0], gi) : ldc<double>(a.IN[0], gi);
           r[0] = r[0] - a.rb_buoy_u * th;
           r[3] = r[3] - a.rb_buoy_t * u1;
         }
         project_rhs(r, NS, dx, ky, kz, K2);
       } else {
 #pragma unroll
-        for (int c = 0; c < NS; ++c) r[c] = a.RHS[c][idx];
+        for (int c = 0; c < NS; ++c) r[c] = a.RHS[c][gi];
       }
-      const double dt = *a.dt;
+      const double dt = a.dt[(long long)blockIdx.y * 8];
       const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
 #pragma unroll
       for (int c = 0; c < NS; ++c) {
-        const double eh = exp(-a.nu[c] * 0.5 * dt * K2);
-        const cx<double> u0 = a.U0[c][idx];
+        const double nu_c = a.nu_tab ? a.nu_tab[blockIdx.y * 6 + c] : a.nu[c];
+        const double eh = exp(-nu_c * 0.5 * dt * K2);
+        const cx<double> u0 = a.U0[c][gi];
         const cx<double> rc = r[c];
         if (a.stage == 1) {
-          const double e1 = exp(-a.nu[c] * dt * K2);
-          stc<Rs>(a.US[c], idx, eh * (u0 + (0.5 * dt) * rc));
-          a.TOT[c][idx] = (dt / 6.0) * (e1 * rc);
+          const double e1 = exp(-nu_c * dt * K2);
+          stc<Rs>(a.US[c], gi, eh * (u0 + (0.5 * dt) * rc));
+          a.TOT[c][gi] = (dt / 6.0) * (e1 * rc);
         } else if (a.stage == 2) {
-          stc<Rs>(a.US[c], idx, eh * u0 + (0.5 * dt) * rc);
-          a.TOT[c][idx] = a.TOT[c][idx] + (dt / 3.0) * (eh * rc);
+          stc<Rs>(a.US[c], gi, eh * u0 + (0.5 * dt) * rc);
+          a.TOT[c][gi] = a.TOT[c][gi] + (dt / 3.0) * (eh * rc);
         } else if (a.stage == 3) {
-          stc<Rs>(a.US[c], idx, eh * (eh * u0 + dt * rc));
-          a.TOT[c][idx] = a.TOT[c][idx] + (dt / 3.0) * (eh * rc);
+          stc<Rs>(a.US[c], gi, eh * (eh * u0 + dt * rc));
+          a.TOT[c][gi] = a.TOT[c][gi] + (dt / 3.0) * (eh * rc);
         } else {
-          const double e1 = exp(-a.nu[c] * dt * K2);
-          const cx<double> tot = a.TOT[c][idx] + (dt / 6.0) * rc;
+          const double e1 = exp(-nu_c * dt * K2);
+          const cx<double> tot = a.TOT[c][gi] + (dt / 6.0) * rc;
           const cx<double> u = e1 * u0 + tot;
-          a.U0[c][idx] = u;
+          a.U0[c][gi] = u;
           const double m2 = u.x * u.x + u.y * u.y;
           const int grp = (PHYS == PH_MHD) ? (c / 3) * 2 : (c < 3 ? 0 : 4);
           double w, m;
@@ -246,15 +248,16 @@ __global__ void __launch_bounds__(TPB) k_rk(RKArgs a) {
     block_sum<6>(acc);
     if (threadIdx.x == 0) {
 #pragma unroll
-      for (int j = 0; j < 6; ++j) a.part[(long long)blockIdx.x * 8 + j] = acc[j];
+      for (int j = 0; j < 6; ++j) a.part[((long long)blockIdx.y * gridDim.x + blockIdx.x) * 8 + j] = acc[j];
     }
   }
 }
 
 template <typename Rp, typename Rs, int PHYS>
 cudaError_t run_rk_src(const RKArgs& a, int src, cudaStream_t s, int nblk) {
-  if (src == 0) k_rk<Rp, Rs, PHYS, 0><<<nblk, TPB, 0, s>>>(a);
-  else k_rk<Rp, Rs, PHYS, 1><<<nblk, TPB, 0, s>>>(a);
+  const dim3 grid(nblk, a.nact > 0 ? a.nact : 1);
+  if (src == 0) k_rk<Rp, Rs, PHYS, 0><<<grid, TPB, 0, s>>>(a);
+  else k_rk<Rp, Rs, PHYS, 1><<<grid, TPB, 0, s>>>(a);
   return cudaGetLastError();
 }
 template <typename Rp, typename Rs>
@@ -489,7 +492,7 @@ __global__ void __launch_bounds__(TPB) k_energy_partials(Geo g, PtrArr6 pa, int 
         w = (l1 == 0 && l2 == 0 && l3 == 0) ? m - 0.5 : m;
       }
       for (int c = 0; c < nf; ++c) {
-        const cx<double> u = pa.p[c][idx];
+        const cx<double> u = pa.p[c][(long long)blockIdx.y * g.S + idx];
         const double m2 = u.x * u.x + u.y * u.y;
         acc[0] += w * m2;
         acc[1] += m * K2 * m2;
@@ -498,54 +501,54 @@ __global__ void __launch_bounds__(TPB) k_energy_partials(Geo g, PtrArr6 pa, int 
   }
   block_sum<2>(acc);
   if (threadIdx.x == 0) {
-    part[(long long)blockIdx.x * nslots + slot] = acc[0];
-    part[(long long)blockIdx.x * nslots + slot + 1] = acc[1];
+    const long long b = (long long)blockIdx.y * gridDim.x + blockIdx.x;
+    part[b * nslots + slot] = acc[0];
+    part[b * nslots + slot + 1] = acc[1];
   }
 }
 
+// one block per request r: sums its partials in a fixed order, then the dt rule of Get_dt
+// (compute_dt.cc:47-108); scal[8 r + 0..4] = dt, t, steps, non-finite flag, Tdt
 __global__ void __launch_bounds__(TPB) k_finalize(FinalizeArgs a) {
   __shared__ double red[TPB];
+  const int r = blockIdx.x;
+  const double* part = a.part + (long long)r * a.nblocks * a.nslots;
+  double* out = a.out + (long long)r * a.nslots;
+  double* scal = a.scal + (long long)r * 8;
   for (int j = 0; j < a.nslots; ++j) {
     double s = 0;
-    for (int b = threadIdx.x; b < a.nblocks; b += TPB) s += a.part[(long long)b * a.nslots + j];
+    for (int b = threadIdx.x; b < a.nblocks; b += TPB) s += part[(long long)b * a.nslots + j];
     red[threadIdx.x] = s;
     __syncthreads();
     for (int o = TPB / 2; o > 0; o >>= 1) {
       if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
       __syncthreads();
     }
-    if (threadIdx.x == 0) a.out[j] = red[0];
+    if (threadIdx.x == 0) out[j] = red[0];
     __syncthreads();
   }
-  if (threadIdx.x == 0 && a.dt_mode == 1) {
-    // time advanced by the step that just ended, then Get_dt for the next step
-    a.scal[1] += a.scal[0];
-    a.scal[2] += 1.0;
-    double E = a.out[0] + (a.mhd ? a.out[2] : 0.0);
-    if (!(E == E) || E > 1e300 || E < -1e300) a.scal[3] = 1.0;
-    if (a.ering != nullptr) {
+  if (threadIdx.x != 0 || a.dt_mode == 0) return;
+  const double Tdt = scal[4] > 0 ? scal[4] : a.Tdt;
+  const double E = out[0] + (a.mhd ? out[2] : 0.0);
+  if (a.dt_mode == 1) {
+    // the step that just ended advanced the time by dt
+    scal[1] += scal[0];
+    scal[2] += 1.0;
+    if (!(E == E) || E > 1e300 || E < -1e300) scal[3] = 1.0;
+    if (a.ering != nullptr && r == 0) {
       const int pos = *a.ering_pos;
       a.ering[pos] = E;
       *a.ering_pos = pos + 1;
     }
-    double dt = (E > 0) ? a.dx / (sqrt(E) * 20.0) : a.Tdt;
-    if (a.mhd && a.B0[0] != nullptr) {
-      const double b0 = a.B0[0][0].x, b1 = a.B0[1][0].x, b2 = a.B0[2][0].x;
-      const double B0sqr = b0 * b0 + b1 * b1 + b2 * b2;
-      if (B0sqr > 1e-15) dt = fmin(dt, a.dx / (sqrt(B0sqr) * 20.0));
-    }
-    a.scal[0] = fmin(dt, a.Tdt);
-  } else if (threadIdx.x == 0 && a.dt_mode == 2) {
-    // Get_dt only (no time advance)
-    double E = a.out[0] + (a.mhd ? a.out[2] : 0.0);
-    double dt = (E > 0) ? a.dx / (sqrt(E) * 20.0) : a.Tdt;
-    if (a.mhd && a.B0[0] != nullptr) {
-      const double b0 = a.B0[0][0].x, b1 = a.B0[1][0].x, b2 = a.B0[2][0].x;
-      const double B0sqr = b0 * b0 + b1 * b1 + b2 * b2;
-      if (B0sqr > 1e-15) dt = fmin(dt, a.dx / (sqrt(B0sqr) * 20.0));
-    }
-    a.scal[0] = fmin(dt, a.Tdt);
   }
+  double dt = (E > 0) ? a.dx / (sqrt(E) * 20.0) : Tdt;
+  if (a.mhd && a.B0[0] != nullptr) {
+    const long long o = (long long)r * a.S;
+    const double b0 = a.B0[0][o].x, b1 = a.B0[1][o].x, b2 = a.B0[2][o].x;
+    const double B0sqr = b0 * b0 + b1 * b1 + b2 * b2;
+    if (B0sqr > 1e-15) dt = fmin(dt, a.dx / (sqrt(B0sqr) * 20.0));
+  }
+  scal[0] = fmin(dt, Tdt);
 }
 
 __global__ void __launch_bounds__(TPB) k_shell_spectrum(Geo g, PtrArr6 pa, int nf, double n_pow, double* ek, double* cnt, int nbins) {
@@ -672,17 +675,17 @@ cudaError_t launch_cross_partials(const Geo& g, const cx<double>* A, const cx<do
   return cudaGetLastError();
 }
 
-cudaError_t launch_energy_partials(const Geo& g, const cx<double>* const* F, int nf, double* part, int slot, int nslots, cudaStream_t s, int* nblocks) {
+cudaError_t launch_energy_partials(const Geo& g, const cx<double>* const* F, int nf, double* part, int slot, int nslots, cudaStream_t s, int* nblocks, int nact) {
   PtrArr6 pa{};
   for (int c = 0; c < nf; ++c) pa.p[c] = const_cast<cx<double>*>(F[c]);
   const int nb = nred(g.S);
   if (nblocks) *nblocks = nb;
-  k_energy_partials<<<nb, TPB, 0, s>>>(g, pa, nf, part, slot, nslots);
+  k_energy_partials<<<dim3(nb, nact > 0 ? nact : 1), TPB, 0, s>>>(g, pa, nf, part, slot, nslots);
   return cudaGetLastError();
 }
 
 cudaError_t launch_finalize(const FinalizeArgs& a, cudaStream_t s) {
-  k_finalize<<<1, TPB, 0, s>>>(a);
+  k_finalize<<<a.nact > 0 ? a.nact : 1, TPB, 0, s>>>(a);
   return cudaGetLastError();
 }
 

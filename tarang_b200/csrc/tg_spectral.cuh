@@ -75,6 +75,10 @@ struct RKArgs {
   double rb_buoy_u, rb_buoy_t;  // RB forces: Force1 = rb_buoy_u * theta, T.Force = rb_buoy_t * u1
   const void* IN[6];       // the stage's input fields (the forces are computed from them)
   int inprec;              // 0 FP64, 1 FP32
+  // batch: requests 0..nact-1 of the same shape, request r's fields at offset r * S, its
+  // viscosities at nu_tab[6 r], its scalars (dt, ...) at dt[8 r], its partials in part[r]
+  int nact;
+  const double* nu_tab;
 };
 
 struct ForceArgs {
@@ -101,7 +105,7 @@ cudaError_t launch_rb_sub_force(const Geo& g, cx<double>* const* NL, const cx<do
 cudaError_t launch_cross_partials(const Geo& g, const cx<double>* A, const cx<double>* B, double* part, int slot,
                                   int nslots, cudaStream_t s, int* nblocks);
 // energy partials of a group of fields (FP64 compact), per block: [E, D]
-cudaError_t launch_energy_partials(const Geo& g, const cx<double>* const* F, int nf, double* part, int slot, int nslots, cudaStream_t s, int* nblocks);
+cudaError_t launch_energy_partials(const Geo& g, const cx<double>* const* F, int nf, double* part, int slot, int nslots, cudaStream_t s, int* nblocks, int nact = 1);
 // reduce partials [nblocks][nslots] -> out[nslots] in fixed order; then the dt rule
 struct FinalizeArgs {
   const double* part;
@@ -114,6 +118,8 @@ struct FinalizeArgs {
   double dx, Tdt;
   int mhd;                 // add slot 2 (B energy) to the CFL energy
   const cx<double>* B0[3]; // mean magnetic field (mode 0) for MHD, or null
+  int nact;                // requests of the batch (one block each)
+  long long S;             // compact elements per request field
 };
 cudaError_t launch_finalize(const FinalizeArgs& a, cudaStream_t s);
 // shell spectrum: ek[c][bin] += mult K^n |A|^2, counts

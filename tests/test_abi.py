@@ -48,3 +48,42 @@ def test_config_default_without_gpu(lib):
     lib.tg_config_default(ctypes.byref(cfg))
     assert list(cfg.N) == [64, 64, 64] and cfg.scheme == 4 and cfg.dealias == 1
     assert ctypes.sizeof(_lib.tg_config) == 168
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """The ctypes mirrors have the sizes and field offsets that a C compiler gives the header."""
+    from tarang_b200 import _lib
+    structs = [_lib.tg_config, _lib.tg_server_config, _lib.tg_request, _lib.tg_request_status,
+               _lib.tg_server_stats, _lib.tg_kernel_stat]
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "tarang_gpu.h"', 'int main(void) {']
+    for s in structs:
+        n = s.__name__
+        lines.append(f'  printf("{n} %zu\\n", sizeof({n}));')
+        for f, _ in s._fields_:
+            lines.append(f'  printf("{n}.{f} %zu\\n", offsetof({n}, {f}));')
+    lines += ['  return 0;', '}']
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines())
+    for s in structs:
+        n = s.__name__
+        assert int(got[n]) == ctypes.sizeof(s), n
+        for f, _ in s._fields_:
+            assert int(got[f"{n}.{f}"]) == getattr(s, f).offset, f"{n}.{f}"
+
+
+def test_request_bytes_without_gpu(lib):
+    """tg_request_bytes is host arithmetic: affine in the batch size, errors for bad configs."""
+    from tarang_b200 import _lib
+    from tarang_b200.serving import request_bytes
+    cfg = dict(N=(64, 64, 64))
+    b1, b2, b3 = (request_bytes(cfg, b) for b in (1, 2, 3))
+    assert b3 - b2 == b2 - b1 > 0
+    assert request_bytes(dict(N=(64, 64, 64), precision="FP32"), 1) < b1
+    try:
+        request_bytes(dict(N=(64, 64, 64), dt=-1.0))
+        raise AssertionError("negative dt accepted")
+    except _lib.TarangError as e:
+        assert e.code == _lib.TG_ERR_ARG
