@@ -43,6 +43,11 @@ def parse():
     p.add_argument("--err-steps", type=int, default=100)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--serve-requests", type=int, default=512,
+                   help="requests of the serving ensemble (0: skip it)")
+    p.add_argument("--serve-steps", type=int, default=200)
+    p.add_argument("--serve-rate", type=float, default=200.0, help="mean arrivals per second")
+    p.add_argument("--serve-budget", type=float, default=150e9)
     return p.parse_args()
 
 
@@ -315,12 +320,178 @@ def run_own(args, rank, world, local):
     }
     if e2e:
         line["e2e"] = e2e
+    if args.serve_requests > 0:
+        s64.close()
+        s32.close()
+        line["serving"] = run_serving(args)
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(n)
     print(json.dumps(line), flush=True)
     if dist:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
+
+
+# --------------------------------------------------------------------------------- serving
+KF_RB = (math.pi, math.pi / math.sqrt(2.0), math.pi / math.sqrt(2.0))
+SERVE_TYPES = [  # name, configuration, initial condition kind
+    ("fluid32", dict(N=(32, 32, 32)), "fluid"),
+    ("fluid64", dict(N=(64, 64, 64)), "fluid"),
+    ("fluid128", dict(N=(128, 128, 128)), "fluid"),
+    ("mhd64", dict(N=(64, 64, 64), physics="MHD"), "mhd"),
+    ("rb65x128x128", dict(N=(65, 128, 128), basis="SCFT", physics="RB", kfactor=KF_RB), "rb"),
+]
+
+
+def serve_ic(kind, N, seed):
+    """Packed initial fields (n_fields, N1, N2, N3/2+1): random-phase k^4 exp(-2 (k/k0)^2)
+    velocity (k0 = 4, E = 0.5); MHD adds a magnetic field of the same shape (k0 = 3, E_u = E_b =
+    0.5); convection starts from rest with a temperature perturbation in the lowest 8 modes."""
+    import numpy as np
+    from tarang_b200 import ic
+    if kind == "fluid":
+        f = ic.random_phase_field(N, k0=4.0, energy=0.5, seed=seed)
+    elif kind == "mhd":
+        f = ic.random_phase_field(N, k0=3.0, energy=0.5, seed=seed) + \
+            ic.random_phase_field(N, k0=3.0, energy=0.5, seed=seed + 1)
+    else:
+        shape = (N[0], N[1], N[2] // 2 + 1)
+        f = [np.zeros(shape, dtype=np.complex128) for _ in range(3)] + [ic.rb_perturbation(N, seed=seed)]
+    return np.ascontiguousarray(np.stack(f))
+
+
+def serve_request_config(base, nu, dt_fluid=DT, dt_rb=1e-4):
+    c = dict(base, precision="FP32")
+    if c.get("physics") == "RB":
+        c.update(Ra=1.0 / (nu * nu), Pr=1.0, dt=dt_rb)     # nu = sqrt(Pr/Ra)
+    elif c.get("physics") == "MHD":
+        c.update(nu=nu, eta=nu, dt=dt_fluid)
+    else:
+        c.update(nu=nu, dt=dt_fluid)
+    return c
+
+
+def lone_run(cfg, init, steps):
+    """One request as a lone context: create, upload, `steps` RK4 steps, download, destroy."""
+    from tarang_b200.solver import IncFluid
+    c = dict(cfg)
+    N = c.pop("N")
+    s = IncFluid(N, **c)
+    s.set_V(init[:3])
+    if init.shape[0] == 6:
+        s.set_W(init[3:])
+    elif init.shape[0] == 4:
+        s.set_T(init[3])
+    s.step(steps, energies=False)
+    out = s.get_V()
+    if init.shape[0] == 6:
+        out += s.get_W()
+    elif init.shape[0] == 4:
+        out.append(s.get_T())
+    s.close()
+    return out
+
+
+def run_serving(args):
+    """A seeded Poisson stream of independent solves (sizes and physics drawn uniformly from
+    SERVE_TYPES, viscosity log-uniform in [1e-3, 1e-2], FP32-mixed) through tg_server, against
+    the same requests solved one after another on lone contexts."""
+    import numpy as np
+    from tarang_b200.serving import Server, request_bytes
+    n_req, steps = args.serve_requests, args.serve_steps
+    rng = np.random.Generator(np.random.PCG64(20261203))
+    kinds = rng.integers(0, len(SERVE_TYPES), n_req)
+    nus = np.exp(rng.uniform(math.log(1e-3), math.log(1e-2), n_req))
+    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, n_req))
+    pool = {}
+    for t, (name, base, kind) in enumerate(SERVE_TYPES):
+        pool[t] = [serve_ic(kind, base["N"], 7000 + 10 * t + j) for j in range(2)]
+    reqs = [(int(k), serve_request_config(SERVE_TYPES[k][1], float(nu)), pool[int(k)][i % 2])
+            for i, (k, nu) in enumerate(zip(kinds, nus))]
+    # sequential baseline: per type, the same solve on a lone context, timed end to end
+    seq_s = {}
+    lone_run(reqs[0][1], reqs[0][2], 2)          # module load and first-launch costs
+    for t in range(len(SERVE_TYPES)):
+        idx = [i for i in range(n_req) if reqs[i][0] == t][:2]
+        if not idx:
+            continue
+        el = []
+        for i in idx:
+            t0 = time.perf_counter()
+            lone_run(reqs[i][1], reqs[i][2], steps)
+            el.append(time.perf_counter() - t0)
+        seq_s[t] = statistics.mean(el)
+    err_ids = {}
+    for t in range(len(SERVE_TYPES)):
+        idx = [i for i in range(n_req) if reqs[i][0] == t]
+        if idx:
+            err_ids[idx[0]] = t
+    srv = Server(hbm_budget=args.serve_budget, max_batch=64, keep_results=True)
+    ids, fin, results, round_ms = {}, {}, {}, []
+    t_base = srv.clock()
+    sub = 0
+    active = 0
+    while True:
+        now = srv.clock() - t_base
+        while sub < n_req and arrivals[sub] <= now:
+            k, cfg, init = reqs[sub]
+            ids[srv.submit(cfg, init, steps)] = sub
+            sub += 1
+        if sub < n_req and active == 0 and arrivals[sub] > now:
+            time.sleep(min(arrivals[sub] - now, 0.05))
+            active = 1
+            continue
+        r0 = time.perf_counter()
+        active = srv.pump()
+        round_ms.append(1e3 * (time.perf_counter() - r0))
+        for rid in srv.take_finished():
+            i = ids[rid]
+            fin[i] = srv.poll(rid)
+            if i in err_ids and fin[i]["state"] == "done":
+                results[i] = srv.result(rid)
+            srv.release(rid)
+        if sub == n_req and active == 0:
+            break
+    st = srv.stats()
+    srv.close()
+    failed = [i for i, f in fin.items() if f["state"] != "done"]
+    comp = np.array([fin[i]["finish_s"] - t_base - arrivals[i] for i in fin if fin[i]["state"] == "done"])
+    per_step = np.array([(fin[i]["finish_s"] - fin[i]["start_s"]) / steps for i in fin if fin[i]["state"] == "done"])
+    makespan = max(f["finish_s"] for f in fin.values()) - t_base - arrivals[0]
+    total_steps = n_req * steps
+    seq_total = sum(seq_s[k] for k, _, _ in reqs)
+    points = sum(float(np.prod(cfg["N"])) for _, cfg, _ in reqs) * steps
+    # FP32-mixed error of one served request per type against its FP64 lone solve
+    errs = {}
+    for i, t in err_ids.items():
+        if i not in results:
+            continue
+        c64 = dict(reqs[i][1], precision="FP64")
+        ref = lone_run(c64, reqs[i][2], steps)
+        errs[SERVE_TYPES[t][0]] = rel_l2(results[i], ref)
+    return {
+        "workload": f"{n_req} requests, Poisson {args.serve_rate:g}/s, {steps} RK4 steps each, FP32-mixed; "
+                    "types uniform over " + ", ".join(n for n, _, _ in SERVE_TYPES) +
+                    "; nu log-uniform [1e-3, 1e-2] (convection: Ra = Pr/nu^2, Pr = 1)",
+        "hbm_budget_bytes": args.serve_budget, "max_batch": 64,
+        "requests_done": len(fin) - len(failed), "requests_failed": len(failed),
+        "aggregate_request_steps_per_s": total_steps / makespan,
+        "aggregate_grid_point_steps_per_s": points / makespan,
+        "makespan_s": makespan,
+        "completion_latency_s": {"p50": float(np.percentile(comp, 50)), "p99": float(np.percentile(comp, 99)),
+                                 "max": float(comp.max())},
+        "step_latency_ms": {"p50": 1e3 * float(np.percentile(per_step, 50)),
+                            "p99": 1e3 * float(np.percentile(per_step, 99))},
+        "round_ms": {"p50": float(np.percentile(round_ms, 50)), "p99": float(np.percentile(round_ms, 99)),
+                     "rounds": len(round_ms)},
+        "sequential": {"request_steps_per_s": total_steps / seq_total, "est_total_s": seq_total,
+                       "per_request_s": {SERVE_TYPES[t][0]: v for t, v in seq_s.items()},
+                       "method": "each type's solve timed alone on a lone context (create, upload, steps, download), x its count"},
+        "speedup_vs_sequential": (total_steps / makespan) / (total_steps / seq_total),
+        "rel_l2_err_vs_fp64": errs,
+        "bytes_peak": st["bytes_peak"], "graph_launches": st["graph_launches"], "eager_steps": st["eager_steps"],
+        "request_bytes": {n: request_bytes(serve_request_config(b, 1e-3)) for n, b, _ in SERVE_TYPES},
+    }
 
 
 def cpu_baseline(n):

@@ -293,6 +293,9 @@ int tg_server_poll(tg_server* srv, long long id, tg_request_status* st);
 int tg_server_result(tg_server* srv, long long id, double* host, size_t n_doubles);
 /* drop a finished request's kept fields */
 int tg_server_release(tg_server* srv, long long id);
+/* ids of requests that finished (done or failed) since the last call, oldest first: up to max
+ * of them into ids, *n = how many were written */
+int tg_server_take_finished(tg_server* srv, long long* ids, int max, int* n);
 int tg_server_stats_get(tg_server* srv, tg_server_stats* st);
 double tg_server_clock(tg_server* srv);
 

@@ -169,6 +169,7 @@ SIGNATURES = {
     "tg_server_poll": (C.c_int, [_VP, C.c_longlong, C.POINTER(tg_request_status)]),
     "tg_server_result": (C.c_int, [_VP, C.c_longlong, _DP, C.c_size_t]),
     "tg_server_release": (C.c_int, [_VP, C.c_longlong]),
+    "tg_server_take_finished": (C.c_int, [_VP, C.POINTER(C.c_longlong), C.c_int, C.POINTER(C.c_int)]),
     "tg_server_stats_get": (C.c_int, [_VP, C.POINTER(tg_server_stats)]),
     "tg_server_clock": (C.c_double, [_VP]),
     "tg_request_bytes": (C.c_int, [C.POINTER(tg_config), C.c_int, C.POINTER(C.c_size_t)]),

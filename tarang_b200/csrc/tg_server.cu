@@ -31,7 +31,8 @@ struct Req {
   int n_steps = 0;
   int nstate = 3;
   std::vector<double> init;    // dropped at admission
-  std::vector<double> result;  // kept when keep_results
+  double* result = nullptr;    // pinned block of the pool, kept when keep_results
+  size_t n_result = 0;
   tg_request_status st{};
   std::string key;
   long long batch = -1;        // batch id while running
@@ -46,8 +47,40 @@ struct Batch {
   std::vector<long long> slot_req;   // request id of active slot r
   std::map<int, cudaGraphExec_t> graphs;  // per active count
   bool warmed = false;               // one eager step ran (module loading outside capture)
-  double* h = nullptr;               // pinned: scal [B][8], red_out [B][8]
+  double* h = nullptr;               // pinned: scal [B][8], red_out [B][8], load rows [B][16]
+  std::vector<std::pair<double*, size_t>> loading;  // pinned init blocks of loads in flight
   size_t bytes = 0;
+};
+
+// Page-locked host blocks, reused by size: initial fields on their way to the device and
+// finished fields on their way back, so that neither copy waits for the batch's stream.
+struct PinnedPool {
+  std::map<size_t, std::vector<double*>> free_;
+  size_t held = 0;
+  double* get(size_t n) {
+    auto it = free_.find(n);
+    if (it != free_.end() && !it->second.empty()) {
+      double* p = it->second.back();
+      it->second.pop_back();
+      return p;
+    }
+    void* p = nullptr;
+    if (cudaMallocHost(&p, sizeof(double) * n) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    held += sizeof(double) * n;
+    return (double*)p;
+  }
+  void put(double* p, size_t n) {
+    if (p) free_[n].push_back(p);
+  }
+  void clear() {
+    for (auto& kv : free_)
+      for (double* p : kv.second) cudaFreeHost(p);
+    free_.clear();
+    held = 0;
+  }
 };
 
 }  // namespace
@@ -59,7 +92,9 @@ struct tg_server {
   long long next_id = 1, next_batch = 1;
   std::map<long long, Req> reqs;
   std::vector<long long> queue;        // FIFO of queued request ids
+  std::vector<long long> finished;     // finished since the last tg_server_take_finished
   std::map<long long, Batch> batches;
+  PinnedPool pinned;
   size_t bytes = 0, bytes_peak = 0;
   long long rounds = 0, request_steps = 0, graph_launches = 0, eager_steps = 0;
   std::string err;
@@ -98,6 +133,8 @@ void destroy_batch(tg_server* s, Batch& b) {
     tg_ctx_destroy(b.c);
     b.c = nullptr;
   }
+  for (auto& blk : b.loading) s->pinned.put(blk.first, blk.second);
+  b.loading.clear();
   if (b.h) cudaFreeHost(b.h);
   b.h = nullptr;
   s->bytes -= b.bytes;
@@ -105,6 +142,7 @@ void destroy_batch(tg_server* s, Batch& b) {
 }
 
 void finish_req(tg_server* s, Req& r, int state, int error) {
+  s->finished.push_back(r.id);
   r.st.state = state;
   r.st.error = error;
   r.st.finish_s = now_s(s);
@@ -112,51 +150,63 @@ void finish_req(tg_server* s, Req& r, int state, int error) {
   std::vector<double>().swap(r.init);
 }
 
-// copy a request's fields into slot `slot` of batch b and set the slot's coefficients, time and
-// dt (Get_dt of the initial state, compute_dt.cc:47-108)
+// Enqueue, on the batch stream, the copy of a request's fields into slot `slot` and the set-up
+// of the slot's coefficients, time and dt (Get_dt of the initial state, compute_dt.cc:47-108).
+// The host only copies into a pinned block; the stream runs the rest after the batch's step.
 int load_slot(tg_server* s, Batch& b, int slot, Req& r) {
   tg_ctx* c = b.c;
   const size_t D2 = 2 * (size_t)c->D;
+  const size_t n = D2 * c->nstate;
+  double* pin = s->pinned.get(n);
+  if (!pin) return set_err(c, TG_ERR_OOM, "pinned host block for a request's fields");
+  std::memcpy(pin, r.init.data(), sizeof(double) * n);
+  b.loading.emplace_back(pin, n);
+  std::vector<double>().swap(r.init);
   cudaError_t e;
   for (int i = 0; i < c->nstate; ++i) {
-    e = cudaMemcpyAsync(c->staging, r.init.data() + (size_t)i * D2, sizeof(double) * D2, cudaMemcpyHostToDevice, c->st);
+    e = cudaMemcpyAsync(c->staging, pin + (size_t)i * D2, sizeof(double) * D2, cudaMemcpyHostToDevice, c->st);
     if (e != cudaSuccess) return cuda_err(c, e, "slot upload");
     e = launch_dense_to_compact(c->g, c->staging, c->U0[i] + (size_t)slot * c->S, 0, c->st);
     if (e != cudaSuccess) return cuda_err(c, e, "slot upload");
   }
   double nu[6];
   state_viscosities(&r.cfg, nu);
-  double* hp = b.h;  // the pinned rows are free between rounds
-  for (int i = 0; i < 6; ++i) hp[i] = nu[i];
+  double* row = b.h + 16 * (size_t)b.B + 16 * (size_t)slot;  // this slot's load row
+  for (int i = 0; i < 6; ++i) row[i] = nu[i];
   const double sc[8] = {r.cfg.dt, 0, 0, 0, r.cfg.dt, 0, 0, 0};
-  for (int i = 0; i < 8; ++i) hp[8 + i] = sc[i];
-  e = cudaMemcpyAsync(c->nu_tab + (size_t)slot * 6, hp, sizeof(double) * 6, cudaMemcpyHostToDevice, c->st);
+  for (int i = 0; i < 8; ++i) row[8 + i] = sc[i];
+  e = cudaMemcpyAsync(c->nu_tab + (size_t)slot * 6, row, sizeof(double) * 6, cudaMemcpyHostToDevice, c->st);
   if (e != cudaSuccess) return cuda_err(c, e, "slot coefficients");
-  e = cudaMemcpyAsync(c->scal + (size_t)slot * 8, hp + 8, sizeof(double) * 8, cudaMemcpyHostToDevice, c->st);
+  e = cudaMemcpyAsync(c->scal + (size_t)slot * 8, row + 8, sizeof(double) * 8, cudaMemcpyHostToDevice, c->st);
   if (e != cudaSuccess) return cuda_err(c, e, "slot scalars");
-  int rc = run_energy_slots(c, 2, slot, 1);
-  if (rc) return rc;
-  // the pinned rows are reused by the next load: wait for the copies out of them
-  e = cudaStreamSynchronize(c->st);
-  if (e != cudaSuccess) return cuda_err(c, e, "slot load");
-  std::vector<double>().swap(r.init);
-  return TG_OK;
+  return run_energy_slots(c, 2, slot, 1);
 }
 
-// fields of slot `slot` into r.result (reference layout)
+// fields of slot `slot` into a pinned block held by the request (reference layout); the batch
+// stream is idle when this runs, so the wait covers these copies only
 int store_slot(tg_server* s, Batch& b, int slot, Req& r) {
   tg_ctx* c = b.c;
   if (!s->cfg.keep_results) return TG_OK;
   const size_t D2 = 2 * (size_t)c->D;
-  r.result.assign(D2 * c->nstate, 0.0);
+  const size_t n = D2 * c->nstate;
+  double* pin = s->pinned.get(n);
+  if (!pin) return set_err(c, TG_ERR_OOM, "pinned host block for a result");
   for (int i = 0; i < c->nstate; ++i) {
     cudaError_t e = launch_compact_to_dense(c->g, c->U0[i] + (size_t)slot * c->S, 0, c->staging, c->st);
-    if (e != cudaSuccess) return cuda_err(c, e, "slot download");
-    e = cudaMemcpyAsync(r.result.data() + (size_t)i * D2, c->staging, sizeof(double) * D2, cudaMemcpyDeviceToHost, c->st);
-    if (e != cudaSuccess) return cuda_err(c, e, "slot download");
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(pin + (size_t)i * D2, c->staging, sizeof(double) * D2, cudaMemcpyDeviceToHost, c->st);
+    if (e != cudaSuccess) {
+      s->pinned.put(pin, n);
+      return cuda_err(c, e, "slot download");
+    }
   }
   cudaError_t e = cudaStreamSynchronize(c->st);
-  if (e != cudaSuccess) return cuda_err(c, e, "slot download");
+  if (e != cudaSuccess) {
+    s->pinned.put(pin, n);
+    return cuda_err(c, e, "slot download");
+  }
+  r.result = pin;
+  r.n_result = n;
   return TG_OK;
 }
 
@@ -210,7 +260,7 @@ int open_batch(tg_server* s, const Req& r, long long* bid) {
   b.B = B;
   b.solo = solo;
   c->graphs = s->cfg.use_graphs != 0;
-  if (cudaMallocHost(&b.h, sizeof(double) * 16 * (size_t)std::max(B, 2)) != cudaSuccess) {
+  if (cudaMallocHost(&b.h, sizeof(double) * 32 * (size_t)B) != cudaSuccess) {
     tg_ctx_destroy(c);
     return TG_ERR_OOM;
   }
@@ -262,12 +312,7 @@ int admit(tg_server* s) {
     }
     r.st.state = TG_REQ_RUNNING;
     r.batch = bid;
-    if (r.n_steps == 0) {
-      rc = store_slot(s, b, slot, r);
-      finish_req(s, r, rc ? TG_REQ_FAILED : TG_REQ_DONE, rc);
-      continue;
-    }
-    b.slot_req.push_back(r.id);
+    b.slot_req.push_back(r.id);  // a request of 0 steps leaves at the collect that follows
   }
   s->queue.swap(still);
   return TG_OK;
@@ -314,11 +359,13 @@ int launch_batch(tg_server* s, Batch& b) {
   return TG_OK;
 }
 
-// after the step: count it, retire finished and non-finite requests, keep the slots dense
-int collect_batch(tg_server* s, Batch& b, int launch_rc) {
+// after the round: count the step of the first nl slots (those that were launched), retire
+// finished and non-finite requests, keep the slots dense
+int collect_batch(tg_server* s, Batch& b, int nl, int launch_rc) {
   tg_ctx* c = b.c;
   cudaError_t e = cudaStreamSynchronize(c->st);
-  const int nact = (int)b.slot_req.size();
+  for (auto& blk : b.loading) s->pinned.put(blk.first, blk.second);
+  b.loading.clear();
   if (launch_rc || e != cudaSuccess) {
     const int code = launch_rc ? launch_rc : cuda_err(c, e, "batch step");
     s->err = c->err;
@@ -327,19 +374,24 @@ int collect_batch(tg_server* s, Batch& b, int launch_rc) {
     return code;
   }
   std::vector<int> leave;
-  for (int r = 0; r < nact; ++r) {
+  const int n = (int)b.slot_req.size();
+  for (int r = 0; r < n; ++r) {
     Req& q = s->reqs[b.slot_req[r]];
-    const double* sc = b.h + 8 * (size_t)r;
-    const double* ro = b.h + 8 * (size_t)b.B + 8 * (size_t)r;
-    q.st.steps_done++;
-    s->request_steps++;
-    q.st.t_final = sc[1];
-    q.st.final_energy = ro[0] + (c->phys == TG_MHD ? ro[2] : 0.0);
-    if (sc[3] != 0.0) {
-      finish_req(s, q, TG_REQ_FAILED, TG_ERR_NONFINITE);
-      leave.push_back(r);
-    } else if (q.st.steps_done >= q.n_steps) {
-      int rc = store_slot(s, b, r, q);
+    if (r < nl) {
+      const double* sc = b.h + 8 * (size_t)r;
+      const double* ro = b.h + 8 * (size_t)b.B + 8 * (size_t)r;
+      q.st.steps_done++;
+      s->request_steps++;
+      q.st.t_final = sc[1];
+      q.st.final_energy = ro[0] + (c->phys == TG_MHD ? ro[2] : 0.0);
+      if (sc[3] != 0.0) {
+        finish_req(s, q, TG_REQ_FAILED, TG_ERR_NONFINITE);
+        leave.push_back(r);
+        continue;
+      }
+    }
+    if (q.st.steps_done >= q.n_steps) {
+      const int rc = store_slot(s, b, r, q);
       finish_req(s, q, rc ? TG_REQ_FAILED : TG_REQ_DONE, rc);
       leave.push_back(r);
     }
@@ -393,6 +445,9 @@ int tg_server_destroy(tg_server* s) {
   if (!s) return TG_ERR_ARG;
   cudaSetDevice(s->dev);
   for (auto& kv : s->batches) destroy_batch(s, kv.second);
+  for (auto& kv : s->reqs)
+    if (kv.second.result) cudaFreeHost(kv.second.result);
+  s->pinned.clear();
   delete s;
   return TG_OK;
 }
@@ -420,6 +475,7 @@ int tg_server_submit(tg_server* s, const tg_request* rq, long long* id) {
     r.st.state = TG_REQ_FAILED;
     r.st.error = TG_ERR_OOM;
     r.st.finish_s = r.st.submit_s;
+    s->finished.push_back(r.id);
   } else {
     r.init.assign(rq->init, rq->init + rq->n_doubles);
     s->queue.push_back(r.id);
@@ -432,17 +488,23 @@ int tg_server_submit(tg_server* s, const tg_request* rq, long long* id) {
 int tg_server_pump(tg_server* s, int* n_active) {
   if (!s) return TG_ERR_ARG;
   cudaSetDevice(s->dev);
-  int rc = admit(s);
-  if (rc) return rc;
-  std::vector<std::pair<long long, int>> launched;
+  // launch a step of every resident batch first, so that the host work of admission (copies
+  // into pinned blocks, new contexts) overlaps the steps on the device
+  std::map<long long, std::pair<int, int>> launched;  // batch -> (slots stepped, launch code)
   for (auto& kv : s->batches) {
     Batch& b = kv.second;
     if (b.slot_req.empty()) continue;
-    launched.emplace_back(kv.first, launch_batch(s, b));
+    const int nl = (int)b.slot_req.size();
+    launched[kv.first] = {nl, launch_batch(s, b)};
   }
-  int first_err = TG_OK;
-  for (auto& lb : launched) {
-    const int r2 = collect_batch(s, s->batches[lb.first], lb.second);
+  int first_err = admit(s);
+  for (auto& kv : s->batches) {
+    Batch& b = kv.second;
+    auto it = launched.find(kv.first);
+    if (it == launched.end() && b.slot_req.empty() && b.loading.empty()) continue;
+    const int nl = it == launched.end() ? 0 : it->second.first;
+    const int lrc = it == launched.end() ? TG_OK : it->second.second;
+    const int r2 = collect_batch(s, b, nl, lrc);
     if (r2 && !first_err) first_err = r2;
   }
   if (!launched.empty()) s->rounds++;
@@ -488,9 +550,9 @@ int tg_server_result(tg_server* s, long long id, double* host, size_t n) {
   auto it = s->reqs.find(id);
   if (it == s->reqs.end()) return TG_ERR_ARG;
   const Req& r = it->second;
-  if (r.st.state != TG_REQ_DONE || r.result.empty()) return TG_ERR_STATE;
-  if (n != r.result.size()) return TG_ERR_ARG;
-  std::memcpy(host, r.result.data(), sizeof(double) * n);
+  if (r.st.state != TG_REQ_DONE || !r.result) return TG_ERR_STATE;
+  if (n != r.n_result) return TG_ERR_ARG;
+  std::memcpy(host, r.result, sizeof(double) * n);
   return TG_OK;
 }
 
@@ -498,7 +560,19 @@ int tg_server_release(tg_server* s, long long id) {
   if (!s) return TG_ERR_ARG;
   auto it = s->reqs.find(id);
   if (it == s->reqs.end()) return TG_ERR_ARG;
-  std::vector<double>().swap(it->second.result);
+  Req& r = it->second;
+  s->pinned.put(r.result, r.n_result);
+  r.result = nullptr;
+  r.n_result = 0;
+  return TG_OK;
+}
+
+int tg_server_take_finished(tg_server* s, long long* ids, int max, int* n) {
+  if (!s || !n || max < 0 || (max > 0 && !ids)) return TG_ERR_ARG;
+  const int k = (int)std::min<size_t>((size_t)max, s->finished.size());
+  for (int i = 0; i < k; ++i) ids[i] = s->finished[i];
+  s->finished.erase(s->finished.begin(), s->finished.begin() + k);
+  *n = k;
   return TG_OK;
 }
 

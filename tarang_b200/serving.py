@@ -76,18 +76,23 @@ class Server:
 
     def submit(self, config: dict, fields, n_steps: int) -> int:
         """config: keyword arguments of ``make_config`` (N, physics, nu, dt, precision, ...);
-        fields: the state fields (V, then W or T), each (N1, N2, N3/2+1) complex128."""
+        fields: the state fields (V, then W or T), each (N1, N2, N3/2+1) complex128, or one
+        C-contiguous complex128 array of shape (n_fields, N1, N2, N3/2+1) (used without a copy)."""
         cfg = make_config(**config)
         N = tuple(cfg.N)
         shape = (N[0], N[1], N[2] // 2 + 1)
         ns = _NSTATE[cfg.physics]
-        if len(fields) != ns:
-            raise ValueError(f"{ns} state fields expected, got {len(fields)}")
-        init = np.empty((ns,) + shape, dtype=np.complex128)
-        for i, f in enumerate(fields):
-            if np.shape(f) != shape:
-                raise ValueError(f"field shape {np.shape(f)} != {shape}")
-            init[i] = f
+        if (isinstance(fields, np.ndarray) and fields.dtype == np.complex128 and fields.shape == (ns,) + shape
+                and fields.flags.c_contiguous):
+            init = fields
+        else:
+            if len(fields) != ns:
+                raise ValueError(f"{ns} state fields expected, got {len(fields)}")
+            init = np.empty((ns,) + shape, dtype=np.complex128)
+            for i, f in enumerate(fields):
+                if np.shape(f) != shape:
+                    raise ValueError(f"field shape {np.shape(f)} != {shape}")
+                init[i] = f
         flat = init.view(np.float64).reshape(-1)
         rq = L.tg_request()
         rq.cfg = cfg
@@ -133,6 +138,19 @@ class Server:
 
     def release(self, rid: int):
         self.lib.tg_server_release(self.h, int(rid))
+
+    def take_finished(self, max_ids: int = 4096) -> list[int]:
+        """Ids of requests finished (done or failed) since the last call."""
+        buf = (C.c_longlong * max_ids)()
+        out: list[int] = []
+        while True:
+            n = C.c_int()
+            rc = self.lib.tg_server_take_finished(self.h, buf, max_ids, C.byref(n))
+            if rc != L.TG_OK:
+                raise L.TarangError(rc, "tg_server_take_finished")
+            out += buf[: n.value]
+            if n.value < max_ids:
+                return out
 
     def stats(self) -> dict:
         st = L.tg_server_stats()

@@ -155,6 +155,7 @@ def test_budget_admission(lib):
         starts = sorted(srv.poll(i)["start_s"] for i in ids)
         finishes = sorted(srv.poll(i)["finish_s"] for i in ids)
         assert starts[1] >= finishes[0] and starts[2] >= finishes[1]
+        assert sorted(srv.take_finished()) == sorted(ids) and srv.take_finished() == []
         for rid, f in zip(ids, reqs):
             want, _, _ = lone(cfg, f, 5)
             assert same_bits(srv.result(rid), want)
@@ -254,3 +255,24 @@ def test_served_request_matches_oracle(lib):
     num = math.sqrt(sum(float(np.sum(np.abs(x - y) ** 2)) for x, y in zip(got, Vw)))
     den = math.sqrt(sum(float(np.sum(np.abs(y) ** 2)) for y in Vw))
     assert num / den < 1e-12
+
+
+def test_zero_step_request_returns_stored_fields(lib):
+    from tarang_b200.serving import Server
+    from tarang_b200.solver import IncFluid
+    N = (32, 32, 32)
+    V = fluid_fields(N, 31)
+    with Server(hbm_budget=8e9) as srv:
+        a = srv.submit(dict(N=N), V, 0)
+        b = srv.submit(dict(N=N, nu=5e-3), fluid_fields(N, 32), 3)
+        srv.drain()
+        st = srv.poll(a)
+        assert st["state"] == "done" and st["steps_done"] == 0
+        got = srv.result(a)
+        srv.release(a)
+        with pytest.raises(L.TarangError):
+            srv.result(a)
+        assert srv.poll(b)["steps_done"] == 3
+    s = IncFluid(N)
+    s.set_V(V)
+    assert same_bits(got, s.get_V())
