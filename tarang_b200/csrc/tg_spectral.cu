@@ -167,88 +167,111 @@ __device__ __forceinline__ void project_rhs(cx<double>* r, int ns, const XDer& d
 //  stage 2: u2 = E(1/2) u0 + dt/2 N1,         tot += dt/3 E(1/2) N1
 //  stage 3: u3 = E(1/2)(E(1/2) u0 + dt N2),   tot += dt/3 E(1/2) N2
 //  stage 4: u  = E(1) u0 + tot + dt/6 N3   (then the energy of u for the NaN check / Get_dt)
-template <typename Rp, typename Rs, int PHYS, int SRC>
-__global__ void __launch_bounds__(TPB) k_rk(RKArgs a) {
+// Resident blocks per SM the RK kernel is built for (fluid/scalar: 3 at 80 registers, MHD: 2).
+template <int PHYS>
+struct RKOcc {
+  static constexpr int v = (PHYS == PH_MHD) ? 2 : 3;
+};
+
+// One thread per stored mode of one request (slot blockIdx.y).  Every value the mode needs
+// (U0, TOT, the products) is loaded before anything is stored, so the loads of an element are
+// in flight together; exp(-nu a dt K^2) is evaluated once per distinct viscosity.
+template <typename Rp, typename Rs, int PHYS, int SRC, int STAGE>
+__global__ void __launch_bounds__(TPB, RKOcc<PHYS>::v) k_rk(RKArgs a) {
   constexpr int NS = NState<PHYS>::v;
   const Geo& g = a.g;
   double acc[6] = {0, 0, 0, 0, 0, 0};
-  const long long stride = (long long)gridDim.x * TPB;
-  for (long long idx = (long long)blockIdx.x * TPB + threadIdx.x; idx < g.S; idx += stride) {
-    int r1, r2, l3;
-    compact_mode(g, idx, r1, r2, l3);
-    if (l3 < g.nkz) {
-      const int kxi = geo_kx(g, r1), kyi = geo_ky(g, r2);
-      const long long gi = (long long)blockIdx.y * g.S + idx;  // request blockIdx.y of the batch
-      const double kx = kxi * g.kf0, ky = kyi * g.kf1, kz = l3 * g.kf2;
-      const double K2 = kx * kx + ky * ky + kz * kz;
-      cx<double> r[NS];
-      if constexpr (SRC == 0) {
-        const XDer dx{kx, g.basis};
-        assemble<Rp, PHYS>(a.PX, gi, dx, ky, kz, r);
-        if (a.FB != nullptr && kxi >= -a.fx && kxi <= a.fx && kyi >= -a.fy && kyi <= a.fy && l3 <= a.fz) {
-          const int box = (2 * a.fx + 1) * (2 * a.fy + 1) * (a.fz + 1);
-          const int p = ((kxi + a.fx) * (2 * a.fy + 1) + (kyi + a.fy)) * (a.fz + 1) + l3;
+  const int slot = blockIdx.y;
+  const long long base = (long long)slot * g.S;
+  const double dt = a.dt[(long long)slot * 8];
+  double nus[NS];
 #pragma unroll
-          for (int c = 0; c < 3; ++c) r[c] = r[c] - a.FB[(long long)c * box + p];
-        }
-        if constexpr (PHYS == PH_RB) {
-          // Compute_force_RB (compute_force_RB.cc:51-105) from the stage's fields, then Add_force:
-          // nlin1 -= fu * theta, T.nlin -= ft * u1
-          const cx<double> th = a.inprec ? ldc<float>(a.IN[3], gi) : ldc<double>(a.IN[3], gi);
-          const cx<double> u1 = a.inprec ? ldc<float>(a.IN[0], gi) : ldc<double>(a.IN[0], gi);
-          r[0] = r[0] - a.rb_buoy_u * th;
-          r[3] = r[3] - a.rb_buoy_t * u1;
-        }
-        project_rhs(r, NS, dx, ky, kz, K2);
-      } else {
+  for (int c = 0; c < NS; ++c) nus[c] = a.nu_tab ? a.nu_tab[slot * 6 + c] : a.nu[c];
+  const unsigned S = (unsigned)g.S, kzp = (unsigned)g.kzp, nky = (unsigned)g.nky;
+  const unsigned stride = gridDim.x * TPB;
+  for (unsigned i = blockIdx.x * TPB + threadIdx.x; i < S; i += stride) {
+    const unsigned rr = i / kzp;
+    const int l3 = (int)(i - rr * kzp);
+    if (l3 >= g.nkz) continue;
+    const int r1 = (int)(rr / nky), r2 = (int)(rr - (unsigned)r1 * nky);
+    const long long gi = base + i;
+    cx<double> u0[NS], tot[NS];
 #pragma unroll
-        for (int c = 0; c < NS; ++c) r[c] = a.RHS[c][gi];
+    for (int c = 0; c < NS; ++c) u0[c] = a.U0[c][gi];
+    if constexpr (STAGE > 1) {
+#pragma unroll
+      for (int c = 0; c < NS; ++c) tot[c] = a.TOT[c][gi];
+    }
+    const int kxi = geo_kx(g, r1), kyi = geo_ky(g, r2);
+    const double kx = kxi * g.kf0, ky = kyi * g.kf1, kz = l3 * g.kf2;
+    const double K2 = kx * kx + ky * ky + kz * kz;
+    cx<double> r[NS];
+    if constexpr (SRC == 0) {
+      const XDer dx{kx, g.basis};
+      assemble<Rp, PHYS>(a.PX, gi, dx, ky, kz, r);
+      if (a.FB != nullptr && kxi >= -a.fx && kxi <= a.fx && kyi >= -a.fy && kyi <= a.fy && l3 <= a.fz) {
+        const int box = (2 * a.fx + 1) * (2 * a.fy + 1) * (a.fz + 1);
+        const int p = ((kxi + a.fx) * (2 * a.fy + 1) + (kyi + a.fy)) * (a.fz + 1) + l3;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) r[c] = r[c] - a.FB[(long long)c * box + p];
       }
-      const double dt = a.dt[(long long)blockIdx.y * 8];
-      const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
+      if constexpr (PHYS == PH_RB) {
+        // Compute_force_RB (compute_force_RB.cc:51-105) from the stage's fields, then Add_force:
+        // nlin1 -= fu * theta, T.nlin -= ft * u1
+        const cx<double> th = a.inprec ? ldc<float>(a.IN[3], gi) : ldc<double>(a.IN[3], gi);
+        const cx<double> u1 = a.inprec ? ldc<float>(a.IN[0], gi) : ldc<double>(a.IN[0], gi);
+        r[0] = r[0] - a.rb_buoy_u * th;
+        r[3] = r[3] - a.rb_buoy_t * u1;
+      }
+      project_rhs(r, NS, dx, ky, kz, K2);
+    } else {
 #pragma unroll
-      for (int c = 0; c < NS; ++c) {
-        const double nu_c = a.nu_tab ? a.nu_tab[blockIdx.y * 6 + c] : a.nu[c];
-        const double eh = exp(-nu_c * 0.5 * dt * K2);
-        const cx<double> u0 = a.U0[c][gi];
-        const cx<double> rc = r[c];
-        if (a.stage == 1) {
-          const double e1 = exp(-nu_c * dt * K2);
-          stc<Rs>(a.US[c], gi, eh * (u0 + (0.5 * dt) * rc));
-          a.TOT[c][gi] = (dt / 6.0) * (e1 * rc);
-        } else if (a.stage == 2) {
-          stc<Rs>(a.US[c], gi, eh * u0 + (0.5 * dt) * rc);
-          a.TOT[c][gi] = a.TOT[c][gi] + (dt / 3.0) * (eh * rc);
-        } else if (a.stage == 3) {
-          stc<Rs>(a.US[c], gi, eh * (eh * u0 + dt * rc));
-          a.TOT[c][gi] = a.TOT[c][gi] + (dt / 3.0) * (eh * rc);
+      for (int c = 0; c < NS; ++c) r[c] = a.RHS[c][gi];
+    }
+    const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
+    double eh = 0, e1 = 0;
+#pragma unroll
+    for (int c = 0; c < NS; ++c) {
+      if (c == 0 || nus[c] != nus[c - 1]) {
+        eh = exp(-nus[c] * 0.5 * dt * K2);
+        if constexpr (STAGE == 1 || STAGE == 4) e1 = exp(-nus[c] * dt * K2);
+      }
+      const cx<double> rc = r[c];
+      if constexpr (STAGE == 1) {
+        stc<Rs>(a.US[c], gi, eh * (u0[c] + (0.5 * dt) * rc));
+        a.TOT[c][gi] = (dt / 6.0) * (e1 * rc);
+      } else if constexpr (STAGE == 2) {
+        stc<Rs>(a.US[c], gi, eh * u0[c] + (0.5 * dt) * rc);
+        a.TOT[c][gi] = tot[c] + (dt / 3.0) * (eh * rc);
+      } else if constexpr (STAGE == 3) {
+        stc<Rs>(a.US[c], gi, eh * (eh * u0[c] + dt * rc));
+        a.TOT[c][gi] = tot[c] + (dt / 3.0) * (eh * rc);
+      } else {
+        const cx<double> u = e1 * u0[c] + (tot[c] + (dt / 6.0) * rc);
+        a.U0[c][gi] = u;
+        const double m2 = u.x * u.x + u.y * u.y;
+        const int grp = (PHYS == PH_MHD) ? (c / 3) * 2 : (c < 3 ? 0 : 4);
+        double w, m;
+        if (g.basis == 0) {
+          w = energy_weight_four(l1, l2, l3, g.N1, g.N2);
+          m = mult_four(l1, l2, l3, g.N1, g.N2);
         } else {
-          const double e1 = exp(-nu_c * dt * K2);
-          const cx<double> tot = a.TOT[c][gi] + (dt / 6.0) * rc;
-          const cx<double> u = e1 * u0 + tot;
-          a.U0[c][gi] = u;
-          const double m2 = u.x * u.x + u.y * u.y;
-          const int grp = (PHYS == PH_MHD) ? (c / 3) * 2 : (c < 3 ? 0 : 4);
-          double w, m;
-          if (g.basis == 0) {
-            w = energy_weight_four(l1, l2, l3, g.N1, g.N2);
-            m = mult_four(l1, l2, l3, g.N1, g.N2);
-          } else {
-            // Get_total_energy_SCFT (scft_energy.cc:51-104): multiplicity, origin excluded
-            m = mult_scft(l1, l2, l3, g.N2);
-            w = (l1 == 0 && l2 == 0 && l3 == 0) ? m - 0.5 : m;
-          }
-          acc[grp] += w * m2;
-          acc[grp + 1] += m * K2 * m2;
+          // Get_total_energy_SCFT (scft_energy.cc:51-104): multiplicity, origin excluded
+          m = mult_scft(l1, l2, l3, g.N2);
+          w = (l1 == 0 && l2 == 0 && l3 == 0) ? m - 0.5 : m;
         }
+        acc[grp] += w * m2;
+        acc[grp + 1] += m * K2 * m2;
       }
     }
   }
-  if (a.stage == 4 && a.part != nullptr) {
-    block_sum<6>(acc);
-    if (threadIdx.x == 0) {
+  if constexpr (STAGE == 4) {
+    if (a.part != nullptr) {
+      block_sum<6>(acc);
+      if (threadIdx.x == 0) {
 #pragma unroll
-      for (int j = 0; j < 6; ++j) a.part[((long long)blockIdx.y * gridDim.x + blockIdx.x) * 8 + j] = acc[j];
+        for (int j = 0; j < 6; ++j) a.part[((long long)blockIdx.y * gridDim.x + blockIdx.x) * 8 + j] = acc[j];
+      }
     }
   }
 }
@@ -256,8 +279,19 @@ __global__ void __launch_bounds__(TPB) k_rk(RKArgs a) {
 template <typename Rp, typename Rs, int PHYS>
 cudaError_t run_rk_src(const RKArgs& a, int src, cudaStream_t s, int nblk) {
   const dim3 grid(nblk, a.nact > 0 ? a.nact : 1);
-  if (src == 0) k_rk<Rp, Rs, PHYS, 0><<<grid, TPB, 0, s>>>(a);
-  else k_rk<Rp, Rs, PHYS, 1><<<grid, TPB, 0, s>>>(a);
+  if (src == 1) {
+    // precomputed right-hand sides enter at stage 1 only (Time_advance after Compute_rhs)
+    if (a.stage != 1) return cudaErrorInvalidValue;
+    k_rk<Rp, Rs, PHYS, 1, 1><<<grid, TPB, 0, s>>>(a);
+  } else {
+    switch (a.stage) {
+      case 1: k_rk<Rp, Rs, PHYS, 0, 1><<<grid, TPB, 0, s>>>(a); break;
+      case 2: k_rk<Rp, Rs, PHYS, 0, 2><<<grid, TPB, 0, s>>>(a); break;
+      case 3: k_rk<Rp, Rs, PHYS, 0, 3><<<grid, TPB, 0, s>>>(a); break;
+      case 4: k_rk<Rp, Rs, PHYS, 0, 4><<<grid, TPB, 0, s>>>(a); break;
+      default: return cudaErrorInvalidValue;
+    }
+  }
   return cudaGetLastError();
 }
 template <typename Rp, typename Rs>
@@ -581,7 +615,8 @@ __global__ void __launch_bounds__(TPB) k_shell_spectrum(Geo g, PtrArr6 pa, int n
 }
 
 inline int nblk(long long n) { return (int)((n + TPB - 1) / TPB); }
-inline int nred(long long n) { return nblk(n) < 148 * 8 ? nblk(n) : 148 * 8; }
+// reducing kernels: whole waves on 148 SMs (2 waves of the RK kernel at 3 blocks per SM, 3 at 2)
+inline int nred(long long n) { return nblk(n) < 148 * 6 ? nblk(n) : 148 * 6; }
 
 }  // namespace
 
