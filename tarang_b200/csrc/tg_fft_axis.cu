@@ -1,14 +1,198 @@
 // Dispatch of the strided-axis c2c kernels (x- and y-passes).
+//
+// Power-of-two lengths 16..256 whose stored input and kept output rows fit one TMA box (<= 256
+// rows) run k_axis_tma: the block's column tile moves HBM -> shared memory and back as single
+// tiled bulk tensor copies, so the threads spend no instructions on addresses or row maps of
+// global memory.  Other lengths run the register-staged k_axis_c2c / k_axis_dft.  Both compute
+// the same butterflies in the same order (identical results).
+#include <cstdlib>
+#include <cstring>
+
 #include "tg_fft_launch.h"
+#include "tg_tma.cuh"
 
 namespace tg {
 
 namespace {
 
+// set by a TMA-staged block whose tile never arrived within the bounded wait
+__device__ int g_axis_tma_timeout = 0;
+
+constexpr int kTmaPolls = 1 << 20;
+
+struct TmaSet {
+  CUtensorMap src[kMaxPtr];
+  CUtensorMap src2[kMaxPtr];
+  CUtensorMap dst[kMaxPtr];
+};
+
+// One block: W = 256/R1 columns of one batch of one field.  Tile rows in shared memory are
+// row-major [row][W]; the same buffer holds the loaded input tile, then the transposed
+// intermediate, then the output tile.
+template <typename Ri, typename Ro, typename Rw, int R1, int R2, int DIR, bool COMB>
+__global__ void __launch_bounds__(256) k_axis_tma(AxisArgs a, const __grid_constant__ TmaSet tm, int nin_rows,
+                                                  int nout_rows, unsigned tile_bytes) {
+  constexpr int L = R1 * R2;
+  constexpr int W = 256 / R1;
+  constexpr int CEi = (int)(sizeof(cx<Ri>) / 8), CEo = (int)(sizeof(cx<Ro>) / 8);
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(base);
+  int* ok_flag = reinterpret_cast<int*>(base + 8);
+  cx<Rw>* tw = reinterpret_cast<cx<Rw>*>(base + 128);
+  unsigned char* buf = base + 128 + ((L * sizeof(cx<Rw>) + 127) & ~(size_t)127);
+  unsigned char* buf2 = buf + tile_bytes;
+  const int tid = threadIdx.x;
+  const int f = blockIdx.z, b = blockIdx.y, col0 = blockIdx.x * W;
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  if (tid == 0) {
+    const unsigned in_bytes = (unsigned)(W * CEi * 8) * (unsigned)nin_rows;
+    mbar_arrive_expect_tx(bar, COMB ? 2 * in_bytes : in_bytes);
+    tma_load_3d(buf, &tm.src[f], col0 * CEi, 0, b, bar);
+    if constexpr (COMB) tma_load_3d(buf2, &tm.src2[f], col0 * CEi, 0, b, bar);
+  }
+  for (int i = tid; i < L; i += 256) {
+    cx<Rw> t = cvt<Rw>(a.tw[i]);
+    if (DIR > 0) t.y = -t.y;
+    tw[i] = t;
+  }
+  if (tid == 0) {
+    const bool ok = mbar_wait_bounded(bar, 0, kTmaPolls);
+    *ok_flag = ok ? 1 : 0;
+    if (!ok) {
+      atomicExch(&g_axis_tma_timeout, 1);
+      mbar_wait_bounded(bar, 0, kTmaPolls);  // let a late copy land before the block leaves
+    }
+  }
+  __syncthreads();
+  if (*ok_flag == 0) return;
+  mbar_wait_bounded(bar, 0, 64);  // the phase has completed: acquire the copied tile
+  const int w = tid % W;
+  const int n2 = tid / W;
+  cx<Rw> v[R1];
+  if (n2 < R2) {
+    const cx<Ri>* tin = reinterpret_cast<const cx<Ri>*>(buf);
+    const cx<Ri>* tin2 = reinterpret_cast<const cx<Ri>*>(buf2);
+    const int comb = COMB ? a.comb[f] : 0;
+#pragma unroll
+    for (int n1 = 0; n1 < R1; ++n1) {
+      const int r = amap_row(a.in, R2 * n1 + n2);
+      v[n1] = mkc<Rw>(0, 0);
+      if (r >= 0) {
+        v[n1] = cvt<Rw>(tin[r * W + w]);
+        if constexpr (COMB) {
+          if (comb > 0) v[n1] = v[n1] + cvt<Rw>(tin2[r * W + w]);
+          else if (comb < 0) v[n1] = v[n1] - cvt<Rw>(tin2[r * W + w]);
+        }
+      }
+    }
+    DFT<R1, DIR, Rw>::run(v);
+  }
+  __syncthreads();  // the input tile is consumed; its buffer takes the intermediate
+  cx<Rw>* ex = reinterpret_cast<cx<Rw>*>(buf);
+  if (n2 < R2) {
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) ex[(k1 * R2 + n2) * W + w] = v[k1] * tw[(n2 * k1) & (L - 1)];
+  }
+  __syncthreads();
+  const int k1 = tid / W;
+  cx<Rw> u[R2];
+#pragma unroll
+  for (int m = 0; m < R2; ++m) u[m] = ex[(k1 * R2 + m) * W + w];
+  DFT<R2, DIR, Rw>::run(u);
+  __syncthreads();  // the intermediate is consumed; the buffer takes the output tile
+  cx<Ro>* tout = reinterpret_cast<cx<Ro>*>(buf);
+  const Rw sc = (Rw)a.scale;
+#pragma unroll
+  for (int k2 = 0; k2 < R2; ++k2) {
+    const int r = amap_row(a.out, k1 + R1 * k2);
+    if (r >= 0) tout[r * W + w] = cvt<Ro>(sc * u[k2]);
+  }
+  fence_proxy_async_smem();
+  __syncthreads();
+  if (tid == 0) {
+    tma_store_3d(&tm.dst[f], col0 * CEo, 0, b, buf);
+    bulk_commit_group();
+    bulk_wait_group_read0();
+  }
+}
+
+bool axis_tma_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("TG_AXIS_TMA");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+template <typename Ri, typename Ro, typename Rw, int R1, int R2, int DIR>
+cudaError_t run_axis_tma(const AxisLaunch& l, cudaStream_t s, bool* used) {
+  *used = false;
+  constexpr int L = R1 * R2;
+  constexpr int W = 256 / R1;
+  constexpr int CEi = (int)(sizeof(cx<Ri>) / 8), CEo = (int)(sizeof(cx<Ro>) / 8);
+  const int nin_rows = amap_count(l.a.in), nout_rows = amap_count(l.a.out);
+  if (nin_rows < 1 || nin_rows > 256 || nout_rows < 1 || nout_rows > 256) return cudaSuccess;
+  if (l.nbatch > 65535) return cudaSuccess;
+  bool comb = false;
+  for (int f = 0; f < l.nfields; ++f) comb = comb || (l.a.comb[f] != 0);
+  TmaSet tm;  // host staging of the maps (copied into the launch parameters)
+  std::memset(&tm, 0, sizeof(tm));
+  for (int f = 0; f < l.nfields; ++f) {
+    if (!tma_map_3d(&tm.src[f], l.ps.src[f], (unsigned long long)l.a.ncols * CEi, (unsigned long long)nin_rows,
+                    (unsigned long long)l.nbatch, (unsigned long long)l.a.sr * sizeof(cx<Ri>),
+                    (unsigned long long)l.a.sb * sizeof(cx<Ri>), W * CEi, nin_rows))
+      return cudaSuccess;
+    if (comb && l.a.comb[f] != 0 &&
+        !tma_map_3d(&tm.src2[f], l.ps.src2[f], (unsigned long long)l.a.ncols * CEi, (unsigned long long)nin_rows,
+                    (unsigned long long)l.nbatch, (unsigned long long)l.a.sr * sizeof(cx<Ri>),
+                    (unsigned long long)l.a.sb * sizeof(cx<Ri>), W * CEi, nin_rows))
+      return cudaSuccess;
+    if (comb && l.a.comb[f] == 0) tm.src2[f] = tm.src[f];
+    if (!tma_map_3d(&tm.dst[f], l.ps.dst[f], (unsigned long long)l.a.ncols * CEo, (unsigned long long)nout_rows,
+                    (unsigned long long)l.nbatch, (unsigned long long)l.a.dr * sizeof(cx<Ro>),
+                    (unsigned long long)l.a.db * sizeof(cx<Ro>), W * CEo, nout_rows))
+      return cudaSuccess;
+  }
+  size_t tile = (size_t)W * nin_rows * sizeof(cx<Ri>);
+  tile = tile > (size_t)W * L * sizeof(cx<Rw>) ? tile : (size_t)W * L * sizeof(cx<Rw>);
+  tile = tile > (size_t)W * nout_rows * sizeof(cx<Ro>) ? tile : (size_t)W * nout_rows * sizeof(cx<Ro>);
+  tile = (tile + 127) & ~(size_t)127;
+  const size_t smem = 128 + 128 + ((L * sizeof(cx<Rw>) + 127) & ~(size_t)127) + tile +
+                      (comb ? (size_t)W * nin_rows * sizeof(cx<Ri>) : 0);
+  if (smem > 200 * 1024) return cudaSuccess;
+  dim3 grid((l.a.ncols + W - 1) / W, l.nbatch, l.nfields);
+  cudaError_t e;
+  if (comb) {
+    auto kern = k_axis_tma<Ri, Ro, Rw, R1, R2, DIR, true>;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    kern<<<grid, 256, smem, s>>>(l.a, tm, nin_rows, nout_rows, (unsigned)tile);
+  } else {
+    auto kern = k_axis_tma<Ri, Ro, Rw, R1, R2, DIR, false>;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    kern<<<grid, 256, smem, s>>>(l.a, tm, nin_rows, nout_rows, (unsigned)tile);
+  }
+  *used = true;
+  return cudaGetLastError();
+}
+
 template <typename Ri, typename Ro, typename Rw, int R1, int R2, int DIR>
 cudaError_t run_axis_fast(const AxisLaunch& l, cudaStream_t s) {
   constexpr int L = R1 * R2;
   constexpr int W = 256 / R1;
+  if constexpr (L >= 16 && L <= 256) {
+    if (axis_tma_enabled()) {
+      bool used = false;
+      cudaError_t e = run_axis_tma<Ri, Ro, Rw, R1, R2, DIR>(l, s, &used);
+      if (e != cudaSuccess || used) return e;
+    }
+  }
   const size_t smem = (size_t)(L + (size_t)L * W) * sizeof(cx<Rw>);
   auto kern = k_axis_c2c<Ri, Ro, Rw, R1, R2, DIR>;
   static bool attr = false;
@@ -97,6 +281,16 @@ cudaError_t launch_axis(const AxisLaunch& l, cudaStream_t s) {
   if (l.pin == F32 && l.pout == F32) return run_axis_prec<float, float, float>(l, s);
   if (l.pin == F32 && l.pout == F64) return run_axis_prec<float, double, float>(l, s);
   return cudaErrorInvalidValue;
+}
+
+int axis_tma_timeout(bool clear) {
+  int h = 0;
+  if (cudaMemcpyFromSymbol(&h, g_axis_tma_timeout, sizeof(int)) != cudaSuccess) return -1;
+  if (clear && h) {
+    const int z = 0;
+    cudaMemcpyToSymbol(g_axis_tma_timeout, &z, sizeof(int));
+  }
+  return h;
 }
 
 }  // namespace tg

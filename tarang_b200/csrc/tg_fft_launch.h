@@ -36,6 +36,9 @@ struct ZProdLaunch {
 };
 
 cudaError_t launch_axis(const AxisLaunch& l, cudaStream_t s);
+// 1 if a TMA-staged axis block gave up waiting for its tile (its output is not written), 0
+// otherwise, -1 if the flag cannot be read; clear resets it
+int axis_tma_timeout(bool clear);
 // SCFT x-pass (real-to-real, per-field kind); l.L = N1, l.dir unused
 cudaError_t launch_r2r(const AxisLaunch& l, const R2RArgs& r, cudaStream_t s);
 cudaError_t launch_z(const ZLaunch& l, cudaStream_t s);
