@@ -29,8 +29,15 @@ struct TmaSet {
 // One block: W = 256/R1 columns of one batch of one field.  Tile rows in shared memory are
 // row-major [row][W]; the same buffer holds the loaded input tile, then the transposed
 // intermediate, then the output tile.
+// resident blocks per SM the TMA axis kernel is built for: 4 (FP32 arithmetic, 64 registers),
+// 3 (FP64, 80 registers); shared memory allows as many at L = 256
+template <typename Rw>
+struct AxisOcc {
+  static constexpr int v = sizeof(Rw) == 4 ? 4 : 3;
+};
+
 template <typename Ri, typename Ro, typename Rw, int R1, int R2, int DIR, bool COMB>
-__global__ void __launch_bounds__(256) k_axis_tma(AxisArgs a, const __grid_constant__ TmaSet tm, int nin_rows,
+__global__ void __launch_bounds__(256, AxisOcc<Rw>::v) k_axis_tma(AxisArgs a, const __grid_constant__ TmaSet tm, int nin_rows,
                                                   int nout_rows, unsigned tile_bytes) {
   constexpr int L = R1 * R2;
   constexpr int W = 256 / R1;
@@ -170,11 +177,13 @@ cudaError_t run_axis_tma(const AxisLaunch& l, cudaStream_t s, bool* used) {
   if (comb) {
     auto kern = k_axis_tma<Ri, Ro, Rw, R1, R2, DIR, true>;
     e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     if (e != cudaSuccess) return e;
     kern<<<grid, 256, smem, s>>>(l.a, tm, nin_rows, nout_rows, (unsigned)tile);
   } else {
     auto kern = k_axis_tma<Ri, Ro, Rw, R1, R2, DIR, false>;
     e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     if (e != cudaSuccess) return e;
     kern<<<grid, 256, smem, s>>>(l.a, tm, nin_rows, nout_rows, (unsigned)tile);
   }
