@@ -4,7 +4,8 @@
 // rows) run k_axis_tma: the block's column tile moves HBM -> shared memory and back as single
 // tiled bulk tensor copies, so the threads spend no instructions on addresses or row maps of
 // global memory.  Other lengths run the register-staged k_axis_c2c / k_axis_dft.  Both compute
-// the same butterflies in the same order (identical results).
+// the same butterflies in the same order (equal results up to how the compiler contracts
+// multiply-adds in each kernel).
 #include <cstdlib>
 #include <cstring>
 
@@ -29,18 +30,22 @@ struct TmaSet {
 // One block: W = 256/R1 columns of one batch of one field.  Tile rows in shared memory are
 // row-major [row][W]; the same buffer holds the loaded input tile, then the transposed
 // intermediate, then the output tile.
-// resident blocks per SM the TMA axis kernel is built for: 4 (FP32 arithmetic, 64 registers),
-// 3 (FP64, 80 registers); shared memory allows as many at L = 256
-template <typename Rw>
+// Tile width of the TMA axis kernel: 8 columns (64 or 128 contiguous bytes per row), so the
+// solver's column counts (kzp, a multiple of 8, and nky * kzp) split into whole tiles; the block
+// has W * R1 threads (128 at L = 256).
+constexpr int kTmaW = 8;
+// resident blocks per SM the kernel is built for: 64 registers (FP32 arithmetic) or 80 (FP64)
+template <typename Rw, int NT>
 struct AxisOcc {
-  static constexpr int v = sizeof(Rw) == 4 ? 4 : 3;
+  static constexpr int v = (65536 / NT) / (sizeof(Rw) == 4 ? 64 : 80);
 };
 
 template <typename Ri, typename Ro, typename Rw, int R1, int R2, int DIR, bool COMB>
-__global__ void __launch_bounds__(256, AxisOcc<Rw>::v) k_axis_tma(AxisArgs a, const __grid_constant__ TmaSet tm, int nin_rows,
-                                                  int nout_rows, unsigned tile_bytes) {
+__global__ void __launch_bounds__(kTmaW * R1, AxisOcc<Rw, kTmaW * R1>::v)
+    k_axis_tma(AxisArgs a, const __grid_constant__ TmaSet tm, int nin_rows, int nout_rows, unsigned tile_bytes) {
   constexpr int L = R1 * R2;
-  constexpr int W = 256 / R1;
+  constexpr int W = kTmaW;
+  constexpr int NT = W * R1;
   constexpr int CEi = (int)(sizeof(cx<Ri>) / 8), CEo = (int)(sizeof(cx<Ro>) / 8);
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
@@ -62,7 +67,7 @@ __global__ void __launch_bounds__(256, AxisOcc<Rw>::v) k_axis_tma(AxisArgs a, co
     tma_load_3d(buf, &tm.src[f], col0 * CEi, 0, b, bar);
     if constexpr (COMB) tma_load_3d(buf2, &tm.src2[f], col0 * CEi, 0, b, bar);
   }
-  for (int i = tid; i < L; i += 256) {
+  for (int i = tid; i < L; i += NT) {
     cx<Rw> t = cvt<Rw>(a.tw[i]);
     if (DIR > 0) t.y = -t.y;
     tw[i] = t;
@@ -140,7 +145,8 @@ template <typename Ri, typename Ro, typename Rw, int R1, int R2, int DIR>
 cudaError_t run_axis_tma(const AxisLaunch& l, cudaStream_t s, bool* used) {
   *used = false;
   constexpr int L = R1 * R2;
-  constexpr int W = 256 / R1;
+  constexpr int W = kTmaW;
+  constexpr int NT = W * R1;
   constexpr int CEi = (int)(sizeof(cx<Ri>) / 8), CEo = (int)(sizeof(cx<Ro>) / 8);
   const int nin_rows = amap_count(l.a.in), nout_rows = amap_count(l.a.out);
   if (nin_rows < 1 || nin_rows > 256 || nout_rows < 1 || nout_rows > 256) return cudaSuccess;
@@ -179,13 +185,13 @@ cudaError_t run_axis_tma(const AxisLaunch& l, cudaStream_t s, bool* used) {
     e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     if (e != cudaSuccess) return e;
-    kern<<<grid, 256, smem, s>>>(l.a, tm, nin_rows, nout_rows, (unsigned)tile);
+    kern<<<grid, NT, smem, s>>>(l.a, tm, nin_rows, nout_rows, (unsigned)tile);
   } else {
     auto kern = k_axis_tma<Ri, Ro, Rw, R1, R2, DIR, false>;
     e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     if (e != cudaSuccess) return e;
-    kern<<<grid, 256, smem, s>>>(l.a, tm, nin_rows, nout_rows, (unsigned)tile);
+    kern<<<grid, NT, smem, s>>>(l.a, tm, nin_rows, nout_rows, (unsigned)tile);
   }
   *used = true;
   return cudaGetLastError();
