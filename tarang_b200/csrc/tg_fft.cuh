@@ -554,17 +554,22 @@ __device__ __forceinline__ cx<R> shfl_c(cx<R> v, int src) {
 // (h = 16 >> s); with p the partner's value the lower lane keeps v + p and the upper lane
 // (p - v) w, w = e^{+2 pi i (l mod h) / (2h)}.  Both are (p + sg v) wl with sg = -1 / +1 and
 // wl = w / 1 on the upper / lower lane (wl[s] precomputed per lane).
+// The last two stages have trivial twiddles: h = 2 multiplies by i on lanes l = 3 mod 4 (w =
+// e^{i pi / 2}) and by 1 elsewhere; h = 1 multiplies by 1.
 template <typename R, int E>
 __device__ __forceinline__ void lane_dif32(cx<R> (&v)[E], const cx<R> (&wl)[5], int lane) {
 #pragma unroll
   for (int s = 0; s < 5; ++s) {
     const int h = 16 >> s;
     const R sg = (lane & h) ? (R)-1 : (R)1;
+    const bool rot = (lane & 3) == 3;
 #pragma unroll
     for (int k = 0; k < E; ++k) {
       const cx<R> p = shfl_xor_c(v[k], h);
       const cx<R> a = mkc<R>(fma(sg, v[k].x, p.x), fma(sg, v[k].y, p.y));
-      v[k] = a * wl[s];
+      if (s == 4) v[k] = a;
+      else if (s == 3) v[k] = rot ? mkc<R>(-a.y, a.x) : a;
+      else v[k] = a * wl[s];
     }
   }
 }
@@ -579,9 +584,13 @@ __device__ __forceinline__ void lane_dit32_fwd(cx<R> (&v)[E], const cx<R> (&wl)[
     const int h = 16 >> s;
     const R sg = (lane & h) ? (R)-1 : (R)1;
     const cx<R> wc = conjc(wl[s]);
+    const bool rot = (lane & 3) == 3;
 #pragma unroll
     for (int k = 0; k < E; ++k) {
-      const cx<R> sv = wc * v[k];
+      cx<R> sv;
+      if (s == 4) sv = v[k];
+      else if (s == 3) sv = rot ? mkc<R>(v[k].y, -v[k].x) : v[k];
+      else sv = wc * v[k];
       const cx<R> r = shfl_xor_c(sv, h);
       v[k] = mkc<R>(fma(sg, sv.x, r.x), fma(sg, sv.y, r.y));
     }
@@ -589,7 +598,8 @@ __device__ __forceinline__ void lane_dit32_fwd(cx<R> (&v)[E], const cx<R> (&wl)[
 }
 
 template <typename Ri, typename Ro, typename Rw, int E, int NIN, int NPROD, int WPB>
-__global__ void __launch_bounds__(32 * WPB) k_z_prod_warp(ZArgs a, PtrSet ps, ProdPairs pp) {
+__global__ void __launch_bounds__(32 * WPB, (E <= 4 ? (sizeof(Rw) == 8 ? 4 : 6) : (sizeof(Rw) == 8 ? 3 : 4)))
+    k_z_prod_warp(ZArgs a, PtrSet ps, ProdPairs pp) {
   constexpr int M = 32 * E;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
