@@ -127,6 +127,12 @@ int tg_device_bytes(const tg_ctx* ctx, size_t* bytes);
 int tg_field_upload(tg_ctx* ctx, int field, const double* host, size_t n_doubles);
 int tg_field_download(tg_ctx* ctx, int field, double* host, size_t n_doubles);
 int tg_field_copy(tg_ctx* ctx, int dst_field, int src_field);
+/* A work field of its own for the caller (the reference's temporary arrays, e.g. the
+ * VF_temp / VF_temp_r fields IncVF.h:75-531 allocates): reserves a free slot among
+ * TG_WORK0 .. TG_WORK0+7, allocates its dense device array (zeroed), returns its id in *field;
+ * TG_ERR_BUSY when all eight are reserved.  tg_field_free releases the slot and its memory. */
+int tg_field_alloc(tg_ctx* ctx, int* field);
+int tg_field_free(tg_ctx* ctx, int field);
 
 /* Forward_transform_array / Inverse_transform_array (universal_tr.cc:66-146) on a work field,
  * in place.  parity: 0 cos/even, 1 sin/odd (SCFT only; ignored for FOUR). */
@@ -169,6 +175,13 @@ int tg_flux(tg_ctx* ctx, int kind, double* flux, int n);
 int tg_shell_to_shell(tg_ctx* ctx, int kind, double* tr, int n);
 /* Get_Nusselt_no (nusselt.cc:53-89), RB only */
 int tg_nusselt(tg_ctx* ctx, double* nusselt);
+/* IncVF::Compute_force_feed_shell (lib/IncFlow/EnergyTrdir/compute_force_feed.cc:70-76, with
+ * Shell_mult_all_FOUR lib/four/four_ET.cc:181-226): energy fed by the force into each shell,
+ * feed[i] = sum over |K| <= R_in with Get_shell_index(|K|) = i of 2 mult Re(F . V*), i = 0..S
+ * (n >= S+1), with the force last computed (tg_compute_force, or the last RK stage of tg_step;
+ * computed from the current field if the context never computed one) and the current field.
+ * Zero for a decaying run.  FOUR fluid only. */
+int tg_force_feed(tg_ctx* ctx, double* feed, int n);
 
 /* ------------------------------------------------------------------------------------------
  * Allocation-free energy reduction.  No counterpart in the reference.
@@ -281,10 +294,11 @@ int tg_server_destroy(tg_server* srv);
  * tg_ctx_create rejects or an init of the wrong length (no id).  A request that cannot fit the
  * budget even alone gets an id and state TG_REQ_FAILED with TG_ERR_OOM. */
 int tg_server_submit(tg_server* srv, const tg_request* req, long long* id);
-/* one scheduling round: admit queued requests that fit (first come first served, later ones
- * may pass one that waits for room), advance every resident batch by one step (batches on
- * their own streams, overlapping), retire finished and failed requests; *n_active = requests
- * running or queued afterwards */
+/* one scheduling round: advance every resident batch (batches on their own streams,
+ * overlapping) by one step, or with graphs on by as many steps as fit in the slowest batch's
+ * step (at most 16, never past a request's last step); meanwhile admit queued requests that fit
+ * (first come first served, later ones may pass one that waits for room); then retire finished
+ * and failed requests.  *n_active = requests running or queued afterwards */
 int tg_server_pump(tg_server* srv, int* n_active);
 /* pump until every submitted request is done or failed (bounded by max_rounds; 0 = no bound) */
 int tg_server_drain(tg_server* srv, long long max_rounds);

@@ -877,6 +877,14 @@ def shell_mult_all(As, Bs, R, kfactor, alias="DEALIAS", basis="FOUR"):
     return np.bincount(idx, weights=val[sel], minlength=len(R))[: len(R)]
 
 
+def force_feed_shell(F, V, kfactor, no_shells, alias="DEALIAS", basis="FOUR"):
+    """IncVF::Compute_force_feed_shell  compute_force_feed.cc:70-76: Shell_mult_all(Force, V)
+    on the energy-transfer shells (forceV_shell, length S+1)."""
+    N = (V[0].shape[0], V[0].shape[1], 2 * (V[0].shape[2] - 1))
+    R = et_radii(N, kfactor, no_shells, alias, basis)
+    return shell_mult_all(F, V, R, kfactor, alias, basis)
+
+
 def compute_flux(V, kfactor, no_shells, alias="DEALIAS", basis="FOUR"):
     """IncVF::Compute_flux()  compute_flux.cc:52-69: for sphere s = 1..S, G = u on
     0 < |K| <= R_s, flux(s) = -sum_{|K| > R_s} 2 mult Re(N(G) . u*).  Length S+1, [0] = 0."""

@@ -141,6 +141,8 @@ SIGNATURES = {
     "tg_field_upload": (C.c_int, [_VP, C.c_int, _DP, C.c_size_t]),
     "tg_field_download": (C.c_int, [_VP, C.c_int, _DP, C.c_size_t]),
     "tg_field_copy": (C.c_int, [_VP, C.c_int, C.c_int]),
+    "tg_field_alloc": (C.c_int, [_VP, C.POINTER(C.c_int)]),
+    "tg_field_free": (C.c_int, [_VP, C.c_int]),
     "tg_forward_transform": (C.c_int, [_VP, C.c_int, C.c_int]),
     "tg_inverse_transform": (C.c_int, [_VP, C.c_int, C.c_int]),
     "tg_compute_force": (C.c_int, [_VP]),
@@ -158,6 +160,7 @@ SIGNATURES = {
     "tg_flux": (C.c_int, [_VP, C.c_int, _DP, C.c_int]),
     "tg_shell_to_shell": (C.c_int, [_VP, C.c_int, _DP, C.c_int]),
     "tg_nusselt": (C.c_int, [_VP, _DP]),
+    "tg_force_feed": (C.c_int, [_VP, _DP, C.c_int]),
     "tg_energy_noalloc": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_int, _VP, _VP]),
     "tg_profile_enable": (C.c_int, [_VP, C.c_int]),
     "tg_profile_read": (C.c_int, [_VP, C.POINTER(tg_kernel_stat), C.c_int, C.POINTER(C.c_int)]),

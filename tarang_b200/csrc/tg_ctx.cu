@@ -154,6 +154,7 @@ int run_force(tg_ctx* c, const void* const* U, int uprec) {
   f.FB = c->FB;
   ProfScope pr(c, "force", 0.0);
   TG_CK(launch_force_supply(f, c->st));
+  c->force_ever = true;
   return TG_OK;
 }
 
@@ -414,6 +415,7 @@ void free_ctx(tg_ctx* c) {
   fr(c->PR);
   fr(c->FB);
   fr(c->trigx);
+  for (int k = 0; k < 4; ++k) fr(c->xmat[k]);
   fr(c->scal);
   fr(c->nu_tab);
   fr(c->red_out);
@@ -613,6 +615,34 @@ int ctx_create_batch(const tg_config* cfg, int B, tg_ctx** out) {
     if ((rc = dalloc(c, (void**)&c->trigx, sizeof(cx<double>) * h.size()))) return fail(rc);
     e = cudaMemcpy(c->trigx, h.data(), sizeof(cx<double>) * h.size(), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return fail(cuda_err(c, e, "trig table"));
+    // the x-pass of the pipeline as matrices [stored input row][output row] (the coefficients
+    // of k_axis_r2r): inverse kinds 2, 3 map the nkx stored slots m to all N1 points,
+    // forward kinds 0, 1 map the N1 points to the nkx kept slots
+    const int nk = g.nkx, fourN = 4 * N1;
+    for (int kind = 0; kind < 4; ++kind) {
+      const bool sine = (kind == 1 || kind == 3);
+      const bool fwd = kind <= 1;
+      const int nin = fwd ? N1 : nk, nout = fwd ? nk : N1;
+      std::vector<double> m((size_t)nin * nout);
+      for (int rr = 0; rr < nin; ++rr)
+        for (int ko = 0; ko < nout; ++ko) {
+          double t;
+          if (fwd) {
+            const int j = (int)(((long long)(2 * rr + 1) * ko) % fourN);
+            t = 2.0 * (sine ? h[j].y : h[j].x);
+          } else {
+            const int mm = amap_index(g.ax, rr);
+            const int j = (int)(((long long)mm * (2 * ko + 1)) % fourN);
+            t = (sine ? h[j].y : h[j].x) * ((mm == 0 && !sine) ? 1.0 : 2.0);
+          }
+          m[(size_t)rr * nout + ko] = t;
+        }
+      if ((rc = dalloc(c, (void**)&c->xmat[kind], sizeof(double) * m.size()))) return fail(rc);
+      e = cudaMemcpy(c->xmat[kind], m.data(), sizeof(double) * m.size(), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) return fail(cuda_err(c, e, "x-pass matrices"));
+      c->xmat_rows[kind] = nout;
+      c->xmat_cols[kind] = nin;
+    }
   }
   for (int L : {N1, N2, Mz, N3}) {
     rc = make_twiddles(c, L);
@@ -727,6 +757,12 @@ void state_viscosities(const tg_config* cfg, double nu[6]) {
 
 int ensure_staging_ctx(tg_ctx* c) { return ensure_staging(c); }
 
+int ensure_force_box(tg_ctx* c) {
+  if (!c->force_on || c->force_ever) return TG_OK;
+  const void* U[3] = {c->U0[0], c->U0[1], c->U0[2]};
+  return run_force(c, U, F64);
+}
+
 // Device bytes that ctx_create_batch(cfg, B) allocates (same sizes, same order), plus the dense
 // staging field that uploads and downloads add (with_staging).  0 for a configuration that
 // ctx_create_batch rejects on its shape.
@@ -759,7 +795,7 @@ size_t ctx_bytes_estimate(const tg_config* cfg, int B, bool with_staging) {
       lens.push_back(L);
       b += sizeof(cx<double>) * (size_t)L;
     }
-  if (cfg->basis == TG_SCFT) b += sizeof(cx<double>) * 4 * (size_t)N1;
+  if (cfg->basis == TG_SCFT) b += sizeof(cx<double>) * 4 * (size_t)N1 + sizeof(double) * 4 * (size_t)N1 * nkx;
   const size_t Sd1 = sizeof(cx<double>) * S;
   const size_t WXb = tsz * (size_t)N1 * nky * kzp * B;
   const size_t WYb = tsz * (size_t)N1 * N2 * kzp * B;
@@ -876,6 +912,38 @@ int tg_field_download(tg_ctx* c, int field, double* host, size_t n) {
   TG_CK(launch_compact_to_dense(c->g, src, sp, c->staging, c->st));
   TG_CK(cudaMemcpyAsync(host, c->staging, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
   TG_CK(cudaStreamSynchronize(c->st));
+  return TG_OK;
+}
+
+int tg_field_alloc(tg_ctx* c, int* field) {
+  if (!c || !field) return TG_ERR_ARG;
+  *field = -1;
+  cudaSetDevice(c->dev);
+  for (int i = 0; i < TG_NWORK; ++i) {
+    if (c->work_reserved[i]) continue;
+    const int f = TG_WORK0 + i;
+    int rc = ensure_dense(c, f);  // zeroed by dalloc when new
+    if (rc) return rc;
+    TG_CK(cudaMemsetAsync(c->dense[f], 0, sizeof(cx<double>) * (size_t)c->D, c->st));
+    c->work_reserved[i] = true;
+    *field = f;
+    return TG_OK;
+  }
+  return set_err(c, TG_ERR_BUSY, "all work fields are reserved");
+}
+
+int tg_field_free(tg_ctx* c, int field) {
+  if (!c || field < TG_WORK0 || field >= TG_WORK0 + TG_NWORK) return TG_ERR_ARG;
+  const int i = field - TG_WORK0;
+  if (!c->work_reserved[i]) return set_err(c, TG_ERR_STATE, "free: work field not reserved");
+  cudaSetDevice(c->dev);
+  TG_CK(cudaStreamSynchronize(c->st));
+  if (c->dense[field]) {
+    cudaFree(c->dense[field]);
+    c->bytes -= sizeof(cx<double>) * (size_t)c->D;
+    c->dense[field] = nullptr;
+  }
+  c->work_reserved[i] = false;
   return TG_OK;
 }
 
@@ -1120,7 +1188,10 @@ int tg_shell_spectrum(tg_ctx* c, int group, double* ek, double* dissk, int n) {
   // scratch: [nf*nbins] ek, [nbins] cnt, [nbins] diss, [nbins] cnt2
   const size_t need = (size_t)(nf + 3) * nbins;
   if (c->diag_cap < need) {
-    if (c->diag) cudaFree(c->diag);
+    if (c->diag) {
+      cudaFree(c->diag);
+      c->bytes -= sizeof(double) * c->diag_cap;
+    }
     c->diag = nullptr;
     c->diag_cap = 0;
     int rc = dalloc(c, (void**)&c->diag, sizeof(double) * need);

@@ -39,6 +39,8 @@ struct tg_ctx {
   // SCFT: (cos, sin)(pi j / 2 N1), j < 4 N1, and the x-pass kind of every pipeline field
   // (0 CFT, 1 SFT forward; 2 ICFT, 3 ISFT inverse)
   tg::cx<double>* trigx = nullptr;
+  double* xmat[4] = {};  // SCFT x-pass of the pipeline as matrices, per kind (see ctx creation)
+  int xmat_rows[4] = {}, xmat_cols[4] = {};
   int xinv_kind[6] = {};
   int xfwd_kind[9] = {};
   double rb_fu = 0, rb_ft = 0;  // RB: Force1 = rb_fu theta, T.Force = rb_ft u1
@@ -61,6 +63,7 @@ struct tg_ctx {
   int fx = 0, fy = 0, fz = 0, fbox = 0;
   int nf_modes = 0;
   tg::cx<double>* FB = nullptr;
+  bool force_ever = false;  // FB holds a force computed by this context
 
   // scalars and reductions
   double* scal = nullptr;   // per slot [8]: [0] dt, [1] t_now, [2] steps, [3] nonfinite, [4] Tdt
@@ -89,6 +92,7 @@ struct tg_ctx {
   // dense fields (reference layout, FP64), allocated on demand
   tg::cx<double>* dense[TG_NFIELDS] = {};
   tg::cx<double>* staging = nullptr;
+  bool work_reserved[TG_NWORK] = {};  // tg_field_alloc
 
   // status
   bool energy_valid = false;  // scal[0] holds Get_dt of the current state
@@ -149,4 +153,6 @@ int enqueue_step(tg_ctx* c, bool ring);
 // each slot's dt by the Get_dt rule without advancing its time
 int run_energy(tg_ctx* c, int dt_mode);
 int run_energy_slots(tg_ctx* c, int dt_mode, int r0, int n);
+// the force box from the current state if this context never computed a force (else unchanged)
+int ensure_force_box(tg_ctx* c);
 }  // namespace tg

@@ -52,6 +52,21 @@ std::vector<double> et_radii(const tg_ctx* c) {
 
 namespace {
 
+// the context's diagnostics scratch, grown to at least `need` doubles
+int ensure_diag(tg_ctx* c, size_t need) {
+  if (c->diag_cap >= need) return TG_OK;
+  if (c->diag) {
+    cudaFree(c->diag);
+    c->bytes -= sizeof(double) * c->diag_cap;
+  }
+  c->diag = nullptr;
+  c->diag_cap = 0;
+  int rc = dalloc_ctx(c, (void**)&c->diag, sizeof(double) * need);
+  if (rc) return rc;
+  c->diag_cap = need;
+  return TG_OK;
+}
+
 constexpr int TPB = 256;
 constexpr int kMaxShells = 63;
 
@@ -210,14 +225,8 @@ int et_tables(tg_ctx* c, int Hg, int Fg, const int* Rg, int nrec, const std::vec
   for (int i = 0; i <= A; ++i) rad.r[i] = rho[i];
   const int nb = A + 1;
   const size_t need = (size_t)nrec * (A + 1) * nb;
-  if (c->diag_cap < need) {
-    if (c->diag) cudaFree(c->diag);
-    c->diag = nullptr;
-    c->diag_cap = 0;
-    rc = dalloc_ctx(c, (void**)&c->diag, sizeof(double) * need);
-    if (rc) return rc;
-    c->diag_cap = need;
-  }
+  rc = ensure_diag(c, need);
+  if (rc) return rc;
   cudaError_t e = cudaMemsetAsync(c->diag, 0, sizeof(double) * need, c->st);
   if (e != cudaSuccess) return cuda_err(c, e, "memset");
   // helper H: inverse x, y once (into etWY[0..2])
@@ -278,6 +287,44 @@ int et_table_kind(tg_ctx* c, int kind, std::vector<double>& T, std::vector<doubl
   return et_tables(c, k.H, k.F, Rg, 1, rho, T);
 }
 
+
+// Force feed per shell (Compute_force_feed_shell compute_force_feed.cc:70-76 with
+// Shell_mult_all_FOUR four_ET.cc:181-226): for |K| <= R_in, result[i] += 2 mult Re(F . V*),
+// i = Get_shell_index(|K|).  The force is nonzero on its box only; thread i sums shell i over
+// the box in a fixed order.
+struct ShellRadii {
+  double r[kMaxShells + 1];
+};
+__global__ void k_force_feed(Geo g, const cx<double>* __restrict__ FB, int fx, int fy, int fz,
+                             const cx<double>* __restrict__ u0, const cx<double>* __restrict__ u1,
+                             const cx<double>* __restrict__ u2, ShellRadii R, int S, double kin, double* out) {
+  const int i = threadIdx.x;
+  if (i > S) return;
+  const int ny = 2 * fy + 1, nz = fz + 1, box = (2 * fx + 1) * ny * nz;
+  const cx<double>* U[3] = {u0, u1, u2};
+  double acc = 0;
+  for (int p = 0; p < box; ++p) {
+    const int kz = p % nz, ky = (p / nz) % ny - fy, kx = p / (nz * ny) - fx;
+    const int l1 = kx >= 0 ? kx : kx + g.N1, l2 = ky >= 0 ? ky : ky + g.N2;
+    if (l1 < 0 || l1 >= g.N1 || l2 < 0 || l2 >= g.N2 || kz >= g.nkz) continue;
+    const int r1 = amap_row(g.ax, l1), r2 = amap_row(g.ay, l2);
+    if (r1 < 0 || r2 < 0) continue;
+    const double a = kx * g.kf0, b = ky * g.kf1, c = kz * g.kf2;
+    const double K = sqrt(a * a + b * b + c * c);
+    if (K > kin) continue;
+    int sh = 0;
+    while (sh <= S && !(K <= R.r[sh])) ++sh;
+    if (sh != i) continue;
+    const long long idx = ((long long)r1 * g.nky + r2) * g.kzp + kz;
+    double re = 0;
+    for (int cc = 0; cc < 3; ++cc) {
+      const cx<double> f = FB[(long long)cc * box + p], v = U[cc][idx];
+      re += f.x * v.x + f.y * v.y;
+    }
+    acc += 2 * mult_four(l1, l2, kz, g.N1, g.N2) * re;
+  }
+  out[i] = acc;
+}
 }  // namespace
 
 extern "C" {
@@ -348,6 +395,32 @@ int tg_shell_to_shell(tg_ctx* c, int kind, double* tr, int n) {
       }
     }
   }
+  return TG_OK;
+}
+
+
+int tg_force_feed(tg_ctx* c, double* feed, int n) {
+  if (!c || !feed) return TG_ERR_ARG;
+  const int S = c->cfg.n_shells;
+  if (S < 6 || S > kMaxShells || n < S + 1) return TG_ERR_ARG;
+  if (c->basis != TG_FOUR || c->phys != TG_FLUID)
+    return set_err(c, TG_ERR_UNSUPPORTED, "force feed: FOUR fluid only");
+  for (int i = 0; i < n; ++i) feed[i] = 0;
+  if (!c->force_on) return TG_OK;  // decaying run: the force is zero
+  cudaSetDevice(c->dev);
+  int rc = ensure_force_box(c);
+  if (rc) return rc;
+  const std::vector<double> R = et_radii(c);
+  ShellRadii rr{};
+  for (int i = 0; i <= S; ++i) rr.r[i] = R[i];
+  rc = ensure_diag(c, (size_t)S + 1);
+  if (rc) return rc;
+  double* d = c->diag;
+  k_force_feed<<<1, 64, 0, c->st>>>(c->g, c->FB, c->fx, c->fy, c->fz, c->U0[0], c->U0[1], c->U0[2], rr, S, R[S - 1], d);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(feed, d, sizeof(double) * (S + 1), cudaMemcpyDeviceToHost, c->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+  if (e != cudaSuccess) return cuda_err(c, e, "force feed");
   return TG_OK;
 }
 

@@ -166,6 +166,11 @@ __global__ void __launch_bounds__(256) k_axis_dft(AxisArgs a, PtrSet ps, int L) 
 struct R2RArgs {
   int kind[kMaxPtr];
   const cx<double>* trig;  // (cos, sin)(pi j / 2N), j in [0, 4N)
+  // optional: per kind the transform as a matrix for this launch's row maps, column-major
+  // [stored input row][output row] (output row = destination row), or null
+  const double* mat[4];
+  int mat_rows[4];         // output rows of mat[kind] (= amap_count(out))
+  int mat_cols[4];         // stored input rows of mat[kind] (= amap_count(in))
 };
 
 template <typename Ri, typename Ro, typename Rw>
@@ -229,6 +234,64 @@ __global__ void __launch_bounds__(256) k_axis_r2r(AxisArgs a, PtrSet ps, R2RArgs
       }
     }
     if (ok) dst[(long long)orow * a.dr + col] = cvt<Ro>(sc * acc);
+  }
+}
+
+// The same transforms as a matrix product Y[orow][col] = scale * sum_rr T[rr][orow] X[rr][col]
+// (T real, X complex).  Block: CW columns of one batch and field; thread (lane, warp) owns
+// columns (2 lane, 2 lane + 1) of the tile and output rows r0 .. r0+3 of each row pass, so every
+// k step is one broadcast load of 4 coefficients, one load of 2 columns and 16 FMAs.
+template <typename Ri, typename Ro, typename Rw>
+__global__ void __launch_bounds__(256) k_axis_r2r_mm(AxisArgs a, PtrSet ps, R2RArgs r) {
+  constexpr int CW = 64, TR = 4;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nin = amap_count(a.in);
+  const int f = blockIdx.z;
+  const int kind = r.kind[f];
+  const int nrows = r.mat_rows[kind];
+  const int rpad = (nrows + 8 * TR - 1) / (8 * TR) * (8 * TR);
+  cx<Rw>* X = reinterpret_cast<cx<Rw>*>(smem_raw);               // [nin][CW]
+  Rw* T = reinterpret_cast<Rw*>(X + (size_t)nin * CW);            // [nin][rpad]
+  const int tid = threadIdx.x, lane = tid & 31, wy = tid >> 5;
+  const cx<Ri>* src = reinterpret_cast<const cx<Ri>*>(ps.src[f]) + (long long)blockIdx.y * a.sb;
+  cx<Ro>* dst = reinterpret_cast<cx<Ro>*>(ps.dst[f]) + (long long)blockIdx.y * a.db;
+  const int c0 = blockIdx.x * CW;
+  for (int i = tid; i < nin * CW; i += 256) {
+    const int row = i / CW, w = i % CW;
+    X[i] = (c0 + w < a.ncols) ? cvt<Rw>(src[(long long)row * a.sr + c0 + w]) : mkc<Rw>(0, 0);
+  }
+  const double* M = r.mat[kind];
+  for (int i = tid; i < nin * rpad; i += 256) {
+    const int k = i / rpad, rr = i % rpad;
+    T[i] = rr < nrows ? (Rw)M[(size_t)k * nrows + rr] : (Rw)0;
+  }
+  __syncthreads();
+  const Rw sc = (Rw)a.scale;
+  const int col = c0 + 2 * lane;
+  for (int rb = 0; rb < rpad; rb += 8 * TR) {
+    const int r0 = rb + wy * TR;
+    cx<Rw> acc[TR][2];
+#pragma unroll
+    for (int i = 0; i < TR; ++i) acc[i][0] = acc[i][1] = mkc<Rw>(0, 0);
+    for (int k = 0; k < nin; ++k) {
+      const cx<Rw> x0 = X[k * CW + 2 * lane], x1 = X[k * CW + 2 * lane + 1];
+#pragma unroll
+      for (int i = 0; i < TR; ++i) {
+        const Rw t = T[k * rpad + r0 + i];
+        acc[i][0].x += t * x0.x;
+        acc[i][0].y += t * x0.y;
+        acc[i][1].x += t * x1.x;
+        acc[i][1].y += t * x1.y;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < TR; ++i) {
+      const int orow = r0 + i;
+      if (orow >= nrows) continue;
+      cx<Ro>* d = dst + (long long)orow * a.dr;
+      if (col < a.ncols) d[col] = cvt<Ro>(sc * acc[i][0]);
+      if (col + 1 < a.ncols) d[col + 1] = cvt<Ro>(sc * acc[i][1]);
+    }
   }
 }
 

@@ -6,6 +6,7 @@
 // global memory.  Other lengths run the register-staged k_axis_c2c / k_axis_dft.  Both compute
 // the same butterflies in the same order (equal results up to how the compiler contracts
 // multiply-adds in each kernel).
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 
@@ -255,8 +256,36 @@ cudaError_t run_axis_prec(const AxisLaunch& l, cudaStream_t s) {
   return l.dir < 0 ? run_axis_dir<Ri, Ro, Rw, -1>(l, s) : run_axis_dir<Ri, Ro, Rw, +1>(l, s);
 }
 
+// the matrix-product x-pass when every field's kind has its matrix and the tiles fit
+template <typename Ri, typename Ro, typename Rw>
+cudaError_t run_r2r_mm(const AxisLaunch& l, const R2RArgs& r, cudaStream_t s, bool* used) {
+  *used = false;
+  const int nin = amap_count(l.a.in);
+  int rpad = 0;
+  for (int f = 0; f < l.nfields; ++f) {
+    const int k = r.kind[f];
+    if (k < 0 || k > 3 || !r.mat[k] || r.mat_rows[k] != amap_count(l.a.out) || r.mat_cols[k] != nin)
+      return cudaSuccess;
+    rpad = std::max(rpad, (r.mat_rows[k] + 31) / 32 * 32);
+  }
+  const size_t smem = (size_t)nin * 64 * sizeof(cx<Rw>) + (size_t)nin * rpad * sizeof(Rw);
+  if (smem > 200 * 1024) return cudaSuccess;
+  auto kern = k_axis_r2r_mm<Ri, Ro, Rw>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid((l.a.ncols + 63) / 64, l.nbatch, l.nfields);
+  kern<<<grid, 256, smem, s>>>(l.a, l.ps, r);
+  *used = true;
+  return cudaGetLastError();
+}
+
 template <typename Ri, typename Ro, typename Rw>
 cudaError_t run_r2r(const AxisLaunch& l, const R2RArgs& r, int N, cudaStream_t s) {
+  {
+    bool used = false;
+    cudaError_t e = run_r2r_mm<Ri, Ro, Rw>(l, r, s, &used);
+    if (e != cudaSuccess || used) return e;
+  }
   const int nin = amap_count(l.a.in);
   const size_t smem = (size_t)(4 * N + (size_t)nin * 32) * sizeof(cx<Rw>);
   auto kern = k_axis_r2r<Ri, Ro, Rw>;

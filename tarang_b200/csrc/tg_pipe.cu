@@ -75,6 +75,11 @@ int pipe_inverse_xy(tg_ctx* c, int nf, const void* const* in, const void* const*
       R2RArgs r{};
       for (int f = 0; f < nf; ++f) r.kind[f] = c->xinv_kind[f];
       r.trig = c->trigx;
+      for (int k = 0; k < 4; ++k) {
+        r.mat[k] = c->xmat[k];
+        r.mat_rows[k] = c->xmat_rows[k];
+        r.mat_cols[k] = c->xmat_cols[k];
+      }
       e = launch_r2r(l, r, c->st);
     } else {
       e = launch_axis(l, c->st);
@@ -187,6 +192,11 @@ int pipe_products_forward(tg_ctx* c, int nin, const void* const* WY, int nprod, 
       R2RArgs r{};
       for (int q = 0; q < nprod; ++q) r.kind[q] = c->xfwd_kind[q];
       r.trig = c->trigx;
+      for (int k = 0; k < 4; ++k) {
+        r.mat[k] = c->xmat[k];
+        r.mat_rows[k] = c->xmat_rows[k];
+        r.mat_cols[k] = c->xmat_cols[k];
+      }
       l.a.scale = 0.5;
       e = launch_r2r(l, r, c->st);
     } else {

@@ -50,6 +50,11 @@ struct Batch {
   double* h = nullptr;               // pinned: scal [B][8], red_out [B][8], load rows [B][16]
   std::vector<std::pair<double*, size_t>> loading;  // pinned init blocks of loads in flight
   size_t bytes = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // around the steps of the current round
+  int launched_steps = 0;
+  double step_ms = 0;                // measured time of one step at the current active count
+  int step_ms_nact = 0;
+  double idle_since = -1;            // server clock when the batch last became empty
 };
 
 // Page-locked host blocks, reused by size: initial fields on their way to the device and
@@ -130,6 +135,9 @@ void destroy_batch(tg_server* s, Batch& b) {
     cudaStreamSynchronize(b.c->st);
     for (auto& kv : b.graphs) cudaGraphExecDestroy(kv.second);
     b.graphs.clear();
+    if (b.ev0) cudaEventDestroy(b.ev0);
+    if (b.ev1) cudaEventDestroy(b.ev1);
+    b.ev0 = b.ev1 = nullptr;
     tg_ctx_destroy(b.c);
     b.c = nullptr;
   }
@@ -272,6 +280,20 @@ int open_batch(tg_server* s, const Req& r, long long* bid) {
   return TG_OK;
 }
 
+// release the idle batch that has been idle longest; false if there is none
+bool evict_idle_batch(tg_server* s) {
+  auto victim = s->batches.end();
+  for (auto it = s->batches.begin(); it != s->batches.end(); ++it) {
+    const Batch& b = it->second;
+    if (!b.slot_req.empty() || !b.loading.empty()) continue;
+    if (victim == s->batches.end() || b.idle_since < victim->second.idle_since) victim = it;
+  }
+  if (victim == s->batches.end()) return false;
+  destroy_batch(s, victim->second);
+  s->batches.erase(victim);
+  return true;
+}
+
 // admit queued requests in arrival order into batches with free slots or into new batches
 int admit(tg_server* s) {
   std::vector<long long> still;
@@ -287,6 +309,7 @@ int admit(tg_server* s) {
     }
     if (bid < 0) {
       int rc = open_batch(s, r, &bid);
+      while (rc == TG_ERR_OOM && evict_idle_batch(s)) rc = open_batch(s, r, &bid);
       if (rc == TG_ERR_OOM) {
         if (s->batches.empty()) {
           // nothing resident and still no room: the allocation itself failed
@@ -319,44 +342,75 @@ int admit(tg_server* s) {
 }
 
 // one step of the active slots of batch b, then the slot scalars into pinned memory
-int launch_batch(tg_server* s, Batch& b) {
+// k steps of the active slots of batch b (one graph replay each, captured per active count;
+// the first step of a batch runs eagerly), timed by events on the batch stream, then the slot
+// scalars and energies into pinned memory
+int launch_batch(tg_server* s, Batch& b, int k) {
   tg_ctx* c = b.c;
   const int nact = (int)b.slot_req.size();
   c->nact = nact;
   cudaError_t e;
-  if (s->cfg.use_graphs && b.warmed) {
-    auto it = b.graphs.find(nact);
-    if (it == b.graphs.end()) {
-      cudaGraph_t gr = nullptr;
-      e = cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal);
-      if (e != cudaSuccess) return cuda_err(c, e, "cudaStreamBeginCapture");
-      int rc = enqueue_step(c, false);
-      cudaError_t e2 = cudaStreamEndCapture(c->st, &gr);
-      if (rc) {
-        if (gr) cudaGraphDestroy(gr);
-        return rc;
-      }
-      if (e2 != cudaSuccess) return cuda_err(c, e2, "cudaStreamEndCapture");
-      cudaGraphExec_t ex = nullptr;
-      e = cudaGraphInstantiate(&ex, gr, 0);
-      cudaGraphDestroy(gr);
-      if (e != cudaSuccess) return cuda_err(c, e, "cudaGraphInstantiate");
-      it = b.graphs.emplace(nact, ex).first;
-    }
-    e = cudaGraphLaunch(it->second, c->st);
-    if (e != cudaSuccess) return cuda_err(c, e, "cudaGraphLaunch");
-    s->graph_launches++;
-  } else {
-    int rc = enqueue_step(c, false);
-    if (rc) return rc;
-    b.warmed = true;
-    s->eager_steps++;
+  if (!b.ev0) {
+    if (cudaEventCreate(&b.ev0) != cudaSuccess || cudaEventCreate(&b.ev1) != cudaSuccess)
+      return cuda_err(c, cudaGetLastError(), "cudaEventCreate");
   }
+  e = cudaEventRecord(b.ev0, c->st);
+  if (e != cudaSuccess) return cuda_err(c, e, "cudaEventRecord");
+  for (int step = 0; step < k; ++step) {
+    if (s->cfg.use_graphs && b.warmed) {
+      auto it = b.graphs.find(nact);
+      if (it == b.graphs.end()) {
+        cudaGraph_t gr = nullptr;
+        e = cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return cuda_err(c, e, "cudaStreamBeginCapture");
+        int rc = enqueue_step(c, false);
+        cudaError_t e2 = cudaStreamEndCapture(c->st, &gr);
+        if (rc) {
+          if (gr) cudaGraphDestroy(gr);
+          return rc;
+        }
+        if (e2 != cudaSuccess) return cuda_err(c, e2, "cudaStreamEndCapture");
+        cudaGraphExec_t ex = nullptr;
+        e = cudaGraphInstantiate(&ex, gr, 0);
+        cudaGraphDestroy(gr);
+        if (e != cudaSuccess) return cuda_err(c, e, "cudaGraphInstantiate");
+        it = b.graphs.emplace(nact, ex).first;
+      }
+      e = cudaGraphLaunch(it->second, c->st);
+      if (e != cudaSuccess) return cuda_err(c, e, "cudaGraphLaunch");
+      s->graph_launches++;
+    } else {
+      int rc = enqueue_step(c, false);
+      if (rc) return rc;
+      b.warmed = true;
+      s->eager_steps++;
+    }
+  }
+  e = cudaEventRecord(b.ev1, c->st);
+  if (e != cudaSuccess) return cuda_err(c, e, "cudaEventRecord");
+  b.launched_steps = k;
   e = cudaMemcpyAsync(b.h, c->scal, sizeof(double) * 8 * nact, cudaMemcpyDeviceToHost, c->st);
   if (e != cudaSuccess) return cuda_err(c, e, "slot scalars");
   e = cudaMemcpyAsync(b.h + 8 * (size_t)b.B, c->red_out, sizeof(double) * 8 * nact, cudaMemcpyDeviceToHost, c->st);
   if (e != cudaSuccess) return cuda_err(c, e, "slot energies");
   return TG_OK;
+}
+
+// Steps per round of each batch: the slowest batch runs one, a faster one about as many as fit
+// in that time (at most kMaxStepsPerRound), never past the fewest steps any of its requests
+// still needs.  Until a batch has a measured step time it runs one.
+constexpr int kMaxStepsPerRound = 16;
+
+int steps_this_round(const tg_server* s, const Batch& b, double slowest_ms) {
+  int left = 1 << 30;
+  for (long long id : b.slot_req) {
+    const Req& q = s->reqs.at(id);
+    left = std::min(left, std::max(1, q.n_steps - q.st.steps_done));
+  }
+  int k = 1;
+  if (b.step_ms > 0 && slowest_ms > 0) k = (int)std::floor(slowest_ms / b.step_ms);
+  k = std::max(1, std::min(k, kMaxStepsPerRound));
+  return std::min(k, left);
 }
 
 // after the round: count the step of the first nl slots (those that were launched), retire
@@ -373,6 +427,14 @@ int collect_batch(tg_server* s, Batch& b, int nl, int launch_rc) {
     b.slot_req.clear();
     return code;
   }
+  if (nl > 0 && b.launched_steps > 0) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, b.ev0, b.ev1) == cudaSuccess) {
+      const double per = ms / b.launched_steps;
+      b.step_ms = (b.step_ms_nact == nl && b.step_ms > 0) ? 0.5 * (b.step_ms + per) : per;
+      b.step_ms_nact = nl;
+    }
+  }
   std::vector<int> leave;
   const int n = (int)b.slot_req.size();
   for (int r = 0; r < n; ++r) {
@@ -380,8 +442,9 @@ int collect_batch(tg_server* s, Batch& b, int nl, int launch_rc) {
     if (r < nl) {
       const double* sc = b.h + 8 * (size_t)r;
       const double* ro = b.h + 8 * (size_t)b.B + 8 * (size_t)r;
-      q.st.steps_done++;
-      s->request_steps++;
+      const int now = (int)sc[2];  // the slot's step counter (Get_dt's finalize counts every step)
+      s->request_steps += now - q.st.steps_done;
+      q.st.steps_done = now;
       q.st.t_final = sc[1];
       q.st.final_energy = ro[0] + (c->phys == TG_MHD ? ro[2] : 0.0);
       if (sc[3] != 0.0) {
@@ -408,12 +471,6 @@ int collect_batch(tg_server* s, Batch& b, int nl, int launch_rc) {
     b.slot_req.pop_back();
   }
   return TG_OK;
-}
-
-bool key_queued(const tg_server* s, const std::string& key) {
-  for (long long id : s->queue)
-    if (s->reqs.at(id).key == key) return true;
-  return false;
 }
 
 }  // namespace
@@ -491,11 +548,15 @@ int tg_server_pump(tg_server* s, int* n_active) {
   // launch a step of every resident batch first, so that the host work of admission (copies
   // into pinned blocks, new contexts) overlaps the steps on the device
   std::map<long long, std::pair<int, int>> launched;  // batch -> (slots stepped, launch code)
+  double slowest = 0;
+  for (auto& kv : s->batches)
+    if (!kv.second.slot_req.empty()) slowest = std::max(slowest, kv.second.step_ms);
   for (auto& kv : s->batches) {
     Batch& b = kv.second;
     if (b.slot_req.empty()) continue;
     const int nl = (int)b.slot_req.size();
-    launched[kv.first] = {nl, launch_batch(s, b)};
+    const int k = s->cfg.use_graphs ? steps_this_round(s, b, slowest) : 1;
+    launched[kv.first] = {nl, launch_batch(s, b, k)};
   }
   int first_err = admit(s);
   for (auto& kv : s->batches) {
@@ -508,10 +569,15 @@ int tg_server_pump(tg_server* s, int* n_active) {
     if (r2 && !first_err) first_err = r2;
   }
   if (!launched.empty()) s->rounds++;
-  // release empty batches that no queued request will use
+  // an idle batch stays resident for later requests of its shape (creating and releasing a
+  // context costs far more than a step) until admission needs its memory; a forced request's
+  // batch serves nobody else and goes at once
   for (auto it = s->batches.begin(); it != s->batches.end();) {
-    if (it->second.slot_req.empty() && !key_queued(s, it->second.key)) {
-      destroy_batch(s, it->second);
+    Batch& b = it->second;
+    if (b.slot_req.empty() && b.idle_since < 0) b.idle_since = now_s(s);
+    if (!b.slot_req.empty()) b.idle_since = -1;
+    if (b.slot_req.empty() && b.solo) {
+      destroy_batch(s, b);
       it = s->batches.erase(it);
     } else {
       ++it;

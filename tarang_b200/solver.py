@@ -112,6 +112,15 @@ class IncFluid:
         self._ck(self.lib.tg_field_download(self.h, field, _dptr(out.view(np.float64)), self.ndoubles), "download")
         return out
 
+    def alloc_field(self) -> int:
+        """A reserved work field id (tg_field_alloc); release it with free_field."""
+        f = C.c_int()
+        self._ck(self.lib.tg_field_alloc(self.h, C.byref(f)), "field alloc")
+        return f.value
+
+    def free_field(self, field: int):
+        self._ck(self.lib.tg_field_free(self.h, int(field)), "field free")
+
     def set_V(self, V):
         for i, v in enumerate(V):
             self.upload(L.TG_V1 + i, v)
@@ -252,3 +261,10 @@ class IncFluid:
         t = np.zeros((S + 1) * (S + 1))
         self._ck(self.lib.tg_shell_to_shell(self.h, kind, _dptr(t), S + 1), "shell_tr")
         return t.reshape(S + 1, S + 1)
+
+    def Compute_force_feed_shell(self):
+        """IncVF::Compute_force_feed_shell (compute_force_feed.cc:70-76): forceV_shell, S+1 entries."""
+        S = self.cfg.n_shells
+        f = np.zeros(S + 1)
+        self._ck(self.lib.tg_force_feed(self.h, _dptr(f), S + 1), "force feed")
+        return f

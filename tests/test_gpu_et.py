@@ -60,3 +60,23 @@ def test_mhd_fluxes(lib, kind, spec):
     assert close(s.Compute_flux(kind), o.compute_flux_generic(H, F, R, sign, KF, 8), 1e-10)
     if kind != L.TG_ET_BU:
         assert close(s.Compute_shell_tr(kind), o.compute_shell_tr_generic(H, F, R, sign, KF, 8), 1e-10)
+
+
+@pytest.mark.parametrize("N,S", [((32, 32, 32), 12), ((64, 64, 64), 16)])
+def test_force_feed_shell(lib, N, S):
+    """forceV_shell of Output_flux: 2 mult Re(F . V*) per energy-transfer shell, with the
+    constant-energy-supply force of the current field; zero without forcing."""
+    from tarang_b200.solver import IncFluid
+    V = ic.random_phase_field(N, seed=41)
+    force = dict(inner=2.0, outer=3.0, eps=0.1, eps_h=0.0)
+    s = IncFluid(N, nu=1e-3, dt=5e-4, force=force, n_shells=S)
+    s.set_V(V)
+    s.Compute_force()
+    got = s.Compute_force_feed_shell()
+    F = o.force_const_energy_supply(V, N, KF, 2.0, 3.0, 0.1, 0.0)
+    want = o.force_feed_shell(F, V, KF, S)
+    assert close(got, want, 1e-12)
+    assert np.count_nonzero(want) >= 1
+    d = IncFluid(N, nu=1e-3, dt=5e-4, n_shells=S)
+    d.set_V(V)
+    assert np.all(d.Compute_force_feed_shell() == 0)

@@ -151,7 +151,8 @@ def test_budget_admission(lib):
         assert s["bytes_resident"] == one
         srv.drain()
         s = srv.stats()
-        assert s["bytes_peak"] <= budget and s["n_batches"] == 0
+        assert s["bytes_peak"] <= budget and s["n_running"] == 0 and s["n_queued"] == 0
+        assert s["n_batches"] == 1     # the idle batch stays resident for the next request
         starts = sorted(srv.poll(i)["start_s"] for i in ids)
         finishes = sorted(srv.poll(i)["finish_s"] for i in ids)
         assert starts[1] >= finishes[0] and starts[2] >= finishes[1]
@@ -276,3 +277,27 @@ def test_zero_step_request_returns_stored_fields(lib):
     s = IncFluid(N)
     s.set_V(V)
     assert same_bits(got, s.get_V())
+
+
+def test_idle_batch_evicted_for_new_shape(lib):
+    """An idle batch stays resident for its shape and is released when a request of another
+    shape needs its memory."""
+    from tarang_b200.serving import Server, request_bytes
+    a_cfg = dict(N=(32, 32, 32), nu=2e-3, dt=1e-3)
+    b_cfg = dict(N=(16, 16, 32), nu=2e-3, dt=1e-3)
+    budget = request_bytes(a_cfg, 1) + request_bytes(b_cfg, 1) // 2
+    fa, fb = fluid_fields((32, 32, 32), 801), fluid_fields((16, 16, 32), 802)
+    with Server(hbm_budget=budget, max_batch=4) as srv:
+        a = srv.submit(a_cfg, fa, 4)
+        srv.drain()
+        s = srv.stats()
+        assert s["n_batches"] == 1 and s["bytes_resident"] == request_bytes(a_cfg, 1)
+        b = srv.submit(b_cfg, fb, 4)
+        srv.drain()
+        s = srv.stats()
+        assert s["n_batches"] == 1 and s["bytes_resident"] == request_bytes(b_cfg, 1)
+        assert s["bytes_peak"] <= budget
+        for rid, cfg, f in ((a, a_cfg, fa), (b, b_cfg, fb)):
+            assert srv.poll(rid)["state"] == "done"
+            want, _, _ = lone(cfg, f, 4)
+            assert same_bits(srv.result(rid), want)

@@ -74,3 +74,33 @@ def test_round_trip_identity_256(lib):
     spec = s.Forward_transform_array(o.pack_real(real))
     back = o.unpack_real(s.Inverse_transform_array(spec))
     assert np.abs(back - real).max() < 1e-13
+
+
+def test_field_alloc_free(lib):
+    """tg_field_alloc reserves distinct zeroed work fields usable by the transforms; the ninth
+    reservation is TG_ERR_BUSY; tg_field_free returns the slot and its memory."""
+    from tarang_b200 import _lib as L
+    from tarang_b200.solver import IncFluid
+    N = (16, 16, 16)
+    s = IncFluid(N)
+    base = s.device_bytes()
+    ids = [s.alloc_field() for _ in range(L.TG_NWORK)]
+    assert sorted(ids) == list(range(L.TG_WORK0, L.TG_WORK0 + L.TG_NWORK))
+    assert s.device_bytes() == base + L.TG_NWORK * 16 * N[0] * N[1] * (N[2] // 2 + 1)
+    with pytest.raises(L.TarangError) as e:
+        s.alloc_field()
+    assert e.value.code == L.TG_ERR_BUSY
+    assert np.all(s.download(ids[3]) == 0)
+    rng = np.random.default_rng(2)
+    real = rng.standard_normal(N)
+    s.upload(ids[3], o.pack_real(real))
+    s._ck(s.lib.tg_forward_transform(s.h, ids[3], 0), "forward")
+    want = o.forward_four(real)
+    assert np.abs(s.download(ids[3]) - want).max() < 1e-13 * np.abs(want).max()
+    for f in ids:
+        s.free_field(f)
+    assert s.device_bytes() == base
+    with pytest.raises(L.TarangError):
+        s.free_field(ids[0])
+    again = s.alloc_field()
+    assert again == L.TG_WORK0 and np.all(s.download(again) == 0)
