@@ -30,7 +30,9 @@ struct Req {
   tg_config cfg{};
   int n_steps = 0;
   int nstate = 3;
-  std::vector<double> init;    // dropped at admission
+  std::vector<double> init;    // dropped at admission (when the pinned pool was full at submit)
+  double* init_pin = nullptr;  // pinned block of the pool holding the fields (usual case)
+  size_t n_init = 0;
   double* result = nullptr;    // pinned block of the pool, kept when keep_results
   size_t n_result = 0;
   tg_request_status st{};
@@ -62,6 +64,7 @@ struct Batch {
 struct PinnedPool {
   std::map<size_t, std::vector<double*>> free_;
   size_t held = 0;
+  static constexpr size_t kCap = (size_t)16 << 30;  // page-locked bytes held at most
   double* get(size_t n) {
     auto it = free_.find(n);
     if (it != free_.end() && !it->second.empty()) {
@@ -70,6 +73,7 @@ struct PinnedPool {
       return p;
     }
     void* p = nullptr;
+    if (held + sizeof(double) * n > kCap) return nullptr;
     if (cudaMallocHost(&p, sizeof(double) * n) != cudaSuccess) {
       cudaGetLastError();
       return nullptr;
@@ -156,6 +160,8 @@ void finish_req(tg_server* s, Req& r, int state, int error) {
   r.st.finish_s = now_s(s);
   r.batch = -1;
   std::vector<double>().swap(r.init);
+  if (r.init_pin) s->pinned.put(r.init_pin, r.n_init);
+  r.init_pin = nullptr;
 }
 
 // Enqueue, on the batch stream, the copy of a request's fields into slot `slot` and the set-up
@@ -165,11 +171,16 @@ int load_slot(tg_server* s, Batch& b, int slot, Req& r) {
   tg_ctx* c = b.c;
   const size_t D2 = 2 * (size_t)c->D;
   const size_t n = D2 * c->nstate;
-  double* pin = s->pinned.get(n);
-  if (!pin) return set_err(c, TG_ERR_OOM, "pinned host block for a request's fields");
-  std::memcpy(pin, r.init.data(), sizeof(double) * n);
+  double* pin = r.init_pin;
+  if (pin) {
+    r.init_pin = nullptr;  // from here on the batch releases it (after the copies ran)
+  } else {
+    pin = s->pinned.get(n);
+    if (!pin) return set_err(c, TG_ERR_OOM, "pinned host block for a request's fields");
+    std::memcpy(pin, r.init.data(), sizeof(double) * n);
+    std::vector<double>().swap(r.init);
+  }
   b.loading.emplace_back(pin, n);
-  std::vector<double>().swap(r.init);
   cudaError_t e;
   for (int i = 0; i < c->nstate; ++i) {
     e = cudaMemcpyAsync(c->staging, pin + (size_t)i * D2, sizeof(double) * D2, cudaMemcpyHostToDevice, c->st);
@@ -504,6 +515,8 @@ int tg_server_destroy(tg_server* s) {
   for (auto& kv : s->batches) destroy_batch(s, kv.second);
   for (auto& kv : s->reqs)
     if (kv.second.result) cudaFreeHost(kv.second.result);
+  for (auto& kv : s->reqs)
+    if (kv.second.init_pin) cudaFreeHost(kv.second.init_pin);
   s->pinned.clear();
   delete s;
   return TG_OK;
@@ -534,7 +547,12 @@ int tg_server_submit(tg_server* s, const tg_request* rq, long long* id) {
     r.st.finish_s = r.st.submit_s;
     s->finished.push_back(r.id);
   } else {
-    r.init.assign(rq->init, rq->init + rq->n_doubles);
+    // into a reused page-locked block when the pool has room (no page faults, and the upload
+    // at admission is a plain asynchronous copy), else into ordinary memory
+    r.n_init = rq->n_doubles;
+    r.init_pin = s->pinned.get(r.n_init);
+    if (r.init_pin) std::memcpy(r.init_pin, rq->init, sizeof(double) * r.n_init);
+    else r.init.assign(rq->init, rq->init + rq->n_doubles);
     s->queue.push_back(r.id);
   }
   *id = r.id;
