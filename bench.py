@@ -43,6 +43,7 @@ def parse(argv=None):
     p.add_argument("--err-steps", type=int, default=100)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-configs", action="store_true", help="skip the MHD and convection sections")
     p.add_argument("--serve-requests", type=int, default=512,
                    help="requests of the serving ensemble (0: skip it)")
     p.add_argument("--serve-steps", type=int, default=200)
@@ -194,16 +195,35 @@ def run_reference(args, rank, world):
 
 
 # --------------------------------------------------------------------------------- own arm
-def run_form(torch, lib_mod, N, precision, steps, warmup, stream, V, dist):
+def set_fields(s, fields):
+    """V, then W (MHD) or T (scalar, convection)."""
+    s.set_V(fields[:3])
+    if len(fields) == 6:
+        s.set_W(fields[3:])
+    elif len(fields) == 4:
+        s.set_T(fields[3])
+
+
+def get_fields(s, n):
+    out = s.get_V()
+    if n == 6:
+        out += s.get_W()
+    elif n == 4:
+        out.append(s.get_T())
+    return out
+
+
+def run_form(torch, N, steps, warmup, stream, fields, dist, **kw):
+    """Device time of `steps` RK4 steps (one CUDA graph each) of one solve, CUDA events on the
+    context's stream, barriers around it; then the same number of steps again with per-launch
+    events (eager) for the per-kernel breakdown, outside the timed region."""
     import ctypes as C
     from tarang_b200 import _lib as L
     from tarang_b200.solver import IncFluid
     # the context queues on the torch stream so the CUDA events see its kernels
-    s = IncFluid(N, nu=NU, dt=DT, force=FORCE, precision=precision, stream=stream.cuda_stream)
-    s.set_V(V)
+    s = IncFluid(N, stream=stream.cuda_stream, **kw)
+    set_fields(s, fields)
     s.step(warmup)
-    s.lib.tg_profile_enable(s.h, 1)
-    s.lib.tg_profile_read(s.h, None, 0, None)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     if dist:
@@ -216,6 +236,9 @@ def run_form(torch, lib_mod, N, precision, steps, warmup, stream, V, dist):
     if dist:
         torch.distributed.barrier()
     ms = ev0.elapsed_time(ev1)
+    s.lib.tg_profile_enable(s.h, 1)
+    s.lib.tg_profile_read(s.h, None, 0, None)
+    s.lib.tg_step(s.h, steps, None)
     stats = (L.tg_kernel_stat * 32)()
     n = C.c_int()
     s.lib.tg_profile_read(s.h, stats, 32, C.byref(n))
@@ -223,6 +246,48 @@ def run_form(torch, lib_mod, N, precision, steps, warmup, stream, V, dist):
     kern = [{"name": stats[i].name.decode(), "launches": stats[i].launches, "total_ms": stats[i].total_ms,
              "bytes_per_launch": stats[i].bytes_per_launch} for i in range(n.value)]
     return s, ms, kern
+
+
+def rel_max(a, b):
+    """max |a - b| / max |b| (0 when both vanish)."""
+    import numpy as np
+    a, b = np.asarray(a), np.asarray(b)
+    d = float(np.abs(b).max())
+    return float(np.abs(a - b).max()) / d if d > 0 else float(np.abs(a).max())
+
+
+def diag_errors(s32, s64, groups=(0,), et_kinds=(0,), force_feed=False):
+    """FP32-mixed against FP64 for the diagnostics of the current fields: energy per group,
+    shell spectra (energy, dissipation), fluxes and shell-to-shell tables per transfer kind."""
+    from tarang_b200 import _lib as L
+    out = {}
+    for g in groups:
+        e32, d32 = s32.CV_Compute_totalenergy_diss(g)
+        e64, d64 = s64.CV_Compute_totalenergy_diss(g)
+        out[f"energy_g{g}"] = abs(e32 - e64) / abs(e64)
+        out[f"dissipation_g{g}"] = abs(d32 - d64) / abs(d64)
+        k32, dk32 = s32.CV_Compute_shell_spectrum(g)
+        k64, dk64 = s64.CV_Compute_shell_spectrum(g)
+        out[f"spectrum_g{g}_max_shell_rel"] = rel_max(k32, k64)
+        out[f"dissipation_spectrum_g{g}_max_shell_rel"] = rel_max(dk32, dk64)
+    names = {L.TG_ET_UU: "UU", L.TG_ET_BB: "BB", L.TG_ET_UB: "UB", L.TG_ET_BU: "BU"}
+    for k in et_kinds:
+        out[f"flux_{names[k]}_max_shell_rel"] = rel_max(s32.Compute_flux(k), s64.Compute_flux(k))
+        out[f"shell_to_shell_{names[k]}_max_rel"] = rel_max(s32.Compute_shell_tr(k), s64.Compute_shell_tr(k))
+    if force_feed:
+        out["force_feed_max_shell_rel"] = rel_max(s32.Compute_force_feed_shell(), s64.Compute_force_feed_shell())
+    return out
+
+
+def et_timing(s, kinds, reps=3):
+    """Wall time of the flux and shell-to-shell tables of every kind (synchronous calls)."""
+    s.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        for k in kinds:
+            s.Compute_flux(k)
+            s.Compute_shell_tr(k)
+    return 1e3 * (time.perf_counter() - t0) / reps
 
 
 def rel_l2(a, b):
@@ -279,12 +344,14 @@ def run_own(args, rank, world, local):
     out = {}
     with torch.cuda.stream(stream):
         with Clocks(dev) as clk:
-            s64, ms64, k64 = run_form(torch, L, N, "FP64", args.steps, args.warmup, stream, V, dist)
-            s32, ms32, k32 = run_form(torch, L, N, "FP32", args.steps, args.warmup, stream, V, dist)
+            kw = dict(nu=NU, dt=DT, force=FORCE, n_shells=16)
+            s64, ms64, k64 = run_form(torch, N, args.steps, args.warmup, stream, V, dist, precision="FP64", **kw)
+            s32, ms32, k32 = run_form(torch, N, args.steps, args.warmup, stream, V, dist, precision="FP32", **kw)
         clocks = clk.summary()
     ms64, ms32 = max_over_ranks([ms64, ms32], dist)
     # FP32-mixed error against the FP64 form after err_steps steps (outside the timed region)
     err = None
+    diag_err, et_ms = None, None
     if args.err_steps > 0:
         s64.set_V(V)
         s32.set_V(V)
@@ -294,16 +361,22 @@ def run_own(args, rank, world, local):
         err = rel_l2(a, b)
         E64 = s64.CV_Compute_totalenergy_diss()[0]
         E32 = s32.CV_Compute_totalenergy_diss()[0]
+        diag_err = diag_errors(s32, s64, force_feed=True)
+        et_ms = {"fp64": et_timing(s64, (0,)), "fp32": et_timing(s32, (0,))}
     e2e = None
     if not args.no_e2e:
         e2e = e2e_measure(s64, V, max(3, min(args.steps, 20)))
         # whole job: the steps of all ranks over the slowest rank's wall time
         (el,) = max_over_ranks([e2e["steps"] / e2e["value"]], dist)
         e2e["value"] = world * e2e["steps"] / el
+    s64.close()
+    s32.close()
+    configs = None
+    if rank == 0 and not args.no_configs:
+        with torch.cuda.stream(stream):
+            configs = run_configs(args, torch, stream)
     serving = None
     if args.serve_requests > 0:
-        s64.close()
-        s32.close()
         serving = run_serving(args, rank, world, dist)
     if rank != 0:
         if dist:
@@ -342,14 +415,19 @@ def run_own(args, rank, world, local):
         "fp32_mixed": {"value": v32, "ms_per_step": ms32 / steps, "speedup_vs_fp64": v32 / v64,
                        "rel_l2_err_vs_fp64": err, "err_steps": args.err_steps,
                        "energy_rel_err_vs_fp64": (abs(E32 - E64) / abs(E64)) if err is not None else None,
+                       "diagnostics_err_vs_fp64": diag_err,
                        "roofline": roof(k32, ms32, steps, f"fluid{n}_fp32")},
         "step_bandwidth": {"convention_bytes_per_step_fp64": b64, "convention_bytes_per_step_fp32": b32,
                            "fp64_GBps": b64 * v64 / world / 1e9, "fp32_GBps": b32 * v32 / world / 1e9},
+        "energy_transfer_ms": ({"shells": 16, "what": "flux + shell-to-shell tables (UU), one call each",
+                                **et_ms} if et_ms else None),
         "kernels_fp64": k64, "kernels_fp32": k32,
         "clocks": clocks,
     }
     if e2e:
         line["e2e"] = e2e
+    if configs is not None:
+        line["configs"] = configs
     if serving is not None:
         line["serving"] = serving
     if not args.no_cpu_baseline:
@@ -358,6 +436,69 @@ def run_own(args, rank, world, local):
     if dist:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
+
+
+# --------------------------------------------------------------------------------- other configs
+def run_configs(args, torch, stream):
+    """The MHD (256^3) and Rayleigh-Benard (SCFT, N1 = 129 and 128 by 256 x 256) workloads on one
+    GPU: device-timed steps/s of the FP64 and FP32-mixed forms and the FP32-mixed error of every
+    field, spectrum and transfer after err_steps steps (synthetic seeded initial fields)."""
+    import numpy as np
+    from tarang_b200 import _lib as L
+    from tarang_b200 import ic
+    out = {}
+    steps, warm = max(3, min(args.steps, 20)), args.warmup
+    es = max(1, min(args.err_steps, 100))
+    # MHD 256^3: u, b random phase E(k) ~ k^4 exp(-2 (k/3)^2), E_u = E_b = 0.5; nu = eta = 1e-3
+    n = args.size
+    N = (n, n, n)
+    f = ic.random_phase_field(N, k0=3.0, energy=0.5, seed=20261203) + \
+        ic.random_phase_field(N, k0=3.0, energy=0.5, seed=20261204)
+    kw = dict(physics="MHD", nu=1e-3, eta=1e-3, dt=5e-4, n_shells=16)
+    s64, ms64, _ = run_form(torch, N, steps, warm, stream, f, False, precision="FP64", **kw)
+    s32, ms32, _ = run_form(torch, N, steps, warm, stream, f, False, precision="FP32", **kw)
+    for s_ in (s64, s32):
+        set_fields(s_, f)
+        s_.step(es, energies=False)
+    kinds = (L.TG_ET_UU, L.TG_ET_BB, L.TG_ET_UB, L.TG_ET_BU)
+    out["mhd"] = {
+        "workload": f"incompressible MHD {n}^3 FOUR, u and b random phase k^4 exp(-2 (k/3)^2), E_u = E_b = 0.5, "
+                    "nu = eta = 1e-3, dt = 5e-4, RK4; fluxes U->U, B->B, U<->B over 16 shells",
+        "steps_per_s_fp64": 1e3 * steps / ms64, "steps_per_s_fp32": 1e3 * steps / ms32,
+        "fp32_speedup": ms64 / ms32, "err_steps": es,
+        "rel_l2_err_vs_fp64": {"u": rel_l2(s32.get_V(), s64.get_V()), "b": rel_l2(s32.get_W(), s64.get_W())},
+        "diagnostics_err_vs_fp64": diag_errors(s32, s64, groups=(0, 1), et_kinds=kinds),
+        "energy_transfer_ms": {"fp64": et_timing(s64, kinds, 1), "fp32": et_timing(s32, kinds, 1),
+                               "what": "flux + shell-to-shell tables of the 4 kinds"},
+    }
+    s64.close()
+    s32.close()
+    # Rayleigh-Benard: SCFT, aspect 1 : 2 sqrt 2 : 2 sqrt 2, Ra = 1e6, Pr = 1, dt = 1e-4, at rest
+    # plus a temperature perturbation of amplitude 1e-3 in the lowest 8 modes
+    for n1 in (129, 128):
+        N = (n1, 2 * (n // 2), 2 * (n // 2))
+        shape = (N[0], N[1], N[2] // 2 + 1)
+        f = [np.zeros(shape, dtype=np.complex128) for _ in range(3)] + [ic.rb_perturbation(N, seed=20261205)]
+        kw = dict(basis="SCFT", physics="RB", Ra=1e6, Pr=1.0, dt=1e-4, kfactor=KF_RB)
+        s64, ms64, _ = run_form(torch, N, steps, warm, stream, f, False, precision="FP64", **kw)
+        s32, ms32, _ = run_form(torch, N, steps, warm, stream, f, False, precision="FP32", **kw)
+        for s_ in (s64, s32):
+            set_fields(s_, f)
+            s_.step(es, energies=False)
+        nu64, nu32 = s64.Get_Nusselt_no(), s32.Get_Nusselt_no()
+        t32, _ = s32.CV_Compute_shell_spectrum(2)
+        t64, _ = s64.CV_Compute_shell_spectrum(2)
+        out[f"rb_{n1}"] = {
+            "workload": f"Rayleigh-Benard SCFT {N[0]}x{N[1]}x{N[2]}, Ra = 1e6, Pr = 1, dt = 1e-4, RK4",
+            "steps_per_s_fp64": 1e3 * steps / ms64, "steps_per_s_fp32": 1e3 * steps / ms32,
+            "fp32_speedup": ms64 / ms32, "err_steps": es,
+            "rel_l2_err_vs_fp64": {"u": rel_l2(s32.get_V(), s64.get_V()), "theta": rel_l2([s32.get_T()], [s64.get_T()])},
+            "nusselt": {"fp64": nu64, "fp32": nu32, "rel_err": abs(nu32 - nu64) / abs(nu64)},
+            "theta_spectrum_max_shell_rel": rel_max(t32, t64),
+        }
+        s64.close()
+        s32.close()
+    return out
 
 
 # --------------------------------------------------------------------------------- serving

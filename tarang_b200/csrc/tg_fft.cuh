@@ -238,12 +238,13 @@ __global__ void __launch_bounds__(256) k_axis_r2r(AxisArgs a, PtrSet ps, R2RArgs
 }
 
 // The same transforms as a matrix product Y[orow][col] = scale * sum_rr T[rr][orow] X[rr][col]
-// (T real, X complex).  Block: CW columns of one batch and field; thread (lane, warp) owns
-// columns (2 lane, 2 lane + 1) of the tile and output rows r0 .. r0+3 of each row pass, so every
-// k step is one broadcast load of 4 coefficients, one load of 2 columns and 16 FMAs.
-template <typename Ri, typename Ro, typename Rw>
+// (T real, X complex).  Block: CW (64 or 32) columns of one batch and field; thread (lane, warp)
+// owns CW/32 adjacent columns of the tile and output rows r0 .. r0+3 of each row pass, so every
+// k step is a broadcast load of 4 coefficients, a load of its columns and 8 or 16 FMAs.
+template <typename Ri, typename Ro, typename Rw, int CW>
 __global__ void __launch_bounds__(256) k_axis_r2r_mm(AxisArgs a, PtrSet ps, R2RArgs r) {
-  constexpr int CW = 64, TR = 4;
+  constexpr int TR = 4;
+  constexpr int CL = CW / 32;  // columns per lane: 2 (64-column tiles) or 1 (32)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int nin = amap_count(a.in);
   const int f = blockIdx.z;
@@ -267,21 +268,26 @@ __global__ void __launch_bounds__(256) k_axis_r2r_mm(AxisArgs a, PtrSet ps, R2RA
   }
   __syncthreads();
   const Rw sc = (Rw)a.scale;
-  const int col = c0 + 2 * lane;
+  const int col = c0 + CL * lane;
   for (int rb = 0; rb < rpad; rb += 8 * TR) {
     const int r0 = rb + wy * TR;
-    cx<Rw> acc[TR][2];
+    cx<Rw> acc[TR][CL];
 #pragma unroll
-    for (int i = 0; i < TR; ++i) acc[i][0] = acc[i][1] = mkc<Rw>(0, 0);
+    for (int i = 0; i < TR; ++i)
+#pragma unroll
+      for (int q = 0; q < CL; ++q) acc[i][q] = mkc<Rw>(0, 0);
     for (int k = 0; k < nin; ++k) {
-      const cx<Rw> x0 = X[k * CW + 2 * lane], x1 = X[k * CW + 2 * lane + 1];
+      cx<Rw> x[CL];
+#pragma unroll
+      for (int q = 0; q < CL; ++q) x[q] = X[k * CW + CL * lane + q];
 #pragma unroll
       for (int i = 0; i < TR; ++i) {
         const Rw t = T[k * rpad + r0 + i];
-        acc[i][0].x += t * x0.x;
-        acc[i][0].y += t * x0.y;
-        acc[i][1].x += t * x1.x;
-        acc[i][1].y += t * x1.y;
+#pragma unroll
+        for (int q = 0; q < CL; ++q) {
+          acc[i][q].x += t * x[q].x;
+          acc[i][q].y += t * x[q].y;
+        }
       }
     }
 #pragma unroll
@@ -289,8 +295,9 @@ __global__ void __launch_bounds__(256) k_axis_r2r_mm(AxisArgs a, PtrSet ps, R2RA
       const int orow = r0 + i;
       if (orow >= nrows) continue;
       cx<Ro>* d = dst + (long long)orow * a.dr;
-      if (col < a.ncols) d[col] = cvt<Ro>(sc * acc[i][0]);
-      if (col + 1 < a.ncols) d[col + 1] = cvt<Ro>(sc * acc[i][1]);
+#pragma unroll
+      for (int q = 0; q < CL; ++q)
+        if (col + q < a.ncols) d[col + q] = cvt<Ro>(sc * acc[i][q]);
     }
   }
 }

@@ -268,12 +268,18 @@ cudaError_t run_r2r_mm(const AxisLaunch& l, const R2RArgs& r, cudaStream_t s, bo
       return cudaSuccess;
     rpad = std::max(rpad, (r.mat_rows[k] + 31) / 32 * 32);
   }
-  const size_t smem = (size_t)nin * 64 * sizeof(cx<Rw>) + (size_t)nin * rpad * sizeof(Rw);
+  // 64-column tiles when they fit in shared memory, else 32
+  int cw = 64;
+  size_t smem = (size_t)nin * cw * sizeof(cx<Rw>) + (size_t)nin * rpad * sizeof(Rw);
+  if (smem > 200 * 1024) {
+    cw = 32;
+    smem = (size_t)nin * cw * sizeof(cx<Rw>) + (size_t)nin * rpad * sizeof(Rw);
+  }
   if (smem > 200 * 1024) return cudaSuccess;
-  auto kern = k_axis_r2r_mm<Ri, Ro, Rw>;
+  auto kern = cw == 64 ? k_axis_r2r_mm<Ri, Ro, Rw, 64> : k_axis_r2r_mm<Ri, Ro, Rw, 32>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  dim3 grid((l.a.ncols + 63) / 64, l.nbatch, l.nfields);
+  dim3 grid((l.a.ncols + cw - 1) / cw, l.nbatch, l.nfields);
   kern<<<grid, 256, smem, s>>>(l.a, l.ps, r);
   *used = true;
   return cudaGetLastError();

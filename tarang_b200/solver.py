@@ -268,3 +268,9 @@ class IncFluid:
         f = np.zeros(S + 1)
         self._ck(self.lib.tg_force_feed(self.h, _dptr(f), S + 1), "force feed")
         return f
+
+    def Get_Nusselt_no(self) -> float:
+        """IncVF::Get_Nusselt_no (nusselt.cc:53-89): Nu = 1 + 2 sqrt(Ra Pr) <u1, theta>."""
+        v = C.c_double()
+        self._ck(self.lib.tg_nusselt(self.h, C.byref(v)), "nusselt")
+        return v.value
