@@ -59,6 +59,11 @@ extern "C" {
 #define TG_FORCE_ENERGY_SUPPLY 1
 #define TG_FORCE_RB 51
 
+#define TG_RB_PRLARGE 0
+#define TG_RB_PRSMALL 1
+#define TG_RB_ULARGE 0
+#define TG_RB_USMALL 1
+
 /* field ids (dense, reference layout) */
 #define TG_V1 0 /* U.V1..V3 */
 #define TG_V2 1
@@ -104,9 +109,15 @@ typedef struct tg_config {
   int force_kind;     /* TG_FORCE_* */
   double force_para[4]; /* energy supply: inner radius, outer radius, epsilon, eps_h/(k eps) */
   int n_shells;       /* energy transfer: no_shells (= no_spheres), scheme 0 radii */
-  double rb_ra, rb_pr;  /* Rayleigh and Prandtl numbers (RB, PRLARGE + ULARGE) */
+  double rb_ra, rb_pr;  /* Rayleigh and Prandtl numbers (RB) */
   int device;         /* CUDA device ordinal */
   void* stream;       /* cudaStream_t to queue on; NULL: the context creates one */
+  /* RB nondimensionalisation (RB_slip_main.cc:222-262, compute_force_RB.cc:50-105):
+   * Pr_switch TG_RB_PRLARGE / TG_RB_PRSMALL, RB_Uscaling TG_RB_ULARGE / TG_RB_USMALL, and
+   * temperature_grad (+1 convection, -1 stable stratification; solver_double_para(6)) */
+  int rb_pr_switch;
+  int rb_u_scaling;
+  double rb_temp_grad;
 } tg_config;
 
 typedef struct tg_ctx tg_ctx;
@@ -133,6 +144,23 @@ int tg_field_copy(tg_ctx* ctx, int dst_field, int src_field);
  * TG_ERR_BUSY when all eight are reserved.  tg_field_free releases the slot and its memory. */
 int tg_field_alloc(tg_ctx* ctx, int* field);
 int tg_field_free(tg_ctx* ctx, int field);
+
+/* Field files in the reference's text format (host memory, no context; the solver mirror moves
+ * fields between them and a context).  tg_write_field_file: IncFluid::Output_field
+ * (lib/IncFluid/output/output_field.cc:43-108) with Write_data_MPI / Write_data_kz0plane_MPI
+ * (lib/fields/array_fn/array_basic.cc:814-898): "%% Time = t", then each field as "(re,im) " per
+ * mode in [l1][l2][l3] order at 12 significant digits, two newlines after each.  fields are the
+ * state fields in reference order (V1 V2 V3, then W1 W2 W3 or T), each 2*N1*N2*(N3/2+1) doubles;
+ * vx_vy = 1 (output_vx_vy_switch) writes the kz = 0 plane only of V3 (and W3).  append = 1 adds
+ * to an existing file.
+ * tg_read_field_file: IncFluid::Init_cond (lib/IncFluid/input/init_cond_field.cc:47-88, 179-223)
+ * with Read_data_MPI (array_basic.cc:294-383); lines starting with '%' are skipped; with vx_vy = 1
+ * V3 (and W3) for kz >= 1 come from incompressibility (IncVF::Last_component
+ * lib/IncFlow/misc/field_k_fns.cc:79-87).  TG_ERR_ARG on a short or malformed file. */
+int tg_write_field_file(const char* path, double time, const int N[3], int n_fields,
+                        const double* const* fields, int vx_vy, int append);
+int tg_read_field_file(const char* path, const int N[3], int basis, const double kfactor[3], int n_fields,
+                       double* const* fields, int vx_vy);
 
 /* Forward_transform_array / Inverse_transform_array (universal_tr.cc:66-146) on a work field,
  * in place.  parity: 0 cos/even, 1 sin/odd (SCFT only; ignored for FOUR). */

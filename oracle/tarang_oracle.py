@@ -721,19 +721,37 @@ class MHDSolver(FluidSolver):
         return u, b, dt
 
 
+def rb_coefficients(Ra, Pr, pr_switch="PRLARGE", u_scaling="ULARGE", temperature_grad=1.0):
+    """(nu, kappa, fu, ft, nuf) of a Rayleigh-Benard nondimensionalisation:
+    RB_slip_main.cc:222-262 (nu = coefficient of grad^2 u, kappa of grad^2 theta),
+    compute_force_RB.cc:50-105 (Force1 = fu theta, T.Force = ft u1) and nusselt.cc:53-89
+    (Nu = 1 + nuf <u1, theta>)."""
+    small = u_scaling == "USMALL"
+    if pr_switch == "PRSMALL":
+        return ((1.0 if small else math.sqrt(Pr / Ra)), (1.0 / Pr if small else 1.0 / math.sqrt(Pr * Ra)),
+                (Ra if small else Pr), temperature_grad / Pr,
+                (2 * Pr * Pr if small else 2 * Pr * math.sqrt(Ra * Pr)))
+    if pr_switch == "PRLARGE":
+        return ((Pr if small else math.sqrt(Pr / Ra)), (1.0 if small else 1.0 / math.sqrt(Pr * Ra)),
+                (Ra * Pr if small else 1.0), temperature_grad,
+                (2.0 if small else 2 * math.sqrt(Ra * Pr)))
+    raise ValueError(pr_switch)
+
+
 class RBSolver:
-    """Rayleigh-Benard convection (RB_SLIP, Pr_switch PRLARGE, RB_Uscaling ULARGE):
-    src/RBslip/RB_slip_main.cc:236-240 (nu = sqrt(Pr/Ra), kappa = 1/sqrt(Pr Ra)) and the loop
-    :365-400; Compute_force_RB compute_force_RB.cc:51-105 (Force1 = theta, T.Force =
-    temperature_grad * u1); Compute_nlin(T) -> Compute_nlin_scalar compute_nlin_SF.cc:80-177 with
-    Dealias_nlin(T); IF-RK4 of time_advance_SF.cc for u (nu) and theta (kappa); Get_dt(T) = Get_dt().
+    """Rayleigh-Benard convection (RB_SLIP; Pr_switch PRLARGE or PRSMALL, RB_Uscaling ULARGE or
+    USMALL, rb_coefficients) and the loop src/RBslip/RB_slip_main.cc:365-400; Compute_force_RB
+    compute_force_RB.cc:51-105 (Force1 = fu theta, T.Force = ft u1); Compute_nlin(T) ->
+    Compute_nlin_scalar compute_nlin_SF.cc:80-177 with Dealias_nlin(T); IF-RK4 of
+    time_advance_SF.cc for u (nu) and theta (kappa); Get_dt(T) = Get_dt().
     Fields: V = [u1 (sin), u2 (cos), u3 (cos)], T = theta (sin) in the SCFT basis."""
 
-    def __init__(self, N, kfactor, Ra, Pr, Tdt, basis="SCFT", alias="DEALIAS", temperature_grad=1.0):
+    def __init__(self, N, kfactor, Ra, Pr, Tdt, basis="SCFT", alias="DEALIAS", temperature_grad=1.0,
+                 pr_switch="PRLARGE", u_scaling="ULARGE"):
         self.N = tuple(N)
         self.kfactor = tuple(kfactor)
-        self.nu = math.sqrt(Pr / Ra)
-        self.kappa = 1.0 / math.sqrt(Pr * Ra)
+        self.nu, self.kappa, self.fu, self.ft, self.nuf = rb_coefficients(Ra, Pr, pr_switch, u_scaling,
+                                                                         temperature_grad)
         self.Ra, self.Pr = Ra, Pr
         self.Tdt = Tdt
         self.basis = basis
@@ -743,8 +761,8 @@ class RBSolver:
     def rhs(self, V, T):
         nl = nlin_fluid(V, self.kfactor, self.basis, self.alias)
         tn = nlin_scalar(V, T, self.kfactor, self.basis, self.alias, dealias_T=True)
-        F1 = T
-        TF = self.tg * V[0]
+        F1 = self.fu * T
+        TF = self.ft * V[0]
         if self.alias == "DEALIAS":     # Dealias_force(T)
             F1 = dealias(F1, self.basis)
             TF = dealias(TF, self.basis)
@@ -788,8 +806,9 @@ class RBSolver:
         return u, t, dt
 
     def nusselt(self, V, T):
-        """Get_Nusselt_no  nusselt.cc:53-89, PRLARGE + ULARGE: 1 + 2 sqrt(Ra Pr) <u1, theta>."""
-        return 1 + 2 * math.sqrt(self.Ra * self.Pr) * total_energy(V[0], self.basis, T)
+        """Get_Nusselt_no  nusselt.cc:53-89: 1 + nuf <u1, theta> (PRLARGE + ULARGE: nuf =
+        2 sqrt(Ra Pr))."""
+        return 1 + self.nuf * total_energy(V[0], self.basis, T)
 
 
 # --------------------------------------------------------------------------------------

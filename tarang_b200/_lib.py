@@ -26,6 +26,8 @@ TG_FLUID, TG_MHD, TG_SCALAR, TG_RB = 0, 1, 2, 3
 TG_FP64, TG_FP32_MIXED = 0, 1
 TG_RK4 = 4
 TG_FORCE_DECAY, TG_FORCE_ENERGY_SUPPLY, TG_FORCE_RB = 0, 1, 51
+TG_RB_PRLARGE, TG_RB_PRSMALL = 0, 1
+TG_RB_ULARGE, TG_RB_USMALL = 0, 1
 
 TG_V1, TG_V2, TG_V3 = 0, 1, 2
 TG_W1, TG_W2, TG_W3 = 3, 4, 5
@@ -70,6 +72,9 @@ class tg_config(C.Structure):
         ("rb_pr", C.c_double),
         ("device", C.c_int),
         ("stream", C.c_void_p),
+        ("rb_pr_switch", C.c_int),
+        ("rb_u_scaling", C.c_int),
+        ("rb_temp_grad", C.c_double),
     ]
 
 
@@ -142,6 +147,8 @@ SIGNATURES = {
     "tg_field_download": (C.c_int, [_VP, C.c_int, _DP, C.c_size_t]),
     "tg_field_copy": (C.c_int, [_VP, C.c_int, C.c_int]),
     "tg_field_alloc": (C.c_int, [_VP, C.POINTER(C.c_int)]),
+    "tg_write_field_file": (C.c_int, [C.c_char_p, C.c_double, C.POINTER(C.c_int), C.c_int, C.POINTER(_DP), C.c_int, C.c_int]),
+    "tg_read_field_file": (C.c_int, [C.c_char_p, C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_double), C.c_int, C.POINTER(_DP), C.c_int]),
     "tg_field_free": (C.c_int, [_VP, C.c_int]),
     "tg_forward_transform": (C.c_int, [_VP, C.c_int, C.c_int]),
     "tg_inverse_transform": (C.c_int, [_VP, C.c_int, C.c_int]),

@@ -478,6 +478,7 @@ void tg_config_default(tg_config* cfg) {
   cfg->dt = 1e-3;
   cfg->force_kind = TG_FORCE_DECAY;
   cfg->n_shells = 12;
+  cfg->rb_temp_grad = 1.0;
   cfg->device = 0;
   cfg->stream = nullptr;
 }
@@ -579,11 +580,11 @@ int ctx_create_batch(const tg_config* cfg, int B, tg_ctx** out) {
       pp.a[q] = PA[q];
       pp.b[q] = PB[q];
     }
-    if (c->phys == TG_RB) {
-      // Compute_force_RB: Force1 = theta, T.Force = temperature_grad (+1) u1
-      const double on = (cfg->force_kind == TG_FORCE_RB) ? 1.0 : 0.0;
-      c->rb_fu = on;
-      c->rb_ft = on;
+    if (c->phys == TG_RB && cfg->force_kind == TG_FORCE_RB) {
+      // Compute_force_RB: Force1 = fu theta, T.Force = ft u1
+      const RBCoef r = rb_coefficients(cfg);
+      c->rb_fu = r.fu;
+      c->rb_ft = r.ft;
     }
   }
 
@@ -727,6 +728,10 @@ int validate_config(const tg_config* cfg) {
   if (cfg->physics < TG_FLUID || cfg->physics > TG_RB) return TG_ERR_ARG;
   if (cfg->basis == TG_SCFT && cfg->physics == TG_MHD) return TG_ERR_UNSUPPORTED;
   if (cfg->physics == TG_RB && !(cfg->rb_ra > 0 && cfg->rb_pr > 0)) return TG_ERR_ARG;
+  if (cfg->physics == TG_RB &&
+      ((cfg->rb_pr_switch != TG_RB_PRLARGE && cfg->rb_pr_switch != TG_RB_PRSMALL) ||
+       (cfg->rb_u_scaling != TG_RB_ULARGE && cfg->rb_u_scaling != TG_RB_USMALL) || !std::isfinite(cfg->rb_temp_grad)))
+    return TG_ERR_ARG;
   if (cfg->precision != TG_FP64 && cfg->precision != TG_FP32_MIXED) return TG_ERR_ARG;
   if (cfg->scheme != TG_RK4) return TG_ERR_UNSUPPORTED;
   if (cfg->force_kind != TG_FORCE_DECAY && cfg->force_kind != TG_FORCE_ENERGY_SUPPLY && cfg->force_kind != TG_FORCE_RB)
@@ -740,6 +745,29 @@ int validate_config(const tg_config* cfg) {
   return TG_OK;
 }
 
+// RB coefficients of a nondimensionalisation (RB_slip_main.cc:222-262, compute_force_RB.cc:
+// 50-105, nusselt.cc:53-89): nu (grad^2 u), kappa (grad^2 theta), Force1 = fu theta,
+// T.Force = ft u1, Nu = 1 + nuf <u1, theta> (nuf times the Get_total_energy cross term)
+RBCoef rb_coefficients(const tg_config* cfg) {
+  const double Ra = cfg->rb_ra, Pr = cfg->rb_pr, g = cfg->rb_temp_grad;
+  RBCoef r{};
+  const bool small_u = cfg->rb_u_scaling == TG_RB_USMALL;
+  if (cfg->rb_pr_switch == TG_RB_PRSMALL) {
+    r.nu = small_u ? 1.0 : std::sqrt(Pr / Ra);
+    r.kappa = small_u ? 1.0 / Pr : 1.0 / std::sqrt(Pr * Ra);
+    r.fu = small_u ? Ra : Pr;
+    r.ft = g / Pr;
+    r.nuf = small_u ? 2 * Pr * Pr : 2 * Pr * std::sqrt(Ra * Pr);
+  } else {
+    r.nu = small_u ? Pr : std::sqrt(Pr / Ra);
+    r.kappa = small_u ? 1.0 : 1.0 / std::sqrt(Pr * Ra);
+    r.fu = small_u ? Ra * Pr : 1.0;
+    r.ft = g;
+    r.nuf = small_u ? 2.0 : 2 * std::sqrt(Ra * Pr);
+  }
+  return r;
+}
+
 void state_viscosities(const tg_config* cfg, double nu[6]) {
   for (int i = 0; i < 6; ++i) nu[i] = 0.0;
   for (int i = 0; i < 3; ++i) nu[i] = cfg->nu;
@@ -748,10 +776,9 @@ void state_viscosities(const tg_config* cfg, double nu[6]) {
   } else if (cfg->physics == TG_SCALAR) {
     nu[3] = cfg->kappa;
   } else if (cfg->physics == TG_RB) {
-    // PRLARGE + ULARGE (RB_slip_main.cc:236-240): nu = sqrt(Pr/Ra), kappa = 1/sqrt(Pr Ra)
-    const double v = std::sqrt(cfg->rb_pr / cfg->rb_ra), ka = 1.0 / std::sqrt(cfg->rb_pr * cfg->rb_ra);
-    for (int i = 0; i < 3; ++i) nu[i] = v;
-    nu[3] = ka;
+    const RBCoef r = rb_coefficients(cfg);
+    for (int i = 0; i < 3; ++i) nu[i] = r.nu;
+    nu[3] = r.kappa;
   }
 }
 
@@ -1298,7 +1325,7 @@ int tg_nusselt(tg_ctx* c, double* nu) {
   TG_CK(cudaStreamSynchronize(c->st));
   double cross = 0;
   for (int b = 0; b < nb; ++b) cross += h[(size_t)b * 8];
-  *nu = 1.0 + 2.0 * std::sqrt(c->cfg.rb_ra * c->cfg.rb_pr) * cross;
+  *nu = 1.0 + rb_coefficients(&c->cfg).nuf * cross;
   return TG_OK;
 }
 

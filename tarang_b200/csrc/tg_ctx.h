@@ -147,6 +147,10 @@ int ensure_staging_ctx(tg_ctx* c);
 int validate_config(const tg_config* cfg);
 // viscosity of each state field (nu, eta, kappa; RB: from Ra and Pr)
 void state_viscosities(const tg_config* cfg, double nu[6]);
+struct RBCoef {
+  double nu, kappa, fu, ft, nuf;
+};
+RBCoef rb_coefficients(const tg_config* cfg);
 // one fused RK4 step of the first nact slots, enqueued on c->st; ring: record slot 0's energy
 int enqueue_step(tg_ctx* c, bool ring);
 // energies of the master state of all active slots, or of slots r0 .. r0+n-1; dt_mode 2 sets

@@ -130,6 +130,12 @@ std::string batch_key(const tg_config& c, long long id) {
                 c.force_kind);
   std::string k(buf);
   if (c.force_kind == TG_FORCE_ENERGY_SUPPLY) k += "|solo" + std::to_string(id);
+  if (c.physics == TG_RB && c.force_kind == TG_FORCE_RB) {
+    // the buoyancy coefficients are per context: requests share a batch only when they agree
+    const RBCoef r = rb_coefficients(&c);
+    std::snprintf(buf, sizeof(buf), "|rb%a,%a", r.fu, r.ft);
+    k += buf;
+  }
   return k;
 }
 

@@ -28,13 +28,17 @@ _PHYS = {"FLUID": L.TG_FLUID, "INC_FLUID": L.TG_FLUID, "MHD": L.TG_MHD, "INC_MHD
 _PREC = {"FP64": L.TG_FP64, "FP32": L.TG_FP32_MIXED, "FP32_MIXED": L.TG_FP32_MIXED}
 
 
+_DP_T = C.POINTER(C.c_double)
+
+
 def _dptr(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
 def make_config(N, basis="FOUR", physics="FLUID", precision="FP64", dealias=True,
                 kfactor=(1.0, 1.0, 1.0), nu=0.01, eta=None, kappa=None, dt=1e-3,
-                force=None, n_shells=12, device=0, Ra=0.0, Pr=0.0, stream=None) -> L.tg_config:
+                force=None, n_shells=12, device=0, Ra=0.0, Pr=0.0, stream=None,
+                Pr_switch="PRLARGE", RB_Uscaling="ULARGE", temperature_grad=1.0) -> L.tg_config:
     lib = L.load()
     cfg = L.tg_config()
     lib.tg_config_default(C.byref(cfg))
@@ -60,9 +64,41 @@ def make_config(N, basis="FOUR", physics="FLUID", precision="FP64", dealias=True
     cfg.n_shells = int(n_shells)
     cfg.rb_ra = float(Ra)
     cfg.rb_pr = float(Pr)
+    cfg.rb_pr_switch = {"PRLARGE": L.TG_RB_PRLARGE, "PRSMALL": L.TG_RB_PRSMALL}[Pr_switch]
+    cfg.rb_u_scaling = {"ULARGE": L.TG_RB_ULARGE, "USMALL": L.TG_RB_USMALL}[RB_Uscaling]
+    cfg.rb_temp_grad = float(temperature_grad)
     cfg.device = int(device)
     cfg.stream = C.c_void_p(int(stream)) if stream else None
     return cfg
+
+
+def write_field_file(path, fields, time=0.0, vx_vy=False, append=False):
+    """Write state fields (each (N1, N2, N3/2+1) complex128, reference order) in the reference's
+    field-file text format (tg_write_field_file)."""
+    lib = L.load()
+    arrs = [np.ascontiguousarray(f, dtype=np.complex128) for f in fields]
+    N1, N2, M3 = arrs[0].shape
+    Nc = (C.c_int * 3)(N1, N2, 2 * (M3 - 1))
+    ptrs = (_DP_T * len(arrs))(*[_dptr(a.view(np.float64)) for a in arrs])
+    rc = lib.tg_write_field_file(str(path).encode(), float(time), Nc, len(arrs), ptrs, 1 if vx_vy else 0,
+                                 1 if append else 0)
+    if rc != L.TG_OK:
+        raise L.TarangError(rc, f"write_field_file {path}")
+
+
+def read_field_file(path, N, n_fields, basis="FOUR", kfactor=(1.0, 1.0, 1.0), vx_vy=False):
+    """Read n_fields state fields of grid N from a reference field file (tg_read_field_file)."""
+    lib = L.load()
+    shape = (N[0], N[1], N[2] // 2 + 1)
+    arrs = [np.zeros(shape, dtype=np.complex128) for _ in range(n_fields)]
+    Nc = (C.c_int * 3)(*[int(n) for n in N])
+    kf = (C.c_double * 3)(*[float(k) for k in kfactor])
+    ptrs = (_DP_T * n_fields)(*[_dptr(a.view(np.float64)) for a in arrs])
+    b = _BASIS[basis] if isinstance(basis, str) else int(basis)
+    rc = lib.tg_read_field_file(str(path).encode(), Nc, b, kf, n_fields, ptrs, 1 if vx_vy else 0)
+    if rc != L.TG_OK:
+        raise L.TarangError(rc, f"read_field_file {path}")
+    return arrs
 
 
 class IncFluid:
@@ -274,3 +310,28 @@ class IncFluid:
         v = C.c_double()
         self._ck(self.lib.tg_nusselt(self.h, C.byref(v)), "nusselt")
         return v.value
+
+    # ------------------------------------------------------------------ field files
+    def state_fields(self):
+        """V, then W (MHD) or T (scalar, convection): the reference's field-file order."""
+        out = self.get_V()
+        if self.cfg.physics == L.TG_MHD:
+            out += self.get_W()
+        elif self.cfg.physics in (L.TG_SCALAR, L.TG_RB):
+            out.append(self.get_T())
+        return out
+
+    def Output_field(self, path, vx_vy=False, append=False):
+        """IncFluid::Output_field (output_field.cc:43-108): the state at the current time."""
+        write_field_file(path, self.state_fields(), self.time()[0], vx_vy, append)
+
+    def Init_cond_from_file(self, path, vx_vy=False):
+        """IncFluid::Init_cond (init_cond_field.cc:47-223): the state read from a field file."""
+        n = {L.TG_MHD: 6, L.TG_SCALAR: 4, L.TG_RB: 4}.get(self.cfg.physics, 3)
+        basis = "SCFT" if self.cfg.basis == L.TG_SCFT else "FOUR"
+        f = read_field_file(path, self.N, n, basis, tuple(self.cfg.kfactor), vx_vy)
+        self.set_V(f[:3])
+        if n == 6:
+            self.set_W(f[3:])
+        elif n == 4:
+            self.set_T(f[3])

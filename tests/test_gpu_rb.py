@@ -104,3 +104,26 @@ def ctypes_nusselt(s):
     v = ctypes.c_double()
     s._ck(s.lib.tg_nusselt(s.h, ctypes.byref(v)), "nusselt")
     return v.value
+
+
+@pytest.mark.parametrize("pr_switch,u_scaling,grad", [("PRLARGE", "USMALL", 1.0), ("PRSMALL", "ULARGE", 1.0),
+                                                      ("PRSMALL", "USMALL", 1.0), ("PRLARGE", "ULARGE", -1.0)])
+def test_rb_scalings_10_steps(lib, pr_switch, u_scaling, grad):
+    """The other nondimensionalisations of RB_slip_main.cc:222-262 (and stable stratification,
+    temperature_grad = -1): diffusivities, buoyancy coefficients and Nusselt factor."""
+    N = (24, 16, 32)
+    Ra, Pr = 2e3, 0.7
+    T = ic.rb_perturbation(N, seed=20261207)
+    V = [np.zeros_like(T) for _ in range(3)]
+    s = make(N, physics="RB", Ra=Ra, Pr=Pr, kfactor=KF_RB, dt=1e-4, Pr_switch=pr_switch, RB_Uscaling=u_scaling,
+             temperature_grad=grad)
+    s.set_V(V)
+    s.set_T(T)
+    s.step(10)
+    ref = o.RBSolver(N, KF_RB, Ra, Pr, 1e-4, pr_switch=pr_switch, u_scaling=u_scaling, temperature_grad=grad)
+    v, t = V, T
+    for _ in range(10):
+        v, t, dt = ref.step(v, t)
+    assert rel_l2([s.get_T()], [t]) < 1e-12
+    assert rel_l2(s.get_V(), v) < 1e-11
+    assert abs(s.Get_Nusselt_no() - ref.nusselt(v, t)) < 1e-12 * abs(ref.nusselt(v, t))
