@@ -57,6 +57,10 @@ extern "C" {
 /* force_field_proc (compute_force_main.cc:43-124) */
 #define TG_FORCE_DECAY 0
 #define TG_FORCE_ENERGY_SUPPLY 1
+#define TG_FORCE_MODES 5      /* a fixed force on given modes, set by tg_set_force_modes: the
+                                 Taylor-Green, ABC and given-mode forcings (force_field_proc 3, 4, 5) */
+#define TG_FORCE_CORIOLIS 21  /* Force = V x Omega, Omega = force_para[0..2], evaluated from each RK
+                                 stage's velocity (compute_force_Coriolis.cc:47-80) */
 #define TG_FORCE_RB 51
 
 #define TG_RB_PRLARGE 0
@@ -174,6 +178,16 @@ int tg_compute_force(tg_ctx* ctx);
 int tg_compute_nlin(tg_ctx* ctx);
 /* IncFluid::Add_force() (add_force.cc:47-84): nlin -= Force */
 int tg_add_force(tg_ctx* ctx);
+/* The fixed force of TG_FORCE_MODES (Setup_Taylor_Green_force_field, Setup_ABC_force_field,
+ * Compute_force_given_modes_SIMPLE: lib/IncFlow/misc/force_model.cc:57-170,
+ * lib/IncFluid/force/compute_force_modes.cc:97-250): n modes, k[3 i + 0..2] = (kx, ky, kz)
+ * wavenumber indices (FOUR: kx, ky signed; SCFT: kx >= 0; kz >= 0; each at most
+ * TG_FORCE_MODES_KMAX in magnitude) of modes the context stores, F[2 nstate i + 2 c + 0..1] =
+ * (Re, Im) of the force on state field c there (V1, V2, V3, then W1..W3 of MHD or T of a
+ * scalar).  Every other mode has no force; a mode listed twice takes its last value.  Replaces
+ * the previous set (n = 0 clears it).  TG_ERR_STATE unless force_kind is TG_FORCE_MODES. */
+#define TG_FORCE_MODES_KMAX 64
+int tg_set_force_modes(tg_ctx* ctx, int n, const int* k, const double* F);
 /* IncVF::Compute_pressure() (compute_pressure.cc:54-62) */
 int tg_compute_pressure(tg_ctx* ctx);
 /* IncFluid::Compute_rhs() (compute_rhs.cc:52-149) */

@@ -590,6 +590,78 @@ def force_const_energy_supply(V, N, kfactor, inner, outer, eps, eps_h=0.0):
     return F
 
 
+def force_coriolis(V, omega):
+    """Compute_force_Coriolis  compute_force_Coriolis.cc:47-80 (three-component form):
+    Force1 = w2 V3 - w3 V2, Force2 = w3 V1 - w1 V3, Force3 = w1 V2 - w2 V1."""
+    w1, w2, w3 = omega
+    return [w2 * V[2] - w3 * V[1], w3 * V[0] - w1 * V[2], w1 * V[1] - w2 * V[0]]
+
+
+def _lx(k, N1, basis):
+    return k if (basis == "SCFT" or k >= 0) else k + N1
+
+
+def taylor_green_force(N, k0, amp, basis="FOUR"):
+    """IncVF::Setup_Taylor_Green_force_field  lib/IncFlow/misc/force_model.cc:57-104 as dense
+    arrays (Force1, Force2, Force3): amp (sin k0x cos k0y cos k0z, -cos k0x sin k0y cos k0z, 0)
+    on the modes (+-k0, +-k0, k0) (SCFT: kx = k0 only)."""
+    N1, N2, N3 = N
+    F = [np.zeros((N1, N2, N3 // 2 + 1), dtype=np.complex128) for _ in range(3)]
+    a = amp / 8
+    yp, ym = k0 % N2, (-k0) % N2
+    if basis == "FOUR":
+        xp, xm = _lx(k0, N1, basis), _lx(-k0, N1, basis)
+        F[0][xp, yp, k0] = -1j * a
+        F[0][xp, ym, k0] = -1j * a
+        F[1][xp, yp, k0] = 1j * a
+        F[1][xp, ym, k0] = -1j * a
+        F[0][xm, yp, k0] = 1j * a
+        F[0][xm, ym, k0] = 1j * a
+        F[1][xm, yp, k0] = 1j * a
+        F[1][xm, ym, k0] = -1j * a
+    else:
+        F[0][k0, yp, k0] = a
+        F[0][k0, ym, k0] = a
+        F[1][k0, yp, k0] = 1j * a
+        F[1][k0, ym, k0] = -1j * a
+    return F
+
+
+def abc_force(N, k0, amp, A, B, C):
+    """IncVF::Setup_ABC_force_field  lib/IncFlow/misc/force_model.cc:122-170 (FOUR) as dense
+    arrays: amp (B cos k0y + C sin k0z, A sin k0x + C cos k0z, A cos k0x + B sin k0y)."""
+    N1, N2, N3 = N
+    F = [np.zeros((N1, N2, N3 // 2 + 1), dtype=np.complex128) for _ in range(3)]
+    yp, ym, xp, xm = k0 % N2, (-k0) % N2, k0 % N1, (-k0) % N1
+    F[0][0, yp, 0] = B * amp / 2
+    F[0][0, ym, 0] = B * amp / 2
+    F[0][0, 0, k0] = -1j * (C * amp / 2)
+    F[1][0, 0, k0] = C * amp / 2
+    F[2][0, yp, 0] = -1j * (B * amp / 2)
+    F[2][0, ym, 0] = 1j * (B * amp / 2)
+    F[1][xp, 0, 0] = -1j * (A * amp / 2)
+    F[2][xp, 0, 0] = A * amp / 2
+    F[1][xm, 0, 0] = 1j * (A * amp / 2)
+    F[2][xm, 0, 0] = A * amp / 2
+    return F
+
+
+def fluid_force(force, V, N, kfactor):
+    """The velocity force of a run: None (decay), energy supply dict(inner, outer, eps, eps_h),
+    dict(kind="static", F=[F1, F2, F3, ...]) (a fixed force field) or
+    dict(kind="coriolis", omega=(w1, w2, w3))."""
+    if force is None:
+        return None
+    kind = force.get("kind", "energy_supply")
+    if kind == "energy_supply":
+        return force_const_energy_supply(V, N, kfactor, **{k: v for k, v in force.items() if k != "kind"})
+    if kind == "static":
+        return list(force["F"][:3])
+    if kind == "coriolis":
+        return force_coriolis(V, force["omega"])
+    raise ValueError(kind)
+
+
 # --------------------------------------------------------------------------------------
 # Integrating-factor RK4  (lib/IncFluid/time_advance)
 # --------------------------------------------------------------------------------------
@@ -614,14 +686,11 @@ class FluidSolver:
         self.Tdt = Tdt
         self.basis = basis
         self.alias = alias
-        self.force = force   # None (decay) or dict(inner, outer, eps, eps_h)
+        self.force = force   # see fluid_force
 
     # Compute_force(); Compute_nlin(); Add_force(); Compute_pressure(); Compute_rhs()
     def rhs(self, V):
-        if self.force is not None:
-            F = force_const_energy_supply(V, self.N, self.kfactor, **self.force)
-        else:
-            F = None
+        F = fluid_force(self.force, V, self.N, self.kfactor)
         nl = nlin_fluid(V, self.kfactor, self.basis, self.alias)
         if F is not None:
             nl = [nl[i] - F[i] for i in range(3)]
@@ -670,12 +739,19 @@ class MHDSolver(FluidSolver):
     time_advance_VF_MHD.cc:59-182: the same IF-RK4 with nu for U and eta for B; only U.nlin is
     projected (Compute_pressure uses U's nlin), W.nlin -> -W.nlin (compute_rhs.cc:111-119)."""
 
-    def __init__(self, N, kfactor, nu, eta, Tdt, basis="FOUR", alias="DEALIAS"):
-        super().__init__(N, kfactor, nu, Tdt, basis, alias, None)
+    def __init__(self, N, kfactor, nu, eta, Tdt, basis="FOUR", alias="DEALIAS", force=None):
+        super().__init__(N, kfactor, nu, Tdt, basis, alias, force)
         self.eta = eta
 
     def rhs2(self, V, W):
+        """Compute_force(W), Compute_nlin(W), Add_force(W) (add_force.cc:58-66): U.nlin -= F,
+        W.nlin -= W.Force (a static force's components 3..5; zero otherwise)."""
         un, bn = nlin_mhd(V, W, self.kfactor, self.basis, self.alias)
+        F = fluid_force(self.force, V, self.N, self.kfactor)
+        if F is not None:
+            un = [un[i] - F[i] for i in range(3)]
+            if self.force.get("kind") == "static" and len(self.force["F"]) > 3:
+                bn = [bn[i] - self.force["F"][3 + i] for i in range(3)]
         p = pressure(un, self.kfactor, self.basis, self.alias)
         ru = rhs_from_nlin(un, p, self.kfactor, self.basis)
         rb = [-b for b in bn]

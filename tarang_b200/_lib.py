@@ -25,7 +25,8 @@ TG_FOUR, TG_SCFT = 0, 1
 TG_FLUID, TG_MHD, TG_SCALAR, TG_RB = 0, 1, 2, 3
 TG_FP64, TG_FP32_MIXED = 0, 1
 TG_RK4 = 4
-TG_FORCE_DECAY, TG_FORCE_ENERGY_SUPPLY, TG_FORCE_RB = 0, 1, 51
+TG_FORCE_DECAY, TG_FORCE_ENERGY_SUPPLY, TG_FORCE_MODES, TG_FORCE_CORIOLIS, TG_FORCE_RB = 0, 1, 5, 21, 51
+TG_FORCE_MODES_KMAX = 64
 TG_RB_PRLARGE, TG_RB_PRSMALL = 0, 1
 TG_RB_ULARGE, TG_RB_USMALL = 0, 1
 
@@ -155,6 +156,7 @@ SIGNATURES = {
     "tg_compute_force": (C.c_int, [_VP]),
     "tg_compute_nlin": (C.c_int, [_VP]),
     "tg_add_force": (C.c_int, [_VP]),
+    "tg_set_force_modes": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_int), _DP]),
     "tg_compute_pressure": (C.c_int, [_VP]),
     "tg_compute_rhs": (C.c_int, [_VP]),
     "tg_get_dt": (C.c_int, [_VP, _DP]),

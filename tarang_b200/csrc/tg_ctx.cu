@@ -139,7 +139,7 @@ int run_pipeline(tg_ctx* c, const void* const* in, int inprec) {
 }
 
 int run_force(tg_ctx* c, const void* const* U, int uprec) {
-  if (!c->force_on) return TG_OK;
+  if (c->force_on != 1) return TG_OK;
   ForceArgs f{};
   f.g = c->g;
   for (int i = 0; i < 3; ++i) f.U[i] = U[i];
@@ -181,6 +181,8 @@ RKArgs rk_args(tg_ctx* c, int stage) {
   a.rb_buoy_t = c->rb_ft;
   a.nact = c->nact;
   a.nu_tab = c->nu_tab;
+  a.coriolis = c->coriolis ? 1 : 0;
+  for (int i = 0; i < 3; ++i) a.om[i] = c->om[i];
   return a;
 }
 
@@ -713,6 +715,12 @@ int ctx_create_batch(const tg_config* cfg, int B, tg_ctx** out) {
     c->nf_modes = count_force_modes(*cfg);
     if (c->nf_modes <= 0) return fail(set_err(c, TG_ERR_ARG, "forcing shell holds no modes"));
     if ((rc = dalloc(c, (void**)&c->FB, sizeof(cx<double>) * 3 * (size_t)c->fbox))) return fail(rc);
+  } else if (cfg->force_kind == TG_FORCE_MODES) {
+    if (B != 1) return fail(set_err(c, TG_ERR_UNSUPPORTED, "forced requests are not batched"));
+    c->force_on = 2;  // the box is allocated by tg_set_force_modes
+  } else if (cfg->force_kind == TG_FORCE_CORIOLIS) {
+    c->coriolis = true;
+    for (int i = 0; i < 3; ++i) c->om[i] = cfg->force_para[i];
   }
   e = cudaStreamSynchronize(c->st);
   if (e != cudaSuccess) return fail(cuda_err(c, e, "create"));
@@ -734,9 +742,16 @@ int validate_config(const tg_config* cfg) {
     return TG_ERR_ARG;
   if (cfg->precision != TG_FP64 && cfg->precision != TG_FP32_MIXED) return TG_ERR_ARG;
   if (cfg->scheme != TG_RK4) return TG_ERR_UNSUPPORTED;
-  if (cfg->force_kind != TG_FORCE_DECAY && cfg->force_kind != TG_FORCE_ENERGY_SUPPLY && cfg->force_kind != TG_FORCE_RB)
+  if (cfg->force_kind != TG_FORCE_DECAY && cfg->force_kind != TG_FORCE_ENERGY_SUPPLY && cfg->force_kind != TG_FORCE_RB &&
+      cfg->force_kind != TG_FORCE_MODES && cfg->force_kind != TG_FORCE_CORIOLIS)
     return TG_ERR_UNSUPPORTED;
   if (cfg->force_kind == TG_FORCE_RB && cfg->physics != TG_RB) return TG_ERR_ARG;
+  // convection has its own force (force_field_proc 51)
+  if ((cfg->force_kind == TG_FORCE_MODES || cfg->force_kind == TG_FORCE_CORIOLIS) && cfg->physics == TG_RB)
+    return TG_ERR_UNSUPPORTED;
+  if (cfg->force_kind == TG_FORCE_CORIOLIS)
+    for (int i = 0; i < 3; ++i)
+      if (!std::isfinite(cfg->force_para[i])) return TG_ERR_ARG;
   if (cfg->force_kind == TG_FORCE_ENERGY_SUPPLY && cfg->basis != TG_FOUR) return TG_ERR_UNSUPPORTED;
   if (cfg->force_kind == TG_FORCE_ENERGY_SUPPLY && cfg->physics != TG_FLUID) return TG_ERR_UNSUPPORTED;
   for (int i = 0; i < 3; ++i)
@@ -785,7 +800,7 @@ void state_viscosities(const tg_config* cfg, double nu[6]) {
 int ensure_staging_ctx(tg_ctx* c) { return ensure_staging(c); }
 
 int ensure_force_box(tg_ctx* c) {
-  if (!c->force_on || c->force_ever) return TG_OK;
+  if (c->force_on != 1 || c->force_ever) return TG_OK;
   const void* U[3] = {c->U0[0], c->U0[1], c->U0[2]};
   return run_force(c, U, F64);
 }
@@ -909,7 +924,19 @@ int tg_field_download(tg_ctx* c, int field, double* host, size_t n) {
   }
   if (field >= TG_FORCE1 && field <= TG_FORCE3) {
     std::memset(host, 0, sizeof(double) * n);
-    if (!c->force_on || !c->have_force) return TG_OK;
+    if (c->coriolis && c->have_force) {
+      // Force = V x Omega of the current velocity
+      std::vector<double> v[3];
+      for (int i = 0; i < 3; ++i) {
+        v[i].resize(n);
+        int rc = tg_field_download(c, TG_V1 + i, v[i].data(), n);
+        if (rc) return rc;
+      }
+      const int a = (field - TG_FORCE1 + 1) % 3, b = (field - TG_FORCE1 + 2) % 3;
+      for (size_t q = 0; q < n; ++q) host[q] = c->om[a] * v[b][q] - c->om[b] * v[a][q];
+      return TG_OK;
+    }
+    if (!c->force_on || !c->FB || (c->force_on == 1 && !c->have_force)) return TG_OK;
     std::vector<cx<double>> box((size_t)c->fbox);
     const int comp = field - TG_FORCE1;
     TG_CK(cudaMemcpyAsync(box.data(), c->FB + (size_t)comp * c->fbox, sizeof(cx<double>) * c->fbox,
@@ -1044,6 +1071,66 @@ int tg_compute_force(tg_ctx* c) {
   return TG_OK;
 }
 
+int tg_set_force_modes(tg_ctx* c, int n, const int* k, const double* F) {
+  if (!c || n < 0 || (n > 0 && (!k || !F))) return TG_ERR_ARG;
+  if (c->cfg.force_kind != TG_FORCE_MODES) return set_err(c, TG_ERR_STATE, "set_force_modes: force_kind is not TG_FORCE_MODES");
+  cudaSetDevice(c->dev);
+  const int ns = c->nstate, K = TG_FORCE_MODES_KMAX;
+  int fx = 0, fy = 0, fz = 0;
+  for (int i = 0; i < n; ++i) {
+    const int kx = k[3 * i], ky = k[3 * i + 1], kz = k[3 * i + 2];
+    if (std::abs(kx) > K || std::abs(ky) > K || kz < 0 || kz > K)
+      return set_err(c, TG_ERR_ARG, "set_force_modes: wavenumber out of range");
+    // the mode must be one the context stores, named by the wavenumber the kernels see for it
+    const int lx = c->basis == TG_FOUR ? (kx >= 0 ? kx : kx + c->N1) : kx;
+    const int ly = ky >= 0 ? ky : ky + c->N2;
+    const int r1 = (lx >= 0 && lx < c->N1) ? amap_row(c->g.ax, lx) : -1;
+    const int r2 = (ly >= 0 && ly < c->N2) ? amap_row(c->g.ay, ly) : -1;
+    if (r1 < 0 || r2 < 0 || geo_kx(c->g, r1) != kx || geo_ky(c->g, r2) != ky || kz >= c->g.nkz)
+      return set_err(c, TG_ERR_ARG, "set_force_modes: mode (" + std::to_string(kx) + "," + std::to_string(ky) + "," +
+                                        std::to_string(kz) + ") is not stored");
+    for (int q = 0; q < 2 * ns; ++q)
+      if (!std::isfinite(F[(size_t)2 * ns * i + q])) return set_err(c, TG_ERR_ARG, "set_force_modes: force not finite");
+    fx = std::max(fx, std::abs(kx));
+    fy = std::max(fy, std::abs(ky));
+    fz = std::max(fz, kz);
+  }
+  const int ny = 2 * fy + 1, nz = fz + 1, box = n > 0 ? (2 * fx + 1) * ny * nz : 0;
+  std::vector<cx<double>> h((size_t)ns * box);
+  for (int i = 0; i < n; ++i) {
+    const int p = ((k[3 * i] + fx) * ny + (k[3 * i + 1] + fy)) * nz + k[3 * i + 2];
+    for (int q = 0; q < ns; ++q) {
+      h[(size_t)q * box + p].x = F[(size_t)2 * ns * i + 2 * q];
+      h[(size_t)q * box + p].y = F[(size_t)2 * ns * i + 2 * q + 1];
+    }
+  }
+  TG_CK(cudaStreamSynchronize(c->st));
+  // a captured step reads the box's address and extents
+  if (c->step_graph) {
+    cudaGraphExecDestroy(c->step_graph);
+    c->step_graph = nullptr;
+  }
+  if (c->FB && box != c->fbox) {
+    TG_CK(cudaFree(c->FB));
+    c->bytes -= sizeof(cx<double>) * (size_t)ns * c->fbox;
+    c->FB = nullptr;
+  }
+  c->fx = fx;
+  c->fy = fy;
+  c->fz = fz;
+  c->fbox = box;
+  if (box > 0) {
+    if (!c->FB) {
+      int rc = dalloc(c, (void**)&c->FB, sizeof(cx<double>) * (size_t)ns * box);
+      if (rc) return rc;
+    }
+    TG_CK(cudaMemcpyAsync(c->FB, h.data(), sizeof(cx<double>) * h.size(), cudaMemcpyHostToDevice, c->st));
+    TG_CK(cudaStreamSynchronize(c->st));
+  }
+  c->force_ever = true;
+  return TG_OK;
+}
+
 int tg_compute_nlin(tg_ctx* c) {
   if (!c) return TG_ERR_ARG;
   cudaSetDevice(c->dev);
@@ -1061,9 +1148,11 @@ int tg_add_force(tg_ctx* c) {
   if (!c) return TG_ERR_ARG;
   if (!c->have_nlin) return set_err(c, TG_ERR_STATE, "Add_force before Compute_nlin");
   cudaSetDevice(c->dev);
-  if (c->force_on) {
-    if (!c->have_force) return set_err(c, TG_ERR_STATE, "Add_force before Compute_force");
-    TG_CK(launch_sub_force_box(c->g, 3, c->FB, c->fx, c->fy, c->fz, c->NL, c->st));
+  if ((c->force_on || c->coriolis) && !c->have_force) return set_err(c, TG_ERR_STATE, "Add_force before Compute_force");
+  if (c->force_on && c->FB) TG_CK(launch_sub_force_box(c->g, c->nstate, c->FB, c->fx, c->fy, c->fz, c->NL, c->st));
+  if (c->coriolis) {
+    const cx<double>* U[3] = {c->U0[0], c->U0[1], c->U0[2]};
+    TG_CK(launch_sub_coriolis(c->g, c->NL, U, c->om, c->st));
   }
   if (c->phys == TG_RB) {
     TG_CK(launch_rb_sub_force(c->g, c->NL, c->U0[0], c->U0[3], c->rb_fu, c->rb_ft, c->st));

@@ -58,12 +58,15 @@ struct tg_ctx {
   void* PY[9] = {};
   void* PX[9] = {};
 
-  // forcing box
+  // forcing box [nstate][(2 fx + 1)(2 fy + 1)(fz + 1)] over kx in [-fx, fx], ky in [-fy, fy],
+  // kz in [0, fz]; force_on 1: energy supply (recomputed every stage), 2: fixed modes
   int force_on = 0;
   int fx = 0, fy = 0, fz = 0, fbox = 0;
   int nf_modes = 0;
   tg::cx<double>* FB = nullptr;
   bool force_ever = false;  // FB holds a force computed by this context
+  bool coriolis = false;    // Force = V x om of every stage's velocity
+  double om[3] = {0, 0, 0};
 
   // scalars and reductions
   double* scal = nullptr;   // per slot [8]: [0] dt, [1] t_now, [2] steps, [3] nonfinite, [4] Tdt

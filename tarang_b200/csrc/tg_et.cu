@@ -406,7 +406,9 @@ int tg_force_feed(tg_ctx* c, double* feed, int n) {
   if (c->basis != TG_FOUR || c->phys != TG_FLUID)
     return set_err(c, TG_ERR_UNSUPPORTED, "force feed: FOUR fluid only");
   for (int i = 0; i < n; ++i) feed[i] = 0;
-  if (!c->force_on) return TG_OK;  // decaying run: the force is zero
+  // decaying run, fixed modes never set: the force is zero; Coriolis: Re(F . V*) = Re(Omega .
+  // (V* x V)) = 0 mode by mode (V* x V is imaginary)
+  if (!c->force_on || (c->force_on == 2 && !c->FB)) return TG_OK;
   cudaSetDevice(c->dev);
   int rc = ensure_force_box(c);
   if (rc) return rc;

@@ -130,6 +130,10 @@ std::string batch_key(const tg_config& c, long long id) {
                 c.force_kind);
   std::string k(buf);
   if (c.force_kind == TG_FORCE_ENERGY_SUPPLY) k += "|solo" + std::to_string(id);
+  if (c.force_kind == TG_FORCE_CORIOLIS) {
+    std::snprintf(buf, sizeof(buf), "|om%a,%a,%a", c.force_para[0], c.force_para[1], c.force_para[2]);
+    k += buf;
+  }
   if (c.physics == TG_RB && c.force_kind == TG_FORCE_RB) {
     // the buoyancy coefficients are per context: requests share a batch only when they agree
     const RBCoef r = rb_coefficients(&c);
@@ -533,6 +537,8 @@ int tg_server_submit(tg_server* s, const tg_request* rq, long long* id) {
   *id = -1;
   const int v = validate_config(&rq->cfg);
   if (v) return v;
+  // a request carries no force modes (tg_set_force_modes is a context call)
+  if (rq->cfg.force_kind == TG_FORCE_MODES) return TG_ERR_UNSUPPORTED;
   const int Mz = rq->cfg.N[2] / 2;
   if (!(Mz >= 4 && Mz <= 256 && (Mz & (Mz - 1)) == 0)) return TG_ERR_UNSUPPORTED;
   if (rq->n_steps < 0) return TG_ERR_ARG;

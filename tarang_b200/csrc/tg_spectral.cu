@@ -213,7 +213,17 @@ __global__ void __launch_bounds__(TPB, RKOcc<PHYS>::v) k_rk(RKArgs a) {
         const int box = (2 * a.fx + 1) * (2 * a.fy + 1) * (a.fz + 1);
         const int p = ((kxi + a.fx) * (2 * a.fy + 1) + (kyi + a.fy)) * (a.fz + 1) + l3;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) r[c] = r[c] - a.FB[(long long)c * box + p];
+        for (int c = 0; c < NS; ++c) r[c] = r[c] - a.FB[(long long)c * box + p];
+      }
+      if (a.coriolis) {
+        // Compute_force_Coriolis (compute_force_Coriolis.cc:47-80) from the stage's velocity:
+        // Force = V x Omega, then Add_force: nlin -= Force
+        cx<double> v[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) v[c] = a.inprec ? ldc<float>(a.IN[c], gi) : ldc<double>(a.IN[c], gi);
+        r[0] = r[0] - (a.om[1] * v[2] - a.om[2] * v[1]);
+        r[1] = r[1] - (a.om[2] * v[0] - a.om[0] * v[2]);
+        r[2] = r[2] - (a.om[0] * v[1] - a.om[1] * v[0]);
       }
       if constexpr (PHYS == PH_RB) {
         // Compute_force_RB (compute_force_RB.cc:51-105) from the stage's fields, then Add_force:
@@ -482,6 +492,15 @@ __global__ void k_rb_sub_force(Geo g, PtrArr6 pa, const cx<double>* u1, const cx
   pa.p[3][idx] = pa.p[3][idx] - ft * u1[idx];
 }
 
+__global__ void k_sub_coriolis(Geo g, PtrArr6 nl, PtrArr6 u, double o0, double o1, double o2) {
+  const long long idx = (long long)blockIdx.x * TPB + threadIdx.x;
+  if (idx >= g.S) return;
+  const cx<double> v0 = u.p[0][idx], v1 = u.p[1][idx], v2 = u.p[2][idx];
+  nl.p[0][idx] = nl.p[0][idx] - (o1 * v2 - o2 * v1);
+  nl.p[1][idx] = nl.p[1][idx] - (o2 * v0 - o0 * v2);
+  nl.p[2][idx] = nl.p[2][idx] - (o0 * v1 - o1 * v0);
+}
+
 // ------------------------------------------------------------------ reductions
 // cross energy Re(A B*) with the energy weights (Get_total_energy(A, B), four_energy.cc:108-168,
 // scft_energy.cc:108-158), per block into part[b * nslots + slot]
@@ -699,6 +718,17 @@ cudaError_t launch_rb_sub_force(const Geo& g, cx<double>* const* NL, const cx<do
   PtrArr6 pa{};
   for (int c = 0; c < 4; ++c) pa.p[c] = NL[c];
   k_rb_sub_force<<<nblk(g.S), TPB, 0, s>>>(g, pa, u1, th, fu, ft);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sub_coriolis(const Geo& g, cx<double>* const* NL, const cx<double>* const* U, const double* om,
+                                cudaStream_t s) {
+  PtrArr6 nl{}, u{};
+  for (int c = 0; c < 3; ++c) {
+    nl.p[c] = NL[c];
+    u.p[c] = const_cast<cx<double>*>(U[c]);
+  }
+  k_sub_coriolis<<<nblk(g.S), TPB, 0, s>>>(g, nl, u, om[0], om[1], om[2]);
   return cudaGetLastError();
 }
 

@@ -79,6 +79,9 @@ struct RKArgs {
   // viscosities at nu_tab[6 r], its scalars (dt, ...) at dt[8 r], its partials in part[r]
   int nact;
   const double* nu_tab;
+  // Coriolis force of the stage's velocity (Compute_force_Coriolis), when coriolis != 0
+  int coriolis;
+  double om[3];
 };
 
 struct ForceArgs {
@@ -100,6 +103,9 @@ cudaError_t launch_assemble_nlin(const Geo& g, int phys, int pprec, const void* 
 cudaError_t launch_sub_force_box(const Geo& g, int ncomp, const cx<double>* FB, int fx, int fy, int fz, cx<double>* const* NL, cudaStream_t s);
 cudaError_t launch_pressure(const Geo& g, const cx<double>* const* NL, cx<double>* PR, cudaStream_t s);
 cudaError_t launch_rhs_from_nlin(const Geo& g, int phys, cx<double>* const* NL, const cx<double>* PR, cudaStream_t s);
+// NL[c] -= (U x om)[c], c < 3 (Add_force with the Coriolis force)
+cudaError_t launch_sub_coriolis(const Geo& g, cx<double>* const* NL, const cx<double>* const* U, const double* om,
+                                cudaStream_t s);
 cudaError_t launch_rb_sub_force(const Geo& g, cx<double>* const* NL, const cx<double>* u1, const cx<double>* th,
                                 double fu, double ft, cudaStream_t s);
 cudaError_t launch_cross_partials(const Geo& g, const cx<double>* A, const cx<double>* B, double* part, int slot,

@@ -185,12 +185,59 @@ def config_from_para(p: dict, kind: str = "FLUID") -> dict:
     elif kind == "RB":
         cfg.update(Ra=ra, Pr=pr, Pr_switch=pr_switch, RB_Uscaling=u_scaling, temperature_grad=temp_grad)
     proc = p["force_int"][1] if len(p["force_int"]) > 1 else 0
+    fd = p["force_double"] + [0.0] * 7
+    run_force = None
     if proc == 1:
-        fd = p["force_double"] + [0.0] * 5
         cfg["force"] = dict(inner=fd[1], outer=fd[2], eps=fd[3], eps_h=fd[4])
+    elif proc in (3, 4) and kind != "RB":
+        # compute_force_TG.cc:47-92, compute_force_ABC.cc:50-131: k0, amplitudes (W: the next)
+        cfg["force"] = dict(kind="modes")
+        if proc == 3:
+            run_force = dict(kind="taylor_green", k0=int(fd[1]), amp=fd[2], ampW=fd[3])
+        else:
+            run_force = dict(kind="abc", k0=int(fd[1]), A=fd[2], B=fd[3], C=fd[4], amp=fd[5], ampW=fd[6])
+    elif proc == 5 and kind != "RB":
+        # the modes come from in/force_field_in.d (forcing.read_force_modes_file)
+        cfg["force"] = dict(kind="modes")
+        run_force = dict(kind="given_modes", file="in/force_field_in.d")
+    elif proc == 21 and kind != "RB":
+        # compute_force_Coriolis.cc:47-80 takes the number of components from force_int(1),
+        # which is also force_field_proc (21), so as written it sets neither branch; the
+        # evident meaning is kept: force_int(2) = 1 with omega along axis force_int(3) given by
+        # force_double(1), else omega = force_double(1..3)
+        fi = p["force_int"] + [0] * 3
+        if fi[2] == 1 and fi[3] in (1, 2, 3):
+            om = [0.0, 0.0, 0.0]
+            om[fi[3] - 1] = fd[1]
+        else:
+            om = [fd[1], fd[2], fd[3]]
+        cfg["force"] = dict(kind="coriolis", omega=tuple(om))
     elif proc != 0 and kind != "RB":
         raise ValueError(f"force_field_proc {proc} is not supported")
     cfg["run"] = dict(Tinit=p["time_para"][1], Tfinal=p["time_para"][2],
                       output_vx_vy=p["switches"][19], input_vx_vy=p["switches"][20],
-                      field_input_proc=p["init_cond_int"][1] if len(p["init_cond_int"]) > 1 else 0)
+                      field_input_proc=p["init_cond_int"][1] if len(p["init_cond_int"]) > 1 else 0,
+                      force_modes=run_force)
     return cfg
+
+
+def force_modes_for(cfg: dict, data_dir: str = "."):
+    """(k, F) for IncFluid.set_force_modes when config_from_para mapped a fixed-mode forcing
+    (cfg["run"]["force_modes"]), else None.  A given-modes forcing reads
+    data_dir/in/force_field_in.d (IncFluid::Open_force_waveno_input_files)."""
+    import os
+
+    from . import forcing
+    fm = cfg.get("run", {}).get("force_modes")
+    if not fm:
+        return None
+    N, basis, physics = cfg["N"], cfg.get("basis", "FOUR"), cfg.get("physics", "FLUID")
+    if fm["kind"] == "taylor_green":
+        return forcing.taylor_green_modes(N, fm["k0"], fm["amp"], basis, physics, fm["ampW"])
+    if fm["kind"] == "abc":
+        if basis != "FOUR":
+            raise ValueError("ABC forcing is FOUR only (force_model.cc:164-168)")
+        return forcing.abc_modes(N, fm["k0"], fm["amp"], fm["A"], fm["B"], fm["C"], physics, fm["ampW"])
+    n_values = {"FLUID": 2, "MHD": 4, "SCALAR": 3}[physics]
+    entries = forcing.read_force_modes_file(os.path.join(data_dir, fm["file"]), N[0], n_values)
+    return forcing.given_modes(entries, N, cfg.get("kfactor", (1.0, 1.0, 1.0)), basis, physics)

@@ -57,6 +57,13 @@ def make_config(N, basis="FOUR", physics="FLUID", precision="FP64", dealias=True
         cfg.force_kind = L.TG_FORCE_RB          # Compute_force_RB (force_field_proc 51)
     elif force is None or force == "decay":
         cfg.force_kind = L.TG_FORCE_DECAY
+    elif force.get("kind") == "modes":
+        cfg.force_kind = L.TG_FORCE_MODES          # fixed modes, IncFluid.set_force_modes
+    elif force.get("kind") == "coriolis":
+        cfg.force_kind = L.TG_FORCE_CORIOLIS       # Force = V x omega (force_field_proc 21)
+        cfg.force_para[:3] = [float(x) for x in force["omega"]]
+    elif force.get("kind", "energy_supply") != "energy_supply":
+        raise ValueError(f"force kind {force.get('kind')}")
     else:
         cfg.force_kind = L.TG_FORCE_ENERGY_SUPPLY
         p = [force.get("inner"), force.get("outer"), force.get("eps"), force.get("eps_h", 0.0)]
@@ -210,6 +217,18 @@ class IncFluid:
     # ------------------------------------------------------------------ solver calls
     def Compute_force(self):
         self._ck(self.lib.tg_compute_force(self.h), "Compute_force")
+
+    def set_force_modes(self, k, F):
+        """The fixed force of force=dict(kind="modes") (tg_set_force_modes): k (n, 3) wavenumber
+        indices, F (n, nstate) complex force on each state field there (tarang_b200.forcing
+        builds both for the Taylor-Green, ABC and given-mode forcings)."""
+        k = np.ascontiguousarray(k, dtype=np.int32).reshape(-1, 3)
+        F = np.ascontiguousarray(F, dtype=np.complex128)
+        ns = {L.TG_FLUID: 3, L.TG_MHD: 6}.get(self.cfg.physics, 4)
+        if F.ndim != 2 or F.shape != (k.shape[0], ns):
+            raise ValueError(f"F must have one row of {ns} values per mode")
+        self._ck(self.lib.tg_set_force_modes(self.h, k.shape[0], k.ctypes.data_as(C.POINTER(C.c_int)),
+                                             _dptr(F.view(np.float64))), "set_force_modes")
 
     def Compute_nlin(self):
         self._ck(self.lib.tg_compute_nlin(self.h), "Compute_nlin")

@@ -1,0 +1,244 @@
+"""Parity of the fixed-mode forcings (Taylor-Green, ABC, given modes: force_field_proc 3, 4, 5)
+and the Coriolis force (proc 21) on the CUDA path with the oracle: 10-step trajectories of fluid
+(FOUR and SCFT) and MHD runs (relative L2 error <= 1e-12 in FP64, 1e-6 in FP32-mixed), the
+method-by-method calls and the force fields they leave, the force feed, batched Coriolis
+requests, and the errors of tg_set_force_modes."""
+
+import math
+
+import numpy as np
+import pytest
+
+from oracle import tarang_oracle as o
+from tarang_b200 import _lib as L
+from tarang_b200 import forcing, ic
+
+pytestmark = pytest.mark.gpu
+
+KF = (1.0, 1.0, 1.0)
+
+
+def rel_l2(a, b):
+    num = math.sqrt(sum(float(np.sum(np.abs(x - y) ** 2)) for x, y in zip(a, b)))
+    den = math.sqrt(sum(float(np.sum(np.abs(y) ** 2)) for y in b))
+    return num / den
+
+
+def make(N, **kw):
+    from tarang_b200.solver import IncFluid
+    return IncFluid(N, **kw)
+
+
+def dense_cols(k, F, N, basis="FOUR"):
+    N1, N2, N3 = N
+    out = []
+    for c in range(F.shape[1]):
+        A = np.zeros((N1, N2, N3 // 2 + 1), dtype=np.complex128)
+        for (kx, ky, kz), f in zip(k, F[:, c]):
+            A[kx if (basis == "SCFT" or kx >= 0) else kx + N1, ky % N2, kz] = f
+        out.append(A)
+    return out
+
+
+@pytest.mark.parametrize("basis,precision,tol", [("FOUR", "FP64", 1e-12), ("SCFT", "FP64", 1e-12),
+                                                 ("FOUR", "FP32", 1e-6)])
+def test_taylor_green_forced_10_steps(lib, basis, precision, tol):
+    N = (32, 32, 32)
+    if basis == "FOUR":
+        V = ic.random_phase_field(N, seed=31)
+    else:
+        # SCFT velocity: V1 a sine series in x, V2 and V3 cosine series (dealiased)
+        rng = np.random.default_rng(31)
+        V = [0.3 * o.dealias(o.forward_scft(rng.standard_normal(N), p), "SCFT") for p in (1, 0, 0)]
+    k, F = forcing.taylor_green_modes(N, 2, 0.8, basis)
+    s = make(N, basis=basis, nu=5e-3, dt=5e-4, force=dict(kind="modes"), precision=precision)
+    s.set_force_modes(k, F)
+    s.set_V(V)
+    s.step(10)
+    ref = o.FluidSolver(N, KF, 5e-3, 5e-4, basis=basis, force=dict(kind="static", F=o.taylor_green_force(N, 2, 0.8, basis)))
+    Vw = V
+    for _ in range(10):
+        Vw, _ = ref.step(Vw)
+    assert rel_l2(s.get_V(), Vw) < tol
+
+
+def test_abc_forced_mhd_10_steps(lib):
+    N = (32, 32, 32)
+    V = ic.random_phase_field(N, seed=32)
+    W = ic.random_phase_field(N, seed=33, energy=0.2)
+    k, F = forcing.abc_modes(N, 1, 0.5, 1.0, 0.7, 0.3, physics="MHD", ampW=0.25)
+    s = make(N, physics="MHD", nu=4e-3, eta=6e-3, dt=5e-4, force=dict(kind="modes"))
+    s.set_force_modes(k, F)
+    s.set_V(V)
+    s.set_W(W)
+    s.step(10)
+    ref = o.MHDSolver(N, KF, 4e-3, 6e-3, 5e-4, force=dict(kind="static", F=dense_cols(k, F, N)))
+    Vw, Ww = V, W
+    for _ in range(10):
+        Vw, Ww, _ = ref.step2(Vw, Ww)
+    assert rel_l2(s.get_V(), Vw) < 1e-12
+    assert rel_l2(s.get_W(), Ww) < 1e-12
+
+
+def test_given_modes_fine_grained_calls(lib):
+    """Compute_force / Compute_nlin / Add_force with given modes: nlin = N(u) - F, the force
+    field downloads as set, and the method-by-method loop equals the fused step."""
+    N = (32, 32, 32)
+    V = ic.random_phase_field(N, seed=34)
+    k, F = forcing.given_modes([(1, 2, 3, 0.3 + 0.1j, -0.2 + 0.4j), (2, 1, 0, 0.5 + 0.2j, 0.1 - 0.3j)], N)
+    Fd = dense_cols(k, F, N)
+    a = make(N, nu=2e-3, dt=5e-4, force=dict(kind="modes"))
+    b = make(N, nu=2e-3, dt=5e-4, force=dict(kind="modes"))
+    for s in (a, b):
+        s.set_force_modes(k, F)
+        s.set_V(V)
+    a.Compute_force()
+    f = a.get_force()
+    assert all(np.array_equal(x, y) for x, y in zip(f, Fd))
+    a.Compute_nlin()
+    a.Add_force()
+    nl = a.get_nlin()
+    want = [x - y for x, y in zip(o.nlin_fluid(V, KF), Fd)]
+    assert rel_l2(nl, want) < 1e-13
+    a.Compute_pressure()
+    a.Get_dt()
+    a.Time_advance()
+    for _ in range(2):
+        a.Compute_force()
+        a.Compute_nlin()
+        a.Add_force()
+        a.Compute_pressure()
+        a.Get_dt()
+        a.Time_advance()
+    b.step(3)
+    assert rel_l2(a.get_V(), b.get_V()) < 1e-14
+
+
+def test_force_modes_reset_between_graph_steps(lib):
+    """A new mode set after graph-replayed steps is used by the following steps (the captured
+    step is rebuilt), and n = 0 clears the force."""
+    N = (32, 32, 32)
+    V = ic.random_phase_field(N, seed=35)
+    k1, F1 = forcing.taylor_green_modes(N, 1, 0.5)
+    k2, F2 = forcing.abc_modes(N, 2, 0.5, 1.0, 1.0, 1.0)
+    s = make(N, nu=5e-3, dt=5e-4, force=dict(kind="modes"))
+    s.set_force_modes(k1, F1)
+    s.set_V(V)
+    s.step(4)
+    s.set_force_modes(k2, F2)
+    s.step(4)
+    s.set_force_modes(np.zeros((0, 3)), np.zeros((0, 3)))
+    s.step(2)
+    r1 = o.FluidSolver(N, KF, 5e-3, 5e-4, force=dict(kind="static", F=dense_cols(k1, F1, N)))
+    r2 = o.FluidSolver(N, KF, 5e-3, 5e-4, force=dict(kind="static", F=dense_cols(k2, F2, N)))
+    r3 = o.FluidSolver(N, KF, 5e-3, 5e-4)
+    Vw = V
+    for r, n in ((r1, 4), (r2, 4), (r3, 2)):
+        for _ in range(n):
+            Vw, _ = r.step(Vw)
+    assert rel_l2(s.get_V(), Vw) < 1e-12
+
+
+def test_force_feed_of_fixed_modes(lib):
+    N = (32, 32, 32)
+    V = ic.random_phase_field(N, seed=36)
+    k, F = forcing.taylor_green_modes(N, 2, 0.8)
+    s = make(N, nu=5e-3, dt=5e-4, force=dict(kind="modes"), n_shells=12)
+    s.set_force_modes(k, F)
+    s.set_V(V)
+    got = s.Compute_force_feed_shell()
+    want = o.force_feed_shell(dense_cols(k, F, N), V, KF, 12)
+    assert np.abs(np.asarray(got) - np.asarray(want)).max() <= 1e-14 * max(1.0, np.abs(want).max())
+
+
+@pytest.mark.parametrize("physics", ["FLUID", "MHD"])
+def test_coriolis_10_steps(lib, physics):
+    N = (32, 32, 32)
+    om = (0.3, -0.5, 2.0)
+    V = ic.random_phase_field(N, seed=37)
+    kw = dict(nu=4e-3, dt=5e-4, force=dict(kind="coriolis", omega=om))
+    if physics == "FLUID":
+        s = make(N, **kw)
+        s.set_V(V)
+        s.step(10)
+        ref = o.FluidSolver(N, KF, 4e-3, 5e-4, force=dict(kind="coriolis", omega=om))
+        Vw = V
+        for _ in range(10):
+            Vw, _ = ref.step(Vw)
+        assert rel_l2(s.get_V(), Vw) < 1e-12
+    else:
+        W = ic.random_phase_field(N, seed=38, energy=0.2)
+        s = make(N, physics="MHD", eta=6e-3, **kw)
+        s.set_V(V)
+        s.set_W(W)
+        s.step(10)
+        ref = o.MHDSolver(N, KF, 4e-3, 6e-3, 5e-4, force=dict(kind="coriolis", omega=om))
+        Vw, Ww = V, W
+        for _ in range(10):
+            Vw, Ww, _ = ref.step2(Vw, Ww)
+        assert rel_l2(s.get_V(), Vw) < 1e-12
+        assert rel_l2(s.get_W(), Ww) < 1e-12
+
+
+def test_coriolis_fine_grained_and_force_field(lib):
+    N = (32, 32, 32)
+    om = (0.0, 0.0, 3.0)
+    V = ic.random_phase_field(N, seed=39)
+    s = make(N, nu=4e-3, dt=5e-4, force=dict(kind="coriolis", omega=om))
+    s.set_V(V)
+    s.Compute_force()
+    f = s.get_force()
+    want = o.force_coriolis(V, om)
+    assert rel_l2(f, want) < 1e-15
+    s.Compute_nlin()
+    s.Add_force()
+    want_nl = [x - y for x, y in zip(o.nlin_fluid(V, KF), want)]
+    assert rel_l2(s.get_nlin(), want_nl) < 1e-13
+    # Re(F . V*) = 0: a rotating frame feeds no energy
+    assert np.abs(s.Compute_force_feed_shell()).max() == 0.0
+
+
+def test_coriolis_requests_batch_alone_equals_mixed(lib):
+    """Coriolis requests with the same Omega share a batch; each result equals a lone context's
+    run bit for bit."""
+    from tarang_b200.serving import Server
+    N = (32, 32, 32)
+    om = (0.0, 1.0, 2.0)
+    Vs = [ic.random_phase_field(N, seed=40 + i) for i in range(3)]
+    cfgs = [dict(N=N, nu=3e-3 * (1 + i), dt=5e-4, force=dict(kind="coriolis", omega=om)) for i in range(3)]
+    with Server(hbm_budget=8e9, max_batch=4) as srv:
+        ids = [srv.submit(c, V, 6) for c, V in zip(cfgs, Vs)]
+        srv.drain()
+        for i, (rid, V) in enumerate(zip(ids, Vs)):
+            got = srv.result(rid)
+            s = make(N, nu=3e-3 * (1 + i), dt=5e-4, force=dict(kind="coriolis", omega=om))
+            s.set_V(V)
+            s.step(6)
+            assert all(np.array_equal(x.view(np.float64), y.view(np.float64)) for x, y in zip(got, s.get_V()))
+        assert srv.stats()["n_batches"] >= 1
+        # a request carries no force modes
+        with pytest.raises(L.TarangError) as e:
+            srv.submit(dict(N=N, nu=1e-3, dt=5e-4, force=dict(kind="modes")), Vs[0], 2)
+        assert e.value.code == L.TG_ERR_UNSUPPORTED
+
+
+def test_set_force_modes_errors(lib):
+    N = (32, 32, 32)
+    s = make(N, nu=1e-3, dt=5e-4, force=dict(kind="modes"))
+    k, F = forcing.taylor_green_modes(N, 11, 1.0)        # |k| = 11 > N/3: not stored
+    with pytest.raises(L.TarangError) as e:
+        s.set_force_modes(k, F)
+    assert e.value.code == L.TG_ERR_ARG
+    with pytest.raises(L.TarangError):
+        s.set_force_modes([(1, 1, -1)], np.zeros((1, 3)))
+    with pytest.raises(L.TarangError):
+        s.set_force_modes([(1, 1, 1)], np.full((1, 3), np.nan))
+    with pytest.raises(ValueError):
+        s.set_force_modes([(1, 1, 1)], np.zeros((1, 6)))
+    d = make(N, nu=1e-3, dt=5e-4)
+    with pytest.raises(L.TarangError) as e:
+        d.set_force_modes(*forcing.taylor_green_modes(N, 1, 1.0))
+    assert e.value.code == L.TG_ERR_STATE
+    with pytest.raises(L.TarangError) as e:
+        make(N, physics="RB", basis="SCFT", Ra=1e4, Pr=1.0, dt=1e-4, force=dict(kind="coriolis", omega=(0, 0, 1)))
+    assert e.value.code == L.TG_ERR_UNSUPPORTED
