@@ -746,4 +746,241 @@ __global__ void __launch_bounds__(32 * WPB, (E <= 4 ? (sizeof(Rw) == 8 ? 4 : 6) 
   }
 }
 
+// ------------------------------------------------------------------------------------------
+// Warp-per-row fused z-pass for M = N3/2 = 128 with two register<->lane transposes.
+//
+// The 32-point lane DFT of k_z_prod_warp costs five shuffle stages, each moving every value of
+// the row.  Here the length-128 inverse DFT is split into digits n = n0 + 4 n1 + 8 n2 + 32 j
+// (n0 = lane bits 0-1, n1 = lane bit 2, n2 = lane bits 3-4, j = register) and run as
+//   DFT4 over j (registers), twiddle, transpose j <-> n2, DFT4 over n2, twiddle,
+//   radix-2 over n1 (one shuffle stage), twiddle, transpose <-> n0, DFT4 over n0,
+// so the lanes exchange 3 + 4 + 3 values instead of 5 x 4.  Each transpose is three shuffles of
+// a fixed register from a lane-dependent source: the sending lane's registers are kept rotated
+// by its lane digit, which costs nothing because a rotation of a DFT's outputs equals a phase
+// i^(j g) on its inputs and the rotation the receiver sees becomes a phase on the next DFT's
+// outputs; both phases are folded into the per-lane twiddles t1, t2, except the first input
+// phase i^(j n2) and the last output phase i^(kB m), which are exact multiplies by i^p.
+// Output layout: lane l, register m holds Z[(l >> 3) + 4 (l & 3) + 16 ((l >> 2) & 1) + 32 m].
+// The forward transform is the adjoint network (reverse order, conjugate factors) and returns
+// natural order.  Index map and factors are those of a CPU emulation checked against an FFT.
+// ------------------------------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ cx<R> cmul_unit(cx<R> a, cx<R> c) {
+  return mkc<R>(c.x * a.x - c.y * a.y, c.x * a.y + c.y * a.x);
+}
+// i^p exactly (p taken mod 4)
+template <typename R>
+__device__ __forceinline__ cx<R> ipow_c(int p) {
+  p &= 3;
+  return mkc<R>(p == 0 ? (R)1 : (p == 2 ? (R)-1 : (R)0), p == 1 ? (R)1 : (p == 3 ? (R)-1 : (R)0));
+}
+
+template <typename R>
+struct Net128 {
+  cx<R> t1[4], t2[4], w8, ca, cb;
+  R sa, sb;  // ca^2, cb^2 (+-1)
+  int lane;
+  // twN[k] = e^{-i pi k / 128}, k < 256; W_N^e (sign +) = conj(twN[(256 / N) e mod 256])
+  __device__ __forceinline__ void init(const cx<double>* twN, int l) {
+    lane = l;
+    const int g0 = l & 3, c2 = (l >> 2) & 1, g3 = l >> 3;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int kA = (r + g3) & 3;
+      t1[r] = cmul_unit(conjc(cvt<R>(twN[(2 * l * kA) & 255])), ipow_c<R>(-r * g0));
+      const int kB = (r + g0) & 3;
+      t2[r] = cmul_unit(conjc(cvt<R>(twN[(8 * (l & 7) * kB) & 255])), ipow_c<R>(g3 * (r + g0)));
+    }
+    w8 = conjc(cvt<R>(twN[(32 * g0 * c2) & 255]));
+    ca = ipow_c<R>(g3);
+    cb = ipow_c<R>(g0);
+    sa = (g3 & 1) ? (R)-1 : (R)1;
+    sb = (g0 & 1) ? (R)-1 : (R)1;
+  }
+  // v[j] *= i^(j n2) (before inv), v[j] *= i^(-j n2) (after fwd)
+  __device__ __forceinline__ void phase_in(cx<R> (&v)[4], bool conj) const {
+    const cx<R> c = conj ? conjc(ca) : ca;
+    v[1] = cmul_unit(v[1], c);
+    v[2] = sa * v[2];
+    v[3] = cmul_unit(v[3], conjc(c));
+  }
+  // inverse (sign +) DFT of the row in natural order -> permuted order
+  __device__ __forceinline__ void inv(cx<R> (&v)[4]) const {
+    DFT<4, +1, R>::run(v);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) v[r] = v[r] * t1[r];
+    const int g3 = lane >> 3, g0 = lane & 3;
+    {
+      const cx<R> z1 = shfl_c(v[1], (lane & 7) | (((g3 - 1) & 3) << 3));
+      const cx<R> z2 = shfl_c(v[2], (lane & 7) | (((g3 - 2) & 3) << 3));
+      const cx<R> z3 = shfl_c(v[3], (lane & 7) | (((g3 - 3) & 3) << 3));
+      v[1] = z1;
+      v[2] = z2;
+      v[3] = z3;
+    }
+    DFT<4, -1, R>::run(v);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) v[r] = v[r] * t2[r];
+    const R sg = (lane & 4) ? (R)-1 : (R)1;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const cx<R> p = shfl_xor_c(v[k], 4);
+      v[k] = mkc<R>(fma(sg, v[k].x, p.x), fma(sg, v[k].y, p.y)) * w8;
+    }
+    {
+      const cx<R> z1 = shfl_c(v[1], (lane & ~3) | ((g0 - 1) & 3));
+      const cx<R> z2 = shfl_c(v[2], (lane & ~3) | ((g0 - 2) & 3));
+      const cx<R> z3 = shfl_c(v[3], (lane & ~3) | ((g0 - 3) & 3));
+      v[1] = z1;
+      v[2] = z2;
+      v[3] = z3;
+    }
+    DFT<4, -1, R>::run(v);
+    v[1] = cmul_unit(v[1], cb);
+    v[2] = sb * v[2];
+    v[3] = cmul_unit(v[3], conjc(cb));
+  }
+  // forward (sign -) DFT: the adjoint of inv, permuted order -> natural order
+  __device__ __forceinline__ void fwd(cx<R> (&v)[4]) const {
+    v[1] = cmul_unit(v[1], conjc(cb));
+    v[2] = sb * v[2];
+    v[3] = cmul_unit(v[3], cb);
+    DFT<4, +1, R>::run(v);
+    const int g3 = lane >> 3, g0 = lane & 3;
+    {
+      const cx<R> z1 = shfl_c(v[1], (lane & ~3) | ((g0 + 1) & 3));
+      const cx<R> z2 = shfl_c(v[2], (lane & ~3) | ((g0 + 2) & 3));
+      const cx<R> z3 = shfl_c(v[3], (lane & ~3) | ((g0 + 3) & 3));
+      v[1] = z1;
+      v[2] = z2;
+      v[3] = z3;
+    }
+    const R sg = (lane & 4) ? (R)-1 : (R)1;
+    const cx<R> w8c = conjc(w8);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const cx<R> sv = v[k] * w8c;
+      const cx<R> p = shfl_xor_c(sv, 4);
+      v[k] = mkc<R>(fma(sg, sv.x, p.x), fma(sg, sv.y, p.y));
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) v[r] = v[r] * conjc(t2[r]);
+    DFT<4, +1, R>::run(v);
+    {
+      const cx<R> z1 = shfl_c(v[1], (lane & 7) | (((g3 + 1) & 3) << 3));
+      const cx<R> z2 = shfl_c(v[2], (lane & 7) | (((g3 + 2) & 3) << 3));
+      const cx<R> z3 = shfl_c(v[3], (lane & 7) | (((g3 + 3) & 3) << 3));
+      v[1] = z1;
+      v[2] = z2;
+      v[3] = z3;
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) v[r] = v[r] * conjc(t1[r]);
+    DFT<4, -1, R>::run(v);
+  }
+};
+
+// 16-byte asynchronous global -> shared copies (completion waited with cp.async.wait_group)
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// PF = 1: the warp's next row is copied into shared memory (cp.async, np entries per input)
+// while the products of the current row are transformed, so the inverse transforms read their
+// inputs from shared memory instead of waiting on global loads.  Requires row strides and
+// input pointers on 16-byte boundaries (the launcher checks) and sizeof(Ri) == sizeof(Rw).
+template <typename Ri, typename Ro, typename Rw, int NIN, int NPROD, int WPB, int PF>
+__global__ void __launch_bounds__(32 * WPB, sizeof(Rw) == 8 ? 4 : 6)
+    k_z_prod_net128(ZArgs a, PtrSet ps, ProdPairs pp, int np) {
+  constexpr int M = 128, E = 4;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const size_t warp_bytes = (size_t)NIN * E * 32 * sizeof(cx<Rw>) + (PF ? (size_t)NIN * np * sizeof(cx<Ri>) : 0);
+  unsigned char* wbase = smem_raw + (size_t)wib * warp_bytes;
+  cx<Rw>* rs = reinterpret_cast<cx<Rw>*>(wbase);
+  cx<Ri>* ib = reinterpret_cast<cx<Ri>*>(wbase + (size_t)NIN * E * 32 * sizeof(cx<Rw>));
+  Net128<Rw> net;
+  net.init(a.twN, lane);
+  cx<Rw> hw[E];
+#pragma unroll
+  for (int j = 0; j < E; ++j) hw[j] = cvt<Rw>(a.twN[lane + 32 * j]);
+  const Rw sc = (Rw)a.scale;
+  const long long nwarps = (long long)gridDim.x * WPB;
+  // copy row `row` of every input into ib (16-byte chunks of the first nin entries)
+  const int chunks = (int)(((size_t)a.nin * sizeof(cx<Ri>) + 15) / 16);
+  auto prefetch = [&](long long row) {
+#pragma unroll 1
+    for (int c = 0; c < NIN; ++c) {
+      const unsigned char* g = reinterpret_cast<const unsigned char*>(ps.src[c]) + (size_t)row * a.ss * sizeof(cx<Ri>);
+      unsigned char* d = reinterpret_cast<unsigned char*>(ib + (size_t)c * np);
+      for (int t = lane; t < chunks; t += 32) cp_async16(d + 16 * t, g + 16 * t);
+    }
+    cp_async_commit();
+  };
+  long long row = (long long)blockIdx.x * WPB + wib;
+  if (PF && row < a.nrows) prefetch(row);
+  for (; row < a.nrows; row += nwarps) {
+    if (PF) {
+      cp_async_wait_all();
+      __syncwarp();
+    }
+    // ---- inverse (c2r) of every input
+#pragma unroll 1
+    for (int c = 0; c < NIN; ++c) {
+      const cx<Ri>* src = PF ? ib + (size_t)c * np : reinterpret_cast<const cx<Ri>*>(ps.src[c]) + row * a.ss;
+      cx<Rw> v[E];
+#pragma unroll
+      for (int j = 0; j < E; ++j) {
+        const int k = lane + 32 * j;
+        cx<Rw> xa = (k < a.nin) ? cvt<Rw>(src[k]) : mkc<Rw>(0, 0);
+        const int km = M - k;
+        cx<Rw> xb = (km < a.nin) ? cvt<Rw>(src[km]) : mkc<Rw>(0, 0);
+        if (k == 0) {
+          xa.y = 0;
+          xb.y = 0;
+        }
+        xb.y = -xb.y;
+        v[j] = (xa + xb) + ione(conjc(hw[j]) * (xa - xb));
+      }
+      net.phase_in(v, false);
+      net.inv(v);
+#pragma unroll
+      for (int k1 = 0; k1 < E; ++k1) rs[(c * E + k1) * 32 + lane] = v[k1];
+    }
+    if (PF) {
+      __syncwarp();  // every lane has read this row's inputs
+      if (row + nwarps < a.nrows) prefetch(row + nwarps);
+    }
+    // ---- products and forward (r2c)
+#pragma unroll 1
+    for (int q = 0; q < NPROD; ++q) {
+      const int pa = pp.a[q], pb = pp.b[q];
+      cx<Rw> v[E];
+#pragma unroll
+      for (int k1 = 0; k1 < E; ++k1) v[k1] = rmul(rs[(pa * E + k1) * 32 + lane], rs[(pb * E + k1) * 32 + lane]);
+      net.fwd(v);
+      net.phase_in(v, true);
+      cx<Ro>* dst = reinterpret_cast<cx<Ro>*>(ps.dst[q]) + row * a.ds;
+      const int pl = (32 - lane) & 31;
+#pragma unroll
+      for (int j = 0; j < E; ++j) {
+        cx<Rw> zm = shfl_c(v[E - 1 - j], pl);
+        if (lane == 0) zm = v[(E - j) % E];
+        zm.y = -zm.y;
+        const cx<Rw> s = v[j] + zm;
+        const cx<Rw> d = hw[j] * (v[j] - zm);
+        const int k = lane + 32 * j;
+        if (k < a.nout) dst[k] = cvt<Ro>(mkc<Rw>(sc * (Rw)0.5 * (s.x + d.y), sc * (Rw)0.5 * (s.y - d.x)));
+      }
+      if (lane == 0 && a.nout > M) dst[M] = cvt<Ro>(mkc<Rw>(sc * (v[0].x - v[0].y), (Rw)0));
+      for (int k = a.nout + lane; k < a.nfill; k += 32) dst[k] = mkc<Ro>(0, 0);
+    }
+  }
+  if (PF) cp_async_wait_all();
+}
+
 }  // namespace tg

@@ -1,4 +1,7 @@
 // Dispatch of the z-pass (contiguous axis) c2r / r2c kernels and of the fused product z-pass.
+#include <cstdint>
+#include <cstdlib>
+
 #include "tg_fft_launch.h"
 
 namespace tg {
@@ -111,8 +114,53 @@ cudaError_t run_zprod_warp(const ZProdLaunch& l, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// M = 128: the transposed lane network (k_z_prod_net128) unless TG_ZPASS_NET=0 selects the
+// five-stage shuffle network of k_z_prod_warp (both compute the same transform)
+bool zpass_net_enabled() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = std::getenv("TG_ZPASS_NET");
+    v = (e && e[0] == '0') ? 0 : 1;
+  }
+  return v == 1;
+}
+
+template <typename Ri, typename Ro, typename Rw, int NIN, int NPROD, int PF>
+cudaError_t run_zprod_net128_pf(const ZProdLaunch& l, int np, cudaStream_t s) {
+  constexpr int WPB = 4;
+  const size_t smem =
+      (size_t)WPB * ((size_t)NIN * 4 * 32 * sizeof(cx<Rw>) + (PF ? (size_t)NIN * np * sizeof(cx<Ri>) : 0));
+  auto kern = k_z_prod_net128<Ri, Ro, Rw, NIN, NPROD, WPB, PF>;
+  static size_t attr = 0;
+  if (smem > attr) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr = smem;
+  }
+  long long blocks = (l.a.nrows + WPB - 1) / WPB;
+  if (blocks > 148LL * 32) blocks = 148LL * 32;
+  kern<<<(unsigned)blocks, 32 * WPB, smem, s>>>(l.a, l.ps, l.pp, np);
+  return cudaGetLastError();
+}
+
+// The prefetching form when its buffers fit beside the register-bound occupancy (at most four
+// inputs) and every input row starts on a 16-byte boundary.
+template <typename Ri, typename Ro, typename Rw, int NIN, int NPROD>
+cudaError_t run_zprod_net128(const ZProdLaunch& l, cudaStream_t s) {
+  bool pf = NIN <= 4 && sizeof(Ri) == sizeof(Rw) && l.a.nin <= 128 &&
+            ((size_t)l.a.ss * sizeof(cx<Ri>)) % 16 == 0 &&
+            ((size_t)l.a.ss * sizeof(cx<Ri>)) >= (((size_t)l.a.nin * sizeof(cx<Ri>) + 15) / 16) * 16;
+  for (int c = 0; c < NIN && pf; ++c) pf = (reinterpret_cast<uintptr_t>(l.ps.src[c]) % 16) == 0;
+  // entries per input buffer: nin rounded up to whole 16-byte chunks
+  const int per16 = (int)(16 / sizeof(cx<Ri>));
+  const int np = ((l.a.nin + per16 - 1) / per16) * per16;
+  if (pf) return run_zprod_net128_pf<Ri, Ro, Rw, NIN, NPROD, 1>(l, np, s);
+  return run_zprod_net128_pf<Ri, Ro, Rw, NIN, NPROD, 0>(l, 0, s);
+}
+
 template <typename Ri, typename Ro, typename Rw, int NIN, int NPROD>
 cudaError_t run_zprod_m(const ZProdLaunch& l, cudaStream_t s) {
+  if (l.M == 128 && zpass_net_enabled()) return run_zprod_net128<Ri, Ro, Rw, NIN, NPROD>(l, s);
   switch (l.M) {
     case 4: return run_zprod_fast<Ri, Ro, Rw, 2, 2, NIN, NPROD>(l, s);
     case 8: return run_zprod_fast<Ri, Ro, Rw, 4, 2, NIN, NPROD>(l, s);

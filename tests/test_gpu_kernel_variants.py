@@ -1,7 +1,8 @@
 """Kernel variants that compute the same transform agree to rounding: fields after a few steps
-with the TMA-staged axis passes equal those with the register-staged ones (TG_AXIS_TMA=0) to
-1e-14 (FP64) / 1e-6 (FP32-mixed) relative L2, for every precision and physics on the fast path
-(the compiler may contract multiply-adds differently in the two kernels)."""
+with the TMA-staged axis passes equal those with the register-staged ones (TG_AXIS_TMA=0), and
+those of the transposed lane network of the N3 = 256 z-pass equal those of the five-stage
+shuffle network (TG_ZPASS_NET=0), to 1e-14 (FP64) / 1e-6 (FP32-mixed) relative L2, for every
+precision and physics on the fast path (the two kernels round differently)."""
 
 import json
 import os
@@ -71,3 +72,15 @@ def compare(a, b, cases):
 
 def test_tma_axis_passes_match_register_staged(lib):
     compare(run("1"), run("0"), CASES)
+
+
+ZCASES = [
+    ("fluid256z_fp64", (32, 32, 256), dict(nu=2e-3, dt=1e-3)),
+    ("fluid256z_fp32", (32, 32, 256), dict(nu=2e-3, dt=1e-3, precision="FP32")),
+    ("mhd256z_fp64", (16, 32, 256), dict(physics="MHD", nu=2e-3, eta=3e-3, dt=1e-3)),
+    ("scalar256z_fp32", (16, 16, 256), dict(physics="SCALAR", nu=2e-3, kappa=3e-3, dt=1e-3, precision="FP32")),
+]
+
+
+def test_transposed_z_network_matches_shuffle_stages(lib):
+    compare(run("1", ZCASES, "TG_ZPASS_NET"), run("0", ZCASES, "TG_ZPASS_NET"), ZCASES)
