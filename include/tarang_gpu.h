@@ -165,6 +165,16 @@ int tg_write_field_file(const char* path, double time, const int N[3], int n_fie
                         const double* const* fields, int vx_vy, int append);
 int tg_read_field_file(const char* path, const int N[3], int basis, const double kfactor[3], int n_fields,
                        double* const* fields, int vx_vy);
+/* Reduced-size field files: the low-wavenumber corner Nr[3] (Nr <= N; FOUR: Nr1 even; Nr2, Nr3
+ * even) of N-grid fields, as IncFluid::Output_field_reduced writes it with Write_data_MPI /
+ * Write_data_kz0plane_MPI (output_field.cc:505-600, array_basic.cc:997-1347: rows kx = 0..Nr1/2
+ * then -Nr1/2+1..-1 (SCFT 0..Nr1-1), ky likewise, kz 0..Nr3/2, values "(re,im)" with no
+ * separator) and Init_cond_reduced reads it (init_cond_field.cc:294-338, array_basic.cc:388-715:
+ * the +Nr/2 rows also fill -Nr/2; everything outside the corner is zero; vx_vy as above). */
+int tg_write_field_file_reduced(const char* path, double time, const int N[3], const int Nr[3], int basis,
+                                int n_fields, const double* const* fields, int vx_vy, int append);
+int tg_read_field_file_reduced(const char* path, const int N[3], const int Nr[3], int basis, const double kfactor[3],
+                               int n_fields, double* const* fields, int vx_vy);
 
 /* Forward_transform_array / Inverse_transform_array (universal_tr.cc:66-146) on a work field,
  * in place.  parity: 0 cos/even, 1 sin/odd (SCFT only; ignored for FOUR). */

@@ -151,6 +151,8 @@ SIGNATURES = {
     "tg_write_field_file": (C.c_int, [C.c_char_p, C.c_double, C.POINTER(C.c_int), C.c_int, C.POINTER(_DP), C.c_int, C.c_int]),
     "tg_read_field_file": (C.c_int, [C.c_char_p, C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_double), C.c_int, C.POINTER(_DP), C.c_int]),
     "tg_field_free": (C.c_int, [_VP, C.c_int]),
+    "tg_write_field_file_reduced": (C.c_int, [C.c_char_p, C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int, C.c_int, C.POINTER(_DP), C.c_int, C.c_int]),
+    "tg_read_field_file_reduced": (C.c_int, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_double), C.c_int, C.POINTER(_DP), C.c_int]),
     "tg_forward_transform": (C.c_int, [_VP, C.c_int, C.c_int]),
     "tg_inverse_transform": (C.c_int, [_VP, C.c_int, C.c_int]),
     "tg_compute_force": (C.c_int, [_VP]),

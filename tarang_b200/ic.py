@@ -1,4 +1,7 @@
-"""Initial conditions of the benchmark configurations (host side, numpy; outside the hot path).
+"""Initial conditions (host side, numpy; outside the hot path): the benchmark configurations and
+the reference's initial-condition procedures (IncFluid::Read_init_cond init_cond_main.cc:52-206,
+field_input_proc 1 field file, 2 reduced field file, 3 given modes, 5 energy spectrum, 7
+Taylor-Green, 8 ABC, 51 RB Lorenz modes), returned as the state fields in the reference layout.
 
 * Taylor-Green: the spectral placement of IncVF::Setup_Taylor_Green_field
   (lib/IncFlow/misc/ic_model.cc:58-89): u = amp sin(k0 x) cos(k0 y) cos(k0 z),
@@ -120,6 +123,15 @@ def rb_perturbation(N, nmodes=8, amp=1e-3, seed=20261205):
 def random_phase_field(N, kfactor=(1.0, 1.0, 1.0), k0=4.0, energy=0.5, seed=20261202, dealias=True):
     """Seeded random-phase divergence-free field with E(k) ~ k^4 exp(-2 (k/k0)^2), total
     energy `energy` in the Get_total_energy convention.  Returns [V1, V2, V3]."""
+    V = _random_phase(N, kfactor, lambda idx: idx ** 4 * np.exp(-2.0 * (idx / k0) ** 2), seed, dealias)
+    E = sum(energy_four(v) for v in V)
+    s = math.sqrt(energy / E) if E > 0 else 0.0
+    return [np.ascontiguousarray(v * s) for v in V]
+
+
+def _random_phase(N, kfactor, shell_energy, seed, dealias):
+    """Random phases with the energy shell_energy(ceil|K|) spread over the shell's
+    Approx_number_modes_in_shell (see the module docstring)."""
     N1, N2, N3 = N
     rng = np.random.Generator(np.random.PCG64(seed))
     Kx, Ky, Kz = _k_grids(N, kfactor)
@@ -129,7 +141,7 @@ def random_phase_field(N, kfactor=(1.0, 1.0, 1.0), k0=4.0, energy=0.5, seed=2026
     Kz = np.broadcast_to(Kz, shape)
     K = np.sqrt(Kx * Kx + Ky * Ky + Kz * Kz)
     idx = np.ceil(K)
-    Ek = idx ** 4 * np.exp(-2.0 * (idx / k0) ** 2)
+    Ek = shell_energy(idx)
     approx = 2 * math.pi * np.maximum(idx, 1) ** 2 / (kfactor[0] * kfactor[1] * kfactor[2])
     amp = np.sqrt(2 * Ek / approx)
     ph = rng.random((3,) + shape) * 2 * math.pi
@@ -153,7 +165,136 @@ def random_phase_field(N, kfactor=(1.0, 1.0, 1.0), k0=4.0, energy=0.5, seed=2026
     if dealias:
         keep = keep_mask(N)
         V = [np.where(keep, v, 0) for v in V]
-    V = [reality_kz0(v) for v in V]
-    E = sum(energy_four(v) for v in V)
-    s = math.sqrt(energy / E) if E > 0 else 0.0
-    return [np.ascontiguousarray(v * s) for v in V]
+    return [np.ascontiguousarray(reality_kz0(v)) for v in V]
+
+
+# --------------------------------------------------------------------------------------------
+# The reference's initial-condition procedures
+# --------------------------------------------------------------------------------------------
+
+def _state_count(physics):
+    return {"FLUID": 3, "MHD": 6, "SCALAR": 4, "RB": 4}[physics.upper()]
+
+
+def modes_to_fields(k, F, N, basis="FOUR"):
+    """Dense fields (N1, N2, N3/2+1) from a mode list (k (n, 3), F (n, m)): F[:, c] at (kx, ky,
+    kz) of field c, zero elsewhere."""
+    N1, N2, N3 = N
+    out = [np.zeros((N1, N2, N3 // 2 + 1), dtype=np.complex128) for _ in range(np.shape(F)[1])]
+    for (kx, ky, kz), f in zip(np.asarray(k).tolist(), np.asarray(F)):
+        lx = kx if (basis == "SCFT" or kx >= 0) else kx + N1
+        for c, v in enumerate(f):
+            out[c][lx, ky % N2, kz] = v
+    return out
+
+
+def taylor_green_field(N, k0=1, amp=1.0, basis="FOUR", physics="FLUID", ampW=0.0):
+    """Init_cond_Taylor_Green (init_cond_TG.cc:47-120): V by Setup_Taylor_Green_field
+    (ic_model.cc:58-104, the same modes and values as the Taylor-Green force), W of MHD by
+    Setup_Taylor_Green_field_mag_field (ic_model.cc:122-183: real amp/8 values,
+    -+ on V1, + on V2), T of a scalar zero.  Returns the state fields."""
+    from . import forcing
+    ns = _state_count(physics)
+    k, F = forcing.taylor_green_modes(N, k0, amp, basis)
+    out = modes_to_fields(k, F, N, basis)
+    if ns == 6:
+        a = ampW / 8
+        table = ([((k0, k0, k0), -a, a), ((k0, -k0, k0), a, a), ((-k0, k0, k0), a, a), ((-k0, -k0, k0), -a, a)]
+                 if basis == "FOUR" else [((k0, k0, k0), a, a), ((k0, -k0, k0), -a, a)])
+        W = [np.zeros_like(out[0]) for _ in range(3)]
+        for (kx, ky, kz), w1, w2 in table:
+            lx = kx if (basis == "SCFT" or kx >= 0) else kx + N[0]
+            W[0][lx, ky % N[1], kz] = w1
+            W[1][lx, ky % N[1], kz] = w2
+        out += W
+    elif ns == 4:
+        out.append(np.zeros_like(out[0]))
+    return out
+
+
+def abc_field(N, k0, amp, A, B, C, physics="FLUID", ampW=0.0):
+    """Init_cond_ABC (init_cond_ABC.cc:52-151, FOUR only): Setup_ABC_field (ic_model.cc:187-236)
+    for V (and W of MHD with ampW); a scalar's T is zero."""
+    from . import forcing
+    ns = _state_count(physics)
+    if ns == 6:
+        k, F = forcing.abc_modes(N, k0, amp, A, B, C, "MHD", ampW)
+        return modes_to_fields(k, F, N)
+    k, F = forcing.abc_modes(N, k0, amp, A, B, C)
+    out = modes_to_fields(k, F, N)
+    if ns == 4:
+        out.append(np.zeros_like(out[0]))
+    return out
+
+
+def modes_field(entries, N, kfactor=(1.0, 1.0, 1.0), basis="FOUR", physics="FLUID"):
+    """Init_cond_modes_SIMPLE (init_cond_modes.cc:107-480): entries (kx, ky, kz, Vx, Vy[, Wx, Wy
+    | G]) as in_field_in.d lists them; Last_component gives each vector's third component and
+    Add_complex_conj the conjugate mode on the kz = 0 and kz = N3/2 planes (the same rules as the
+    given-mode force, forcing.given_modes)."""
+    from . import forcing
+    k, F = forcing.given_modes(entries, N, kfactor, basis, physics)
+    return modes_to_fields(k, F, N, basis)
+
+
+def model_shell_spectrum(n, a):
+    """Model_initial_shell_spectrum (array_basic.cc:1400-1425): Sk(k) = a k^4 exp(-b k^1.1) /
+    (k^4 + q^4)^(1 + 2.8/12), q = 1.5, b = 0.02, for k = 0 .. n-1."""
+    kk = np.arange(n, dtype=np.float64)
+    return a * kk ** 4 * np.exp(-0.02 * kk ** 1.1) / (kk ** 4 + 1.5 ** 4) ** (1.0 + 2.8 / 12.0)
+
+
+def energy_spectrum_field(N, a, kfactor=(1.0, 1.0, 1.0), seed=20261202, dealias=True):
+    """Init_cond_energy_spectrum (init_cond_energy.cc:65-138, FOUR): the energy of shell ceil|K|
+    of the model spectrum, divided equally among the shell's modes, with random phases
+    (Put_vector_amp_phase_comp_conj), the mean mode zero, dealiased, reality condition.  The
+    reference seeds from time(0); numpy's PCG64 with `seed` stands in.  Returns [V1, V2, V3]."""
+    kmax = int(math.ceil(math.sqrt(sum((N[i] // 2 * kfactor[i]) ** 2 for i in range(3))))) + 2
+    Sk = model_shell_spectrum(kmax + 1, a)
+    return _random_phase(N, kfactor, lambda idx: Sk[np.minimum(idx.astype(int), kmax)], seed, dealias)
+
+
+def rb_lorenz_field(N, W101, T101, T200, kfactor=(1.0, 1.0, 1.0)):
+    """Init_cond_RB_Lorenz (init_cond_RB_misc.cc:55-85, SCFT): V1(1,0,1) = W101, V2(1,0,1) = 0, V3
+    from Last_component, theta(1,0,1) = T101, theta(2,0,0) = T200.  Returns [V1, V2, V3, theta]."""
+    from . import forcing
+    N1, N2, N3 = N
+    out = [np.zeros((N1, N2, N3 // 2 + 1), dtype=np.complex128) for _ in range(4)]
+    vx, vy, vz = forcing.last_component(1, 0, 1, complex(W101), 0j, kfactor, "SCFT")
+    out[0][1, 0, 1], out[1][1, 0, 1], out[2][1, 0, 1] = vx, vy, vz
+    out[3][1, 0, 1] = T101
+    out[3][2, 0, 0] = T200
+    return out
+
+
+def read_init_cond(cfg, data_dir=".", seed=20261202):
+    """IncFluid::Read_init_cond (init_cond_main.cc:52-206) for a configuration from
+    para.config_from_para: the initial state fields of its field_input_proc, read from
+    data_dir/in/field_in.d where the procedure reads a file."""
+    import os
+
+    run = cfg.get("run", {})
+    proc = run.get("field_input_proc", 0)
+    N, basis, physics = tuple(cfg["N"]), cfg.get("basis", "FOUR"), cfg.get("physics", "FLUID")
+    kf = tuple(cfg.get("kfactor", (1.0, 1.0, 1.0)))
+    dp = list(run.get("init_cond_double", [])) + [0.0] * 8
+    path = os.path.join(data_dir, "in", "field_in.d")
+    ns = _state_count(physics)
+    if proc in (1, 2):
+        from .solver import read_field_file
+        red = run.get("N_in_reduced") if proc == 2 else None
+        return read_field_file(path, N, ns, basis, kf, bool(run.get("input_vx_vy", 0)), red)
+    if proc == 3:
+        from . import forcing
+        nv = {3: 2, 6: 4, 4: 3}[ns]
+        return modes_field(forcing.read_force_modes_file(path, N[0], nv), N, kf, basis, physics)
+    if proc == 5 and ns == 3 and basis == "FOUR":
+        return energy_spectrum_field(N, dp[1], kf, seed)
+    if proc == 7 and physics.upper() != "RB":
+        # (convection: Init_cond_Taylor_Green_RB recurses into itself in the reference)
+        return taylor_green_field(N, int(dp[1]), dp[2], basis, physics, dp[3])
+    if proc == 8 and basis == "FOUR":
+        return abc_field(N, int(dp[1]), dp[5], dp[2], dp[3], dp[4], physics, dp[6])
+    if proc == 51 and physics.upper() == "RB":
+        return rb_lorenz_field(N, dp[1], dp[2], dp[3], kf)
+    raise ValueError(f"field_input_proc {proc} ({physics}, {basis}) is not built")

@@ -217,6 +217,10 @@ def config_from_para(p: dict, kind: str = "FLUID") -> dict:
     cfg["run"] = dict(Tinit=p["time_para"][1], Tfinal=p["time_para"][2],
                       output_vx_vy=p["switches"][19], input_vx_vy=p["switches"][20],
                       field_input_proc=p["init_cond_int"][1] if len(p["init_cond_int"]) > 1 else 0,
+                      init_cond_double=list(p["init_cond_double"]),
+                      N_in_reduced=tuple(p["init_cond_int"][2:5]) if (len(p["init_cond_int"]) > 4 and
+                                                                       p["init_cond_int"][1] == 2) else None,
+                      N_out_reduced=tuple(p["misc_output"][6:9]),
                       force_modes=run_force)
     return cfg
 

@@ -79,22 +79,31 @@ def make_config(N, basis="FOUR", physics="FLUID", precision="FP64", dealias=True
     return cfg
 
 
-def write_field_file(path, fields, time=0.0, vx_vy=False, append=False):
+def write_field_file(path, fields, time=0.0, vx_vy=False, append=False, reduced=None, basis="FOUR"):
     """Write state fields (each (N1, N2, N3/2+1) complex128, reference order) in the reference's
-    field-file text format (tg_write_field_file)."""
+    field-file text format (tg_write_field_file); with reduced = (Nr1, Nr2, Nr3) only the
+    low-wavenumber corner, as Output_field_reduced writes it (tg_write_field_file_reduced)."""
     lib = L.load()
     arrs = [np.ascontiguousarray(f, dtype=np.complex128) for f in fields]
     N1, N2, M3 = arrs[0].shape
     Nc = (C.c_int * 3)(N1, N2, 2 * (M3 - 1))
     ptrs = (_DP_T * len(arrs))(*[_dptr(a.view(np.float64)) for a in arrs])
-    rc = lib.tg_write_field_file(str(path).encode(), float(time), Nc, len(arrs), ptrs, 1 if vx_vy else 0,
-                                 1 if append else 0)
+    if reduced is None:
+        rc = lib.tg_write_field_file(str(path).encode(), float(time), Nc, len(arrs), ptrs, 1 if vx_vy else 0,
+                                     1 if append else 0)
+    else:
+        Nr = (C.c_int * 3)(*[int(n) for n in reduced])
+        b = _BASIS[basis] if isinstance(basis, str) else int(basis)
+        rc = lib.tg_write_field_file_reduced(str(path).encode(), float(time), Nc, Nr, b, len(arrs), ptrs,
+                                             1 if vx_vy else 0, 1 if append else 0)
     if rc != L.TG_OK:
         raise L.TarangError(rc, f"write_field_file {path}")
 
 
-def read_field_file(path, N, n_fields, basis="FOUR", kfactor=(1.0, 1.0, 1.0), vx_vy=False):
-    """Read n_fields state fields of grid N from a reference field file (tg_read_field_file)."""
+def read_field_file(path, N, n_fields, basis="FOUR", kfactor=(1.0, 1.0, 1.0), vx_vy=False, reduced=None):
+    """Read n_fields state fields of grid N from a reference field file (tg_read_field_file);
+    with reduced = (Nr1, Nr2, Nr3) the file holds the low-wavenumber corner only (a smaller run's
+    field file or Output_field_reduced; tg_read_field_file_reduced, as Init_cond_reduced)."""
     lib = L.load()
     shape = (N[0], N[1], N[2] // 2 + 1)
     arrs = [np.zeros(shape, dtype=np.complex128) for _ in range(n_fields)]
@@ -102,7 +111,11 @@ def read_field_file(path, N, n_fields, basis="FOUR", kfactor=(1.0, 1.0, 1.0), vx
     kf = (C.c_double * 3)(*[float(k) for k in kfactor])
     ptrs = (_DP_T * n_fields)(*[_dptr(a.view(np.float64)) for a in arrs])
     b = _BASIS[basis] if isinstance(basis, str) else int(basis)
-    rc = lib.tg_read_field_file(str(path).encode(), Nc, b, kf, n_fields, ptrs, 1 if vx_vy else 0)
+    if reduced is None:
+        rc = lib.tg_read_field_file(str(path).encode(), Nc, b, kf, n_fields, ptrs, 1 if vx_vy else 0)
+    else:
+        Nr = (C.c_int * 3)(*[int(n) for n in reduced])
+        rc = lib.tg_read_field_file_reduced(str(path).encode(), Nc, Nr, b, kf, n_fields, ptrs, 1 if vx_vy else 0)
     if rc != L.TG_OK:
         raise L.TarangError(rc, f"read_field_file {path}")
     return arrs
@@ -340,15 +353,18 @@ class IncFluid:
             out.append(self.get_T())
         return out
 
-    def Output_field(self, path, vx_vy=False, append=False):
-        """IncFluid::Output_field (output_field.cc:43-108): the state at the current time."""
-        write_field_file(path, self.state_fields(), self.time()[0], vx_vy, append)
+    def Output_field(self, path, vx_vy=False, append=False, reduced=None):
+        """IncFluid::Output_field (output_field.cc:43-108): the state at the current time; with
+        reduced = N_out_reduced, Output_field_reduced (output_field.cc:505-600)."""
+        basis = "SCFT" if self.cfg.basis == L.TG_SCFT else "FOUR"
+        write_field_file(path, self.state_fields(), self.time()[0], vx_vy, append, reduced, basis)
 
-    def Init_cond_from_file(self, path, vx_vy=False):
-        """IncFluid::Init_cond (init_cond_field.cc:47-223): the state read from a field file."""
+    def Init_cond_from_file(self, path, vx_vy=False, reduced=None):
+        """IncFluid::Init_cond (init_cond_field.cc:47-223): the state read from a field file;
+        with reduced = N_in_reduced, Init_cond_reduced (init_cond_field.cc:294-400)."""
         n = {L.TG_MHD: 6, L.TG_SCALAR: 4, L.TG_RB: 4}.get(self.cfg.physics, 3)
         basis = "SCFT" if self.cfg.basis == L.TG_SCFT else "FOUR"
-        f = read_field_file(path, self.N, n, basis, tuple(self.cfg.kfactor), vx_vy)
+        f = read_field_file(path, self.N, n, basis, tuple(self.cfg.kfactor), vx_vy, reduced)
         self.set_V(f[:3])
         if n == 6:
             self.set_W(f[3:])

@@ -70,6 +70,74 @@ def test_short_or_malformed_file(lib, tmp_path):
         read_field_file(tmp_path / "missing.d", (1, 2, 2), 1)
 
 
+def test_reduced_exact_text(lib, tmp_path):
+    """Output_field_reduced of a 4 x 4 x 4 field to (2, 2, 2): rows kx 0, 1 (FOUR, Nr1/2 + 1 rows
+    then none below), ky 0, 1, kz 0, 1, no separators."""
+    from tarang_b200.solver import write_field_file
+    A = np.zeros((4, 4, 3), dtype=np.complex128)
+    for i in range(4):
+        for j in range(4):
+            for k in range(3):
+                A[i, j, k] = complex(100 * i + 10 * j + k, 1)
+    p = tmp_path / "r.d"
+    write_field_file(p, [A], time=1.0, reduced=(2, 2, 2))
+    want = "%% Time = 1\n(0,1)(1,1)(10,1)(11,1)(100,1)(101,1)(110,1)(111,1)\n\n"
+    assert p.read_text() == want
+
+
+@pytest.mark.parametrize("basis", ["FOUR", "SCFT"])
+def test_reduced_embeds_a_smaller_run(lib, tmp_path, basis):
+    """A field file of an Nr grid read with N_in_reduced = Nr into an N grid: every mode of the
+    smaller grid lands at the same wavenumber; the +Nr/2 rows also fill -Nr/2; the rest is zero.
+    Writing the N-grid field reduced to Nr gives back the smaller grid's text."""
+    from tarang_b200.solver import read_field_file, write_field_file
+    Nr, N = (8, 8, 8), (16, 12, 16)
+    rng = np.random.default_rng(5)
+    small = [rng.standard_normal((8, 8, 5)) + 1j * rng.standard_normal((8, 8, 5)) for _ in range(3)]
+    p = tmp_path / "small.d"
+    write_field_file(p, small, time=0.0)
+    big = read_field_file(p, N, 3, basis, reduced=Nr)
+    four = basis == "FOUR"
+    for s_, b_ in zip(small, big):
+        for i in range(8):
+            kx = (i if i <= 4 else i - 8) if four else i
+            li = kx % 16 if four else kx
+            for j in range(8):
+                ky = j if j <= 4 else j - 8
+                assert np.allclose(b_[li, ky % 12, :5], s_[i, j, :5], rtol=1e-11, atol=0)
+        # duplicated Nyquist rows and zeros elsewhere
+        assert np.allclose(b_[:, 12 - 4, :5][[0, 1, 2, 3]], b_[:, 4, :5][[0, 1, 2, 3]])
+        assert np.all(b_[:, :, 5:] == 0)
+        if four:
+            assert np.allclose(b_[16 - 4], b_[4])
+            assert np.all(b_[5:12] == 0)
+    q = tmp_path / "again.d"
+    write_field_file(q, big, time=0.0, reduced=Nr, basis=basis)
+    again = read_field_file(q, Nr, 3, basis, reduced=Nr)
+    for s_, a_ in zip(small, again):
+        assert np.abs(s_ - a_).max() <= 1e-11 * np.abs(s_).max()
+
+
+def test_reduced_vx_vy_and_errors(lib, tmp_path):
+    from tarang_b200.solver import read_field_file, write_field_file
+    N, Nr = (16, 16, 16), (8, 8, 8)
+    V = ic.random_phase_field(Nr, k0=2.0, seed=3)
+    p = tmp_path / "vxvy.d"
+    write_field_file(p, V, vx_vy=True)
+    g = read_field_file(p, N, 3, vx_vy=True, reduced=Nr)
+    # V3 rebuilt from incompressibility on the big grid; the stored corner equals the small field
+    Kx = np.fft.fftfreq(16, 1 / 16)[:, None, None]
+    Ky = np.fft.fftfreq(16, 1 / 16)[None, :, None]
+    Kz = np.arange(9)[None, None, :]
+    div = 1j * (Kx * g[0] + Ky * g[1] + Kz * g[2])
+    assert np.abs(div[:, :, 1:]).max() <= 1e-10 * np.abs(g[0]).max()
+    assert np.allclose(g[2][1, 1, :5], V[2][1, 1, :5], rtol=1e-9)
+    with pytest.raises(L.TarangError):
+        read_field_file(p, N, 3, reduced=(7, 8, 8))          # FOUR Nr1 odd
+    with pytest.raises(L.TarangError):
+        read_field_file(p, N, 3, reduced=(32, 8, 8))         # larger than N
+
+
 @pytest.mark.gpu
 def test_context_round_trip(lib, tmp_path):
     """Output_field of a context, read into a new context: the same stored state."""
