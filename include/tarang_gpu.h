@@ -219,6 +219,26 @@ int tg_energy(tg_ctx* ctx, int group, double* energy, double* dissipation);
 /* CV_Compute_shell_spectrum (Cvf.cc:419-449): ek = [3][n] per component (group T: [1][n]),
  * dissk = [n] (may be NULL).  n must be >= kmax_outside + 1. */
 int tg_shell_spectrum(tg_ctx* ctx, int group, double* ek, double* dissk, int n);
+/* Anisotropic spectra of the velocity (group 0) or magnetic field (group 1, MHD), FOUR basis,
+ * about the anisotropy axis `axis` (1 x, 2 y, 3 z: globalvar_anisotropy_switch).
+ * tg_ring_spectrum: CVF::CV_Compute_ring_spectrum (fields/Cvf.cc:484-504 with
+ * Compute_local_ring_spectrum_FOUR four/four_energy.cc:828-955): spherical shells 0 .. kmax
+ * (Max_radius_inside) x polar sectors 0 .. n_sectors of equal angle up to pi/2 (Cvf.cc:84-100,
+ * Get_sector_index basis_basicfn.cc:304-320); ek1 sums mult |(V x K)_axis / K_perp|^2 (on the
+ * axis, the first transverse component), ek2 the rest of mult |V|^2, dissk = 2 (S1 + S2) with a
+ * K^2 weight.  tg_cylinder_ring_spectrum: CV_Compute_cylinder_ring_spectrum (Cvf.cc:537-559
+ * with four_energy.cc:1450-1516): cylindrical shells ceil(K_perp) 0 .. Anis_max_Krho_radius_inside
+ * x slabs 0 .. n_slabs of equal |K_par| up to Anis_max_Kpll (Cvf.cc:168-190, Get_slab_index
+ * basis_basicfn.cc:373-390); ek1 sums mult |V_axis|^2, ek2 the rest.  Arrays are
+ * [shells][n + 1] row-major (column 0 stays empty as in the reference); n = capacity of each
+ * array in doubles; ek2, dissk may be NULL.  n_sectors, n_slabs <= TG_RING_MAX_SECTORS.
+ * For axis 3 the reference's on-axis and cylinder branches test the axis-2 switch twice (an
+ * uninitialised value); the z-axis components are used. */
+#define TG_RING_MAX_SECTORS 64
+int tg_ring_sizes(tg_ctx* ctx, int axis, int* ring_shells, int* cylinder_shells);
+int tg_ring_spectrum(tg_ctx* ctx, int group, int axis, int n_sectors, double* ek1, double* ek2, double* dissk, int n);
+int tg_cylinder_ring_spectrum(tg_ctx* ctx, int group, int axis, int n_slabs, double* ek1, double* ek2, double* dissk,
+                              int n);
 /* shell radii of the energy transfer (EnergyTr.cc:136-160): n_shells + 1 doubles */
 int tg_et_radii(tg_ctx* ctx, double* radii, int n);
 /* Compute_flux (compute_flux.cc:52-304): flux[s], s = 0..n_shells (index 0 unused) */

@@ -521,6 +521,111 @@ def rhs_from_nlin(nl, p, kfactor, basis="FOUR"):
 
 
 # --------------------------------------------------------------------------------------
+# Anisotropic spectra  (lib/four/four_energy.cc ring parts, lib/fields/Cvf.cc:84-190, 484-560)
+# --------------------------------------------------------------------------------------
+
+def _polar_angle(kperp, kpll):
+    """Get_polar_angle  basis_basicfn_inline.h:89-113: atan(k_perp/k_par) in [0, pi)."""
+    if abs(kperp) > MYEPS:
+        t = math.atan(kperp / kpll) if abs(kpll) > MYEPS else math.pi / 2
+    else:
+        t = 0.0 if kpll >= 0 else math.pi
+    return t if t >= 0 else t + math.pi
+
+
+def _sector_index(theta, bounds):
+    """Get_sector_index  basis_basicfn.cc:304-320."""
+    if theta > math.pi / 2:
+        theta = math.pi - theta
+    if abs(theta) < MYEPS:
+        return 1
+    for i, b in enumerate(bounds):
+        if theta <= b:
+            return i
+    return len(bounds)
+
+
+def _slab_index(kpll, bounds):
+    """Get_slab_index  basis_basicfn.cc:373-390."""
+    kpll = abs(kpll)
+    if kpll < MYEPS:
+        return 1
+    for i in range(1, len(bounds)):
+        if kpll <= bounds[i]:
+            return i
+    return len(bounds)
+
+
+def ring_spectrum(V, kfactor, axis, n_sectors, alias="DEALIAS", cylinder=False):
+    """CVF::CV_Compute_ring_spectrum (Cvf.cc:484-504; Compute_local_ring_spectrum_FOUR
+    four_energy.cc:828-955) or, with cylinder=True, CV_Compute_cylinder_ring_spectrum
+    (Cvf.cc:537-559; Compute_local_cylinder_ring_spectrum_FOUR four_energy.cc:1450-1516), FOUR,
+    anisotropy axis 1..3.  Returns (ek1, ek2, dissk), each [shells][n + 1]; dissk = 2 (S1 + S2)
+    with weight K^2.  Pure-Python loop over the modes: small grids only."""
+    N1, N2 = V[0].shape[0], V[0].shape[1]
+    N3 = 2 * (V[0].shape[2] - 1)
+    N = (N1, N2, N3)
+    d = 3 if alias == "DEALIAS" else 2
+    ax = axis - 1
+    p1, p2 = (ax + 1) % 3, (ax + 2) % 3
+    Nn = (N1, N2, N3)
+    n = n_sectors
+    if not cylinder:
+        rows = max_radius_inside(N, kfactor, alias) + 1
+        dth = (math.pi / 2) / n
+        bounds = [i * dth for i in range(n)] + [math.pi / 2]
+    else:
+        rows = int(min((Nn[p1] // d) * kfactor[p1], (Nn[p2] // d) * kfactor[p2])) + 1
+        kmax = (Nn[ax] // d) * kfactor[ax]
+        dk = kmax / n
+        bounds = [0.0] + [i * dk for i in range(1, n)] + [kmax]
+    out = np.zeros((4, rows, n + 1))
+    mult = multiplicity_four(N)
+    kx_, ky_, kz_ = kx_four(N1), ky_four(N2), kz_four(N3)
+    A = [np.asarray(v) for v in V]
+    for l1 in range(N1):
+        for l2 in range(N2):
+            for l3 in range(N3 // 2 + 1):
+                vals = [A[c][l1, l2, l3] for c in range(3)]
+                vv = sum(abs(x) ** 2 for x in vals)
+                if vv == 0.0:
+                    continue
+                k = (kx_[l1] * kfactor[0], ky_[l2] * kfactor[1], kz_[l3] * kfactor[2])
+                kpll = k[ax]
+                kperp = math.sqrt(k[p1] ** 2 + k[p2] ** 2)
+                K2 = k[0] ** 2 + k[1] ** 2 + k[2] ** 2
+                K = math.sqrt(K2)
+                f = mult[l1, l2, l3]
+                if not cylinder:
+                    row = math.ceil(K)
+                    if not (K > MYEPS) or row >= rows:
+                        continue
+                    col = _sector_index(_polar_angle(kperp, kpll), bounds)
+                    if kperp < MYEPS:
+                        c1, c2 = {0: (1, 2), 1: (2, 1), 2: (0, 1)}[ax]
+                        e1, e2 = abs(vals[c1]) ** 2, abs(vals[c2]) ** 2
+                    else:
+                        # cross(V, K)_axis / k_perp
+                        c = vals[p1] * k[p2] - vals[p2] * k[p1]
+                        e1 = abs(c) ** 2 / kperp ** 2
+                        e2 = vv - e1
+                else:
+                    row = math.ceil(kperp)
+                    if row >= rows:
+                        continue
+                    col = _slab_index(kpll, bounds)
+                    e1 = abs(vals[ax]) ** 2
+                    e2 = vv - e1
+                if col >= n + 1:
+                    continue
+                out[0, row, col] += f * e1
+                out[1, row, col] += f * e2
+                out[2, row, col] += f * K2 * e1
+                out[3, row, col] += f * K2 * e2
+    return out[0], out[1], 2.0 * (out[2] + out[3])
+
+
+# --------------------------------------------------------------------------------------
 # Forcing  (lib/IncFluid/force)
 # --------------------------------------------------------------------------------------
 

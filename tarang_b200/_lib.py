@@ -27,6 +27,7 @@ TG_FP64, TG_FP32_MIXED = 0, 1
 TG_RK4 = 4
 TG_FORCE_DECAY, TG_FORCE_ENERGY_SUPPLY, TG_FORCE_MODES, TG_FORCE_CORIOLIS, TG_FORCE_RB = 0, 1, 5, 21, 51
 TG_FORCE_MODES_KMAX = 64
+TG_RING_MAX_SECTORS = 64
 TG_RB_PRLARGE, TG_RB_PRSMALL = 0, 1
 TG_RB_ULARGE, TG_RB_USMALL = 0, 1
 
@@ -168,6 +169,9 @@ SIGNATURES = {
     "tg_energy": (C.c_int, [_VP, C.c_int, _DP, _DP]),
     "tg_shell_spectrum": (C.c_int, [_VP, C.c_int, _DP, _DP, C.c_int]),
     "tg_et_radii": (C.c_int, [_VP, _DP, C.c_int]),
+    "tg_ring_sizes": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "tg_ring_spectrum": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, _DP, _DP, _DP, C.c_int]),
+    "tg_cylinder_ring_spectrum": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, _DP, _DP, _DP, C.c_int]),
     "tg_flux": (C.c_int, [_VP, C.c_int, _DP, C.c_int]),
     "tg_shell_to_shell": (C.c_int, [_VP, C.c_int, _DP, C.c_int]),
     "tg_nusselt": (C.c_int, [_VP, _DP]),

@@ -799,6 +799,8 @@ void state_viscosities(const tg_config* cfg, double nu[6]) {
 
 int ensure_staging_ctx(tg_ctx* c) { return ensure_staging(c); }
 
+int radius_inside(const tg_ctx* c) { return max_radius_inside(c); }
+
 int ensure_force_box(tg_ctx* c) {
   if (c->force_on != 1 || c->force_ever) return TG_OK;
   const void* U[3] = {c->U0[0], c->U0[1], c->U0[2]};

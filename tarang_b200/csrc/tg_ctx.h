@@ -162,4 +162,8 @@ int run_energy(tg_ctx* c, int dt_mode);
 int run_energy_slots(tg_ctx* c, int dt_mode, int r0, int n);
 // the force box from the current state if this context never computed a force (else unchanged)
 int ensure_force_box(tg_ctx* c);
+// Max_radius_inside (four_inline.h:190-257, scft_inline.h) of the context's grid
+int radius_inside(const tg_ctx* c);
+// the diagnostics scratch c->diag grown to at least `need` doubles
+int ensure_diag(tg_ctx* c, size_t need);
 }  // namespace tg

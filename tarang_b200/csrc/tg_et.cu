@@ -48,11 +48,7 @@ std::vector<double> et_radii(const tg_ctx* c) {
   return R;
 }
 
-}  // namespace tg
-
-namespace {
-
-// the context's diagnostics scratch, grown to at least `need` doubles
+// the context's diagnostics scratch (c->diag) grown to at least `need` doubles
 int ensure_diag(tg_ctx* c, size_t need) {
   if (c->diag_cap >= need) return TG_OK;
   if (c->diag) {
@@ -66,6 +62,10 @@ int ensure_diag(tg_ctx* c, size_t need) {
   c->diag_cap = need;
   return TG_OK;
 }
+
+}  // namespace tg
+
+namespace {
 
 constexpr int TPB = 256;
 constexpr int kMaxShells = 63;

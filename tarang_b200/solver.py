@@ -330,6 +330,25 @@ class IncFluid:
         self._ck(self.lib.tg_shell_to_shell(self.h, kind, _dptr(t), S + 1), "shell_tr")
         return t.reshape(S + 1, S + 1)
 
+    def _ring(self, fn, cyl, n, axis, group):
+        rs, cs = C.c_int(), C.c_int()
+        self._ck(self.lib.tg_ring_sizes(self.h, axis, C.byref(rs), C.byref(cs)), "ring sizes")
+        rows = cs.value if cyl else rs.value
+        out = [np.zeros((rows, n + 1)) for _ in range(3)]
+        self._ck(fn(self.h, group, axis, n, *[_dptr(a) for a in out], rows * (n + 1)), "ring spectrum")
+        return tuple(out)
+
+    def CV_Compute_ring_spectrum(self, n_sectors, axis=1, group=0):
+        """CVF::CV_Compute_ring_spectrum (tg_ring_spectrum): (ek1, ek2, dissk), each
+        [shell][sector] over shells 0..Max_radius_inside and sectors 0..n_sectors about `axis`
+        (1 x, 2 y, 3 z); group 0 velocity, 1 magnetic field."""
+        return self._ring(self.lib.tg_ring_spectrum, False, n_sectors, axis, group)
+
+    def CV_Compute_cylinder_ring_spectrum(self, n_slabs, axis=1, group=0):
+        """CVF::CV_Compute_cylinder_ring_spectrum (tg_cylinder_ring_spectrum): (ek1, ek2,
+        dissk), each [cylindrical shell][slab] along `axis`."""
+        return self._ring(self.lib.tg_cylinder_ring_spectrum, True, n_slabs, axis, group)
+
     def Compute_force_feed_shell(self):
         """IncVF::Compute_force_feed_shell (compute_force_feed.cc:70-76): forceV_shell, S+1 entries."""
         S = self.cfg.n_shells

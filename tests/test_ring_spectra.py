@@ -1,0 +1,87 @@
+"""Ring and cylindrical-ring spectra (CV_Compute_ring_spectrum / CV_Compute_cylinder_ring_spectrum,
+FOUR): the oracle against a hand-computed single mode and against the isotropic shell spectrum
+(summing the sectors of a shell gives the shell), and the CUDA path against the oracle on random
+fields for every anisotropy axis, the magnetic field of MHD and anisotropic grids."""
+
+import math
+
+import numpy as np
+import pytest
+
+from oracle import tarang_oracle as o
+from tarang_b200 import ic
+
+KF = (1.0, 1.0, 1.0)
+
+
+def test_single_mode_by_hand():
+    N = (16, 16, 16)
+    V = [np.zeros((16, 16, 9), dtype=np.complex128) for _ in range(3)]
+    V[0][0, 1, 1] = 1.0          # V = (1, 0, 0) at K = (0, 1, 1)
+    e1, e2, d = o.ring_spectrum(V, KF, 3, 3)
+    # theta = atan(1 / 1) = pi/4 <= pi/3: sector 2; shell ceil(sqrt 2) = 2;
+    # (V x K)_z / K_perp = (1 * 1 - 0) / 1 = 1, so all of |V|^2 is in S1
+    assert e1[2, 2] == 1.0 and e1.sum() == 1.0 and e2.sum() == 0.0
+    assert d[2, 2] == pytest.approx(2 * 2.0)
+    c1, c2, _ = o.ring_spectrum(V, KF, 3, 4, cylinder=True)
+    # cylinder about z: K_perp = 1 (shell 1), |K_par| = 1 in slab ceil(1 / (5 / 4)) = 1
+    assert c1.sum() == 0.0 and c2[1, 1] == 1.0
+
+
+@pytest.mark.parametrize("axis", [1, 2, 3])
+def test_sectors_sum_to_the_shell_spectrum(axis):
+    """Summed over sectors a shell holds the shell spectrum, except that for the y axis the
+    reference records (V_z, V_y) on the axis itself (four_energy.cc:870-874), so |V_x|^2 of the
+    modes on the y axis is missing from its ring spectrum; there the identity holds off the axis."""
+    N = (16, 16, 16)
+    V = ic.random_phase_field(N, seed=11 + axis)
+    if axis == 2:
+        for v in V:
+            v[0, :, 0] = 0          # no modes on the y axis
+    e1, e2, d = o.ring_spectrum(V, KF, axis, 5)
+    shell = sum(o.shell_spectrum(v, 0, KF) for v in V)
+    kin = o.max_radius_inside(N, KF)
+    tot = (e1 + e2).sum(axis=1)
+    assert np.allclose(tot[1:kin + 1], shell[1:kin + 1], rtol=1e-12, atol=1e-18)
+    dshell = 2 * sum(o.shell_spectrum(v, 2, KF) for v in V)
+    assert np.allclose(d.sum(axis=1)[1:kin + 1], dshell[1:kin + 1], rtol=1e-12, atol=1e-18)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("axis", [1, 2, 3])
+@pytest.mark.parametrize("n", [1, 4, 5])
+def test_gpu_ring_spectra_match_oracle(lib, axis, n):
+    from tarang_b200.solver import IncFluid
+    N = (32, 16, 24)
+    kf = (1.0, 2.0, 0.5)
+    V = ic.random_phase_field(N, kfactor=kf, seed=40 + 3 * axis + n)
+    s = IncFluid(N, kfactor=kf, nu=1e-3, dt=1e-3)
+    s.set_V(V)
+    for cyl in (False, True):
+        got = s.CV_Compute_cylinder_ring_spectrum(n, axis) if cyl else s.CV_Compute_ring_spectrum(n, axis)
+        want = o.ring_spectrum(V, kf, axis, n, cylinder=cyl)
+        for g, w in zip(got, want):
+            assert g.shape == w.shape
+            assert np.abs(g - w).max() <= 1e-12 * np.abs(w).max(), (cyl, axis, n)
+
+
+@pytest.mark.gpu
+def test_gpu_ring_spectra_mhd_magnetic_field(lib):
+    from tarang_b200 import _lib as L
+    from tarang_b200.solver import IncFluid
+    N = (32, 32, 32)
+    V = ic.random_phase_field(N, seed=61)
+    W = ic.random_phase_field(N, k0=3.0, seed=62)
+    s = IncFluid(N, physics="MHD", nu=1e-3, eta=1e-3, dt=1e-3)
+    s.set_V(V)
+    s.set_W(W)
+    for group, F in ((0, V), (1, W)):
+        got = s.CV_Compute_ring_spectrum(6, 3, group)
+        want = o.ring_spectrum(F, KF, 3, 6)
+        for g, w in zip(got, want):
+            assert np.abs(g - w).max() <= 1e-12 * np.abs(w).max()
+    f = IncFluid(N, nu=1e-3, dt=1e-3)
+    with pytest.raises(L.TarangError):
+        f.CV_Compute_ring_spectrum(6, 3, 1)          # no magnetic field
+    with pytest.raises(L.TarangError):
+        f.CV_Compute_ring_spectrum(65, 1)             # more sectors than the maximum
