@@ -239,6 +239,17 @@ int tg_ring_sizes(tg_ctx* ctx, int axis, int* ring_shells, int* cylinder_shells)
 int tg_ring_spectrum(tg_ctx* ctx, int group, int axis, int n_sectors, double* ek1, double* ek2, double* dissk, int n);
 int tg_cylinder_ring_spectrum(tg_ctx* ctx, int group, int axis, int n_slabs, double* ek1, double* ek2, double* dissk,
                               int n);
+/* Ring-to-ring energy transfer (IncVF::Compute_ring_tr, EnergyTrdir/compute_ring_tr.cc:60-90 and
+ * the MHD kinds :174-215; Fill_array_ring universal_ET.cc:70-100, Local_ring_mult_all_FOUR
+ * four/four_ET.cc:330-386), FOUR: tr[i][j][m][s], (n_ring_shells+1) x (n_sectors+1) x
+ * (n_ring_shells+1) x (n_sectors+1) doubles, is the transfer from giver ring (shell i =
+ * 1..n_ring_shells-1, sector j = 1..n_sectors) to receiver ring (m, s).  kind TG_ET_UU
+ * (ring_to_ring_self), and for MHD TG_ET_BB (W.ring_to_ring_self) and TG_ET_UB
+ * (ring_to_ring_VF, U to B).  Ring radii: scheme 0 (EnergyTr.cc:190-210; tg_ring_radii), 5 <=
+ * n_ring_shells <= 32; sectors of equal angle up to pi/2 about `axis`.  As in the reference, a
+ * giver ring holds only the modes with theta <= pi/2 (K_par >= 0), while receivers fold theta. */
+int tg_ring_radii(tg_ctx* ctx, int n_ring_shells, double* radii, int n);
+int tg_ring_to_ring(tg_ctx* ctx, int kind, int axis, int n_ring_shells, int n_sectors, double* tr, int n);
 /* shell radii of the energy transfer (EnergyTr.cc:136-160): n_shells + 1 doubles */
 int tg_et_radii(tg_ctx* ctx, double* radii, int n);
 /* Compute_flux (compute_flux.cc:52-304): flux[s], s = 0..n_shells (index 0 unused) */

@@ -1143,6 +1143,71 @@ def compute_shell_tr_generic(H, F, Rf, sign, kfactor, no_shells, alias="DEALIAS"
     return T
 
 
+def ring_radii(N, kfactor, n_ring_shells, alias="DEALIAS", basis="FOUR"):
+    """EnergyTr::EnergyTr ring shell radii, scheme 0  EnergyTr.cc:190-210."""
+    Rin = float(max_radius_inside(N, kfactor, alias, basis))
+    n = n_ring_shells
+    r = [0.0] * (n + 1)
+    r[1], r[2] = 4.0, 8.0
+    r[n - 2], r[n - 1], r[n] = Rin / 2, Rin, INF_RADIUS
+    if n > 5:
+        s = math.log2(Rin / 16.0) / (n - 4)
+        for i in range(3, n - 2):
+            r[i] = 8 * 2.0 ** (s * (i - 2))
+    return r
+
+
+def _theta_grid(N, kfactor, axis):
+    """AnisKvect_polar_angle_FOUR on the dense grid: unfolded, in [0, pi)."""
+    K = kvec(N, kfactor)
+    shape = (N[0], N[1], N[2] // 2 + 1)
+    K = [np.broadcast_to(k, shape) for k in K]
+    ax = axis - 1
+    kpll = K[ax]
+    kperp = np.sqrt(K[(ax + 1) % 3] ** 2 + K[(ax + 2) % 3] ** 2)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        t = np.where(np.abs(kperp) > MYEPS,
+                     np.where(np.abs(kpll) > MYEPS, np.arctan(kperp / kpll), math.pi / 2),
+                     np.where(kpll >= 0, 0.0, math.pi))
+    return np.where(t >= 0, t, t + math.pi)
+
+
+def compute_ring_tr_generic(H, F, Rf, sign, kfactor, axis, n_ring_shells, n_sectors, alias="DEALIAS"):
+    """IncVF::Compute_ring_tr  compute_ring_tr.cc:60-90 (MHD kinds :174-215) in one form:
+    giver ring (i, j): G = F on r[i-1] < |K| <= r[i], sector_{j-1} < theta <= sector_j
+    (Fill_array_ring universal_ET.cc:70-100), N = D_j F(H_j G_i); T[i, j, m, s] = sign *
+    sum over receiver ring (m, s) of 2 mult Re(N . Rf*) (Local_ring_mult_all_FOUR
+    four_ET.cc:330-386 with Compute_ring_index basis_basicfn.cc:324-352)."""
+    N = (H[0].shape[0], H[0].shape[1], 2 * (H[0].shape[2] - 1))
+    R = ring_radii(N, kfactor, n_ring_shells, alias)
+    dth = (math.pi / 2) / n_sectors
+    sec = [i * dth for i in range(n_sectors)] + [math.pi / 2]
+    K = kmag(N, kfactor)
+    th = _theta_grid(N, kfactor, axis)
+    kin = max_radius_inside(N, kfactor, alias)
+    mult = multiplicity_four(N)
+    sel = (K <= kin) & (K > MYEPS)
+    shell = shell_index(K, R)
+    thf = np.where(th > math.pi / 2, math.pi - th, th)
+    sector = np.full(K.shape, len(sec), dtype=np.int64)
+    for i in range(len(sec) - 1, -1, -1):
+        sector = np.where(thf <= sec[i], i, sector)
+    sector = np.where(np.abs(thf) < MYEPS, 1, sector)
+    n1, n2 = n_ring_shells + 1, n_sectors + 1
+    ok = sel & (shell <= n_ring_shells) & (sector <= n_sectors)
+    flat = (shell * n2 + sector)[ok]
+    T = np.zeros((n1, n2, n1, n2))
+    for i in range(1, n_ring_shells):
+        for j in range(1, n_sectors + 1):
+            lo, hi, left, right = R[i - 1], R[i], sec[j - 1], sec[j]
+            inr = (K > lo) & (K <= hi) & (((th > left) & (th <= right)) | ((np.abs(th) < MYEPS) & (left < MYEPS)))
+            G = [np.where(inr, f, 0) for f in F]
+            nl = et_nlin(H, G, kfactor)
+            val = 2 * mult * sum(np.real(a * np.conj(b)) for a, b in zip(nl, Rf))
+            T[i, j] = sign * np.bincount(flat, weights=val[ok], minlength=n1 * n2).reshape(n1, n2)
+    return T
+
+
 # --------------------------------------------------------------------------------------
 # Convenience: the reference's packed real layout (N1, N2, N3/2+1) complex <-> (N1, N2, N3)
 # --------------------------------------------------------------------------------------

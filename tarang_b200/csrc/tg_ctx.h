@@ -166,4 +166,6 @@ int ensure_force_box(tg_ctx* c);
 int radius_inside(const tg_ctx* c);
 // the diagnostics scratch c->diag grown to at least `need` doubles
 int ensure_diag(tg_ctx* c, size_t need);
+// energy-transfer buffers (giver fields etG, helper transforms etWY, products etPP/PY/PX)
+int ensure_et_buffers(tg_ctx* c);
 }  // namespace tg

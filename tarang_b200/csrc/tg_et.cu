@@ -63,6 +63,46 @@ int ensure_diag(tg_ctx* c, size_t need) {
   return TG_OK;
 }
 
+// transfer scratch: etG (giver fields) and the helper / product pipeline buffers
+int ensure_et_buffers(tg_ctx* c) {
+  if (c->et_ready) return TG_OK;
+  const Geo& g = c->g;
+  const size_t Sd = sizeof(cx<double>) * (size_t)g.S;
+  const size_t St = c->tsz * (size_t)g.S;
+  const size_t WXb = c->tsz * (size_t)c->N1 * g.nky * g.kzp;
+  const size_t WYb = c->tsz * (size_t)c->N1 * c->N2 * g.kzp;
+  for (int i = 0; i < 3; ++i) {
+    int rc = dalloc_ctx(c, (void**)&c->etG[i], Sd);
+    if (rc) return rc;
+  }
+  for (int i = 0; i < 6; ++i) {
+    if (i < c->nin) {
+      c->etWY[i] = c->WY[i];
+    } else {
+      int rc = dalloc_ctx(c, &c->etWY[i], WYb);
+      if (rc) return rc;
+      c->et_own[c->n_et_own++] = c->etWY[i];
+    }
+  }
+  for (int q = 0; q < 9; ++q) {
+    if (q < c->nprod) {
+      c->etPP[q] = c->PP[q];
+      c->etPY[q] = c->PY[q];
+      c->etPX[q] = c->PX[q];
+    } else {
+      int rc = dalloc_ctx(c, &c->etPP[q], WYb);
+      if (!rc) rc = dalloc_ctx(c, &c->etPY[q], WXb);
+      if (!rc) rc = dalloc_ctx(c, &c->etPX[q], St);
+      if (rc) return rc;
+      c->et_own[c->n_et_own++] = c->etPP[q];
+      c->et_own[c->n_et_own++] = c->etPY[q];
+      c->et_own[c->n_et_own++] = c->etPX[q];
+    }
+  }
+  c->et_ready = true;
+  return TG_OK;
+}
+
 }  // namespace tg
 
 namespace {
@@ -161,44 +201,6 @@ bool kind_spec(const tg_ctx* c, int kind, KindSpec& k) {
   return c->phys == TG_MHD;
 }
 
-int ensure_et_buffers(tg_ctx* c) {
-  if (c->et_ready) return TG_OK;
-  const Geo& g = c->g;
-  const size_t Sd = sizeof(cx<double>) * (size_t)g.S;
-  const size_t St = c->tsz * (size_t)g.S;
-  const size_t WXb = c->tsz * (size_t)c->N1 * g.nky * g.kzp;
-  const size_t WYb = c->tsz * (size_t)c->N1 * c->N2 * g.kzp;
-  for (int i = 0; i < 3; ++i) {
-    int rc = dalloc_ctx(c, (void**)&c->etG[i], Sd);
-    if (rc) return rc;
-  }
-  for (int i = 0; i < 6; ++i) {
-    if (i < c->nin) {
-      c->etWY[i] = c->WY[i];
-    } else {
-      int rc = dalloc_ctx(c, &c->etWY[i], WYb);
-      if (rc) return rc;
-      c->et_own[c->n_et_own++] = c->etWY[i];
-    }
-  }
-  for (int q = 0; q < 9; ++q) {
-    if (q < c->nprod) {
-      c->etPP[q] = c->PP[q];
-      c->etPY[q] = c->PY[q];
-      c->etPX[q] = c->PX[q];
-    } else {
-      int rc = dalloc_ctx(c, &c->etPP[q], WYb);
-      if (!rc) rc = dalloc_ctx(c, &c->etPY[q], WXb);
-      if (!rc) rc = dalloc_ctx(c, &c->etPX[q], St);
-      if (rc) return rc;
-      c->et_own[c->n_et_own++] = c->etPP[q];
-      c->et_own[c->n_et_own++] = c->etPY[q];
-      c->et_own[c->n_et_own++] = c->etPX[q];
-    }
-  }
-  c->et_ready = true;
-  return TG_OK;
-}
 
 // Sorted distinct radii of the transfer shells (the reference's radii need not be monotonic
 // when R_in <= 16: EnergyTr.cc:118-126 only warns).

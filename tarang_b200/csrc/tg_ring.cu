@@ -14,6 +14,7 @@
 // One thread per stored mode; each block bins its modes in shared memory (atomics) and adds
 // its bins to the output once.  Modes the 2/3 rule does not store are zero in the reference's
 // arrays and add nothing there either.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -192,9 +193,209 @@ int run_ring(tg_ctx* c, int group, int axis, int n, int cyl, double* ek1, double
   return TG_OK;
 }
 
+// ---------------------------------------------------------------------------------- ring-to-ring
+// IncVF::Compute_ring_tr (EnergyTrdir/compute_ring_tr.cc:60-90, MHD kinds :174-215): for every
+// giver ring (ring shell i = 1 .. n-1, sector j = 1 .. n_sectors) G = F on that ring (Fill_ring
+// fill_ring.cc:70-90, Fill_array_ring universal_ET.cc:70-100), N = D_j F(H_j G_i)
+// (EnergyTr_Compute_nlin) and T[i][j][shell][sector] = sign * sum 2 mult Re(N . R*) over the
+// receiver rings (Local_ring_mult_all_FOUR four_ET.cc:330-386, Compute_ring_index
+// basis_basicfn.cc:324-352).  Ring radii: scheme 0 of EnergyTr.cc:190-210.
+
+constexpr int kMaxRingShells = 32;
+
+struct RingBins {
+  double r[kMaxRingShells + 1];  // ring shell radii 0 .. n (r[n] = INF_RADIUS)
+  int n;
+  double bound[kMaxBounds];      // sector angles 0 .. ns
+  int ns;
+  int axis;
+  double kin;                    // Max_radius_inside
+};
+
+__device__ __forceinline__ void mode_angle(const Geo& g, long long idx, int axis, int& r1, int& r2, int& l3,
+                                           double& K, double& theta, double k[3]) {
+  compact_mode(g, idx, r1, r2, l3);
+  k[0] = geo_kx(g, r1) * g.kf0;
+  k[1] = geo_ky(g, r2) * g.kf1;
+  k[2] = l3 * g.kf2;
+  const int ax = axis - 1, p1 = (ax + 1) % 3, p2 = (ax + 2) % 3;
+  K = sqrt(k[0] * k[0] + k[1] * k[1] + k[2] * k[2]);
+  theta = polar_angle(sqrt(k[p1] * k[p1] + k[p2] * k[p2]), k[ax]);
+}
+
+// G = F where inner < |K| <= outer and left < theta <= right (theta unfolded, in [0, pi)), or
+// theta = 0 in the first sector
+__global__ void k_fill_ring(Geo g, const cx<double>* F0, const cx<double>* F1, const cx<double>* F2, cx<double>* G0,
+                            cx<double>* G1, cx<double>* G2, double lo, double hi, double left, double right, int axis) {
+  const long long idx = (long long)blockIdx.x * TPB + threadIdx.x;
+  if (idx >= g.S) return;
+  int r1, r2, l3;
+  double K, th, k[3];
+  mode_angle(g, idx, axis, r1, r2, l3, K, th, k);
+  const bool in = (l3 < g.nkz) && (K > lo) && (K <= hi) &&
+                  ((th > left && th <= right) || (fabs(th) < kEps && left < kEps));
+  const cx<double> z = mkc<double>(0, 0);
+  G0[idx] = in ? F0[idx] : z;
+  G1[idx] = in ? F1[idx] : z;
+  G2[idx] = in ? F2[idx] : z;
+}
+
+struct RingContractArgs {
+  Geo g;
+  const void* PX[9];  // P(i, j) = F(H_j G_i), q = 3 i + j
+  const cx<double>* R[3];
+  RingBins b;
+  double* out;        // [n + 1][ns + 1]
+};
+
+template <typename Rp>
+__global__ void __launch_bounds__(TPB) k_ring_contract(RingContractArgs a) {
+  extern __shared__ double sh[];
+  const int cols = a.b.ns + 1, nbins = (a.b.n + 1) * cols;
+  for (int i = threadIdx.x; i < nbins; i += TPB) sh[i] = 0;
+  __syncthreads();
+  const Geo& g = a.g;
+  const long long stride = (long long)gridDim.x * TPB;
+  for (long long idx = (long long)blockIdx.x * TPB + threadIdx.x; idx < g.S; idx += stride) {
+    int r1, r2, l3;
+    double K, th, k[3];
+    mode_angle(g, idx, a.b.axis, r1, r2, l3, K, th, k);
+    if (l3 >= g.nkz || !(K <= a.b.kin && K > kEps)) continue;
+    int shell = 0;  // first radius >= |K| (the radii need not be sorted)
+    while (shell <= a.b.n && !(K <= a.b.r[shell])) ++shell;
+    if (shell > a.b.n) continue;
+    if (th > M_PI / 2) th = M_PI - th;
+    int sector = 1;
+    if (!(fabs(th) < kEps)) {
+      sector = 0;
+      while (sector <= a.b.ns && !(th <= a.b.bound[sector])) ++sector;
+    }
+    if (sector > a.b.ns) continue;
+    const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
+    double v = 0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const cx<double> p0 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 0])[idx]);
+      const cx<double> p1 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 1])[idx]);
+      const cx<double> p2 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 2])[idx]);
+      // N_i = i (k . P(i, .)); Re(N_i conj(R_i))
+      const cx<double> s = mkc<double>(k[0] * p0.x + k[1] * p1.x + k[2] * p2.x, k[0] * p0.y + k[1] * p1.y + k[2] * p2.y);
+      const cx<double> Ni = ione(s);
+      const cx<double> r = a.R[i][idx];
+      v += Ni.x * r.x + Ni.y * r.y;
+    }
+    atomicAdd(&sh[shell * cols + sector], 2.0 * mult_four(l1, l2, l3, g.N1, g.N2) * v);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nbins; i += TPB)
+    if (sh[i] != 0) atomicAdd(&a.out[i], sh[i]);
+}
+
+// EnergyTr.cc:190-210, scheme 0
+void ring_radii(const tg_ctx* c, int n, double* r) {
+  const double Rin = (double)radius_inside(c);
+  for (int i = 0; i <= n; ++i) r[i] = 0.0;
+  r[1] = 4.0;
+  r[2] = 8.0;
+  r[n - 2] = Rin / 2;
+  r[n - 1] = Rin;
+  r[n] = 10000.0;  // INF_RADIUS
+  if (n > 5) {
+    const double s = std::log2(Rin / 16.0) / (n - 4);
+    for (int i = 3; i <= n - 3; ++i) r[i] = 8 * std::pow(2.0, s * (i - 2));
+  }
+}
+
 }  // namespace
 
 extern "C" {
+
+int tg_ring_radii(tg_ctx* c, int n_ring_shells, double* radii, int n) {
+  if (!c || !radii || n_ring_shells < 5 || n_ring_shells > kMaxRingShells || n < n_ring_shells + 1) return TG_ERR_ARG;
+  ring_radii(c, n_ring_shells, radii);
+  return TG_OK;
+}
+
+int tg_ring_to_ring(tg_ctx* c, int kind, int axis, int n_ring_shells, int n_sectors, double* tr, int n) {
+  if (!c || !tr) return TG_ERR_ARG;
+  if (c->basis != TG_FOUR) return set_err(c, TG_ERR_UNSUPPORTED, "ring transfers: FOUR basis only");
+  if (axis < 1 || axis > 3 || n_sectors < 1 || n_sectors > TG_RING_MAX_SECTORS) return TG_ERR_ARG;
+  if (n_ring_shells < 5 || n_ring_shells > kMaxRingShells) return TG_ERR_ARG;
+  // (H, F, receiver, sign): U->U ring_to_ring_self, B->B W.ring_to_ring_self, U->B ring_to_ring_VF
+  int H, F, R;
+  double sign;
+  if (kind == TG_ET_UU) { H = 0; F = 0; R = 0; sign = -1.0; }
+  else if (kind == TG_ET_BB && c->phys == TG_MHD) { H = 0; F = 1; R = 1; sign = -1.0; }
+  else if (kind == TG_ET_UB && c->phys == TG_MHD) { H = 1; F = 0; R = 1; sign = 1.0; }
+  else return set_err(c, TG_ERR_ARG, "ring transfer kind not available for this physics");
+  const int rows = n_ring_shells + 1, cols = n_sectors + 1, per = rows * cols;
+  if ((size_t)n < (size_t)per * per) return set_err(c, TG_ERR_ARG, "ring transfer: output shorter than (n+1)^2 (ns+1)^2");
+  cudaSetDevice(c->dev);
+  int rc = ensure_et_buffers(c);
+  if (rc) return rc;
+  RingBins b{};
+  b.n = n_ring_shells;
+  ring_radii(c, n_ring_shells, b.r);
+  b.ns = n_sectors;
+  const double dtheta = (M_PI / 2) / n_sectors;
+  for (int i = 0; i < n_sectors; ++i) b.bound[i] = i * dtheta;
+  b.bound[n_sectors] = M_PI / 2;
+  b.axis = axis;
+  b.kin = (double)radius_inside(c);
+  const size_t need = (size_t)per * per;  // [giver shell][giver sector][shell][sector]
+  rc = ensure_diag(c, need);
+  if (rc) return rc;
+  cudaError_t e = cudaMemsetAsync(c->diag, 0, sizeof(double) * need, c->st);
+  if (e != cudaSuccess) return cuda_err(c, e, "ring transfer");
+  const Geo& g = c->g;
+  const void* Hf[3] = {c->U0[3 * H + 0], c->U0[3 * H + 1], c->U0[3 * H + 2]};
+  rc = pipe_inverse_xy(c, 3, Hf, nullptr, nullptr, F64, 3, c->WX, c->etWY);
+  if (rc) return rc;
+  ProdPairs pp{};
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      pp.a[3 * i + j] = (signed char)(3 + i);  // G_i
+      pp.b[3 * i + j] = (signed char)j;        // H_j
+    }
+  const size_t smem = sizeof(double) * per;
+  if (smem > 48 * 1024) {
+    e = cudaFuncSetAttribute(k_ring_contract<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_ring_contract<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_err(c, e, "ring transfer");
+  }
+  const int nblk = (int)std::min<long long>((g.S + TPB - 1) / TPB, 148LL * 8);
+  for (int i = 1; i < n_ring_shells; ++i)
+    for (int j = 1; j <= n_sectors; ++j) {
+      k_fill_ring<<<(int)((g.S + TPB - 1) / TPB), TPB, 0, c->st>>>(g, c->U0[3 * F + 0], c->U0[3 * F + 1],
+                                                                   c->U0[3 * F + 2], c->etG[0], c->etG[1], c->etG[2],
+                                                                   b.r[i - 1], b.r[i], b.bound[j - 1], b.bound[j], axis);
+      e = cudaGetLastError();
+      if (e != cudaSuccess) return cuda_err(c, e, "fill ring");
+      const void* G[3] = {c->etG[0], c->etG[1], c->etG[2]};
+      rc = pipe_inverse_xy(c, 3, G, nullptr, nullptr, F64, 3, c->WX, c->etWY + 3);
+      if (rc) return rc;
+      rc = pipe_products_forward(c, 6, c->etWY, 9, pp, c->etPP, c->etPY, c->etPX);
+      if (rc) return rc;
+      RingContractArgs a{};
+      a.g = g;
+      for (int q = 0; q < 9; ++q) a.PX[q] = c->etPX[q];
+      for (int q = 0; q < 3; ++q) a.R[q] = c->U0[3 * R + q];
+      a.b = b;
+      a.out = c->diag + ((size_t)i * cols + j) * per;
+      if (c->tprec == F64) k_ring_contract<double><<<nblk, TPB, smem, c->st>>>(a);
+      else k_ring_contract<float><<<nblk, TPB, smem, c->st>>>(a);
+      e = cudaGetLastError();
+      if (e != cudaSuccess) return cuda_err(c, e, "ring contract");
+    }
+  std::vector<double> h(need);
+  e = cudaMemcpyAsync(h.data(), c->diag, sizeof(double) * need, cudaMemcpyDeviceToHost, c->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+  if (e != cudaSuccess) return cuda_err(c, e, "ring transfer");
+  for (size_t q = 0; q < need; ++q) tr[q] = sign * h[q];
+  return TG_OK;
+}
+
 
 int tg_ring_sizes(tg_ctx* c, int axis, int* ring_shells, int* cylinder_shells) {
   if (!c || axis < 1 || axis > 3) return TG_ERR_ARG;

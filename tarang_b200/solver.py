@@ -349,6 +349,18 @@ class IncFluid:
         dissk), each [cylindrical shell][slab] along `axis`."""
         return self._ring(self.lib.tg_cylinder_ring_spectrum, True, n_slabs, axis, group)
 
+    def Compute_ring_tr(self, n_ring_shells, n_sectors, axis=1, kind=L.TG_ET_UU):
+        """IncVF::Compute_ring_tr (tg_ring_to_ring): T[i, j, m, s], the transfer from giver
+        ring (shell i, sector j) to receiver ring (m, s); kind TG_ET_UU, or for MHD TG_ET_BB,
+        TG_ET_UB.  Also returns the ring radii."""
+        r = np.zeros(n_ring_shells + 1)
+        self._ck(self.lib.tg_ring_radii(self.h, n_ring_shells, _dptr(r), r.size), "ring radii")
+        n1, n2 = n_ring_shells + 1, n_sectors + 1
+        T = np.zeros((n1, n2, n1, n2))
+        self._ck(self.lib.tg_ring_to_ring(self.h, kind, axis, n_ring_shells, n_sectors, _dptr(T), T.size),
+                 "ring transfer")
+        return T, r
+
     def Compute_force_feed_shell(self):
         """IncVF::Compute_force_feed_shell (compute_force_feed.cc:70-76): forceV_shell, S+1 entries."""
         S = self.cfg.n_shells

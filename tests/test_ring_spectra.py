@@ -85,3 +85,57 @@ def test_gpu_ring_spectra_mhd_magnetic_field(lib):
         f.CV_Compute_ring_spectrum(6, 3, 1)          # no magnetic field
     with pytest.raises(L.TarangError):
         f.CV_Compute_ring_spectrum(65, 1)             # more sectors than the maximum
+
+
+def test_ring_transfer_oracle_identities():
+    """Ring-to-ring transfer (oracle): with the z axis every mode has theta <= pi/2, so summed
+    over sectors a giver ring row is the shell-to-shell transfer of its shell; and the transfer
+    between two rings is antisymmetric (the helper is the whole solenoidal field; 64^3, where the
+    scheme-0 radii increase, so giver and receiver rings are the same sets)."""
+    N = (64, 64, 64)
+    V = ic.random_phase_field(N, seed=71)
+    n, ns = 6, 3
+    T = o.compute_ring_tr_generic(V, V, V, -1.0, KF, 3, n, ns)
+    R = o.ring_radii(N, KF, n)
+    for i in range(1, n):
+        G = [o.fill_array_shell(v, R[i - 1], R[i], KF) for v in V]
+        want = -o.shell_mult_all(o.et_nlin(V, G, KF), V, R, KF)
+        assert np.allclose(T[i].sum(axis=(0, 2)), want, rtol=1e-10, atol=1e-14 * np.abs(want).max())
+    scale = np.abs(T).max()
+    for i in range(1, n):
+        for j in range(1, ns + 1):
+            for m in range(1, n):
+                for s in range(1, ns + 1):
+                    assert abs(T[i, j, m, s] + T[m, s, i, j]) <= 1e-12 * scale
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("N,axis,n,ns", [((32, 32, 32), 3, 6, 3), ((64, 64, 64), 1, 7, 4), ((64, 32, 32), 2, 5, 2)])
+def test_gpu_ring_to_ring_matches_oracle(lib, N, axis, n, ns):
+    from tarang_b200.solver import IncFluid
+    V = ic.random_phase_field(N, seed=80 + axis)
+    s = IncFluid(N, nu=1e-3, dt=1e-3)
+    s.set_V(V)
+    T, r = s.Compute_ring_tr(n, ns, axis)
+    assert np.allclose(r, o.ring_radii(N, KF, n), rtol=0, atol=0)
+    want = o.compute_ring_tr_generic(V, V, V, -1.0, KF, axis, n, ns)
+    assert np.abs(T - want).max() <= 1e-12 * np.abs(want).max()
+
+
+@pytest.mark.gpu
+def test_gpu_ring_to_ring_mhd_kinds(lib):
+    from tarang_b200 import _lib as L
+    from tarang_b200.solver import IncFluid
+    N = (32, 32, 32)
+    U = ic.random_phase_field(N, seed=91)
+    B = ic.random_phase_field(N, k0=3.0, seed=92)
+    s = IncFluid(N, physics="MHD", nu=1e-3, eta=1e-3, dt=1e-3)
+    s.set_V(U)
+    s.set_W(B)
+    for kind, (H, F, Rf, sign) in ((L.TG_ET_UU, (U, U, U, -1.0)), (L.TG_ET_BB, (U, B, B, -1.0)),
+                                   (L.TG_ET_UB, (B, U, B, 1.0))):
+        T, _ = s.Compute_ring_tr(6, 2, 1, kind)
+        want = o.compute_ring_tr_generic(H, F, Rf, sign, KF, 1, 6, 2)
+        assert np.abs(T - want).max() <= 1e-12 * np.abs(want).max(), kind
+    with pytest.raises(L.TarangError):
+        s.Compute_ring_tr(6, 2, 1, L.TG_ET_BU)       # not a ring transfer of the reference
