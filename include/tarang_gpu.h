@@ -256,6 +256,12 @@ int tg_et_radii(tg_ctx* ctx, double* radii, int n);
 int tg_flux(tg_ctx* ctx, int kind, double* flux, int n);
 /* Compute_shell_tr (compute_shell_tr.cc:59-281): (n_shells+1) x (n_shells+1) row-major */
 int tg_shell_to_shell(tg_ctx* ctx, int kind, double* tr, int n);
+/* IncVF::Compute_kinetic_helicity_flux (EnergyTrdir/compute_helicity_flux.cc:47-75), FOUR: the
+ * helicity flux out of each sphere s = 1 .. n_shells of the energy-transfer radii,
+ * -P(U.grad U<, omega>)/2 - P(U.grad omega<, U>)/2 + P(omega.grad U<, U>)/2 with omega = i K x U,
+ * X< the field inside the sphere and P(N, R>) = sum over |K| > R_s of 2 mult Re(N . R*)
+ * (Prod_out_sphere_nlinV / Prod_out_sphere_nlin_vorticity prod_nlinV.cc:62-150).  n >= n_shells + 1. */
+int tg_helicity_flux(tg_ctx* ctx, double* flux, int n);
 /* Get_Nusselt_no (nusselt.cc:53-89), RB only */
 int tg_nusselt(tg_ctx* ctx, double* nusselt);
 /* IncVF::Compute_force_feed_shell (lib/IncFlow/EnergyTrdir/compute_force_feed.cc:70-76, with

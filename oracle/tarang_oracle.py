@@ -1143,6 +1143,40 @@ def compute_shell_tr_generic(H, F, Rf, sign, kfactor, no_shells, alias="DEALIAS"
     return T
 
 
+def vorticity_four(V, kfactor):
+    """Compute_Modal_vorticity_FOUR  four_basic.cc:166-186 on every mode: omega = i K x V."""
+    N = (V[0].shape[0], V[0].shape[1], 2 * (V[0].shape[2] - 1))
+    kx, ky, kz = kvec(N, kfactor)
+    return [1j * (ky * V[2] - kz * V[1]), 1j * (kz * V[0] - kx * V[2]), 1j * (kx * V[1] - ky * V[0])]
+
+
+def kinetic_helicity_flux(V, kfactor, no_shells, alias="DEALIAS"):
+    """IncVF::Compute_kinetic_helicity_flux  compute_helicity_flux.cc:47-75 (FOUR): for sphere s
+    (radius R_s of the energy-transfer radii), with X< = X on 0 < |K| <= R_s and
+    P(N, R) = sum_{|K| > R_s} 2 mult Re(N . R*) (Shell_mult_single / Shell_mult_vorticity
+    four_ET.cc:811-890): flux(s) = -P(N(U, U<), omega)/2 - P(N(U, omega<), U)/2
+    + P(N(omega, U<), U)/2, N(H, G) = D_j F(H_j G_i)."""
+    N = (V[0].shape[0], V[0].shape[1], 2 * (V[0].shape[2] - 1))
+    R = et_radii(N, kfactor, no_shells, alias)
+    K = kmag(N, kfactor)
+    mult = multiplicity_four(N)
+    W = vorticity_four(V, kfactor)
+    out = np.zeros(no_shells + 1)
+
+    def P(nl, Rf, r):
+        sel = K > r
+        return float(np.sum((2 * mult * sum(np.real(a * np.conj(b)) for a, b in zip(nl, Rf)))[sel]))
+
+    for s_ in range(1, no_shells + 1):
+        r = R[s_]
+        inside = (K > 0) & (K <= r)
+        U_in = [np.where(inside, v, 0) for v in V]
+        W_in = [np.where(inside, w, 0) for w in W]
+        out[s_] = (-P(et_nlin(V, U_in, kfactor), W, r) / 2 - P(et_nlin(V, W_in, kfactor), V, r) / 2
+                   + P(et_nlin(W, U_in, kfactor), V, r) / 2)
+    return out
+
+
 def ring_radii(N, kfactor, n_ring_shells, alias="DEALIAS", basis="FOUR"):
     """EnergyTr::EnergyTr ring shell radii, scheme 0  EnergyTr.cc:190-210."""
     Rin = float(max_radius_inside(N, kfactor, alias, basis))

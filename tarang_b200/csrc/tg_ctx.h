@@ -84,6 +84,7 @@ struct tg_ctx {
   // energy-transfer buffers (pipeline buffers reused where the physics already has them)
   bool et_ready = false;
   tg::cx<double>* etG[3] = {};
+  tg::cx<double>* etVort[3] = {};  // vorticity of the velocity (helicity flux), owned via et_own
   void* etWY[6] = {};
   void* etPP[9] = {};
   void* etPY[9] = {};

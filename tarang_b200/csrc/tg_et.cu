@@ -215,8 +215,24 @@ std::vector<double> et_annuli(const tg_ctx* c) {
 
 // T[r][g][a]: giver annulus g = 1..A (field F inside (rho[g-1], rho[g]]), receiver annulus
 // a = 0..A, receivers r of the given (H, F) pair
+int et_tables_ptr(tg_ctx* c, const cx<double>* const* Hp, const cx<double>* const* Fp,
+                  const cx<double>* const (*Rp)[3], int nrec, const std::vector<double>& rho,
+                  std::vector<double>& T);
+
 int et_tables(tg_ctx* c, int Hg, int Fg, const int* Rg, int nrec, const std::vector<double>& rho,
               std::vector<double>& T) {
+  const cx<double>* Hp[3] = {c->U0[3 * Hg], c->U0[3 * Hg + 1], c->U0[3 * Hg + 2]};
+  const cx<double>* Fp[3] = {c->U0[3 * Fg], c->U0[3 * Fg + 1], c->U0[3 * Fg + 2]};
+  const cx<double>* Rp[2][3];
+  for (int r = 0; r < nrec && r < 2; ++r)
+    for (int i = 0; i < 3; ++i) Rp[r][i] = c->U0[3 * Rg[r] + i];
+  return et_tables_ptr(c, Hp, Fp, Rp, nrec, rho, T);
+}
+
+// T[r][g][a] for helper fields Hp, giver fields Fp and receivers Rp (any compact FP64 fields)
+int et_tables_ptr(tg_ctx* c, const cx<double>* const* Hp, const cx<double>* const* Fp,
+                  const cx<double>* const (*Rp)[3], int nrec, const std::vector<double>& rho,
+                  std::vector<double>& T) {
   const int A = (int)rho.size() - 1;
   if (A < 1 || A > kMaxShells) return set_err(c, TG_ERR_ARG, "energy transfer needs 6 <= n_shells <= 63");
   int rc = ensure_et_buffers(c);
@@ -232,7 +248,7 @@ int et_tables(tg_ctx* c, int Hg, int Fg, const int* Rg, int nrec, const std::vec
   cudaError_t e = cudaMemsetAsync(c->diag, 0, sizeof(double) * need, c->st);
   if (e != cudaSuccess) return cuda_err(c, e, "memset");
   // helper H: inverse x, y once (into etWY[0..2])
-  const void* H[3] = {c->U0[3 * Hg + 0], c->U0[3 * Hg + 1], c->U0[3 * Hg + 2]};
+  const void* H[3] = {Hp[0], Hp[1], Hp[2]};
   rc = pipe_inverse_xy(c, 3, H, nullptr, nullptr, F64, 3, c->WX, c->etWY);
   if (rc) return rc;
   ProdPairs pp{};
@@ -244,7 +260,7 @@ int et_tables(tg_ctx* c, int Hg, int Fg, const int* Rg, int nrec, const std::vec
   const int nblk = (int)std::min<long long>((g.S + TPB - 1) / TPB, 148LL * 8);
   for (int n = 1; n <= A; ++n) {
     k_fill_shell<<<(int)((g.S + TPB - 1) / TPB), TPB, 0, c->st>>>(
-        g, c->U0[3 * Fg + 0], c->U0[3 * Fg + 1], c->U0[3 * Fg + 2], c->etG[0], c->etG[1], c->etG[2], rho[n - 1], rho[n]);
+        g, Fp[0], Fp[1], Fp[2], c->etG[0], c->etG[1], c->etG[2], rho[n - 1], rho[n]);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_err(c, e, "fill shell");
     const void* G[3] = {c->etG[0], c->etG[1], c->etG[2]};
@@ -256,7 +272,7 @@ int et_tables(tg_ctx* c, int Hg, int Fg, const int* Rg, int nrec, const std::vec
     a.g = g;
     for (int q = 0; q < 9; ++q) a.PX[q] = c->etPX[q];
     for (int r = 0; r < nrec; ++r)
-      for (int i = 0; i < 3; ++i) a.R[r][i] = c->U0[3 * Rg[r] + i];
+      for (int i = 0; i < 3; ++i) a.R[r][i] = Rp[r][i];
     a.nrec = nrec;
     a.rad = rad;
     a.hist = c->diag + (size_t)n * nrec * nb;  // layout [g][r][a]
@@ -289,6 +305,20 @@ int et_table_kind(tg_ctx* c, int kind, std::vector<double>& T, std::vector<doubl
   return et_tables(c, k.H, k.F, Rg, 1, rho, T);
 }
 
+
+// omega = i K x V (Compute_Modal_vorticity_FOUR four_basic.cc:166-186), compact layout
+__global__ void k_vorticity(Geo g, const cx<double>* V0, const cx<double>* V1, const cx<double>* V2, cx<double>* W0,
+                            cx<double>* W1, cx<double>* W2) {
+  const long long idx = (long long)blockIdx.x * TPB + threadIdx.x;
+  if (idx >= g.S) return;
+  int r1, r2, l3;
+  compact_mode(g, idx, r1, r2, l3);
+  const double kx = geo_kx(g, r1) * g.kf0, ky = geo_ky(g, r2) * g.kf1, kz = l3 * g.kf2;
+  const cx<double> a = V0[idx], b = V1[idx], d = V2[idx];
+  W0[idx] = ione(ky * d - kz * b);
+  W1[idx] = ione(kz * a - kx * d);
+  W2[idx] = ione(kx * b - ky * a);
+}
 
 // Force feed per shell (Compute_force_feed_shell compute_force_feed.cc:70-76 with
 // Shell_mult_all_FOUR four_ET.cc:181-226): for |K| <= R_in, result[i] += 2 mult Re(F . V*),
@@ -362,6 +392,59 @@ int tg_flux(tg_ctx* c, int kind, double* flux, int n) {
         if (rho[a - 1] >= R[s]) acc += T[(size_t)g * nb + a];
     }
     flux[s] = sign * acc;
+  }
+  return TG_OK;
+}
+
+// Kinetic helicity flux (IncVF::Compute_kinetic_helicity_flux compute_helicity_flux.cc:47-75):
+// flux(s) = -P(U.grad U<, omega>)/2 - P(U.grad omega<, U>)/2 + P(omega.grad U<, U>)/2, with
+// P(N, R>) = sum over |K| > R_s of 2 mult Re(N . R*) (Prod_out_sphere_nlinV,
+// Prod_out_sphere_nlin_vorticity prod_nlinV.cc:62-150) and X< = X on 0 < |K| <= R_s
+// (Fill_in_sphere, Fill_in_sphere_vorticity fill_sphere_shell.cc:57-210).
+int tg_helicity_flux(tg_ctx* c, double* flux, int n) {
+  if (!c || !flux) return TG_ERR_ARG;
+  const int S = c->cfg.n_shells;
+  if (S < 6 || n < S + 1) return TG_ERR_ARG;
+  if (c->basis != TG_FOUR) return set_err(c, TG_ERR_UNSUPPORTED, "helicity flux is built for the FOUR basis");
+  cudaSetDevice(c->dev);
+  int rc = ensure_et_buffers(c);
+  if (rc) return rc;
+  const Geo& g = c->g;
+  if (!c->etVort[0]) {
+    for (int i = 0; i < 3; ++i) {
+      rc = dalloc_ctx(c, (void**)&c->etVort[i], sizeof(cx<double>) * (size_t)g.S);
+      if (rc) return rc;
+      c->et_own[c->n_et_own++] = c->etVort[i];
+    }
+  }
+  k_vorticity<<<(int)((g.S + TPB - 1) / TPB), TPB, 0, c->st>>>(g, c->U0[0], c->U0[1], c->U0[2], c->etVort[0],
+                                                               c->etVort[1], c->etVort[2]);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_err(c, e, "vorticity");
+  const cx<double>* U[3] = {c->U0[0], c->U0[1], c->U0[2]};
+  const cx<double>* W[3] = {c->etVort[0], c->etVort[1], c->etVort[2]};
+  const cx<double>* RW[1][3] = {{W[0], W[1], W[2]}};
+  const cx<double>* RU[1][3] = {{U[0], U[1], U[2]}};
+  const std::vector<double> rho = et_annuli(c);
+  std::vector<double> T1, T2, T3;
+  rc = et_tables_ptr(c, U, U, RW, 1, rho, T1);       // U.grad U<  against omega
+  if (!rc) rc = et_tables_ptr(c, U, W, RU, 1, rho, T2);  // U.grad omega< against U
+  if (!rc) rc = et_tables_ptr(c, W, U, RU, 1, rho, T3);  // omega.grad U< against U
+  if (rc) return rc;
+  const std::vector<double> R = et_radii(c);
+  const int A = (int)rho.size() - 1, nb = A + 1;
+  for (int s = 0; s < n; ++s) flux[s] = 0;
+  for (int s = 1; s <= S; ++s) {
+    double acc = 0;
+    for (int gg = 1; gg <= A; ++gg) {
+      if (rho[gg] > R[s]) continue;
+      for (int a = 1; a <= A; ++a)
+        if (rho[a - 1] >= R[s]) {
+          const size_t q = (size_t)gg * nb + a;
+          acc += -0.5 * T1[q] - 0.5 * T2[q] + 0.5 * T3[q];
+        }
+    }
+    flux[s] = acc;
   }
   return TG_OK;
 }

@@ -349,6 +349,13 @@ class IncFluid:
         dissk), each [cylindrical shell][slab] along `axis`."""
         return self._ring(self.lib.tg_cylinder_ring_spectrum, True, n_slabs, axis, group)
 
+    def Compute_kinetic_helicity_flux(self):
+        """IncVF::Compute_kinetic_helicity_flux (tg_helicity_flux): flux_hk, n_shells + 1 entries."""
+        S = self.cfg.n_shells
+        out = np.zeros(S + 1)
+        self._ck(self.lib.tg_helicity_flux(self.h, _dptr(out), out.size), "helicity flux")
+        return out
+
     def Compute_ring_tr(self, n_ring_shells, n_sectors, axis=1, kind=L.TG_ET_UU):
         """IncVF::Compute_ring_tr (tg_ring_to_ring): T[i, j, m, s], the transfer from giver
         ring (shell i, sector j) to receiver ring (m, s); kind TG_ET_UU, or for MHD TG_ET_BB,
