@@ -96,7 +96,9 @@ extern "C" {
 #define TG_ET_BB 1 /* B< -> B> */
 #define TG_ET_UB 2 /* U< -> B> */
 #define TG_ET_BU 3 /* B< -> U> */
-#define TG_ET_TT 4 /* T< -> T> (scalar) */
+#define TG_ET_TT 4 /* T< -> T> (passive scalar, FOUR) */
+#define TG_ET_ZP 5 /* Z+< -> Z+> with Z- as helper (MHD Elsasser, flux_Elsasser) */
+#define TG_ET_ZM 6 /* Z-< -> Z-> with Z+ as helper (MHD Elsasser, W.flux_Elsasser) */
 
 typedef struct tg_config {
   int N[3];           /* N1, N2, N3 (N3 even) */
@@ -252,7 +254,8 @@ int tg_ring_radii(tg_ctx* ctx, int n_ring_shells, double* radii, int n);
 int tg_ring_to_ring(tg_ctx* ctx, int kind, int axis, int n_ring_shells, int n_sectors, double* tr, int n);
 /* shell radii of the energy transfer (EnergyTr.cc:136-160): n_shells + 1 doubles */
 int tg_et_radii(tg_ctx* ctx, double* radii, int n);
-/* Compute_flux (compute_flux.cc:52-304): flux[s], s = 0..n_shells (index 0 unused) */
+/* Compute_flux (compute_flux.cc:52-304): flux[s], s = 0..n_shells (index 0 unused); kind
+ * TG_ET_UU/BB/UB/BU, TG_ET_ZP/ZM (Elsasser, :228-255) or TG_ET_TT (Compute_flux_scalar :82-95) */
 int tg_flux(tg_ctx* ctx, int kind, double* flux, int n);
 /* Compute_shell_tr (compute_shell_tr.cc:59-281): (n_shells+1) x (n_shells+1) row-major */
 int tg_shell_to_shell(tg_ctx* ctx, int kind, double* tr, int n);

@@ -43,7 +43,7 @@ TG_WORK0 = 24
 TG_NWORK = 8
 TG_NFIELDS = 32
 
-TG_ET_UU, TG_ET_BB, TG_ET_UB, TG_ET_BU, TG_ET_TT = 0, 1, 2, 3, 4
+TG_ET_UU, TG_ET_BB, TG_ET_UB, TG_ET_BU, TG_ET_TT, TG_ET_ZP, TG_ET_ZM = 0, 1, 2, 3, 4, 5, 6
 
 TG_REQ_QUEUED, TG_REQ_RUNNING, TG_REQ_DONE, TG_REQ_FAILED = 0, 1, 2, 3
 

@@ -85,6 +85,8 @@ struct tg_ctx {
   bool et_ready = false;
   tg::cx<double>* etG[3] = {};
   tg::cx<double>* etVort[3] = {};  // vorticity of the velocity (helicity flux), owned via et_own
+  tg::cx<double>* etZ[6] = {};     // Elsasser fields Z+ = U + B, Z- = U - B (MHD), via et_own
+  tg::cx<double>* etZero = nullptr;  // a compact field of zeros (scalar transfers), via et_own
   void* etWY[6] = {};
   void* etPP[9] = {};
   void* etPY[9] = {};

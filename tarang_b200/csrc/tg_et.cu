@@ -295,8 +295,72 @@ int et_tables_ptr(tg_ctx* c, const cx<double>* const* Hp, const cx<double>* cons
   return TG_OK;
 }
 
+struct PtrPair6 {
+  const cx<double>* in[6];
+  cx<double>* out[6];
+};
+
+// Z+ = U + B, Z- = U - B (UB_to_Elsasser_field elsasser.cc:53-90)
+__global__ void k_elsasser(Geo g, PtrPair6 p) {
+  const long long idx = (long long)blockIdx.x * TPB + threadIdx.x;
+  if (idx >= g.S) return;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const cx<double> u = p.in[i][idx], b = p.in[3 + i][idx];
+    p.out[i][idx] = u + b;
+    p.out[3 + i][idx] = u - b;
+  }
+}
+
+int own_field(tg_ctx* c, cx<double>** f) {
+  if (*f) return TG_OK;
+  if (c->n_et_own >= 32) return set_err(c, TG_ERR_STATE, "energy transfer: too many scratch fields");
+  int rc = dalloc_ctx(c, (void**)f, sizeof(cx<double>) * (size_t)c->g.S);
+  if (rc) return rc;
+  c->et_own[c->n_et_own++] = *f;
+  return TG_OK;
+}
+
 int et_table_kind(tg_ctx* c, int kind, std::vector<double>& T, std::vector<double>& rho, double& sign) {
   if (c->basis != TG_FOUR) return set_err(c, TG_ERR_UNSUPPORTED, "energy transfer is built for the FOUR basis");
+  if (kind == TG_ET_TT) {
+    // Compute_flux_scalar / Compute_shell_tr_scalar (compute_flux.cc:82-95,
+    // compute_shell_tr.cc:93-109): G = T<, N = D_j F(U_j T<) against T, sign -1; run as the
+    // vector form with the giver and receiver (T, 0, 0)
+    if (c->phys != TG_SCALAR && c->phys != TG_RB) return set_err(c, TG_ERR_ARG, "scalar transfer needs a scalar");
+    int rc = ensure_et_buffers(c);
+    if (!rc) rc = own_field(c, &c->etZero);
+    if (rc) return rc;
+    sign = -1.0;
+    rho = et_annuli(c);
+    const cx<double>* H[3] = {c->U0[0], c->U0[1], c->U0[2]};
+    const cx<double>* F[3] = {c->U0[3], c->etZero, c->etZero};
+    const cx<double>* R[1][3] = {{c->U0[3], c->etZero, c->etZero}};
+    return et_tables_ptr(c, H, F, R, 1, rho, T);
+  }
+  if (kind == TG_ET_ZP || kind == TG_ET_ZM) {
+    // flux_Elsasser / shelltoshell_Elsasser (compute_flux.cc:228-255, compute_shell_tr.cc:201-246):
+    // Z+: G = Z+<, N = D_j F(Z-_j G_i) against Z+; Z-: with + and - exchanged; sign -1
+    if (c->phys != TG_MHD) return set_err(c, TG_ERR_ARG, "Elsasser transfers need MHD");
+    int rc = ensure_et_buffers(c);
+    for (int i = 0; i < 6 && !rc; ++i) rc = own_field(c, &c->etZ[i]);
+    if (rc) return rc;
+    PtrPair6 p{};
+    for (int i = 0; i < 6; ++i) {
+      p.in[i] = c->U0[i];
+      p.out[i] = c->etZ[i];
+    }
+    k_elsasser<<<(int)((c->g.S + TPB - 1) / TPB), TPB, 0, c->st>>>(c->g, p);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_err(c, e, "elsasser");
+    sign = -1.0;
+    rho = et_annuli(c);
+    const int a = (kind == TG_ET_ZP) ? 0 : 3, b = 3 - a;
+    const cx<double>* H[3] = {c->etZ[b], c->etZ[b + 1], c->etZ[b + 2]};
+    const cx<double>* F[3] = {c->etZ[a], c->etZ[a + 1], c->etZ[a + 2]};
+    const cx<double>* R[1][3] = {{F[0], F[1], F[2]}};
+    return et_tables_ptr(c, H, F, R, 1, rho, T);
+  }
   KindSpec k{};
   if (!kind_spec(c, kind, k)) return set_err(c, TG_ERR_ARG, "energy-transfer kind not available for this physics");
   sign = k.sign;
