@@ -140,9 +140,16 @@ int tg_device_bytes(const tg_ctx* ctx, size_t* bytes);
 
 /* Field I/O in the reference layout (Read_data_MPI / Write_data_MPI array_basic.cc:294-858
  * without the MPI gather).  With dealias on, uploads of solver fields keep the 2/3 support
- * only (the reference dealiases every initial condition, init_cond_*.cc). */
+ * only (the reference dealiases every initial condition, init_cond_*.cc): for the state fields
+ * (V, W, T) only those modes cross the bus, as up to four strided copies into the solver's
+ * compact rows.  tg_field_download writes every entry (zeros outside the support). */
 int tg_field_upload(tg_ctx* ctx, int field, const double* host, size_t n_doubles);
 int tg_field_download(tg_ctx* ctx, int field, double* host, size_t n_doubles);
+/* A state field's stored (dealiased) modes only, into the caller's dense reference-layout
+ * array; its other entries are left as they are.  For a driver that keeps the fields in host
+ * memory between steps, where those entries are zero already (as in the reference after
+ * Dealias): the transfer is the stored 30 % of the array (no counterpart in the reference). */
+int tg_field_download_stored(tg_ctx* ctx, int field, double* host, size_t n_doubles);
 int tg_field_copy(tg_ctx* ctx, int dst_field, int src_field);
 /* A work field of its own for the caller (the reference's temporary arrays, e.g. the
  * VF_temp / VF_temp_r fields IncVF.h:75-531 allocates): reserves a free slot among

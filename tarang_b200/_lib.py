@@ -147,6 +147,7 @@ SIGNATURES = {
     "tg_device_bytes": (C.c_int, [_VP, C.POINTER(C.c_size_t)]),
     "tg_field_upload": (C.c_int, [_VP, C.c_int, _DP, C.c_size_t]),
     "tg_field_download": (C.c_int, [_VP, C.c_int, _DP, C.c_size_t]),
+    "tg_field_download_stored": (C.c_int, [_VP, C.c_int, _DP, C.c_size_t]),
     "tg_field_copy": (C.c_int, [_VP, C.c_int, C.c_int]),
     "tg_field_alloc": (C.c_int, [_VP, C.POINTER(C.c_int)]),
     "tg_write_field_file": (C.c_int, [C.c_char_p, C.c_double, C.POINTER(C.c_int), C.c_int, C.POINTER(_DP), C.c_int, C.c_int]),

@@ -884,6 +884,64 @@ int tg_device_bytes(const tg_ctx* c, size_t* bytes) {
   return TG_OK;
 }
 
+namespace {
+
+// The stored modes of a dense reference-layout field [l1][l2][0..N3/2] are up to four boxes
+// (kept x rows [0, lo) and [N1 - hi, N1), the same for y, kz < nkz); each box is one 3-D
+// pitched copy between the dense array and the compact rows [r1][r2][0..kzp).
+cudaError_t copy_stored(tg_ctx* c, cx<double>* compact, double* dense, bool to_device) {
+  const Geo& g = c->g;
+  const size_t e = sizeof(cx<double>);
+  const int xs[2][2] = {{0, g.ax.lo}, {g.ax.L - g.ax.hi, g.ax.hi}};
+  const int ys[2][2] = {{0, g.ay.lo}, {g.ay.L - g.ay.hi, g.ay.hi}};
+  int r1 = 0;
+  for (int bx = 0; bx < 2; ++bx) {
+    const int x0 = xs[bx][0], nx = xs[bx][1];
+    if (nx <= 0) continue;
+    int r2 = 0;
+    for (int by = 0; by < 2; ++by) {
+      const int y0 = ys[by][0], ny = ys[by][1];
+      if (ny <= 0) continue;
+      cudaMemcpy3DParms p = {};
+      cudaPitchedPtr hp = make_cudaPitchedPtr(dense, (size_t)c->M3 * e, (size_t)c->M3 * e, (size_t)c->N2);
+      cudaPitchedPtr dp = make_cudaPitchedPtr(compact, (size_t)g.kzp * e, (size_t)g.kzp * e, (size_t)g.nky);
+      const cudaPos hpos = make_cudaPos(0, (size_t)y0, (size_t)x0), dpos = make_cudaPos(0, (size_t)r2, (size_t)r1);
+      if (to_device) {
+        p.srcPtr = hp;
+        p.srcPos = hpos;
+        p.dstPtr = dp;
+        p.dstPos = dpos;
+        p.kind = cudaMemcpyHostToDevice;
+      } else {
+        p.srcPtr = dp;
+        p.srcPos = dpos;
+        p.dstPtr = hp;
+        p.dstPos = hpos;
+        p.kind = cudaMemcpyDeviceToHost;
+      }
+      p.extent = make_cudaExtent((size_t)g.nkz * e, (size_t)ny, (size_t)nx);
+      cudaError_t err = cudaMemcpy3DAsync(&p, c->st);
+      if (err != cudaSuccess) return err;
+      r2 += ny;
+    }
+    r1 += nx;
+  }
+  return cudaSuccess;
+}
+
+}  // namespace
+
+int tg_field_download_stored(tg_ctx* c, int field, double* host, size_t n) {
+  if (!c || !host || field < 0 || field >= TG_NFIELDS) return TG_ERR_ARG;
+  if (n != 2 * (size_t)c->D) return set_err(c, TG_ERR_ARG, "download: n_doubles must be 2*N1*N2*(N3/2+1)");
+  const int si = field_state_index(c, field);
+  if (si < 0) return set_err(c, TG_ERR_ARG, "download_stored: state fields only");
+  cudaSetDevice(c->dev);
+  TG_CK(copy_stored(c, c->U0[si], host, false));
+  TG_CK(cudaStreamSynchronize(c->st));
+  return TG_OK;
+}
+
 int tg_field_upload(tg_ctx* c, int field, const double* host, size_t n) {
   if (!c || !host || field < 0 || field >= TG_NFIELDS) return TG_ERR_ARG;
   if (n != 2 * (size_t)c->D) return set_err(c, TG_ERR_ARG, "upload: n_doubles must be 2*N1*N2*(N3/2+1)");
@@ -897,9 +955,16 @@ int tg_field_upload(tg_ctx* c, int field, const double* host, size_t n) {
     TG_CK(cudaStreamSynchronize(c->st));
     return TG_OK;
   }
+  if (si >= 0) {
+    // state fields: only the stored modes cross the bus, straight into the compact rows
+    TG_CK(copy_stored(c, c->U0[si], const_cast<double*>(host), true));
+    TG_CK(cudaStreamSynchronize(c->st));
+    c->energy_valid = false;
+    c->have_nlin = c->have_pressure = c->have_force = false;
+    return TG_OK;
+  }
   cx<double>* target = nullptr;
-  if (si >= 0) target = c->U0[si];
-  else if (ni >= 0) target = c->NL[ni];
+  if (ni >= 0) target = c->NL[ni];
   else if (field == TG_PRESSURE) target = c->PR;
   else return set_err(c, TG_ERR_ARG, "upload: field not stored by this context");
   int rc = ensure_staging(c);

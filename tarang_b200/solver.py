@@ -168,6 +168,15 @@ class IncFluid:
         self._ck(self.lib.tg_field_download(self.h, field, _dptr(out.view(np.float64)), self.ndoubles), "download")
         return out
 
+    def download_stored(self, field: int, out: np.ndarray):
+        """The stored (dealiased) modes of a state field into `out` (complex128, reference
+        layout), leaving its other entries as they are (tg_field_download_stored)."""
+        if out.shape != self.shape or out.dtype != np.complex128 or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous complex128 array of the field's shape")
+        self._ck(self.lib.tg_field_download_stored(self.h, field, _dptr(out.view(np.float64)), self.ndoubles),
+                 "download_stored")
+        return out
+
     def alloc_field(self) -> int:
         """A reserved work field id (tg_field_alloc); release it with free_field."""
         f = C.c_int()
