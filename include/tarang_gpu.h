@@ -259,6 +259,16 @@ int tg_cylinder_ring_spectrum(tg_ctx* ctx, int group, int axis, int n_slabs, dou
  * giver ring holds only the modes with theta <= pi/2 (K_par >= 0), while receivers fold theta. */
 int tg_ring_radii(tg_ctx* ctx, int n_ring_shells, double* radii, int n);
 int tg_ring_to_ring(tg_ctx* ctx, int kind, int axis, int n_ring_shells, int n_sectors, double* tr, int n);
+/* Cylinder-ring-to-ring transfer (IncVF::Compute_cylinder_ring_tr, EnergyTrdir/
+ * compute_cylin_ring_tr.cc:53-80; Fill_array_cylinder_ring universal_ET.cc:100-125,
+ * Local_cyl_ring_mult_all_FOUR four/four_ET.cc:422-530): as tg_ring_to_ring with cylindrical
+ * shells of K_perp (scheme 0 radii up to Anis_max_Krho_radius_inside, EnergyTr.cc:300-320;
+ * tg_cylinder_radii) and slabs of K_par of equal width up to Anis_max_Kpll in place of sectors.
+ * A giver holds the modes with K_par >= 0 (the reference compares the signed K_par); receivers
+ * take |K_par|.  The reference sets the middle radii only when no_ring_shells > 5; here
+ * whenever n_cylinder_shells > 5. */
+int tg_cylinder_radii(tg_ctx* ctx, int axis, int n_cylinder_shells, double* radii, int n);
+int tg_cylinder_ring_to_ring(tg_ctx* ctx, int kind, int axis, int n_cylinder_shells, int n_slabs, double* tr, int n);
 /* shell radii of the energy transfer (EnergyTr.cc:136-160): n_shells + 1 doubles */
 int tg_et_radii(tg_ctx* ctx, double* radii, int n);
 /* Compute_flux (compute_flux.cc:52-304): flux[s], s = 0..n_shells (index 0 unused); kind

@@ -1177,9 +1177,18 @@ def kinetic_helicity_flux(V, kfactor, no_shells, alias="DEALIAS"):
     return out
 
 
-def ring_radii(N, kfactor, n_ring_shells, alias="DEALIAS", basis="FOUR"):
-    """EnergyTr::EnergyTr ring shell radii, scheme 0  EnergyTr.cc:190-210."""
-    Rin = float(max_radius_inside(N, kfactor, alias, basis))
+def krho_inside(N, kfactor, axis, alias="DEALIAS"):
+    """Anis_max_Krho_radius_inside_FOUR  four_inline.h:517-546."""
+    d = 3 if alias == "DEALIAS" else 2
+    p1, p2 = axis % 3, (axis + 1) % 3
+    return int(min((N[p1] // d) * kfactor[p1], (N[p2] // d) * kfactor[p2]))
+
+
+def ring_radii(N, kfactor, n_ring_shells, alias="DEALIAS", basis="FOUR", Rin=None):
+    """EnergyTr::EnergyTr ring shell radii, scheme 0  EnergyTr.cc:190-210 (cylinder shells
+    :300-320 with Rin = Anis_max_Krho_radius_inside)."""
+    if Rin is None:
+        Rin = float(max_radius_inside(N, kfactor, alias, basis))
     n = n_ring_shells
     r = [0.0] * (n + 1)
     r[1], r[2] = 4.0, 8.0
@@ -1204,6 +1213,45 @@ def _theta_grid(N, kfactor, axis):
                      np.where(np.abs(kpll) > MYEPS, np.arctan(kperp / kpll), math.pi / 2),
                      np.where(kpll >= 0, 0.0, math.pi))
     return np.where(t >= 0, t, t + math.pi)
+
+
+def compute_cylinder_ring_tr_generic(H, F, Rf, sign, kfactor, axis, n_shells, n_slabs, alias="DEALIAS"):
+    """IncVF::Compute_cylinder_ring_tr  compute_cylin_ring_tr.cc:53-80: giver (i, j) = F on
+    r[i-1] < K_perp <= r[i], h_{j-1} < K_par <= h_j (signed; K_par = 0 in slab 1;
+    Fill_array_cylinder_ring universal_ET.cc:100-125); T[i, j, m, s] = sign * sum over receiver
+    (m, s) with K_perp <= Krho_max of 2 mult Re(N . Rf*) (Local_cyl_ring_mult_all_FOUR
+    four_ET.cc:492-530, Compute_cylinder_ring_index basis_basicfn.cc:412-445)."""
+    N = (H[0].shape[0], H[0].shape[1], 2 * (H[0].shape[2] - 1))
+    d = 3 if alias == "DEALIAS" else 2
+    kr = krho_inside(N, kfactor, axis, alias)
+    R = ring_radii(N, kfactor, n_shells, alias, Rin=float(kr))
+    ax = axis - 1
+    kmax = (N[ax] // d) * kfactor[ax]
+    dk = kmax / n_slabs
+    hb = [0.0] + [i * dk for i in range(1, n_slabs)] + [kmax]
+    Kv = [np.broadcast_to(k, (N[0], N[1], N[2] // 2 + 1)) for k in kvec(N, kfactor)]
+    kpll = Kv[ax]
+    kperp = np.sqrt(Kv[(ax + 1) % 3] ** 2 + Kv[(ax + 2) % 3] ** 2)
+    mult = multiplicity_four(N)
+    shell = shell_index(kperp, R)
+    akp = np.abs(kpll)
+    slab = np.full(kperp.shape, len(hb), dtype=np.int64)
+    for i in range(len(hb) - 1, 0, -1):
+        slab = np.where(akp <= hb[i], i, slab)
+    slab = np.where(akp < MYEPS, 1, slab)
+    n1, n2 = n_shells + 1, n_slabs + 1
+    ok = (kperp <= kr) & (shell <= n_shells) & (slab <= n_slabs)
+    flat = (shell * n2 + slab)[ok]
+    T = np.zeros((n1, n2, n1, n2))
+    for i in range(1, n_shells):
+        for j in range(1, n_slabs + 1):
+            lo, hi, hl, hh = R[i - 1], R[i], hb[j - 1], hb[j]
+            inr = (kperp > lo) & (kperp <= hi) & (((kpll > hl) & (kpll <= hh)) | ((np.abs(kpll) < MYEPS) & (hl < MYEPS)))
+            G = [np.where(inr, f, 0) for f in F]
+            nl = et_nlin(H, G, kfactor)
+            val = 2 * mult * sum(np.real(a * np.conj(b)) for a, b in zip(nl, Rf))
+            T[i, j] = sign * np.bincount(flat, weights=val[ok], minlength=n1 * n2).reshape(n1, n2)
+    return T
 
 
 def compute_ring_tr_generic(H, F, Rf, sign, kfactor, axis, n_ring_shells, n_sectors, alias="DEALIAS"):

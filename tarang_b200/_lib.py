@@ -176,6 +176,8 @@ SIGNATURES = {
     "tg_ring_radii": (C.c_int, [_VP, C.c_int, _DP, C.c_int]),
     "tg_helicity_flux": (C.c_int, [_VP, _DP, C.c_int]),
     "tg_ring_to_ring": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, C.c_int, _DP, C.c_int]),
+    "tg_cylinder_radii": (C.c_int, [_VP, C.c_int, C.c_int, _DP, C.c_int]),
+    "tg_cylinder_ring_to_ring": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, C.c_int, _DP, C.c_int]),
     "tg_flux": (C.c_int, [_VP, C.c_int, _DP, C.c_int]),
     "tg_shell_to_shell": (C.c_int, [_VP, C.c_int, _DP, C.c_int]),
     "tg_nusselt": (C.c_int, [_VP, _DP]),

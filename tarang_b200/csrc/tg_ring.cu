@@ -209,29 +209,38 @@ struct RingBins {
   double bound[kMaxBounds];      // sector angles 0 .. ns
   int ns;
   int axis;
-  double kin;                    // Max_radius_inside
+  double kin;                    // rings: Max_radius_inside; cylinders: Anis_max_Krho_radius_inside
+  int cyl;                       // 0: shells x sectors, 1: cylindrical shells x k_par slabs
 };
 
-__device__ __forceinline__ void mode_angle(const Geo& g, long long idx, int axis, int& r1, int& r2, int& l3,
+// rings: K = |K| and theta the unfolded polar angle; cylinders: K = K_perp and theta = K_par
+__device__ __forceinline__ void mode_angle(const Geo& g, long long idx, int axis, int cyl, int& r1, int& r2, int& l3,
                                            double& K, double& theta, double k[3]) {
   compact_mode(g, idx, r1, r2, l3);
   k[0] = geo_kx(g, r1) * g.kf0;
   k[1] = geo_ky(g, r2) * g.kf1;
   k[2] = l3 * g.kf2;
   const int ax = axis - 1, p1 = (ax + 1) % 3, p2 = (ax + 2) % 3;
-  K = sqrt(k[0] * k[0] + k[1] * k[1] + k[2] * k[2]);
-  theta = polar_angle(sqrt(k[p1] * k[p1] + k[p2] * k[p2]), k[ax]);
+  const double kperp = sqrt(k[p1] * k[p1] + k[p2] * k[p2]);
+  if (cyl) {
+    K = kperp;
+    theta = k[ax];
+  } else {
+    K = sqrt(k[0] * k[0] + k[1] * k[1] + k[2] * k[2]);
+    theta = polar_angle(kperp, k[ax]);
+  }
 }
 
-// G = F where inner < |K| <= outer and left < theta <= right (theta unfolded, in [0, pi)), or
-// theta = 0 in the first sector
+// G = F where inner < K <= outer and left < theta <= right, or theta = 0 in the first sector or
+// slab (Fill_array_ring / Fill_array_cylinder_ring: theta unfolded, K_par signed)
 __global__ void k_fill_ring(Geo g, const cx<double>* F0, const cx<double>* F1, const cx<double>* F2, cx<double>* G0,
-                            cx<double>* G1, cx<double>* G2, double lo, double hi, double left, double right, int axis) {
+                            cx<double>* G1, cx<double>* G2, double lo, double hi, double left, double right, int axis,
+                            int cyl) {
   const long long idx = (long long)blockIdx.x * TPB + threadIdx.x;
   if (idx >= g.S) return;
   int r1, r2, l3;
   double K, th, k[3];
-  mode_angle(g, idx, axis, r1, r2, l3, K, th, k);
+  mode_angle(g, idx, axis, cyl, r1, r2, l3, K, th, k);
   const bool in = (l3 < g.nkz) && (K > lo) && (K <= hi) &&
                   ((th > left && th <= right) || (fabs(th) < kEps && left < kEps));
   const cx<double> z = mkc<double>(0, 0);
@@ -259,16 +268,29 @@ __global__ void __launch_bounds__(TPB) k_ring_contract(RingContractArgs a) {
   for (long long idx = (long long)blockIdx.x * TPB + threadIdx.x; idx < g.S; idx += stride) {
     int r1, r2, l3;
     double K, th, k[3];
-    mode_angle(g, idx, a.b.axis, r1, r2, l3, K, th, k);
-    if (l3 >= g.nkz || !(K <= a.b.kin && K > kEps)) continue;
-    int shell = 0;  // first radius >= |K| (the radii need not be sorted)
+    mode_angle(g, idx, a.b.axis, a.b.cyl, r1, r2, l3, K, th, k);
+    if (l3 >= g.nkz) continue;
+    // Local_ring_mult_all: 0 < |K| <= R_in; Local_cyl_ring_mult_all: K_perp <= K_perp,max
+    if (a.b.cyl ? !(K <= a.b.kin) : !(K <= a.b.kin && K > kEps)) continue;
+    int shell = 0;  // first radius >= K (the radii need not be sorted)
     while (shell <= a.b.n && !(K <= a.b.r[shell])) ++shell;
     if (shell > a.b.n) continue;
-    if (th > M_PI / 2) th = M_PI - th;
-    int sector = 1;
-    if (!(fabs(th) < kEps)) {
-      sector = 0;
-      while (sector <= a.b.ns && !(th <= a.b.bound[sector])) ++sector;
+    int sector;
+    if (!a.b.cyl) {
+      // Compute_ring_index: the angle folded to [0, pi/2]
+      if (th > M_PI / 2) th = M_PI - th;
+      sector = 1;
+      if (!(fabs(th) < kEps)) {
+        sector = 0;
+        while (sector <= a.b.ns && !(th <= a.b.bound[sector])) ++sector;
+      }
+    } else {
+      // Compute_cylinder_ring_index: |K_par|, K_par = 0 in slab 1
+      th = fabs(th);
+      sector = 1;
+      if (!(th < kEps)) {
+        while (sector <= a.b.ns && !(th <= a.b.bound[sector])) ++sector;
+      }
     }
     if (sector > a.b.ns) continue;
     const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
@@ -291,9 +313,17 @@ __global__ void __launch_bounds__(TPB) k_ring_contract(RingContractArgs a) {
     if (sh[i] != 0) atomicAdd(&a.out[i], sh[i]);
 }
 
-// EnergyTr.cc:190-210, scheme 0
-void ring_radii(const tg_ctx* c, int n, double* r) {
-  const double Rin = (double)radius_inside(c);
+int krho_inside(const tg_ctx* c, int axis) {
+  const int d = c->cfg.dealias ? 3 : 2;
+  const double* kf = c->cfg.kfactor;
+  const int Nax[3] = {c->N1, c->N2, c->N3};
+  const int p1 = axis % 3, p2 = (axis + 1) % 3;
+  return (int)std::min((Nax[p1] / d) * kf[p1], (Nax[p2] / d) * kf[p2]);
+}
+
+// EnergyTr.cc:190-210 (rings, Rin = Max_radius_inside) and :300-320 (cylinders, Rin =
+// Anis_max_Krho_radius_inside), scheme 0
+void ring_radii_from(double Rin, int n, double* r) {
   for (int i = 0; i <= n; ++i) r[i] = 0.0;
   r[1] = 4.0;
   r[2] = 8.0;
@@ -306,6 +336,8 @@ void ring_radii(const tg_ctx* c, int n, double* r) {
   }
 }
 
+void ring_radii(const tg_ctx* c, int n, double* r) { ring_radii_from((double)radius_inside(c), n, r); }
+
 }  // namespace
 
 extern "C" {
@@ -316,7 +348,11 @@ int tg_ring_radii(tg_ctx* c, int n_ring_shells, double* radii, int n) {
   return TG_OK;
 }
 
-int tg_ring_to_ring(tg_ctx* c, int kind, int axis, int n_ring_shells, int n_sectors, double* tr, int n) {
+}  // extern "C"
+
+namespace {
+
+int run_ring_tr(tg_ctx* c, int kind, int axis, int n_ring_shells, int n_sectors, int cyl, double* tr, int n) {
   if (!c || !tr) return TG_ERR_ARG;
   if (c->basis != TG_FOUR) return set_err(c, TG_ERR_UNSUPPORTED, "ring transfers: FOUR basis only");
   if (axis < 1 || axis > 3 || n_sectors < 1 || n_sectors > TG_RING_MAX_SECTORS) return TG_ERR_ARG;
@@ -335,13 +371,27 @@ int tg_ring_to_ring(tg_ctx* c, int kind, int axis, int n_ring_shells, int n_sect
   if (rc) return rc;
   RingBins b{};
   b.n = n_ring_shells;
-  ring_radii(c, n_ring_shells, b.r);
   b.ns = n_sectors;
-  const double dtheta = (M_PI / 2) / n_sectors;
-  for (int i = 0; i < n_sectors; ++i) b.bound[i] = i * dtheta;
-  b.bound[n_sectors] = M_PI / 2;
   b.axis = axis;
-  b.kin = (double)radius_inside(c);
+  b.cyl = cyl;
+  if (!cyl) {
+    ring_radii(c, n_ring_shells, b.r);
+    const double dtheta = (M_PI / 2) / n_sectors;
+    for (int i = 0; i < n_sectors; ++i) b.bound[i] = i * dtheta;
+    b.bound[n_sectors] = M_PI / 2;
+    b.kin = (double)radius_inside(c);
+  } else {
+    const int kr = krho_inside(c, axis);
+    ring_radii_from((double)kr, n_ring_shells, b.r);
+    const int d = c->cfg.dealias ? 3 : 2;
+    const int Nax[3] = {c->N1, c->N2, c->N3};
+    const double kmax = (Nax[axis - 1] / d) * c->cfg.kfactor[axis - 1];
+    const double dk = kmax / n_sectors;
+    b.bound[0] = 0.0;
+    for (int i = 1; i < n_sectors; ++i) b.bound[i] = i * dk;
+    b.bound[n_sectors] = kmax;
+    b.kin = (double)kr;
+  }
   const size_t need = (size_t)per * per;  // [giver shell][giver sector][shell][sector]
   rc = ensure_diag(c, need);
   if (rc) return rc;
@@ -369,7 +419,8 @@ int tg_ring_to_ring(tg_ctx* c, int kind, int axis, int n_ring_shells, int n_sect
     for (int j = 1; j <= n_sectors; ++j) {
       k_fill_ring<<<(int)((g.S + TPB - 1) / TPB), TPB, 0, c->st>>>(g, c->U0[3 * F + 0], c->U0[3 * F + 1],
                                                                    c->U0[3 * F + 2], c->etG[0], c->etG[1], c->etG[2],
-                                                                   b.r[i - 1], b.r[i], b.bound[j - 1], b.bound[j], axis);
+                                                                   b.r[i - 1], b.r[i], b.bound[j - 1], b.bound[j], axis,
+                                                                   cyl);
       e = cudaGetLastError();
       if (e != cudaSuccess) return cuda_err(c, e, "fill ring");
       const void* G[3] = {c->etG[0], c->etG[1], c->etG[2]};
@@ -397,6 +448,10 @@ int tg_ring_to_ring(tg_ctx* c, int kind, int axis, int n_ring_shells, int n_sect
 }
 
 
+}  // namespace
+
+extern "C" {
+
 int tg_ring_sizes(tg_ctx* c, int axis, int* ring_shells, int* cylinder_shells) {
   if (!c || axis < 1 || axis > 3) return TG_ERR_ARG;
   const int d = c->cfg.dealias ? 3 : 2;
@@ -415,6 +470,22 @@ int tg_ring_spectrum(tg_ctx* c, int group, int axis, int n_sectors, double* ek1,
 int tg_cylinder_ring_spectrum(tg_ctx* c, int group, int axis, int n_slabs, double* ek1, double* ek2, double* dissk,
                               int n) {
   return run_ring(c, group, axis, n_slabs, 1, ek1, ek2, dissk, n);
+}
+
+int tg_ring_to_ring(tg_ctx* c, int kind, int axis, int n_ring_shells, int n_sectors, double* tr, int n) {
+  return run_ring_tr(c, kind, axis, n_ring_shells, n_sectors, 0, tr, n);
+}
+
+int tg_cylinder_ring_to_ring(tg_ctx* c, int kind, int axis, int n_cylinder_shells, int n_slabs, double* tr, int n) {
+  return run_ring_tr(c, kind, axis, n_cylinder_shells, n_slabs, 1, tr, n);
+}
+
+int tg_cylinder_radii(tg_ctx* c, int axis, int n_cylinder_shells, double* radii, int n) {
+  if (!c || !radii || axis < 1 || axis > 3 || n_cylinder_shells < 5 || n_cylinder_shells > kMaxRingShells ||
+      n < n_cylinder_shells + 1)
+    return TG_ERR_ARG;
+  ring_radii_from((double)krho_inside(c, axis), n_cylinder_shells, radii);
+  return TG_OK;
 }
 
 }  // extern "C"

@@ -377,6 +377,17 @@ class IncFluid:
                  "ring transfer")
         return T, r
 
+    def Compute_cylinder_ring_tr(self, n_cylinder_shells, n_slabs, axis=1, kind=L.TG_ET_UU):
+        """IncVF::Compute_cylinder_ring_tr (tg_cylinder_ring_to_ring): T[i, j, m, s] from giver
+        cylinder ring (shell i, slab j) to receiver (m, s), and the cylinder radii."""
+        r = np.zeros(n_cylinder_shells + 1)
+        self._ck(self.lib.tg_cylinder_radii(self.h, axis, n_cylinder_shells, _dptr(r), r.size), "cylinder radii")
+        n1, n2 = n_cylinder_shells + 1, n_slabs + 1
+        T = np.zeros((n1, n2, n1, n2))
+        self._ck(self.lib.tg_cylinder_ring_to_ring(self.h, kind, axis, n_cylinder_shells, n_slabs, _dptr(T),
+                                                   T.size), "cylinder ring transfer")
+        return T, r
+
     def Compute_force_feed_shell(self):
         """IncVF::Compute_force_feed_shell (compute_force_feed.cc:70-76): forceV_shell, S+1 entries."""
         S = self.cfg.n_shells

@@ -139,3 +139,32 @@ def test_gpu_ring_to_ring_mhd_kinds(lib):
         assert np.abs(T - want).max() <= 1e-12 * np.abs(want).max(), kind
     with pytest.raises(L.TarangError):
         s.Compute_ring_tr(6, 2, 1, L.TG_ET_BU)       # not a ring transfer of the reference
+
+
+def test_cylinder_ring_transfer_oracle_identity():
+    """Cylinder-ring-to-ring transfer (oracle, z axis: every stored mode has K_par >= 0, so the
+    givers cover the field): the transfer between two cylinder rings is antisymmetric."""
+    N = (64, 64, 64)
+    V = ic.random_phase_field(N, seed=72)
+    n, ns = 6, 3
+    T = o.compute_cylinder_ring_tr_generic(V, V, V, -1.0, KF, 3, n, ns)
+    scale = np.abs(T).max()
+    assert scale > 0
+    for i in range(1, n):
+        for j in range(1, ns + 1):
+            for m in range(1, n):
+                for s in range(1, ns + 1):
+                    assert abs(T[i, j, m, s] + T[m, s, i, j]) <= 1e-12 * scale
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("N,axis,n,ns", [((64, 64, 64), 3, 6, 3), ((64, 64, 32), 1, 5, 4), ((32, 64, 64), 2, 7, 2)])
+def test_gpu_cylinder_ring_to_ring_matches_oracle(lib, N, axis, n, ns):
+    from tarang_b200.solver import IncFluid
+    V = ic.random_phase_field(N, seed=90 + axis)
+    s = IncFluid(N, nu=1e-3, dt=1e-3)
+    s.set_V(V)
+    T, r = s.Compute_cylinder_ring_tr(n, ns, axis)
+    assert np.allclose(r, o.ring_radii(N, KF, n, Rin=float(o.krho_inside(N, KF, axis))), rtol=0, atol=0)
+    want = o.compute_cylinder_ring_tr_generic(V, V, V, -1.0, KF, axis, n, ns)
+    assert np.abs(T - want).max() <= 1e-12 * np.abs(want).max()
