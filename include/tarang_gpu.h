@@ -245,6 +245,17 @@ int tg_shell_spectrum(tg_ctx* ctx, int group, double* ek, double* dissk, int n);
  * uninitialised value); the z-axis components are used. */
 #define TG_RING_MAX_SECTORS 64
 int tg_ring_sizes(tg_ctx* ctx, int axis, int* ring_shells, int* cylinder_shells);
+/* Helicity spectra (FOUR): modal helicity 2 mult K . (Vr x Vi) per mode.
+ * tg_shell_spectrum_helicity: CVF::CV_Compute_shell_spectrum_helicity (Cvf.cc:640-646,
+ * Compute_shell_spectrum_helicity_FOUR four/four_energy.cc:551-651): the three terms
+ * 2 mult K_i (Vr x Vi)_i in h1, h2, h3 over shells 0 .. Min_radius_outside (n >= that + 1),
+ * shells beyond Max_radius_inside rescaled by Approx_number_modes_in_shell / (sum of 2 mult
+ * over the shell).  tg_ring_spectrum_helicity / tg_cylinder_ring_spectrum_helicity:
+ * CV_Compute_ring_spectrum_helicity / CV_Compute_cylinder_ring_spectrum_helicity (Cvf.cc:648-665,
+ * four_energy.cc:1357-1450, 1825-1910), binned as tg_ring_spectrum / tg_cylinder_ring_spectrum. */
+int tg_shell_spectrum_helicity(tg_ctx* ctx, int group, double* h1, double* h2, double* h3, int n);
+int tg_ring_spectrum_helicity(tg_ctx* ctx, int group, int axis, int n_sectors, double* h, int n);
+int tg_cylinder_ring_spectrum_helicity(tg_ctx* ctx, int group, int axis, int n_slabs, double* h, int n);
 int tg_ring_spectrum(tg_ctx* ctx, int group, int axis, int n_sectors, double* ek1, double* ek2, double* dissk, int n);
 int tg_cylinder_ring_spectrum(tg_ctx* ctx, int group, int axis, int n_slabs, double* ek1, double* ek2, double* dissk,
                               int n);

@@ -556,7 +556,40 @@ def _slab_index(kpll, bounds):
     return len(bounds)
 
 
-def ring_spectrum(V, kfactor, axis, n_sectors, alias="DEALIAS", cylinder=False):
+def min_radius_outside_four(N, kfactor, alias="DEALIAS"):
+    """Min_radius_outside_FOUR  four_inline.h:172-228."""
+    d = 3 if alias == "DEALIAS" else 2
+    return int(math.ceil(math.sqrt(sum(((N[i] // d) * kfactor[i]) ** 2 for i in range(3)))))
+
+
+def shell_spectrum_helicity(V, kfactor, alias="DEALIAS"):
+    """Compute_shell_spectrum_helicity_FOUR  four_energy.cc:551-651: H_i(k) = sum over shell
+    ceil|K| = k of 2 mult K_i (Vr x Vi)_i, k <= Min_radius_outside; shells beyond
+    Max_radius_inside rescaled by Approx_number_modes_in_shell / sum(2 mult) over the shell."""
+    N = (V[0].shape[0], V[0].shape[1], 2 * (V[0].shape[2] - 1))
+    kmax = min_radius_outside_four(N, kfactor, alias)
+    kin = max_radius_inside(N, kfactor, alias)
+    Kx, Ky, Kz = kvec(N, kfactor)
+    shape = V[0].shape
+    K = [np.broadcast_to(k, shape) for k in (Kx, Ky, Kz)]
+    idx = np.ceil(np.sqrt(K[0] ** 2 + K[1] ** 2 + K[2] ** 2)).astype(np.int64)
+    f = 2 * multiplicity_four(N)
+    Vr = [v.real for v in V]
+    Vi = [v.imag for v in V]
+    cr = [Vr[1] * Vi[2] - Vr[2] * Vi[1], Vr[2] * Vi[0] - Vr[0] * Vi[2], Vr[0] * Vi[1] - Vr[1] * Vi[0]]
+    sel = idx <= kmax
+    cnt = np.bincount(idx[sel], weights=f[sel], minlength=kmax + 1)
+    out = []
+    for i in range(3):
+        h = np.bincount(idx[sel], weights=(f * K[i] * cr[i])[sel], minlength=kmax + 1)
+        for k in range(kin + 1, kmax + 1):
+            if cnt[k] >= 1:
+                h[k] *= approx_number_modes_in_shell(N, k, kfactor) / cnt[k]
+        out.append(h)
+    return tuple(out)
+
+
+def ring_spectrum(V, kfactor, axis, n_sectors, alias="DEALIAS", cylinder=False, helicity=False):
     """CVF::CV_Compute_ring_spectrum (Cvf.cc:484-504; Compute_local_ring_spectrum_FOUR
     four_energy.cc:828-955) or, with cylinder=True, CV_Compute_cylinder_ring_spectrum
     (Cvf.cc:537-559; Compute_local_cylinder_ring_spectrum_FOUR four_energy.cc:1450-1516), FOUR,
@@ -616,6 +649,12 @@ def ring_spectrum(V, kfactor, axis, n_sectors, alias="DEALIAS", cylinder=False):
                     col = _slab_index(kpll, bounds)
                     e1 = abs(vals[ax]) ** 2
                     e2 = vv - e1
+                if helicity:
+                    # Compute_local_(cylinder_)ring_spectrum_helicity_FOUR: 2 mult K . (Vr x Vi)
+                    vr = np.array([x.real for x in vals])
+                    vi = np.array([x.imag for x in vals])
+                    e1 = 2.0 * float(np.dot(k, np.cross(vr, vi)))
+                    e2 = 0.0
                 if col >= n + 1:
                     continue
                 out[0, row, col] += f * e1

@@ -174,6 +174,9 @@ SIGNATURES = {
     "tg_ring_spectrum": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, _DP, _DP, _DP, C.c_int]),
     "tg_cylinder_ring_spectrum": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, _DP, _DP, _DP, C.c_int]),
     "tg_ring_radii": (C.c_int, [_VP, C.c_int, _DP, C.c_int]),
+    "tg_shell_spectrum_helicity": (C.c_int, [_VP, C.c_int, _DP, _DP, _DP, C.c_int]),
+    "tg_ring_spectrum_helicity": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, _DP, C.c_int]),
+    "tg_cylinder_ring_spectrum_helicity": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, _DP, C.c_int]),
     "tg_helicity_flux": (C.c_int, [_VP, _DP, C.c_int]),
     "tg_ring_to_ring": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, C.c_int, _DP, C.c_int]),
     "tg_cylinder_radii": (C.c_int, [_VP, C.c_int, C.c_int, _DP, C.c_int]),

@@ -37,6 +37,7 @@ struct RingArgs {
   int nb;               // entries of bound[] used: n + 1
   double bound[kMaxBounds];  // sector angles or slab k_par values
   double* out;          // [4][rows][cols]: S1, S2 (|K|^0), S1, S2 (|K|^2)
+  int hel;              // 1: S1 = modal helicity 2 K . (Vr x Vi) (the helicity ring spectra)
 };
 
 // Get_polar_angle: atan(k_perp / k_par) in [0, pi)
@@ -117,6 +118,14 @@ __global__ void __launch_bounds__(TPB) k_ring(RingArgs a, int use_smem) {
       e1 = v[ax].x * v[ax].x + v[ax].y * v[ax].y;
       e2 = vv - e1;
     }
+    if (a.hel) {
+      // Compute_local_(cylinder_)ring_spectrum_helicity_FOUR (four_energy.cc:1357-1413,
+      // 1825-1880): 2 mult K . (Vr x Vi)
+      const double c0 = v[1].x * v[2].y - v[2].x * v[1].y, c1 = v[2].x * v[0].y - v[0].x * v[2].y,
+                   c2 = v[0].x * v[1].y - v[1].x * v[0].y;
+      e1 = 2.0 * (k[0] * c0 + k[1] * c1 + k[2] * c2);
+      e2 = 0.0;
+    }
     if (col < 0 || col >= a.cols) continue;
     const int b = row * a.cols + col;
     atomicAdd(&acc[b], f * e1);
@@ -131,7 +140,35 @@ __global__ void __launch_bounds__(TPB) k_ring(RingArgs a, int use_smem) {
   }
 }
 
-int run_ring(tg_ctx* c, int group, int axis, int n, int cyl, double* ek1, double* ek2, double* dissk, int cap) {
+// Compute_local_shell_spectrum_helicity_FOUR (four_energy.cc:551-603): shell ceil|K| <=
+// Min_radius_outside gets 2 mult K_i (Vr x Vi)_i per component i
+__global__ void __launch_bounds__(TPB) k_shell_helicity(Geo g, const cx<double>* V0, const cx<double>* V1,
+                                                        const cx<double>* V2, int nbins, double* out) {
+  extern __shared__ double sh[];
+  for (int i = threadIdx.x; i < 3 * nbins; i += TPB) sh[i] = 0;
+  __syncthreads();
+  const long long stride = (long long)gridDim.x * TPB;
+  for (long long idx = (long long)blockIdx.x * TPB + threadIdx.x; idx < g.S; idx += stride) {
+    int r1, r2, l3;
+    compact_mode(g, idx, r1, r2, l3);
+    if (l3 >= g.nkz) continue;
+    const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
+    const double kx = geo_kx(g, r1) * g.kf0, ky = geo_ky(g, r2) * g.kf1, kz = l3 * g.kf2;
+    const int b = (int)ceil(sqrt(kx * kx + ky * ky + kz * kz));
+    if (b >= nbins) continue;
+    const cx<double> a = V0[idx], bb = V1[idx], d = V2[idx];
+    const double f = 2.0 * mult_four(l1, l2, l3, g.N1, g.N2);
+    atomicAdd(&sh[b], f * kx * (bb.x * d.y - d.x * bb.y));
+    atomicAdd(&sh[nbins + b], f * ky * (d.x * a.y - a.x * d.y));
+    atomicAdd(&sh[2 * nbins + b], f * kz * (a.x * bb.y - bb.x * a.y));
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 3 * nbins; i += TPB)
+    if (sh[i] != 0) atomicAdd(&out[i], sh[i]);
+}
+
+int run_ring(tg_ctx* c, int group, int axis, int n, int cyl, double* ek1, double* ek2, double* dissk, int cap,
+             int hel = 0) {
   if (!c || !ek1) return TG_ERR_ARG;
   if (c->basis != TG_FOUR) return set_err(c, TG_ERR_UNSUPPORTED, "ring spectra: FOUR basis only");
   if (axis < 1 || axis > 3 || n < 1 || n > TG_RING_MAX_SECTORS) return TG_ERR_ARG;
@@ -143,6 +180,7 @@ int run_ring(tg_ctx* c, int group, int axis, int n, int cyl, double* ek1, double
   a.g = c->g;
   for (int i = 0; i < 3; ++i) a.V[i] = c->U0[3 * group + i];
   a.cyl = cyl;
+  a.hel = hel;
   a.axis = axis;
   a.cols = n + 1;
   a.nb = n + 1;
@@ -474,6 +512,72 @@ int tg_cylinder_ring_spectrum(tg_ctx* c, int group, int axis, int n_slabs, doubl
 
 int tg_ring_to_ring(tg_ctx* c, int kind, int axis, int n_ring_shells, int n_sectors, double* tr, int n) {
   return run_ring_tr(c, kind, axis, n_ring_shells, n_sectors, 0, tr, n);
+}
+
+int tg_ring_spectrum_helicity(tg_ctx* c, int group, int axis, int n_sectors, double* h, int n) {
+  return run_ring(c, group, axis, n_sectors, 0, h, nullptr, nullptr, n, 1);
+}
+
+int tg_cylinder_ring_spectrum_helicity(tg_ctx* c, int group, int axis, int n_slabs, double* h, int n) {
+  return run_ring(c, group, axis, n_slabs, 1, h, nullptr, nullptr, n, 1);
+}
+
+int tg_shell_spectrum_helicity(tg_ctx* c, int group, double* h1, double* h2, double* h3, int n) {
+  if (!c || !h1) return TG_ERR_ARG;
+  if (c->basis != TG_FOUR) return set_err(c, TG_ERR_UNSUPPORTED, "helicity spectrum: FOUR basis only");
+  if (group != 0 && !(group == 1 && c->phys == TG_MHD)) return TG_ERR_ARG;
+  // Min_radius_outside_FOUR (four_inline.h:172-228) and Max_radius_inside
+  const int d = c->cfg.dealias ? 3 : 2;
+  const double* kf = c->cfg.kfactor;
+  const double a0 = (c->N1 / d) * kf[0], a1 = (c->N2 / d) * kf[1], a2 = (c->N3 / d) * kf[2];
+  const int kkmax = (int)std::ceil(std::sqrt(a0 * a0 + a1 * a1 + a2 * a2));
+  const int kin = radius_inside(c);
+  const int nbins = kkmax + 1;
+  if (n < nbins) return set_err(c, TG_ERR_ARG, "helicity spectrum: n < kmax_outside + 1");
+  cudaSetDevice(c->dev);
+  int rc = ensure_diag(c, (size_t)3 * nbins);
+  if (rc) return rc;
+  cudaError_t e = cudaMemsetAsync(c->diag, 0, sizeof(double) * 3 * nbins, c->st);
+  if (e != cudaSuccess) return cuda_err(c, e, "helicity spectrum");
+  const size_t smem = sizeof(double) * 3 * (size_t)nbins;
+  if (smem > 48 * 1024) {
+    e = cudaFuncSetAttribute(k_shell_helicity, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_err(c, e, "helicity spectrum");
+  }
+  long long nb = (c->g.S + TPB - 1) / TPB;
+  if (nb > 148 * 4) nb = 148 * 4;
+  k_shell_helicity<<<(unsigned)nb, TPB, smem, c->st>>>(c->g, c->U0[3 * group], c->U0[3 * group + 1],
+                                                       c->U0[3 * group + 2], nbins, c->diag);
+  e = cudaGetLastError();
+  std::vector<double> hh((size_t)3 * nbins);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(hh.data(), c->diag, sizeof(double) * hh.size(), cudaMemcpyDeviceToHost, c->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+  if (e != cudaSuccess) return cuda_err(c, e, "helicity spectrum");
+  // H1k_count: 2 mult over every mode of the dense grid (geometry only); partial shells
+  // (kmax_inside, kmax] rescaled by Approx_number_modes_in_shell / count (four_energy.cc:637-651)
+  std::vector<double> cnt(nbins, 0.0);
+  for (int l1 = 0; l1 < c->N1; ++l1) {
+    const int kxi = l1 > c->N1 / 2 ? l1 - c->N1 : l1;
+    for (int l2 = 0; l2 < c->N2; ++l2) {
+      const int kyi = l2 <= c->N2 / 2 ? l2 : l2 - c->N2;
+      for (int l3 = 0; l3 < c->M3; ++l3) {
+        const double kx = kxi * kf[0], ky = kyi * kf[1], kz = l3 * kf[2];
+        const int b = (int)std::ceil(std::sqrt(kx * kx + ky * ky + kz * kz));
+        if (b < nbins) cnt[b] += 2.0 * mult_four(l1, l2, l3, c->N1, c->N2);
+      }
+    }
+  }
+  const double approx_fac = 2 * M_PI / (kf[0] * kf[1] * kf[2]);
+  double* out[3] = {h1, h2, h3};
+  for (int i = 0; i < 3; ++i) {
+    if (!out[i]) continue;
+    for (int b = 0; b < n; ++b) out[i][b] = 0.0;
+    for (int b = 0; b < nbins; ++b) {
+      const bool resc = (b > kin) && (cnt[b] >= 1);
+      out[i][b] = hh[(size_t)i * nbins + b] * (resc ? approx_fac * b * b / cnt[b] : 1.0);
+    }
+  }
+  return TG_OK;
 }
 
 int tg_cylinder_ring_to_ring(tg_ctx* c, int kind, int axis, int n_cylinder_shells, int n_slabs, double* tr, int n) {

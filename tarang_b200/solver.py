@@ -358,6 +358,32 @@ class IncFluid:
         dissk), each [cylindrical shell][slab] along `axis`."""
         return self._ring(self.lib.tg_cylinder_ring_spectrum, True, n_slabs, axis, group)
 
+    def CV_Compute_shell_spectrum_helicity(self, group=0):
+        """CVF::CV_Compute_shell_spectrum_helicity (tg_shell_spectrum_helicity): (h1, h2, h3)."""
+        n = self.kmax_outside() + 1
+        out = [np.zeros(n) for _ in range(3)]
+        self._ck(self.lib.tg_shell_spectrum_helicity(self.h, group, *[_dptr(a) for a in out], n),
+                 "helicity spectrum")
+        return tuple(out)
+
+    def CV_Compute_ring_spectrum_helicity(self, n_sectors, axis=1, group=0):
+        """CV_Compute_ring_spectrum_helicity (tg_ring_spectrum_helicity): [shell][sector]."""
+        rs = C.c_int()
+        self._ck(self.lib.tg_ring_sizes(self.h, axis, C.byref(rs), None), "ring sizes")
+        h = np.zeros((rs.value, n_sectors + 1))
+        self._ck(self.lib.tg_ring_spectrum_helicity(self.h, group, axis, n_sectors, _dptr(h), h.size),
+                 "ring helicity")
+        return h
+
+    def CV_Compute_cylinder_ring_spectrum_helicity(self, n_slabs, axis=1, group=0):
+        """CV_Compute_cylinder_ring_spectrum_helicity (tg_cylinder_ring_spectrum_helicity)."""
+        cs = C.c_int()
+        self._ck(self.lib.tg_ring_sizes(self.h, axis, None, C.byref(cs)), "ring sizes")
+        h = np.zeros((cs.value, n_slabs + 1))
+        self._ck(self.lib.tg_cylinder_ring_spectrum_helicity(self.h, group, axis, n_slabs, _dptr(h), h.size),
+                 "cylinder helicity")
+        return h
+
     def Compute_kinetic_helicity_flux(self):
         """IncVF::Compute_kinetic_helicity_flux (tg_helicity_flux): flux_hk, n_shells + 1 entries."""
         S = self.cfg.n_shells

@@ -168,3 +168,38 @@ def test_gpu_cylinder_ring_to_ring_matches_oracle(lib, N, axis, n, ns):
     assert np.allclose(r, o.ring_radii(N, KF, n, Rin=float(o.krho_inside(N, KF, axis))), rtol=0, atol=0)
     want = o.compute_cylinder_ring_tr_generic(V, V, V, -1.0, KF, axis, n, ns)
     assert np.abs(T - want).max() <= 1e-12 * np.abs(want).max()
+
+
+def test_helicity_spectra_oracle_identities():
+    """The shell helicity spectrum sums to the total helicity sum 2 mult K . (Vr x Vi) within
+    Max_radius_inside, and the ring helicity spectrum summed over sectors gives its shells; a
+    Beltrami (ABC) field has helicity spectrum k0 times twice its energy spectrum."""
+    N = (32, 32, 32)
+    V = ic.random_phase_field(N, seed=21)
+    h = o.shell_spectrum_helicity(V, KF)
+    ring = o.ring_spectrum(V, KF, 3, 4, helicity=True)[0]
+    kin = o.max_radius_inside(N, KF)
+    tot = sum(h)
+    assert np.allclose(ring.sum(axis=1)[1:kin + 1], tot[1:kin + 1], rtol=1e-12, atol=1e-16)
+    A = o.abc_force(N, 2, 1.0, 1.0, 0.7, 0.4)          # curl A = k0 A
+    H = sum(o.shell_spectrum_helicity(A, KF))
+    E = sum(o.shell_spectrum(a, 0, KF) for a in A)
+    assert abs(H[2] - 2 * E[2]) <= 1e-12 * abs(E[2]) and abs(H).sum() == pytest.approx(abs(H[2]), rel=1e-12)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("N,kf", [((32, 32, 32), (1.0, 1.0, 1.0)), ((64, 32, 32), (1.0, 2.0, 0.5))])
+def test_gpu_helicity_spectra_match_oracle(lib, N, kf):
+    from tarang_b200.solver import IncFluid
+    V = ic.random_phase_field(N, kfactor=kf, seed=33)
+    s = IncFluid(N, kfactor=kf, nu=1e-3, dt=1e-3)
+    s.set_V(V)
+    for g, w in zip(s.CV_Compute_shell_spectrum_helicity(), o.shell_spectrum_helicity(V, kf)):
+        assert np.abs(g - w).max() <= 1e-12 * np.abs(w).max()
+    for axis in (1, 3):
+        g = s.CV_Compute_ring_spectrum_helicity(4, axis)
+        w = o.ring_spectrum(V, kf, axis, 4, helicity=True)[0]
+        assert np.abs(g - w).max() <= 1e-12 * np.abs(w).max()
+        g = s.CV_Compute_cylinder_ring_spectrum_helicity(3, axis)
+        w = o.ring_spectrum(V, kf, axis, 3, cylinder=True, helicity=True)[0]
+        assert np.abs(g - w).max() <= 1e-12 * np.abs(w).max()
