@@ -62,6 +62,10 @@ extern "C" {
 #define TG_FORCE_CORIOLIS 21  /* Force = V x Omega, Omega = force_para[0..2], evaluated from each RK
                                  stage's velocity (compute_force_Coriolis.cc:47-80) */
 #define TG_FORCE_RB 51
+#define TG_FORCE_RB_ROTATION 52  /* convection with rotation (compute_force_RB.cc:132-195): the
+                                    buoyancy of TG_FORCE_RB plus c V x Omega, Omega =
+                                    force_para[0..2], c = Pr (PRLARGE, USMALL), 1 (PRSMALL, USMALL)
+                                    or sqrt(Pr/Ra) (ULARGE) */
 
 #define TG_RB_PRLARGE 0
 #define TG_RB_PRSMALL 1

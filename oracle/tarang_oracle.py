@@ -967,7 +967,7 @@ class RBSolver:
     Fields: V = [u1 (sin), u2 (cos), u3 (cos)], T = theta (sin) in the SCFT basis."""
 
     def __init__(self, N, kfactor, Ra, Pr, Tdt, basis="SCFT", alias="DEALIAS", temperature_grad=1.0,
-                 pr_switch="PRLARGE", u_scaling="ULARGE"):
+                 pr_switch="PRLARGE", u_scaling="ULARGE", omega=None):
         self.N = tuple(N)
         self.kfactor = tuple(kfactor)
         self.nu, self.kappa, self.fu, self.ft, self.nuf = rb_coefficients(Ra, Pr, pr_switch, u_scaling,
@@ -977,6 +977,13 @@ class RBSolver:
         self.basis = basis
         self.alias = alias
         self.tg = temperature_grad
+        # Compute_force_RB_rotation (compute_force_RB.cc:132-165): the Coriolis force V x omega
+        # scaled by Pr (PRLARGE, USMALL), 1 (PRSMALL, USMALL) or sqrt(Pr/Ra) (ULARGE)
+        self.omega = omega
+        if u_scaling == "ULARGE":
+            self.cor = math.sqrt(Pr / Ra)
+        else:
+            self.cor = Pr if pr_switch == "PRLARGE" else 1.0
 
     def rhs(self, V, T):
         nl = nlin_fluid(V, self.kfactor, self.basis, self.alias)
@@ -986,6 +993,9 @@ class RBSolver:
         if self.alias == "DEALIAS":     # Dealias_force(T)
             F1 = dealias(F1, self.basis)
             TF = dealias(TF, self.basis)
+        if self.omega is not None:
+            C = force_coriolis(V, self.omega)
+            nl = [nl[0] - self.cor * C[0], nl[1] - self.cor * C[1], nl[2] - self.cor * C[2]]
         nl = [nl[0] - F1, nl[1], nl[2]]
         tn = tn - TF
         p = pressure(nl, self.kfactor, self.basis, self.alias)

@@ -582,7 +582,7 @@ int ctx_create_batch(const tg_config* cfg, int B, tg_ctx** out) {
       pp.a[q] = PA[q];
       pp.b[q] = PB[q];
     }
-    if (c->phys == TG_RB && cfg->force_kind == TG_FORCE_RB) {
+    if (c->phys == TG_RB && (cfg->force_kind == TG_FORCE_RB || cfg->force_kind == TG_FORCE_RB_ROTATION)) {
       // Compute_force_RB: Force1 = fu theta, T.Force = ft u1
       const RBCoef r = rb_coefficients(cfg);
       c->rb_fu = r.fu;
@@ -718,9 +718,15 @@ int ctx_create_batch(const tg_config* cfg, int B, tg_ctx** out) {
   } else if (cfg->force_kind == TG_FORCE_MODES) {
     if (B != 1) return fail(set_err(c, TG_ERR_UNSUPPORTED, "forced requests are not batched"));
     c->force_on = 2;  // the box is allocated by tg_set_force_modes
-  } else if (cfg->force_kind == TG_FORCE_CORIOLIS) {
+  } else if (cfg->force_kind == TG_FORCE_CORIOLIS || cfg->force_kind == TG_FORCE_RB_ROTATION) {
     c->coriolis = true;
-    for (int i = 0; i < 3; ++i) c->om[i] = cfg->force_para[i];
+    // Compute_force_RB_rotation scales the Coriolis force with the nondimensionalisation
+    double sc = 1.0;
+    if (cfg->force_kind == TG_FORCE_RB_ROTATION) {
+      if (cfg->rb_u_scaling == TG_RB_ULARGE) sc = std::sqrt(cfg->rb_pr / cfg->rb_ra);
+      else if (cfg->rb_pr_switch == TG_RB_PRLARGE) sc = cfg->rb_pr;
+    }
+    for (int i = 0; i < 3; ++i) c->om[i] = sc * cfg->force_para[i];
   }
   e = cudaStreamSynchronize(c->st);
   if (e != cudaSuccess) return fail(cuda_err(c, e, "create"));
@@ -743,9 +749,13 @@ int validate_config(const tg_config* cfg) {
   if (cfg->precision != TG_FP64 && cfg->precision != TG_FP32_MIXED) return TG_ERR_ARG;
   if (cfg->scheme != TG_RK4) return TG_ERR_UNSUPPORTED;
   if (cfg->force_kind != TG_FORCE_DECAY && cfg->force_kind != TG_FORCE_ENERGY_SUPPLY && cfg->force_kind != TG_FORCE_RB &&
-      cfg->force_kind != TG_FORCE_MODES && cfg->force_kind != TG_FORCE_CORIOLIS)
+      cfg->force_kind != TG_FORCE_MODES && cfg->force_kind != TG_FORCE_CORIOLIS && cfg->force_kind != TG_FORCE_RB_ROTATION)
     return TG_ERR_UNSUPPORTED;
-  if (cfg->force_kind == TG_FORCE_RB && cfg->physics != TG_RB) return TG_ERR_ARG;
+  if ((cfg->force_kind == TG_FORCE_RB || cfg->force_kind == TG_FORCE_RB_ROTATION) && cfg->physics != TG_RB)
+    return TG_ERR_ARG;
+  if (cfg->force_kind == TG_FORCE_RB_ROTATION)
+    for (int i = 0; i < 3; ++i)
+      if (!std::isfinite(cfg->force_para[i])) return TG_ERR_ARG;
   // convection has its own force (force_field_proc 51)
   if ((cfg->force_kind == TG_FORCE_MODES || cfg->force_kind == TG_FORCE_CORIOLIS) && cfg->physics == TG_RB)
     return TG_ERR_UNSUPPORTED;

@@ -130,11 +130,11 @@ std::string batch_key(const tg_config& c, long long id) {
                 c.force_kind);
   std::string k(buf);
   if (c.force_kind == TG_FORCE_ENERGY_SUPPLY) k += "|solo" + std::to_string(id);
-  if (c.force_kind == TG_FORCE_CORIOLIS) {
+  if (c.force_kind == TG_FORCE_CORIOLIS || c.force_kind == TG_FORCE_RB_ROTATION) {
     std::snprintf(buf, sizeof(buf), "|om%a,%a,%a", c.force_para[0], c.force_para[1], c.force_para[2]);
     k += buf;
   }
-  if (c.physics == TG_RB && c.force_kind == TG_FORCE_RB) {
+  if (c.physics == TG_RB && (c.force_kind == TG_FORCE_RB || c.force_kind == TG_FORCE_RB_ROTATION)) {
     // the buoyancy coefficients are per context: requests share a batch only when they agree
     const RBCoef r = rb_coefficients(&c);
     std::snprintf(buf, sizeof(buf), "|rb%a,%a", r.fu, r.ft);

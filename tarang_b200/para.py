@@ -212,6 +212,16 @@ def config_from_para(p: dict, kind: str = "FLUID") -> dict:
         else:
             om = [fd[1], fd[2], fd[3]]
         cfg["force"] = dict(kind="coriolis", omega=tuple(om))
+    elif proc == 52 and kind == "RB":
+        # Compute_force_RB_rotation (compute_force_RB.cc:132-195): buoyancy plus the Coriolis
+        # force, Omega read as for proc 21
+        fi = p["force_int"] + [0] * 3
+        if fi[2] == 1 and fi[3] in (1, 2, 3):
+            om = [0.0, 0.0, 0.0]
+            om[fi[3] - 1] = fd[1]
+        else:
+            om = [fd[1], fd[2], fd[3]]
+        cfg["force"] = dict(kind="rb_rotation", omega=tuple(om))
     elif proc != 0 and kind != "RB":
         raise ValueError(f"force_field_proc {proc} is not supported")
     cfg["run"] = dict(Tinit=p["time_para"][1], Tfinal=p["time_para"][2],

@@ -62,6 +62,9 @@ def make_config(N, basis="FOUR", physics="FLUID", precision="FP64", dealias=True
     elif force.get("kind") == "coriolis":
         cfg.force_kind = L.TG_FORCE_CORIOLIS       # Force = V x omega (force_field_proc 21)
         cfg.force_para[:3] = [float(x) for x in force["omega"]]
+    elif force.get("kind") == "rb_rotation":
+        cfg.force_kind = L.TG_FORCE_RB_ROTATION    # buoyancy + scaled V x omega (proc 52)
+        cfg.force_para[:3] = [float(x) for x in force["omega"]]
     elif force.get("kind", "energy_supply") != "energy_supply":
         raise ValueError(f"force kind {force.get('kind')}")
     else:

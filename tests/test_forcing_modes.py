@@ -182,3 +182,19 @@ def test_force_modes_for_para(tmp_path):
     assert k.tolist() == [[1, 1, 1]] and abs(F[0, 0] - 0.1) < 1e-15
     c = config_from_para(read_para(para(1, [2.0, 3.0, 0.1, 0.0]), n_fields=1), "FLUID")
     assert force_modes_for(c) is None
+
+
+def test_para_rb_rotation(lib):
+    from tests.test_field_io import PARA
+    from tarang_b200.para import config_from_para, read_para
+    from tarang_b200.solver import make_config
+    from tarang_b200 import _lib as L
+    t = PARA.format(N1=33, N2=32, N3=32, Ra=1e6, Pr=1.0, basis="SCFT", nu=0, kappa=0, dt=1e-4, S=10, proc=52)
+    t = t.replace("(3)force-float	2.0	3.0	0.1	0.0", "(3)force-float	0.0	0.0	4.0")
+    t = t.replace("(1)force-meta	1	4	1", "(1)force-meta	1	3	1")
+    c = config_from_para(read_para(t, n_fields=2), "RB")
+    assert c["force"] == dict(kind="rb_rotation", omega=(0.0, 0.0, 4.0))
+    kw = dict(c)
+    kw.pop("run")
+    cfg = make_config(**kw)
+    assert cfg.force_kind == L.TG_FORCE_RB_ROTATION and list(cfg.force_para[:3]) == [0.0, 0.0, 4.0]

@@ -127,3 +127,32 @@ def test_rb_scalings_10_steps(lib, pr_switch, u_scaling, grad):
     assert rel_l2([s.get_T()], [t]) < 1e-12
     assert rel_l2(s.get_V(), v) < 1e-11
     assert abs(s.Get_Nusselt_no() - ref.nusselt(v, t)) < 1e-12 * abs(ref.nusselt(v, t))
+
+
+@pytest.mark.parametrize("pr_switch,u_scaling", [("PRLARGE", "ULARGE"), ("PRLARGE", "USMALL"), ("PRSMALL", "USMALL")])
+def test_rb_rotation_10_steps(lib, pr_switch, u_scaling):
+    """Convection with rotation (force_field_proc 52, Compute_force_RB_rotation): the buoyancy of
+    proc 51 plus the Coriolis force V x Omega scaled by the nondimensionalisation."""
+    N = (24, 16, 32)
+    Ra, Pr = 2e3, 0.7
+    om = (0.0, 0.5, 2.0)
+    rng = np.random.default_rng(3)
+    V = [1e-2 * o.dealias(o.forward_scft(rng.standard_normal(N), p), "SCFT") for p in (1, 0, 0)]
+    T = ic.rb_perturbation(N, seed=20261208)
+    s = make(N, physics="RB", Ra=Ra, Pr=Pr, kfactor=KF_RB, dt=1e-4, Pr_switch=pr_switch, RB_Uscaling=u_scaling,
+             force=dict(kind="rb_rotation", omega=om))
+    s.set_V(V)
+    s.set_T(T)
+    s.step(10)
+    ref = o.RBSolver(N, KF_RB, Ra, Pr, 1e-4, pr_switch=pr_switch, u_scaling=u_scaling, omega=om)
+    v, t = V, T
+    for _ in range(10):
+        v, t, dt = ref.step(v, t)
+    assert rel_l2(s.get_V(), v) < 1e-11
+    assert rel_l2([s.get_T()], [t]) < 1e-12
+    # without rotation the trajectory differs
+    ref0 = o.RBSolver(N, KF_RB, Ra, Pr, 1e-4, pr_switch=pr_switch, u_scaling=u_scaling)
+    v0, t0 = V, T
+    for _ in range(10):
+        v0, t0, _ = ref0.step(v0, t0)
+    assert rel_l2(v0, v) > 1e-6

@@ -171,7 +171,8 @@ def test_request_bytes_match_allocation(lib):
         c = dict(cfg)
         N = c.pop("N")
         s = IncFluid(N, **c)
-        s.set_V(fluid_fields(N, 1))      # the upload allocates the dense staging field
+        s.set_V(fluid_fields(N, 1))
+        s.get_V()                        # the whole-array download allocates the dense staging field
         assert s.device_bytes() == request_bytes(cfg, 1), cfg
         s.close()
 
