@@ -297,6 +297,22 @@ int tg_shell_to_shell(tg_ctx* ctx, int kind, double* tr, int n);
  * X< the field inside the sphere and P(N, R>) = sum over |K| > R_s of 2 mult Re(N . R*)
  * (Prod_out_sphere_nlinV / Prod_out_sphere_nlin_vorticity prod_nlinV.cc:62-150).  n >= n_shells + 1. */
 int tg_helicity_flux(tg_ctx* ctx, double* flux, int n);
+/* IncVF::Compute_magnetic_helicity_flux (EnergyTrdir/compute_helicity_flux.cc:94-135), FOUR MHD:
+ * the magnetic helicity flux out of each sphere s = 1 .. n_shells, P(B.grad U<, a>)/2
+ * - P(U.grad B<, a>)/2 + P(U x B<, B>)/2 with a = i K x B / K^2
+ * (Prod_out_sphere_nlin_vector_potential prod_nlinV.cc:154-162, Shell_mult_vector_potential_FOUR
+ * four_ET.cc:905-965; U x B< of EnergyTr_Compute_nlin_UcrossB ET_compute_nlin.cc:317-337).
+ * n >= n_shells + 1. */
+int tg_magnetic_helicity_flux(tg_ctx* ctx, double* flux, int n);
+/* IncVF::Compute_kinetic_helicity_shell_tr (compute_helicity_shell_tr.cc:56-109) and
+ * Compute_magnetic_helicity_shell_tr (:114-172), FOUR: the three terms of the fluxes above with the
+ * giver held to shell n = 1 .. n_shells-1 (R_{n-1} < |K| <= R_n) and the receivers binned by shell
+ * over |K| <= R_in (Shell_mult_all_FOUR, Shell_mult_vorticity_all_FOUR,
+ * Shell_mult_vector_potential_all_FOUR four_ET.cc:181-256, 999-1090, 1094-1190).  tr is n x n
+ * row-major, n >= n_shells + 1.  The reference's K = 0 entry of the vector-potential sum is 0/0;
+ * here a(0) = 0. */
+int tg_helicity_shell_to_shell(tg_ctx* ctx, double* tr, int n);
+int tg_magnetic_helicity_shell_to_shell(tg_ctx* ctx, double* tr, int n);
 /* Get_Nusselt_no (nusselt.cc:53-89), RB only */
 int tg_nusselt(tg_ctx* ctx, double* nusselt);
 /* IncVF::Compute_force_feed_shell (lib/IncFlow/EnergyTrdir/compute_force_feed.cc:70-76, with

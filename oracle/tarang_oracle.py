@@ -1233,6 +1233,87 @@ def krho_inside(N, kfactor, axis, alias="DEALIAS"):
     return int(min((N[p1] // d) * kfactor[p1], (N[p2] // d) * kfactor[p2]))
 
 
+def vector_potential_four(B, kfactor):
+    """a = i K x B / K^2 (the potential Shell_mult_vector_potential four_ET.cc:905-965 pairs
+    with: 2 mult / K^2 Re(N . conj(i K x B))), zero at K = 0."""
+    N = (B[0].shape[0], B[0].shape[1], 2 * (B[0].shape[2] - 1))
+    K2 = ksqr(N, kfactor)
+    W = vorticity_four(B, kfactor)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        return [np.where(K2 > 0, w / K2, 0) for w in W]
+
+
+def et_nlin_cross(V, G, kfactor, basis="FOUR"):
+    """IncVF::EnergyTr_Compute_nlin_UcrossB  ET_compute_nlin.cc:317-337: F(V x G)."""
+    N3 = 2 * (V[0].shape[2] - 1)
+    vr = [inverse(V[i], basis, 0, N3) for i in range(3)]
+    gr = [inverse(G[i], basis, 0, N3) for i in range(3)]
+    return [forward(vr[1] * gr[2] - vr[2] * gr[1], basis, 0), forward(vr[2] * gr[0] - vr[0] * gr[2], basis, 0),
+            forward(vr[0] * gr[1] - vr[1] * gr[0], basis, 0)]
+
+
+def magnetic_helicity_flux(U, B, kfactor, no_shells, alias="DEALIAS"):
+    """IncVF::Compute_magnetic_helicity_flux  compute_helicity_flux.cc:94-135 (FOUR): for
+    sphere s, flux(s) = P(N(B, U<), a)/2 - P(N(U, B<), a)/2 + P(F(U x B<), B)/2, with
+    a = i K x B / K^2, X< = X on 0 < |K| <= R_s, P(N, R) = sum_{|K| > R_s} 2 mult Re(N . R*)."""
+    N = (U[0].shape[0], U[0].shape[1], 2 * (U[0].shape[2] - 1))
+    R = et_radii(N, kfactor, no_shells, alias)
+    K = kmag(N, kfactor)
+    mult = multiplicity_four(N)
+    A = vector_potential_four(B, kfactor)
+    out = np.zeros(no_shells + 1)
+
+    def P(nl, Rf, r):
+        return float(np.sum((2 * mult * sum(np.real(x * np.conj(y)) for x, y in zip(nl, Rf)))[K > r]))
+
+    for s_ in range(1, no_shells + 1):
+        r = R[s_]
+        inside = (K > 0) & (K <= r)
+        U_in = [np.where(inside, v, 0) for v in U]
+        B_in = [np.where(inside, b, 0) for b in B]
+        out[s_] = (P(et_nlin(B, U_in, kfactor), A, r) / 2 - P(et_nlin(U, B_in, kfactor), A, r) / 2
+                   + P(et_nlin_cross(U, B_in, kfactor), B, r) / 2)
+    return out
+
+
+def kinetic_helicity_shell_tr(V, kfactor, no_shells, alias="DEALIAS"):
+    """IncVF::Compute_kinetic_helicity_shell_tr  compute_helicity_shell_tr.cc:56-109 (FOUR): row n
+    (giver shell R_{n-1} < |K| <= R_n, n = 1 .. no_shells-1) = -Sv(N(U, U^(n)), U)/2
+    - Sa(N(U, omega^(n)), U)/2 + Sa(N(omega, U^(n)), U)/2, where Sa(N, R) bins
+    2 mult Re(N . R*) by Get_shell_index over |K| <= R_in (Shell_mult_all_FOUR four_ET.cc:181-256)
+    and Sv(N, U) = Sa(N, i K x U) (Shell_mult_vorticity_all_FOUR four_ET.cc:999-1090)."""
+    N = (V[0].shape[0], V[0].shape[1], 2 * (V[0].shape[2] - 1))
+    R = et_radii(N, kfactor, no_shells, alias)
+    W = vorticity_four(V, kfactor)
+    T = np.zeros((no_shells + 1, no_shells + 1))
+    for n_ in range(1, no_shells):
+        G = [fill_array_shell(f, R[n_ - 1], R[n_], kfactor) for f in V]
+        Gw = [fill_array_shell(f, R[n_ - 1], R[n_], kfactor) for f in W]
+        T[n_, :] = (-shell_mult_all(et_nlin(V, G, kfactor), W, R, kfactor, alias) / 2
+                    - shell_mult_all(et_nlin(V, Gw, kfactor), V, R, kfactor, alias) / 2
+                    + shell_mult_all(et_nlin(W, G, kfactor), V, R, kfactor, alias) / 2)
+    return T
+
+
+def magnetic_helicity_shell_tr(U, B, kfactor, no_shells, alias="DEALIAS"):
+    """IncVF::Compute_magnetic_helicity_shell_tr  compute_helicity_shell_tr.cc:114-172 (FOUR): row n
+    = Sp(N(B, U^(n)), B)/2 - Sp(N(U, B^(n)), B)/2 + Sa(F(U x B^(n)), B)/2 with
+    Sp(N, B) = Sa(N, a), a = i K x B / K^2 (Shell_mult_vector_potential_all_FOUR
+    four_ET.cc:1094-1190).  At K = 0 the reference divides 0 by |K|^2 = 0; the oracle takes a = 0
+    there, so column 0 holds the U x B< term alone."""
+    N = (U[0].shape[0], U[0].shape[1], 2 * (U[0].shape[2] - 1))
+    R = et_radii(N, kfactor, no_shells, alias)
+    A = vector_potential_four(B, kfactor)
+    T = np.zeros((no_shells + 1, no_shells + 1))
+    for n_ in range(1, no_shells):
+        Gu = [fill_array_shell(f, R[n_ - 1], R[n_], kfactor) for f in U]
+        Gb = [fill_array_shell(f, R[n_ - 1], R[n_], kfactor) for f in B]
+        T[n_, :] = (shell_mult_all(et_nlin(B, Gu, kfactor), A, R, kfactor, alias) / 2
+                    - shell_mult_all(et_nlin(U, Gb, kfactor), A, R, kfactor, alias) / 2
+                    + shell_mult_all(et_nlin_cross(U, Gb, kfactor), B, R, kfactor, alias) / 2)
+    return T
+
+
 def ring_radii(N, kfactor, n_ring_shells, alias="DEALIAS", basis="FOUR", Rin=None):
     """EnergyTr::EnergyTr ring shell radii, scheme 0  EnergyTr.cc:190-210 (cylinder shells
     :300-320 with Rin = Anis_max_Krho_radius_inside)."""

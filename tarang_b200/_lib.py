@@ -179,6 +179,9 @@ SIGNATURES = {
     "tg_ring_spectrum_helicity": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, _DP, C.c_int]),
     "tg_cylinder_ring_spectrum_helicity": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, _DP, C.c_int]),
     "tg_helicity_flux": (C.c_int, [_VP, _DP, C.c_int]),
+    "tg_magnetic_helicity_flux": (C.c_int, [_VP, _DP, C.c_int]),
+    "tg_helicity_shell_to_shell": (C.c_int, [_VP, _DP, C.c_int]),
+    "tg_magnetic_helicity_shell_to_shell": (C.c_int, [_VP, _DP, C.c_int]),
     "tg_ring_to_ring": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, C.c_int, _DP, C.c_int]),
     "tg_cylinder_radii": (C.c_int, [_VP, C.c_int, C.c_int, _DP, C.c_int]),
     "tg_cylinder_ring_to_ring": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, C.c_int, _DP, C.c_int]),

@@ -139,6 +139,7 @@ struct ContractArgs {
   int nrec;
   Radii rad;
   double* hist;           // [nrec][S+1]
+  int cross;              // 1: N = F(H x G) (EnergyTr_Compute_nlin_UcrossB) instead of D_j F(H_j G_i)
 };
 
 // N_i = i k_j P(i, j); hist[r][shell(|K|)] += 2 mult Re(sum_i N_i conj(R_i))
@@ -160,13 +161,21 @@ __global__ void __launch_bounds__(TPB) k_et_contract(ContractArgs a) {
     int bin = 0;  // receiver annulus: first rho >= |K|
     while (bin < a.rad.S && K > a.rad.r[bin]) ++bin;
     cx<double> N[3];
+    if (a.cross) {
+      // (H x G)_i from P(i, j) = F(H_j G_i): x = P(2,1) - P(1,2), y = P(0,2) - P(2,0), z = P(1,0) - P(0,1)
+      auto P = [&](int i, int j) { return cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + j])[idx]); };
+      N[0] = P(2, 1) - P(1, 2);
+      N[1] = P(0, 2) - P(2, 0);
+      N[2] = P(1, 0) - P(0, 1);
+    } else {
 #pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      const cx<double> p0 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 0])[idx]);
-      const cx<double> p1 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 1])[idx]);
-      const cx<double> p2 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 2])[idx]);
-      const cx<double> s = mkc<double>(kx * p0.x + ky * p1.x + kz * p2.x, kx * p0.y + ky * p1.y + kz * p2.y);
-      N[i] = ione(s);
+      for (int i = 0; i < 3; ++i) {
+        const cx<double> p0 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 0])[idx]);
+        const cx<double> p1 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 1])[idx]);
+        const cx<double> p2 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 2])[idx]);
+        const cx<double> s = mkc<double>(kx * p0.x + ky * p1.x + kz * p2.x, kx * p0.y + ky * p1.y + kz * p2.y);
+        N[i] = ione(s);
+      }
     }
     const double m = mult_four(l1, l2, l3, g.N1, g.N2);
     for (int r = 0; r < a.nrec; ++r) {
@@ -217,7 +226,7 @@ std::vector<double> et_annuli(const tg_ctx* c) {
 // a = 0..A, receivers r of the given (H, F) pair
 int et_tables_ptr(tg_ctx* c, const cx<double>* const* Hp, const cx<double>* const* Fp,
                   const cx<double>* const (*Rp)[3], int nrec, const std::vector<double>& rho,
-                  std::vector<double>& T);
+                  std::vector<double>& T, int cross = 0);
 
 int et_tables(tg_ctx* c, int Hg, int Fg, const int* Rg, int nrec, const std::vector<double>& rho,
               std::vector<double>& T) {
@@ -232,7 +241,7 @@ int et_tables(tg_ctx* c, int Hg, int Fg, const int* Rg, int nrec, const std::vec
 // T[r][g][a] for helper fields Hp, giver fields Fp and receivers Rp (any compact FP64 fields)
 int et_tables_ptr(tg_ctx* c, const cx<double>* const* Hp, const cx<double>* const* Fp,
                   const cx<double>* const (*Rp)[3], int nrec, const std::vector<double>& rho,
-                  std::vector<double>& T) {
+                  std::vector<double>& T, int cross) {
   const int A = (int)rho.size() - 1;
   if (A < 1 || A > kMaxShells) return set_err(c, TG_ERR_ARG, "energy transfer needs 6 <= n_shells <= 63");
   int rc = ensure_et_buffers(c);
@@ -275,6 +284,7 @@ int et_tables_ptr(tg_ctx* c, const cx<double>* const* Hp, const cx<double>* cons
       for (int i = 0; i < 3; ++i) a.R[r][i] = Rp[r][i];
     a.nrec = nrec;
     a.rad = rad;
+    a.cross = cross;
     a.hist = c->diag + (size_t)n * nrec * nb;  // layout [g][r][a]
     {
       ProfScope pr(c, "et_contract", 0.0);
@@ -384,6 +394,23 @@ __global__ void k_vorticity(Geo g, const cx<double>* V0, const cx<double>* V1, c
   W2[idx] = ione(kx * b - ky * a);
 }
 
+// a = i K x B / K^2 (zero at K = 0): the potential Shell_mult_vector_potential pairs with
+// (four_ET.cc:905-965)
+__global__ void k_vector_potential(Geo g, const cx<double>* B0, const cx<double>* B1, const cx<double>* B2,
+                                   cx<double>* A0, cx<double>* A1, cx<double>* A2) {
+  const long long idx = (long long)blockIdx.x * TPB + threadIdx.x;
+  if (idx >= g.S) return;
+  int r1, r2, l3;
+  compact_mode(g, idx, r1, r2, l3);
+  const double kx = geo_kx(g, r1) * g.kf0, ky = geo_ky(g, r2) * g.kf1, kz = l3 * g.kf2;
+  const double K2 = kx * kx + ky * ky + kz * kz;
+  const double w = K2 > 0 ? 1.0 / K2 : 0.0;
+  const cx<double> a = B0[idx], b = B1[idx], d = B2[idx];
+  A0[idx] = w * ione(ky * d - kz * b);
+  A1[idx] = w * ione(kz * a - kx * d);
+  A2[idx] = w * ione(kx * b - ky * a);
+}
+
 // Force feed per shell (Compute_force_feed_shell compute_force_feed.cc:70-76 with
 // Shell_mult_all_FOUR four_ET.cc:181-226): for |K| <= R_in, result[i] += 2 mult Re(F . V*),
 // i = Get_shell_index(|K|).  The force is nonzero on its box only; thread i sums shell i over
@@ -421,6 +448,111 @@ __global__ void k_force_feed(Geo g, const cx<double>* __restrict__ FB, int fx, i
   }
   out[i] = acc;
 }
+// Rows n = 1 .. S-1 of a shell-to-shell table (compute_shell_tr.cc: shell_from_index <
+// no_shells) from a giver-annulus x receiver-annulus table T; receivers |K| <= R_in go to column
+// Get_shell_index (first i with R[i] >= |K|), which is constant on an annulus.  tr is n x n.
+void shell_rows(const std::vector<double>& R, const std::vector<double>& rho, const std::vector<double>& T,
+                double sign, int S, double* tr, int n) {
+  const int A = (int)rho.size() - 1, nb = A + 1;
+  const double Rin = R[S - 1];
+  std::vector<int> bin(nb, S);
+  for (int a = 0; a <= A; ++a) {
+    int i = 0;
+    while (i <= S && !(rho[a] <= R[i])) ++i;
+    bin[a] = i;
+  }
+  for (int i = 0; i < n * n; ++i) tr[i] = 0;
+  for (int sh = 1; sh < S; ++sh) {
+    const double lo = R[sh - 1], hi = R[sh];
+    for (int g = 1; g <= A; ++g) {
+      if (!(rho[g - 1] >= lo && rho[g] <= hi)) continue;
+      for (int a = 0; a <= A; ++a) {
+        if (rho[a] > Rin || bin[a] >= n) continue;
+        tr[(size_t)sh * n + bin[a]] += sign * T[(size_t)g * nb + a];
+      }
+    }
+  }
+}
+
+// Giver-annulus x receiver-annulus table of a helicity transfer, the three terms combined.
+// Kinetic (IncVF::Compute_kinetic_helicity_flux compute_helicity_flux.cc:52-86 and
+// Compute_kinetic_helicity_shell_tr compute_helicity_shell_tr.cc:56-109):
+//   -(U.grad U<).omega/2 - (U.grad omega<).U/2 + (omega.grad U<).U/2, omega = i K x U.
+// Magnetic (Compute_magnetic_helicity_flux compute_helicity_flux.cc:94-135 and
+// Compute_magnetic_helicity_shell_tr compute_helicity_shell_tr.cc:114-172):
+//   (B.grad U<).a/2 - (U.grad B<).a/2 + (U x B<).B/2, a = i K x B / K^2
+// (Shell_mult_vector_potential_FOUR four_ET.cc:905-965; U x B< of EnergyTr_Compute_nlin_UcrossB
+// ET_compute_nlin.cc:317-337).  At K = 0 the reference divides 0 by |K|^2 = 0 in the shell
+// table; a is taken as 0 there.
+int helicity_table(tg_ctx* c, int magnetic, const std::vector<double>& rho, std::vector<double>& Tc) {
+  if (c->basis != TG_FOUR) return set_err(c, TG_ERR_UNSUPPORTED, "helicity transfer is built for the FOUR basis");
+  if (magnetic && c->phys != TG_MHD) return set_err(c, TG_ERR_ARG, "magnetic helicity transfer needs MHD");
+  int rc = ensure_et_buffers(c);
+  for (int i = 0; i < 3 && !rc; ++i) rc = own_field(c, &c->etVort[i]);
+  if (rc) return rc;
+  const Geo& g = c->g;
+  const int grid = (int)((g.S + TPB - 1) / TPB);
+  const cx<double>* U[3] = {c->U0[0], c->U0[1], c->U0[2]};
+  const cx<double>* W[3] = {c->etVort[0], c->etVort[1], c->etVort[2]};
+  std::vector<double> T1, T2, T3;
+  if (!magnetic) {
+    k_vorticity<<<grid, TPB, 0, c->st>>>(g, U[0], U[1], U[2], c->etVort[0], c->etVort[1], c->etVort[2]);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_err(c, e, "vorticity");
+    const cx<double>* RW[1][3] = {{W[0], W[1], W[2]}};
+    const cx<double>* RU[1][3] = {{U[0], U[1], U[2]}};
+    rc = et_tables_ptr(c, U, U, RW, 1, rho, T1);              // U.grad U<  against omega
+    if (!rc) rc = et_tables_ptr(c, U, W, RU, 1, rho, T2);     // U.grad omega< against U
+    if (!rc) rc = et_tables_ptr(c, W, U, RU, 1, rho, T3);     // omega.grad U< against U
+  } else {
+    const cx<double>* B[3] = {c->U0[3], c->U0[4], c->U0[5]};
+    k_vector_potential<<<grid, TPB, 0, c->st>>>(g, B[0], B[1], B[2], c->etVort[0], c->etVort[1], c->etVort[2]);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_err(c, e, "vector potential");
+    const cx<double>* RA[1][3] = {{W[0], W[1], W[2]}};
+    const cx<double>* RB[1][3] = {{B[0], B[1], B[2]}};
+    rc = et_tables_ptr(c, B, U, RA, 1, rho, T1);              // B.grad U< against a
+    if (!rc) rc = et_tables_ptr(c, U, B, RA, 1, rho, T2);     // U.grad B< against a
+    if (!rc) rc = et_tables_ptr(c, U, B, RB, 1, rho, T3, 1);  // U x B< against B
+  }
+  if (rc) return rc;
+  const double s1 = magnetic ? 0.5 : -0.5;
+  Tc.assign(T1.size(), 0.0);
+  for (size_t q = 0; q < Tc.size(); ++q) Tc[q] = s1 * T1[q] - 0.5 * T2[q] + 0.5 * T3[q];
+  return TG_OK;
+}
+
+// Sphere fluxes (giver annuli inside R_s, receivers outside; Prod_out_sphere_* prod_nlinV.cc:62-162;
+// out has n >= S+1 entries) or the n x n shell-to-shell table (giver rows 1 .. S-1, receivers binned by Get_shell_index over
+// |K| <= R_in; Shell_mult_*_all four_ET.cc:181-256, 999-1090, 1094-1190) of a helicity table.
+int helicity_out(tg_ctx* c, int magnetic, int shells, double* out, int n) {
+  if (!c || !out) return TG_ERR_ARG;
+  const int S = c->cfg.n_shells;
+  if (S < 6 || n < S + 1) return TG_ERR_ARG;
+  cudaSetDevice(c->dev);
+  const std::vector<double> rho = et_annuli(c);
+  std::vector<double> T;
+  const int rc = helicity_table(c, magnetic, rho, T);
+  if (rc) return rc;
+  const std::vector<double> R = et_radii(c);
+  if (shells) {
+    shell_rows(R, rho, T, 1.0, S, out, n);
+    return TG_OK;
+  }
+  const int A = (int)rho.size() - 1, nb = A + 1;
+  for (int s = 0; s < n; ++s) out[s] = 0;
+  for (int s = 1; s <= S; ++s) {
+    double acc = 0;
+    for (int gg = 1; gg <= A; ++gg) {
+      if (rho[gg] > R[s]) continue;
+      for (int a = 1; a <= A; ++a)
+        if (rho[a - 1] >= R[s]) acc += T[(size_t)gg * nb + a];
+    }
+    out[s] = acc;
+  }
+  return TG_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -465,53 +597,13 @@ int tg_flux(tg_ctx* c, int kind, double* flux, int n) {
 // P(N, R>) = sum over |K| > R_s of 2 mult Re(N . R*) (Prod_out_sphere_nlinV,
 // Prod_out_sphere_nlin_vorticity prod_nlinV.cc:62-150) and X< = X on 0 < |K| <= R_s
 // (Fill_in_sphere, Fill_in_sphere_vorticity fill_sphere_shell.cc:57-210).
-int tg_helicity_flux(tg_ctx* c, double* flux, int n) {
-  if (!c || !flux) return TG_ERR_ARG;
-  const int S = c->cfg.n_shells;
-  if (S < 6 || n < S + 1) return TG_ERR_ARG;
-  if (c->basis != TG_FOUR) return set_err(c, TG_ERR_UNSUPPORTED, "helicity flux is built for the FOUR basis");
-  cudaSetDevice(c->dev);
-  int rc = ensure_et_buffers(c);
-  if (rc) return rc;
-  const Geo& g = c->g;
-  if (!c->etVort[0]) {
-    for (int i = 0; i < 3; ++i) {
-      rc = dalloc_ctx(c, (void**)&c->etVort[i], sizeof(cx<double>) * (size_t)g.S);
-      if (rc) return rc;
-      c->et_own[c->n_et_own++] = c->etVort[i];
-    }
-  }
-  k_vorticity<<<(int)((g.S + TPB - 1) / TPB), TPB, 0, c->st>>>(g, c->U0[0], c->U0[1], c->U0[2], c->etVort[0],
-                                                               c->etVort[1], c->etVort[2]);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return cuda_err(c, e, "vorticity");
-  const cx<double>* U[3] = {c->U0[0], c->U0[1], c->U0[2]};
-  const cx<double>* W[3] = {c->etVort[0], c->etVort[1], c->etVort[2]};
-  const cx<double>* RW[1][3] = {{W[0], W[1], W[2]}};
-  const cx<double>* RU[1][3] = {{U[0], U[1], U[2]}};
-  const std::vector<double> rho = et_annuli(c);
-  std::vector<double> T1, T2, T3;
-  rc = et_tables_ptr(c, U, U, RW, 1, rho, T1);       // U.grad U<  against omega
-  if (!rc) rc = et_tables_ptr(c, U, W, RU, 1, rho, T2);  // U.grad omega< against U
-  if (!rc) rc = et_tables_ptr(c, W, U, RU, 1, rho, T3);  // omega.grad U< against U
-  if (rc) return rc;
-  const std::vector<double> R = et_radii(c);
-  const int A = (int)rho.size() - 1, nb = A + 1;
-  for (int s = 0; s < n; ++s) flux[s] = 0;
-  for (int s = 1; s <= S; ++s) {
-    double acc = 0;
-    for (int gg = 1; gg <= A; ++gg) {
-      if (rho[gg] > R[s]) continue;
-      for (int a = 1; a <= A; ++a)
-        if (rho[a - 1] >= R[s]) {
-          const size_t q = (size_t)gg * nb + a;
-          acc += -0.5 * T1[q] - 0.5 * T2[q] + 0.5 * T3[q];
-        }
-    }
-    flux[s] = acc;
-  }
-  return TG_OK;
-}
+int tg_helicity_flux(tg_ctx* c, double* flux, int n) { return helicity_out(c, 0, 0, flux, n); }
+
+int tg_magnetic_helicity_flux(tg_ctx* c, double* flux, int n) { return helicity_out(c, 1, 0, flux, n); }
+
+int tg_helicity_shell_to_shell(tg_ctx* c, double* tr, int n) { return helicity_out(c, 0, 1, tr, n); }
+
+int tg_magnetic_helicity_shell_to_shell(tg_ctx* c, double* tr, int n) { return helicity_out(c, 1, 1, tr, n); }
 
 int tg_shell_to_shell(tg_ctx* c, int kind, double* tr, int n) {
   if (!c || !tr) return TG_ERR_ARG;
@@ -522,28 +614,7 @@ int tg_shell_to_shell(tg_ctx* c, int kind, double* tr, int n) {
   double sign = 1;
   int rc = et_table_kind(c, kind, T, rho, sign);
   if (rc) return rc;
-  const std::vector<double> R = et_radii(c);
-  const int A = (int)rho.size() - 1, nb = A + 1;
-  const double Rin = R[S - 1];
-  // receiver bin of an annulus: Get_shell_index (first i with R[i] >= |K|) is constant on it
-  std::vector<int> bin(nb, S);
-  for (int a = 0; a <= A; ++a) {
-    int i = 0;
-    while (i <= S && !(rho[a] <= R[i])) ++i;
-    bin[a] = i;
-  }
-  for (int i = 0; i < n * n; ++i) tr[i] = 0;
-  // rows n = 1..S-1 (compute_shell_tr.cc: shell_from_index < no_shells), receivers |K| <= R_in
-  for (int sh = 1; sh < S; ++sh) {
-    const double lo = R[sh - 1], hi = R[sh];
-    for (int g = 1; g <= A; ++g) {
-      if (!(rho[g - 1] >= lo && rho[g] <= hi)) continue;
-      for (int a = 0; a <= A; ++a) {
-        if (rho[a] > Rin || bin[a] >= n) continue;
-        tr[(size_t)sh * n + bin[a]] += sign * T[(size_t)g * nb + a];
-      }
-    }
-  }
+  shell_rows(et_radii(c), rho, T, sign, S, tr, n);
   return TG_OK;
 }
 

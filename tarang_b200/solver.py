@@ -394,6 +394,30 @@ class IncFluid:
         self._ck(self.lib.tg_helicity_flux(self.h, _dptr(out), out.size), "helicity flux")
         return out
 
+    def Compute_magnetic_helicity_flux(self):
+        """IncVF::Compute_magnetic_helicity_flux (tg_magnetic_helicity_flux), MHD: W.flux_hk,
+        n_shells + 1 entries."""
+        S = self.cfg.n_shells
+        out = np.zeros(S + 1)
+        self._ck(self.lib.tg_magnetic_helicity_flux(self.h, _dptr(out), out.size), "magnetic helicity flux")
+        return out
+
+    def Compute_kinetic_helicity_shell_tr(self):
+        """IncVF::Compute_kinetic_helicity_shell_tr (tg_helicity_shell_to_shell): shelltoshell_hk,
+        (n_shells + 1) x (n_shells + 1)."""
+        S = self.cfg.n_shells
+        t = np.zeros((S + 1) * (S + 1))
+        self._ck(self.lib.tg_helicity_shell_to_shell(self.h, _dptr(t), S + 1), "helicity shell_tr")
+        return t.reshape(S + 1, S + 1)
+
+    def Compute_magnetic_helicity_shell_tr(self):
+        """IncVF::Compute_magnetic_helicity_shell_tr (tg_magnetic_helicity_shell_to_shell), MHD:
+        W.shelltoshell_hk, (n_shells + 1) x (n_shells + 1)."""
+        S = self.cfg.n_shells
+        t = np.zeros((S + 1) * (S + 1))
+        self._ck(self.lib.tg_magnetic_helicity_shell_to_shell(self.h, _dptr(t), S + 1), "magnetic helicity shell_tr")
+        return t.reshape(S + 1, S + 1)
+
     def Compute_ring_tr(self, n_ring_shells, n_sectors, axis=1, kind=L.TG_ET_UU):
         """IncVF::Compute_ring_tr (tg_ring_to_ring): T[i, j, m, s], the transfer from giver
         ring (shell i, sector j) to receiver ring (m, s); kind TG_ET_UU, or for MHD TG_ET_BB,
