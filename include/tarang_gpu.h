@@ -268,8 +268,10 @@ int tg_cylinder_ring_spectrum(tg_ctx* ctx, int group, int axis, int n_slabs, dou
  * four/four_ET.cc:330-386), FOUR: tr[i][j][m][s], (n_ring_shells+1) x (n_sectors+1) x
  * (n_ring_shells+1) x (n_sectors+1) doubles, is the transfer from giver ring (shell i =
  * 1..n_ring_shells-1, sector j = 1..n_sectors) to receiver ring (m, s).  kind TG_ET_UU
- * (ring_to_ring_self), and for MHD TG_ET_BB (W.ring_to_ring_self) and TG_ET_UB
- * (ring_to_ring_VF, U to B).  Ring radii: scheme 0 (EnergyTr.cc:190-210; tg_ring_radii), 5 <=
+ * (ring_to_ring_self), for MHD TG_ET_BB (W.ring_to_ring_self), TG_ET_UB (ring_to_ring_VF, U to
+ * B), TG_ET_ZP and TG_ET_ZM (ring_to_ring_Elsasser, W.ring_to_ring_Elsasser;
+ * compute_ring_tr.cc:226-285), and for a passive scalar TG_ET_TT (ring_to_ring_SF,
+ * Compute_ring_tr_scalar :104-131).  TG_ET_BU has no ring table in the reference (TG_ERR_ARG).  Ring radii: scheme 0 (EnergyTr.cc:190-210; tg_ring_radii), 5 <=
  * n_ring_shells <= 32; sectors of equal angle up to pi/2 about `axis`.  As in the reference, a
  * giver ring holds only the modes with theta <= pi/2 (K_par >= 0), while receivers fold theta. */
 int tg_ring_radii(tg_ctx* ctx, int n_ring_shells, double* radii, int n);

@@ -171,4 +171,8 @@ int radius_inside(const tg_ctx* c);
 int ensure_diag(tg_ctx* c, size_t need);
 // energy-transfer buffers (giver fields etG, helper transforms etWY, products etPP/PY/PX)
 int ensure_et_buffers(tg_ctx* c);
+// helper, giver and receiver fields of an energy-transfer kind (TG_ET_*) and its sign; Elsasser
+// kinds fill scratch fields first (tg_et.cu)
+int et_kind_fields(tg_ctx* c, int kind, const cx<double>* H[3], const cx<double>* F[3], const cx<double>* R[3],
+                   double& sign);
 }  // namespace tg

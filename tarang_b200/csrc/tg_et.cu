@@ -228,16 +228,6 @@ int et_tables_ptr(tg_ctx* c, const cx<double>* const* Hp, const cx<double>* cons
                   const cx<double>* const (*Rp)[3], int nrec, const std::vector<double>& rho,
                   std::vector<double>& T, int cross = 0);
 
-int et_tables(tg_ctx* c, int Hg, int Fg, const int* Rg, int nrec, const std::vector<double>& rho,
-              std::vector<double>& T) {
-  const cx<double>* Hp[3] = {c->U0[3 * Hg], c->U0[3 * Hg + 1], c->U0[3 * Hg + 2]};
-  const cx<double>* Fp[3] = {c->U0[3 * Fg], c->U0[3 * Fg + 1], c->U0[3 * Fg + 2]};
-  const cx<double>* Rp[2][3];
-  for (int r = 0; r < nrec && r < 2; ++r)
-    for (int i = 0; i < 3; ++i) Rp[r][i] = c->U0[3 * Rg[r] + i];
-  return et_tables_ptr(c, Hp, Fp, Rp, nrec, rho, T);
-}
-
 // T[r][g][a] for helper fields Hp, giver fields Fp and receivers Rp (any compact FP64 fields)
 int et_tables_ptr(tg_ctx* c, const cx<double>* const* Hp, const cx<double>* const* Fp,
                   const cx<double>* const (*Rp)[3], int nrec, const std::vector<double>& rho,
@@ -331,28 +321,34 @@ int own_field(tg_ctx* c, cx<double>** f) {
   return TG_OK;
 }
 
-int et_table_kind(tg_ctx* c, int kind, std::vector<double>& T, std::vector<double>& rho, double& sign) {
-  if (c->basis != TG_FOUR) return set_err(c, TG_ERR_UNSUPPORTED, "energy transfer is built for the FOUR basis");
+}  // namespace
+
+namespace tg {
+
+// The helper H, giver F and receiver R of an energy-transfer kind, and its sign.
+//   U->U, B->B, U->B, B->U: the state fields (kind_spec).
+//   T->T (Compute_flux_scalar / Compute_shell_tr_scalar compute_flux.cc:82-95,
+//   compute_shell_tr.cc:93-109; Compute_ring_tr_scalar compute_ring_tr.cc:104-131): G = T<,
+//   N = D_j F(U_j T<) against T, sign -1, run as the vector form with giver and receiver (T, 0, 0).
+//   Z+->Z+, Z-->Z- (flux_Elsasser / shelltoshell_Elsasser compute_flux.cc:228-255,
+//   compute_shell_tr.cc:201-246, ring_to_ring_Elsasser compute_ring_tr.cc:240-285): Z+ = U + B,
+//   Z- = U - B written to scratch fields, G = Z+<, N = D_j F(Z-_j G_i) against Z+ (and with + and -
+//   exchanged), sign -1.
+int et_kind_fields(tg_ctx* c, int kind, const cx<double>* H[3], const cx<double>* F[3], const cx<double>* R[3],
+                   double& sign) {
   if (kind == TG_ET_TT) {
-    // Compute_flux_scalar / Compute_shell_tr_scalar (compute_flux.cc:82-95,
-    // compute_shell_tr.cc:93-109): G = T<, N = D_j F(U_j T<) against T, sign -1; run as the
-    // vector form with the giver and receiver (T, 0, 0)
     if (c->phys != TG_SCALAR && c->phys != TG_RB) return set_err(c, TG_ERR_ARG, "scalar transfer needs a scalar");
-    int rc = ensure_et_buffers(c);
-    if (!rc) rc = own_field(c, &c->etZero);
+    const int rc = own_field(c, &c->etZero);
     if (rc) return rc;
     sign = -1.0;
-    rho = et_annuli(c);
-    const cx<double>* H[3] = {c->U0[0], c->U0[1], c->U0[2]};
-    const cx<double>* F[3] = {c->U0[3], c->etZero, c->etZero};
-    const cx<double>* R[1][3] = {{c->U0[3], c->etZero, c->etZero}};
-    return et_tables_ptr(c, H, F, R, 1, rho, T);
+    for (int i = 0; i < 3; ++i) H[i] = c->U0[i];
+    F[0] = R[0] = c->U0[3];
+    F[1] = F[2] = R[1] = R[2] = c->etZero;
+    return TG_OK;
   }
   if (kind == TG_ET_ZP || kind == TG_ET_ZM) {
-    // flux_Elsasser / shelltoshell_Elsasser (compute_flux.cc:228-255, compute_shell_tr.cc:201-246):
-    // Z+: G = Z+<, N = D_j F(Z-_j G_i) against Z+; Z-: with + and - exchanged; sign -1
     if (c->phys != TG_MHD) return set_err(c, TG_ERR_ARG, "Elsasser transfers need MHD");
-    int rc = ensure_et_buffers(c);
+    int rc = TG_OK;
     for (int i = 0; i < 6 && !rc; ++i) rc = own_field(c, &c->etZ[i]);
     if (rc) return rc;
     PtrPair6 p{};
@@ -361,22 +357,42 @@ int et_table_kind(tg_ctx* c, int kind, std::vector<double>& T, std::vector<doubl
       p.out[i] = c->etZ[i];
     }
     k_elsasser<<<(int)((c->g.S + TPB - 1) / TPB), TPB, 0, c->st>>>(c->g, p);
-    cudaError_t e = cudaGetLastError();
+    const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_err(c, e, "elsasser");
     sign = -1.0;
-    rho = et_annuli(c);
     const int a = (kind == TG_ET_ZP) ? 0 : 3, b = 3 - a;
-    const cx<double>* H[3] = {c->etZ[b], c->etZ[b + 1], c->etZ[b + 2]};
-    const cx<double>* F[3] = {c->etZ[a], c->etZ[a + 1], c->etZ[a + 2]};
-    const cx<double>* R[1][3] = {{F[0], F[1], F[2]}};
-    return et_tables_ptr(c, H, F, R, 1, rho, T);
+    for (int i = 0; i < 3; ++i) {
+      H[i] = c->etZ[b + i];
+      F[i] = R[i] = c->etZ[a + i];
+    }
+    return TG_OK;
   }
   KindSpec k{};
   if (!kind_spec(c, kind, k)) return set_err(c, TG_ERR_ARG, "energy-transfer kind not available for this physics");
   sign = k.sign;
+  for (int i = 0; i < 3; ++i) {
+    H[i] = c->U0[3 * k.H + i];
+    F[i] = c->U0[3 * k.F + i];
+    R[i] = c->U0[3 * k.R + i];
+  }
+  return TG_OK;
+}
+
+}  // namespace tg
+
+namespace {
+
+int et_table_kind(tg_ctx* c, int kind, std::vector<double>& T, std::vector<double>& rho, double& sign) {
+  if (c->basis != TG_FOUR) return set_err(c, TG_ERR_UNSUPPORTED, "energy transfer is built for the FOUR basis");
+  int rc = ensure_et_buffers(c);
+  if (rc) return rc;
+  const cx<double>* H[3];
+  const cx<double>* F[3];
+  const cx<double>* R[1][3];
+  rc = et_kind_fields(c, kind, H, F, R[0], sign);
+  if (rc) return rc;
   rho = et_annuli(c);
-  int Rg[1] = {k.R};
-  return et_tables(c, k.H, k.F, Rg, 1, rho, T);
+  return et_tables_ptr(c, H, F, R, 1, rho, T);
 }
 
 

@@ -232,7 +232,8 @@ int run_ring(tg_ctx* c, int group, int axis, int n, int cyl, double* ek1, double
 }
 
 // ---------------------------------------------------------------------------------- ring-to-ring
-// IncVF::Compute_ring_tr (EnergyTrdir/compute_ring_tr.cc:60-90, MHD kinds :174-215): for every
+// IncVF::Compute_ring_tr (EnergyTrdir/compute_ring_tr.cc:60-90, scalar :104-131, MHD and Elsasser
+// kinds :174-285; cylinders compute_cylin_ring_tr.cc:54-330): for every
 // giver ring (ring shell i = 1 .. n-1, sector j = 1 .. n_sectors) G = F on that ring (Fill_ring
 // fill_ring.cc:70-90, Fill_array_ring universal_ET.cc:70-100), N = D_j F(H_j G_i)
 // (EnergyTr_Compute_nlin) and T[i][j][shell][sector] = sign * sum 2 mult Re(N . R*) over the
@@ -395,17 +396,19 @@ int run_ring_tr(tg_ctx* c, int kind, int axis, int n_ring_shells, int n_sectors,
   if (c->basis != TG_FOUR) return set_err(c, TG_ERR_UNSUPPORTED, "ring transfers: FOUR basis only");
   if (axis < 1 || axis > 3 || n_sectors < 1 || n_sectors > TG_RING_MAX_SECTORS) return TG_ERR_ARG;
   if (n_ring_shells < 5 || n_ring_shells > kMaxRingShells) return TG_ERR_ARG;
-  // (H, F, receiver, sign): U->U ring_to_ring_self, B->B W.ring_to_ring_self, U->B ring_to_ring_VF
-  int H, F, R;
-  double sign;
-  if (kind == TG_ET_UU) { H = 0; F = 0; R = 0; sign = -1.0; }
-  else if (kind == TG_ET_BB && c->phys == TG_MHD) { H = 0; F = 1; R = 1; sign = -1.0; }
-  else if (kind == TG_ET_UB && c->phys == TG_MHD) { H = 1; F = 0; R = 1; sign = 1.0; }
-  else return set_err(c, TG_ERR_ARG, "ring transfer kind not available for this physics");
+  // U->U ring_to_ring_self, B->B W.ring_to_ring_self, U->B ring_to_ring_VF, Z+->Z+ and Z-->Z-
+  // ring_to_ring_Elsasser, T->T ring_to_ring_SF; the reference has no B->U ring table
+  if (kind == TG_ET_BU) return set_err(c, TG_ERR_ARG, "ring transfers have no B->U kind");
   const int rows = n_ring_shells + 1, cols = n_sectors + 1, per = rows * cols;
   if ((size_t)n < (size_t)per * per) return set_err(c, TG_ERR_ARG, "ring transfer: output shorter than (n+1)^2 (ns+1)^2");
   cudaSetDevice(c->dev);
   int rc = ensure_et_buffers(c);
+  if (rc) return rc;
+  const cx<double>* Hp[3];
+  const cx<double>* Fp[3];
+  const cx<double>* Rp[3];
+  double sign = 1.0;
+  rc = et_kind_fields(c, kind, Hp, Fp, Rp, sign);
   if (rc) return rc;
   RingBins b{};
   b.n = n_ring_shells;
@@ -436,7 +439,7 @@ int run_ring_tr(tg_ctx* c, int kind, int axis, int n_ring_shells, int n_sectors,
   cudaError_t e = cudaMemsetAsync(c->diag, 0, sizeof(double) * need, c->st);
   if (e != cudaSuccess) return cuda_err(c, e, "ring transfer");
   const Geo& g = c->g;
-  const void* Hf[3] = {c->U0[3 * H + 0], c->U0[3 * H + 1], c->U0[3 * H + 2]};
+  const void* Hf[3] = {Hp[0], Hp[1], Hp[2]};
   rc = pipe_inverse_xy(c, 3, Hf, nullptr, nullptr, F64, 3, c->WX, c->etWY);
   if (rc) return rc;
   ProdPairs pp{};
@@ -455,8 +458,8 @@ int run_ring_tr(tg_ctx* c, int kind, int axis, int n_ring_shells, int n_sectors,
   const int nblk = (int)std::min<long long>((g.S + TPB - 1) / TPB, 148LL * 8);
   for (int i = 1; i < n_ring_shells; ++i)
     for (int j = 1; j <= n_sectors; ++j) {
-      k_fill_ring<<<(int)((g.S + TPB - 1) / TPB), TPB, 0, c->st>>>(g, c->U0[3 * F + 0], c->U0[3 * F + 1],
-                                                                   c->U0[3 * F + 2], c->etG[0], c->etG[1], c->etG[2],
+      k_fill_ring<<<(int)((g.S + TPB - 1) / TPB), TPB, 0, c->st>>>(g, Fp[0], Fp[1], Fp[2], c->etG[0], c->etG[1],
+                                                                   c->etG[2],
                                                                    b.r[i - 1], b.r[i], b.bound[j - 1], b.bound[j], axis,
                                                                    cyl);
       e = cudaGetLastError();
@@ -469,7 +472,7 @@ int run_ring_tr(tg_ctx* c, int kind, int axis, int n_ring_shells, int n_sectors,
       RingContractArgs a{};
       a.g = g;
       for (int q = 0; q < 9; ++q) a.PX[q] = c->etPX[q];
-      for (int q = 0; q < 3; ++q) a.R[q] = c->U0[3 * R + q];
+      for (int q = 0; q < 3; ++q) a.R[q] = Rp[q];
       a.b = b;
       a.out = c->diag + ((size_t)i * cols + j) * per;
       if (c->tprec == F64) k_ring_contract<double><<<nblk, TPB, smem, c->st>>>(a);

@@ -132,13 +132,46 @@ def test_gpu_ring_to_ring_mhd_kinds(lib):
     s = IncFluid(N, physics="MHD", nu=1e-3, eta=1e-3, dt=1e-3)
     s.set_V(U)
     s.set_W(B)
+    Zp = [u + b for u, b in zip(U, B)]
+    Zm = [u - b for u, b in zip(U, B)]
     for kind, (H, F, Rf, sign) in ((L.TG_ET_UU, (U, U, U, -1.0)), (L.TG_ET_BB, (U, B, B, -1.0)),
-                                   (L.TG_ET_UB, (B, U, B, 1.0))):
+                                   (L.TG_ET_UB, (B, U, B, 1.0)), (L.TG_ET_ZP, (Zm, Zp, Zp, -1.0)),
+                                   (L.TG_ET_ZM, (Zp, Zm, Zm, -1.0))):
         T, _ = s.Compute_ring_tr(6, 2, 1, kind)
         want = o.compute_ring_tr_generic(H, F, Rf, sign, KF, 1, 6, 2)
         assert np.abs(T - want).max() <= 1e-12 * np.abs(want).max(), kind
+        if kind in (L.TG_ET_ZP, L.TG_ET_ZM):
+            Tc, _ = s.Compute_cylinder_ring_tr(5, 3, 2, kind)
+            want = o.compute_cylinder_ring_tr_generic(H, F, Rf, sign, KF, 2, 5, 3)
+            assert np.abs(Tc - want).max() <= 1e-12 * np.abs(want).max(), kind
     with pytest.raises(L.TarangError):
         s.Compute_ring_tr(6, 2, 1, L.TG_ET_BU)       # not a ring transfer of the reference
+    # the Elsasser tables leave U and B as they were (Elsasser_to_UB_field)
+    assert np.abs(s.get_W()[1] - B[1]).max() == 0
+
+
+@pytest.mark.gpu
+def test_gpu_ring_to_ring_scalar(lib):
+    """ring_to_ring_SF (Compute_ring_tr_scalar compute_ring_tr.cc:104-131) and the cylinder form:
+    giver T on the ring, N = U.grad T<, against T; U->U of the same run."""
+    from tarang_b200 import _lib as L
+    from tarang_b200.solver import IncFluid
+    N = (32, 32, 32)
+    U = ic.random_phase_field(N, seed=93)
+    T = ic.random_phase_field(N, k0=3.0, seed=94)[0]
+    z = np.zeros_like(T)
+    s = IncFluid(N, physics="SCALAR", nu=1e-3, kappa=2e-3, dt=1e-3)
+    s.set_V(U)
+    s.set_T(T)
+    got, _ = s.Compute_ring_tr(6, 3, 3, L.TG_ET_TT)
+    want = o.compute_ring_tr_generic(U, [T, z, z], [T, z, z], -1.0, KF, 3, 6, 3)
+    assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
+    got, _ = s.Compute_cylinder_ring_tr(5, 2, 1, L.TG_ET_TT)
+    want = o.compute_cylinder_ring_tr_generic(U, [T, z, z], [T, z, z], -1.0, KF, 1, 5, 2)
+    assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
+    got, _ = s.Compute_ring_tr(6, 3, 3, L.TG_ET_UU)
+    want = o.compute_ring_tr_generic(U, U, U, -1.0, KF, 3, 6, 3)
+    assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
 
 
 def test_cylinder_ring_transfer_oracle_identity():
