@@ -289,7 +289,10 @@ int tg_cylinder_ring_to_ring(tg_ctx* ctx, int kind, int axis, int n_cylinder_she
 /* shell radii of the energy transfer (EnergyTr.cc:136-160): n_shells + 1 doubles */
 int tg_et_radii(tg_ctx* ctx, double* radii, int n);
 /* Compute_flux (compute_flux.cc:52-304): flux[s], s = 0..n_shells (index 0 unused); kind
- * TG_ET_UU/BB/UB/BU, TG_ET_ZP/ZM (Elsasser, :228-255) or TG_ET_TT (Compute_flux_scalar :82-95) */
+ * TG_ET_UU/BB/UB/BU, TG_ET_ZP/ZM (Elsasser, :228-255) or TG_ET_TT (Compute_flux_scalar :82-95;
+ * convection: Compute_flux_RB).  FOUR and SCFT (Shell_mult_single_SCFT / Shell_mult_all_SCFT
+ * scft/scft_ET.cc:53-265: Kmagnitude_SCFT, Multiplicity_factor_SCFT, x derivatives of the sine and
+ * cosine product series). */
 int tg_flux(tg_ctx* ctx, int kind, double* flux, int n);
 /* Compute_shell_tr (compute_shell_tr.cc:59-281): (n_shells+1) x (n_shells+1) row-major */
 int tg_shell_to_shell(tg_ctx* ctx, int kind, double* tr, int n);

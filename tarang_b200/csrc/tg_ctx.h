@@ -141,9 +141,10 @@ double el_ystage(const tg_ctx* c);
 // nread = number of distinct compact fields read (for the byte count)
 int pipe_inverse_xy(tg_ctx* c, int nf, const void* const* in, const void* const* in2, const int* comb,
                     int inprec, int nread, void* const* WX, void* const* WY);
-// fused z-pass products (pairs pp of the nin inputs), then y- and x-forward passes into PX
+// fused z-pass products (pairs pp of the nin inputs), then y- and x-forward passes into PX;
+// SCFT: product q takes the x transform xkinds[q] (0 cosine, 1 sine; default c->xfwd_kind)
 int pipe_products_forward(tg_ctx* c, int nin, const void* const* WY, int nprod, const ProdPairs& pp,
-                          void* const* PP, void* const* PY, void* const* PX);
+                          void* const* PP, void* const* PY, void* const* PX, const int* xkinds = nullptr);
 int dalloc_ctx(tg_ctx* c, void** p, size_t bytes);
 // a context holding B same-shape request slots (B = 1: tg_ctx_create)
 int ctx_create_batch(const tg_config* cfg, int B, tg_ctx** out);

@@ -132,6 +132,11 @@ __global__ void k_fill_shell(Geo g, const cx<double>* F0, const cx<double>* F1, 
   G2[idx] = in ? F2[idx] : z;
 }
 
+// SCFT x transforms of P(i, j) = F(H_j G_i), q = 3 i + j, with H and G of parities (sin, cos,
+// cos) along x: sin x sin and cos x cos products are cosine series (0), mixed ones sine (1)
+// (ET_Forward_transform_RSprod_G ET_transform.cc:49-113 with the parities of ET_RSprod.cc:49-169)
+constexpr int kEtXKinds[9] = {0, 1, 1, 1, 0, 0, 1, 0, 0};
+
 struct ContractArgs {
   Geo g;
   const void* PX[9];      // P(i, j) = F(H_j G_i), q = 3 i + j
@@ -142,7 +147,10 @@ struct ContractArgs {
   int cross;              // 1: N = F(H x G) (EnergyTr_Compute_nlin_UcrossB) instead of D_j F(H_j G_i)
 };
 
-// N_i = i k_j P(i, j); hist[r][shell(|K|)] += 2 mult Re(sum_i N_i conj(R_i))
+// N_i = D_j P(i, j): FOUR i k_j P(i, j); SCFT (Xderiv_SCFT scft_tr.cc:649-707) the x derivative
+// of the cosine series P(0, 0) is -kx P and of the sine series P(1, 0), P(2, 0) is +kx P, y and z
+// as FOUR.  hist[r][shell(|K|)] += 2 mult Re(sum_i N_i conj(R_i)) (Multiplicity_factor_FOUR or
+// _SCFT).
 template <typename Rp>
 __global__ void __launch_bounds__(TPB) k_et_contract(ContractArgs a) {
   __shared__ double sh[2 * (kMaxShells + 1)];
@@ -167,7 +175,7 @@ __global__ void __launch_bounds__(TPB) k_et_contract(ContractArgs a) {
       N[0] = P(2, 1) - P(1, 2);
       N[1] = P(0, 2) - P(2, 0);
       N[2] = P(1, 0) - P(0, 1);
-    } else {
+    } else if (g.basis == 0) {
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
         const cx<double> p0 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 0])[idx]);
@@ -176,8 +184,17 @@ __global__ void __launch_bounds__(TPB) k_et_contract(ContractArgs a) {
         const cx<double> s = mkc<double>(kx * p0.x + ky * p1.x + kz * p2.x, kx * p0.y + ky * p1.y + kz * p2.y);
         N[i] = ione(s);
       }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const cx<double> p0 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 0])[idx]);
+        const cx<double> p1 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 1])[idx]);
+        const cx<double> p2 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 2])[idx]);
+        const double dx = (i == 0) ? -kx : kx;
+        N[i] = mkc<double>(dx * p0.x - (ky * p1.y + kz * p2.y), dx * p0.y + (ky * p1.x + kz * p2.x));
+      }
     }
-    const double m = mult_four(l1, l2, l3, g.N1, g.N2);
+    const double m = g.basis == 0 ? mult_four(l1, l2, l3, g.N1, g.N2) : mult_scft(l1, l2, l3, g.N2);
     for (int r = 0; r < a.nrec; ++r) {
       double v = 0;
 #pragma unroll
@@ -265,7 +282,7 @@ int et_tables_ptr(tg_ctx* c, const cx<double>* const* Hp, const cx<double>* cons
     const void* G[3] = {c->etG[0], c->etG[1], c->etG[2]};
     rc = pipe_inverse_xy(c, 3, G, nullptr, nullptr, F64, 3, c->WX, c->etWY + 3);
     if (rc) return rc;
-    rc = pipe_products_forward(c, 6, c->etWY, 9, pp, c->etPP, c->etPY, c->etPX);
+    rc = pipe_products_forward(c, 6, c->etWY, 9, pp, c->etPP, c->etPY, c->etPX, kEtXKinds);
     if (rc) return rc;
     ContractArgs a{};
     a.g = g;
@@ -383,7 +400,6 @@ int et_kind_fields(tg_ctx* c, int kind, const cx<double>* H[3], const cx<double>
 namespace {
 
 int et_table_kind(tg_ctx* c, int kind, std::vector<double>& T, std::vector<double>& rho, double& sign) {
-  if (c->basis != TG_FOUR) return set_err(c, TG_ERR_UNSUPPORTED, "energy transfer is built for the FOUR basis");
   int rc = ensure_et_buffers(c);
   if (rc) return rc;
   const cx<double>* H[3];

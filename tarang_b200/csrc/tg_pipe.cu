@@ -114,7 +114,7 @@ int pipe_inverse_xy(tg_ctx* c, int nf, const void* const* in, const void* const*
 }
 
 int pipe_products_forward(tg_ctx* c, int nin, const void* const* WY, int nprod, const ProdPairs& pp,
-                          void* const* PP, void* const* PY, void* const* PX) {
+                          void* const* PP, void* const* PY, void* const* PX, const int* xkinds) {
   if (!c->pipeline_ok) return set_err(c, TG_ERR_UNSUPPORTED, "nonlinear term needs N3/2 a power of two in [4, 256]");
   const Geo& g = c->g;
   {
@@ -190,7 +190,7 @@ int pipe_products_forward(tg_ctx* c, int nin, const void* const* WY, int nprod, 
       // SFT / CFT along x with Norm_SCFT's extra 1/2 (scft_tr.cc:89-92; the z-pass applied
       // 1/(N1 N2 N3))
       R2RArgs r{};
-      for (int q = 0; q < nprod; ++q) r.kind[q] = c->xfwd_kind[q];
+      for (int q = 0; q < nprod; ++q) r.kind[q] = xkinds ? xkinds[q] : c->xfwd_kind[q];
       r.trig = c->trigx;
       for (int k = 0; k < 4; ++k) {
         r.mat[k] = c->xmat[k];
