@@ -56,7 +56,13 @@ extern "C" {
 #define TG_RK4 4
 /* force_field_proc (compute_force_main.cc:43-124) */
 #define TG_FORCE_DECAY 0
-#define TG_FORCE_ENERGY_SUPPLY 1
+#define TG_FORCE_ENERGY_SUPPLY 1  /* Compute_force_const_energy_helicity_supply (FOUR; fluid, MHD,
+                                     passive scalar): force_para = inner, outer, eps, eps_h/(k eps),
+                                     then eps_B, epsh_B/(k eps_B) (MHD) or eps_T (scalar) */
+#define TG_FORCE_ENERGY_HELICITY 2  /* Compute_force_const_energy_helicity (compute_force_const_ek_hk.cc,
+                                       FOUR; fluid, MHD, passive scalar): force_para = inner, outer,
+                                       energy level, H/(k E), then the B level and H/(k E) of B (MHD)
+                                       or the scalar level (scalar) */
 #define TG_FORCE_MODES 5      /* a fixed force on given modes, set by tg_set_force_modes: the
                                  Taylor-Green, ABC and given-mode forcings (force_field_proc 3, 4, 5) */
 #define TG_FORCE_CORIOLIS 21  /* Force = V x Omega, Omega = force_para[0..2], evaluated from each RK
@@ -117,7 +123,7 @@ typedef struct tg_config {
   double kappa;       /* diffusion_coefficient of T */
   double dt;          /* Tdt: the upper bound of Get_dt (compute_dt.cc:47-59) */
   int force_kind;     /* TG_FORCE_* */
-  double force_para[4]; /* energy supply: inner radius, outer radius, epsilon, eps_h/(k eps) */
+  double force_para[6]; /* force_double_para(1..6) of the force_field_proc (see TG_FORCE_*) */
   int n_shells;       /* energy transfer: no_shells (= no_spheres), scheme 0 radii */
   double rb_ra, rb_pr;  /* Rayleigh and Prandtl numbers (RB) */
   int device;         /* CUDA device ordinal */

@@ -686,52 +686,104 @@ def number_modes_in_shell(N, inner, outer, kfactor, basis="FOUR"):
     return cnt
 
 
-def force_const_energy_supply(V, N, kfactor, inner, outer, eps, eps_h=0.0):
-    """Compute_force_const_energy_helicity_supply  compute_force_ek_hk_supply.cc:51-157 with
-    Force_alpha_beta  force_alpha_beta.cc:60-121 (FOUR) and Satisfy_reality_array on F.
-    F = alpha u + beta omega on inner < |K| <= outer; alpha = temp(1 - s h)/(1 - s^2),
-    beta = temp (h - s)/(1 - s^2), temp = eps/(nf 2 E_k), s = H_k/(k E_k); vorticity is used
-    only when beta > MYEPS."""
+def _band_modes(N, kfactor, outer):
+    """The (kx, ky, kz) loop of the band forcings (FOUR): kx in [-ceil(outer/kf1), +..], ky
+    likewise, kz in [0, ceil(outer/kf3)], with the stored index (lx, ly, lz)."""
     N1, N2, N3 = N
-    nf = number_modes_in_shell(N, inner, outer, kfactor)
-    e_per_mode = eps / nf
-    F = [np.zeros_like(V[0]) for _ in range(3)]
     kxm = int(math.ceil(outer / kfactor[0]))
     kym = int(math.ceil(outer / kfactor[1]))
     kzm = int(math.ceil(outer / kfactor[2]))
     for kx in range(-kxm, kxm + 1):
         for ky in range(-kym, kym + 1):
             for kz in range(0, kzm + 1):
-                lx = kx if kx >= 0 else kx + N1
-                ly = ky if ky >= 0 else ky + N2
-                lz = kz
-                km = math.sqrt((kx * kfactor[0]) ** 2 + (ky * kfactor[1]) ** 2 + (kz * kfactor[2]) ** 2)
-                if not (inner < km <= outer):
-                    continue
-                v = np.array([V[0][lx, ly, lz], V[1][lx, ly, lz], V[2][lx, ly, lz]])
-                Ek = float(np.sum(np.abs(v) ** 2)) / 2.0        # CV_Modal_energy (Cvf.cc:595-600)
-                if Ek <= MYEPS:
-                    continue
-                kk = np.array([kx * kfactor[0], ky * kfactor[1], kz * kfactor[2]])
-                vr, vi = v.real, v.imag
-                Hk = float(np.dot(kk, np.cross(vr, vi)))       # Get_Modal_helicity_FOUR four_basic.cc:136-155
-                temp = e_per_mode / (2 * Ek)
-                sk = Hk / (km * Ek)
-                if abs(sk * sk - 1) > MYEPS2:
-                    alpha = temp * (1 - sk * eps_h) / (1 - sk * sk)
-                    beta = temp * (eps_h - sk) / (1 - sk * sk)
-                else:
-                    alpha = temp / 2
-                    beta = alpha / (sk * km)
-                vort = np.zeros(3, dtype=np.complex128)
-                if beta > MYEPS:                                 # Compute_Modal_vorticity_FOUR four_basic.cc:166-186
-                    vort = 1j * np.array([kk[1] * v[2] - kk[2] * v[1],
-                                          kk[2] * v[0] - kk[0] * v[2],
-                                          kk[0] * v[1] - kk[1] * v[0]])
-                for c in range(3):
-                    F[c][lx, ly, lz] = alpha * v[c] + beta * vort[c]
-    F = [satisfy_reality(f) for f in F]
-    return F
+                yield kx, ky, kz, (kx if kx >= 0 else kx + N1), (ky if ky >= 0 else ky + N2), kz
+
+
+def _alpha_beta(mode, v, kk, km, e_mode, h):
+    """alpha_k, beta_k of one mode with modal energy E_k = |v|^2/2 (CV_Modal_energy Cvf.cc:595-600)
+    and helicity H_k = K . (Vr x Vi) (Get_Modal_helicity_FOUR four_basic.cc:136-155), s = H_k/(k E_k):
+      mode 1 (supply, compute_force_ek_hk_supply.cc:120-138): temp = e/(2 E_k),
+        alpha = temp (1 - s h)/(1 - s^2), beta = temp (h - s)/(1 - s^2); |s^2 - 1| <= MYEPS2:
+        alpha = temp/2, beta = alpha/(s k);
+      mode 2 (constant energy and helicity, compute_force_const_ek_hk.cc:124-147): t1 = sqrt(e/E_k),
+        t2 = sqrt((1 + h)/(1 + s)), t3 = sqrt((1 - h)/(1 - s)), alpha = t1 (t2 + t3)/2,
+        beta = t1 (t2 - t3)/(2 k); |s^2 - 1| <= MYEPS2: alpha = t1, beta = 0.
+    None when E_k <= MYEPS."""
+    Ek = float(np.sum(np.abs(v) ** 2)) / 2.0
+    if Ek <= MYEPS:
+        return None
+    Hk = float(np.dot(kk, np.cross(v.real, v.imag)))
+    sk = Hk / (km * Ek)
+    if mode == 1:
+        temp = e_mode / (2 * Ek)
+        if abs(sk * sk - 1) > MYEPS2:
+            return temp * (1 - sk * h) / (1 - sk * sk), temp * (h - sk) / (1 - sk * sk)
+        alpha = temp / 2
+        return alpha, alpha / (sk * km)
+    t1 = math.sqrt(e_mode / Ek)
+    if abs(sk * sk - 1) > MYEPS2:
+        t2 = math.sqrt((1 + h) / (1 + sk))
+        t3 = math.sqrt((1 - h) / (1 - sk))
+        return t1 / 2 * (t2 + t3), t1 / (2 * km) * (t2 - t3)
+    return t1, 0.0
+
+
+def force_band(V, N, kfactor, inner, outer, eps, eps_h=0.0, mode=1, gate=False):
+    """The vector force of force_field_proc 1 (Compute_force_const_energy_helicity_supply
+    compute_force_ek_hk_supply.cc:51-157) or 2 (Compute_force_const_energy_helicity
+    compute_force_const_ek_hk.cc:53-165), FOUR: on inner < |K| <= outer, F = alpha V + beta omega
+    (Force_alpha_beta force_alpha_beta.cc:60-88: the vorticity i K x V only when beta > MYEPS),
+    with e = eps / nf per mode (nf = Get_number_modes_in_shell); then Satisfy_reality_array.
+    gate: the mode is skipped unless e > MYEPS (the MHD and scalar variants of proc 1 and every
+    variant of proc 2)."""
+    nf = number_modes_in_shell(N, inner, outer, kfactor)
+    e_mode = eps / nf
+    F = [np.zeros_like(V[0]) for _ in range(3)]
+    if gate and not e_mode > MYEPS:
+        return F
+    for kx, ky, kz, lx, ly, lz in _band_modes(N, kfactor, outer):
+        km = math.sqrt((kx * kfactor[0]) ** 2 + (ky * kfactor[1]) ** 2 + (kz * kfactor[2]) ** 2)
+        if not (inner < km <= outer):
+            continue
+        v = np.array([V[0][lx, ly, lz], V[1][lx, ly, lz], V[2][lx, ly, lz]])
+        kk = np.array([kx * kfactor[0], ky * kfactor[1], kz * kfactor[2]])
+        ab = _alpha_beta(mode, v, kk, km, e_mode, eps_h)
+        if ab is None:
+            continue
+        alpha, beta = ab
+        vort = np.zeros(3, dtype=np.complex128)
+        if beta > MYEPS:                                 # Compute_Modal_vorticity_FOUR four_basic.cc:166-186
+            vort = 1j * np.array([kk[1] * v[2] - kk[2] * v[1], kk[2] * v[0] - kk[0] * v[2], kk[0] * v[1] - kk[1] * v[0]])
+        for c in range(3):
+            F[c][lx, ly, lz] = alpha * v[c] + beta * vort[c]
+    return [satisfy_reality(f) for f in F]
+
+
+def force_band_scalar(T, N, kfactor, inner, outer, eps_T, mode=1):
+    """The scalar force of procs 1 and 2 with a passive scalar (compute_force_ek_hk_supply.cc:
+    270-277, compute_force_const_ek_hk.cc:262-269; Force_scalar_alpha force_alpha_beta.cc:183-198):
+    F_T = alpha T with alpha = e_T / E_T(k) (proc 1) or sqrt(e_T / E_T(k)) (proc 2),
+    E_T(k) = |T|^2/2, when e_T = eps_T / nf > MYEPS and E_T(k) > MYEPS."""
+    nf = number_modes_in_shell(N, inner, outer, kfactor)
+    e_mode = eps_T / nf
+    F = np.zeros_like(T)
+    if not e_mode > MYEPS:
+        return F
+    for kx, ky, kz, lx, ly, lz in _band_modes(N, kfactor, outer):
+        km = math.sqrt((kx * kfactor[0]) ** 2 + (ky * kfactor[1]) ** 2 + (kz * kfactor[2]) ** 2)
+        if not (inner < km <= outer):
+            continue
+        Et = abs(T[lx, ly, lz]) ** 2 / 2
+        if Et > MYEPS:
+            alpha = e_mode / Et if mode == 1 else math.sqrt(e_mode / Et)
+            F[lx, ly, lz] = alpha * T[lx, ly, lz]
+    return satisfy_reality(F)
+
+
+def force_const_energy_supply(V, N, kfactor, inner, outer, eps, eps_h=0.0):
+    """Compute_force_const_energy_helicity_supply  compute_force_ek_hk_supply.cc:51-157 (fluid):
+    force_band with mode 1 and no gate on the energy per mode."""
+    return force_band(V, N, kfactor, inner, outer, eps, eps_h, mode=1, gate=False)
 
 
 def force_coriolis(V, omega):
@@ -791,14 +843,19 @@ def abc_force(N, k0, amp, A, B, C):
 
 
 def fluid_force(force, V, N, kfactor):
-    """The velocity force of a run: None (decay), energy supply dict(inner, outer, eps, eps_h),
+    """The velocity force of a run: None (decay), energy supply dict(inner, outer, eps, eps_h)
+    (proc 1), dict(kind="energy_helicity", inner, outer, eps, eps_h) (proc 2),
     dict(kind="static", F=[F1, F2, F3, ...]) (a fixed force field) or
     dict(kind="coriolis", omega=(w1, w2, w3))."""
     if force is None:
         return None
     kind = force.get("kind", "energy_supply")
     if kind == "energy_supply":
-        return force_const_energy_supply(V, N, kfactor, **{k: v for k, v in force.items() if k != "kind"})
+        return force_const_energy_supply(V, N, kfactor, force["inner"], force["outer"], force["eps"],
+                                         force.get("eps_h", 0.0))
+    if kind == "energy_helicity":
+        return force_band(V, N, kfactor, force["inner"], force["outer"], force["eps"], force.get("eps_h", 0.0),
+                          mode=2, gate=True)
     if kind == "static":
         return list(force["F"][:3])
     if kind == "coriolis":
@@ -891,11 +948,22 @@ class MHDSolver(FluidSolver):
         """Compute_force(W), Compute_nlin(W), Add_force(W) (add_force.cc:58-66): U.nlin -= F,
         W.nlin -= W.Force (a static force's components 3..5; zero otherwise)."""
         un, bn = nlin_mhd(V, W, self.kfactor, self.basis, self.alias)
-        F = fluid_force(self.force, V, self.N, self.kfactor)
-        if F is not None:
+        kind = self.force.get("kind", "energy_supply") if self.force is not None else None
+        if kind in ("energy_supply", "energy_helicity"):
+            # Compute_force_const_energy_helicity_supply(W) compute_force_ek_hk_supply.cc:292-437,
+            # Compute_force_const_energy_helicity(W) compute_force_const_ek_hk.cc:296-446
+            f, mode = self.force, (1 if kind == "energy_supply" else 2)
+            F = force_band(V, self.N, self.kfactor, f["inner"], f["outer"], f["eps"], f.get("eps_h", 0.0), mode, True)
+            FW = force_band(W, self.N, self.kfactor, f["inner"], f["outer"], f.get("eps_W", 0.0), f.get("eps_hW", 0.0),
+                            mode, True)
             un = [un[i] - F[i] for i in range(3)]
-            if self.force.get("kind") == "static" and len(self.force["F"]) > 3:
-                bn = [bn[i] - self.force["F"][3 + i] for i in range(3)]
+            bn = [bn[i] - FW[i] for i in range(3)]
+        else:
+            F = fluid_force(self.force, V, self.N, self.kfactor)
+            if F is not None:
+                un = [un[i] - F[i] for i in range(3)]
+                if self.force.get("kind") == "static" and len(self.force["F"]) > 3:
+                    bn = [bn[i] - self.force["F"][3 + i] for i in range(3)]
         p = pressure(un, self.kfactor, self.basis, self.alias)
         ru = rhs_from_nlin(un, p, self.kfactor, self.basis)
         rb = [-b for b in bn]
@@ -1039,6 +1107,40 @@ class RBSolver:
         """Get_Nusselt_no  nusselt.cc:53-89: 1 + nuf <u1, theta> (PRLARGE + ULARGE: nuf =
         2 sqrt(Ra Pr))."""
         return 1 + self.nuf * total_energy(V[0], self.basis, T)
+
+
+class ScalarSolver(RBSolver):
+    """The passive-scalar loop src/IScalar/Iscalar_main.cc:272-300: Compute_force(T),
+    Compute_nlin(T) (Compute_nlin_scalar compute_nlin_SF.cc:80-177 with Dealias_nlin(T)),
+    Add_force(T) (add_force.cc:57-63), Compute_pressure, Get_dt(T) = Get_dt() (compute_dt.cc:66-69)
+    and the IF-RK4 of time_advance_SF.cc with nu for u and kappa for T: the convection loop
+    without buoyancy.  force: None, or dict(kind="energy_supply" | "energy_helicity", inner, outer,
+    eps, eps_h, eps_T) (procs 1, 2 with the scalar variants compute_force_ek_hk_supply.cc:164-289,
+    compute_force_const_ek_hk.cc:167-293)."""
+
+    def __init__(self, N, kfactor, nu, kappa, Tdt, basis="FOUR", alias="DEALIAS", force=None):
+        self.N = tuple(N)
+        self.kfactor = tuple(kfactor)
+        self.nu, self.kappa = nu, kappa
+        self.fu = self.ft = 0.0
+        self.Tdt = Tdt
+        self.basis = basis
+        self.alias = alias
+        self.omega = None
+        self.force = force
+
+    def rhs(self, V, T):
+        nl = nlin_fluid(V, self.kfactor, self.basis, self.alias)
+        tn = nlin_scalar(V, T, self.kfactor, self.basis, self.alias, dealias_T=True)
+        if self.force is not None:
+            f = self.force
+            mode = 1 if f.get("kind", "energy_supply") == "energy_supply" else 2
+            F = force_band(V, self.N, self.kfactor, f["inner"], f["outer"], f["eps"], f.get("eps_h", 0.0), mode, True)
+            FT = force_band_scalar(T, self.N, self.kfactor, f["inner"], f["outer"], f.get("eps_T", 0.0), mode)
+            nl = [nl[i] - F[i] for i in range(3)]
+            tn = tn - FT
+        p = pressure(nl, self.kfactor, self.basis, self.alias)
+        return rhs_from_nlin(nl, p, self.kfactor, self.basis), -tn
 
 
 # --------------------------------------------------------------------------------------

@@ -26,6 +26,7 @@ TG_FLUID, TG_MHD, TG_SCALAR, TG_RB = 0, 1, 2, 3
 TG_FP64, TG_FP32_MIXED = 0, 1
 TG_RK4 = 4
 TG_FORCE_DECAY, TG_FORCE_ENERGY_SUPPLY, TG_FORCE_MODES, TG_FORCE_CORIOLIS, TG_FORCE_RB = 0, 1, 5, 21, 51
+TG_FORCE_ENERGY_HELICITY = 2
 TG_FORCE_RB_ROTATION = 52
 TG_FORCE_MODES_KMAX = 64
 TG_RING_MAX_SECTORS = 64
@@ -69,7 +70,7 @@ class tg_config(C.Structure):
         ("kappa", C.c_double),
         ("dt", C.c_double),
         ("force_kind", C.c_int),
-        ("force_para", C.c_double * 4),
+        ("force_para", C.c_double * 6),
         ("n_shells", C.c_int),
         ("rb_ra", C.c_double),
         ("rb_pr", C.c_double),

@@ -138,19 +138,28 @@ int run_pipeline(tg_ctx* c, const void* const* in, int inprec) {
   return pipe_products_forward(c, c->nin, c->WY, c->nprod, c->pairs, c->PP, c->PY, c->PX);
 }
 
+// U: the c->nstate fields the force is computed from (the stage input)
 int run_force(tg_ctx* c, const void* const* U, int uprec) {
   if (c->force_on != 1) return TG_OK;
   ForceArgs f{};
   f.g = c->g;
-  for (int i = 0; i < 3; ++i) f.U[i] = U[i];
+  f.ns = c->nstate;
+  for (int i = 0; i < c->nstate; ++i) f.U[i] = U[i];
   f.uprec = uprec;
+  f.mode = c->cfg.force_kind == TG_FORCE_ENERGY_HELICITY ? 2 : 1;
+  // the fluid-only supply does not test the energy per mode (compute_force_ek_hk_supply.cc:120)
+  f.gate = (f.mode == 2 || c->phys != TG_FLUID) ? 1 : 0;
   f.fx = c->fx;
   f.fy = c->fy;
   f.fz = c->fz;
-  f.inner = c->cfg.force_para[0];
-  f.outer = c->cfg.force_para[1];
-  f.e_per_mode = c->nf_modes > 0 ? c->cfg.force_para[2] / c->nf_modes : 0.0;
-  f.eps_h = c->cfg.force_para[3];
+  const double* fp = c->cfg.force_para;
+  const double nf = c->nf_modes > 0 ? (double)c->nf_modes : 0.0;
+  f.inner = fp[0];
+  f.outer = fp[1];
+  f.e_per_mode = nf > 0 ? fp[2] / nf : 0.0;
+  f.eps_h = fp[3];
+  f.e_per_mode_b = (nf > 0 && c->nstate > 3) ? fp[4] / nf : 0.0;
+  f.eps_h_b = c->nstate == 6 ? fp[5] : 0.0;
   f.FB = c->FB;
   ProfScope pr(c, "force", 0.0);
   TG_CK(launch_force_supply(f, c->st));
@@ -704,7 +713,7 @@ int ctx_create_batch(const tg_config* cfg, int B, tg_ctx** out) {
     if (e != cudaSuccess) return fail(cuda_err(c, e, "init scalars"));
   }
   c->dx_cfl = 2 * M_PI / std::max(1, max_radius_inside(c));
-  if (cfg->force_kind == TG_FORCE_ENERGY_SUPPLY) {
+  if (cfg->force_kind == TG_FORCE_ENERGY_SUPPLY || cfg->force_kind == TG_FORCE_ENERGY_HELICITY) {
     if (B != 1) return fail(set_err(c, TG_ERR_UNSUPPORTED, "forced requests are not batched"));
     c->force_on = 1;
     const double outer = cfg->force_para[1];
@@ -714,7 +723,7 @@ int ctx_create_batch(const tg_config* cfg, int B, tg_ctx** out) {
     c->fbox = (2 * c->fx + 1) * (2 * c->fy + 1) * (c->fz + 1);
     c->nf_modes = count_force_modes(*cfg);
     if (c->nf_modes <= 0) return fail(set_err(c, TG_ERR_ARG, "forcing shell holds no modes"));
-    if ((rc = dalloc(c, (void**)&c->FB, sizeof(cx<double>) * 3 * (size_t)c->fbox))) return fail(rc);
+    if ((rc = dalloc(c, (void**)&c->FB, sizeof(cx<double>) * c->nstate * (size_t)c->fbox))) return fail(rc);
   } else if (cfg->force_kind == TG_FORCE_MODES) {
     if (B != 1) return fail(set_err(c, TG_ERR_UNSUPPORTED, "forced requests are not batched"));
     c->force_on = 2;  // the box is allocated by tg_set_force_modes
@@ -748,7 +757,8 @@ int validate_config(const tg_config* cfg) {
     return TG_ERR_ARG;
   if (cfg->precision != TG_FP64 && cfg->precision != TG_FP32_MIXED) return TG_ERR_ARG;
   if (cfg->scheme != TG_RK4) return TG_ERR_UNSUPPORTED;
-  if (cfg->force_kind != TG_FORCE_DECAY && cfg->force_kind != TG_FORCE_ENERGY_SUPPLY && cfg->force_kind != TG_FORCE_RB &&
+  if (cfg->force_kind != TG_FORCE_DECAY && cfg->force_kind != TG_FORCE_ENERGY_SUPPLY &&
+      cfg->force_kind != TG_FORCE_ENERGY_HELICITY && cfg->force_kind != TG_FORCE_RB &&
       cfg->force_kind != TG_FORCE_MODES && cfg->force_kind != TG_FORCE_CORIOLIS && cfg->force_kind != TG_FORCE_RB_ROTATION)
     return TG_ERR_UNSUPPORTED;
   if ((cfg->force_kind == TG_FORCE_RB || cfg->force_kind == TG_FORCE_RB_ROTATION) && cfg->physics != TG_RB)
@@ -762,8 +772,13 @@ int validate_config(const tg_config* cfg) {
   if (cfg->force_kind == TG_FORCE_CORIOLIS)
     for (int i = 0; i < 3; ++i)
       if (!std::isfinite(cfg->force_para[i])) return TG_ERR_ARG;
-  if (cfg->force_kind == TG_FORCE_ENERGY_SUPPLY && cfg->basis != TG_FOUR) return TG_ERR_UNSUPPORTED;
-  if (cfg->force_kind == TG_FORCE_ENERGY_SUPPLY && cfg->physics != TG_FLUID) return TG_ERR_UNSUPPORTED;
+  if (cfg->force_kind == TG_FORCE_ENERGY_SUPPLY || cfg->force_kind == TG_FORCE_ENERGY_HELICITY) {
+    // band forcings: FOUR; fluid, MHD and passive scalar (convection has its own force)
+    if (cfg->basis != TG_FOUR || cfg->physics == TG_RB) return TG_ERR_UNSUPPORTED;
+    if (!(cfg->force_para[1] > cfg->force_para[0])) return TG_ERR_ARG;
+    for (int i = 0; i < 6; ++i)
+      if (!std::isfinite(cfg->force_para[i])) return TG_ERR_ARG;
+  }
   for (int i = 0; i < 3; ++i)
     if (!(cfg->kfactor[i] > 0)) return TG_ERR_ARG;
   if (!(cfg->dt > 0)) return TG_ERR_ARG;
@@ -813,7 +828,8 @@ int radius_inside(const tg_ctx* c) { return max_radius_inside(c); }
 
 int ensure_force_box(tg_ctx* c) {
   if (c->force_on != 1 || c->force_ever) return TG_OK;
-  const void* U[3] = {c->U0[0], c->U0[1], c->U0[2]};
+  const void* U[6];
+  for (int i = 0; i < c->nstate; ++i) U[i] = c->U0[i];
   return run_force(c, U, F64);
 }
 
@@ -859,11 +875,11 @@ size_t ctx_bytes_estimate(const tg_config* cfg, int B, bool with_staging) {
   b += sizeof(double) * 8 * (size_t)reduction_blocks((long long)S) * B;
   b += sizeof(double) * (8 + 8 + 6) * (size_t)B;
   b += sizeof(double) * (1 << 16) + sizeof(int) * 4;
-  if (cfg->force_kind == TG_FORCE_ENERGY_SUPPLY) {
+  if (cfg->force_kind == TG_FORCE_ENERGY_SUPPLY || cfg->force_kind == TG_FORCE_ENERGY_HELICITY) {
     const double outer = cfg->force_para[1];
     const int fx = (int)std::ceil(outer / cfg->kfactor[0]), fy = (int)std::ceil(outer / cfg->kfactor[1]),
               fz = (int)std::ceil(outer / cfg->kfactor[2]);
-    b += sizeof(cx<double>) * 3 * (size_t)(2 * fx + 1) * (2 * fy + 1) * (fz + 1);
+    b += sizeof(cx<double>) * nstate * (size_t)(2 * fx + 1) * (2 * fy + 1) * (fz + 1);
   }
   if (with_staging) b += sizeof(cx<double>) * (size_t)N1 * N2 * (N3 / 2 + 1);
   return b;
@@ -1140,7 +1156,8 @@ int tg_compute_force(tg_ctx* c) {
   if (!c) return TG_ERR_ARG;
   cudaSetDevice(c->dev);
   if (c->force_on) {
-    const void* in[3] = {c->U0[0], c->U0[1], c->U0[2]};
+    const void* in[6];
+    for (int i = 0; i < c->nstate; ++i) in[i] = c->U0[i];
     int rc = run_force(c, in, F64);
     if (rc) return rc;
   }

@@ -129,7 +129,8 @@ std::string batch_key(const tg_config& c, long long id) {
                 c.physics, c.precision, c.dealias, c.scheme, c.kfactor[0], c.kfactor[1], c.kfactor[2],
                 c.force_kind);
   std::string k(buf);
-  if (c.force_kind == TG_FORCE_ENERGY_SUPPLY) k += "|solo" + std::to_string(id);
+  if (c.force_kind == TG_FORCE_ENERGY_SUPPLY || c.force_kind == TG_FORCE_ENERGY_HELICITY)
+    k += "|solo" + std::to_string(id);
   if (c.force_kind == TG_FORCE_CORIOLIS || c.force_kind == TG_FORCE_RB_ROTATION) {
     std::snprintf(buf, sizeof(buf), "|om%a,%a,%a", c.force_para[0], c.force_para[1], c.force_para[2]);
     k += buf;
@@ -260,7 +261,7 @@ int move_slot(Batch& b, int from, int to) {
 // a new batch for request r's key: as many slots as fit in a quarter of the budget (at least
 // one) and in what is left of it, at most max_batch
 int open_batch(tg_server* s, const Req& r, long long* bid) {
-  const bool solo = r.cfg.force_kind == TG_FORCE_ENERGY_SUPPLY;
+  const bool solo = r.cfg.force_kind == TG_FORCE_ENERGY_SUPPLY || r.cfg.force_kind == TG_FORCE_ENERGY_HELICITY;
   const size_t budget = s->cfg.hbm_budget_bytes;
   const size_t left = budget > s->bytes ? budget - s->bytes : 0;
   const size_t one = ctx_bytes_estimate(&r.cfg, 1, true);

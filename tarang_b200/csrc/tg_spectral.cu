@@ -316,9 +316,71 @@ cudaError_t run_rk_phys(const RKArgs& a, int phys, int src, cudaStream_t s, int 
 }
 
 // ------------------------------------------------------------------ forcing
-// Compute_force_const_energy_helicity_supply (compute_force_ek_hk_supply.cc:51-157) with
-// Force_alpha_beta (force_alpha_beta.cc:60-121) and the reality condition of the force
-// (Satisfy_reality_array universal_misc.cc:51-109).  One block.
+// Band forcings on inner < |K| <= outer (FOUR), mode by mode from the current field:
+//   proc 1, Compute_force_const_energy_helicity_supply (compute_force_ek_hk_supply.cc:51-437):
+//     temp = e/(2 E_k), alpha = temp (1 - s h)/(1 - s^2), beta = temp (h - s)/(1 - s^2),
+//     |s^2 - 1| <= MYEPS2: alpha = temp/2, beta = alpha/(s k);
+//   proc 2, Compute_force_const_energy_helicity (compute_force_const_ek_hk.cc:53-446):
+//     t1 = sqrt(e/E_k), t2 = sqrt((1 + h)/(1 + s)), t3 = sqrt((1 - h)/(1 - s)),
+//     alpha = t1 (t2 + t3)/2, beta = t1 (t2 - t3)/(2 k); |s^2 - 1| <= MYEPS2: alpha = t1, beta = 0;
+// with s = H_k/(k E_k), F = alpha V + beta omega (Force_alpha_beta force_alpha_beta.cc:60-88; the
+// vorticity only when beta > MYEPS), the same for B with its own (e, h) in MHD, and for a passive
+// scalar F_T = alpha_T T, alpha_T = e_T/E_T (proc 1) or sqrt(e_T/E_T) (proc 2)
+// (Force_scalar_alpha force_alpha_beta.cc:183-198); then the reality condition of every force
+// component (Satisfy_reality_array universal_misc.cc:51-109).  One block.
+__device__ __forceinline__ void band_alpha_beta(int mode, const cx<double> (&v)[3], double kkx, double kky, double kkz,
+                                                double km, double e, double h, double& alpha, double& beta,
+                                                bool& on) {
+  const double Ek = 0.5 * (v[0].x * v[0].x + v[0].y * v[0].y + v[1].x * v[1].x + v[1].y * v[1].y +
+                           v[2].x * v[2].x + v[2].y * v[2].y);
+  on = Ek > 1e-15;
+  alpha = beta = 0;
+  if (!on) return;
+  // modal helicity k . (Vr x Vi)  (Get_Modal_helicity_FOUR four_basic.cc:136-155)
+  const double cx_ = v[1].x * v[2].y - v[2].x * v[1].y;
+  const double cy_ = v[2].x * v[0].y - v[0].x * v[2].y;
+  const double cz_ = v[0].x * v[1].y - v[1].x * v[0].y;
+  const double Hk = kkx * cx_ + kky * cy_ + kkz * cz_;
+  const double sk = Hk / (km * Ek);
+  if (mode == 1) {
+    const double temp = e / (2 * Ek);
+    if (fabs(sk * sk - 1) > 1e-5) {
+      alpha = temp * (1 - sk * h) / (1 - sk * sk);
+      beta = temp * (h - sk) / (1 - sk * sk);
+    } else {
+      alpha = temp / 2;
+      beta = alpha / (sk * km);
+    }
+  } else {
+    const double t1 = sqrt(e / Ek);
+    if (fabs(sk * sk - 1) > 1e-5) {
+      const double t2 = sqrt((1 + h) / (1 + sk)), t3 = sqrt((1 - h) / (1 - sk));
+      alpha = (t1 / 2) * (t2 + t3);
+      beta = (t1 / (2 * km)) * (t2 - t3);
+    } else {
+      alpha = t1;
+      beta = 0;
+    }
+  }
+}
+
+__device__ __forceinline__ void band_vector_force(int mode, const cx<double> (&v)[3], double kkx, double kky,
+                                                  double kkz, double km, double e, double h, cx<double> (&F)[3]) {
+  double alpha, beta;
+  bool on;
+  band_alpha_beta(mode, v, kkx, kky, kkz, km, e, h, alpha, beta, on);
+  if (!on) return;
+  cx<double> w[3] = {mkc<double>(0, 0), mkc<double>(0, 0), mkc<double>(0, 0)};
+  if (beta > 1e-15) {
+    // vorticity i K x V (Compute_Modal_vorticity_FOUR four_basic.cc:166-186)
+    w[0] = ione(kky * v[2] - kkz * v[1]);
+    w[1] = ione(kkz * v[0] - kkx * v[2]);
+    w[2] = ione(kkx * v[1] - kky * v[0]);
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) F[c] = alpha * v[c] + beta * w[c];
+}
+
 template <typename Ru>
 __global__ void __launch_bounds__(TPB) k_force_supply(ForceArgs a) {
   const Geo& g = a.g;
@@ -328,7 +390,9 @@ __global__ void __launch_bounds__(TPB) k_force_supply(ForceArgs a) {
     const int kz = p % nz;
     const int ky = (p / nz) % ny - a.fy;
     const int kx = p / (nz * ny) - a.fx;
-    cx<double> F[3] = {mkc<double>(0, 0), mkc<double>(0, 0), mkc<double>(0, 0)};
+    cx<double> F[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) F[c] = mkc<double>(0, 0);
     const double kkx = kx * g.kf0, kky = ky * g.kf1, kkz = kz * g.kf2;
     const double km = sqrt(kkx * kkx + kky * kky + kkz * kkz);
     if (km > a.inner && km <= a.outer) {
@@ -336,43 +400,37 @@ __global__ void __launch_bounds__(TPB) k_force_supply(ForceArgs a) {
       const int ly = ky >= 0 ? ky : ky + g.N2;
       const int r1 = (lx >= 0 && lx < g.N1) ? amap_row(g.ax, lx) : -1;
       const int r2 = (ly >= 0 && ly < g.N2) ? amap_row(g.ay, ly) : -1;
-      cx<double> v[3] = {mkc<double>(0, 0), mkc<double>(0, 0), mkc<double>(0, 0)};
+      cx<double> v[6];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) v[c] = mkc<double>(0, 0);
       if (r1 >= 0 && r2 >= 0 && kz < g.nkz) {
         const long long i = ((long long)r1 * g.nky + r2) * g.kzp + kz;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) v[c] = ldc<Ru>(a.U[c], i);
+        for (int c = 0; c < a.ns; ++c) v[c] = ldc<Ru>(a.U[c], i);
       }
-      const double Ek = 0.5 * (v[0].x * v[0].x + v[0].y * v[0].y + v[1].x * v[1].x + v[1].y * v[1].y +
-                               v[2].x * v[2].x + v[2].y * v[2].y);
-      if (Ek > 1e-15) {
-        // modal helicity k . (Vr x Vi)  (Get_Modal_helicity_FOUR four_basic.cc:136-155)
-        const double cx_ = v[1].x * v[2].y - v[2].x * v[1].y;
-        const double cy_ = v[2].x * v[0].y - v[0].x * v[2].y;
-        const double cz_ = v[0].x * v[1].y - v[1].x * v[0].y;
-        const double Hk = kkx * cx_ + kky * cy_ + kkz * cz_;
-        const double temp = a.e_per_mode / (2 * Ek);
-        const double sk = Hk / (km * Ek);
-        double alpha, beta;
-        if (fabs(sk * sk - 1) > 1e-5) {
-          alpha = temp * (1 - sk * a.eps_h) / (1 - sk * sk);
-          beta = temp * (a.eps_h - sk) / (1 - sk * sk);
-        } else {
-          alpha = temp / 2;
-          beta = alpha / (sk * km);
+      if (!a.gate || a.e_per_mode > 1e-15) {
+        const cx<double> u[3] = {v[0], v[1], v[2]};
+        cx<double> f[3] = {F[0], F[1], F[2]};
+        band_vector_force(a.mode, u, kkx, kky, kkz, km, a.e_per_mode, a.eps_h, f);
+        F[0] = f[0];
+        F[1] = f[1];
+        F[2] = f[2];
+      }
+      if (a.ns == 6 && a.e_per_mode_b > 1e-15) {
+        const cx<double> b[3] = {v[3], v[4], v[5]};
+        cx<double> f[3] = {F[3], F[4], F[5]};
+        band_vector_force(a.mode, b, kkx, kky, kkz, km, a.e_per_mode_b, a.eps_h_b, f);
+        F[3] = f[0];
+        F[4] = f[1];
+        F[5] = f[2];
+      } else if (a.ns == 4 && a.e_per_mode_b > 1e-15) {
+        const double Et = 0.5 * (v[3].x * v[3].x + v[3].y * v[3].y);
+        if (Et > 1e-15) {
+          const double al = a.mode == 1 ? a.e_per_mode_b / Et : sqrt(a.e_per_mode_b / Et);
+          F[3] = al * v[3];
         }
-        cx<double> w[3] = {mkc<double>(0, 0), mkc<double>(0, 0), mkc<double>(0, 0)};
-        if (beta > 1e-15) {
-          // vorticity i K x V (Compute_Modal_vorticity_FOUR four_basic.cc:166-186)
-          w[0] = ione(kky * v[2] - kkz * v[1]);
-          w[1] = ione(kkz * v[0] - kkx * v[2]);
-          w[2] = ione(kkx * v[1] - kky * v[0]);
-        }
-#pragma unroll
-        for (int c = 0; c < 3; ++c) F[c] = alpha * v[c] + beta * w[c];
       }
     }
-#pragma unroll
-    for (int c = 0; c < 3; ++c) a.FB[(long long)c * box + p] = F[c];
+    for (int c = 0; c < a.ns; ++c) a.FB[(long long)c * box + p] = F[c];
   }
   __syncthreads();
   // reality condition on the kz = 0 plane: F(kx, ky<0) = conj F(-kx, -ky); F(kx<0, 0) = conj F(-kx, 0)
@@ -385,8 +443,7 @@ __global__ void __launch_bounds__(TPB) k_force_supply(ForceArgs a) {
     const int mx = -kx, my = -ky;
     if (mx < -a.fx || mx > a.fx || my < -a.fy || my > a.fy) continue;
     const int pm = ((mx + a.fx) * ny + (my + a.fy)) * nz;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) a.FB[(long long)c * box + p] = conjc(a.FB[(long long)c * box + pm]);
+    for (int c = 0; c < a.ns; ++c) a.FB[(long long)c * box + p] = conjc(a.FB[(long long)c * box + pm]);
   }
 }
 

@@ -86,11 +86,16 @@ struct RKArgs {
 
 struct ForceArgs {
   Geo g;
-  const void* U[3];
+  const void* U[6];        // the state fields the force reads (ns of them)
+  int ns;                  // 3 fluid, 6 MHD (U, B), 4 passive scalar (U, T)
   int uprec;               // 0 FP64, 1 FP32
+  int mode;                // 1: energy-helicity supply (proc 1), 2: constant energy-helicity (proc 2)
+  int gate;                // skip U unless e_per_mode > MYEPS (all variants but proc 1 fluid)
   int fx, fy, fz;
-  double inner, outer, e_per_mode, eps_h;
-  cx<double>* FB;          // [3][box]
+  double inner, outer;
+  double e_per_mode, eps_h;      // U
+  double e_per_mode_b, eps_h_b;  // B (MHD) or e_per_mode_b = the scalar's energy per mode
+  cx<double>* FB;          // [ns][box]
 };
 
 // launchers (tg_spectral.cu)

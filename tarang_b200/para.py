@@ -187,8 +187,16 @@ def config_from_para(p: dict, kind: str = "FLUID") -> dict:
     proc = p["force_int"][1] if len(p["force_int"]) > 1 else 0
     fd = p["force_double"] + [0.0] * 7
     run_force = None
-    if proc == 1:
-        cfg["force"] = dict(inner=fd[1], outer=fd[2], eps=fd[3], eps_h=fd[4])
+    if proc in (1, 2) and kind != "RB":
+        # compute_force_ek_hk_supply.cc / compute_force_const_ek_hk.cc: force_double(1..4) for U,
+        # (5, 6) the energy and helicity ratio of W (MHD) or (5) the scalar's energy (scalar)
+        f = dict(kind="energy_supply" if proc == 1 else "energy_helicity", inner=fd[1], outer=fd[2], eps=fd[3],
+                 eps_h=fd[4])
+        if kind == "MHD":
+            f.update(eps_W=fd[5], eps_hW=fd[6])
+        elif kind == "SCALAR":
+            f.update(eps_T=fd[5])
+        cfg["force"] = f
     elif proc in (3, 4) and kind != "RB":
         # compute_force_TG.cc:47-92, compute_force_ABC.cc:50-131: k0, amplitudes (W: the next)
         cfg["force"] = dict(kind="modes")

@@ -65,11 +65,15 @@ def make_config(N, basis="FOUR", physics="FLUID", precision="FP64", dealias=True
     elif force.get("kind") == "rb_rotation":
         cfg.force_kind = L.TG_FORCE_RB_ROTATION    # buoyancy + scaled V x omega (proc 52)
         cfg.force_para[:3] = [float(x) for x in force["omega"]]
-    elif force.get("kind", "energy_supply") != "energy_supply":
+    elif force.get("kind", "energy_supply") not in ("energy_supply", "energy_helicity"):
         raise ValueError(f"force kind {force.get('kind')}")
     else:
-        cfg.force_kind = L.TG_FORCE_ENERGY_SUPPLY
-        p = [force.get("inner"), force.get("outer"), force.get("eps"), force.get("eps_h", 0.0)]
+        # force_field_proc 1 (energy supply) or 2 (constant energy and helicity): U's parameters,
+        # then B's (MHD) or the scalar's energy (passive scalar)
+        supply = force.get("kind", "energy_supply") == "energy_supply"
+        cfg.force_kind = L.TG_FORCE_ENERGY_SUPPLY if supply else L.TG_FORCE_ENERGY_HELICITY
+        p = [force.get("inner"), force.get("outer"), force.get("eps"), force.get("eps_h", 0.0),
+             force.get("eps_W", force.get("eps_T", 0.0)), force.get("eps_hW", 0.0)]
         cfg.force_para[:] = [float(x) for x in p]
     cfg.n_shells = int(n_shells)
     cfg.rb_ra = float(Ra)

@@ -286,13 +286,26 @@ def test_read_para_fluid(lib):
     assert p["out_k"] == [(1, 0, 1), (2, 1, 0)] and p["out_r"] == [(0, 0, 1)]
     c = config_from_para(p, "FLUID")
     assert c["N"] == (64, 32, 16) and c["nu"] == 0.003 and c["dt"] == 0.0005 and c["n_shells"] == 16
-    assert c["force"] == dict(inner=2.0, outer=3.0, eps=0.1, eps_h=0.0)
+    assert c["force"] == dict(kind="energy_supply", inner=2.0, outer=3.0, eps=0.1, eps_h=0.0)
     assert c["run"]["Tfinal"] == 0.25 and c["run"]["output_vx_vy"] == 1
     from tarang_b200.solver import make_config
     kw = dict(c)
     kw.pop("run")
     cfg = make_config(**kw)
     assert cfg.force_kind == L.TG_FORCE_ENERGY_SUPPLY and list(cfg.N) == [64, 32, 16]
+    # force_field_proc 2 (constant energy and helicity) with the same parameters; for MHD the
+    # next two are B's energy and helicity ratio, for a passive scalar the next one its energy
+    text2 = PARA.format(N1=64, N2=32, N3=16, Ra=0, Pr=0, basis="FOUR", nu=0.003, kappa=0, dt=0.0005, S=16, proc=2)
+    c2 = config_from_para(read_para(text2, n_fields=1), "FLUID")
+    assert c2["force"] == dict(kind="energy_helicity", inner=2.0, outer=3.0, eps=0.1, eps_h=0.0)
+    kw = dict(c2)
+    kw.pop("run")
+    assert make_config(**kw).force_kind == L.TG_FORCE_ENERGY_HELICITY
+    cm = make_config((16, 16, 16), physics="MHD", force=dict(kind="energy_helicity", inner=1.0, outer=2.0, eps=0.3,
+                                                                 eps_h=0.2, eps_W=0.4, eps_hW=-0.1))
+    assert list(cm.force_para) == [1.0, 2.0, 0.3, 0.2, 0.4, -0.1]
+    cs = make_config((16, 16, 16), physics="SCALAR", force=dict(inner=1.0, outer=2.0, eps=0.3, eps_T=0.5))
+    assert cs.force_kind == L.TG_FORCE_ENERGY_SUPPLY and list(cs.force_para) == [1.0, 2.0, 0.3, 0.0, 0.5, 0.0]
 
 
 def test_read_para_convection(lib):

@@ -242,3 +242,82 @@ def test_set_force_modes_errors(lib):
     with pytest.raises(L.TarangError) as e:
         make(N, physics="RB", basis="SCFT", Ra=1e4, Pr=1.0, dt=1e-4, force=dict(kind="coriolis", omega=(0, 0, 1)))
     assert e.value.code == L.TG_ERR_UNSUPPORTED
+
+
+BAND = [
+    ("FLUID", "energy_helicity", dict(eps=0.1, eps_h=0.3), "FP64", 1e-12),
+    ("FLUID", "energy_helicity", dict(eps=0.1, eps_h=0.3), "FP32", 1e-6),
+    ("MHD", "energy_supply", dict(eps=0.1, eps_h=0.2, eps_W=0.05, eps_hW=-0.4), "FP64", 1e-12),
+    ("MHD", "energy_helicity", dict(eps=0.1, eps_h=0.0, eps_W=0.05, eps_hW=0.5), "FP64", 1e-12),
+    ("SCALAR", "energy_supply", dict(eps=0.1, eps_h=0.0, eps_T=0.02), "FP64", 1e-12),
+    ("SCALAR", "energy_helicity", dict(eps=0.1, eps_h=0.1, eps_T=0.02), "FP64", 1e-12),
+]
+
+
+@pytest.mark.parametrize("physics,kind,par,precision,tol", BAND)
+def test_band_forcing_10_steps(lib, physics, kind, par, precision, tol):
+    """force_field_proc 1 (energy-helicity supply) and 2 (constant energy and helicity) on the
+    velocity, and on B (MHD) or the passive scalar with their own parameters: 10 steps against
+    the oracle's loops (MHDSolver, ScalarSolver)."""
+    N = (32, 32, 32)
+    force = dict(kind=kind, inner=2.0, outer=3.0, **par)
+    U = ic.random_phase_field(N, seed=51)
+    s = make(N, physics=physics, nu=2e-3, eta=3e-3, kappa=4e-3, dt=5e-4, force=force, precision=precision)
+    s.set_V(U)
+    if physics == "FLUID":
+        s.step(10)
+        ref = o.FluidSolver(N, KF, 2e-3, 5e-4, force=force)
+        Uw = U
+        for _ in range(10):
+            Uw, _ = ref.step(Uw)
+        assert rel_l2(s.get_V(), Uw) < tol
+    elif physics == "MHD":
+        W = ic.random_phase_field(N, seed=52, energy=0.3)
+        s.set_W(W)
+        s.step(10)
+        ref = o.MHDSolver(N, KF, 2e-3, 3e-3, 5e-4, force=force)
+        Uw, Ww = U, W
+        for _ in range(10):
+            Uw, Ww, _ = ref.step2(Uw, Ww)
+        assert rel_l2(s.get_V(), Uw) < tol
+        assert rel_l2(s.get_W(), Ww) < tol
+        # the magnetic force is on: without it B differs
+        ref0 = o.MHDSolver(N, KF, 2e-3, 3e-3, 5e-4, force=dict(force, eps_W=0.0))
+        U0, W0 = U, W
+        for _ in range(10):
+            U0, W0, _ = ref0.step2(U0, W0)
+        assert rel_l2(W0, Ww) > 1e-6
+    else:
+        T = ic.random_phase_field(N, k0=2.0, seed=53)[0]
+        s.set_T(T)
+        s.step(10)
+        ref = o.ScalarSolver(N, KF, 2e-3, 4e-3, 5e-4, force=force)
+        Uw, Tw = U, T
+        for _ in range(10):
+            Uw, Tw, _ = ref.step(Uw, Tw)
+        assert rel_l2(s.get_V(), Uw) < tol
+        assert rel_l2([s.get_T()], [Tw]) < tol
+        ref0 = o.ScalarSolver(N, KF, 2e-3, 4e-3, 5e-4, force=dict(force, eps_T=0.0))
+        U0, T0 = U, T
+        for _ in range(10):
+            U0, T0, _ = ref0.step(U0, T0)
+        assert rel_l2([T0], [Tw]) > 1e-6
+
+
+@pytest.mark.parametrize("precision,tol", [("FP64", 1e-12), ("FP32", 1e-6)])
+def test_passive_scalar_decay_10_steps(lib, precision, tol):
+    """The passive-scalar loop (Iscalar_main.cc:272-300) without forcing: u and T after 10 steps,
+    and the scalar's energy and dissipation."""
+    N = (32, 32, 64)
+    U = ic.random_phase_field(N, seed=54)
+    T = ic.random_phase_field(N, k0=3.0, seed=55)[0]
+    s = make(N, physics="SCALAR", nu=2e-3, kappa=5e-3, dt=5e-4, precision=precision)
+    s.set_V(U)
+    s.set_T(T)
+    s.step(10)
+    ref = o.ScalarSolver(N, KF, 2e-3, 5e-3, 5e-4)
+    Uw, Tw = U, T
+    for _ in range(10):
+        Uw, Tw, _ = ref.step(Uw, Tw)
+    assert rel_l2(s.get_V(), Uw) < tol
+    assert rel_l2([s.get_T()], [Tw]) < tol
