@@ -67,6 +67,9 @@ extern "C" {
                                  Taylor-Green, ABC and given-mode forcings (force_field_proc 3, 4, 5) */
 #define TG_FORCE_CORIOLIS 21  /* Force = V x Omega, Omega = force_para[0..2], evaluated from each RK
                                  stage's velocity (compute_force_Coriolis.cc:47-80) */
+#define TG_FORCE_LIQUID_METAL 101 /* Compute_force_Liquid_metal (compute_force_LM.cc:46-70), FOUR fluid:
+                                     Force = -(B0 . K)^2 / K^2 V, B0 = force_para[0..2], from each RK
+                                     stage's velocity */
 #define TG_FORCE_RB 51
 #define TG_FORCE_RB_ROTATION 52  /* convection with rotation (compute_force_RB.cc:132-195): the
                                     buoyancy of TG_FORCE_RB plus c V x Omega, Omega =

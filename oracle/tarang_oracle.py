@@ -793,6 +793,18 @@ def force_coriolis(V, omega):
     return [w2 * V[2] - w3 * V[1], w3 * V[0] - w1 * V[2], w1 * V[1] - w2 * V[0]]
 
 
+def force_liquid_metal(V, kfactor, B0):
+    """Compute_force_Liquid_metal  compute_force_LM.cc:46-70 with Array_mult_V0_khat_sqr_FOUR
+    four_basic.cc:413-439: Force = -(B0 . K)^2 / K^2 V (0 at K = 0), dealiased."""
+    N = (V[0].shape[0], V[0].shape[1], 2 * (V[0].shape[2] - 1))
+    Kx, Ky, Kz = kvec(N, kfactor)
+    K2 = Kx * Kx + Ky * Ky + Kz * Kz
+    bk = B0[0] * Kx + B0[1] * Ky + B0[2] * Kz
+    with np.errstate(divide="ignore", invalid="ignore"):
+        f = np.where(K2 > 0, bk * bk / K2, 0.0)
+    return [dealias(-f * v) for v in V]
+
+
 def _lx(k, N1, basis):
     return k if (basis == "SCFT" or k >= 0) else k + N1
 
@@ -860,6 +872,8 @@ def fluid_force(force, V, N, kfactor):
         return list(force["F"][:3])
     if kind == "coriolis":
         return force_coriolis(V, force["omega"])
+    if kind == "liquid_metal":
+        return force_liquid_metal(V, kfactor, force["B0"])
     raise ValueError(kind)
 
 

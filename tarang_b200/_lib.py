@@ -27,6 +27,7 @@ TG_FP64, TG_FP32_MIXED = 0, 1
 TG_RK4 = 4
 TG_FORCE_DECAY, TG_FORCE_ENERGY_SUPPLY, TG_FORCE_MODES, TG_FORCE_CORIOLIS, TG_FORCE_RB = 0, 1, 5, 21, 51
 TG_FORCE_ENERGY_HELICITY = 2
+TG_FORCE_LIQUID_METAL = 101
 TG_FORCE_RB_ROTATION = 52
 TG_FORCE_MODES_KMAX = 64
 TG_RING_MAX_SECTORS = 64

@@ -192,6 +192,8 @@ RKArgs rk_args(tg_ctx* c, int stage) {
   a.nu_tab = c->nu_tab;
   a.coriolis = c->coriolis ? 1 : 0;
   for (int i = 0; i < 3; ++i) a.om[i] = c->om[i];
+  a.lm = c->lm ? 1 : 0;
+  for (int i = 0; i < 3; ++i) a.b0[i] = c->b0[i];
   return a;
 }
 
@@ -727,6 +729,9 @@ int ctx_create_batch(const tg_config* cfg, int B, tg_ctx** out) {
   } else if (cfg->force_kind == TG_FORCE_MODES) {
     if (B != 1) return fail(set_err(c, TG_ERR_UNSUPPORTED, "forced requests are not batched"));
     c->force_on = 2;  // the box is allocated by tg_set_force_modes
+  } else if (cfg->force_kind == TG_FORCE_LIQUID_METAL) {
+    c->lm = true;
+    for (int i = 0; i < 3; ++i) c->b0[i] = cfg->force_para[i];
   } else if (cfg->force_kind == TG_FORCE_CORIOLIS || cfg->force_kind == TG_FORCE_RB_ROTATION) {
     c->coriolis = true;
     // Compute_force_RB_rotation scales the Coriolis force with the nondimensionalisation
@@ -759,6 +764,7 @@ int validate_config(const tg_config* cfg) {
   if (cfg->scheme != TG_RK4) return TG_ERR_UNSUPPORTED;
   if (cfg->force_kind != TG_FORCE_DECAY && cfg->force_kind != TG_FORCE_ENERGY_SUPPLY &&
       cfg->force_kind != TG_FORCE_ENERGY_HELICITY && cfg->force_kind != TG_FORCE_RB &&
+      cfg->force_kind != TG_FORCE_LIQUID_METAL &&
       cfg->force_kind != TG_FORCE_MODES && cfg->force_kind != TG_FORCE_CORIOLIS && cfg->force_kind != TG_FORCE_RB_ROTATION)
     return TG_ERR_UNSUPPORTED;
   if ((cfg->force_kind == TG_FORCE_RB || cfg->force_kind == TG_FORCE_RB_ROTATION) && cfg->physics != TG_RB)
@@ -769,9 +775,12 @@ int validate_config(const tg_config* cfg) {
   // convection has its own force (force_field_proc 51)
   if ((cfg->force_kind == TG_FORCE_MODES || cfg->force_kind == TG_FORCE_CORIOLIS) && cfg->physics == TG_RB)
     return TG_ERR_UNSUPPORTED;
-  if (cfg->force_kind == TG_FORCE_CORIOLIS)
+  if (cfg->force_kind == TG_FORCE_CORIOLIS || cfg->force_kind == TG_FORCE_LIQUID_METAL)
     for (int i = 0; i < 3; ++i)
       if (!std::isfinite(cfg->force_para[i])) return TG_ERR_ARG;
+  // the liquid-metal force is the fluid's force_field_proc 101 (FOUR: Array_mult_V0_khat_sqr_FOUR)
+  if (cfg->force_kind == TG_FORCE_LIQUID_METAL && (cfg->physics != TG_FLUID || cfg->basis != TG_FOUR))
+    return TG_ERR_UNSUPPORTED;
   if (cfg->force_kind == TG_FORCE_ENERGY_SUPPLY || cfg->force_kind == TG_FORCE_ENERGY_HELICITY) {
     // band forcings: FOUR; fluid, MHD and passive scalar (convection has its own force)
     if (cfg->basis != TG_FOUR || cfg->physics == TG_RB) return TG_ERR_UNSUPPORTED;
@@ -1029,6 +1038,24 @@ int tg_field_download(tg_ctx* c, int field, double* host, size_t n) {
       for (size_t q = 0; q < n; ++q) host[q] = c->om[a] * v[b][q] - c->om[b] * v[a][q];
       return TG_OK;
     }
+    if (c->lm && c->have_force) {
+      // Force = -(B0 . K)^2/K^2 V of the current velocity
+      int rc = tg_field_download(c, TG_V1 + (field - TG_FORCE1), host, n);
+      if (rc) return rc;
+      for (int l1 = 0; l1 < c->N1; ++l1)
+        for (int l2 = 0; l2 < c->N2; ++l2)
+          for (int l3 = 0; l3 < c->M3; ++l3) {
+            const double kx = (l1 <= c->N1 / 2 ? l1 : l1 - c->N1) * c->cfg.kfactor[0];
+            const double ky = (l2 <= c->N2 / 2 ? l2 : l2 - c->N2) * c->cfg.kfactor[1];
+            const double kz = l3 * c->cfg.kfactor[2];
+            const double K2 = kx * kx + ky * ky + kz * kz, bk = c->b0[0] * kx + c->b0[1] * ky + c->b0[2] * kz;
+            const double f = K2 > 0 ? -bk * bk / K2 : 0.0;
+            const size_t o = (((size_t)l1 * c->N2 + l2) * c->M3 + l3) * 2;
+            host[o] *= f;
+            host[o + 1] *= f;
+          }
+      return TG_OK;
+    }
     if (!c->force_on || !c->FB || (c->force_on == 1 && !c->have_force)) return TG_OK;
     std::vector<cx<double>> box((size_t)c->fbox);
     const int comp = field - TG_FORCE1;
@@ -1242,11 +1269,16 @@ int tg_add_force(tg_ctx* c) {
   if (!c) return TG_ERR_ARG;
   if (!c->have_nlin) return set_err(c, TG_ERR_STATE, "Add_force before Compute_nlin");
   cudaSetDevice(c->dev);
-  if ((c->force_on || c->coriolis) && !c->have_force) return set_err(c, TG_ERR_STATE, "Add_force before Compute_force");
+  if ((c->force_on || c->coriolis || c->lm) && !c->have_force)
+    return set_err(c, TG_ERR_STATE, "Add_force before Compute_force");
   if (c->force_on && c->FB) TG_CK(launch_sub_force_box(c->g, c->nstate, c->FB, c->fx, c->fy, c->fz, c->NL, c->st));
   if (c->coriolis) {
     const cx<double>* U[3] = {c->U0[0], c->U0[1], c->U0[2]};
     TG_CK(launch_sub_coriolis(c->g, c->NL, U, c->om, c->st));
+  }
+  if (c->lm) {
+    const cx<double>* U[3] = {c->U0[0], c->U0[1], c->U0[2]};
+    TG_CK(launch_sub_liquid_metal(c->g, c->NL, U, c->b0, c->st));
   }
   if (c->phys == TG_RB) {
     TG_CK(launch_rb_sub_force(c->g, c->NL, c->U0[0], c->U0[3], c->rb_fu, c->rb_ft, c->st));

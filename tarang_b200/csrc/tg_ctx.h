@@ -67,6 +67,8 @@ struct tg_ctx {
   bool force_ever = false;  // FB holds a force computed by this context
   bool coriolis = false;    // Force = V x om of every stage's velocity
   double om[3] = {0, 0, 0};
+  bool lm = false;  // liquid-metal force (force_field_proc 101, fluid)
+  double b0[3] = {0, 0, 0};
 
   // scalars and reductions
   double* scal = nullptr;   // per slot [8]: [0] dt, [1] t_now, [2] steps, [3] nonfinite, [4] Tdt

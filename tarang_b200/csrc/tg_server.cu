@@ -131,7 +131,9 @@ std::string batch_key(const tg_config& c, long long id) {
   std::string k(buf);
   if (c.force_kind == TG_FORCE_ENERGY_SUPPLY || c.force_kind == TG_FORCE_ENERGY_HELICITY)
     k += "|solo" + std::to_string(id);
-  if (c.force_kind == TG_FORCE_CORIOLIS || c.force_kind == TG_FORCE_RB_ROTATION) {
+  if (c.force_kind == TG_FORCE_CORIOLIS || c.force_kind == TG_FORCE_RB_ROTATION ||
+      c.force_kind == TG_FORCE_LIQUID_METAL) {
+    // Omega (Coriolis) or B0 (liquid metal): one value per batch
     std::snprintf(buf, sizeof(buf), "|om%a,%a,%a", c.force_para[0], c.force_para[1], c.force_para[2]);
     k += buf;
   }

@@ -225,6 +225,17 @@ __global__ void __launch_bounds__(TPB, RKOcc<PHYS>::v) k_rk(RKArgs a) {
         r[1] = r[1] - (a.om[2] * v[0] - a.om[0] * v[2]);
         r[2] = r[2] - (a.om[0] * v[1] - a.om[1] * v[0]);
       }
+      if (a.lm) {
+        // Compute_force_Liquid_metal (compute_force_LM.cc:46-70): Force = -(B0 . K)^2/K^2 V
+        // (Array_mult_V0_khat_sqr_FOUR four_basic.cc:413-439), then Add_force: nlin -= Force
+        const double bk = a.b0[0] * kx + a.b0[1] * ky + a.b0[2] * kz;
+        const double f = K2 > 0 ? bk * bk / K2 : 0.0;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const cx<double> v = a.inprec ? ldc<float>(a.IN[c], gi) : ldc<double>(a.IN[c], gi);
+          r[c] = r[c] + f * v;
+        }
+      }
       if constexpr (PHYS == PH_RB) {
         // Compute_force_RB (compute_force_RB.cc:51-105) from the stage's fields, then Add_force:
         // nlin1 -= fu * theta, T.nlin -= ft * u1
@@ -549,6 +560,18 @@ __global__ void k_rb_sub_force(Geo g, PtrArr6 pa, const cx<double>* u1, const cx
   pa.p[3][idx] = pa.p[3][idx] - ft * u1[idx];
 }
 
+__global__ void k_sub_liquid_metal(Geo g, PtrArr6 nl, PtrArr6 u, double b0, double b1, double b2) {
+  const long long idx = (long long)blockIdx.x * TPB + threadIdx.x;
+  if (idx >= g.S) return;
+  int r1, r2, l3;
+  compact_mode(g, idx, r1, r2, l3);
+  const double kx = geo_kx(g, r1) * g.kf0, ky = geo_ky(g, r2) * g.kf1, kz = l3 * g.kf2;
+  const double K2 = kx * kx + ky * ky + kz * kz, bk = b0 * kx + b1 * ky + b2 * kz;
+  const double f = K2 > 0 ? bk * bk / K2 : 0.0;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) nl.p[c][idx] = nl.p[c][idx] + f * u.p[c][idx];
+}
+
 __global__ void k_sub_coriolis(Geo g, PtrArr6 nl, PtrArr6 u, double o0, double o1, double o2) {
   const long long idx = (long long)blockIdx.x * TPB + threadIdx.x;
   if (idx >= g.S) return;
@@ -775,6 +798,17 @@ cudaError_t launch_rb_sub_force(const Geo& g, cx<double>* const* NL, const cx<do
   PtrArr6 pa{};
   for (int c = 0; c < 4; ++c) pa.p[c] = NL[c];
   k_rb_sub_force<<<nblk(g.S), TPB, 0, s>>>(g, pa, u1, th, fu, ft);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sub_liquid_metal(const Geo& g, cx<double>* const* NL, const cx<double>* const* U, const double* b0,
+                                    cudaStream_t s) {
+  PtrArr6 nl{}, u{};
+  for (int c = 0; c < 3; ++c) {
+    nl.p[c] = NL[c];
+    u.p[c] = const_cast<cx<double>*>(U[c]);
+  }
+  k_sub_liquid_metal<<<nblk(g.S), TPB, 0, s>>>(g, nl, u, b0[0], b0[1], b0[2]);
   return cudaGetLastError();
 }
 

@@ -82,6 +82,10 @@ struct RKArgs {
   // Coriolis force of the stage's velocity (Compute_force_Coriolis), when coriolis != 0
   int coriolis;
   double om[3];
+  // liquid-metal force -(B0 . K)^2 / K^2 V of the stage's velocity (Compute_force_Liquid_metal),
+  // when lm != 0
+  int lm;
+  double b0[3];
 };
 
 struct ForceArgs {
@@ -109,6 +113,9 @@ cudaError_t launch_sub_force_box(const Geo& g, int ncomp, const cx<double>* FB, 
 cudaError_t launch_pressure(const Geo& g, const cx<double>* const* NL, cx<double>* PR, cudaStream_t s);
 cudaError_t launch_rhs_from_nlin(const Geo& g, int phys, cx<double>* const* NL, const cx<double>* PR, cudaStream_t s);
 // NL[c] -= (U x om)[c], c < 3 (Add_force with the Coriolis force)
+// NL[c] -= -(B0 . K)^2/K^2 U[c], c < 3 (Add_force with the liquid-metal force)
+cudaError_t launch_sub_liquid_metal(const Geo& g, cx<double>* const* NL, const cx<double>* const* U, const double* b0,
+                                    cudaStream_t s);
 cudaError_t launch_sub_coriolis(const Geo& g, cx<double>* const* NL, const cx<double>* const* U, const double* om,
                                 cudaStream_t s);
 cudaError_t launch_rb_sub_force(const Geo& g, cx<double>* const* NL, const cx<double>* u1, const cx<double>* th,

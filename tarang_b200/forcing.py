@@ -17,6 +17,8 @@ Setup_ABC_force_field 122-170) and lib/IncFluid/force/compute_force_modes.cc:97-
 
 from __future__ import annotations
 
+import math
+
 import numpy as np
 
 _NSTATE = {"FLUID": 3, "MHD": 6, "SCALAR": 4}
@@ -104,6 +106,40 @@ def abc_modes(N, k0: int, amp: float, A: float, B: float, C: float, physics: str
     return _pack(modes, ns)
 
 
+def six_mode_table(k0: int, amp101: float, amp011: float, amp112: float, h: float) -> dict:
+    """The six modes of IncVF::Setup_SIX_MODE_force_field (force_model.cc:172-236) and
+    Setup_SIX_MODE_field (ic_model.cc:238-301), FOUR: {(kx, ky, kz): (V1, V2, V3)} at
+    (0, +-k0, k0), (+-k0, 0, k0) and (+-k0, +-k0, 2 k0) with f1 = 2 amp101/sqrt(2 + h^2),
+    f2 = 2 amp011/sqrt(2 + h^2), f3 = 4 amp112/sqrt(6 + 10 h^2).  The values are the reference's
+    table as written."""
+    f1 = 2.0 / math.sqrt(2 + h * h) * amp101
+    f2 = 2.0 / math.sqrt(2 + h * h) * amp011
+    f3 = 4.0 / math.sqrt(6 + 10 * h * h) * amp112
+    I = 1j
+    t = {
+        (0, k0, k0): (-h * f2 / 4 + 0j, I * f2 / 4, -I * f2 / 4),
+        (0, -k0, k0): (h * f2 / 4 + 0j, -I * f2 / 4, -I * f2 / 4),
+        (k0, 0, k0): (I * f1 / 4, -h * f1 / 4 + 0j, -I * f1 / 4),
+        (k0, k0, 2 * k0): (I * f3 / 8, I * f3 / 8 + h * f3 / 4, -I * f3 / 8 - h * f3 / 8),
+        (k0, -k0, 2 * k0): (I * f3 / 8, -I * f3 / 8 + h * f3 / 4, -I * f3 / 8 + h * f3 / 8),
+        (-k0, 0, k0): (-I * f1 / 4, h * f1 / 4 + 0j, -I * f1 / 4),
+        (-k0, k0, 2 * k0): (-I * f3 / 8, I * f3 / 8 - h * f3 / 4, -I * f3 / 8 + h * f3 / 8),
+        (-k0, -k0, 2 * k0): (-I * f3 / 8, -I * f3 / 8 - h * f3 / 4, -I * f3 / 8 - h * f3 / 8),
+    }
+    return t
+
+
+def six_mode_modes(N, k0: int, amp101: float, amp011: float, amp112: float, h: float, physics: str = "MHD"):
+    """Compute_force_DYNAMO_SIX_MODE (compute_force_dynamo_6mode.cc:45-80): the six-mode force on
+    the velocity only (B's force zero), as (k, F) for IncFluid.set_force_modes."""
+    ns = _nstate(physics)
+    modes: dict = {}
+    for key, vals in six_mode_table(k0, amp101, amp011, amp112, h).items():
+        for c, v in enumerate(vals):
+            _set(modes, key, c, v, ns)
+    return _pack(modes, ns)
+
+
 def _dx(basis, kfactor, kx, v):
     """DxVx (universal_inline.h): FOUR i kx kf1 v, SCFT kx kf1 v."""
     return (1j * kx * kfactor[0] * v) if basis == "FOUR" else (kx * kfactor[0] * v)
@@ -121,11 +157,27 @@ def last_component(kx, ky, kz, Fx, Fy, kfactor, basis="FOUR"):
     return Fx, _dx(basis, kfactor, kx, Fx) / (-1j * ky * kfactor[1]), Fz
 
 
-def given_modes(entries, N, kfactor=(1.0, 1.0, 1.0), basis: str = "FOUR", physics: str = "FLUID"):
+def compute_vyvz(kx, ky, kz, Vx, Omega, kfactor, basis="FOUR"):
+    """IncVF::Compute_VyVz (field_k_fns.cc:126-157): the (Vx, Vy, Vz) of a divergence-free mode
+    with the given Vx and x-vorticity Omega, K_perp^2 = Ky^2 + Kz^2:
+    Vy = (i Ky DxVx + i Kz Omega)/K_perp^2, Vz = (i Kz DxVx - i Ky Omega)/K_perp^2; on the kx axis
+    (ky = kz = 0) all three are 0."""
+    Ky, Kz = ky * kfactor[1], kz * kfactor[2]
+    kp2 = Ky * Ky + Kz * Kz
+    if ky == 0 and kz == 0:
+        return 0j, 0j, 0j
+    d = _dx(basis, kfactor, kx, Vx)
+    return Vx, (1j * Ky * d + 1j * Kz * Omega) / kp2, (1j * Kz * d - 1j * Ky * Omega) / kp2
+
+
+def given_modes(entries, N, kfactor=(1.0, 1.0, 1.0), basis: str = "FOUR", physics: str = "FLUID",
+                rule: str = "simple"):
     """Compute_force_given_modes_SIMPLE (compute_force_modes.cc:97-440): entries are
     (kx, ky, kz, Fx, Fy) for a fluid, (kx, ky, kz, Fx, Fy, FxW, FyW) for MHD and
     (kx, ky, kz, Fx, Fy, G) for a scalar.  Each vector's third component comes from
-    Last_component; on the kz = 0 and kz = N3/2 planes the conjugate mode is added to the force
+    Last_component.  rule "vorticity": Compute_force_given_modes_VORTICITY (:470-700), the second
+    value of each vector is its x-vorticity and Compute_VyVz gives (Fx, Fy, Fz).  On the kz = 0
+    and kz = N3/2 planes the conjugate mode is added to the force
     (FOUR: F(-kx, -ky, kz) = F*; SCFT: F(kx, -ky, kz) = F*, or on ky = 0 F1 = 0 and the
     imaginary parts of F2, F3 and G dropped), which is what Assign_force_and_comp_conj
     (field_k_fns.cc:462-500) states as its purpose."""
@@ -134,9 +186,10 @@ def given_modes(entries, N, kfactor=(1.0, 1.0, 1.0), basis: str = "FOUR", physic
     modes: dict = {}
     for e in entries:
         kx, ky, kz = (int(x) for x in e[:3])
-        vals = list(last_component(kx, ky, kz, complex(e[3]), complex(e[4]), kfactor, basis))
+        third = compute_vyvz if rule == "vorticity" else last_component
+        vals = list(third(kx, ky, kz, complex(e[3]), complex(e[4]), kfactor, basis))
         if ns == 6:
-            vals += list(last_component(kx, ky, kz, complex(e[5]), complex(e[6]), kfactor, basis))
+            vals += list(third(kx, ky, kz, complex(e[5]), complex(e[6]), kfactor, basis))
         elif ns == 4:
             vals.append(complex(e[5]))
         for c, v in enumerate(vals):

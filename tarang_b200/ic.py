@@ -1,7 +1,8 @@
 """Initial conditions (host side, numpy; outside the hot path): the benchmark configurations and
 the reference's initial-condition procedures (IncFluid::Read_init_cond init_cond_main.cc:52-206,
-field_input_proc 1 field file, 2 reduced field file, 3 given modes, 5 energy spectrum, 7
-Taylor-Green, 8 ABC, 51 RB Lorenz modes), returned as the state fields in the reference layout.
+field_input_proc 1 field file, 2 reduced field file, 3 and 4 given modes, 5 energy spectrum, 6
+energy-helicity spectrum, 7 Taylor-Green, 8 ABC, 51 RB Lorenz modes), returned as the state
+fields in the reference layout.
 
 * Taylor-Green: the spectral placement of IncVF::Setup_Taylor_Green_field
   (lib/IncFlow/misc/ic_model.cc:58-89): u = amp sin(k0 x) cos(k0 y) cos(k0 z),
@@ -129,11 +130,9 @@ def random_phase_field(N, kfactor=(1.0, 1.0, 1.0), k0=4.0, energy=0.5, seed=2026
     return [np.ascontiguousarray(v * s) for v in V]
 
 
-def _random_phase(N, kfactor, shell_energy, seed, dealias):
-    """Random phases with the energy shell_energy(ceil|K|) spread over the shell's
-    Approx_number_modes_in_shell (see the module docstring)."""
+def _shell_amp(N, kfactor, shell_energy):
+    """(amp, |K|): amp = sqrt(2 E(ceil|K|) / Approx_number_modes_in_shell) per stored mode."""
     N1, N2, N3 = N
-    rng = np.random.Generator(np.random.PCG64(seed))
     Kx, Ky, Kz = _k_grids(N, kfactor)
     shape = (N1, N2, N3 // 2 + 1)
     Kx = np.broadcast_to(Kx, shape)
@@ -143,10 +142,22 @@ def _random_phase(N, kfactor, shell_energy, seed, dealias):
     idx = np.ceil(K)
     Ek = shell_energy(idx)
     approx = 2 * math.pi * np.maximum(idx, 1) ** 2 / (kfactor[0] * kfactor[1] * kfactor[2])
-    amp = np.sqrt(2 * Ek / approx)
-    ph = rng.random((3,) + shape) * 2 * math.pi
-    u1 = amp * np.exp(1j * ph[0]) * np.cos(ph[2])
-    u2 = amp * np.exp(1j * ph[1]) * np.sin(ph[2])
+    return np.sqrt(2 * Ek / approx), K
+
+
+def _put_vector(N, kfactor, amp, ph1, ph2, ph3, dealias):
+    """Put_vector_amp_phase_comp_conj (ic_amp_phase.cc:54-157, anisotropy axis x) on every mode:
+    uperp1 = amp e^{i ph1} cos(ph3), uperp2 = amp e^{i ph2} sin(ph3) turned into (Vx, Vy, Vz) by
+    the polar and azimuthal angles of K; origin zeroed, dealiased, reality condition."""
+    N1, N2, N3 = N
+    Kx, Ky, Kz = _k_grids(N, kfactor)
+    shape = (N1, N2, N3 // 2 + 1)
+    Kx = np.broadcast_to(Kx, shape)
+    Ky = np.broadcast_to(Ky, shape)
+    Kz = np.broadcast_to(Kz, shape)
+    K = np.sqrt(Kx * Kx + Ky * Ky + Kz * Kz)
+    u1 = amp * np.exp(1j * ph1) * np.cos(ph3)
+    u2 = amp * np.exp(1j * ph2) * np.sin(ph3)
     # polar angle from the x axis, azimuth in the (y, z) plane (anisotropy switch 1)
     kperp = np.sqrt(Ky * Ky + Kz * Kz)
     with np.errstate(invalid="ignore", divide="ignore"):
@@ -166,6 +177,25 @@ def _random_phase(N, kfactor, shell_energy, seed, dealias):
         keep = keep_mask(N)
         V = [np.where(keep, v, 0) for v in V]
     return [np.ascontiguousarray(reality_kz0(v)) for v in V]
+
+
+def _put_scalar(N, kfactor, amp, ph, dealias):
+    """Put_scalar_amp_phase_comp_conj (ic_amp_phase.cc): F = amp e^{i ph}; origin zeroed,
+    dealiased, reality condition."""
+    _, K = _shell_amp(N, kfactor, lambda idx: idx)
+    F = np.where(K <= 1e-15, 0, amp * np.exp(1j * ph))
+    if dealias:
+        F = np.where(keep_mask(N), F, 0)
+    return np.ascontiguousarray(reality_kz0(F))
+
+
+def _random_phase(N, kfactor, shell_energy, seed, dealias):
+    """Random phases with the energy shell_energy(ceil|K|) spread over the shell's
+    Approx_number_modes_in_shell (see the module docstring)."""
+    amp, _ = _shell_amp(N, kfactor, shell_energy)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ph = rng.random((3,) + amp.shape) * 2 * math.pi
+    return _put_vector(N, kfactor, amp, ph[0], ph[1], ph[2], dealias)
 
 
 # --------------------------------------------------------------------------------------------
@@ -227,13 +257,14 @@ def abc_field(N, k0, amp, A, B, C, physics="FLUID", ampW=0.0):
     return out
 
 
-def modes_field(entries, N, kfactor=(1.0, 1.0, 1.0), basis="FOUR", physics="FLUID"):
+def modes_field(entries, N, kfactor=(1.0, 1.0, 1.0), basis="FOUR", physics="FLUID", rule="simple"):
     """Init_cond_modes_SIMPLE (init_cond_modes.cc:107-480): entries (kx, ky, kz, Vx, Vy[, Wx, Wy
     | G]) as in_field_in.d lists them; Last_component gives each vector's third component and
     Add_complex_conj the conjugate mode on the kz = 0 and kz = N3/2 planes (the same rules as the
-    given-mode force, forcing.given_modes)."""
+    given-mode force, forcing.given_modes).  rule "vorticity": Init_cond_modes_VORTICITY
+    (:520-760), entries (kx, ky, kz, Vx, Omega_x[, Wx, OmegaW_x | G]) through Compute_VyVz."""
     from . import forcing
-    k, F = forcing.given_modes(entries, N, kfactor, basis, physics)
+    k, F = forcing.given_modes(entries, N, kfactor, basis, physics, rule)
     return modes_to_fields(k, F, N, basis)
 
 
@@ -244,14 +275,73 @@ def model_shell_spectrum(n, a):
     return a * kk ** 4 * np.exp(-0.02 * kk ** 1.1) / (kk ** 4 + 1.5 ** 4) ** (1.0 + 2.8 / 12.0)
 
 
-def energy_spectrum_field(N, a, kfactor=(1.0, 1.0, 1.0), seed=20261202, dealias=True):
-    """Init_cond_energy_spectrum (init_cond_energy.cc:65-138, FOUR): the energy of shell ceil|K|
-    of the model spectrum, divided equally among the shell's modes, with random phases
-    (Put_vector_amp_phase_comp_conj), the mean mode zero, dealiased, reality condition.  The
-    reference seeds from time(0); numpy's PCG64 with `seed` stands in.  Returns [V1, V2, V3]."""
+def _model_spectrum(N, kfactor, a):
     kmax = int(math.ceil(math.sqrt(sum((N[i] // 2 * kfactor[i]) ** 2 for i in range(3))))) + 2
     Sk = model_shell_spectrum(kmax + 1, a)
-    return _random_phase(N, kfactor, lambda idx: Sk[np.minimum(idx.astype(int), kmax)], seed, dealias)
+    return lambda idx: Sk[np.minimum(idx.astype(int), kmax)]
+
+
+def energy_spectrum_field(N, a, kfactor=(1.0, 1.0, 1.0), seed=20261202, dealias=True, physics="FLUID", a2=0.0):
+    """Init_cond_energy_spectrum (init_cond_energy.cc:65-138, FOUR): the energy of shell ceil|K|
+    of the model spectrum, divided equally among the shell's modes, with random phases
+    (Put_vector_amp_phase_comp_conj), the mean mode zero, dealiased, reality condition.  MHD
+    (:318-413): W the same with the model spectrum of a2 = init_cond_double_para(2); passive
+    scalar (Init_cond_energy_spectrum_scalar :152-223): T = ampT e^{i phaseT} with the spectrum
+    of a2.  The reference seeds from time(0); numpy's PCG64 with `seed` stands in.  Returns the
+    state fields [V1, V2, V3(, W1, W2, W3 | , T)]."""
+    amp, _ = _shell_amp(N, kfactor, _model_spectrum(N, kfactor, a))
+    ns = _state_count(physics)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ph = rng.random(({3: 3, 6: 6, 4: 4}[ns],) + amp.shape) * 2 * math.pi
+    out = _put_vector(N, kfactor, amp, ph[0], ph[1], ph[2], dealias)
+    if ns == 6:
+        ampW, _ = _shell_amp(N, kfactor, _model_spectrum(N, kfactor, a2))
+        out += _put_vector(N, kfactor, ampW, ph[3], ph[4], ph[5], dealias)
+    elif ns == 4:
+        ampT, _ = _shell_amp(N, kfactor, _model_spectrum(N, kfactor, a2))
+        out.append(_put_scalar(N, kfactor, ampT, ph[3], dealias))
+    return out
+
+
+def energy_helicity_spectrum_field(N, a, sk, kfactor=(1.0, 1.0, 1.0), seed=20261202, dealias=True, physics="FLUID",
+                                   a2=0.0, skW=0.0, h=0.0):
+    """Init_cond_energy_helicity_spectrum (init_cond_energy.cc:519-590, FOUR): as
+    energy_spectrum_field with phase2 = phase1 + pi/2 and phase3 = asin(sk)/2, so every mode
+    carries the relative helicity sk.  MHD (:721-824): W from the spectrum of a2 with
+    zeta_b = asin(skW)/2, phase1W = phase1 - acos(h / cos(zeta - zeta_b)), phase2W = phase1W + pi/2
+    (h = 2 Hc/(amp ampW)); passive scalar (:604-681): T with the spectrum of a2 and a random phase.
+    Returns the state fields."""
+    amp, _ = _shell_amp(N, kfactor, _model_spectrum(N, kfactor, a))
+    ns = _state_count(physics)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ph1 = rng.random(amp.shape) * 2 * math.pi
+    zeta = math.asin(sk) / 2.0
+    out = _put_vector(N, kfactor, amp, ph1, ph1 + math.pi / 2, np.full(amp.shape, zeta), dealias)
+    if ns == 6:
+        ampW, _ = _shell_amp(N, kfactor, _model_spectrum(N, kfactor, a2))
+        zb = math.asin(skW) / 2.0
+        p1w = ph1 - math.acos(h / math.cos(zeta - zb))
+        out += _put_vector(N, kfactor, ampW, p1w, p1w + math.pi / 2, np.full(amp.shape, zb), dealias)
+    elif ns == 4:
+        ampT, _ = _shell_amp(N, kfactor, _model_spectrum(N, kfactor, a2))
+        out.append(_put_scalar(N, kfactor, ampT, rng.random(amp.shape) * 2 * math.pi, dealias))
+    return out
+
+
+def six_mode_field(N, k0, amp, ampW=None):
+    """Init_cond_DYNAMO_SIX_MODE (init_cond_dynamo_6mode.cc:45-70, FOUR): V and W from
+    Setup_SIX_MODE_field with amp = (amp101, amp011, amp112, h) and ampW likewise (W zero when
+    ampW is None).  Returns [V1, V2, V3, W1, W2, W3]."""
+    from . import forcing
+    N1, N2, N3 = N
+    out = [np.zeros((N1, N2, N3 // 2 + 1), dtype=np.complex128) for _ in range(6)]
+    for g, a in ((0, amp), (3, ampW)):
+        if a is None:
+            continue
+        for (kx, ky, kz), vals in forcing.six_mode_table(int(k0), *a).items():
+            for c, v in enumerate(vals):
+                out[g + c][kx % N1, ky % N2, kz] = v
+    return out
 
 
 def rb_lorenz_field(N, W101, T101, T200, kfactor=(1.0, 1.0, 1.0)):
@@ -277,24 +367,30 @@ def read_init_cond(cfg, data_dir=".", seed=20261202):
     proc = run.get("field_input_proc", 0)
     N, basis, physics = tuple(cfg["N"]), cfg.get("basis", "FOUR"), cfg.get("physics", "FLUID")
     kf = tuple(cfg.get("kfactor", (1.0, 1.0, 1.0)))
-    dp = list(run.get("init_cond_double", [])) + [0.0] * 8
+    dp = list(run.get("init_cond_double", [])) + [0.0] * 10
     path = os.path.join(data_dir, "in", "field_in.d")
     ns = _state_count(physics)
     if proc in (1, 2):
         from .solver import read_field_file
         red = run.get("N_in_reduced") if proc == 2 else None
         return read_field_file(path, N, ns, basis, kf, bool(run.get("input_vx_vy", 0)), red)
-    if proc == 3:
+    if proc in (3, 4):
         from . import forcing
         nv = {3: 2, 6: 4, 4: 3}[ns]
-        return modes_field(forcing.read_force_modes_file(path, N[0], nv), N, kf, basis, physics)
-    if proc == 5 and ns == 3 and basis == "FOUR":
-        return energy_spectrum_field(N, dp[1], kf, seed)
+        return modes_field(forcing.read_force_modes_file(path, N[0], nv), N, kf, basis, physics,
+                           "simple" if proc == 3 else "vorticity")
+    if proc == 5 and basis == "FOUR" and physics.upper() != "RB":
+        return energy_spectrum_field(N, dp[1], kf, seed, physics=physics, a2=dp[2])
+    if proc == 6 and basis == "FOUR" and physics.upper() != "RB":
+        # fluid: a, sk; scalar: a, sk, a_T; MHD: a, sk, a_W, skW, h
+        return energy_helicity_spectrum_field(N, dp[1], dp[2], kf, seed, physics=physics, a2=dp[3], skW=dp[4], h=dp[5])
     if proc == 7 and physics.upper() != "RB":
         # (convection: Init_cond_Taylor_Green_RB recurses into itself in the reference)
         return taylor_green_field(N, int(dp[1]), dp[2], basis, physics, dp[3])
     if proc == 8 and basis == "FOUR":
         return abc_field(N, int(dp[1]), dp[5], dp[2], dp[3], dp[4], physics, dp[6])
+    if proc == 101 and physics.upper() == "MHD" and basis == "FOUR":
+        return six_mode_field(N, int(dp[1]), tuple(dp[2:6]), tuple(dp[6:10]))
     if proc == 51 and physics.upper() == "RB":
         return rb_lorenz_field(N, dp[1], dp[2], dp[3], kf)
     raise ValueError(f"field_input_proc {proc} ({physics}, {basis}) is not built")

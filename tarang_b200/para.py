@@ -204,10 +204,19 @@ def config_from_para(p: dict, kind: str = "FLUID") -> dict:
             run_force = dict(kind="taylor_green", k0=int(fd[1]), amp=fd[2], ampW=fd[3])
         else:
             run_force = dict(kind="abc", k0=int(fd[1]), A=fd[2], B=fd[3], C=fd[4], amp=fd[5], ampW=fd[6])
-    elif proc == 5 and kind != "RB":
-        # the modes come from in/force_field_in.d (forcing.read_force_modes_file)
+    elif proc in (5, 6) and kind != "RB":
+        # the modes come from in/force_field_in.d (forcing.read_force_modes_file); proc 6 gives
+        # each vector's x-vorticity in place of its y component (Compute_VyVz)
         cfg["force"] = dict(kind="modes")
-        run_force = dict(kind="given_modes", file="in/force_field_in.d")
+        run_force = dict(kind="given_modes", file="in/force_field_in.d", rule="simple" if proc == 5 else "vorticity")
+    elif proc == 101 and kind == "FLUID":
+        # Compute_force_Liquid_metal (compute_force_LM.cc:46-70): B0 = force_double(1..3)
+        cfg["force"] = dict(kind="liquid_metal", B0=(fd[1], fd[2], fd[3]))
+    elif proc == 101 and kind == "MHD":
+        # Compute_force_DYNAMO_SIX_MODE (compute_force_dynamo_6mode.cc:45-80): k0, amp101,
+        # amp011, amp112, h
+        cfg["force"] = dict(kind="modes")
+        run_force = dict(kind="six_mode", k0=int(fd[1]), amp=(fd[2], fd[3], fd[4], fd[5]))
     elif proc == 21 and kind != "RB":
         # compute_force_Coriolis.cc:47-80 takes the number of components from force_int(1),
         # which is also force_field_proc (21), so as written it sets neither branch; the
@@ -256,10 +265,15 @@ def force_modes_for(cfg: dict, data_dir: str = "."):
     N, basis, physics = cfg["N"], cfg.get("basis", "FOUR"), cfg.get("physics", "FLUID")
     if fm["kind"] == "taylor_green":
         return forcing.taylor_green_modes(N, fm["k0"], fm["amp"], basis, physics, fm["ampW"])
+    if fm["kind"] == "six_mode":
+        if basis != "FOUR":
+            raise ValueError("the six-mode force is FOUR only (force_model.cc:238-243)")
+        return forcing.six_mode_modes(N, fm["k0"], *fm["amp"], physics=physics)
     if fm["kind"] == "abc":
         if basis != "FOUR":
             raise ValueError("ABC forcing is FOUR only (force_model.cc:164-168)")
         return forcing.abc_modes(N, fm["k0"], fm["amp"], fm["A"], fm["B"], fm["C"], physics, fm["ampW"])
     n_values = {"FLUID": 2, "MHD": 4, "SCALAR": 3}[physics]
     entries = forcing.read_force_modes_file(os.path.join(data_dir, fm["file"]), N[0], n_values)
-    return forcing.given_modes(entries, N, cfg.get("kfactor", (1.0, 1.0, 1.0)), basis, physics)
+    return forcing.given_modes(entries, N, cfg.get("kfactor", (1.0, 1.0, 1.0)), basis, physics,
+                               fm.get("rule", "simple"))

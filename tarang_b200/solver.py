@@ -62,6 +62,9 @@ def make_config(N, basis="FOUR", physics="FLUID", precision="FP64", dealias=True
     elif force.get("kind") == "coriolis":
         cfg.force_kind = L.TG_FORCE_CORIOLIS       # Force = V x omega (force_field_proc 21)
         cfg.force_para[:3] = [float(x) for x in force["omega"]]
+    elif force.get("kind") == "liquid_metal":
+        cfg.force_kind = L.TG_FORCE_LIQUID_METAL   # -(B0 . K)^2/K^2 V (force_field_proc 101)
+        cfg.force_para[:3] = [float(x) for x in force["B0"]]
     elif force.get("kind") == "rb_rotation":
         cfg.force_kind = L.TG_FORCE_RB_ROTATION    # buoyancy + scaled V x omega (proc 52)
         cfg.force_para[:3] = [float(x) for x in force["omega"]]

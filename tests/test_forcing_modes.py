@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from oracle import tarang_oracle as o
-from tarang_b200 import forcing
+from tarang_b200 import forcing, ic
 
 
 def dense(k, F, N, comp, basis="FOUR"):
@@ -102,6 +102,33 @@ def test_given_modes_mhd_and_scalar():
     assert F.shape == (2, 4) and F[0, 3] == 0.5j and F[1, 3] == -0.5j
 
 
+@pytest.mark.parametrize("basis", ["FOUR", "SCFT"])
+def test_given_modes_vorticity(basis):
+    """Compute_force_given_modes_VORTICITY / Init_cond_modes_VORTICITY: (Vx, Omega_x) give a
+    divergence-free mode whose x-vorticity i(Ky Vz - Kz Vy) is Omega_x; on the kx axis the mode
+    is zero (Compute_VyVz); the conjugates on kz = 0 follow the same rule as the simple modes."""
+    N = (16, 16, 16)
+    kf = (1.0, 0.5, 2.0)
+    entries = [(1, 2, 3, 0.3 + 0.1j, -0.2 + 0.4j), (2, 1, 0, 0.5 + 0.2j, 0.1 - 0.3j), (3, 0, 0, 0.7, 0.2)]
+    k, F = forcing.given_modes(entries, N, kf, basis, rule="vorticity")
+    kk = {tuple(x): f for x, f in zip(k.tolist(), F)}
+    for (kx, ky, kz, vx, om) in entries[:2]:
+        f = kk[(kx, ky, kz)]
+        dx = (1j * kx * kf[0] * f[0]) if basis == "FOUR" else (kx * kf[0] * f[0])
+        assert abs(dx + 1j * ky * kf[1] * f[1] + 1j * kz * kf[2] * f[2]) < 1e-14
+        assert abs(1j * (ky * kf[1] * f[2] - kz * kf[2] * f[1]) - om) < 1e-14 and f[0] == vx
+    assert np.all(kk[(3, 0, 0)] == 0)
+    conj = (-2, -1, 0) if basis == "FOUR" else (2, -1, 0)
+    assert np.array_equal(kk[conj], np.conj(kk[(2, 1, 0)]))
+    # MHD: each vector by its own (x, Omega_x); scalar: G as given
+    k, F = forcing.given_modes([(1, 1, 1, 0.1, 0.2, 0.3, 0.4)], N, physics="MHD", rule="vorticity")
+    assert abs(1j * (F[0, 5] - F[0, 4]) - 0.4) < 1e-15 and abs(1j * (F[0, 2] - F[0, 1]) - 0.2) < 1e-15
+    k, F = forcing.given_modes([(1, 1, 2, 0.1, 0.2, 0.5j)], N, physics="SCALAR", rule="vorticity")
+    assert F[0, 3] == 0.5j
+    V = ic.modes_field(entries, N, kf, basis, rule="vorticity")
+    assert V[1][2, 1, 0] == kk[(2, 1, 0)][1]
+
+
 def test_read_force_modes_file(tmp_path):
     p = tmp_path / "force_field_in.d"
     p.write_text("1 2 3 (0.5,0.25) (1,-1)\n2 0 0 (0.1,0) 2.0\n64 0 0\n5 5 5 (9,9) (9,9)\n")
@@ -144,8 +171,10 @@ def test_para_force_procs(lib):
     kw.pop("run")
     cfg = make_config(**kw)
     assert cfg.force_kind == L.TG_FORCE_CORIOLIS and list(cfg.force_para[:3]) == [0.0, 0.0, 3.0]
+    c = cfg_for(6, [0.0])
+    assert c["force"] == dict(kind="modes") and c["run"]["force_modes"]["rule"] == "vorticity"
     with pytest.raises(ValueError):
-        cfg_for(6, [0.0])
+        cfg_for(7, [0.0])
 
 
 def test_coriolis_oracle_identities():
@@ -198,3 +227,39 @@ def test_para_rb_rotation(lib):
     kw.pop("run")
     cfg = make_config(**kw)
     assert cfg.force_kind == L.TG_FORCE_RB_ROTATION and list(cfg.force_para[:3]) == [0.0, 0.0, 4.0]
+
+
+def test_six_mode_force_and_field():
+    """Setup_SIX_MODE_force_field / Setup_SIX_MODE_field: eight divergence-free modes off the kz = 0
+    plane; the dynamo force (proc 101, MHD) drives the velocity only; the initial condition
+    (field_input_proc 101) fills V and W from their own amplitudes."""
+    N = (16, 16, 16)
+    t = forcing.six_mode_table(2, 0.3, 0.5, 0.7, 0.4)
+    assert len(t) == 8
+    for (kx, ky, kz), v in t.items():
+        assert kz > 0 and abs(kx * v[0] + ky * v[1] + kz * v[2]) < 1e-15
+    k, F = forcing.six_mode_modes(N, 2, 0.3, 0.5, 0.7, 0.4)
+    assert F.shape == (8, 6) and np.all(F[:, 3:] == 0)
+    f = ic.six_mode_field(N, 2, (0.3, 0.5, 0.7, 0.4), (0.1, 0.2, 0.3, -0.5))
+    assert f[0][2, 0, 2] == t[(2, 0, 2)][0] and f[4][(-2) % 16, 2, 4] == forcing.six_mode_table(2, 0.1, 0.2, 0.3, -0.5)[(-2, 2, 4)][1]
+
+
+def test_para_liquid_metal_and_six_mode(lib):
+    from tests.test_field_io import PARA
+    from tarang_b200.para import config_from_para, force_modes_for, read_para
+    from tarang_b200.solver import make_config
+    from tarang_b200 import _lib as L
+    t = PARA.format(N1=32, N2=32, N3=32, Ra=0, Pr=0, basis="FOUR", nu=0.01, kappa=0, dt=1e-3, S=12, proc=101)
+    t = t.replace("(3)force-float	2.0	3.0	0.1	0.0", "(3)force-float	1.0	0.0	2.0	0.5	0.25")
+    t = t.replace("(1)force-meta	1	4	1", "(1)force-meta	1	5	1")
+    c = config_from_para(read_para(t, n_fields=1), "FLUID")
+    assert c["force"] == dict(kind="liquid_metal", B0=(1.0, 0.0, 2.0))
+    kw = dict(c)
+    kw.pop("run")
+    cfg = make_config(**kw)
+    assert cfg.force_kind == L.TG_FORCE_LIQUID_METAL and list(cfg.force_para[:3]) == [1.0, 0.0, 2.0]
+    c = config_from_para(read_para(t, n_fields=2), "MHD")
+    assert c["force"] == dict(kind="modes") and c["run"]["force_modes"]["kind"] == "six_mode"
+    k, F = force_modes_for(c)
+    k2, F2 = forcing.six_mode_modes((32, 32, 32), 1, 0.0, 2.0, 0.5, 0.25)
+    assert np.array_equal(k, k2) and np.array_equal(F, F2)

@@ -321,3 +321,40 @@ def test_passive_scalar_decay_10_steps(lib, precision, tol):
         Uw, Tw, _ = ref.step(Uw, Tw)
     assert rel_l2(s.get_V(), Uw) < tol
     assert rel_l2([s.get_T()], [Tw]) < tol
+
+
+@pytest.mark.parametrize("precision,tol", [("FP64", 1e-12), ("FP32", 1e-6)])
+def test_liquid_metal_10_steps(lib, precision, tol):
+    """force_field_proc 101 for a fluid (Compute_force_Liquid_metal): Force = -(B0 . K)^2/K^2 V
+    from each RK stage's velocity; 10 steps against the oracle, and the damping it adds."""
+    N = (32, 32, 32)
+    B0 = (0.0, 0.5, 2.0)
+    V = ic.random_phase_field(N, seed=61)
+    s = make(N, nu=4e-3, dt=5e-4, force=dict(kind="liquid_metal", B0=B0), precision=precision)
+    s.set_V(V)
+    s.step(10)
+    ref = o.FluidSolver(N, KF, 4e-3, 5e-4, force=dict(kind="liquid_metal", B0=B0))
+    Vw = V
+    for _ in range(10):
+        Vw, _ = ref.step(Vw)
+    assert rel_l2(s.get_V(), Vw) < tol
+    free = o.FluidSolver(N, KF, 4e-3, 5e-4)
+    Vf = V
+    for _ in range(10):
+        Vf, _ = free.step(Vf)
+    assert sum(o.total_energy(v) for v in Vw) < sum(o.total_energy(v) for v in Vf)
+
+
+def test_liquid_metal_fine_grained_and_force_field(lib):
+    N = (32, 32, 32)
+    B0 = (1.0, 0.0, 0.5)
+    V = ic.random_phase_field(N, seed=62)
+    s = make(N, nu=4e-3, dt=5e-4, force=dict(kind="liquid_metal", B0=B0))
+    s.set_V(V)
+    s.Compute_force()
+    want = o.force_liquid_metal(V, KF, B0)
+    assert rel_l2(s.get_force(), want) < 1e-15
+    s.Compute_nlin()
+    s.Add_force()
+    want_nl = [x - y for x, y in zip(o.nlin_fluid(V, KF), want)]
+    assert rel_l2(s.get_nlin(), want_nl) < 1e-13

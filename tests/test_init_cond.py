@@ -68,6 +68,46 @@ def test_energy_spectrum_field():
         assert abs(Ek[k] / want - 1.0) < 1e-12, (k, Ek[k], want)
 
 
+def _relative_helicity(V, N):
+    kf = (1.0, 1.0, 1.0)
+    Kx, Ky, Kz = o.kvec(N, kf)
+    vr, vi = [v.real for v in V], [v.imag for v in V]
+    H = Kx * (vr[1] * vi[2] - vr[2] * vi[1]) + Ky * (vr[2] * vi[0] - vr[0] * vi[2]) + Kz * (vr[0] * vi[1] - vr[1] * vi[0])
+    E = sum(np.abs(v) ** 2 for v in V) / 2
+    with np.errstate(all="ignore"):
+        return H / (o.kmag(N, kf) * E), E
+
+
+def test_energy_helicity_spectrum_field():
+    """Init_cond_energy_helicity_spectrum: every mode off the kz = 0 plane has relative helicity
+    H_k/(k E_k) = sk; MHD: W's is skW and the cross helicity Re(u . b*) / (amp ampW) is h (the
+    reference's h = 2 Hc/(amp ampW), Hc = Re(u . b*)/2); divergence-free, origin zero; the
+    scalar variant adds T with the a_T spectrum."""
+    N = (16, 16, 16)
+    F = ic.energy_helicity_spectrum_field(N, 1.0, 0.6, physics="MHD", a2=0.5, skW=-0.3, h=0.4, seed=3)
+    V, W = F[:3], F[3:]
+    sv, Ev = _relative_helicity(V, N)
+    sw, Ew = _relative_helicity(W, N)
+    sel = (Ev > 1e-30) & (Ew > 1e-30) & (np.arange(N[2] // 2 + 1)[None, None, :] > 0)
+    assert sel.sum() > 100
+    assert np.abs(sv[sel] - 0.6).max() < 1e-12 and np.abs(sw[sel] - (-0.3)).max() < 1e-12
+    hc = sum((a * np.conj(b)).real for a, b in zip(V, W))
+    assert np.abs(hc[sel] / np.sqrt(4 * Ev[sel] * Ew[sel]) - 0.4).max() < 1e-12
+    K = o.kvec(N, (1.0, 1.0, 1.0))
+    for X in (V, W):
+        assert np.abs(sum(1j * Ki * x for Ki, x in zip(K, X))).max() < 1e-14
+        assert all(x[0, 0, 0] == 0 for x in X)
+    S = ic.energy_helicity_spectrum_field(N, 1.0, -0.2, physics="SCALAR", a2=0.7, seed=4)
+    assert len(S) == 4 and S[3][0, 0, 0] == 0 and np.abs(S[3]).max() > 0
+    s4, E4 = _relative_helicity(S[:3], N)
+    m = (E4 > 1e-30) & (np.arange(N[2] // 2 + 1)[None, None, :] > 0)
+    assert np.abs(s4[m] + 0.2).max() < 1e-12
+    # the energy-spectrum procedure for MHD and a scalar: W and T from their own spectra
+    M = ic.energy_spectrum_field(N, 1.0, physics="MHD", a2=0.3, seed=5)
+    T = ic.energy_spectrum_field(N, 1.0, physics="SCALAR", a2=0.3, seed=5)
+    assert len(M) == 6 and len(T) == 4 and np.abs(M[4]).max() > 0 and np.abs(T[3]).max() > 0
+
+
 def test_rb_lorenz_field():
     N = (17, 16, 16)
     kf = (math.pi, math.pi / math.sqrt(2), math.pi / math.sqrt(2))
@@ -103,5 +143,8 @@ def test_read_init_cond_dispatch(tmp_path):
     (tmp_path / "in" / "field_in.d").write_text("1 1 1 (0.1,0) (0.2,0)\n99 0 0\n")
     f = ic.read_init_cond(cfg(3), data_dir=str(tmp_path))
     assert f[0][1, 1, 1] == 0.1
+    # proc 4: the second value is the x-vorticity (Compute_VyVz)
+    f = ic.read_init_cond(cfg(4), data_dir=str(tmp_path))
+    assert f[0][1, 1, 1] == 0.1 and abs(1j * (f[2][1, 1, 1] - f[1][1, 1, 1]) - 0.2) < 1e-15
     with pytest.raises(ValueError):
-        ic.read_init_cond(cfg(4))
+        ic.read_init_cond(cfg(511))
