@@ -48,6 +48,20 @@ __host__ __device__ __forceinline__ cx<R> rmul(cx<R> a, cx<R> b) { return mkc<R>
 template <typename Rd, typename Rs>
 __host__ __device__ __forceinline__ cx<Rd> cvt(cx<Rs> a) { return mkc<Rd>((Rd)a.x, (Rd)a.y); }
 
+// FP32 complex arithmetic on the packed two-wide FP32 instructions of sm_100 (__fadd2_rn,
+// __fmul2_rn: per component the same rounding as the scalar operation), one instruction per
+// complex add, subtract, scaling or pointwise product instead of two.
+#if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ >= 1000) && !defined(TG_NO_F32X2)
+__device__ __forceinline__ float2 f2(cx<float> a) { return make_float2(a.x, a.y); }
+__device__ __forceinline__ cx<float> c2(float2 a) { return mkc<float>(a.x, a.y); }
+__device__ __forceinline__ cx<float> operator+(cx<float> a, cx<float> b) { return c2(__fadd2_rn(f2(a), f2(b))); }
+__device__ __forceinline__ cx<float> operator-(cx<float> a, cx<float> b) {
+  return c2(__fadd2_rn(f2(a), make_float2(-b.x, -b.y)));
+}
+__device__ __forceinline__ cx<float> operator*(float s, cx<float> a) { return c2(__fmul2_rn(make_float2(s, s), f2(a))); }
+__device__ __forceinline__ cx<float> rmul(cx<float> a, cx<float> b) { return c2(__fmul2_rn(f2(a), f2(b))); }
+#endif
+
 // Which FFT indices of an axis of length L are stored: [0, lo) and [L - hi, L), in that order,
 // as rows 0 .. lo+hi-1.  A full axis has lo = L, hi = 0.
 struct AxisMap {

@@ -1,7 +1,8 @@
 """Initial conditions (host side, numpy; outside the hot path): the benchmark configurations and
 the reference's initial-condition procedures (IncFluid::Read_init_cond init_cond_main.cc:52-206,
 field_input_proc 1 field file, 2 reduced field file, 3 and 4 given modes, 5 energy spectrum, 6
-energy-helicity spectrum, 7 Taylor-Green, 8 ABC, 51 RB Lorenz modes), returned as the state
+energy-helicity spectrum, 7 Taylor-Green, 8 ABC, 51 RB Lorenz modes, 101 six-mode dynamo, 511
+Rayleigh-Taylor), returned as the state
 fields in the reference layout.
 
 * Taylor-Green: the spectral placement of IncVF::Setup_Taylor_Green_field
@@ -344,6 +345,25 @@ def six_mode_field(N, k0, amp, ampW=None):
     return out
 
 
+def rayleigh_taylor_field(N, slope):
+    """Init_cond_Rayleigh_Taylor (init_cond_RayleighTaylor.cc:50-90, SCFT convection): u = 0 and
+    theta(x) = x - (1 + tanh(slope (x - 1/2)))/2, uniform in y and z, sine-transformed along x.
+    The reference computes x = lx / (local_N1_start + lx), which is 0/0 on the first plane and 1
+    on every other; x = lx / N1 is used here.  The transform is the reference's forward SCFT of a
+    field constant in y, z: theta(m, 0, 0) = (1/N1) sum_j theta_j sin(pi m (j + 1/2)/N1) for
+    m = 1 .. N1 - 1 (slot 0 empty), then the 2/3 rule along x.  Returns [V1, V2, V3, theta]."""
+    N1, N2, N3 = N
+    out = [np.zeros((N1, N2, N3 // 2 + 1), dtype=np.complex128) for _ in range(4)]
+    x = np.arange(N1, dtype=np.float64) / N1
+    th = x - (1.0 + np.tanh(slope * (x - 0.5))) / 2.0
+    j = np.arange(N1, dtype=np.float64) + 0.5
+    m = np.arange(1, N1, dtype=np.float64)
+    S = np.sin(np.pi * np.outer(m, j) / N1) @ th / N1
+    keep = np.arange(1, N1) < (2 * N1) // 3 if N1 >= 3 else np.ones(N1 - 1, dtype=bool)
+    out[3][1:, 0, 0] = np.where(keep, S, 0.0)
+    return out
+
+
 def rb_lorenz_field(N, W101, T101, T200, kfactor=(1.0, 1.0, 1.0)):
     """Init_cond_RB_Lorenz (init_cond_RB_misc.cc:55-85, SCFT): V1(1,0,1) = W101, V2(1,0,1) = 0, V3
     from Last_component, theta(1,0,1) = T101, theta(2,0,0) = T200.  Returns [V1, V2, V3, theta]."""
@@ -391,6 +411,8 @@ def read_init_cond(cfg, data_dir=".", seed=20261202):
         return abc_field(N, int(dp[1]), dp[5], dp[2], dp[3], dp[4], physics, dp[6])
     if proc == 101 and physics.upper() == "MHD" and basis == "FOUR":
         return six_mode_field(N, int(dp[1]), tuple(dp[2:6]), tuple(dp[6:10]))
+    if proc == 511 and physics.upper() == "RB" and basis == "SCFT":
+        return rayleigh_taylor_field(N, dp[1])
     if proc == 51 and physics.upper() == "RB":
         return rb_lorenz_field(N, dp[1], dp[2], dp[3], kf)
     raise ValueError(f"field_input_proc {proc} ({physics}, {basis}) is not built")

@@ -108,6 +108,18 @@ def test_energy_helicity_spectrum_field():
     assert len(M) == 6 and len(T) == 4 and np.abs(M[4]).max() > 0 and np.abs(T[3]).max() > 0
 
 
+def test_rayleigh_taylor_field():
+    """field_input_proc 511: the tanh temperature profile in x, sine-transformed as the oracle's
+    forward SCFT transform of the real field (uniform in y, z), dealiased; velocity zero."""
+    N = (33, 8, 8)
+    f = ic.rayleigh_taylor_field(N, 20.0)
+    x = np.arange(N[0]) / N[0]
+    th = x - (1 + np.tanh(20 * (x - 0.5))) / 2
+    want = o.dealias(o.forward_scft(np.broadcast_to(th[:, None, None], N).copy(), 1), "SCFT")
+    assert np.abs(f[3] - want).max() < 1e-14 * np.abs(want).max()
+    assert all(np.all(v == 0) for v in f[:3])
+
+
 def test_rb_lorenz_field():
     N = (17, 16, 16)
     kf = (math.pi, math.pi / math.sqrt(2), math.pi / math.sqrt(2))
