@@ -880,10 +880,6 @@ struct Net128 {
   }
 };
 
-#ifndef TG_NET128_FP64_BLOCKS
-#define TG_NET128_FP64_BLOCKS 3
-#endif
-
 // 16-byte asynchronous global -> shared copies (completion waited with cp.async.wait_group)
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem)
@@ -897,7 +893,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // inputs from shared memory instead of waiting on global loads.  Requires row strides and
 // input pointers on 16-byte boundaries (the launcher checks) and sizeof(Ri) == sizeof(Rw).
 template <typename Ri, typename Ro, typename Rw, int NIN, int NPROD, int WPB, int PF>
-__global__ void __launch_bounds__(32 * WPB, sizeof(Rw) == 8 ? TG_NET128_FP64_BLOCKS : 6)
+__global__ void __launch_bounds__(32 * WPB, sizeof(Rw) == 8 ? 4 : 6)
     k_z_prod_net128(ZArgs a, PtrSet ps, ProdPairs pp, int np) {
   constexpr int M = 128, E = 4;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -960,14 +956,15 @@ __global__ void __launch_bounds__(32 * WPB, sizeof(Rw) == 8 ? TG_NET128_FP64_BLO
       if (row + nwarps < a.nrows) prefetch(row + nwarps);
     }
     // ---- products and forward (r2c); unrolled in FP32 (fewer issued instructions, no spills
-    // at the 80-register bound: z-pass 209 -> 200 us at 256^3); in FP64 two products per
-    // iteration, their transforms independent chains for the scheduler to interleave
-    auto prod_load = [&](int q, cx<Rw> (&v)[E]) {
+    // at the 80-register bound: z-pass 209 -> 200 us at 256^3), rolled in FP64 (no gain there)
+#pragma unroll (sizeof(Rw) == 4 ? NPROD : 1)
+    for (int q = 0; q < NPROD; ++q) {
       const int pa = pp.a[q], pb = pp.b[q];
+      cx<Rw> v[E];
 #pragma unroll
       for (int k1 = 0; k1 < E; ++k1) v[k1] = rmul(rs[(pa * E + k1) * 32 + lane], rs[(pb * E + k1) * 32 + lane]);
-    };
-    auto prod_store = [&](int q, cx<Rw> (&v)[E]) {
+      net.fwd(v);
+      net.phase_in(v, true);
       cx<Ro>* dst = reinterpret_cast<cx<Ro>*>(ps.dst[q]) + row * a.ds;
       const int pl = (32 - lane) & 31;
 #pragma unroll
@@ -982,37 +979,6 @@ __global__ void __launch_bounds__(32 * WPB, sizeof(Rw) == 8 ? TG_NET128_FP64_BLO
       }
       if (lane == 0 && a.nout > M) dst[M] = cvt<Ro>(mkc<Rw>(sc * (v[0].x - v[0].y), (Rw)0));
       for (int k = a.nout + lane; k < a.nfill; k += 32) dst[k] = mkc<Ro>(0, 0);
-    };
-    if constexpr (sizeof(Rw) == 8) {
-      int q = 0;
-#pragma unroll 1
-      for (; q + 1 < NPROD; q += 2) {
-        cx<Rw> v[E], w[E];
-        prod_load(q, v);
-        prod_load(q + 1, w);
-        net.fwd(v);
-        net.fwd(w);
-        net.phase_in(v, true);
-        net.phase_in(w, true);
-        prod_store(q, v);
-        prod_store(q + 1, w);
-      }
-      if (q < NPROD) {
-        cx<Rw> v[E];
-        prod_load(q, v);
-        net.fwd(v);
-        net.phase_in(v, true);
-        prod_store(q, v);
-      }
-    } else {
-#pragma unroll
-      for (int q = 0; q < NPROD; ++q) {
-        cx<Rw> v[E];
-        prod_load(q, v);
-        net.fwd(v);
-        net.phase_in(v, true);
-        prod_store(q, v);
-      }
     }
   }
   if (PF) cp_async_wait_all();
