@@ -334,8 +334,14 @@ int tg_nusselt(tg_ctx* ctx, double* nusselt);
  * feed[i] = sum over |K| <= R_in with Get_shell_index(|K|) = i of 2 mult Re(F . V*), i = 0..S
  * (n >= S+1), with the force last computed (tg_compute_force, or the last RK stage of tg_step;
  * computed from the current field if the context never computed one) and the current field.
- * Zero for a decaying run.  FOUR fluid only. */
+ * Zero for a decaying run.  FOUR; fluid, MHD and passive scalar (the velocity's feed). */
 int tg_force_feed(tg_ctx* ctx, double* feed, int n);
+/* The force feed of one field group: 0 the velocity (as tg_force_feed), 1 the magnetic field of
+ * an MHD context (W.forceV_shell of Compute_force_feed_shell(W)), 2 the passive scalar
+ * (forceSF_shell of Compute_force_feed_shell_scalar, Re(F_T . T*)) (compute_force_feed.cc:70-155).
+ * FOUR; fluid, MHD and passive scalar.  With the liquid-metal force the velocity feed is
+ * sum 2 mult Re(F . V*) = -2 mult (B0 . K)^2/K^2 |V|^2 per shell. */
+int tg_force_feed_group(tg_ctx* ctx, int group, double* feed, int n);
 
 /* ------------------------------------------------------------------------------------------
  * Allocation-free energy reduction.  No counterpart in the reference.

@@ -450,7 +450,8 @@ __global__ void k_vector_potential(Geo g, const cx<double>* B0, const cx<double>
 struct ShellRadii {
   double r[kMaxShells + 1];
 };
-__global__ void k_force_feed(Geo g, const cx<double>* __restrict__ FB, int fx, int fy, int fz,
+// components c0 .. c0+nc-1 of the force box against the fields u0 .. (nc of them)
+__global__ void k_force_feed(Geo g, const cx<double>* __restrict__ FB, int fx, int fy, int fz, int c0, int nc,
                              const cx<double>* __restrict__ u0, const cx<double>* __restrict__ u1,
                              const cx<double>* __restrict__ u2, ShellRadii R, int S, double kin, double* out) {
   const int i = threadIdx.x;
@@ -472,13 +473,43 @@ __global__ void k_force_feed(Geo g, const cx<double>* __restrict__ FB, int fx, i
     if (sh != i) continue;
     const long long idx = ((long long)r1 * g.nky + r2) * g.kzp + kz;
     double re = 0;
-    for (int cc = 0; cc < 3; ++cc) {
-      const cx<double> f = FB[(long long)cc * box + p], v = U[cc][idx];
+    for (int cc = 0; cc < nc; ++cc) {
+      const cx<double> f = FB[(long long)(c0 + cc) * box + p], v = U[cc][idx];
       re += f.x * v.x + f.y * v.y;
     }
     acc += 2 * mult_four(l1, l2, kz, g.N1, g.N2) * re;
   }
   out[i] = acc;
+}
+
+// the liquid-metal force -(B0 . K)^2/K^2 V against V: -2 mult (B0 . K)^2/K^2 |V|^2, binned by
+// Get_shell_index over |K| <= R_in (out zeroed by the caller, S + 1 bins)
+__global__ void __launch_bounds__(256) k_force_feed_lm(Geo g, const cx<double>* u0, const cx<double>* u1,
+                                                       const cx<double>* u2, double b0, double b1, double b2,
+                                                       ShellRadii R, int S, double kin, double* out) {
+  __shared__ double sh[kMaxShells + 1];
+  for (int i = threadIdx.x; i <= S; i += blockDim.x) sh[i] = 0;
+  __syncthreads();
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < g.S; idx += stride) {
+    int r1, r2, l3;
+    compact_mode(g, idx, r1, r2, l3);
+    if (l3 >= g.nkz) continue;
+    const double kx = geo_kx(g, r1) * g.kf0, ky = geo_ky(g, r2) * g.kf1, kz = l3 * g.kf2;
+    const double K2 = kx * kx + ky * ky + kz * kz, K = sqrt(K2);
+    if (K > kin || K2 <= 0) continue;
+    int sh_i = 0;
+    while (sh_i <= S && !(K <= R.r[sh_i])) ++sh_i;
+    if (sh_i > S) continue;
+    const double bk = b0 * kx + b1 * ky + b2 * kz;
+    const cx<double> a = u0[idx], b = u1[idx], d = u2[idx];
+    const double v2 = a.x * a.x + a.y * a.y + b.x * b.x + b.y * b.y + d.x * d.x + d.y * d.y;
+    const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
+    atomicAdd(&sh[sh_i], -2 * mult_four(l1, l2, l3, g.N1, g.N2) * (bk * bk / K2) * v2);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i <= S; i += blockDim.x)
+    if (sh[i] != 0) atomicAdd(&out[i], sh[i]);
 }
 // Rows n = 1 .. S-1 of a shell-to-shell table (compute_shell_tr.cc: shell_from_index <
 // no_shells) from a giver-annulus x receiver-annulus table T; receivers |K| <= R_in go to column
@@ -651,31 +682,50 @@ int tg_shell_to_shell(tg_ctx* c, int kind, double* tr, int n) {
 }
 
 
-int tg_force_feed(tg_ctx* c, double* feed, int n) {
+// group 0: Compute_force_feed_shell (forceV_shell, Re(F . V*)); 1: W.forceV_shell of
+// Compute_force_feed_shell(W) (Re(F_B . B*), MHD); 2: forceSF_shell of
+// Compute_force_feed_shell_scalar (Re(F_T . T*), passive scalar) (compute_force_feed.cc:70-155)
+int tg_force_feed_group(tg_ctx* c, int group, double* feed, int n) {
   if (!c || !feed) return TG_ERR_ARG;
   const int S = c->cfg.n_shells;
-  if (S < 6 || S > kMaxShells || n < S + 1) return TG_ERR_ARG;
-  if (c->basis != TG_FOUR || c->phys != TG_FLUID)
-    return set_err(c, TG_ERR_UNSUPPORTED, "force feed: FOUR fluid only");
+  if (S < 6 || S > kMaxShells || n < S + 1 || group < 0 || group > 2) return TG_ERR_ARG;
+  if (c->basis != TG_FOUR || c->phys == TG_RB) return set_err(c, TG_ERR_UNSUPPORTED, "force feed: FOUR, no convection");
+  if ((group == 1 && c->phys != TG_MHD) || (group == 2 && c->phys != TG_SCALAR))
+    return set_err(c, TG_ERR_ARG, "force feed: the group is not a field of this physics");
   for (int i = 0; i < n; ++i) feed[i] = 0;
-  // decaying run, fixed modes never set: the force is zero; Coriolis: Re(F . V*) = Re(Omega .
-  // (V* x V)) = 0 mode by mode (V* x V is imaginary)
-  if (!c->force_on || (c->force_on == 2 && !c->FB)) return TG_OK;
   cudaSetDevice(c->dev);
-  int rc = ensure_force_box(c);
-  if (rc) return rc;
   const std::vector<double> R = et_radii(c);
   ShellRadii rr{};
   for (int i = 0; i <= S; ++i) rr.r[i] = R[i];
-  rc = ensure_diag(c, (size_t)S + 1);
+  int rc = ensure_diag(c, (size_t)S + 1);
   if (rc) return rc;
   double* d = c->diag;
-  k_force_feed<<<1, 64, 0, c->st>>>(c->g, c->FB, c->fx, c->fy, c->fz, c->U0[0], c->U0[1], c->U0[2], rr, S, R[S - 1], d);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e = cudaSuccess;
+  if (c->lm && group == 0) {
+    e = cudaMemsetAsync(d, 0, sizeof(double) * (S + 1), c->st);
+    if (e == cudaSuccess) {
+      const int nb = (int)std::min<long long>((c->g.S + 255) / 256, 148LL * 4);
+      k_force_feed_lm<<<nb, 256, 0, c->st>>>(c->g, c->U0[0], c->U0[1], c->U0[2], c->b0[0], c->b0[1], c->b0[2], rr, S,
+                                             R[S - 1], d);
+      e = cudaGetLastError();
+    }
+  } else {
+    // decaying run, fixed modes never set: the force is zero; Coriolis: Re(F . V*) = Re(Omega .
+    // (V* x V)) = 0 mode by mode (V* x V is imaginary)
+    if (!c->force_on || (c->force_on == 2 && !c->FB)) return TG_OK;
+    rc = ensure_force_box(c);
+    if (rc) return rc;
+    const int c0 = 3 * (group == 0 ? 0 : 1), nc = group == 2 ? 1 : 3;
+    k_force_feed<<<1, 64, 0, c->st>>>(c->g, c->FB, c->fx, c->fy, c->fz, c0, nc, c->U0[c0], c->U0[c0 + (nc > 1)],
+                                      c->U0[c0 + 2 * (nc > 1)], rr, S, R[S - 1], d);
+    e = cudaGetLastError();
+  }
   if (e == cudaSuccess) e = cudaMemcpyAsync(feed, d, sizeof(double) * (S + 1), cudaMemcpyDeviceToHost, c->st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
   if (e != cudaSuccess) return cuda_err(c, e, "force feed");
   return TG_OK;
 }
+
+int tg_force_feed(tg_ctx* c, double* feed, int n) { return tg_force_feed_group(c, 0, feed, n); }
 
 }  // extern "C"

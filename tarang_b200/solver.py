@@ -448,11 +448,12 @@ class IncFluid:
                                                    T.size), "cylinder ring transfer")
         return T, r
 
-    def Compute_force_feed_shell(self):
-        """IncVF::Compute_force_feed_shell (compute_force_feed.cc:70-76): forceV_shell, S+1 entries."""
+    def Compute_force_feed_shell(self, group: int = 0):
+        """IncVF::Compute_force_feed_shell (compute_force_feed.cc:70-155): forceV_shell (group 0),
+        W.forceV_shell (group 1, MHD) or forceSF_shell (group 2, passive scalar), S+1 entries."""
         S = self.cfg.n_shells
         f = np.zeros(S + 1)
-        self._ck(self.lib.tg_force_feed(self.h, _dptr(f), S + 1), "force feed")
+        self._ck(self.lib.tg_force_feed_group(self.h, int(group), _dptr(f), S + 1), "force feed")
         return f
 
     def Get_Nusselt_no(self) -> float:

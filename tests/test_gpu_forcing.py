@@ -358,3 +358,40 @@ def test_liquid_metal_fine_grained_and_force_field(lib):
     s.Add_force()
     want_nl = [x - y for x, y in zip(o.nlin_fluid(V, KF), want)]
     assert rel_l2(s.get_nlin(), want_nl) < 1e-13
+
+
+def test_force_feed_of_every_field(lib):
+    """Compute_force_feed_shell for B (MHD, W.forceV_shell) and the passive scalar (forceSF_shell)
+    under the band forcing, and the velocity's feed under the liquid-metal force, against the
+    oracle's shell sums of 2 mult Re(F . X*)."""
+    N, S = (32, 32, 32), 10
+    force = dict(kind="energy_supply", inner=2.0, outer=3.0, eps=0.1, eps_h=0.0, eps_W=0.05, eps_hW=0.3)
+    U = ic.random_phase_field(N, seed=71)
+    W = ic.random_phase_field(N, seed=72, energy=0.3)
+    s = make(N, physics="MHD", nu=2e-3, eta=3e-3, dt=5e-4, force=force, n_shells=S)
+    s.set_V(U)
+    s.set_W(W)
+    s.Compute_force()
+    FW = o.force_band(W, N, KF, 2.0, 3.0, 0.05, 0.3, mode=1, gate=True)
+    want = o.force_feed_shell(FW, W, KF, S)
+    assert np.count_nonzero(want) >= 1
+    assert np.abs(s.Compute_force_feed_shell(1) - want).max() <= 1e-12 * np.abs(want).max()
+    FU = o.force_band(U, N, KF, 2.0, 3.0, 0.1, 0.0, mode=1, gate=True)
+    want = o.force_feed_shell(FU, U, KF, S)
+    assert np.abs(s.Compute_force_feed_shell(0) - want).max() <= 1e-12 * np.abs(want).max()
+    T = ic.random_phase_field(N, k0=2.0, seed=73)[0]
+    fs = dict(kind="energy_helicity", inner=2.0, outer=3.0, eps=0.1, eps_T=0.02)
+    c = make(N, physics="SCALAR", nu=2e-3, kappa=4e-3, dt=5e-4, force=fs, n_shells=S)
+    c.set_V(U)
+    c.set_T(T)
+    c.Compute_force()
+    FT = o.force_band_scalar(T, N, KF, 2.0, 3.0, 0.02, mode=2)
+    want = o.force_feed_shell([FT], [T], KF, S)
+    assert np.abs(c.Compute_force_feed_shell(2) - want).max() <= 1e-12 * np.abs(want).max()
+    B0 = (0.0, 0.5, 2.0)
+    m = make(N, nu=2e-3, dt=5e-4, force=dict(kind="liquid_metal", B0=B0), n_shells=S)
+    m.set_V(U)
+    m.Compute_force()
+    want = o.force_feed_shell(o.force_liquid_metal(U, KF, B0), U, KF, S)
+    assert np.all(want[1:] <= 0) and want.min() < 0
+    assert np.abs(m.Compute_force_feed_shell() - want).max() <= 1e-12 * np.abs(want).max()
