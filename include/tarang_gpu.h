@@ -342,6 +342,14 @@ int tg_force_feed(tg_ctx* ctx, double* feed, int n);
  * FOUR; fluid, MHD and passive scalar.  With the liquid-metal force the velocity feed is
  * sum 2 mult Re(F . V*) = -2 mult (B0 . K)^2/K^2 |V|^2 per shell. */
 int tg_force_feed_group(tg_ctx* ctx, int group, double* feed, int n);
+/* IncVF::Compute_force_feed_ring / Compute_force_feed_cylinder_ring (compute_force_feed.cc:162-300,
+ * Ring_mult_all / Cyl_ring_mult_all four_ET.cc:335-386, 492-530): the force feed 2 mult Re(F . X*)
+ * of field group 0 (velocity), 1 (B, MHD) or 2 (passive scalar) binned by receiver ring
+ * (cylinder = 0: tg_ring_radii shells x n_sectors polar sectors) or cylinder ring (cylinder = 1:
+ * tg_cylinder_radii shells x n_sectors K_par slabs) about `axis`; out is
+ * [n_ring_shells + 1][n_sectors + 1] row-major (n >= that many).  FOUR; no convection. */
+int tg_force_feed_ring(tg_ctx* ctx, int group, int cylinder, int axis, int n_ring_shells, int n_sectors, double* out,
+                       int n);
 
 /* ------------------------------------------------------------------------------------------
  * Allocation-free energy reduction.  No counterpart in the reference.

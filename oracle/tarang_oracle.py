@@ -1500,6 +1500,52 @@ def compute_cylinder_ring_tr_generic(H, F, Rf, sign, kfactor, axis, n_shells, n_
     return T
 
 
+def ring_mult_all(A, B, kfactor, axis, n_ring_shells, n_sectors, alias="DEALIAS", cylinder=False):
+    """Ring_mult_all / Local_ring_mult_all_FOUR (four_ET.cc:335-386) and Cyl_ring_mult_all /
+    Local_cyl_ring_mult_all_FOUR (:492-530): sum of 2 mult Re(A . B*) binned by receiver ring
+    (scheme-0 ring radii, equal sectors of the folded polar angle up to pi/2, |K| <= R_in,
+    |K| > MYEPS) or cylinder ring (radii up to Anis_max_Krho_radius_inside, slabs of |K_par|).
+    [shell][sector] of shape (n+1, ns+1).  It gives Compute_force_feed_ring and
+    Compute_force_feed_cylinder_ring (compute_force_feed.cc:162-300) with A the force."""
+    N = (A[0].shape[0], A[0].shape[1], 2 * (A[0].shape[2] - 1))
+    mult = multiplicity_four(N)
+    val = 2 * mult * sum(np.real(a * np.conj(b)) for a, b in zip(A, B))
+    n1, n2 = n_ring_shells + 1, n_sectors + 1
+    if not cylinder:
+        R = ring_radii(N, kfactor, n_ring_shells, alias)
+        dth = (math.pi / 2) / n_sectors
+        sec = [i * dth for i in range(n_sectors)] + [math.pi / 2]
+        K = kmag(N, kfactor)
+        th = _theta_grid(N, kfactor, axis)
+        kin = max_radius_inside(N, kfactor, alias)
+        shell = shell_index(K, R)
+        thf = np.where(th > math.pi / 2, math.pi - th, th)
+        sector = np.full(K.shape, len(sec), dtype=np.int64)
+        for i in range(len(sec) - 1, -1, -1):
+            sector = np.where(thf <= sec[i], i, sector)
+        sector = np.where(np.abs(thf) < MYEPS, 1, sector)
+        ok = (K <= kin) & (K > MYEPS) & (shell <= n_ring_shells) & (sector <= n_sectors)
+    else:
+        d = 3 if alias == "DEALIAS" else 2
+        kr = krho_inside(N, kfactor, axis, alias)
+        R = ring_radii(N, kfactor, n_ring_shells, alias, Rin=float(kr))
+        ax = axis - 1
+        kmax = (N[ax] // d) * kfactor[ax]
+        dk = kmax / n_sectors
+        hb = [0.0] + [i * dk for i in range(1, n_sectors)] + [kmax]
+        Kv = [np.broadcast_to(k, (N[0], N[1], N[2] // 2 + 1)) for k in kvec(N, kfactor)]
+        kperp = np.sqrt(Kv[(ax + 1) % 3] ** 2 + Kv[(ax + 2) % 3] ** 2)
+        shell = shell_index(kperp, R)
+        akp = np.abs(Kv[ax])
+        sector = np.full(kperp.shape, len(hb), dtype=np.int64)
+        for i in range(len(hb) - 1, 0, -1):
+            sector = np.where(akp <= hb[i], i, sector)
+        sector = np.where(akp < MYEPS, 1, sector)
+        ok = (kperp <= kr) & (shell <= n_ring_shells) & (sector <= n_sectors)
+    flat = (shell * n2 + sector)[ok]
+    return np.bincount(flat, weights=val[ok], minlength=n1 * n2).reshape(n1, n2)
+
+
 def compute_ring_tr_generic(H, F, Rf, sign, kfactor, axis, n_ring_shells, n_sectors, alias="DEALIAS"):
     """IncVF::Compute_ring_tr  compute_ring_tr.cc:60-90 (MHD kinds :174-215) in one form:
     giver ring (i, j): G = F on r[i-1] < |K| <= r[i], sector_{j-1} < theta <= sector_j

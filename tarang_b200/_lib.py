@@ -192,6 +192,7 @@ SIGNATURES = {
     "tg_nusselt": (C.c_int, [_VP, _DP]),
     "tg_force_feed": (C.c_int, [_VP, _DP, C.c_int]),
     "tg_force_feed_group": (C.c_int, [_VP, C.c_int, _DP, C.c_int]),
+    "tg_force_feed_ring": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _DP, C.c_int]),
     "tg_energy_noalloc": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_int, _VP, _VP]),
     "tg_profile_enable": (C.c_int, [_VP, C.c_int]),
     "tg_profile_read": (C.c_int, [_VP, C.POINTER(tg_kernel_stat), C.c_int, C.POINTER(C.c_int)]),

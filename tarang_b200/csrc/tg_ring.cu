@@ -296,6 +296,90 @@ struct RingContractArgs {
   double* out;        // [n + 1][ns + 1]
 };
 
+// receiver ring of a mode, shell * (ns + 1) + sector, or -1 outside the rings
+// (Local_ring_mult_all: 0 < |K| <= R_in, Compute_ring_index with the angle folded to [0, pi/2];
+// Local_cyl_ring_mult_all: K_perp <= K_perp,max, Compute_cylinder_ring_index with |K_par|, K_par = 0
+// in slab 1; first radius >= K, the radii need not be sorted)
+__device__ __forceinline__ int ring_bin(const RingBins& b, double K, double th) {
+  if (b.cyl ? !(K <= b.kin) : !(K <= b.kin && K > kEps)) return -1;
+  int shell = 0;
+  while (shell <= b.n && !(K <= b.r[shell])) ++shell;
+  if (shell > b.n) return -1;
+  int sector;
+  if (!b.cyl) {
+    if (th > M_PI / 2) th = M_PI - th;
+    sector = 1;
+    if (!(fabs(th) < kEps)) {
+      sector = 0;
+      while (sector <= b.ns && !(th <= b.bound[sector])) ++sector;
+    }
+  } else {
+    th = fabs(th);
+    sector = 1;
+    if (!(th < kEps)) {
+      while (sector <= b.ns && !(th <= b.bound[sector])) ++sector;
+    }
+  }
+  if (sector > b.ns) return -1;
+  return shell * (b.ns + 1) + sector;
+}
+
+// Compute_force_feed_ring / _cylinder_ring (compute_force_feed.cc:162-300): 2 mult Re(F . X*)
+// binned by receiver ring, F from the force box (components c0 .. c0+nc-1) or, with lm, the
+// liquid-metal force -(B0 . K)^2/K^2 V
+struct RingFeedArgs {
+  Geo g;
+  RingBins b;
+  const cx<double>* FB;
+  int fx, fy, fz, c0, nc;
+  const cx<double>* X[3];
+  int lm;
+  double b0[3];
+  double* out;
+};
+
+__global__ void __launch_bounds__(TPB) k_ring_feed(RingFeedArgs a) {
+  extern __shared__ double sh[];
+  const int nbins = (a.b.n + 1) * (a.b.ns + 1);
+  for (int i = threadIdx.x; i < nbins; i += TPB) sh[i] = 0;
+  __syncthreads();
+  const Geo& g = a.g;
+  const int ny = 2 * a.fy + 1, nz = a.fz + 1;
+  const long long stride = (long long)gridDim.x * TPB;
+  for (long long idx = (long long)blockIdx.x * TPB + threadIdx.x; idx < g.S; idx += stride) {
+    int r1, r2, l3;
+    double K, th, k[3];
+    mode_angle(g, idx, a.b.axis, a.b.cyl, r1, r2, l3, K, th, k);
+    if (l3 >= g.nkz) continue;
+    const int bin = ring_bin(a.b, K, th);
+    if (bin < 0) continue;
+    const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
+    double re = 0;
+    if (a.lm) {
+      const double K2 = k[0] * k[0] + k[1] * k[1] + k[2] * k[2];
+      const double bk = a.b0[0] * k[0] + a.b0[1] * k[1] + a.b0[2] * k[2];
+      const double f = K2 > 0 ? -bk * bk / K2 : 0.0;
+      for (int c = 0; c < 3; ++c) {
+        const cx<double> v = a.X[c][idx];
+        re += f * (v.x * v.x + v.y * v.y);
+      }
+    } else {
+      const int kx = geo_kx(g, r1), ky = geo_ky(g, r2);
+      if (kx < -a.fx || kx > a.fx || ky < -a.fy || ky > a.fy || l3 > a.fz) continue;
+      const int box = (2 * a.fx + 1) * ny * nz;
+      const int p = ((kx + a.fx) * ny + (ky + a.fy)) * nz + l3;
+      for (int c = 0; c < a.nc; ++c) {
+        const cx<double> f = a.FB[(long long)(a.c0 + c) * box + p], v = a.X[c][idx];
+        re += f.x * v.x + f.y * v.y;
+      }
+    }
+    if (re != 0) atomicAdd(&sh[bin], 2 * mult_four(l1, l2, l3, g.N1, g.N2) * re);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nbins; i += TPB)
+    if (sh[i] != 0) atomicAdd(&a.out[i], sh[i]);
+}
+
 template <typename Rp>
 __global__ void __launch_bounds__(TPB) k_ring_contract(RingContractArgs a) {
   extern __shared__ double sh[];
@@ -309,29 +393,9 @@ __global__ void __launch_bounds__(TPB) k_ring_contract(RingContractArgs a) {
     double K, th, k[3];
     mode_angle(g, idx, a.b.axis, a.b.cyl, r1, r2, l3, K, th, k);
     if (l3 >= g.nkz) continue;
-    // Local_ring_mult_all: 0 < |K| <= R_in; Local_cyl_ring_mult_all: K_perp <= K_perp,max
-    if (a.b.cyl ? !(K <= a.b.kin) : !(K <= a.b.kin && K > kEps)) continue;
-    int shell = 0;  // first radius >= K (the radii need not be sorted)
-    while (shell <= a.b.n && !(K <= a.b.r[shell])) ++shell;
-    if (shell > a.b.n) continue;
-    int sector;
-    if (!a.b.cyl) {
-      // Compute_ring_index: the angle folded to [0, pi/2]
-      if (th > M_PI / 2) th = M_PI - th;
-      sector = 1;
-      if (!(fabs(th) < kEps)) {
-        sector = 0;
-        while (sector <= a.b.ns && !(th <= a.b.bound[sector])) ++sector;
-      }
-    } else {
-      // Compute_cylinder_ring_index: |K_par|, K_par = 0 in slab 1
-      th = fabs(th);
-      sector = 1;
-      if (!(th < kEps)) {
-        while (sector <= a.b.ns && !(th <= a.b.bound[sector])) ++sector;
-      }
-    }
-    if (sector > a.b.ns) continue;
+    const int bin = ring_bin(a.b, K, th);
+    if (bin < 0) continue;
+    const int shell = bin / cols, sector = bin - shell * cols;
     const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
     double v = 0;
 #pragma unroll
@@ -391,26 +455,10 @@ int tg_ring_radii(tg_ctx* c, int n_ring_shells, double* radii, int n) {
 
 namespace {
 
-int run_ring_tr(tg_ctx* c, int kind, int axis, int n_ring_shells, int n_sectors, int cyl, double* tr, int n) {
-  if (!c || !tr) return TG_ERR_ARG;
-  if (c->basis != TG_FOUR) return set_err(c, TG_ERR_UNSUPPORTED, "ring transfers: FOUR basis only");
-  if (axis < 1 || axis > 3 || n_sectors < 1 || n_sectors > TG_RING_MAX_SECTORS) return TG_ERR_ARG;
-  if (n_ring_shells < 5 || n_ring_shells > kMaxRingShells) return TG_ERR_ARG;
-  // U->U ring_to_ring_self, B->B W.ring_to_ring_self, U->B ring_to_ring_VF, Z+->Z+ and Z-->Z-
-  // ring_to_ring_Elsasser, T->T ring_to_ring_SF; the reference has no B->U ring table
-  if (kind == TG_ET_BU) return set_err(c, TG_ERR_ARG, "ring transfers have no B->U kind");
-  const int rows = n_ring_shells + 1, cols = n_sectors + 1, per = rows * cols;
-  if ((size_t)n < (size_t)per * per) return set_err(c, TG_ERR_ARG, "ring transfer: output shorter than (n+1)^2 (ns+1)^2");
-  cudaSetDevice(c->dev);
-  int rc = ensure_et_buffers(c);
-  if (rc) return rc;
-  const cx<double>* Hp[3];
-  const cx<double>* Fp[3];
-  const cx<double>* Rp[3];
-  double sign = 1.0;
-  rc = et_kind_fields(c, kind, Hp, Fp, Rp, sign);
-  if (rc) return rc;
-  RingBins b{};
+// the receiver rings of a ring (scheme-0 radii, equal sectors up to pi/2) or cylinder-ring (radii
+// up to Anis_max_Krho_radius_inside, slabs of K_par up to Anis_max_Kpll) table
+void ring_bins_for(tg_ctx* c, int axis, int n_ring_shells, int n_sectors, int cyl, RingBins& b) {
+  b = RingBins{};
   b.n = n_ring_shells;
   b.ns = n_sectors;
   b.axis = axis;
@@ -433,6 +481,29 @@ int run_ring_tr(tg_ctx* c, int kind, int axis, int n_ring_shells, int n_sectors,
     b.bound[n_sectors] = kmax;
     b.kin = (double)kr;
   }
+}
+
+int run_ring_tr(tg_ctx* c, int kind, int axis, int n_ring_shells, int n_sectors, int cyl, double* tr, int n) {
+  if (!c || !tr) return TG_ERR_ARG;
+  if (c->basis != TG_FOUR) return set_err(c, TG_ERR_UNSUPPORTED, "ring transfers: FOUR basis only");
+  if (axis < 1 || axis > 3 || n_sectors < 1 || n_sectors > TG_RING_MAX_SECTORS) return TG_ERR_ARG;
+  if (n_ring_shells < 5 || n_ring_shells > kMaxRingShells) return TG_ERR_ARG;
+  // U->U ring_to_ring_self, B->B W.ring_to_ring_self, U->B ring_to_ring_VF, Z+->Z+ and Z-->Z-
+  // ring_to_ring_Elsasser, T->T ring_to_ring_SF; the reference has no B->U ring table
+  if (kind == TG_ET_BU) return set_err(c, TG_ERR_ARG, "ring transfers have no B->U kind");
+  const int rows = n_ring_shells + 1, cols = n_sectors + 1, per = rows * cols;
+  if ((size_t)n < (size_t)per * per) return set_err(c, TG_ERR_ARG, "ring transfer: output shorter than (n+1)^2 (ns+1)^2");
+  cudaSetDevice(c->dev);
+  int rc = ensure_et_buffers(c);
+  if (rc) return rc;
+  const cx<double>* Hp[3];
+  const cx<double>* Fp[3];
+  const cx<double>* Rp[3];
+  double sign = 1.0;
+  rc = et_kind_fields(c, kind, Hp, Fp, Rp, sign);
+  if (rc) return rc;
+  RingBins b{};
+  ring_bins_for(c, axis, n_ring_shells, n_sectors, cyl, b);
   const size_t need = (size_t)per * per;  // [giver shell][giver sector][shell][sector]
   rc = ensure_diag(c, need);
   if (rc) return rc;
@@ -580,6 +651,53 @@ int tg_shell_spectrum_helicity(tg_ctx* c, int group, double* h1, double* h2, dou
       out[i][b] = hh[(size_t)i * nbins + b] * (resc ? approx_fac * b * b / cnt[b] : 1.0);
     }
   }
+  return TG_OK;
+}
+
+// Compute_force_feed_ring / Compute_force_feed_cylinder_ring (compute_force_feed.cc:162-300)
+int tg_force_feed_ring(tg_ctx* c, int group, int cylinder, int axis, int n_ring_shells, int n_sectors, double* out,
+                       int n) {
+  if (!c || !out) return TG_ERR_ARG;
+  if (c->basis != TG_FOUR || c->phys == TG_RB) return set_err(c, TG_ERR_UNSUPPORTED, "ring force feed: FOUR, no convection");
+  if (axis < 1 || axis > 3 || n_sectors < 1 || n_sectors > TG_RING_MAX_SECTORS) return TG_ERR_ARG;
+  if (n_ring_shells < 5 || n_ring_shells > kMaxRingShells || group < 0 || group > 2) return TG_ERR_ARG;
+  if ((group == 1 && c->phys != TG_MHD) || (group == 2 && c->phys != TG_SCALAR))
+    return set_err(c, TG_ERR_ARG, "ring force feed: the group is not a field of this physics");
+  const int per = (n_ring_shells + 1) * (n_sectors + 1);
+  if (n < per) return set_err(c, TG_ERR_ARG, "ring force feed: output shorter than (n+1)(ns+1)");
+  for (int i = 0; i < n; ++i) out[i] = 0;
+  const bool lm = c->lm && group == 0;
+  if (!lm && (!c->force_on || (c->force_on == 2 && !c->FB))) return TG_OK;  // no force, or Coriolis
+  cudaSetDevice(c->dev);
+  int rc = TG_OK;
+  if (!lm) rc = ensure_force_box(c);
+  if (!rc) rc = ensure_diag(c, (size_t)per);
+  if (rc) return rc;
+  RingFeedArgs a{};
+  a.g = c->g;
+  ring_bins_for(c, axis, n_ring_shells, n_sectors, cylinder ? 1 : 0, a.b);
+  a.FB = c->FB;
+  a.fx = c->fx;
+  a.fy = c->fy;
+  a.fz = c->fz;
+  a.c0 = group == 0 ? 0 : 3;
+  a.nc = group == 2 ? 1 : 3;
+  for (int i = 0; i < 3; ++i) a.X[i] = c->U0[a.c0 + (a.nc > 1 ? i : 0)];
+  a.lm = lm ? 1 : 0;
+  for (int i = 0; i < 3; ++i) a.b0[i] = c->b0[i];
+  a.out = c->diag;
+  cudaError_t e = cudaMemsetAsync(c->diag, 0, sizeof(double) * per, c->st);
+  const size_t smem = sizeof(double) * per;
+  if (e == cudaSuccess && smem > 48 * 1024)
+    e = cudaFuncSetAttribute(k_ring_feed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) {
+    const int nblk = (int)std::min<long long>((c->g.S + TPB - 1) / TPB, 148LL * 8);
+    k_ring_feed<<<nblk, TPB, smem, c->st>>>(a);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, c->diag, sizeof(double) * per, cudaMemcpyDeviceToHost, c->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+  if (e != cudaSuccess) return cuda_err(c, e, "ring force feed");
   return TG_OK;
 }
 

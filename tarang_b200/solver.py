@@ -456,6 +456,14 @@ class IncFluid:
         self._ck(self.lib.tg_force_feed_group(self.h, int(group), _dptr(f), S + 1), "force feed")
         return f
 
+    def Compute_force_feed_ring(self, n_ring_shells, n_sectors, axis=1, group=0, cylinder=False):
+        """IncVF::Compute_force_feed_ring / Compute_force_feed_cylinder_ring (tg_force_feed_ring):
+        forceV_ring (group 0), W.forceV_ring (1) or forceSF_ring (2) as [shell][sector]."""
+        out = np.zeros((n_ring_shells + 1) * (n_sectors + 1))
+        self._ck(self.lib.tg_force_feed_ring(self.h, int(group), 1 if cylinder else 0, int(axis), int(n_ring_shells),
+                                             int(n_sectors), _dptr(out), out.size), "ring force feed")
+        return out.reshape(n_ring_shells + 1, n_sectors + 1)
+
     def Get_Nusselt_no(self) -> float:
         """IncVF::Get_Nusselt_no (nusselt.cc:53-89): Nu = 1 + 2 sqrt(Ra Pr) <u1, theta>."""
         v = C.c_double()

@@ -395,3 +395,41 @@ def test_force_feed_of_every_field(lib):
     want = o.force_feed_shell(o.force_liquid_metal(U, KF, B0), U, KF, S)
     assert np.all(want[1:] <= 0) and want.min() < 0
     assert np.abs(m.Compute_force_feed_shell() - want).max() <= 1e-12 * np.abs(want).max()
+
+
+def test_ring_force_feed(lib):
+    """Compute_force_feed_ring / Compute_force_feed_cylinder_ring: the force feed of U, B and a
+    passive scalar binned by receiver ring and cylinder ring, and the liquid-metal feed, against
+    the oracle's Ring_mult_all / Cyl_ring_mult_all restatement."""
+    N = (32, 32, 32)
+    U = ic.random_phase_field(N, seed=81)
+    W = ic.random_phase_field(N, seed=82, energy=0.3)
+    force = dict(kind="energy_helicity", inner=1.0, outer=3.0, eps=0.1, eps_h=0.2, eps_W=0.05, eps_hW=-0.3)
+    s = make(N, physics="MHD", nu=2e-3, eta=3e-3, dt=5e-4, force=force)
+    s.set_V(U)
+    s.set_W(W)
+    s.Compute_force()
+    FU = o.force_band(U, N, KF, 1.0, 3.0, 0.1, 0.2, mode=2, gate=True)
+    FW = o.force_band(W, N, KF, 1.0, 3.0, 0.05, -0.3, mode=2, gate=True)
+    for group, F, X in ((0, FU, U), (1, FW, W)):
+        for cyl, axis, n, ns in ((False, 3, 6, 3), (True, 1, 5, 4)):
+            got = s.Compute_force_feed_ring(n, ns, axis, group, cyl)
+            want = o.ring_mult_all(F, X, KF, axis, n, ns, cylinder=cyl)
+            assert np.count_nonzero(want) >= 1
+            assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max(), (group, cyl)
+    T = ic.random_phase_field(N, k0=2.0, seed=83)[0]
+    c = make(N, physics="SCALAR", nu=2e-3, kappa=4e-3, dt=5e-4,
+             force=dict(kind="energy_supply", inner=1.0, outer=3.0, eps=0.1, eps_T=0.02))
+    c.set_V(U)
+    c.set_T(T)
+    c.Compute_force()
+    FT = o.force_band_scalar(T, N, KF, 1.0, 3.0, 0.02, mode=1)
+    got = c.Compute_force_feed_ring(6, 2, 2, 2)
+    want = o.ring_mult_all([FT], [T], KF, 2, 6, 2)
+    assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
+    B0 = (0.3, 0.0, 1.0)
+    m = make(N, nu=2e-3, dt=5e-4, force=dict(kind="liquid_metal", B0=B0))
+    m.set_V(U)
+    got = m.Compute_force_feed_ring(6, 3, 3, 0, True)
+    want = o.ring_mult_all(o.force_liquid_metal(U, KF, B0), U, KF, 3, 6, 3, cylinder=True)
+    assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
