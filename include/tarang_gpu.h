@@ -340,7 +340,9 @@ int tg_force_feed(tg_ctx* ctx, double* feed, int n);
  * an MHD context (W.forceV_shell of Compute_force_feed_shell(W)), 2 the passive scalar
  * (forceSF_shell of Compute_force_feed_shell_scalar, Re(F_T . T*)) (compute_force_feed.cc:70-155).
  * FOUR; fluid, MHD and passive scalar.  With the liquid-metal force the velocity feed is
- * sum 2 mult Re(F . V*) = -2 mult (B0 . K)^2/K^2 |V|^2 per shell. */
+ * sum 2 mult Re(F . V*) = -2 mult (B0 . K)^2/K^2 |V|^2 per shell.  Convection (FOUR or SCFT;
+ * Compute_force_feed_shell_RB, PRLARGE / PRSMALL): group 0 the buoyancy fu theta against u1,
+ * group 2 ft u1 against theta. */
 int tg_force_feed_group(tg_ctx* ctx, int group, double* feed, int n);
 /* IncVF::Compute_force_feed_ring / Compute_force_feed_cylinder_ring (compute_force_feed.cc:162-300,
  * Ring_mult_all / Cyl_ring_mult_all four_ET.cc:335-386, 492-530): the force feed 2 mult Re(F . X*)

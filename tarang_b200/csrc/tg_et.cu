@@ -682,6 +682,36 @@ int tg_shell_to_shell(tg_ctx* c, int kind, double* tr, int n) {
 }
 
 
+// convection (Compute_force_feed_shell_RB -> Compute_force_feed_shell_scalar, PRLARGE and
+// PRSMALL): with Force1 = fu theta and T.Force = ft u1 (Compute_force_RB), group 0 bins
+// 2 mult fu Re(theta u1*) and group 2 bins 2 mult ft Re(u1 theta*) by Get_shell_index over
+// |K| <= R_in, SCFT or FOUR multiplicity (out zeroed by the caller)
+__global__ void __launch_bounds__(256) k_force_feed_rb(Geo g, const cx<double>* u1, const cx<double>* th, double coef,
+                                                       ShellRadii R, int S, double kin, double* out) {
+  __shared__ double sh[kMaxShells + 1];
+  for (int i = threadIdx.x; i <= S; i += blockDim.x) sh[i] = 0;
+  __syncthreads();
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < g.S; idx += stride) {
+    int r1, r2, l3;
+    compact_mode(g, idx, r1, r2, l3);
+    if (l3 >= g.nkz) continue;
+    const double kx = geo_kx(g, r1) * g.kf0, ky = geo_ky(g, r2) * g.kf1, kz = l3 * g.kf2;
+    const double K = sqrt(kx * kx + ky * ky + kz * kz);
+    if (K > kin) continue;
+    int sh_i = 0;
+    while (sh_i <= S && !(K <= R.r[sh_i])) ++sh_i;
+    if (sh_i > S) continue;
+    const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
+    const double m = g.basis == 0 ? mult_four(l1, l2, l3, g.N1, g.N2) : mult_scft(l1, l2, l3, g.N2);
+    const cx<double> a = u1[idx], b = th[idx];
+    atomicAdd(&sh[sh_i], 2 * m * coef * (a.x * b.x + a.y * b.y));
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i <= S; i += blockDim.x)
+    if (sh[i] != 0) atomicAdd(&out[i], sh[i]);
+}
+
 // group 0: Compute_force_feed_shell (forceV_shell, Re(F . V*)); 1: W.forceV_shell of
 // Compute_force_feed_shell(W) (Re(F_B . B*), MHD); 2: forceSF_shell of
 // Compute_force_feed_shell_scalar (Re(F_T . T*), passive scalar) (compute_force_feed.cc:70-155)
@@ -689,8 +719,8 @@ int tg_force_feed_group(tg_ctx* c, int group, double* feed, int n) {
   if (!c || !feed) return TG_ERR_ARG;
   const int S = c->cfg.n_shells;
   if (S < 6 || S > kMaxShells || n < S + 1 || group < 0 || group > 2) return TG_ERR_ARG;
-  if (c->basis != TG_FOUR || c->phys == TG_RB) return set_err(c, TG_ERR_UNSUPPORTED, "force feed: FOUR, no convection");
-  if ((group == 1 && c->phys != TG_MHD) || (group == 2 && c->phys != TG_SCALAR))
+  if (c->basis != TG_FOUR && c->phys != TG_RB) return set_err(c, TG_ERR_UNSUPPORTED, "force feed: FOUR (or convection)");
+  if ((group == 1 && c->phys != TG_MHD) || (group == 2 && c->phys != TG_SCALAR && c->phys != TG_RB))
     return set_err(c, TG_ERR_ARG, "force feed: the group is not a field of this physics");
   for (int i = 0; i < n; ++i) feed[i] = 0;
   cudaSetDevice(c->dev);
@@ -701,7 +731,15 @@ int tg_force_feed_group(tg_ctx* c, int group, double* feed, int n) {
   if (rc) return rc;
   double* d = c->diag;
   cudaError_t e = cudaSuccess;
-  if (c->lm && group == 0) {
+  if (c->phys == TG_RB) {
+    e = cudaMemsetAsync(d, 0, sizeof(double) * (S + 1), c->st);
+    if (e == cudaSuccess) {
+      const int nb = (int)std::min<long long>((c->g.S + 255) / 256, 148LL * 4);
+      k_force_feed_rb<<<nb, 256, 0, c->st>>>(c->g, c->U0[0], c->U0[3], group == 0 ? c->rb_fu : c->rb_ft, rr, S,
+                                             R[S - 1], d);
+      e = cudaGetLastError();
+    }
+  } else if (c->lm && group == 0) {
     e = cudaMemsetAsync(d, 0, sizeof(double) * (S + 1), c->st);
     if (e == cudaSuccess) {
       const int nb = (int)std::min<long long>((c->g.S + 255) / 256, 148LL * 4);

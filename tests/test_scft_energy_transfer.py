@@ -71,3 +71,21 @@ def test_gpu_scft_flux_and_shell_tr(lib, Nn):
         assert np.abs(got - fw).max() <= 1e-10 * np.abs(fw).max(), kind
         got = s.Compute_shell_tr(kind)
         assert np.abs(got - tw).max() <= 1e-10 * np.abs(tw).max(), kind
+
+
+@pytest.mark.gpu
+def test_gpu_convection_force_feed(lib):
+    """Compute_force_feed_shell_RB (PRLARGE): the buoyancy force fu theta fed into u1 and the
+    force ft u1 fed into theta, per energy-transfer shell in the SCFT basis."""
+    from tarang_b200.solver import IncFluid
+    V, T = scft_fields(N, 13)
+    s = IncFluid(N, basis="SCFT", physics="RB", Ra=1e6, Pr=1.0, kfactor=KF, dt=1e-4, n_shells=S)
+    s.set_V(V)
+    s.set_T(T)
+    _, _, fu, ft, _ = o.rb_coefficients(1e6, 1.0)
+    z = np.zeros_like(T)
+    want_u = o.force_feed_shell([fu * T, z, z], V, KF, S, basis="SCFT")
+    want_t = o.force_feed_shell([ft * V[0]], [T], KF, S, basis="SCFT")
+    got_u, got_t = s.Compute_force_feed_shell(0), s.Compute_force_feed_shell(2)
+    assert np.abs(got_u - want_u).max() <= 1e-12 * np.abs(want_u).max()
+    assert np.abs(got_t - want_t).max() <= 1e-12 * np.abs(want_t).max()
