@@ -371,8 +371,11 @@ int tg_force_feed_ring(tg_ctx* ctx, int group, int cylinder, int axis, int n_rin
  * No cudaMalloc/cudaFree or allocating library call: the per-block partial sums live in a
  * fixed device array of 8 x 1184 x 2 doubles (151,552 bytes) that every GPU loading this library
  * holds until exit.  Limit: 1 <= n_fields <= TG_NOALLOC_MAX_FIELDS; anything beyond returns
- * TG_ERR_ARG.  The first call on a device looks up that array's device address (with the
- * caller's current device) and caches it: make that first call before any stream capture.
+ * TG_ERR_ARG.  d_fields must lie on a 16-byte boundary (the fields are read as 16-byte complex
+ * values) and d_out on an 8-byte boundary; otherwise TG_ERR_ARG.  The first call in a CUDA
+ * context looks up that array's device address in the context current on the calling thread
+ * and caches it per context (keyed on the context's unique id, so a reset device or a caller's
+ * own context gets its own lookup): make that first call before any stream capture.
  * Work is queued on `stream` (cudaStream_t; NULL = default stream) and the call returns
  * without waiting.  Every call shares the array and it keeps the last call's partials; calls
  * that overlap on the GPU (different streams, or concurrent host threads) race on it.
@@ -397,6 +400,25 @@ typedef struct tg_kernel_stat {
 int tg_profile_enable(tg_ctx* ctx, int enable);
 /* synchronises; fills up to max stats, sets *n; clears the records */
 int tg_profile_read(tg_ctx* ctx, tg_kernel_stat* out, int max, int* n);
+
+/* ------------------------------------------------------------------------------------------
+ * Failure-path test hook (no counterpart in the reference, which has no bounded waits).
+ *
+ * The TMA-staged transform passes wait for each tile with a bounded number of polls; a block
+ * whose wait runs out skips its tile (its output is not written), waits again with the full
+ * limit so that its copy lands before it leaves, and sets the context's status word.  The next
+ * call that synchronises the context (tg_step after each chunk, tg_synchronize, downloads,
+ * energies, spectra, transfer tables, ...) then returns TG_ERR_TIMEOUT with a message in
+ * tg_last_error and clears the word: the fields written since the last check are not valid,
+ * the context itself stays usable.  In the serving loop the requests of that batch fail with
+ * TG_ERR_TIMEOUT.
+ *
+ * TG_DEBUG_SHORT_TMA_WAIT (value 1 / 0) gives the first wait for a tile no polls at all, so
+ * every TMA-staged block reports a timeout; value 0 restores the normal limit.  Changing it
+ * drops the context's captured step graph.  For tests of the failure path only.
+ * ---------------------------------------------------------------------------------------- */
+#define TG_DEBUG_SHORT_TMA_WAIT 1
+int tg_debug_set(tg_ctx* ctx, int what, long long value);
 
 /* ------------------------------------------------------------------------------------------
  * Serving (no counterpart in the reference, whose programs run one solve per process,

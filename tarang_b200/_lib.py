@@ -18,6 +18,7 @@ TG_ERR_NONFINITE = -3
 TG_ERR_CUDA = -4
 TG_ERR_UNSUPPORTED = -5
 TG_ERR_TIMEOUT = -6
+TG_DEBUG_SHORT_TMA_WAIT = 1
 TG_ERR_STATE = -7
 TG_ERR_BUSY = -8
 
@@ -195,6 +196,7 @@ SIGNATURES = {
     "tg_force_feed_ring": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _DP, C.c_int]),
     "tg_energy_noalloc": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_int, _VP, _VP]),
     "tg_profile_enable": (C.c_int, [_VP, C.c_int]),
+    "tg_debug_set": (C.c_int, [_VP, C.c_int, C.c_longlong]),
     "tg_profile_read": (C.c_int, [_VP, C.POINTER(tg_kernel_stat), C.c_int, C.POINTER(C.c_int)]),
     "tg_server_create": (C.c_int, [C.POINTER(tg_server_config), C.POINTER(_VP)]),
     "tg_server_destroy": (C.c_int, [_VP]),

@@ -37,6 +37,30 @@ int dalloc_ctx(tg_ctx* c, void** p, size_t bytes) {
   return TG_OK;
 }
 
+void wait_args(const tg_ctx* c, AxisArgs& a) {
+  a.wait_flag = c->wait_status;
+  a.wait_short = c->wait_short;
+}
+
+int ctx_sync(tg_ctx* c, const char* where) {
+  cudaError_t e = cudaSuccess;
+  if (c->wait_status && c->h_wait) {
+    *c->h_wait = 0;
+    e = cudaMemcpyAsync(c->h_wait, c->wait_status, sizeof(int), cudaMemcpyDeviceToHost, c->st);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+  if (e != cudaSuccess) return cuda_err(c, e, where);
+  if (c->h_wait && *c->h_wait) {
+    *c->h_wait = 0;
+    e = cudaMemsetAsync(c->wait_status, 0, sizeof(int), c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    if (e != cudaSuccess) return cuda_err(c, e, where);
+    return set_err(c, TG_ERR_TIMEOUT,
+                   std::string(where) + ": a transform pass gave up waiting for its tile; the fields it wrote are not valid");
+  }
+  return TG_OK;
+}
+
 }  // namespace tg
 
 #define TG_CK(call)                                        \
@@ -348,6 +372,7 @@ int dense_transform(tg_ctx* c, cx<double>* f, int forward, int parity) {
     // inverse: x then y; forward: y then x
     const bool xpass = forward ? (pass == 1) : (pass == 0);
     AxisLaunch l;
+    wait_args(c, l.a);
     l.dir = forward ? -1 : +1;
     l.pin = F64;
     l.pout = F64;
@@ -446,6 +471,7 @@ void free_ctx(tg_ctx* c) {
   }
   for (auto e : c->ev_pool) cudaEventDestroy(e);
   if (c->h_pinned) cudaFreeHost(c->h_pinned);
+  if (c->h_wait) cudaFreeHost(c->h_wait);
   if (c->own_stream && c->st) cudaStreamDestroy(c->st);
   delete c;
 }
@@ -701,7 +727,10 @@ int ctx_create_batch(const tg_config* cfg, int B, tg_ctx** out) {
   c->ering_cap = 1 << 16;
   if ((rc = dalloc(c, (void**)&c->ering, sizeof(double) * c->ering_cap))) return fail(rc);
   if ((rc = dalloc(c, (void**)&c->ering_pos, sizeof(int) * 4))) return fail(rc);
+  c->wait_status = c->ering_pos + 2;
   if (cudaMallocHost(&c->h_pinned, sizeof(double) * 1024) != cudaSuccess) return fail(TG_ERR_OOM);
+  if (cudaMallocHost(&c->h_wait, sizeof(int) * 4) != cudaSuccess) return fail(TG_ERR_OOM);
+  *c->h_wait = 0;
   {
     // per request: dt, t, steps, non-finite flag, Tdt
     std::vector<double> init((size_t)8 * B, 0.0);
@@ -907,9 +936,23 @@ int tg_ctx_destroy(tg_ctx* c) {
   return TG_OK;
 }
 
+int tg_debug_set(tg_ctx* c, int what, long long value) {
+  if (!c) return TG_ERR_ARG;
+  if (what != TG_DEBUG_SHORT_TMA_WAIT || (value != 0 && value != 1)) return TG_ERR_ARG;
+  cudaSetDevice(c->dev);
+  TG_SYNC(c, "tg_debug_set");
+  c->wait_short = (int)value;
+  // the step graph holds the pass arguments it was captured with
+  if (c->step_graph) {
+    cudaGraphExecDestroy(c->step_graph);
+    c->step_graph = nullptr;
+  }
+  return TG_OK;
+}
+
 int tg_synchronize(tg_ctx* c) {
   if (!c) return TG_ERR_ARG;
-  TG_CK(cudaStreamSynchronize(c->st));
+  TG_SYNC(c, __func__);
   return TG_OK;
 }
 
@@ -973,7 +1016,7 @@ int tg_field_download_stored(tg_ctx* c, int field, double* host, size_t n) {
   if (si < 0) return set_err(c, TG_ERR_ARG, "download_stored: state fields only");
   cudaSetDevice(c->dev);
   TG_CK(copy_stored(c, c->U0[si], host, false));
-  TG_CK(cudaStreamSynchronize(c->st));
+  TG_SYNC(c, __func__);
   return TG_OK;
 }
 
@@ -987,13 +1030,13 @@ int tg_field_upload(tg_ctx* c, int field, const double* host, size_t n) {
     int rc = ensure_dense(c, field);
     if (rc) return rc;
     TG_CK(cudaMemcpyAsync(c->dense[field], host, sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
-    TG_CK(cudaStreamSynchronize(c->st));
+    TG_SYNC(c, __func__);
     return TG_OK;
   }
   if (si >= 0) {
     // state fields: only the stored modes cross the bus, straight into the compact rows
     TG_CK(copy_stored(c, c->U0[si], const_cast<double*>(host), true));
-    TG_CK(cudaStreamSynchronize(c->st));
+    TG_SYNC(c, __func__);
     c->energy_valid = false;
     c->have_nlin = c->have_pressure = c->have_force = false;
     return TG_OK;
@@ -1006,7 +1049,7 @@ int tg_field_upload(tg_ctx* c, int field, const double* host, size_t n) {
   if (rc) return rc;
   TG_CK(cudaMemcpyAsync(c->staging, host, sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
   TG_CK(launch_dense_to_compact(c->g, c->staging, target, 0, c->st));
-  TG_CK(cudaStreamSynchronize(c->st));
+  TG_SYNC(c, __func__);
   if (si >= 0) {
     c->energy_valid = false;
     c->have_nlin = c->have_pressure = c->have_force = false;
@@ -1021,7 +1064,7 @@ int tg_field_download(tg_ctx* c, int field, double* host, size_t n) {
   if (field >= TG_WORK0 && field < TG_WORK0 + TG_NWORK) {
     if (!c->dense[field]) return set_err(c, TG_ERR_STATE, "download: work field never written");
     TG_CK(cudaMemcpyAsync(host, c->dense[field], sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
-    TG_CK(cudaStreamSynchronize(c->st));
+    TG_SYNC(c, __func__);
     return TG_OK;
   }
   if (field >= TG_FORCE1 && field <= TG_FORCE3) {
@@ -1061,7 +1104,7 @@ int tg_field_download(tg_ctx* c, int field, double* host, size_t n) {
     const int comp = field - TG_FORCE1;
     TG_CK(cudaMemcpyAsync(box.data(), c->FB + (size_t)comp * c->fbox, sizeof(cx<double>) * c->fbox,
                           cudaMemcpyDeviceToHost, c->st));
-    TG_CK(cudaStreamSynchronize(c->st));
+    TG_SYNC(c, __func__);
     const int ny = 2 * c->fy + 1, nz = c->fz + 1;
     for (int p = 0; p < c->fbox; ++p) {
       const int kz = p % nz, ky = (p / nz) % ny - c->fy, kx = p / (nz * ny) - c->fx;
@@ -1085,7 +1128,7 @@ int tg_field_download(tg_ctx* c, int field, double* host, size_t n) {
   if (rc) return rc;
   TG_CK(launch_compact_to_dense(c->g, src, sp, c->staging, c->st));
   TG_CK(cudaMemcpyAsync(host, c->staging, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
-  TG_CK(cudaStreamSynchronize(c->st));
+  TG_SYNC(c, __func__);
   return TG_OK;
 }
 
@@ -1111,7 +1154,7 @@ int tg_field_free(tg_ctx* c, int field) {
   const int i = field - TG_WORK0;
   if (!c->work_reserved[i]) return set_err(c, TG_ERR_STATE, "free: work field not reserved");
   cudaSetDevice(c->dev);
-  TG_CK(cudaStreamSynchronize(c->st));
+  TG_SYNC(c, __func__);
   if (c->dense[field]) {
     cudaFree(c->dense[field]);
     c->bytes -= sizeof(cx<double>) * (size_t)c->D;
@@ -1225,7 +1268,7 @@ int tg_set_force_modes(tg_ctx* c, int n, const int* k, const double* F) {
       h[(size_t)q * box + p].y = F[(size_t)2 * ns * i + 2 * q + 1];
     }
   }
-  TG_CK(cudaStreamSynchronize(c->st));
+  TG_SYNC(c, __func__);
   // a captured step reads the box's address and extents
   if (c->step_graph) {
     cudaGraphExecDestroy(c->step_graph);
@@ -1246,7 +1289,7 @@ int tg_set_force_modes(tg_ctx* c, int n, const int* k, const double* F) {
       if (rc) return rc;
     }
     TG_CK(cudaMemcpyAsync(c->FB, h.data(), sizeof(cx<double>) * h.size(), cudaMemcpyHostToDevice, c->st));
-    TG_CK(cudaStreamSynchronize(c->st));
+    TG_SYNC(c, __func__);
   }
   c->force_ever = true;
   return TG_OK;
@@ -1311,7 +1354,7 @@ int tg_get_dt(tg_ctx* c, double* dt) {
   c->energy_valid = true;
   if (dt) {
     TG_CK(cudaMemcpyAsync(c->h_pinned, c->scal, sizeof(double), cudaMemcpyDeviceToHost, c->st));
-    TG_CK(cudaStreamSynchronize(c->st));
+    TG_SYNC(c, __func__);
     *dt = c->h_pinned[0];
   }
   return TG_OK;
@@ -1370,7 +1413,7 @@ int tg_step(tg_ctx* c, int n, double* energies) {
       TG_CK(cudaMemcpyAsync(energies + done, c->ering, sizeof(double) * chunk, cudaMemcpyDeviceToHost, c->st));
     }
     TG_CK(cudaMemcpyAsync(c->h_pinned, c->scal, sizeof(double) * 8, cudaMemcpyDeviceToHost, c->st));
-    TG_CK(cudaStreamSynchronize(c->st));
+    TG_SYNC(c, __func__);
     done += chunk;
     if (c->h_pinned[3] != 0.0) return set_err(c, TG_ERR_NONFINITE, "ERROR: Numerical Overflow (total energy is not finite)");
   }
@@ -1400,7 +1443,7 @@ int tg_energy(tg_ctx* c, int group, double* energy, double* diss) {
   int rc = run_energy(c, 0);
   if (rc) return rc;
   TG_CK(cudaMemcpyAsync(c->h_pinned, c->red_out, sizeof(double) * 8, cudaMemcpyDeviceToHost, c->st));
-  TG_CK(cudaStreamSynchronize(c->st));
+  TG_SYNC(c, __func__);
   const int s = group * 2;
   // CV_total_energy and CV_total_dissipation = 2 sum mult K^2 |u|^2 (Cvf.cc:385-397)
   if (energy) *energy = c->h_pinned[s];
@@ -1455,7 +1498,7 @@ int tg_shell_spectrum(tg_ctx* c, int group, double* ek, double* dissk, int n) {
   }
   std::vector<double> h(need);
   TG_CK(cudaMemcpyAsync(h.data(), dbuf, sizeof(double) * need, cudaMemcpyDeviceToHost, c->st));
-  TG_CK(cudaStreamSynchronize(c->st));
+  TG_SYNC(c, __func__);
   // Sk_count of the reference runs over every mode of its dense array, the dealiased zeros
   // included (four_energy.cc:271-286, scft_energy.cc:266-281): geometry only, computed once
   if ((int)c->shell_count.size() != nbins) {
@@ -1500,7 +1543,7 @@ int tg_profile_enable(tg_ctx* c, int enable) {
 int tg_profile_read(tg_ctx* c, tg_kernel_stat* out, int max, int* n) {
   if (!c || (max > 0 && !out)) return TG_ERR_ARG;
   cudaSetDevice(c->dev);
-  TG_CK(cudaStreamSynchronize(c->st));
+  TG_SYNC(c, __func__);
   std::vector<tg_kernel_stat> agg;
   for (auto& r : c->prof_recs) {
     float ms = 0;
@@ -1537,7 +1580,7 @@ int tg_nusselt(tg_ctx* c, double* nu) {
   TG_CK(launch_cross_partials(c->g, c->U0[0], c->U0[3], c->part, 0, 8, c->st, &nb));
   std::vector<double> h((size_t)nb * 8);
   TG_CK(cudaMemcpyAsync(h.data(), c->part, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->st));
-  TG_CK(cudaStreamSynchronize(c->st));
+  TG_SYNC(c, __func__);
   double cross = 0;
   for (int b = 0; b < nb; ++b) cross += h[(size_t)b * 8];
   *nu = 1.0 + rb_coefficients(&c->cfg).nuf * cross;

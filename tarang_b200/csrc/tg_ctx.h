@@ -76,7 +76,12 @@ struct tg_ctx {
   double* part = nullptr;   // per slot [nblocks][8]
   int npart_blocks = 0;
   double* ering = nullptr;  // energy per step of the current tg_step call
-  int* ering_pos = nullptr;
+  int* ering_pos = nullptr;   // [0] ring position, [2] bounded-wait status (wait_status)
+  // 1 when a TMA-staged pass of this context gave up waiting for its tile since the last
+  // check (points into the ering_pos allocation); read and cleared by ctx_sync
+  int* wait_status = nullptr;
+  int* h_wait = nullptr;      // pinned host copy of *wait_status
+  int wait_short = 0;         // test hook (tg_debug_set): first TMA wait gets no polls
   int ering_cap = 0;
   double* h_pinned = nullptr;  // small pinned host buffer
   double* diag = nullptr;      // diagnostics scratch (spectra, transfer tables)
@@ -127,6 +132,17 @@ struct tg_ctx {
 namespace tg {
 int set_err(tg_ctx* c, int code, const std::string& msg);
 int cuda_err(tg_ctx* c, cudaError_t e, const char* where);
+// the context's bounded-wait status word and test hook, into the arguments of an axis pass
+void wait_args(const tg_ctx* c, AxisArgs& a);
+// synchronises the context's stream, then reports a TMA-staged pass that gave up waiting for
+// its tile since the last check (TG_ERR_TIMEOUT: the results of that work are not valid; the
+// word is cleared, so the context stays usable) or a CUDA error
+int ctx_sync(tg_ctx* c, const char* where);
+#define TG_SYNC(c, where)                      \
+  do {                                         \
+    const int _rs = tg::ctx_sync((c), (where)); \
+    if (_rs) return _rs;                       \
+  } while (0)
 
 // per-launch CUDA events while profiling is enabled (tg_profile_enable)
 struct ProfScope {

@@ -303,8 +303,8 @@ int et_tables_ptr(tg_ctx* c, const cx<double>* const* Hp, const cx<double>* cons
   }
   std::vector<double> h(need);
   e = cudaMemcpyAsync(h.data(), c->diag, sizeof(double) * need, cudaMemcpyDeviceToHost, c->st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
   if (e != cudaSuccess) return cuda_err(c, e, "et tables");
+  TG_SYNC(c, "et tables");
   T.assign((size_t)nrec * (A + 1) * nb, 0.0);
   for (int n = 1; n <= A; ++n)
     for (int r = 0; r < nrec; ++r)
@@ -759,8 +759,8 @@ int tg_force_feed_group(tg_ctx* c, int group, double* feed, int n) {
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaMemcpyAsync(feed, d, sizeof(double) * (S + 1), cudaMemcpyDeviceToHost, c->st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
   if (e != cudaSuccess) return cuda_err(c, e, "force feed");
+  TG_SYNC(c, "force feed");
   return TG_OK;
 }
 

@@ -34,6 +34,13 @@ struct AxisArgs {
   double scale;       // output scale
   const cx<double>* tw;  // exp(-2 pi i m / L), m in [0, L)
   int comb[kMaxPtr];  // per field: 0, or +1 / -1 to read src + comb * src2 (Elsasser z+-)
+  // TMA-staged passes: set to 1 by a block whose tile did not arrive within the bounded wait
+  // (the owning context's status word; null: a library-wide word)
+  int* wait_flag;
+  // test hook: 1 gives the first wait for a tile no polls at all, so every block reports a
+  // timeout (the second, draining wait keeps its full limit and the copy lands before the
+  // block leaves)
+  int wait_short;
 };
 
 // ------------------------------------------------------------------------------------------

@@ -74,10 +74,10 @@ __global__ void __launch_bounds__(kTmaW * R1, AxisOcc<Rw, kTmaW * R1>::v)
     tw[i] = t;
   }
   if (tid == 0) {
-    const bool ok = mbar_wait_bounded(bar, 0, kTmaPolls);
+    const bool ok = mbar_wait_bounded(bar, 0, a.wait_short ? 0 : kTmaPolls);
     *ok_flag = ok ? 1 : 0;
     if (!ok) {
-      atomicExch(&g_axis_tma_timeout, 1);
+      atomicExch(a.wait_flag ? a.wait_flag : &g_axis_tma_timeout, 1);
       mbar_wait_bounded(bar, 0, kTmaPolls);  // let a late copy land before the block leaves
     }
   }

@@ -1,6 +1,9 @@
 // tg_energy_noalloc: the energy / dissipation reduction of tg_energy for callers that cannot
 // allocate device memory.  Its per-block partial sums live in a fixed file-scope device array
 // instead of context-owned scratch, so the call allocates nothing.
+#include <cuda.h>
+
+#include <map>
 #include <mutex>
 
 #include "../../include/tarang_gpu.h"
@@ -18,10 +21,46 @@ constexpr int kMaxFields = TG_NOALLOC_MAX_FIELDS;
 // every call on a device and left holding the last call's partials.
 static __device__ __align__(256) double g_energy_partials[kMaxFields * kBlocks * 2];
 
-// Device address of g_energy_partials per device (the host-side name is only a stand-in).
-constexpr int kMaxDevices = 64;
-double* g_partials_addr[kMaxDevices] = {};
+// Device address of g_energy_partials per CUDA context (the host-side name is only a
+// stand-in).  The address belongs to the context that loaded the module, so the cache is keyed
+// on the context's unique id (cuCtxGetId never repeats within a process), not on the device
+// ordinal: after cudaDeviceReset, or with a caller's own non-primary context current, the
+// lookup runs again.
 std::mutex g_partials_mu;
+std::map<unsigned long long, double*> g_partials_addr;
+
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+
+template <typename Fn>
+Fn driver_fn(const char* name) {
+  void* p = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q) == cudaSuccess && q == cudaDriverEntryPointSuccess)
+    return reinterpret_cast<Fn>(p);
+  cudaGetLastError();
+  return nullptr;
+}
+
+// unique id of the context current on this thread; with none current yet, the symbol lookup
+// (which initialises the runtime's primary context of the current device) runs first
+int current_context_id(unsigned long long* id) {
+  static CtxGetCurrentFn get_current = driver_fn<CtxGetCurrentFn>("cuCtxGetCurrent");
+  static CtxGetIdFn get_id = driver_fn<CtxGetIdFn>("cuCtxGetId");
+  if (!get_current || !get_id) return TG_ERR_CUDA;
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) != CUDA_SUCCESS) return TG_ERR_CUDA;
+  if (ctx == nullptr) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_energy_partials) != cudaSuccess) {
+      cudaGetLastError();
+      return TG_ERR_CUDA;
+    }
+    if (get_current(&ctx) != CUDA_SUCCESS || ctx == nullptr) return TG_ERR_CUDA;
+  }
+  if (get_id(ctx, id) != CUDA_SUCCESS) return TG_ERR_CUDA;
+  return TG_OK;
+}
 
 struct DenseArgs {
   const cx<double>* f;   // n_fields consecutive fields, reference layout
@@ -109,17 +148,23 @@ __global__ void __launch_bounds__(kThreads) k_energy_dense_final(const double* p
   }
 }
 
-// once per device, with that device current
+// once per context, with that context current
 int partials_address(double** out) {
-  int dev = -1;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return TG_ERR_CUDA;
+  unsigned long long id = 0;
+  int rc = current_context_id(&id);
+  if (rc) return rc;
   std::lock_guard<std::mutex> lock(g_partials_mu);
-  if (!g_partials_addr[dev]) {
+  auto it = g_partials_addr.find(id);
+  if (it == g_partials_addr.end()) {
     void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_energy_partials) != cudaSuccess || p == nullptr) return TG_ERR_CUDA;
-    g_partials_addr[dev] = static_cast<double*>(p);
+    if (cudaGetSymbolAddress(&p, g_energy_partials) != cudaSuccess || p == nullptr) {
+      cudaGetLastError();
+      return TG_ERR_CUDA;
+    }
+    if (g_partials_addr.size() >= 4096) g_partials_addr.clear();
+    it = g_partials_addr.emplace(id, static_cast<double*>(p)).first;
   }
-  *out = g_partials_addr[dev];
+  *out = it->second;
   return TG_OK;
 }
 
@@ -129,6 +174,8 @@ extern "C" int tg_energy_noalloc(const double* d_fields, int n_fields, const int
                                  int dealias, double* d_out, void* stream) {
   if (!d_fields || !d_out || !N || !kfactor) return TG_ERR_ARG;
   if (n_fields < 1 || n_fields > kMaxFields) return TG_ERR_ARG;   // scratch holds 8 fields
+  // the fields are read as 16-byte complex values, the output written as doubles
+  if (((uintptr_t)d_fields & 15) != 0 || ((uintptr_t)d_out & 7) != 0) return TG_ERR_ARG;
   if (N[0] < 2 || N[1] < 2 || N[2] < 2 || (N[2] & 1)) return TG_ERR_ARG;
   if (!(kfactor[0] > 0 && kfactor[1] > 0 && kfactor[2] > 0)) return TG_ERR_ARG;
   double* part = nullptr;

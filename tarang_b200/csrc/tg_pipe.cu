@@ -45,6 +45,7 @@ int pipe_inverse_xy(tg_ctx* c, int nf, const void* const* in, const void* const*
   const Geo& g = c->g;
   {
     AxisLaunch l;
+    wait_args(c, l.a);
     l.L = c->N1;
     l.dir = +1;
     l.pin = inprec;
@@ -88,6 +89,7 @@ int pipe_inverse_xy(tg_ctx* c, int nf, const void* const* in, const void* const*
   }
   {
     AxisLaunch l;
+    wait_args(c, l.a);
     l.L = c->N2;
     l.dir = +1;
     l.pin = l.pout = l.pwork = c->tprec;
@@ -142,6 +144,7 @@ int pipe_products_forward(tg_ctx* c, int nin, const void* const* WY, int nprod, 
   }
   {
     AxisLaunch l;
+    wait_args(c, l.a);
     l.L = c->N2;
     l.dir = -1;
     l.pin = l.pout = l.pwork = c->tprec;
@@ -166,6 +169,7 @@ int pipe_products_forward(tg_ctx* c, int nin, const void* const* WY, int nprod, 
   }
   {
     AxisLaunch l;
+    wait_args(c, l.a);
     l.L = c->N1;
     l.dir = -1;
     l.pin = l.pout = l.pwork = c->tprec;

@@ -220,8 +220,8 @@ int run_ring(tg_ctx* c, int group, int axis, int n, int cyl, double* ek1, double
   e = cudaGetLastError();
   std::vector<double> h((size_t)4 * nbins);
   if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), a.out, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
   if (e != cudaSuccess) return cuda_err(c, e, "ring spectrum");
+  TG_SYNC(c, "ring spectrum");
   for (int i = 0; i < nbins; ++i) {
     ek1[i] = h[i];
     if (ek2) ek2[i] = h[nbins + i];
@@ -553,8 +553,8 @@ int run_ring_tr(tg_ctx* c, int kind, int axis, int n_ring_shells, int n_sectors,
     }
   std::vector<double> h(need);
   e = cudaMemcpyAsync(h.data(), c->diag, sizeof(double) * need, cudaMemcpyDeviceToHost, c->st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
   if (e != cudaSuccess) return cuda_err(c, e, "ring transfer");
+  TG_SYNC(c, "ring transfer");
   for (size_t q = 0; q < need; ++q) tr[q] = sign * h[q];
   return TG_OK;
 }
@@ -625,8 +625,8 @@ int tg_shell_spectrum_helicity(tg_ctx* c, int group, double* h1, double* h2, dou
   e = cudaGetLastError();
   std::vector<double> hh((size_t)3 * nbins);
   if (e == cudaSuccess) e = cudaMemcpyAsync(hh.data(), c->diag, sizeof(double) * hh.size(), cudaMemcpyDeviceToHost, c->st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
   if (e != cudaSuccess) return cuda_err(c, e, "helicity spectrum");
+  TG_SYNC(c, "helicity spectrum");
   // H1k_count: 2 mult over every mode of the dense grid (geometry only); partial shells
   // (kmax_inside, kmax] rescaled by Approx_number_modes_in_shell / count (four_energy.cc:637-651)
   std::vector<double> cnt(nbins, 0.0);
@@ -696,8 +696,8 @@ int tg_force_feed_ring(tg_ctx* c, int group, int cylinder, int axis, int n_ring_
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaMemcpyAsync(out, c->diag, sizeof(double) * per, cudaMemcpyDeviceToHost, c->st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
   if (e != cudaSuccess) return cuda_err(c, e, "ring force feed");
+  TG_SYNC(c, "ring force feed");
   return TG_OK;
 }
 

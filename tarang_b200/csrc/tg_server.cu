@@ -441,11 +441,13 @@ int steps_this_round(const tg_server* s, const Batch& b, double slowest_ms) {
 // finished and non-finite requests, keep the slots dense
 int collect_batch(tg_server* s, Batch& b, int nl, int launch_rc) {
   tg_ctx* c = b.c;
-  cudaError_t e = cudaStreamSynchronize(c->st);
+  // a bounded wait that ran out (TG_ERR_TIMEOUT) fails every request of this batch; the
+  // batch itself stays usable for later requests
+  const int sync_rc = ctx_sync(c, "batch step");
   for (auto& blk : b.loading) s->pinned.put(blk.first, blk.second);
   b.loading.clear();
-  if (launch_rc || e != cudaSuccess) {
-    const int code = launch_rc ? launch_rc : cuda_err(c, e, "batch step");
+  if (launch_rc || sync_rc) {
+    const int code = launch_rc ? launch_rc : sync_rc;
     s->err = c->err;
     for (long long id : b.slot_req) finish_req(s, s->reqs[id], TG_REQ_FAILED, code);
     b.slot_req.clear();

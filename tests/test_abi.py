@@ -87,3 +87,19 @@ def test_request_bytes_without_gpu(lib):
         raise AssertionError("negative dt accepted")
     except _lib.TarangError as e:
         assert e.code == _lib.TG_ERR_ARG
+
+
+def test_energy_noalloc_rejects_bad_arguments_without_gpu(lib):
+    """Argument checks of the allocation-free energy reduction run before any CUDA call: more
+    fields than its fixed scratch holds, fields not on a 16-byte boundary (they are read as
+    16-byte complex values), an output not on an 8-byte boundary."""
+    from tarang_b200 import _lib
+    n3 = (ctypes.c_int * 3)(16, 16, 16)
+    kf = (ctypes.c_double * 3)(1.0, 1.0, 1.0)
+    ok16 = ctypes.c_void_p(4096)   # never dereferenced: each call is rejected before any launch
+    assert lib.tg_energy_noalloc(ok16, 9, n3, kf, 1, ok16, None) == _lib.TG_ERR_ARG
+    assert lib.tg_energy_noalloc(ok16, 0, n3, kf, 1, ok16, None) == _lib.TG_ERR_ARG
+    assert lib.tg_energy_noalloc(ctypes.c_void_p(4096 + 8), 3, n3, kf, 1, ok16, None) == _lib.TG_ERR_ARG
+    assert lib.tg_energy_noalloc(ok16, 3, n3, kf, 1, ctypes.c_void_p(4096 + 4), None) == _lib.TG_ERR_ARG
+    odd = (ctypes.c_int * 3)(16, 16, 15)
+    assert lib.tg_energy_noalloc(ok16, 3, odd, kf, 1, ok16, None) == _lib.TG_ERR_ARG

@@ -319,13 +319,24 @@ def test_read_para_convection(lib):
 
 
 def test_reference_para_files_parse(lib):
-    """The reference's own example para.d files, where the reference tree is present."""
+    """The reference's own example para.d files (trunk/info/new4.21/{fluid3d,mhd3d,RB}/in/para.d,
+    copied into tests/golden/para by tests/golden/make_para_fixtures.py)."""
+    import math
     import os
     from tarang_b200.para import config_from_para, read_para
-    base = "/root/reference/trunk/info/new4.21"
-    if not os.path.isdir(base):
-        pytest.skip("reference tree absent")
+    from tarang_b200.solver import make_config
+    base = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "para")
+    got = {}
     for kind, d, n in (("FLUID", "fluid3d", 1), ("MHD", "mhd3d", 2), ("RB", "RB", 2)):
-        path = os.path.join(base, d, "in", "para.d")
-        c = config_from_para(read_para(path, n_fields=n), kind)
-        assert c["basis"] in ("FOUR", "SCFT") and c["dt"] > 0 and c["n_shells"] > 0
+        c = config_from_para(read_para(os.path.join(base, d + ".para.d"), n_fields=n), kind)
+        assert c["dt"] == 1e-3 and c["n_shells"] == 10 and c["dealias"] is True
+        assert c["run"]["Tfinal"] == 0.005 and c["run"]["N_out_reduced"] == (4, 4, 4)
+        kw = dict(c)
+        kw.pop("run")
+        make_config(**kw)
+        got[kind] = c
+    assert got["FLUID"]["N"] == (8, 8, 8) and got["FLUID"]["basis"] == "FOUR"
+    assert got["MHD"]["N"] == (16, 16, 16) and got["MHD"]["physics"] == "MHD"
+    rb = got["RB"]
+    assert rb["basis"] == "SCFT" and rb["Pr"] == 6.8 and rb["Pr_switch"] == "PRLARGE"
+    assert rb["RB_Uscaling"] == "USMALL" and abs(rb["kfactor"][1] - math.pi / math.sqrt(2.0)) < 1e-15

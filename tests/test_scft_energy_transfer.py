@@ -74,18 +74,35 @@ def test_gpu_scft_flux_and_shell_tr(lib, Nn):
 
 
 @pytest.mark.gpu
-def test_gpu_convection_force_feed(lib):
-    """Compute_force_feed_shell_RB (PRLARGE): the buoyancy force fu theta fed into u1 and the
-    force ft u1 fed into theta, per energy-transfer shell in the SCFT basis."""
+@pytest.mark.parametrize("basis", ["FOUR", "SCFT"])
+@pytest.mark.parametrize("pr_switch,u_scaling", [("PRLARGE", "USMALL"), ("PRLARGE", "ULARGE"),
+                                                 ("PRSMALL", "USMALL"), ("PRSMALL", "ULARGE")])
+def test_gpu_convection_force_feed(lib, basis, pr_switch, u_scaling):
+    """Compute_force_feed_shell_RB: the buoyancy force fu theta fed into u1 and the force
+    ft u1 fed into theta, per energy-transfer shell, in both bases and for every
+    nondimensionalisation.  Pr != 1 and a temperature gradient of -1 keep fu, ft and the
+    scalings apart (at Pr = 1 PRLARGE/USMALL has ft = 1 and a swap of fu and ft would pass)."""
     from tarang_b200.solver import IncFluid
-    V, T = scft_fields(N, 13)
-    s = IncFluid(N, basis="SCFT", physics="RB", Ra=1e6, Pr=1.0, kfactor=KF, dt=1e-4, n_shells=S)
-    s.set_V(V)
-    s.set_T(T)
-    _, _, fu, ft, _ = o.rb_coefficients(1e6, 1.0)
-    z = np.zeros_like(T)
-    want_u = o.force_feed_shell([fu * T, z, z], V, KF, S, basis="SCFT")
-    want_t = o.force_feed_shell([ft * V[0]], [T], KF, S, basis="SCFT")
-    got_u, got_t = s.Compute_force_feed_shell(0), s.Compute_force_feed_shell(2)
+    Ra, Pr, tg = 2.0e5, 0.7, -1.0
+    if basis == "SCFT":
+        Nn, kf = N, KF
+        V, T = scft_fields(N, 13)
+    else:
+        Nn, kf = (32, 32, 32), (1.0, 1.0, 1.0)
+        rng = np.random.default_rng(14)
+        V = [o.dealias(o.forward_four(rng.standard_normal(Nn))) for _ in range(3)]
+        T = o.dealias(o.forward_four(rng.standard_normal(Nn)))
+    s = IncFluid(Nn, basis=basis, physics="RB", Ra=Ra, Pr=Pr, kfactor=kf, dt=1e-4, n_shells=S,
+                 Pr_switch=pr_switch, RB_Uscaling=u_scaling, temperature_grad=tg)
+    try:
+        s.set_V(V)
+        s.set_T(T)
+        _, _, fu, ft, _ = o.rb_coefficients(Ra, Pr, pr_switch, u_scaling, tg)
+        z = np.zeros_like(T)
+        want_u = o.force_feed_shell([fu * T, z, z], V, kf, S, basis=basis)
+        want_t = o.force_feed_shell([ft * V[0]], [T], kf, S, basis=basis)
+        got_u, got_t = s.Compute_force_feed_shell(0), s.Compute_force_feed_shell(2)
+    finally:
+        s.close()
     assert np.abs(got_u - want_u).max() <= 1e-12 * np.abs(want_u).max()
     assert np.abs(got_t - want_t).max() <= 1e-12 * np.abs(want_t).max()
