@@ -1602,3 +1602,34 @@ def unpack_real(packed):
     out[:, :, 0::2] = packed[:, :, : N3 // 2].real
     out[:, :, 1::2] = packed[:, :, : N3 // 2].imag
     return out
+
+
+# --------------------------------------------------------------------------------------
+# Test infrastructure: a random-projection sketch of a set of spectral fields, so that golden
+# fixtures of large grids can hold a few numbers per field instead of the fields themselves.
+# --------------------------------------------------------------------------------------
+
+def sketch(fields, n_proj=64, seed=7919):
+    """Projections p_j = sum over every entry of Re(F) Re(w_j) + Im(F) Im(w_j), j < n_proj, of
+    the fields (concatenated), with weights w_j uniform in [-1, 1] per real component from the
+    seeded PCG64 stream (seed, j).  For a difference d of two field sets, the projections of
+    d have variance |d|^2 / 3, so rel_from_sketch estimates |d| / |F| (within ~20 % for 64
+    projections).  Returns (p, |F|)."""
+    flat = [np.ascontiguousarray(f).view(np.float64).ravel() for f in fields]
+    n = sum(x.size for x in flat)
+    p = np.zeros(n_proj)
+    for j in range(n_proj):
+        rng = np.random.Generator(np.random.PCG64([seed, j]))
+        w = rng.random(n) * 2.0 - 1.0
+        o = 0
+        for x in flat:
+            p[j] += float(np.dot(x, w[o:o + x.size]))
+            o += x.size
+    norm = math.sqrt(sum(float(np.dot(x, x)) for x in flat))
+    return p, norm
+
+
+def rel_from_sketch(p_got, p_want, norm_want):
+    """Estimate of |F_got - F_want| / |F_want| from two sketches with the same weights."""
+    d = np.asarray(p_got) - np.asarray(p_want)
+    return math.sqrt(3.0 * float(np.dot(d, d)) / len(d)) / norm_want

@@ -323,6 +323,7 @@ struct ZArgs {
   double scale;
   const cx<double>* twM;  // exp(-2 pi i m / M), m in [0, M)
   const cx<double>* twN;  // exp(-2 pi i k / N), k in [0, N), N = 2M
+  const cx<double>* oct;  // N = 256: coefficient table of k_z_prod_oct (zoct_table), or null
 };
 
 // c2r pre-twiddle: Z[k] = (X[k] + conj(X[M-k])) + i e^{+i pi k/M} (X[k] - conj(X[M-k])); the

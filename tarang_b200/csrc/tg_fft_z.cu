@@ -2,7 +2,10 @@
 #include <cstdint>
 #include <cstdlib>
 
+#include <cmath>
+
 #include "tg_fft_launch.h"
+#include "tg_fft_zoct.cuh"
 
 namespace tg {
 
@@ -158,8 +161,76 @@ cudaError_t run_zprod_net128(const ZProdLaunch& l, cudaStream_t s) {
   return run_zprod_net128_pf<Ri, Ro, Rw, NIN, NPROD, 0>(l, 0, s);
 }
 
+// M = 128: the eight-lane network (k_z_prod_oct) unless TG_ZPASS_OCT=0
+bool zpass_oct_enabled() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = std::getenv("TG_ZPASS_OCT");
+    v = (e && e[0] == '0') ? 0 : 1;
+  }
+  return v == 1;
+}
+
+// the physics layout k_z_prod_oct hard-codes (OctLayout), if the launch's product pairs are it
+template <int NIN, int NPROD>
+int oct_phys(const ProdPairs& pp) {
+  static const signed char F_A[6] = {0, 1, 2, 0, 1, 2}, F_B[6] = {0, 1, 2, 1, 2, 0};
+  static const signed char M_A[9] = {0, 1, 2, 0, 3, 1, 4, 2, 5}, M_B[9] = {3, 4, 5, 4, 1, 5, 2, 3, 0};
+  static const signed char S_A[9] = {0, 1, 2, 0, 1, 2, 0, 1, 2}, S_B[9] = {0, 1, 2, 1, 2, 0, 3, 3, 3};
+  const signed char *A, *B;
+  int ph;
+  if (NIN == 3 && NPROD == 6) {
+    A = F_A, B = F_B, ph = 0;
+  } else if (NIN == 6 && NPROD == 9) {
+    A = M_A, B = M_B, ph = 1;
+  } else if (NIN == 4 && NPROD == 9) {
+    A = S_A, B = S_B, ph = 2;
+  } else {
+    return -1;
+  }
+  for (int q = 0; q < NPROD; ++q)
+    if (pp.a[q] != A[q] || pp.b[q] != B[q]) return -1;
+  return ph;
+}
+
+template <typename Ri, typename Ro, typename Rw, int PHYS, bool PRUNE>
+cudaError_t run_zprod_oct(const ZProdLaunch& l, cudaStream_t s) {
+  constexpr int WPB = 4;
+  const size_t smem = sizeof(cx<Rw>) * ((size_t)kOctEntries * 8 + (size_t)WPB * OctLayout<PHYS>::npark * 16 * 32);
+  auto kern = k_z_prod_oct<Ri, Ro, Rw, PHYS, PRUNE>;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  const long long nquad = (l.a.nrows + 3) / 4;
+  long long blocks = (nquad + WPB - 1) / WPB;
+  const long long resident = 148LL * OctOcc<Rw, PHYS>::v;
+  if (blocks > resident) blocks = resident;
+  kern<<<(unsigned)blocks, 32 * WPB, smem, s>>>(l.a, l.ps);
+  return cudaGetLastError();
+}
+
+template <typename Ri, typename Ro, typename Rw, int NIN, int NPROD>
+cudaError_t run_zprod_oct_any(const ZProdLaunch& l, int ph, cudaStream_t s) {
+  const bool prune = l.a.nin <= 96 && l.a.nout <= 96;
+  if (ph == 0) return prune ? run_zprod_oct<Ri, Ro, Rw, 0, true>(l, s) : run_zprod_oct<Ri, Ro, Rw, 0, false>(l, s);
+  if (ph == 1) return prune ? run_zprod_oct<Ri, Ro, Rw, 1, true>(l, s) : run_zprod_oct<Ri, Ro, Rw, 1, false>(l, s);
+  return prune ? run_zprod_oct<Ri, Ro, Rw, 2, true>(l, s) : run_zprod_oct<Ri, Ro, Rw, 2, false>(l, s);
+}
+
 template <typename Ri, typename Ro, typename Rw, int NIN, int NPROD>
 cudaError_t run_zprod_m(const ZProdLaunch& l, cudaStream_t s) {
+  if (l.M == 128 && l.a.oct && zpass_oct_enabled() && l.a.nin <= 129 && l.a.nout <= 129) {
+    // the paired output stores need even row strides and 2-entry-aligned product buffers
+    bool aligned = (l.a.ds % 2) == 0;
+    for (int q = 0; q < NPROD && aligned; ++q)
+      aligned = (reinterpret_cast<uintptr_t>(l.ps.dst[q]) % (2 * sizeof(cx<Ro>))) == 0;
+    const int ph = aligned ? oct_phys<NIN, NPROD>(l.pp) : -1;
+    if (ph >= 0) return run_zprod_oct_any<Ri, Ro, Rw, NIN, NPROD>(l, ph, s);
+  }
   if (l.M == 128 && zpass_net_enabled()) return run_zprod_net128<Ri, Ro, Rw, NIN, NPROD>(l, s);
   switch (l.M) {
     case 4: return run_zprod_fast<Ri, Ro, Rw, 2, 2, NIN, NPROD>(l, s);
@@ -182,6 +253,48 @@ cudaError_t run_zprod_prec(const ZProdLaunch& l, cudaStream_t s) {
 }
 
 }  // namespace
+
+void zoct_table(cx<double>* out) {
+  // entries [e][p] of k_z_prod_oct (tg_fft_zoct.cuh), M = 128; W_N^e = exp(+2 pi i e / N)
+  const long double two_pi = 6.283185307179586476925286766559005768L;
+  auto put = [&](int e, int p, long double N, long double k) {
+    out[e * 8 + p].x = (double)cosl(two_pi * k / N);
+    out[e * 8 + p].y = (double)sinl(two_pi * k / N);
+  };
+  for (int e = 0; e < kOctEntries * 8; ++e) out[e].x = out[e].y = 0.0;
+  const int M = 128;
+  for (int p = 0; p < 8; ++p) {
+    for (int t = 0; t < 8; ++t)
+      for (int b = 0; b < 2; ++b) put(kOctTw2 + 2 * t + b, p, (long double)M, (2 * p + b) * ((p + t) & 7));
+    // W16^(-sl k0) W8^(p k0) = W16^(2 p k0 - sl k0)
+    for (int sl = 0; sl < 4; ++sl)
+      for (int k0 = 0; k0 < 4; ++k0) put(kOctMid + 4 * sl + k0, p, 16.0L, 2 * p * k0 - sl * k0);
+    put(kOctG, p, 2.0L * M, 2 * p);
+    put(kOctG + 1, p, 2.0L * M, 2 * p + 1);
+    put(kOctW8, p, 8.0L, p);
+    for (int q = 0; q < 8; ++q)
+      for (int b = 0; b < 2; ++b) {
+        const int n = 16 * q + 2 * p + b, slot = 2 * q + b;
+        const long double hr = cosl(two_pi * n / (2.0L * M)), hi = sinl(two_pi * n / (2.0L * M));
+        const long double fr = cosl(two_pi * (p * q) / 8.0L), fi = sinl(two_pi * (p * q) / 8.0L);
+        auto set = [&](int e, long double re, long double im) {
+          out[e * 8 + p].x = (double)re;
+          out[e * 8 + p].y = (double)im;
+        };
+        // alpha = (1 + i h) phi, beta = (1 - i h) phi
+        const long double ar = 1 - hi, ai = hr, br = 1 + hi, bi = -hr;
+        set(kOctAlpha + slot, ar * fr - ai * fi, ar * fi + ai * fr);
+        set(kOctBeta + slot, br * fr - bi * fi, br * fi + bi * fr);
+        // e = conj(h); A = (1 - i e) / 2, B = (1 + i e) / 2; alpha' = A conj(phi), beta' = B phi(M - n)
+        const long double er = hr, ei = -hi;
+        const long double Ar = 0.5L * (1 + ei), Ai = -0.5L * er, Br = 0.5L * (1 - ei), Bi = 0.5L * er;
+        set(kOctAlphaF + slot, Ar * fr + Ai * fi, Ai * fr - Ar * fi);
+        const int k2 = (M - n) % M, q2 = k2 / 16, p2 = (k2 % 16) / 2;
+        const long double gr = cosl(two_pi * (p2 * q2) / 8.0L), gi = sinl(two_pi * (p2 * q2) / 8.0L);
+        set(kOctBetaF + slot, Br * gr - Bi * gi, Br * gi + Bi * gr);
+      }
+  }
+}
 
 cudaError_t launch_z(const ZLaunch& l, cudaStream_t s) {
   if (l.a.nrows <= 0 || l.nfields <= 0) return cudaSuccess;

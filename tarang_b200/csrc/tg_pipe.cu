@@ -135,6 +135,7 @@ int pipe_products_forward(tg_ctx* c, int nin, const void* const* WY, int nprod, 
     l.a.scale = 1.0 / ((double)c->N1 * c->N2 * c->N3);
     l.a.twM = c->tw[c->Mz];
     l.a.twN = c->tw[c->N3];
+    l.a.oct = c->zoct;
     for (int f = 0; f < nin; ++f) l.ps.src[f] = WY[f];
     for (int q = 0; q < nprod; ++q) l.ps.dst[q] = PP[q];
     l.pp = pp;

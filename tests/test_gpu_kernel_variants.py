@@ -1,8 +1,10 @@
 """Kernel variants that compute the same transform agree to rounding: fields after a few steps
-with the TMA-staged axis passes equal those with the register-staged ones (TG_AXIS_TMA=0), and
-those of the transposed lane network of the N3 = 256 z-pass equal those of the five-stage
-shuffle network (TG_ZPASS_NET=0), to 1e-14 (FP64) / 1e-6 (FP32-mixed) relative L2, for every
-precision and physics on the fast path (the two kernels round differently)."""
+with the TMA-staged axis passes equal those with the register-staged ones (TG_AXIS_TMA=0); for
+the N3 = 256 z-pass, those of the eight-lane network (the default) equal those of the 32-lane
+transposed network (TG_ZPASS_OCT=0), and those equal the five-stage shuffle network's
+(TG_ZPASS_OCT=0 TG_ZPASS_NET=0), to 1e-14 (FP64) / 1e-6 (FP32-mixed) relative L2, for every
+precision and physics on the fast path, dealiased rows and full rows (the kernels round
+differently)."""
 
 import json
 import os
@@ -30,11 +32,11 @@ for name, N, kw in cases:
     s.set_V(ic.random_phase_field(N, seed=3))
     if kw.get("physics") == "MHD":
         s.set_W(ic.random_phase_field(N, k0=3.0, seed=4))
-    if kw.get("physics") == "SCALAR":
+    if kw.get("physics") in ("SCALAR", "RB"):
         s.set_T(ic.random_phase_field(N, seed=5)[0])
     s.step(3)
     f = s.get_V() + (s.get_W() if kw.get("physics") == "MHD" else [])
-    f += [s.get_T()] if kw.get("physics") == "SCALAR" else []
+    f += [s.get_T()] if kw.get("physics") in ("SCALAR", "RB") else []
     out[name] = [x.view(np.float64).tobytes().hex() for x in f]
 print(json.dumps(out))
 """ % ROOT
@@ -48,9 +50,10 @@ CASES = [
 ]
 
 
-def run(env_tma, cases=CASES, var="TG_AXIS_TMA"):
+def run(env_tma, cases=CASES, var="TG_AXIS_TMA", extra=None):
     env = dict(os.environ)
     env[var] = env_tma
+    env.update(extra or {})
     r = subprocess.run([sys.executable, "-c", SCRIPT, json.dumps(cases)], capture_output=True, text=True,
                        env=env, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
@@ -83,4 +86,21 @@ ZCASES = [
 
 
 def test_transposed_z_network_matches_shuffle_stages(lib):
-    compare(run("1", ZCASES, "TG_ZPASS_NET"), run("0", ZCASES, "TG_ZPASS_NET"), ZCASES)
+    off = {"TG_ZPASS_OCT": "0"}
+    compare(run("1", ZCASES, "TG_ZPASS_NET", off), run("0", ZCASES, "TG_ZPASS_NET", off), ZCASES)
+
+
+KF_RB = [3.141592653589793, 2.221441469079183, 2.221441469079183]
+OCASES = ZCASES + [
+    ("fluid256z_full", (16, 16, 256), dict(nu=2e-3, dt=1e-3, dealias=False)),
+    ("mhd256z_fp32", (16, 32, 256), dict(physics="MHD", nu=2e-3, eta=3e-3, dt=1e-3, precision="FP32")),
+    ("mhd256z_full", (16, 16, 256), dict(physics="MHD", nu=2e-3, eta=3e-3, dt=1e-3, dealias=False)),
+    ("scalar256z_fp64", (16, 16, 256), dict(physics="SCALAR", nu=2e-3, kappa=3e-3, dt=1e-3)),
+    ("rb256z_fp64", (17, 16, 256), dict(basis="SCFT", physics="RB", Ra=1e4, Pr=1.0, kfactor=KF_RB, dt=1e-4)),
+    ("rb256z_fp32", (17, 16, 256), dict(basis="SCFT", physics="RB", Ra=1e4, Pr=1.0, kfactor=KF_RB, dt=1e-4,
+                                        precision="FP32")),
+]
+
+
+def test_eight_lane_z_network_matches_transposed_network(lib):
+    compare(run("1", OCASES, "TG_ZPASS_OCT"), run("0", OCASES, "TG_ZPASS_OCT"), OCASES)
