@@ -4,8 +4,8 @@
  * The reference has no FFI layer: its "operator API" is the C++ class interface that the
  * solver drivers call (trunk/src/IFluid/Ifluid_main.cc:258-301, IMHD/IMHD_main.cc,
  * RBslip/RB_slip_main.cc:365-400).  Each entry point below replaces one of those calls; the
- * C++ mirror classes in tarang_b200.hpp (CVF, RVF, IncVF, IncFluid, ...) keep the reference
- * method names and call these functions.
+ * header-only C++ mirror classes in tarang_b200.hpp (CVF, CSF, IncVF, IncSF, IncFluid) keep
+ * the reference's method and member names and call these functions.
  *
  * Conventions
  *  - Every function returns an int status: TG_OK (0) or a negative TG_ERR_* code.  The last

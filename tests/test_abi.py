@@ -103,3 +103,19 @@ def test_energy_noalloc_rejects_bad_arguments_without_gpu(lib):
     assert lib.tg_energy_noalloc(ok16, 3, n3, kf, 1, ctypes.c_void_p(4096 + 4), None) == _lib.TG_ERR_ARG
     odd = (ctypes.c_int * 3)(16, 16, 15)
     assert lib.tg_energy_noalloc(ok16, 3, odd, kf, 1, ok16, None) == _lib.TG_ERR_ARG
+
+
+def test_cpp_mirror_header_builds_and_links(tmp_path):
+    """include/tarang_b200.hpp compiles with g++ (C++17, warnings as errors) and a driver written
+    against it links with the library (no GPU needed to build)."""
+    from tarang_b200 import _lib
+    _lib.load()
+    lib_dir = os.path.dirname(_lib.LIB_PATH)
+    exe = str(tmp_path / "ifluid_driver")
+    cmd = ["g++", "-std=c++17", "-O0", "-Wall", "-Wextra", "-Werror", "-I" + os.path.join(ROOT, "include"),
+           os.path.join(ROOT, "tests", "cpp", "ifluid_driver.cc"), "-L" + lib_dir, "-ltarang_gpu",
+           "-Wl,-rpath," + lib_dir, "-o", exe]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([exe], capture_output=True, text=True)
+    assert r.returncode == 2 and "usage" in r.stderr
