@@ -248,6 +248,23 @@ def run_form(torch, N, steps, warmup, stream, fields, dist, **kw):
     return s, ms, kern
 
 
+def kernel_roofline(kern):
+    """Per pass kernel of a step: average launch time (live CUDA events), algorithmic bytes per
+    launch and their rate against the measured HBM copy bandwidth, and the share of the step."""
+    peak = peaks()[0]
+    total = sum(k["total_ms"] for k in kern) or 1.0
+    out = []
+    for k in kern:
+        if not k["launches"]:
+            continue
+        ms = k["total_ms"] / k["launches"]
+        gbs = k["bytes_per_launch"] / (ms * 1e-3) / 1e9 if ms > 0 and k["bytes_per_launch"] else 0.0
+        out.append({"name": k["name"], "avg_us": 1e3 * ms, "bytes_per_launch": k["bytes_per_launch"],
+                    "achieved_gbs": gbs, "frac_of_measured_hbm": gbs / peak if peak else None,
+                    "share": k["total_ms"] / total})
+    return out
+
+
 def rel_max(a, b):
     """max |a - b| / max |b| (0 when both vanish)."""
     import numpy as np
@@ -459,8 +476,8 @@ def run_configs(args, torch, stream):
     f = ic.random_phase_field(N, k0=3.0, energy=0.5, seed=20261203) + \
         ic.random_phase_field(N, k0=3.0, energy=0.5, seed=20261204)
     kw = dict(physics="MHD", nu=1e-3, eta=1e-3, dt=5e-4, n_shells=16)
-    s64, ms64, _ = run_form(torch, N, steps, warm, stream, f, False, precision="FP64", **kw)
-    s32, ms32, _ = run_form(torch, N, steps, warm, stream, f, False, precision="FP32", **kw)
+    s64, ms64, k64 = run_form(torch, N, steps, warm, stream, f, False, precision="FP64", **kw)
+    s32, ms32, k32 = run_form(torch, N, steps, warm, stream, f, False, precision="FP32", **kw)
     for s_ in (s64, s32):
         set_fields(s_, f)
         s_.step(es, energies=False)
@@ -474,6 +491,7 @@ def run_configs(args, torch, stream):
         "diagnostics_err_vs_fp64": diag_errors(s32, s64, groups=(0, 1), et_kinds=kinds),
         "energy_transfer_ms": {"fp64": et_timing(s64, kinds, 1), "fp32": et_timing(s32, kinds, 1),
                                "what": "flux + shell-to-shell tables of the 4 kinds"},
+        "kernel_roofline_fp64": kernel_roofline(k64), "kernel_roofline_fp32": kernel_roofline(k32),
     }
     s64.close()
     s32.close()
@@ -484,8 +502,8 @@ def run_configs(args, torch, stream):
         shape = (N[0], N[1], N[2] // 2 + 1)
         f = [np.zeros(shape, dtype=np.complex128) for _ in range(3)] + [ic.rb_perturbation(N, seed=20261205)]
         kw = dict(basis="SCFT", physics="RB", Ra=1e6, Pr=1.0, dt=1e-4, kfactor=KF_RB)
-        s64, ms64, _ = run_form(torch, N, steps, warm, stream, f, False, precision="FP64", **kw)
-        s32, ms32, _ = run_form(torch, N, steps, warm, stream, f, False, precision="FP32", **kw)
+        s64, ms64, k64 = run_form(torch, N, steps, warm, stream, f, False, precision="FP64", **kw)
+        s32, ms32, k32 = run_form(torch, N, steps, warm, stream, f, False, precision="FP32", **kw)
         for s_ in (s64, s32):
             set_fields(s_, f)
             s_.step(es, energies=False)
@@ -499,6 +517,7 @@ def run_configs(args, torch, stream):
             "rel_l2_err_vs_fp64": {"u": rel_l2(s32.get_V(), s64.get_V()), "theta": rel_l2([s32.get_T()], [s64.get_T()])},
             "nusselt": {"fp64": nu64, "fp32": nu32, "rel_err": abs(nu32 - nu64) / abs(nu64)},
             "theta_spectrum_max_shell_rel": rel_max(t32, t64),
+            "kernel_roofline_fp64": kernel_roofline(k64), "kernel_roofline_fp32": kernel_roofline(k32),
         }
         s64.close()
         s32.close()

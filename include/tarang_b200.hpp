@@ -277,8 +277,7 @@ class IncVF : public CVF {
   void Compute_shell_tr(int kind = TG_ET_UU) {
     const int S = ctx_->config().n_shells;
     shelltoshell_self.assign((size_t)(S + 1) * (S + 1), 0.0);
-    check(tg_shell_to_shell(ctx_->get(), kind, shelltoshell_self.data(), (S + 1) * (S + 1)), ctx_->get(),
-          "tg_shell_to_shell");
+    check(tg_shell_to_shell(ctx_->get(), kind, shelltoshell_self.data(), S + 1), ctx_->get(), "tg_shell_to_shell");
   }
   void Compute_force_feed_shell() {
     const int S = ctx_->config().n_shells;

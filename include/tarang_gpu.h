@@ -303,7 +303,8 @@ int tg_et_radii(tg_ctx* ctx, double* radii, int n);
  * scft/scft_ET.cc:53-265: Kmagnitude_SCFT, Multiplicity_factor_SCFT, x derivatives of the sine and
  * cosine product series). */
 int tg_flux(tg_ctx* ctx, int kind, double* flux, int n);
-/* Compute_shell_tr (compute_shell_tr.cc:59-281): (n_shells+1) x (n_shells+1) row-major */
+/* Compute_shell_tr (compute_shell_tr.cc:59-281): n is the table's dimension (>= n_shells + 1);
+ * tr holds n x n doubles, row-major, giver shell by row, receiver shell by column */
 int tg_shell_to_shell(tg_ctx* ctx, int kind, double* tr, int n);
 /* IncVF::Compute_kinetic_helicity_flux (EnergyTrdir/compute_helicity_flux.cc:47-75), FOUR: the
  * helicity flux out of each sphere s = 1 .. n_shells of the energy-transfer radii,

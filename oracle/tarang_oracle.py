@@ -686,20 +686,36 @@ def number_modes_in_shell(N, inner, outer, kfactor, basis="FOUR"):
     return cnt
 
 
-def _band_modes(N, kfactor, outer):
-    """The (kx, ky, kz) loop of the band forcings (FOUR): kx in [-ceil(outer/kf1), +..], ky
-    likewise, kz in [0, ceil(outer/kf3)], with the stored index (lx, ly, lz)."""
+def _band_modes(N, kfactor, outer, basis="FOUR"):
+    """The (kx, ky, kz) loop of the band forcings: kx in [-ceil(outer/kf1), +..] (FOUR) or
+    [0, ceil(outer/kf1)] (SCFT, kx_min = 0, compute_force_ek_hk_supply.cc:91-95), ky in
+    [-ceil(outer/kf2), +..], kz in [0, ceil(outer/kf3)], with the stored index (lx, ly, lz)."""
     N1, N2, N3 = N
     kxm = int(math.ceil(outer / kfactor[0]))
     kym = int(math.ceil(outer / kfactor[1]))
     kzm = int(math.ceil(outer / kfactor[2]))
-    for kx in range(-kxm, kxm + 1):
+    for kx in range(-kxm if basis == "FOUR" else 0, kxm + 1):
         for ky in range(-kym, kym + 1):
             for kz in range(0, kzm + 1):
                 yield kx, ky, kz, (kx if kx >= 0 else kx + N1), (ky if ky >= 0 else ky + N2), kz
 
 
-def _alpha_beta(mode, v, kk, km, e_mode, h):
+def _modal_energy(v, kx, basis):
+    """CV_Modal_energy (Cvf.cc:595-600): sum of Modal_energy_FOUR |A|^2/2 (four_inline.h:370) or
+    Modal_energy_SCFT |A|^2 for kx > 0, |A|^2/2 for kx = 0 (scft_inline.h:347-354)."""
+    w = 0.5 if (basis == "FOUR" or kx == 0) else 1.0
+    return w * float(np.sum(np.abs(v) ** 2))
+
+
+def _fourier_x(v, basis):
+    """The SCFT sine component along x taken to the Fourier basis, (-i V1, V2, V3)
+    (Get_Modal_helicity_SCFT, Compute_Modal_vorticity_SCFT scft_basic.cc:137-186)."""
+    if basis == "FOUR":
+        return v
+    return np.array([-1j * v[0], v[1], v[2]])
+
+
+def _alpha_beta(mode, v, kk, km, e_mode, h, Ek=None):
     """alpha_k, beta_k of one mode with modal energy E_k = |v|^2/2 (CV_Modal_energy Cvf.cc:595-600)
     and helicity H_k = K . (Vr x Vi) (Get_Modal_helicity_FOUR four_basic.cc:136-155), s = H_k/(k E_k):
       mode 1 (supply, compute_force_ek_hk_supply.cc:120-138): temp = e/(2 E_k),
@@ -708,8 +724,10 @@ def _alpha_beta(mode, v, kk, km, e_mode, h):
       mode 2 (constant energy and helicity, compute_force_const_ek_hk.cc:124-147): t1 = sqrt(e/E_k),
         t2 = sqrt((1 + h)/(1 + s)), t3 = sqrt((1 - h)/(1 - s)), alpha = t1 (t2 + t3)/2,
         beta = t1 (t2 - t3)/(2 k); |s^2 - 1| <= MYEPS2: alpha = t1, beta = 0.
-    None when E_k <= MYEPS."""
-    Ek = float(np.sum(np.abs(v) ** 2)) / 2.0
+    None when E_k <= MYEPS.  Ek: the modal energy when it is not |v|^2/2 (SCFT); v is then the
+    vector in the Fourier basis for the helicity."""
+    if Ek is None:
+        Ek = float(np.sum(np.abs(v) ** 2)) / 2.0
     if Ek <= MYEPS:
         return None
     Hk = float(np.dot(kk, np.cross(v.real, v.imag)))
@@ -728,62 +746,71 @@ def _alpha_beta(mode, v, kk, km, e_mode, h):
     return t1, 0.0
 
 
-def force_band(V, N, kfactor, inner, outer, eps, eps_h=0.0, mode=1, gate=False):
+def force_band(V, N, kfactor, inner, outer, eps, eps_h=0.0, mode=1, gate=False, basis="FOUR"):
     """The vector force of force_field_proc 1 (Compute_force_const_energy_helicity_supply
     compute_force_ek_hk_supply.cc:51-157) or 2 (Compute_force_const_energy_helicity
     compute_force_const_ek_hk.cc:53-165), FOUR: on inner < |K| <= outer, F = alpha V + beta omega
     (Force_alpha_beta force_alpha_beta.cc:60-88: the vorticity i K x V only when beta > MYEPS),
     with e = eps / nf per mode (nf = Get_number_modes_in_shell); then Satisfy_reality_array.
     gate: the mode is skipped unless e > MYEPS (the MHD and scalar variants of proc 1 and every
-    variant of proc 2)."""
-    nf = number_modes_in_shell(N, inner, outer, kfactor)
+    variant of proc 2).
+    SCFT (the basis_type == "SCFT" branches): kx >= 0, the SCFT modal energy and multiplicity of
+    the mode count, the helicity and vorticity of (-i V1, V2, V3), and Force_alpha_beta's SCFT
+    form F1 = I (alpha (-I) V1 + beta omega_1), F2, F3 = alpha V + beta omega
+    (force_alpha_beta.cc:90-110); the SCFT reality condition."""
+    nf = number_modes_in_shell(N, inner, outer, kfactor, basis)
     e_mode = eps / nf
     F = [np.zeros_like(V[0]) for _ in range(3)]
     if gate and not e_mode > MYEPS:
         return F
-    for kx, ky, kz, lx, ly, lz in _band_modes(N, kfactor, outer):
+    for kx, ky, kz, lx, ly, lz in _band_modes(N, kfactor, outer, basis):
         km = math.sqrt((kx * kfactor[0]) ** 2 + (ky * kfactor[1]) ** 2 + (kz * kfactor[2]) ** 2)
         if not (inner < km <= outer):
             continue
         v = np.array([V[0][lx, ly, lz], V[1][lx, ly, lz], V[2][lx, ly, lz]])
         kk = np.array([kx * kfactor[0], ky * kfactor[1], kz * kfactor[2]])
-        ab = _alpha_beta(mode, v, kk, km, e_mode, eps_h)
+        vf = _fourier_x(v, basis)
+        ab = _alpha_beta(mode, vf, kk, km, e_mode, eps_h, _modal_energy(v, kx, basis))
         if ab is None:
             continue
         alpha, beta = ab
         vort = np.zeros(3, dtype=np.complex128)
-        if beta > MYEPS:                                 # Compute_Modal_vorticity_FOUR four_basic.cc:166-186
-            vort = 1j * np.array([kk[1] * v[2] - kk[2] * v[1], kk[2] * v[0] - kk[0] * v[2], kk[0] * v[1] - kk[1] * v[0]])
+        if beta > MYEPS:      # Compute_Modal_vorticity_FOUR / _SCFT (four_basic.cc:166-186, scft_basic.cc:167-186)
+            vort = 1j * np.array([kk[1] * vf[2] - kk[2] * vf[1], kk[2] * vf[0] - kk[0] * vf[2],
+                                  kk[0] * vf[1] - kk[1] * vf[0]])
         for c in range(3):
             F[c][lx, ly, lz] = alpha * v[c] + beta * vort[c]
-    return [satisfy_reality(f) for f in F]
+        if basis != "FOUR":
+            F[0][lx, ly, lz] = alpha * v[0] + 1j * beta * vort[0]
+    return [satisfy_reality(f, basis) for f in F]
 
 
-def force_band_scalar(T, N, kfactor, inner, outer, eps_T, mode=1):
+def force_band_scalar(T, N, kfactor, inner, outer, eps_T, mode=1, basis="FOUR"):
     """The scalar force of procs 1 and 2 with a passive scalar (compute_force_ek_hk_supply.cc:
     270-277, compute_force_const_ek_hk.cc:262-269; Force_scalar_alpha force_alpha_beta.cc:183-198):
     F_T = alpha T with alpha = e_T / E_T(k) (proc 1) or sqrt(e_T / E_T(k)) (proc 2),
-    E_T(k) = |T|^2/2, when e_T = eps_T / nf > MYEPS and E_T(k) > MYEPS."""
-    nf = number_modes_in_shell(N, inner, outer, kfactor)
+    E_T(k) = CS_Modal_energy (FOUR |T|^2/2; SCFT |T|^2, at kx = 0 |T|^2/2), when
+    e_T = eps_T / nf > MYEPS and E_T(k) > MYEPS."""
+    nf = number_modes_in_shell(N, inner, outer, kfactor, basis)
     e_mode = eps_T / nf
     F = np.zeros_like(T)
     if not e_mode > MYEPS:
         return F
-    for kx, ky, kz, lx, ly, lz in _band_modes(N, kfactor, outer):
+    for kx, ky, kz, lx, ly, lz in _band_modes(N, kfactor, outer, basis):
         km = math.sqrt((kx * kfactor[0]) ** 2 + (ky * kfactor[1]) ** 2 + (kz * kfactor[2]) ** 2)
         if not (inner < km <= outer):
             continue
-        Et = abs(T[lx, ly, lz]) ** 2 / 2
+        Et = _modal_energy(np.array([T[lx, ly, lz]]), kx, basis)
         if Et > MYEPS:
             alpha = e_mode / Et if mode == 1 else math.sqrt(e_mode / Et)
             F[lx, ly, lz] = alpha * T[lx, ly, lz]
-    return satisfy_reality(F)
+    return satisfy_reality(F, basis)
 
 
-def force_const_energy_supply(V, N, kfactor, inner, outer, eps, eps_h=0.0):
+def force_const_energy_supply(V, N, kfactor, inner, outer, eps, eps_h=0.0, basis="FOUR"):
     """Compute_force_const_energy_helicity_supply  compute_force_ek_hk_supply.cc:51-157 (fluid):
     force_band with mode 1 and no gate on the energy per mode."""
-    return force_band(V, N, kfactor, inner, outer, eps, eps_h, mode=1, gate=False)
+    return force_band(V, N, kfactor, inner, outer, eps, eps_h, mode=1, gate=False, basis=basis)
 
 
 def force_coriolis(V, omega):
@@ -854,7 +881,7 @@ def abc_force(N, k0, amp, A, B, C):
     return F
 
 
-def fluid_force(force, V, N, kfactor):
+def fluid_force(force, V, N, kfactor, basis="FOUR"):
     """The velocity force of a run: None (decay), energy supply dict(inner, outer, eps, eps_h)
     (proc 1), dict(kind="energy_helicity", inner, outer, eps, eps_h) (proc 2),
     dict(kind="static", F=[F1, F2, F3, ...]) (a fixed force field) or
@@ -864,10 +891,10 @@ def fluid_force(force, V, N, kfactor):
     kind = force.get("kind", "energy_supply")
     if kind == "energy_supply":
         return force_const_energy_supply(V, N, kfactor, force["inner"], force["outer"], force["eps"],
-                                         force.get("eps_h", 0.0))
+                                         force.get("eps_h", 0.0), basis)
     if kind == "energy_helicity":
         return force_band(V, N, kfactor, force["inner"], force["outer"], force["eps"], force.get("eps_h", 0.0),
-                          mode=2, gate=True)
+                          mode=2, gate=True, basis=basis)
     if kind == "static":
         return list(force["F"][:3])
     if kind == "coriolis":
@@ -905,7 +932,7 @@ class FluidSolver:
 
     # Compute_force(); Compute_nlin(); Add_force(); Compute_pressure(); Compute_rhs()
     def rhs(self, V):
-        F = fluid_force(self.force, V, self.N, self.kfactor)
+        F = fluid_force(self.force, V, self.N, self.kfactor, self.basis)
         nl = nlin_fluid(V, self.kfactor, self.basis, self.alias)
         if F is not None:
             nl = [nl[i] - F[i] for i in range(3)]
@@ -1149,8 +1176,10 @@ class ScalarSolver(RBSolver):
         if self.force is not None:
             f = self.force
             mode = 1 if f.get("kind", "energy_supply") == "energy_supply" else 2
-            F = force_band(V, self.N, self.kfactor, f["inner"], f["outer"], f["eps"], f.get("eps_h", 0.0), mode, True)
-            FT = force_band_scalar(T, self.N, self.kfactor, f["inner"], f["outer"], f.get("eps_T", 0.0), mode)
+            F = force_band(V, self.N, self.kfactor, f["inner"], f["outer"], f["eps"], f.get("eps_h", 0.0), mode, True,
+                           self.basis)
+            FT = force_band_scalar(T, self.N, self.kfactor, f["inner"], f["outer"], f.get("eps_T", 0.0), mode,
+                                   self.basis)
             nl = [nl[i] - F[i] for i in range(3)]
             tn = tn - FT
         p = pressure(nl, self.kfactor, self.basis, self.alias)

@@ -485,7 +485,9 @@ int count_force_modes(const tg_config& cfg) {
   const int kym = (int)std::ceil(outer / cfg.kfactor[1]);
   const int kzm = (int)std::ceil(outer / cfg.kfactor[2]);
   int cnt = 0;
-  for (int kx = -kxm; kx <= kxm; ++kx)
+  // Get_number_modes_in_shell_FOUR / _SCFT (four_basic.cc:48-105, scft_basic.cc:48-106): SCFT
+  // counts kx >= 0 only
+  for (int kx = cfg.basis == TG_SCFT ? 0 : -kxm; kx <= kxm; ++kx)
     for (int ky = -kym; ky <= kym; ++ky)
       for (int kz = 0; kz <= kzm; ++kz) {
         const double a = kx * cfg.kfactor[0], b = ky * cfg.kfactor[1], d = kz * cfg.kfactor[2];
@@ -819,8 +821,9 @@ int validate_config(const tg_config* cfg) {
   if (cfg->force_kind == TG_FORCE_LIQUID_METAL && (cfg->physics != TG_FLUID || cfg->basis != TG_FOUR))
     return TG_ERR_UNSUPPORTED;
   if (cfg->force_kind == TG_FORCE_ENERGY_SUPPLY || cfg->force_kind == TG_FORCE_ENERGY_HELICITY) {
-    // band forcings: FOUR; fluid, MHD and passive scalar (convection has its own force)
-    if (cfg->basis != TG_FOUR || cfg->physics == TG_RB) return TG_ERR_UNSUPPORTED;
+    // band forcings: fluid, MHD and passive scalar (convection has its own force); FOUR, and
+    // SCFT for the fluid and the passive scalar (MHD runs FOUR only here)
+    if (cfg->physics == TG_RB) return TG_ERR_UNSUPPORTED;
     if (!(cfg->force_para[1] > cfg->force_para[0])) return TG_ERR_ARG;
     for (int i = 0; i < 6; ++i)
       if (!std::isfinite(cfg->force_para[i])) return TG_ERR_ARG;
@@ -1117,6 +1120,7 @@ int tg_field_download(tg_ctx* c, int field, double* host, size_t n) {
     const int ny = 2 * c->fy + 1, nz = c->fz + 1;
     for (int p = 0; p < c->fbox; ++p) {
       const int kz = p % nz, ky = (p / nz) % ny - c->fy, kx = p / (nz * ny) - c->fx;
+      if (c->basis == TG_SCFT && kx < 0) continue;  // SCFT: kx >= 0
       const int lx = kx >= 0 ? kx : kx + c->N1, ly = ky >= 0 ? ky : ky + c->N2;
       if (lx < 0 || lx >= c->N1 || ly < 0 || ly >= c->N2 || kz >= c->M3) continue;
       const size_t o = (((size_t)lx * c->N2 + ly) * c->M3 + kz) * 2;

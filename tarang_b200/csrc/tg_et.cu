@@ -461,6 +461,7 @@ __global__ void k_force_feed(Geo g, const cx<double>* __restrict__ FB, int fx, i
   double acc = 0;
   for (int p = 0; p < box; ++p) {
     const int kz = p % nz, ky = (p / nz) % ny - fy, kx = p / (nz * ny) - fx;
+    if (g.basis == 1 && kx < 0) continue;  // SCFT: kx >= 0
     const int l1 = kx >= 0 ? kx : kx + g.N1, l2 = ky >= 0 ? ky : ky + g.N2;
     if (l1 < 0 || l1 >= g.N1 || l2 < 0 || l2 >= g.N2 || kz >= g.nkz) continue;
     const int r1 = amap_row(g.ax, l1), r2 = amap_row(g.ay, l2);
@@ -477,7 +478,7 @@ __global__ void k_force_feed(Geo g, const cx<double>* __restrict__ FB, int fx, i
       const cx<double> f = FB[(long long)(c0 + cc) * box + p], v = U[cc][idx];
       re += f.x * v.x + f.y * v.y;
     }
-    acc += 2 * mult_four(l1, l2, kz, g.N1, g.N2) * re;
+    acc += 2 * (g.basis == 1 ? mult_scft(l1, l2, kz, g.N2) : mult_four(l1, l2, kz, g.N1, g.N2)) * re;
   }
   out[i] = acc;
 }
@@ -719,7 +720,8 @@ int tg_force_feed_group(tg_ctx* c, int group, double* feed, int n) {
   if (!c || !feed) return TG_ERR_ARG;
   const int S = c->cfg.n_shells;
   if (S < 6 || S > kMaxShells || n < S + 1 || group < 0 || group > 2) return TG_ERR_ARG;
-  if (c->basis != TG_FOUR && c->phys != TG_RB) return set_err(c, TG_ERR_UNSUPPORTED, "force feed: FOUR (or convection)");
+  if (c->basis != TG_FOUR && c->phys != TG_RB && !(c->force_on == 1 && c->phys != TG_MHD))
+    return set_err(c, TG_ERR_UNSUPPORTED, "force feed: FOUR, convection, or an SCFT band forcing");
   if ((group == 1 && c->phys != TG_MHD) || (group == 2 && c->phys != TG_SCALAR && c->phys != TG_RB))
     return set_err(c, TG_ERR_ARG, "force feed: the group is not a field of this physics");
   for (int i = 0; i < n; ++i) feed[i] = 0;

@@ -339,11 +339,13 @@ cudaError_t run_rk_phys(const RKArgs& a, int phys, int src, cudaStream_t s, int 
 // scalar F_T = alpha_T T, alpha_T = e_T/E_T (proc 1) or sqrt(e_T/E_T) (proc 2)
 // (Force_scalar_alpha force_alpha_beta.cc:183-198); then the reality condition of every force
 // component (Satisfy_reality_array universal_misc.cc:51-109).  One block.
+// v: the mode in the Fourier basis (SCFT: (-i V1, V2, V3)); wE: the modal-energy weight, 1/2
+// (Modal_energy_FOUR, and SCFT at kx = 0) or 1 (Modal_energy_SCFT at kx > 0, scft_inline.h:347)
 __device__ __forceinline__ void band_alpha_beta(int mode, const cx<double> (&v)[3], double kkx, double kky, double kkz,
-                                                double km, double e, double h, double& alpha, double& beta,
-                                                bool& on) {
-  const double Ek = 0.5 * (v[0].x * v[0].x + v[0].y * v[0].y + v[1].x * v[1].x + v[1].y * v[1].y +
-                           v[2].x * v[2].x + v[2].y * v[2].y);
+                                                double km, double e, double h, double wE, double& alpha,
+                                                double& beta, bool& on) {
+  const double Ek = wE * (v[0].x * v[0].x + v[0].y * v[0].y + v[1].x * v[1].x + v[1].y * v[1].y +
+                          v[2].x * v[2].x + v[2].y * v[2].y);
   on = Ek > 1e-15;
   alpha = beta = 0;
   if (!on) return;
@@ -375,21 +377,29 @@ __device__ __forceinline__ void band_alpha_beta(int mode, const cx<double> (&v)[
   }
 }
 
+// scft: the mode is a sin/cos-Fourier one (kx >= 0): the helicity and vorticity take
+// (-i V1, V2, V3) (Get_Modal_helicity_SCFT, Compute_Modal_vorticity_SCFT scft_basic.cc:137-186),
+// the modal energy Modal_energy_SCFT, and Force_alpha_beta's SCFT form gives
+// F1 = I (alpha (-I) V1 + beta omega_1) = alpha V1 + i beta omega_1 (force_alpha_beta.cc:90-110)
 __device__ __forceinline__ void band_vector_force(int mode, const cx<double> (&v)[3], double kkx, double kky,
-                                                  double kkz, double km, double e, double h, cx<double> (&F)[3]) {
+                                                  double kkz, double km, double e, double h, bool scft, int kx,
+                                                  cx<double> (&F)[3]) {
+  const cx<double> vf[3] = {scft ? mkc<double>(v[0].y, -v[0].x) : v[0], v[1], v[2]};
+  const double wE = (scft && kx > 0) ? 1.0 : 0.5;
   double alpha, beta;
   bool on;
-  band_alpha_beta(mode, v, kkx, kky, kkz, km, e, h, alpha, beta, on);
+  band_alpha_beta(mode, vf, kkx, kky, kkz, km, e, h, wE, alpha, beta, on);
   if (!on) return;
   cx<double> w[3] = {mkc<double>(0, 0), mkc<double>(0, 0), mkc<double>(0, 0)};
   if (beta > 1e-15) {
     // vorticity i K x V (Compute_Modal_vorticity_FOUR four_basic.cc:166-186)
-    w[0] = ione(kky * v[2] - kkz * v[1]);
-    w[1] = ione(kkz * v[0] - kkx * v[2]);
-    w[2] = ione(kkx * v[1] - kky * v[0]);
+    w[0] = ione(kky * vf[2] - kkz * vf[1]);
+    w[1] = ione(kkz * vf[0] - kkx * vf[2]);
+    w[2] = ione(kkx * vf[1] - kky * vf[0]);
   }
 #pragma unroll
   for (int c = 0; c < 3; ++c) F[c] = alpha * v[c] + beta * w[c];
+  if (scft) F[0] = alpha * v[0] + ione(beta * w[0]);
 }
 
 template <typename Ru>
@@ -397,6 +407,7 @@ __global__ void __launch_bounds__(TPB) k_force_supply(ForceArgs a) {
   const Geo& g = a.g;
   const int ny = 2 * a.fy + 1, nz = a.fz + 1;
   const int box = (2 * a.fx + 1) * ny * nz;
+  const bool scft = g.basis == 1;  // SCFT: kx >= 0 only (kx_min = 0, compute_force_ek_hk_supply.cc:91-95)
   for (int p = threadIdx.x; p < box; p += TPB) {
     const int kz = p % nz;
     const int ky = (p / nz) % ny - a.fy;
@@ -406,8 +417,8 @@ __global__ void __launch_bounds__(TPB) k_force_supply(ForceArgs a) {
     for (int c = 0; c < 6; ++c) F[c] = mkc<double>(0, 0);
     const double kkx = kx * g.kf0, kky = ky * g.kf1, kkz = kz * g.kf2;
     const double km = sqrt(kkx * kkx + kky * kky + kkz * kkz);
-    if (km > a.inner && km <= a.outer) {
-      const int lx = kx >= 0 ? kx : kx + g.N1;
+    if (km > a.inner && km <= a.outer && !(scft && kx < 0)) {
+      const int lx = (kx >= 0 || scft) ? kx : kx + g.N1;
       const int ly = ky >= 0 ? ky : ky + g.N2;
       const int r1 = (lx >= 0 && lx < g.N1) ? amap_row(g.ax, lx) : -1;
       const int r2 = (ly >= 0 && ly < g.N2) ? amap_row(g.ay, ly) : -1;
@@ -421,7 +432,7 @@ __global__ void __launch_bounds__(TPB) k_force_supply(ForceArgs a) {
       if (!a.gate || a.e_per_mode > 1e-15) {
         const cx<double> u[3] = {v[0], v[1], v[2]};
         cx<double> f[3] = {F[0], F[1], F[2]};
-        band_vector_force(a.mode, u, kkx, kky, kkz, km, a.e_per_mode, a.eps_h, f);
+        band_vector_force(a.mode, u, kkx, kky, kkz, km, a.e_per_mode, a.eps_h, scft, kx, f);
         F[0] = f[0];
         F[1] = f[1];
         F[2] = f[2];
@@ -429,12 +440,13 @@ __global__ void __launch_bounds__(TPB) k_force_supply(ForceArgs a) {
       if (a.ns == 6 && a.e_per_mode_b > 1e-15) {
         const cx<double> b[3] = {v[3], v[4], v[5]};
         cx<double> f[3] = {F[3], F[4], F[5]};
-        band_vector_force(a.mode, b, kkx, kky, kkz, km, a.e_per_mode_b, a.eps_h_b, f);
+        band_vector_force(a.mode, b, kkx, kky, kkz, km, a.e_per_mode_b, a.eps_h_b, scft, kx, f);
         F[3] = f[0];
         F[4] = f[1];
         F[5] = f[2];
       } else if (a.ns == 4 && a.e_per_mode_b > 1e-15) {
-        const double Et = 0.5 * (v[3].x * v[3].x + v[3].y * v[3].y);
+        // CS_Modal_energy: |T|^2/2 (FOUR; SCFT at kx = 0), |T|^2 (SCFT, kx > 0)
+        const double Et = ((scft && kx > 0) ? 1.0 : 0.5) * (v[3].x * v[3].x + v[3].y * v[3].y);
         if (Et > 1e-15) {
           const double al = a.mode == 1 ? a.e_per_mode_b / Et : sqrt(a.e_per_mode_b / Et);
           F[3] = al * v[3];
@@ -445,13 +457,14 @@ __global__ void __launch_bounds__(TPB) k_force_supply(ForceArgs a) {
   }
   __syncthreads();
   // reality condition on the kz = 0 plane: F(kx, ky<0) = conj F(-kx, -ky); F(kx<0, 0) = conj F(-kx, 0)
+  // (FOUR); F(kx, ky<0) = conj F(kx, -ky) (SCFT, Satisfy_reality_array universal_misc.cc:93-104)
   for (int p = threadIdx.x; p < box; p += TPB) {
     const int kz = p % nz;
     const int ky = (p / nz) % ny - a.fy;
     const int kx = p / (nz * ny) - a.fx;
     if (kz != 0) continue;
-    if (!(ky < 0 || (ky == 0 && kx < 0))) continue;
-    const int mx = -kx, my = -ky;
+    if (scft ? !(ky < 0 && kx >= 0) : !(ky < 0 || (ky == 0 && kx < 0))) continue;
+    const int mx = scft ? kx : -kx, my = -ky;
     if (mx < -a.fx || mx > a.fx || my < -a.fy || my > a.fy) continue;
     const int pm = ((mx + a.fx) * ny + (my + a.fy)) * nz;
     for (int c = 0; c < a.ns; ++c) a.FB[(long long)c * box + p] = conjc(a.FB[(long long)c * box + pm]);
@@ -510,6 +523,7 @@ __global__ void k_sub_force_box(Geo g, int ncomp, const cx<double>* FB, int fx, 
   const int kz = p % nz;
   const int ky = (p / nz) % ny - fy;
   const int kx = p / (nz * ny) - fx;
+  if (g.basis == 1 && kx < 0) return;  // SCFT: kx >= 0
   const int lx = kx >= 0 ? kx : kx + g.N1;
   const int ly = ky >= 0 ? ky : ky + g.N2;
   if (lx < 0 || lx >= g.N1 || ly < 0 || ly >= g.N2 || kz >= g.nkz) return;
