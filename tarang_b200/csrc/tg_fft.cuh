@@ -309,6 +309,51 @@ __global__ void __launch_bounds__(256) k_axis_r2r_mm(AxisArgs a, PtrSet ps, R2RA
   }
 }
 
+// The same transforms as a register-tiled matrix product: a thread owns one complex column and
+// RT consecutive output rows (the row tile blockIdx.z % ntile of field blockIdx.z / ntile), with
+// the accumulators in registers; the tile's coefficients T[k][m0 .. m0 + RT) are broadcast from
+// shared memory and the input column streams from global memory, coalesced across the block's
+// columns.  Each input value feeds 2 RT fused multiply-adds (the matrix-product form above does
+// five shared-memory loads per eight), so the FP64 form runs at the FP64 pipe's rate.  RT = 43
+// tiles the row counts of N1 = 129 and 128 (129, 128, 86, 85 rows) with at most one idle row;
+// RT = 22 those of N1 = 65 (65, 43).  Sums run over k in order, as in the forms above.
+template <typename Ri, typename Ro, typename Rw, int RT>
+__global__ void __launch_bounds__(128) k_axis_r2r_gemm(AxisArgs a, PtrSet ps, R2RArgs r, int ntile) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Rw* Ts = reinterpret_cast<Rw*>(smem_raw);  // [nin][RT]
+  const int f = blockIdx.z / ntile, tile = blockIdx.z - f * ntile;
+  const int kind = r.kind[f];
+  const int nrows = r.mat_rows[kind], nin = r.mat_cols[kind];
+  const int m0 = tile * RT;
+  const double* M = r.mat[kind];
+  for (int i = threadIdx.x; i < nin * RT; i += blockDim.x) {
+    const int k = i / RT, m = i - k * RT;
+    Ts[i] = (m0 + m < nrows) ? (Rw)M[(size_t)k * nrows + m0 + m] : (Rw)0;
+  }
+  __syncthreads();
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= a.ncols) return;
+  const cx<Ri>* src = reinterpret_cast<const cx<Ri>*>(ps.src[f]) + (long long)blockIdx.y * a.sb + col;
+  cx<Ro>* dst = reinterpret_cast<cx<Ro>*>(ps.dst[f]) + (long long)blockIdx.y * a.db + col;
+  Rw ax[RT], ay[RT];
+#pragma unroll
+  for (int m = 0; m < RT; ++m) ax[m] = ay[m] = (Rw)0;
+#pragma unroll 2
+  for (int k = 0; k < nin; ++k) {
+    const cx<Rw> x = cvt<Rw>(src[(long long)k * a.sr]);
+    const Rw* t = Ts + k * RT;
+#pragma unroll
+    for (int m = 0; m < RT; ++m) {
+      ax[m] = fma(t[m], x.x, ax[m]);
+      ay[m] = fma(t[m], x.y, ay[m]);
+    }
+  }
+  const Rw sc = (Rw)a.scale;
+#pragma unroll
+  for (int m = 0; m < RT; ++m)
+    if (m0 + m < nrows) dst[(long long)(m0 + m) * a.dr] = cvt<Ro>(mkc<Rw>(sc * ax[m], sc * ay[m]));
+}
+
 // ------------------------------------------------------------------------------------------
 // z-pass (contiguous axis) c2r / r2c.  Rows hold N3/2+1 spectral values of which the first
 // `nin` are stored (the rest are zero); the real row of N3 = 2M values is packed as M complex

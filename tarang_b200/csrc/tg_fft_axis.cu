@@ -285,8 +285,52 @@ cudaError_t run_r2r_mm(const AxisLaunch& l, const R2RArgs& r, cudaStream_t s, bo
   return cudaGetLastError();
 }
 
+// the register-tiled matrix product (k_axis_r2r_gemm) unless TG_R2R_GEMM=0
+bool r2r_gemm_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("TG_R2R_GEMM");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+template <typename Ri, typename Ro, typename Rw, int RT>
+cudaError_t run_r2r_gemm_rt(const AxisLaunch& l, const R2RArgs& r, int nrows, int nin, cudaStream_t s) {
+  const int ntile = (nrows + RT - 1) / RT;
+  const size_t smem = (size_t)nin * RT * sizeof(Rw);
+  auto kern = k_axis_r2r_gemm<Ri, Ro, Rw, RT>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid((l.a.ncols + 127) / 128, l.nbatch, l.nfields * ntile);
+  kern<<<grid, 128, smem, s>>>(l.a, l.ps, r, ntile);
+  return cudaGetLastError();
+}
+
+// when every field's kind has its matrix (all of the same size); the row tile leaving the fewest
+// idle rows
+template <typename Ri, typename Ro, typename Rw>
+cudaError_t run_r2r_gemm(const AxisLaunch& l, const R2RArgs& r, cudaStream_t s, bool* used) {
+  *used = false;
+  if (!r2r_gemm_enabled()) return cudaSuccess;
+  const int nin = amap_count(l.a.in), nout = amap_count(l.a.out);
+  for (int f = 0; f < l.nfields; ++f) {
+    const int k = r.kind[f];
+    if (k < 0 || k > 3 || !r.mat[k] || r.mat_rows[k] != nout || r.mat_cols[k] != nin) return cudaSuccess;
+  }
+  if (nin < 1 || nout < 1 || (size_t)l.nfields * ((nout + 21) / 22) > 65535) return cudaSuccess;
+  const int w43 = (nout + 42) / 43 * 43 - nout, w22 = (nout + 21) / 22 * 22 - nout;
+  *used = true;
+  if (w43 <= w22) return run_r2r_gemm_rt<Ri, Ro, Rw, 43>(l, r, nout, nin, s);
+  return run_r2r_gemm_rt<Ri, Ro, Rw, 22>(l, r, nout, nin, s);
+}
+
 template <typename Ri, typename Ro, typename Rw>
 cudaError_t run_r2r(const AxisLaunch& l, const R2RArgs& r, int N, cudaStream_t s) {
+  {
+    bool used = false;
+    cudaError_t e = run_r2r_gemm<Ri, Ro, Rw>(l, r, s, &used);
+    if (e != cudaSuccess || used) return e;
+  }
   {
     bool used = false;
     cudaError_t e = run_r2r_mm<Ri, Ro, Rw>(l, r, s, &used);

@@ -24,23 +24,28 @@ import math
 import numpy as np
 
 
-def _k_grids(N, kfactor):
+def _k_grids(N, kfactor, basis="FOUR"):
     N1, N2, N3 = N
     l1 = np.arange(N1)
     l2 = np.arange(N2)
-    kx = np.where(l1 <= N1 // 2, l1, l1 - N1).astype(np.float64) * kfactor[0]
+    if basis == "SCFT":
+        kx = l1.astype(np.float64) * kfactor[0]      # Get_kx_SCFT: the sine/cosine index m >= 0
+    else:
+        kx = np.where(l1 <= N1 // 2, l1, l1 - N1).astype(np.float64) * kfactor[0]
     ky = np.where(l2 <= N2 // 2, l2, l2 - N2).astype(np.float64) * kfactor[1]
     kz = np.arange(N3 // 2 + 1).astype(np.float64) * kfactor[2]
     return kx[:, None, None], ky[None, :, None], kz[None, None, :]
 
 
-def keep_mask(N):
-    """Modes kept by the 2/3 rule (universal_misc.cc:118-159, FOUR)."""
+def keep_mask(N, basis="FOUR"):
+    """Modes kept by the 2/3 rule (universal_misc.cc:118-159: FOUR |kx| < N1/3; SCFT m < 2 N1/3)."""
     N1, N2, N3 = N
     keep = np.ones((N1, N2, N3 // 2 + 1), dtype=bool)
     l1 = np.arange(N1)
     kx = np.where(l1 <= N1 // 2, l1, l1 - N1)
-    if N1 >= 3:
+    if N1 >= 3 and basis == "SCFT":
+        keep[2 * N1 // 3:] = False
+    elif N1 >= 3:
         keep[np.abs(kx) >= N1 // 3] = False
     if N2 >= 3:
         keep[:, N2 // 3: 2 * N2 // 3 + 2] = False
@@ -59,11 +64,16 @@ def energy_four(A):
     return float(t)
 
 
-def reality_kz0(A):
-    """Satisfy_reality_array on the kz = 0 plane (universal_misc.cc:51-109, FOUR)."""
+def reality_kz0(A, basis="FOUR"):
+    """Satisfy_reality_array on the kz = 0 plane (universal_misc.cc:51-109): FOUR
+    A(kx, ky<0) = conj A(-kx, -ky), A(kx<0, 0) = conj A(-kx, 0); SCFT A(m, ky<0) = conj A(m, -ky)."""
     A = A.copy()
     N1, N2 = A.shape[0], A.shape[1]
     plane = A[:, :, 0].copy()
+    if basis == "SCFT":
+        for ly in range(N2 // 2 + 1, N2):
+            A[:, ly, 0] = np.conj(plane[:, N2 - ly])
+        return A
     l1 = np.arange(N1)
     kx = np.where(l1 <= N1 // 2, l1, l1 - N1)
     conj_nx = np.where(-kx >= 0, -kx, -kx + N1)
@@ -131,10 +141,12 @@ def random_phase_field(N, kfactor=(1.0, 1.0, 1.0), k0=4.0, energy=0.5, seed=2026
     return [np.ascontiguousarray(v * s) for v in V]
 
 
-def _shell_amp(N, kfactor, shell_energy):
-    """(amp, |K|): amp = sqrt(2 E(ceil|K|) / Approx_number_modes_in_shell) per stored mode."""
+def _shell_amp(N, kfactor, shell_energy, basis="FOUR"):
+    """(amp, |K|): amp = sqrt(2 E(ceil|K|) / Approx_number_modes_in_shell) per stored mode
+    (Approx_number_modes_in_shell: FOUR 2 pi r^2, SCFT pi r^2 over kf1 kf2 kf3, four_inline.h:
+    276-306, scft_inline.h:242-260)."""
     N1, N2, N3 = N
-    Kx, Ky, Kz = _k_grids(N, kfactor)
+    Kx, Ky, Kz = _k_grids(N, kfactor, basis)
     shape = (N1, N2, N3 // 2 + 1)
     Kx = np.broadcast_to(Kx, shape)
     Ky = np.broadcast_to(Ky, shape)
@@ -142,16 +154,17 @@ def _shell_amp(N, kfactor, shell_energy):
     K = np.sqrt(Kx * Kx + Ky * Ky + Kz * Kz)
     idx = np.ceil(K)
     Ek = shell_energy(idx)
-    approx = 2 * math.pi * np.maximum(idx, 1) ** 2 / (kfactor[0] * kfactor[1] * kfactor[2])
+    approx = (2 if basis == "FOUR" else 1) * math.pi * np.maximum(idx, 1) ** 2 / (kfactor[0] * kfactor[1] * kfactor[2])
     return np.sqrt(2 * Ek / approx), K
 
 
-def _put_vector(N, kfactor, amp, ph1, ph2, ph3, dealias):
+def _put_vector(N, kfactor, amp, ph1, ph2, ph3, dealias, basis="FOUR"):
     """Put_vector_amp_phase_comp_conj (ic_amp_phase.cc:54-157, anisotropy axis x) on every mode:
     uperp1 = amp e^{i ph1} cos(ph3), uperp2 = amp e^{i ph2} sin(ph3) turned into (Vx, Vy, Vz) by
-    the polar and azimuthal angles of K; origin zeroed, dealiased, reality condition."""
+    the polar and azimuthal angles of K; origin zeroed, dealiased, reality condition.  SCFT: the
+    SCFT wavenumbers, and V1 -> i V1 (V1 is a sine series along x, ic_amp_phase.cc:151-153)."""
     N1, N2, N3 = N
-    Kx, Ky, Kz = _k_grids(N, kfactor)
+    Kx, Ky, Kz = _k_grids(N, kfactor, basis)
     shape = (N1, N2, N3 // 2 + 1)
     Kx = np.broadcast_to(Kx, shape)
     Ky = np.broadcast_to(Ky, shape)
@@ -174,20 +187,24 @@ def _put_vector(N, kfactor, amp, ph1, ph2, ph3, dealias):
     V = [vpll, vh1, vh2]
     for v in V:
         v[K <= 1e-15] = 0
+    if basis == "SCFT":
+        V[0] = 1j * V[0]
     if dealias:
-        keep = keep_mask(N)
+        keep = keep_mask(N, basis)
         V = [np.where(keep, v, 0) for v in V]
-    return [np.ascontiguousarray(reality_kz0(v)) for v in V]
+    return [np.ascontiguousarray(reality_kz0(v, basis)) for v in V]
 
 
-def _put_scalar(N, kfactor, amp, ph, dealias):
-    """Put_scalar_amp_phase_comp_conj (ic_amp_phase.cc): F = amp e^{i ph}; origin zeroed,
-    dealiased, reality condition."""
-    _, K = _shell_amp(N, kfactor, lambda idx: idx)
+def _put_scalar(N, kfactor, amp, ph, dealias, basis="FOUR"):
+    """Put_scalar_amp_phase_comp_conj (ic_amp_phase.cc:167-190): F = amp e^{i ph} (SCFT: i amp
+    e^{i ph}, a sine series); origin zeroed, dealiased, reality condition."""
+    _, K = _shell_amp(N, kfactor, lambda idx: idx, basis)
     F = np.where(K <= 1e-15, 0, amp * np.exp(1j * ph))
+    if basis == "SCFT":
+        F = 1j * F
     if dealias:
-        F = np.where(keep_mask(N), F, 0)
-    return np.ascontiguousarray(reality_kz0(F))
+        F = np.where(keep_mask(N, basis), F, 0)
+    return np.ascontiguousarray(reality_kz0(F, basis))
 
 
 def _random_phase(N, kfactor, shell_energy, seed, dealias):
@@ -277,55 +294,60 @@ def model_shell_spectrum(n, a):
 
 
 def _model_spectrum(N, kfactor, a):
-    kmax = int(math.ceil(math.sqrt(sum((N[i] // 2 * kfactor[i]) ** 2 for i in range(3))))) + 2
+    # shells up to the largest |K| of the grid (the SCFT x index runs to N1 - 1)
+    kmax = int(math.ceil(math.sqrt((N[0] * kfactor[0]) ** 2 + sum((N[i] // 2 * kfactor[i]) ** 2 for i in (1, 2))))) + 2
     Sk = model_shell_spectrum(kmax + 1, a)
     return lambda idx: Sk[np.minimum(idx.astype(int), kmax)]
 
 
-def energy_spectrum_field(N, a, kfactor=(1.0, 1.0, 1.0), seed=20261202, dealias=True, physics="FLUID", a2=0.0):
-    """Init_cond_energy_spectrum (init_cond_energy.cc:65-138, FOUR): the energy of shell ceil|K|
-    of the model spectrum, divided equally among the shell's modes, with random phases
-    (Put_vector_amp_phase_comp_conj), the mean mode zero, dealiased, reality condition.  MHD
-    (:318-413): W the same with the model spectrum of a2 = init_cond_double_para(2); passive
-    scalar (Init_cond_energy_spectrum_scalar :152-223): T = ampT e^{i phaseT} with the spectrum
-    of a2.  The reference seeds from time(0); numpy's PCG64 with `seed` stands in.  Returns the
-    state fields [V1, V2, V3(, W1, W2, W3 | , T)]."""
-    amp, _ = _shell_amp(N, kfactor, _model_spectrum(N, kfactor, a))
+def energy_spectrum_field(N, a, kfactor=(1.0, 1.0, 1.0), seed=20261202, dealias=True, physics="FLUID", a2=0.0,
+                          basis="FOUR"):
+    """Init_cond_energy_spectrum (init_cond_energy.cc:65-138): the energy of shell ceil|K| of the
+    model spectrum, divided equally among the shell's modes (Approx_number_modes_in_shell of the
+    basis), with random phases (Put_vector_amp_phase_comp_conj), the mean mode zero, dealiased,
+    reality condition.  MHD (:318-413): W the same with the model spectrum of
+    a2 = init_cond_double_para(2); passive scalar and convection (Init_cond_energy_spectrum(T)
+    :152-223): T = ampT e^{i phaseT} with the spectrum of a2.  SCFT: the SCFT wavenumbers, mode
+    count, 2/3 rule and reality condition, and V1, T multiplied by i (sine series along x).
+    The reference seeds from time(0); numpy's PCG64 with `seed` stands in.  Returns the state
+    fields [V1, V2, V3(, W1, W2, W3 | , T)]."""
+    amp, _ = _shell_amp(N, kfactor, _model_spectrum(N, kfactor, a), basis)
     ns = _state_count(physics)
     rng = np.random.Generator(np.random.PCG64(seed))
     ph = rng.random(({3: 3, 6: 6, 4: 4}[ns],) + amp.shape) * 2 * math.pi
-    out = _put_vector(N, kfactor, amp, ph[0], ph[1], ph[2], dealias)
+    out = _put_vector(N, kfactor, amp, ph[0], ph[1], ph[2], dealias, basis)
     if ns == 6:
-        ampW, _ = _shell_amp(N, kfactor, _model_spectrum(N, kfactor, a2))
-        out += _put_vector(N, kfactor, ampW, ph[3], ph[4], ph[5], dealias)
+        ampW, _ = _shell_amp(N, kfactor, _model_spectrum(N, kfactor, a2), basis)
+        out += _put_vector(N, kfactor, ampW, ph[3], ph[4], ph[5], dealias, basis)
     elif ns == 4:
-        ampT, _ = _shell_amp(N, kfactor, _model_spectrum(N, kfactor, a2))
-        out.append(_put_scalar(N, kfactor, ampT, ph[3], dealias))
+        ampT, _ = _shell_amp(N, kfactor, _model_spectrum(N, kfactor, a2), basis)
+        out.append(_put_scalar(N, kfactor, ampT, ph[3], dealias, basis))
     return out
 
 
 def energy_helicity_spectrum_field(N, a, sk, kfactor=(1.0, 1.0, 1.0), seed=20261202, dealias=True, physics="FLUID",
-                                   a2=0.0, skW=0.0, h=0.0):
+                                   a2=0.0, skW=0.0, h=0.0, basis="FOUR"):
     """Init_cond_energy_helicity_spectrum (init_cond_energy.cc:519-590, FOUR): as
     energy_spectrum_field with phase2 = phase1 + pi/2 and phase3 = asin(sk)/2, so every mode
     carries the relative helicity sk.  MHD (:721-824): W from the spectrum of a2 with
     zeta_b = asin(skW)/2, phase1W = phase1 - acos(h / cos(zeta - zeta_b)), phase2W = phase1W + pi/2
-    (h = 2 Hc/(amp ampW)); passive scalar (:604-681): T with the spectrum of a2 and a random phase.
-    Returns the state fields."""
-    amp, _ = _shell_amp(N, kfactor, _model_spectrum(N, kfactor, a))
+    (h = 2 Hc/(amp ampW)); passive scalar and convection (:604-681): T with the spectrum of a2
+    and a random phase.  SCFT as in energy_spectrum_field (the relative helicity sk holds for the
+    Fourier-basis vector (-i V1, V2, V3)).  Returns the state fields."""
+    amp, _ = _shell_amp(N, kfactor, _model_spectrum(N, kfactor, a), basis)
     ns = _state_count(physics)
     rng = np.random.Generator(np.random.PCG64(seed))
     ph1 = rng.random(amp.shape) * 2 * math.pi
     zeta = math.asin(sk) / 2.0
-    out = _put_vector(N, kfactor, amp, ph1, ph1 + math.pi / 2, np.full(amp.shape, zeta), dealias)
+    out = _put_vector(N, kfactor, amp, ph1, ph1 + math.pi / 2, np.full(amp.shape, zeta), dealias, basis)
     if ns == 6:
-        ampW, _ = _shell_amp(N, kfactor, _model_spectrum(N, kfactor, a2))
+        ampW, _ = _shell_amp(N, kfactor, _model_spectrum(N, kfactor, a2), basis)
         zb = math.asin(skW) / 2.0
         p1w = ph1 - math.acos(h / math.cos(zeta - zb))
-        out += _put_vector(N, kfactor, ampW, p1w, p1w + math.pi / 2, np.full(amp.shape, zb), dealias)
+        out += _put_vector(N, kfactor, ampW, p1w, p1w + math.pi / 2, np.full(amp.shape, zb), dealias, basis)
     elif ns == 4:
-        ampT, _ = _shell_amp(N, kfactor, _model_spectrum(N, kfactor, a2))
-        out.append(_put_scalar(N, kfactor, ampT, rng.random(amp.shape) * 2 * math.pi, dealias))
+        ampT, _ = _shell_amp(N, kfactor, _model_spectrum(N, kfactor, a2), basis)
+        out.append(_put_scalar(N, kfactor, ampT, rng.random(amp.shape) * 2 * math.pi, dealias, basis))
     return out
 
 
@@ -399,11 +421,12 @@ def read_init_cond(cfg, data_dir=".", seed=20261202):
         nv = {3: 2, 6: 4, 4: 3}[ns]
         return modes_field(forcing.read_force_modes_file(path, N[0], nv), N, kf, basis, physics,
                            "simple" if proc == 3 else "vorticity")
-    if proc == 5 and basis == "FOUR" and physics.upper() != "RB":
-        return energy_spectrum_field(N, dp[1], kf, seed, physics=physics, a2=dp[2])
-    if proc == 6 and basis == "FOUR" and physics.upper() != "RB":
-        # fluid: a, sk; scalar: a, sk, a_T; MHD: a, sk, a_W, skW, h
-        return energy_helicity_spectrum_field(N, dp[1], dp[2], kf, seed, physics=physics, a2=dp[3], skW=dp[4], h=dp[5])
+    if proc == 5:
+        return energy_spectrum_field(N, dp[1], kf, seed, physics=physics, a2=dp[2], basis=basis)
+    if proc == 6:
+        # fluid: a, sk; scalar and convection: a, sk, a_T; MHD: a, sk, a_W, skW, h
+        return energy_helicity_spectrum_field(N, dp[1], dp[2], kf, seed, physics=physics, a2=dp[3], skW=dp[4], h=dp[5],
+                                              basis=basis)
     if proc == 7 and physics.upper() != "RB":
         # (convection: Init_cond_Taylor_Green_RB recurses into itself in the reference)
         return taylor_green_field(N, int(dp[1]), dp[2], basis, physics, dp[3])

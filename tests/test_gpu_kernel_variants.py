@@ -104,3 +104,19 @@ OCASES = ZCASES + [
 
 def test_eight_lane_z_network_matches_transposed_network(lib):
     compare(run("1", OCASES, "TG_ZPASS_OCT"), run("0", OCASES, "TG_ZPASS_OCT"), OCASES)
+
+
+RCASES = [
+    ("rb129_fp64", (129, 32, 32), dict(basis="SCFT", physics="RB", Ra=1e4, Pr=1.0, kfactor=KF_RB, dt=1e-4)),
+    ("rb129_fp32", (129, 32, 32), dict(basis="SCFT", physics="RB", Ra=1e4, Pr=1.0, kfactor=KF_RB, dt=1e-4,
+                                       precision="FP32")),
+    ("rb65_fp64", (65, 16, 32), dict(basis="SCFT", physics="RB", Ra=1e4, Pr=1.0, kfactor=KF_RB, dt=1e-4)),
+    ("rb33_fp64", (33, 16, 16), dict(basis="SCFT", physics="RB", Ra=1e4, Pr=1.0, kfactor=KF_RB, dt=1e-4)),
+    ("scft_fluid_full", (24, 16, 32), dict(basis="SCFT", nu=2e-3, dt=1e-3, kfactor=KF_RB, dealias=False)),
+]
+
+
+def test_register_tiled_x_pass_matches_matrix_product(lib):
+    """The SCFT x-pass as a register-tiled matrix product (default) equals the shared-memory
+    matrix product (TG_R2R_GEMM=0): same sums in the same order."""
+    compare(run("1", RCASES, "TG_R2R_GEMM"), run("0", RCASES, "TG_R2R_GEMM"), RCASES)

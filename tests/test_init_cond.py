@@ -108,6 +108,54 @@ def test_energy_helicity_spectrum_field():
     assert len(M) == 6 and len(T) == 4 and np.abs(M[4]).max() > 0 and np.abs(T[3]).max() > 0
 
 
+def test_scft_spectrum_initial_conditions():
+    """The SCFT variants of field_input_procs 5 and 6 (Init_cond_energy_spectrum,
+    Init_cond_energy_helicity_spectrum with basis_type SCFT, and their (T) forms for a scalar or
+    convection): divergence-free in the SCFT sense (Xderiv of the sine series V1 plus i ky V2 +
+    i kz V3), zero outside the SCFT 2/3 rule, the SCFT reality condition on kz = 0, the relative
+    helicity sk of every mode in the Fourier basis (-i V1, V2, V3), energy per shell near the
+    model spectrum, and T a sine series (imaginary phase factor i)."""
+    import math
+    KF = (math.pi, math.pi / math.sqrt(2.0), math.pi / math.sqrt(2.0))
+    N = (33, 16, 32)
+    F = ic.energy_helicity_spectrum_field(N, 1.0, 0.5, KF, seed=6, physics="RB", a2=0.4, basis="SCFT")
+    V, T = F[:3], F[3]
+    div = o.xderiv(V[0], KF, "SCFT", 1) + o.yderiv(V[1], KF) + o.zderiv(V[2], KF)
+    scale = max(float(np.abs(v).max()) for v in V) * o.kmag(N, KF, "SCFT").max()
+    assert np.abs(div).max() <= 1e-13 * scale
+    keep = ic.keep_mask(N, "SCFT")
+    for X in V + [T]:
+        assert np.all(X[~keep] == 0) and X[0, 0, 0] == 0
+        for ly in range(N[1] // 2 + 1, N[1]):
+            assert np.array_equal(X[:, ly, 0], np.conj(X[:, N[1] - ly, 0]))
+    Kx, Ky, Kz = o.kvec(N, KF, "SCFT")
+    vf = [-1j * V[0], V[1], V[2]]
+    vr, vi = [v.real for v in vf], [v.imag for v in vf]
+    H = Kx * (vr[1] * vi[2] - vr[2] * vi[1]) + Ky * (vr[2] * vi[0] - vr[0] * vi[2]) + Kz * (vr[0] * vi[1] - vr[1] * vi[0])
+    E = sum(np.abs(v) ** 2 for v in vf) / 2
+    sel = (E > 1e-30) & (np.arange(N[2] // 2 + 1)[None, None, :] > 0)
+    assert sel.sum() > 100
+    with np.errstate(all="ignore"):
+        assert np.abs(H[sel] / (o.kmag(N, KF, "SCFT")[sel] * E[sel]) - 0.5).max() < 1e-12
+    # every mode of shell k has |V|^2 = 2 Sk(k) / Approx_number_modes_in_shell_SCFT(k) (pi r^2):
+    # the oracle's SCFT shell sum adds Multiplicity_factor_SCFT |V|^2
+    S = ic.energy_spectrum_field(N, 1.0, KF, seed=7, physics="FLUID", basis="SCFT")
+    ek = sum(o.shell_spectrum(v, 0, KF, basis="SCFT") for v in S)
+    Sk = ic.model_shell_spectrum(len(ek) + 2, 1.0)
+    shell = np.ceil(o.kmag(N, KF, "SCFT"))
+    mult = o.multiplicity(N, "SCFT")
+    kin = o.max_radius_inside(N, KF, "DEALIAS", "SCFT")
+    for k in range(1, kin):
+        want = 2 * Sk[k] / o.approx_number_modes_in_shell(N, k, KF, "SCFT") * mult[(shell == k) & keep].sum()
+        if want == 0:          # no mode in the shell (|K| >= kf2 = 2.22)
+            assert ek[k] == 0
+            continue
+        assert abs(ek[k] / want - 1.0) < 1e-12, (k, ek[k], want)
+    # the read_init_cond dispatch reaches the SCFT procedures
+    cfg = dict(N=N, basis="SCFT", physics="RB", kfactor=KF, run=dict(field_input_proc=5, init_cond_double=[0.0, 1.0, 0.3]))
+    assert len(ic.read_init_cond(cfg)) == 4
+
+
 def test_rayleigh_taylor_field():
     """field_input_proc 511: the tanh temperature profile in x, sine-transformed as the oracle's
     forward SCFT transform of the real field (uniform in y, z), dealiased; velocity zero."""
