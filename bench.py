@@ -658,6 +658,46 @@ def sequential_solves(batch, steps):
     return statistics.mean(el) if el else float("nan")
 
 
+def serving_shapes(n_batch=64, steps=20):
+    """Per request type (FP32-mixed, nu = 3e-3): the device time of one request-step on a lone
+    context (graph replay, CUDA events on its stream) and in a batch of n_batch requests of that
+    type alone on a server (the batch step's event time / n_batch); the algorithmic bytes of one
+    request-step (sum over the step's kernels of bytes per launch x launches, the convention of
+    the per-kernel roofline) and both rates against the measured HBM copy bandwidth."""
+    import torch
+    from tarang_b200.serving import Server
+    hbm, peak_kind = peaks()
+    out = {}
+    stream = torch.cuda.Stream()
+    for name, base, kind in SERVE_TYPES:
+        cfg = serve_request_config(base, 3e-3)
+        init = serve_ic(kind, base["N"], 7000)
+        c = dict(cfg)
+        N = c.pop("N")
+        with torch.cuda.stream(stream):
+            s, ms, kern = run_form(torch, N, steps, 3, stream, init, False, **c)
+        s.close()
+        lone = ms / steps
+        bstep = sum(k["bytes_per_launch"] * k["launches"] for k in kern) / steps
+        srv = Server(hbm_budget=150e9, max_batch=n_batch, keep_results=False)
+        for _ in range(n_batch):
+            srv.submit(cfg, init, steps)
+        srv.drain()
+        timed = [b for b in srv.batch_stats() if b["step_ms"] > 0]
+        srv.close()
+        b = max(timed, key=lambda b: b["step_ms_n_active"])
+        per = b["step_ms"] / b["step_ms_n_active"]
+        out[name] = {"grid": list(N), "bytes_per_request_step": bstep,
+                     "lone_ms_per_step": lone, "lone_frac_of_hbm": bstep / (lone * 1e-3) / 1e9 / hbm,
+                     "batched_requests": b["step_ms_n_active"], "batched_ms_per_request_step": per,
+                     "batched_frac_of_hbm": bstep / (per * 1e-3) / 1e9 / hbm,
+                     "batched_speedup_vs_lone": lone / per}
+    return {"per_type": out, "peak_gbs": hbm, "peak_kind": peak_kind,
+            "method": f"lone: {steps} graph-replayed steps of one context, CUDA events; batched: {n_batch} "
+                      f"requests of the type alone on a server, {steps} steps, the batch step's CUDA-event time "
+                      f"(average over rounds at that active count) / {n_batch}"}
+
+
 def run_serving(args, rank=0, world=1, dist=False):
     """A seeded Poisson stream of independent solves (sizes and physics drawn uniformly from
     SERVE_TYPES, viscosity log-uniform in [1e-3, 1e-2], FP32-mixed) through tg_server, one
@@ -698,6 +738,7 @@ def run_serving(args, rank=0, world=1, dist=False):
     # and, as the reference runs solves (one program run each), every request on a context of
     # its own: create, upload, steps, download, release
     seq_s, fresh_s = {}, {}
+    shapes = serving_shapes() if rank == 0 else None
     if rank == 0:
         for t in range(len(SERVE_TYPES)):
             idx = [i for i in range(n_req) if reqs[i][0] == t][:3]
@@ -751,6 +792,7 @@ def run_serving(args, rank=0, world=1, dist=False):
         "speedup_vs_sequential_reused_context": agg / (total_steps / seq_total),
         "speedup_vs_sequential_per_gpu": agg / world / (total_steps / fresh_total),
         "rel_l2_err_vs_fp64": errs,
+        "per_type_step": shapes,
         "bytes_peak": max(p["bytes_peak"] for p in parts),
         "graph_launches": sum(p["graph_launches"] for p in parts),
         "eager_steps": sum(p["eager_steps"] for p in parts),

@@ -241,7 +241,7 @@ int tg_energy(tg_ctx* ctx, int group, double* energy, double* dissipation);
 /* CV_Compute_shell_spectrum (Cvf.cc:419-449): ek = [3][n] per component (group T: [1][n]),
  * dissk = [n] (may be NULL).  n must be >= kmax_outside + 1. */
 int tg_shell_spectrum(tg_ctx* ctx, int group, double* ek, double* dissk, int n);
-/* Anisotropic spectra of the velocity (group 0) or magnetic field (group 1, MHD), FOUR basis,
+/* Anisotropic spectra of the velocity (group 0) or magnetic field (group 1, MHD), FOUR or SCFT,
  * about the anisotropy axis `axis` (1 x, 2 y, 3 z: globalvar_anisotropy_switch).
  * tg_ring_spectrum: CVF::CV_Compute_ring_spectrum (fields/Cvf.cc:484-504 with
  * Compute_local_ring_spectrum_FOUR four/four_energy.cc:828-955): spherical shells 0 .. kmax
@@ -255,10 +255,17 @@ int tg_shell_spectrum(tg_ctx* ctx, int group, double* ek, double* dissk, int n);
  * [shells][n + 1] row-major (column 0 stays empty as in the reference); n = capacity of each
  * array in doubles; ek2, dissk may be NULL.  n_sectors, n_slabs <= TG_RING_MAX_SECTORS.
  * For axis 3 the reference's on-axis and cylinder branches test the axis-2 switch twice (an
- * uninitialised value); the z-axis components are used. */
+ * uninitialised value); the z-axis components are used.
+ * SCFT (Compute_local_ring_spectrum_SCFT / _cylinder_ scft/scft_energy.cc:814-940, 1423-1480):
+ * kx >= 0, Multiplicity_factor_SCFT, V = (-i V1, V2, V3), on-axis components (V2, V3),
+ * (V3, -i V1), (-i V1, V2) for axes 1, 2, 3, the SCFT box (kx up to 2 N1/3 dealiased, N1 - 1
+ * aliased; Anis_max_Kpll_SCFT's dealiased y extent is (N2/2) kf as written there).  As written
+ * in the reference, the off-axis modes of the SCFT spherical ring spectrum (ek1, ek2, dissk)
+ * carry no multiplicity factor. */
 #define TG_RING_MAX_SECTORS 64
 int tg_ring_sizes(tg_ctx* ctx, int axis, int* ring_shells, int* cylinder_shells);
-/* Helicity spectra (FOUR): modal helicity 2 mult K . (Vr x Vi) per mode.
+/* Helicity spectra: modal helicity 2 mult K . (Vr x Vi) per mode (shell form FOUR; ring forms
+ * FOUR and SCFT, scft_energy.cc:1334-1370, 1794-1830, with V = (-i V1, V2, V3)).
  * tg_shell_spectrum_helicity: CVF::CV_Compute_shell_spectrum_helicity (Cvf.cc:640-646,
  * Compute_shell_spectrum_helicity_FOUR four/four_energy.cc:551-651): the three terms
  * 2 mult K_i (Vr x Vi)_i in h1, h2, h3 over shells 0 .. Min_radius_outside (n >= that + 1),
@@ -274,7 +281,8 @@ int tg_cylinder_ring_spectrum(tg_ctx* ctx, int group, int axis, int n_slabs, dou
                               int n);
 /* Ring-to-ring energy transfer (IncVF::Compute_ring_tr, EnergyTrdir/compute_ring_tr.cc:60-90 and
  * the MHD kinds :174-215; Fill_array_ring universal_ET.cc:70-100, Local_ring_mult_all_FOUR
- * four/four_ET.cc:330-386), FOUR: tr[i][j][m][s], (n_ring_shells+1) x (n_sectors+1) x
+ * four/four_ET.cc:330-386; SCFT Local_ring_mult_all_SCFT scft/scft_ET.cc:273-346 with the SCFT
+ * products and derivatives of the shell transfers): tr[i][j][m][s], (n_ring_shells+1) x (n_sectors+1) x
  * (n_ring_shells+1) x (n_sectors+1) doubles, is the transfer from giver ring (shell i =
  * 1..n_ring_shells-1, sector j = 1..n_sectors) to receiver ring (m, s).  kind TG_ET_UU
  * (ring_to_ring_self), for MHD TG_ET_BB (W.ring_to_ring_self), TG_ET_UB (ring_to_ring_VF, U to
@@ -287,7 +295,7 @@ int tg_ring_radii(tg_ctx* ctx, int n_ring_shells, double* radii, int n);
 int tg_ring_to_ring(tg_ctx* ctx, int kind, int axis, int n_ring_shells, int n_sectors, double* tr, int n);
 /* Cylinder-ring-to-ring transfer (IncVF::Compute_cylinder_ring_tr, EnergyTrdir/
  * compute_cylin_ring_tr.cc:53-80; Fill_array_cylinder_ring universal_ET.cc:100-125,
- * Local_cyl_ring_mult_all_FOUR four/four_ET.cc:422-530): as tg_ring_to_ring with cylindrical
+ * Local_cyl_ring_mult_all_FOUR four/four_ET.cc:422-530, _SCFT scft_ET.cc:436-478): as tg_ring_to_ring with cylindrical
  * shells of K_perp (scheme 0 radii up to Anis_max_Krho_radius_inside, EnergyTr.cc:300-320;
  * tg_cylinder_radii) and slabs of K_par of equal width up to Anis_max_Kpll in place of sectors.
  * A giver holds the modes with K_par >= 0 (the reference compares the signed K_par); receivers
@@ -350,7 +358,8 @@ int tg_force_feed_group(tg_ctx* ctx, int group, double* feed, int n);
  * of field group 0 (velocity), 1 (B, MHD) or 2 (passive scalar) binned by receiver ring
  * (cylinder = 0: tg_ring_radii shells x n_sectors polar sectors) or cylinder ring (cylinder = 1:
  * tg_cylinder_radii shells x n_sectors K_par slabs) about `axis`; out is
- * [n_ring_shells + 1][n_sectors + 1] row-major (n >= that many).  FOUR; no convection. */
+ * [n_ring_shells + 1][n_sectors + 1] row-major (n >= that many).  FOUR, or an SCFT band forcing
+ * (Ring_mult_all_SCFT scft_ET.cc:273-346); no convection. */
 int tg_force_feed_ring(tg_ctx* ctx, int group, int cylinder, int axis, int n_ring_shells, int n_sectors, double* out,
                        int n);
 
@@ -504,6 +513,19 @@ int tg_server_release(tg_server* srv, long long id);
  * of them into ids, *n = how many were written */
 int tg_server_take_finished(tg_server* srv, long long* ids, int max, int* n);
 int tg_server_stats_get(tg_server* srv, tg_server_stats* st);
+/* One entry per resident batch: its shape and physics, slot capacity, active requests and the
+ * device time of one batch step (CUDA events on the batch's stream around the steps of its last
+ * timed round, averaged over rounds at the same active count) with the active count it was
+ * taken at.  Up to max entries into out; *n = entries written. */
+typedef struct tg_batch_stat {
+  int N[3];
+  int basis, physics, precision;
+  int capacity;          /* request slots of the batch */
+  int n_active;          /* requests running in it now */
+  int step_ms_n_active;  /* active requests during the timed steps (0: none timed yet) */
+  double step_ms;        /* device ms of one step of the whole batch */
+} tg_batch_stat;
+int tg_server_batch_stats(tg_server* srv, tg_batch_stat* out, int max, int* n);
 double tg_server_clock(tg_server* srv);
 
 #ifdef __cplusplus

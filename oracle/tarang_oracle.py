@@ -98,13 +98,13 @@ def max_radius_inside(N, kfactor, alias="DEALIAS", basis="FOUR"):
         if N3 > 2:
             kmag_ = min(kmag_, (N3 // d) * kfactor[2])
         return int(kmag_)
-    # SCFT: x extent is N1 (dealiased 2N1/3), y/z as FOUR
+    # SCFT: x extent is N1 - 1 (dealiased 2N1/3), y/z as FOUR (scft_inline.h:144-220)
     if alias == "DEALIAS":
         kmag_ = min((2 * N1 // 3) * kfactor[0], (N2 // 3) * kfactor[1])
         if N3 > 2:
             kmag_ = min(kmag_, (N3 // 3) * kfactor[2])
     else:
-        kmag_ = min(N1 * kfactor[0], (N2 // 2) * kfactor[1])
+        kmag_ = min((N1 - 1) * kfactor[0], (N2 // 2) * kfactor[1])
         if N3 > 2:
             kmag_ = min(kmag_, (N3 // 2) * kfactor[2])
     return int(kmag_)
@@ -120,7 +120,7 @@ def min_radius_outside(N, kfactor, alias="DEALIAS", basis="FOUR"):
     if alias == "DEALIAS":
         return int(math.ceil(math.sqrt(((2 * N1 // 3) * kfactor[0]) ** 2 + ((N2 // 3) * kfactor[1]) ** 2
                                        + ((N3 // 3) * kfactor[2]) ** 2)))
-    return int(math.ceil(math.sqrt((N1 * kfactor[0]) ** 2 + ((N2 // 2) * kfactor[1]) ** 2
+    return int(math.ceil(math.sqrt(((N1 - 1) * kfactor[0]) ** 2 + ((N2 // 2) * kfactor[1]) ** 2
                                    + ((N3 // 2) * kfactor[2]) ** 2)))
 
 
@@ -589,37 +589,45 @@ def shell_spectrum_helicity(V, kfactor, alias="DEALIAS"):
     return tuple(out)
 
 
-def ring_spectrum(V, kfactor, axis, n_sectors, alias="DEALIAS", cylinder=False, helicity=False):
+def ring_spectrum(V, kfactor, axis, n_sectors, alias="DEALIAS", cylinder=False, helicity=False, basis="FOUR"):
     """CVF::CV_Compute_ring_spectrum (Cvf.cc:484-504; Compute_local_ring_spectrum_FOUR
     four_energy.cc:828-955) or, with cylinder=True, CV_Compute_cylinder_ring_spectrum
-    (Cvf.cc:537-559; Compute_local_cylinder_ring_spectrum_FOUR four_energy.cc:1450-1516), FOUR,
+    (Cvf.cc:537-559; Compute_local_cylinder_ring_spectrum_FOUR four_energy.cc:1450-1516),
     anisotropy axis 1..3.  Returns (ek1, ek2, dissk), each [shells][n + 1]; dissk = 2 (S1 + S2)
-    with weight K^2.  Pure-Python loop over the modes: small grids only."""
+    with weight K^2.  Pure-Python loop over the modes: small grids only.
+
+    basis="SCFT": Compute_local_ring_spectrum_SCFT (scft_energy.cc:814-940), the helicity and
+    cylinder variants (:1334-1370, :1423-1480, :1794-1830): kx = l1 kfactor >= 0,
+    Multiplicity_factor_SCFT, V = (-i V1, V2, V3), on-axis components (V2, V3), (V3, -i V1),
+    (-i V1, V2) for axes 1, 2, 3, the SCFT box radii (scft_inline.h:455-520), and, as written
+    there, no multiplicity factor in the off-axis branch of the spherical (V, V) spectrum."""
     N1, N2 = V[0].shape[0], V[0].shape[1]
     N3 = 2 * (V[0].shape[2] - 1)
     N = (N1, N2, N3)
-    d = 3 if alias == "DEALIAS" else 2
+    scft = basis != "FOUR"
     ax = axis - 1
     p1, p2 = (ax + 1) % 3, (ax + 2) % 3
-    Nn = (N1, N2, N3)
     n = n_sectors
     if not cylinder:
-        rows = max_radius_inside(N, kfactor, alias) + 1
+        rows = max_radius_inside(N, kfactor, alias, basis) + 1
         dth = (math.pi / 2) / n
         bounds = [i * dth for i in range(n)] + [math.pi / 2]
     else:
-        rows = int(min((Nn[p1] // d) * kfactor[p1], (Nn[p2] // d) * kfactor[p2])) + 1
-        kmax = (Nn[ax] // d) * kfactor[ax]
+        rows = krho_inside(N, kfactor, axis, alias, basis) + 1
+        kmax = kpll_max(N, kfactor, axis, alias, basis)
         dk = kmax / n
         bounds = [0.0] + [i * dk for i in range(1, n)] + [kmax]
     out = np.zeros((4, rows, n + 1))
-    mult = multiplicity_four(N)
-    kx_, ky_, kz_ = kx_four(N1), ky_four(N2), kz_four(N3)
+    mult = multiplicity(N, basis)
+    kx_, ky_, kz_ = (kx_scft(N1) if scft else kx_four(N1)), ky_four(N2), kz_four(N3)
     A = [np.asarray(v) for v in V]
+    on_axis = {0: (1, 2), 1: (2, 0 if scft else 1), 2: (0, 1)}[ax]
     for l1 in range(N1):
         for l2 in range(N2):
             for l3 in range(N3 // 2 + 1):
                 vals = [A[c][l1, l2, l3] for c in range(3)]
+                if scft:
+                    vals[0] = -1j * vals[0]
                 vv = sum(abs(x) ** 2 for x in vals)
                 if vv == 0.0:
                     continue
@@ -635,13 +643,15 @@ def ring_spectrum(V, kfactor, axis, n_sectors, alias="DEALIAS", cylinder=False, 
                         continue
                     col = _sector_index(_polar_angle(kperp, kpll), bounds)
                     if kperp < MYEPS:
-                        c1, c2 = {0: (1, 2), 1: (2, 1), 2: (0, 1)}[ax]
+                        c1, c2 = on_axis
                         e1, e2 = abs(vals[c1]) ** 2, abs(vals[c2]) ** 2
                     else:
                         # cross(V, K)_axis / k_perp
                         c = vals[p1] * k[p2] - vals[p2] * k[p1]
                         e1 = abs(c) ** 2 / kperp ** 2
                         e2 = vv - e1
+                        if scft and not helicity:
+                            f = 1.0
                 else:
                     row = math.ceil(kperp)
                     if row >= rows:
@@ -650,11 +660,12 @@ def ring_spectrum(V, kfactor, axis, n_sectors, alias="DEALIAS", cylinder=False, 
                     e1 = abs(vals[ax]) ** 2
                     e2 = vv - e1
                 if helicity:
-                    # Compute_local_(cylinder_)ring_spectrum_helicity_FOUR: 2 mult K . (Vr x Vi)
+                    # Compute_local_(cylinder_)ring_spectrum_helicity_FOUR / _SCFT: 2 mult K . (Vr x Vi)
                     vr = np.array([x.real for x in vals])
                     vi = np.array([x.imag for x in vals])
                     e1 = 2.0 * float(np.dot(k, np.cross(vr, vi)))
                     e2 = 0.0
+                    f = mult[l1, l2, l3]
                 if col >= n + 1:
                     continue
                 out[0, row, col] += f * e1
@@ -1371,11 +1382,27 @@ def kinetic_helicity_flux(V, kfactor, no_shells, alias="DEALIAS"):
     return out
 
 
-def krho_inside(N, kfactor, axis, alias="DEALIAS"):
-    """Anis_max_Krho_radius_inside_FOUR  four_inline.h:517-546."""
+def _axis_extent(N, kfactor, i, alias="DEALIAS", basis="FOUR"):
+    """Largest |k_i| of the (de)aliased box along axis i = 0, 1, 2; SCFT x: 2 N1/3 dealiased,
+    N1 - 1 aliased (scft_inline.h:489-520)."""
     d = 3 if alias == "DEALIAS" else 2
+    if basis != "FOUR" and i == 0:
+        return ((2 * N[0] // 3) if alias == "DEALIAS" else (N[0] - 1)) * kfactor[0]
+    return (N[i] // d) * kfactor[i]
+
+
+def krho_inside(N, kfactor, axis, alias="DEALIAS", basis="FOUR"):
+    """Anis_max_Krho_radius_inside_FOUR  four_inline.h:517-546 (_SCFT scft_inline.h:489-520)."""
     p1, p2 = axis % 3, (axis + 1) % 3
-    return int(min((N[p1] // d) * kfactor[p1], (N[p2] // d) * kfactor[p2]))
+    return int(min(_axis_extent(N, kfactor, p1, alias, basis), _axis_extent(N, kfactor, p2, alias, basis)))
+
+
+def kpll_max(N, kfactor, axis, alias="DEALIAS", basis="FOUR"):
+    """Anis_max_Kpll_FOUR / _SCFT (scft_inline.h:455-485; dealiased SCFT axis 2 is (N2/2) kf as
+    written there)."""
+    if basis != "FOUR" and alias == "DEALIAS" and axis == 2:
+        return (N[1] // 2) * kfactor[1]
+    return _axis_extent(N, kfactor, axis - 1, alias, basis)
 
 
 def vector_potential_four(B, kfactor):
@@ -1475,9 +1502,9 @@ def ring_radii(N, kfactor, n_ring_shells, alias="DEALIAS", basis="FOUR", Rin=Non
     return r
 
 
-def _theta_grid(N, kfactor, axis):
-    """AnisKvect_polar_angle_FOUR on the dense grid: unfolded, in [0, pi)."""
-    K = kvec(N, kfactor)
+def _theta_grid(N, kfactor, axis, basis="FOUR"):
+    """AnisKvect_polar_angle_FOUR (_SCFT) on the dense grid: unfolded, in [0, pi)."""
+    K = kvec(N, kfactor, basis)
     shape = (N[0], N[1], N[2] // 2 + 1)
     K = [np.broadcast_to(k, shape) for k in K]
     ax = axis - 1
@@ -1490,24 +1517,25 @@ def _theta_grid(N, kfactor, axis):
     return np.where(t >= 0, t, t + math.pi)
 
 
-def compute_cylinder_ring_tr_generic(H, F, Rf, sign, kfactor, axis, n_shells, n_slabs, alias="DEALIAS"):
+def compute_cylinder_ring_tr_generic(H, F, Rf, sign, kfactor, axis, n_shells, n_slabs, alias="DEALIAS",
+                                     basis="FOUR"):
     """IncVF::Compute_cylinder_ring_tr  compute_cylin_ring_tr.cc:53-80: giver (i, j) = F on
     r[i-1] < K_perp <= r[i], h_{j-1} < K_par <= h_j (signed; K_par = 0 in slab 1;
     Fill_array_cylinder_ring universal_ET.cc:100-125); T[i, j, m, s] = sign * sum over receiver
     (m, s) with K_perp <= Krho_max of 2 mult Re(N . Rf*) (Local_cyl_ring_mult_all_FOUR
-    four_ET.cc:492-530, Compute_cylinder_ring_index basis_basicfn.cc:412-445)."""
+    four_ET.cc:492-530, Compute_cylinder_ring_index basis_basicfn.cc:412-445; SCFT
+    Local_cyl_ring_mult_all_SCFT scft_ET.cc:436-478)."""
     N = (H[0].shape[0], H[0].shape[1], 2 * (H[0].shape[2] - 1))
-    d = 3 if alias == "DEALIAS" else 2
-    kr = krho_inside(N, kfactor, axis, alias)
-    R = ring_radii(N, kfactor, n_shells, alias, Rin=float(kr))
+    kr = krho_inside(N, kfactor, axis, alias, basis)
+    R = ring_radii(N, kfactor, n_shells, alias, basis, Rin=float(kr))
     ax = axis - 1
-    kmax = (N[ax] // d) * kfactor[ax]
+    kmax = kpll_max(N, kfactor, axis, alias, basis)
     dk = kmax / n_slabs
     hb = [0.0] + [i * dk for i in range(1, n_slabs)] + [kmax]
-    Kv = [np.broadcast_to(k, (N[0], N[1], N[2] // 2 + 1)) for k in kvec(N, kfactor)]
+    Kv = [np.broadcast_to(k, (N[0], N[1], N[2] // 2 + 1)) for k in kvec(N, kfactor, basis)]
     kpll = Kv[ax]
     kperp = np.sqrt(Kv[(ax + 1) % 3] ** 2 + Kv[(ax + 2) % 3] ** 2)
-    mult = multiplicity_four(N)
+    mult = multiplicity(N, basis)
     shell = shell_index(kperp, R)
     akp = np.abs(kpll)
     slab = np.full(kperp.shape, len(hb), dtype=np.int64)
@@ -1523,30 +1551,31 @@ def compute_cylinder_ring_tr_generic(H, F, Rf, sign, kfactor, axis, n_shells, n_
             lo, hi, hl, hh = R[i - 1], R[i], hb[j - 1], hb[j]
             inr = (kperp > lo) & (kperp <= hi) & (((kpll > hl) & (kpll <= hh)) | ((np.abs(kpll) < MYEPS) & (hl < MYEPS)))
             G = [np.where(inr, f, 0) for f in F]
-            nl = et_nlin(H, G, kfactor)
+            nl = et_nlin(H, G, kfactor, basis)
             val = 2 * mult * sum(np.real(a * np.conj(b)) for a, b in zip(nl, Rf))
             T[i, j] = sign * np.bincount(flat, weights=val[ok], minlength=n1 * n2).reshape(n1, n2)
     return T
 
 
-def ring_mult_all(A, B, kfactor, axis, n_ring_shells, n_sectors, alias="DEALIAS", cylinder=False):
+def ring_mult_all(A, B, kfactor, axis, n_ring_shells, n_sectors, alias="DEALIAS", cylinder=False, basis="FOUR"):
     """Ring_mult_all / Local_ring_mult_all_FOUR (four_ET.cc:335-386) and Cyl_ring_mult_all /
     Local_cyl_ring_mult_all_FOUR (:492-530): sum of 2 mult Re(A . B*) binned by receiver ring
     (scheme-0 ring radii, equal sectors of the folded polar angle up to pi/2, |K| <= R_in,
     |K| > MYEPS) or cylinder ring (radii up to Anis_max_Krho_radius_inside, slabs of |K_par|).
     [shell][sector] of shape (n+1, ns+1).  It gives Compute_force_feed_ring and
-    Compute_force_feed_cylinder_ring (compute_force_feed.cc:162-300) with A the force."""
+    Compute_force_feed_cylinder_ring (compute_force_feed.cc:162-300) with A the force.  SCFT:
+    Local_ring_mult_all_SCFT / Local_cyl_ring_mult_all_SCFT (scft_ET.cc:273-478)."""
     N = (A[0].shape[0], A[0].shape[1], 2 * (A[0].shape[2] - 1))
-    mult = multiplicity_four(N)
+    mult = multiplicity(N, basis)
     val = 2 * mult * sum(np.real(a * np.conj(b)) for a, b in zip(A, B))
     n1, n2 = n_ring_shells + 1, n_sectors + 1
     if not cylinder:
-        R = ring_radii(N, kfactor, n_ring_shells, alias)
+        R = ring_radii(N, kfactor, n_ring_shells, alias, basis)
         dth = (math.pi / 2) / n_sectors
         sec = [i * dth for i in range(n_sectors)] + [math.pi / 2]
-        K = kmag(N, kfactor)
-        th = _theta_grid(N, kfactor, axis)
-        kin = max_radius_inside(N, kfactor, alias)
+        K = kmag(N, kfactor, basis)
+        th = _theta_grid(N, kfactor, axis, basis)
+        kin = max_radius_inside(N, kfactor, alias, basis)
         shell = shell_index(K, R)
         thf = np.where(th > math.pi / 2, math.pi - th, th)
         sector = np.full(K.shape, len(sec), dtype=np.int64)
@@ -1555,14 +1584,13 @@ def ring_mult_all(A, B, kfactor, axis, n_ring_shells, n_sectors, alias="DEALIAS"
         sector = np.where(np.abs(thf) < MYEPS, 1, sector)
         ok = (K <= kin) & (K > MYEPS) & (shell <= n_ring_shells) & (sector <= n_sectors)
     else:
-        d = 3 if alias == "DEALIAS" else 2
-        kr = krho_inside(N, kfactor, axis, alias)
-        R = ring_radii(N, kfactor, n_ring_shells, alias, Rin=float(kr))
+        kr = krho_inside(N, kfactor, axis, alias, basis)
+        R = ring_radii(N, kfactor, n_ring_shells, alias, basis, Rin=float(kr))
         ax = axis - 1
-        kmax = (N[ax] // d) * kfactor[ax]
+        kmax = kpll_max(N, kfactor, axis, alias, basis)
         dk = kmax / n_sectors
         hb = [0.0] + [i * dk for i in range(1, n_sectors)] + [kmax]
-        Kv = [np.broadcast_to(k, (N[0], N[1], N[2] // 2 + 1)) for k in kvec(N, kfactor)]
+        Kv = [np.broadcast_to(k, (N[0], N[1], N[2] // 2 + 1)) for k in kvec(N, kfactor, basis)]
         kperp = np.sqrt(Kv[(ax + 1) % 3] ** 2 + Kv[(ax + 2) % 3] ** 2)
         shell = shell_index(kperp, R)
         akp = np.abs(Kv[ax])
@@ -1575,20 +1603,21 @@ def ring_mult_all(A, B, kfactor, axis, n_ring_shells, n_sectors, alias="DEALIAS"
     return np.bincount(flat, weights=val[ok], minlength=n1 * n2).reshape(n1, n2)
 
 
-def compute_ring_tr_generic(H, F, Rf, sign, kfactor, axis, n_ring_shells, n_sectors, alias="DEALIAS"):
+def compute_ring_tr_generic(H, F, Rf, sign, kfactor, axis, n_ring_shells, n_sectors, alias="DEALIAS", basis="FOUR"):
     """IncVF::Compute_ring_tr  compute_ring_tr.cc:60-90 (MHD kinds :174-215) in one form:
     giver ring (i, j): G = F on r[i-1] < |K| <= r[i], sector_{j-1} < theta <= sector_j
     (Fill_array_ring universal_ET.cc:70-100), N = D_j F(H_j G_i); T[i, j, m, s] = sign *
     sum over receiver ring (m, s) of 2 mult Re(N . Rf*) (Local_ring_mult_all_FOUR
-    four_ET.cc:330-386 with Compute_ring_index basis_basicfn.cc:324-352)."""
+    four_ET.cc:330-386 with Compute_ring_index basis_basicfn.cc:324-352; SCFT
+    Local_ring_mult_all_SCFT scft_ET.cc:273-346)."""
     N = (H[0].shape[0], H[0].shape[1], 2 * (H[0].shape[2] - 1))
-    R = ring_radii(N, kfactor, n_ring_shells, alias)
+    R = ring_radii(N, kfactor, n_ring_shells, alias, basis)
     dth = (math.pi / 2) / n_sectors
     sec = [i * dth for i in range(n_sectors)] + [math.pi / 2]
-    K = kmag(N, kfactor)
-    th = _theta_grid(N, kfactor, axis)
-    kin = max_radius_inside(N, kfactor, alias)
-    mult = multiplicity_four(N)
+    K = kmag(N, kfactor, basis)
+    th = _theta_grid(N, kfactor, axis, basis)
+    kin = max_radius_inside(N, kfactor, alias, basis)
+    mult = multiplicity(N, basis)
     sel = (K <= kin) & (K > MYEPS)
     shell = shell_index(K, R)
     thf = np.where(th > math.pi / 2, math.pi - th, th)
@@ -1605,7 +1634,7 @@ def compute_ring_tr_generic(H, F, Rf, sign, kfactor, axis, n_ring_shells, n_sect
             lo, hi, left, right = R[i - 1], R[i], sec[j - 1], sec[j]
             inr = (K > lo) & (K <= hi) & (((th > left) & (th <= right)) | ((np.abs(th) < MYEPS) & (left < MYEPS)))
             G = [np.where(inr, f, 0) for f in F]
-            nl = et_nlin(H, G, kfactor)
+            nl = et_nlin(H, G, kfactor, basis)
             val = 2 * mult * sum(np.real(a * np.conj(b)) for a, b in zip(nl, Rf))
             T[i, j] = sign * np.bincount(flat, weights=val[ok], minlength=n1 * n2).reshape(n1, n2)
     return T

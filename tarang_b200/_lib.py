@@ -130,6 +130,19 @@ class tg_server_stats(C.Structure):
     ]
 
 
+class tg_batch_stat(C.Structure):
+    _fields_ = [
+        ("N", C.c_int * 3),
+        ("basis", C.c_int),
+        ("physics", C.c_int),
+        ("precision", C.c_int),
+        ("capacity", C.c_int),
+        ("n_active", C.c_int),
+        ("step_ms_n_active", C.c_int),
+        ("step_ms", C.c_double),
+    ]
+
+
 class tg_kernel_stat(C.Structure):
     _fields_ = [
         ("name", C.c_char * 48),
@@ -208,6 +221,7 @@ SIGNATURES = {
     "tg_server_release": (C.c_int, [_VP, C.c_longlong]),
     "tg_server_take_finished": (C.c_int, [_VP, C.POINTER(C.c_longlong), C.c_int, C.POINTER(C.c_int)]),
     "tg_server_stats_get": (C.c_int, [_VP, C.POINTER(tg_server_stats)]),
+    "tg_server_batch_stats": (C.c_int, [_VP, C.POINTER(tg_batch_stat), C.c_int, C.POINTER(C.c_int)]),
     "tg_server_clock": (C.c_double, [_VP]),
     "tg_request_bytes": (C.c_int, [C.POINTER(tg_config), C.c_int, C.POINTER(C.c_size_t)]),
 }

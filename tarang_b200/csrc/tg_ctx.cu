@@ -133,7 +133,8 @@ int max_radius_inside(const tg_ctx* c) {
     km = std::min((c->N1 / d) * kf[0], (c->N2 / d) * kf[1]);
     if (c->N3 > 2) km = std::min(km, (c->N3 / d) * kf[2]);
   } else {
-    const int nx = c->cfg.dealias ? (2 * c->N1 / 3) : c->N1;
+    // Max_radius_inside_(de)aliased_SCFT scft_inline.h:160-220: 2 N1/3 dealiased, N1 - 1 aliased
+    const int nx = c->cfg.dealias ? (2 * c->N1 / 3) : c->N1 - 1;
     km = std::min(nx * kf[0], (c->N2 / d) * kf[1]);
     if (c->N3 > 2) km = std::min(km, (c->N3 / d) * kf[2]);
   }
@@ -1473,8 +1474,8 @@ int tg_shell_spectrum(tg_ctx* c, int group, double* ek, double* dissk, int n) {
   // Min_radius_outside / Max_radius_inside (four_inline.h:172-257)
   const int d = c->cfg.dealias ? 3 : 2;
   const double* kf = c->cfg.kfactor;
-  // SCFT: kx extent 2 N1/3 dealiased, N1 aliased (scft_inline.h:180-200)
-  const int nx = (c->basis == TG_FOUR) ? c->N1 / d : (c->cfg.dealias ? 2 * c->N1 / 3 : c->N1);
+  // SCFT: kx extent 2 N1/3 dealiased, N1 - 1 aliased (scft_inline.h:144-200)
+  const int nx = (c->basis == TG_FOUR) ? c->N1 / d : (c->cfg.dealias ? 2 * c->N1 / 3 : c->N1 - 1);
   const double a0 = nx * kf[0], a1 = (c->N2 / d) * kf[1], a2 = (c->N3 / d) * kf[2];
   const int kkmax = (int)std::ceil(std::sqrt(a0 * a0 + a1 * a1 + a2 * a2));
   const int kin = max_radius_inside(c);

@@ -191,6 +191,10 @@ int radius_inside(const tg_ctx* c);
 int ensure_diag(tg_ctx* c, size_t need);
 // energy-transfer buffers (giver fields etG, helper transforms etWY, products etPP/PY/PX)
 int ensure_et_buffers(tg_ctx* c);
+// SCFT x transforms of P(i, j) = F(H_j G_i), q = 3 i + j, with H and G of parities (sin, cos,
+// cos) along x: sin x sin and cos x cos products are cosine series (0), mixed ones sine (1)
+// (ET_Forward_transform_RSprod_G ET_transform.cc:49-113 with the parities of ET_RSprod.cc:49-169)
+constexpr int kEtXKinds[9] = {0, 1, 1, 1, 0, 0, 1, 0, 0};
 // helper, giver and receiver fields of an energy-transfer kind (TG_ET_*) and its sign; Elsasser
 // kinds fill scratch fields first (tg_et.cu)
 int et_kind_fields(tg_ctx* c, int kind, const cx<double>* H[3], const cx<double>* F[3], const cx<double>* R[3],

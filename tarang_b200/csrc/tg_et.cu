@@ -132,11 +132,6 @@ __global__ void k_fill_shell(Geo g, const cx<double>* F0, const cx<double>* F1, 
   G2[idx] = in ? F2[idx] : z;
 }
 
-// SCFT x transforms of P(i, j) = F(H_j G_i), q = 3 i + j, with H and G of parities (sin, cos,
-// cos) along x: sin x sin and cos x cos products are cosine series (0), mixed ones sine (1)
-// (ET_Forward_transform_RSprod_G ET_transform.cc:49-113 with the parities of ET_RSprod.cc:49-169)
-constexpr int kEtXKinds[9] = {0, 1, 1, 1, 0, 0, 1, 0, 0};
-
 struct ContractArgs {
   Geo g;
   const void* PX[9];      // P(i, j) = F(H_j G_i), q = 3 i + j

@@ -1,6 +1,14 @@
-// Anisotropic energy spectra of a context's vector state (FOUR basis): the ring spectrum
-// E(k, theta) over spherical shells x polar sectors about an anisotropy axis, and the
+// Anisotropic energy spectra of a context's vector state (FOUR and SCFT bases): the ring
+// spectrum E(k, theta) over spherical shells x polar sectors about an anisotropy axis, and the
 // cylindrical ring spectrum E(k_perp, k_par) over cylindrical shells x slabs along the axis.
+//
+// SCFT: Compute_local_ring_spectrum_SCFT (lib/scft/scft_energy.cc:814-940), the helicity ring
+// spectrum (:1334-1370), the cylinder ring spectra (:1423-1480, :1794-1830) with
+// Multiplicity_factor_SCFT, kx = l1 kfactor[1] >= 0, the Fourier-basis vector (-i V1, V2, V3) and
+// the SCFT radii AnisKpll/AnisKperp/Anis_max_Kpll/Anis_max_Krho_radius_inside_SCFT
+// (lib/scft/scft_inline.h:361-535).  As written there, the off-axis branch of the spherical ring
+// spectrum adds |V x K|_axis^2/k_perp^2 and its complement WITHOUT the multiplicity factor (the
+// on-axis branch and every other SCFT spectrum apply it); this file does the same.
 //
 // Reference: CVF::CV_Compute_ring_spectrum / CV_Compute_cylinder_ring_spectrum
 // (lib/fields/Cvf.cc:484-560, sector and slab arrays Cvf.cc:84-190) with
@@ -89,10 +97,13 @@ __global__ void __launch_bounds__(TPB) k_ring(RingArgs a, int use_smem) {
     const double kperp = sqrt(k[p1] * k[p1] + k[p2] * k[p2]);
     const double K2 = k[0] * k[0] + k[1] * k[1] + k[2] * k[2];
     const double K = sqrt(K2);
-    const cx<double> v[3] = {a.V[0][idx], a.V[1][idx], a.V[2][idx]};
+    const bool scft = g.basis == 1;
+    cx<double> v[3] = {a.V[0][idx], a.V[1][idx], a.V[2][idx]};
+    if (scft) v[0] = mkc<double>(v[0].y, -v[0].x);  // -i V1: the SCFT x component in the Fourier basis
     const double vv = v[0].x * v[0].x + v[0].y * v[0].y + v[1].x * v[1].x + v[1].y * v[1].y +
                       v[2].x * v[2].x + v[2].y * v[2].y;
-    const double f = mult_four(l1, l2, l3, g.N1, g.N2);
+    const double f = scft ? mult_scft(l1, l2, l3, g.N2) : mult_four(l1, l2, l3, g.N1, g.N2);
+    double fe = f;  // the factor on e1, e2 (see the SCFT off-axis note at the top of the file)
     int row, col;
     double e1, e2;
     if (!a.cyl) {
@@ -100,8 +111,9 @@ __global__ void __launch_bounds__(TPB) k_ring(RingArgs a, int use_smem) {
       if (!(K > kEps) || row >= a.rows) continue;
       col = sector_index(polar_angle(kperp, kpll), a);
       if (kperp < kEps) {
-        // on the axis: the two components across it (axis x: y, z; y: z, y; z: x, y)
-        const int c1 = (ax == 0) ? 1 : (ax == 1 ? 2 : 0), c2 = (ax == 0) ? 2 : 1;
+        // on the axis: two components (axis x: y, z; y: z, then y in FOUR and x in SCFT; z: x, y)
+        const int c1 = (ax == 0) ? 1 : (ax == 1 ? 2 : 0);
+        const int c2 = (ax == 0) ? 2 : (ax == 1 ? (scft ? 0 : 1) : 1);
         e1 = v[c1].x * v[c1].x + v[c1].y * v[c1].y;
         e2 = v[c2].x * v[c2].x + v[c2].y * v[c2].y;
       } else {
@@ -110,6 +122,7 @@ __global__ void __launch_bounds__(TPB) k_ring(RingArgs a, int use_smem) {
         const cx<double> c = k[p2] * v[p1] - k[p1] * v[p2];
         e1 = (c.x * c.x + c.y * c.y) / (kperp * kperp);
         e2 = vv - e1;
+        if (scft) fe = 1.0;
       }
     } else {
       row = (int)ceil(kperp);
@@ -125,13 +138,14 @@ __global__ void __launch_bounds__(TPB) k_ring(RingArgs a, int use_smem) {
                    c2 = v[0].x * v[1].y - v[1].x * v[0].y;
       e1 = 2.0 * (k[0] * c0 + k[1] * c1 + k[2] * c2);
       e2 = 0.0;
+      fe = f;
     }
     if (col < 0 || col >= a.cols) continue;
     const int b = row * a.cols + col;
-    atomicAdd(&acc[b], f * e1);
-    atomicAdd(&acc[nbins + b], f * e2);
-    atomicAdd(&acc[2 * nbins + b], f * K2 * e1);
-    atomicAdd(&acc[3 * nbins + b], f * K2 * e2);
+    atomicAdd(&acc[b], fe * e1);
+    atomicAdd(&acc[nbins + b], fe * e2);
+    atomicAdd(&acc[2 * nbins + b], fe * K2 * e1);
+    atomicAdd(&acc[3 * nbins + b], fe * K2 * e2);
   }
   if (use_smem) {
     __syncthreads();
@@ -167,15 +181,34 @@ __global__ void __launch_bounds__(TPB) k_shell_helicity(Geo g, const cx<double>*
     if (sh[i] != 0) atomicAdd(&out[i], sh[i]);
 }
 
+// largest |k_i| inside the (de)aliased box along axis i = 0, 1, 2: FOUR (N_i/d) kf_i
+// (Anis_max_Krho_radius_inside_FOUR four_inline.h); SCFT x: 2 N1/3 dealiased, N1 - 1 aliased
+// (Anis_max_Krho_radius_inside_SCFT scft_inline.h:489-520)
+double axis_extent(const tg_ctx* c, int i) {
+  const int d = c->cfg.dealias ? 3 : 2;
+  const int Nax[3] = {c->N1, c->N2, c->N3};
+  if (c->basis != TG_FOUR && i == 0) return (c->cfg.dealias ? 2 * c->N1 / 3 : c->N1 - 1) * c->cfg.kfactor[0];
+  return (Nax[i] / d) * c->cfg.kfactor[i];
+}
+
+// Anis_max_Krho_radius_inside: the cylinder radius inside the box across `axis` (1..3)
+int krho_inside(const tg_ctx* c, int axis) {
+  const int p1 = axis % 3, p2 = (axis + 1) % 3;
+  return (int)std::min(axis_extent(c, p1), axis_extent(c, p2));
+}
+
+// Anis_max_Kpll: the largest K_par.  SCFT dealiased, axis y: (N2/2) kf (scft_inline.h:475-481,
+// as written there; the box edge would be N2/3)
+double kpll_max(const tg_ctx* c, int axis) {
+  if (c->basis != TG_FOUR && c->cfg.dealias && axis == 2) return (c->N2 / 2) * c->cfg.kfactor[1];
+  return axis_extent(c, axis - 1);
+}
+
 int run_ring(tg_ctx* c, int group, int axis, int n, int cyl, double* ek1, double* ek2, double* dissk, int cap,
              int hel = 0) {
   if (!c || !ek1) return TG_ERR_ARG;
-  if (c->basis != TG_FOUR) return set_err(c, TG_ERR_UNSUPPORTED, "ring spectra: FOUR basis only");
   if (axis < 1 || axis > 3 || n < 1 || n > TG_RING_MAX_SECTORS) return TG_ERR_ARG;
   if (group != 0 && !(group == 1 && c->phys == TG_MHD)) return TG_ERR_ARG;
-  const int d = c->cfg.dealias ? 3 : 2;
-  const double* kf = c->cfg.kfactor;
-  const int Nax[3] = {c->N1, c->N2, c->N3};
   RingArgs a{};
   a.g = c->g;
   for (int i = 0; i < 3; ++i) a.V[i] = c->U0[3 * group + i];
@@ -192,9 +225,8 @@ int run_ring(tg_ctx* c, int group, int axis, int n, int cyl, double* ek1, double
     a.bound[n] = M_PI / 2;
   } else {
     // shells 0 .. Anis_max_Krho_radius_inside; slabs of equal k_par up to Anis_max_Kpll
-    const int p1 = axis % 3, p2 = (axis + 1) % 3;
-    a.rows = (int)std::min((Nax[p1] / d) * kf[p1], (Nax[p2] / d) * kf[p2]) + 1;
-    const double kmax = (Nax[axis - 1] / d) * kf[axis - 1];
+    a.rows = krho_inside(c, axis) + 1;
+    const double kmax = kpll_max(c, axis);
     const double dk = kmax / n;
     a.bound[0] = 0.0;
     for (int i = 1; i < n; ++i) a.bound[i] = i * dk;
@@ -373,7 +405,8 @@ __global__ void __launch_bounds__(TPB) k_ring_feed(RingFeedArgs a) {
         re += f.x * v.x + f.y * v.y;
       }
     }
-    if (re != 0) atomicAdd(&sh[bin], 2 * mult_four(l1, l2, l3, g.N1, g.N2) * re);
+    if (re != 0)
+      atomicAdd(&sh[bin], 2 * (g.basis == 1 ? mult_scft(l1, l2, l3, g.N2) : mult_four(l1, l2, l3, g.N1, g.N2)) * re);
   }
   __syncthreads();
   for (int i = threadIdx.x; i < nbins; i += TPB)
@@ -403,25 +436,24 @@ __global__ void __launch_bounds__(TPB) k_ring_contract(RingContractArgs a) {
       const cx<double> p0 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 0])[idx]);
       const cx<double> p1 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 1])[idx]);
       const cx<double> p2 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 2])[idx]);
-      // N_i = i (k . P(i, .)); Re(N_i conj(R_i))
-      const cx<double> s = mkc<double>(k[0] * p0.x + k[1] * p1.x + k[2] * p2.x, k[0] * p0.y + k[1] * p1.y + k[2] * p2.y);
-      const cx<double> Ni = ione(s);
+      // N_i = D_j P(i, j): FOUR i (k . P(i, .)); SCFT the x derivative of the cosine series P(0, 0)
+      // is -kx P and of the sine series P(1, 0), P(2, 0) +kx P (Xderiv_SCFT scft_tr.cc:649-707)
+      cx<double> Ni;
+      if (g.basis == 0) {
+        Ni = ione(mkc<double>(k[0] * p0.x + k[1] * p1.x + k[2] * p2.x, k[0] * p0.y + k[1] * p1.y + k[2] * p2.y));
+      } else {
+        const double dx = (i == 0) ? -k[0] : k[0];
+        Ni = mkc<double>(dx * p0.x - (k[1] * p1.y + k[2] * p2.y), dx * p0.y + (k[1] * p1.x + k[2] * p2.x));
+      }
       const cx<double> r = a.R[i][idx];
       v += Ni.x * r.x + Ni.y * r.y;
     }
-    atomicAdd(&sh[shell * cols + sector], 2.0 * mult_four(l1, l2, l3, g.N1, g.N2) * v);
+    const double m = g.basis == 1 ? mult_scft(l1, l2, l3, g.N2) : mult_four(l1, l2, l3, g.N1, g.N2);
+    atomicAdd(&sh[shell * cols + sector], 2.0 * m * v);
   }
   __syncthreads();
   for (int i = threadIdx.x; i < nbins; i += TPB)
     if (sh[i] != 0) atomicAdd(&a.out[i], sh[i]);
-}
-
-int krho_inside(const tg_ctx* c, int axis) {
-  const int d = c->cfg.dealias ? 3 : 2;
-  const double* kf = c->cfg.kfactor;
-  const int Nax[3] = {c->N1, c->N2, c->N3};
-  const int p1 = axis % 3, p2 = (axis + 1) % 3;
-  return (int)std::min((Nax[p1] / d) * kf[p1], (Nax[p2] / d) * kf[p2]);
 }
 
 // EnergyTr.cc:190-210 (rings, Rin = Max_radius_inside) and :300-320 (cylinders, Rin =
@@ -472,9 +504,7 @@ void ring_bins_for(tg_ctx* c, int axis, int n_ring_shells, int n_sectors, int cy
   } else {
     const int kr = krho_inside(c, axis);
     ring_radii_from((double)kr, n_ring_shells, b.r);
-    const int d = c->cfg.dealias ? 3 : 2;
-    const int Nax[3] = {c->N1, c->N2, c->N3};
-    const double kmax = (Nax[axis - 1] / d) * c->cfg.kfactor[axis - 1];
+    const double kmax = kpll_max(c, axis);
     const double dk = kmax / n_sectors;
     b.bound[0] = 0.0;
     for (int i = 1; i < n_sectors; ++i) b.bound[i] = i * dk;
@@ -485,7 +515,6 @@ void ring_bins_for(tg_ctx* c, int axis, int n_ring_shells, int n_sectors, int cy
 
 int run_ring_tr(tg_ctx* c, int kind, int axis, int n_ring_shells, int n_sectors, int cyl, double* tr, int n) {
   if (!c || !tr) return TG_ERR_ARG;
-  if (c->basis != TG_FOUR) return set_err(c, TG_ERR_UNSUPPORTED, "ring transfers: FOUR basis only");
   if (axis < 1 || axis > 3 || n_sectors < 1 || n_sectors > TG_RING_MAX_SECTORS) return TG_ERR_ARG;
   if (n_ring_shells < 5 || n_ring_shells > kMaxRingShells) return TG_ERR_ARG;
   // U->U ring_to_ring_self, B->B W.ring_to_ring_self, U->B ring_to_ring_VF, Z+->Z+ and Z-->Z-
@@ -538,7 +567,7 @@ int run_ring_tr(tg_ctx* c, int kind, int axis, int n_ring_shells, int n_sectors,
       const void* G[3] = {c->etG[0], c->etG[1], c->etG[2]};
       rc = pipe_inverse_xy(c, 3, G, nullptr, nullptr, F64, 3, c->WX, c->etWY + 3);
       if (rc) return rc;
-      rc = pipe_products_forward(c, 6, c->etWY, 9, pp, c->etPP, c->etPY, c->etPX);
+      rc = pipe_products_forward(c, 6, c->etWY, 9, pp, c->etPP, c->etPY, c->etPX, kEtXKinds);
       if (rc) return rc;
       RingContractArgs a{};
       a.g = g;
@@ -566,12 +595,8 @@ extern "C" {
 
 int tg_ring_sizes(tg_ctx* c, int axis, int* ring_shells, int* cylinder_shells) {
   if (!c || axis < 1 || axis > 3) return TG_ERR_ARG;
-  const int d = c->cfg.dealias ? 3 : 2;
-  const double* kf = c->cfg.kfactor;
-  const int Nax[3] = {c->N1, c->N2, c->N3};
-  const int p1 = axis % 3, p2 = (axis + 1) % 3;
   if (ring_shells) *ring_shells = radius_inside(c) + 1;
-  if (cylinder_shells) *cylinder_shells = (int)std::min((Nax[p1] / d) * kf[p1], (Nax[p2] / d) * kf[p2]) + 1;
+  if (cylinder_shells) *cylinder_shells = krho_inside(c, axis) + 1;
   return TG_OK;
 }
 
@@ -658,7 +683,8 @@ int tg_shell_spectrum_helicity(tg_ctx* c, int group, double* h1, double* h2, dou
 int tg_force_feed_ring(tg_ctx* c, int group, int cylinder, int axis, int n_ring_shells, int n_sectors, double* out,
                        int n) {
   if (!c || !out) return TG_ERR_ARG;
-  if (c->basis != TG_FOUR || c->phys == TG_RB) return set_err(c, TG_ERR_UNSUPPORTED, "ring force feed: FOUR, no convection");
+  if (c->phys == TG_RB || (c->basis != TG_FOUR && !(c->force_on == 1 && c->phys != TG_MHD)))
+    return set_err(c, TG_ERR_UNSUPPORTED, "ring force feed: FOUR or an SCFT band forcing, no convection");
   if (axis < 1 || axis > 3 || n_sectors < 1 || n_sectors > TG_RING_MAX_SECTORS) return TG_ERR_ARG;
   if (n_ring_shells < 5 || n_ring_shells > kMaxRingShells || group < 0 || group > 2) return TG_ERR_ARG;
   if ((group == 1 && c->phys != TG_MHD) || (group == 2 && c->phys != TG_SCALAR))

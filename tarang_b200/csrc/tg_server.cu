@@ -692,6 +692,27 @@ int tg_server_stats_get(tg_server* s, tg_server_stats* st) {
   return TG_OK;
 }
 
+int tg_server_batch_stats(tg_server* s, tg_batch_stat* out, int max, int* n) {
+  if (!s || !n || max < 0 || (max > 0 && !out)) return TG_ERR_ARG;
+  int k = 0;
+  for (auto& kv : s->batches) {
+    if (k >= max) break;
+    const Batch& b = kv.second;
+    tg_batch_stat& o = out[k++];
+    std::memset(&o, 0, sizeof(o));
+    for (int i = 0; i < 3; ++i) o.N[i] = b.c->cfg.N[i];
+    o.basis = b.c->cfg.basis;
+    o.physics = b.c->cfg.physics;
+    o.precision = b.c->cfg.precision;
+    o.capacity = b.B;
+    o.n_active = (int)b.slot_req.size();
+    o.step_ms_n_active = b.step_ms > 0 ? b.step_ms_nact : 0;
+    o.step_ms = b.step_ms;
+  }
+  *n = k;
+  return TG_OK;
+}
+
 double tg_server_clock(tg_server* s) { return s ? now_s(s) : 0.0; }
 
 }  // extern "C"

@@ -159,5 +159,20 @@ class Server:
             raise L.TarangError(rc, "tg_server_stats_get")
         return {k: getattr(st, k) for k, _ in L.tg_server_stats._fields_}
 
+    def batch_stats(self) -> list:
+        """Per resident batch: shape N, physics, precision, capacity, n_active and step_ms, the
+        device time of one step of the whole batch at step_ms_n_active running requests."""
+        buf = (L.tg_batch_stat * 64)()
+        n = C.c_int()
+        rc = self.lib.tg_server_batch_stats(self.h, buf, 64, C.byref(n))
+        if rc != L.TG_OK:
+            raise L.TarangError(rc, "tg_server_batch_stats")
+        out = []
+        for b in buf[: n.value]:
+            d = {k: getattr(b, k) for k, _ in L.tg_batch_stat._fields_}
+            d["N"] = tuple(b.N)
+            out.append(d)
+        return out
+
     def clock(self) -> float:
         return self.lib.tg_server_clock(self.h)
