@@ -692,9 +692,9 @@ int ctx_create_batch(const tg_config* cfg, int B, tg_ctx** out) {
     rc = make_twiddles(c, L);
     if (rc) return fail(rc);
   }
-  if (N3 == 256) {
+  if (N3 == 256 || N3 == 128) {
     std::vector<cx<double>> t(kZoctTableLen);
-    zoct_table(t.data());
+    zoct_table(N3 / 2, t.data());
     if ((rc = dalloc(c, (void**)&c->zoct, sizeof(cx<double>) * t.size()))) return fail(rc);
     e = cudaMemcpy(c->zoct, t.data(), sizeof(cx<double>) * t.size(), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return fail(cuda_err(c, e, "z-pass table"));
@@ -916,7 +916,7 @@ size_t ctx_bytes_estimate(const tg_config* cfg, int B, bool with_staging) {
       b += sizeof(cx<double>) * (size_t)L;
     }
   if (cfg->basis == TG_SCFT) b += sizeof(cx<double>) * 4 * (size_t)N1 + sizeof(double) * 4 * (size_t)N1 * nkx;
-  if (N3 == 256) b += sizeof(cx<double>) * (size_t)kZoctTableLen;
+  if (N3 == 256 || N3 == 128) b += sizeof(cx<double>) * (size_t)kZoctTableLen;
   const size_t Sd1 = sizeof(cx<double>) * S;
   const size_t WXb = tsz * (size_t)N1 * nky * kzp * B;
   const size_t WYb = tsz * (size_t)N1 * N2 * kzp * B;

@@ -38,7 +38,7 @@ struct tg_ctx {
   std::map<int, tg::cx<double>*> tw;
   // SCFT: (cos, sin)(pi j / 2 N1), j < 4 N1, and the x-pass kind of every pipeline field
   // (0 CFT, 1 SFT forward; 2 ICFT, 3 ISFT inverse)
-  tg::cx<double>* zoct = nullptr;  // N3 = 256: coefficient table of the eight-lane z-pass
+  tg::cx<double>* zoct = nullptr;  // N3 = 256 or 128: coefficient table of the eight-lane z-pass
   tg::cx<double>* trigx = nullptr;
   double* xmat[4] = {};  // SCFT x-pass of the pipeline as matrices, per kind (see ctx creation)
   int xmat_rows[4] = {}, xmat_cols[4] = {};

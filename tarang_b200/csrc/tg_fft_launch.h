@@ -42,10 +42,11 @@ int axis_tma_timeout(bool clear);
 // SCFT x-pass (real-to-real, per-field kind); l.L = N1, l.dir unused
 cudaError_t launch_r2r(const AxisLaunch& l, const R2RArgs& r, cudaStream_t s);
 cudaError_t launch_z(const ZLaunch& l, cudaStream_t s);
-// coefficient table of the eight-lane z-pass for N3 = 256 (k_z_prod_oct): kZoctTableLen complex
-// values, evaluated in long double and rounded
+// coefficient table of the eight-lane z-pass for N3 = 256 (M = 128, k_z_prod_oct) or N3 = 128
+// (M = 64, k_z_prod_oct64): at most kZoctTableLen complex values, evaluated in long double and
+// rounded; M is 128 or 64
 constexpr int kZoctTableLen = 100 * 8;
-void zoct_table(cx<double>* out);
+void zoct_table(int M, cx<double>* out);
 cudaError_t launch_zprod(const ZProdLaunch& l, cudaStream_t s);
 
 inline bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }

@@ -6,6 +6,7 @@
 
 #include "tg_fft_launch.h"
 #include "tg_fft_zoct.cuh"
+#include "tg_fft_zoct64.cuh"
 
 namespace tg {
 
@@ -161,7 +162,7 @@ cudaError_t run_zprod_net128(const ZProdLaunch& l, cudaStream_t s) {
   return run_zprod_net128_pf<Ri, Ro, Rw, NIN, NPROD, 0>(l, 0, s);
 }
 
-// M = 128: the eight-lane network (k_z_prod_oct) unless TG_ZPASS_OCT=0
+// M = 128 and M = 64: the eight-lane networks (k_z_prod_oct, k_z_prod_oct64) unless TG_ZPASS_OCT=0
 bool zpass_oct_enabled() {
   static int v = -1;
   if (v < 0) {
@@ -221,8 +222,40 @@ cudaError_t run_zprod_oct_any(const ZProdLaunch& l, int ph, cudaStream_t s) {
   return prune ? run_zprod_oct<Ri, Ro, Rw, 2, true>(l, s) : run_zprod_oct<Ri, Ro, Rw, 2, false>(l, s);
 }
 
+template <typename Ri, typename Ro, typename Rw, int PHYS, bool PRUNE>
+cudaError_t run_zprod_oct64(const ZProdLaunch& l, cudaStream_t s) {
+  constexpr int WPB = 4;
+  const size_t smem = sizeof(cx<Rw>) * ((size_t)kO64Entries * 8 + (size_t)WPB * OctLayout<PHYS>::npark * 8 * 32);
+  auto kern = k_z_prod_oct64<Ri, Ro, Rw, PHYS, PRUNE>;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  const long long nquad = (l.a.nrows + 3) / 4;
+  long long blocks = (nquad + WPB - 1) / WPB;
+  const long long resident = 148LL * Oct64Occ<Rw, PHYS>::v;
+  if (blocks > resident) blocks = resident;
+  kern<<<(unsigned)blocks, 32 * WPB, smem, s>>>(l.a, l.ps);
+  return cudaGetLastError();
+}
+
+template <typename Ri, typename Ro, typename Rw, int NIN, int NPROD>
+cudaError_t run_zprod_oct64_any(const ZProdLaunch& l, int ph, cudaStream_t s) {
+  const bool prune = l.a.nin <= 48 && l.a.nout <= 48;
+  if (ph == 0) return prune ? run_zprod_oct64<Ri, Ro, Rw, 0, true>(l, s) : run_zprod_oct64<Ri, Ro, Rw, 0, false>(l, s);
+  if (ph == 1) return prune ? run_zprod_oct64<Ri, Ro, Rw, 1, true>(l, s) : run_zprod_oct64<Ri, Ro, Rw, 1, false>(l, s);
+  return prune ? run_zprod_oct64<Ri, Ro, Rw, 2, true>(l, s) : run_zprod_oct64<Ri, Ro, Rw, 2, false>(l, s);
+}
+
 template <typename Ri, typename Ro, typename Rw, int NIN, int NPROD>
 cudaError_t run_zprod_m(const ZProdLaunch& l, cudaStream_t s) {
+  if (l.M == 64 && l.a.oct && zpass_oct_enabled() && l.a.nin <= 65 && l.a.nout <= 65) {
+    const int ph = oct_phys<NIN, NPROD>(l.pp);
+    if (ph >= 0) return run_zprod_oct64_any<Ri, Ro, Rw, NIN, NPROD>(l, ph, s);
+  }
   if (l.M == 128 && l.a.oct && zpass_oct_enabled() && l.a.nin <= 129 && l.a.nout <= 129) {
     // the paired output stores need even row strides and 2-entry-aligned product buffers
     bool aligned = (l.a.ds % 2) == 0;
@@ -254,15 +287,57 @@ cudaError_t run_zprod_prec(const ZProdLaunch& l, cudaStream_t s) {
 
 }  // namespace
 
-void zoct_table(cx<double>* out) {
+// entries [e][p] of k_z_prod_oct64 (tg_fft_zoct64.cuh), M = 64; W_N^e = exp(+2 pi i e / N)
+void zoct64_table(cx<double>* out) {
+  const long double two_pi = 6.283185307179586476925286766559005768L;
+  auto put = [&](int e, int p, long double N, long double k) {
+    out[e * 8 + p].x = (double)cosl(two_pi * k / N);
+    out[e * 8 + p].y = (double)sinl(two_pi * k / N);
+  };
+  auto set = [&](int e, int p, long double re, long double im) {
+    out[e * 8 + p].x = (double)re;
+    out[e * 8 + p].y = (double)im;
+  };
+  const int M = 64;
+  for (int p = 0; p < 8; ++p) {
+    for (int t = 0; t < 8; ++t) put(kO64Tw + t, p, (long double)M, p * ((p + t) & 7));
+    // W8^(-tB k0) W8^(p k0)
+    for (int tB = 0; tB < 2; ++tB)
+      for (int k0 = 0; k0 < 4; ++k0) put(kO64Mid + 4 * tB + k0, p, 8.0L, (p - tB) * k0);
+    put(kO64G, p, 2.0L * M, p);
+    put(kO64W8, p, 8.0L, p);
+    for (int q = 0; q < 8; ++q) {
+      const int n = 8 * q + p;
+      const long double hr = cosl(two_pi * n / (2.0L * M)), hi = sinl(two_pi * n / (2.0L * M));
+      const long double fr = cosl(two_pi * (p * q) / 8.0L), fi = sinl(two_pi * (p * q) / 8.0L);
+      // alpha = (1 + i h) phi, beta = (1 - i h) phi
+      const long double ar = 1 - hi, ai = hr, br = 1 + hi, bi = -hr;
+      set(kO64Alpha + q, p, ar * fr - ai * fi, ar * fi + ai * fr);
+      set(kO64Beta + q, p, br * fr - bi * fi, br * fi + bi * fr);
+      // e = conj(h); A = (1 - i e) / 2, B = (1 + i e) / 2; alpha' = A conj(phi), beta' = B phi(M - n)
+      const long double er = hr, ei = -hi;
+      const long double Ar = 0.5L * (1 + ei), Ai = -0.5L * er, Br = 0.5L * (1 - ei), Bi = 0.5L * er;
+      set(kO64AlphaF + q, p, Ar * fr + Ai * fi, Ai * fr - Ar * fi);
+      const int k2 = (M - n) % M, q2 = k2 / 8, p2 = k2 % 8;
+      const long double gr = cosl(two_pi * (p2 * q2) / 8.0L), gi = sinl(two_pi * (p2 * q2) / 8.0L);
+      set(kO64BetaF + q, p, Br * gr - Bi * gi, Br * gi + Bi * gr);
+    }
+  }
+}
+
+void zoct_table(int M, cx<double>* out) {
+  for (int e = 0; e < kZoctTableLen; ++e) out[e].x = out[e].y = 0.0;
+  if (M == 64) {
+    zoct64_table(out);
+    return;
+  }
   // entries [e][p] of k_z_prod_oct (tg_fft_zoct.cuh), M = 128; W_N^e = exp(+2 pi i e / N)
   const long double two_pi = 6.283185307179586476925286766559005768L;
   auto put = [&](int e, int p, long double N, long double k) {
     out[e * 8 + p].x = (double)cosl(two_pi * k / N);
     out[e * 8 + p].y = (double)sinl(two_pi * k / N);
   };
-  for (int e = 0; e < kOctEntries * 8; ++e) out[e].x = out[e].y = 0.0;
-  const int M = 128;
+  M = 128;
   for (int p = 0; p < 8; ++p) {
     for (int t = 0; t < 8; ++t)
       for (int b = 0; b < 2; ++b) put(kOctTw2 + 2 * t + b, p, (long double)M, (2 * p + b) * ((p + t) & 7));

@@ -2,7 +2,8 @@
 with the TMA-staged axis passes equal those with the register-staged ones (TG_AXIS_TMA=0); for
 the N3 = 256 z-pass, those of the eight-lane network (the default) equal those of the 32-lane
 transposed network (TG_ZPASS_OCT=0), and those equal the five-stage shuffle network's
-(TG_ZPASS_OCT=0 TG_ZPASS_NET=0), to 1e-14 (FP64) / 1e-6 (FP32-mixed) relative L2, for every
+(TG_ZPASS_OCT=0 TG_ZPASS_NET=0); for N3 = 128 the eight-lane network equals the five-stage one
+(TG_ZPASS_OCT=0); all to 1e-14 (FP64) / 1e-6 (FP32-mixed) relative L2, for every
 precision and physics on the fast path, dealiased rows and full rows (the kernels round
 differently)."""
 
@@ -104,6 +105,27 @@ OCASES = ZCASES + [
 
 def test_eight_lane_z_network_matches_transposed_network(lib):
     compare(run("1", OCASES, "TG_ZPASS_OCT"), run("0", OCASES, "TG_ZPASS_OCT"), OCASES)
+
+
+O64CASES = [
+    ("fluid128z_fp64", (32, 32, 128), dict(nu=2e-3, dt=1e-3)),
+    ("fluid128z_fp32", (32, 32, 128), dict(nu=2e-3, dt=1e-3, precision="FP32")),
+    ("fluid128z_full", (16, 16, 128), dict(nu=2e-3, dt=1e-3, dealias=False)),
+    ("fluid128z_full32", (16, 16, 128), dict(nu=2e-3, dt=1e-3, dealias=False, precision="FP32")),
+    ("mhd128z_fp64", (16, 32, 128), dict(physics="MHD", nu=2e-3, eta=3e-3, dt=1e-3)),
+    ("mhd128z_fp32", (16, 32, 128), dict(physics="MHD", nu=2e-3, eta=3e-3, dt=1e-3, precision="FP32")),
+    ("mhd128z_full", (16, 16, 128), dict(physics="MHD", nu=2e-3, eta=3e-3, dt=1e-3, dealias=False)),
+    ("scalar128z_fp64", (16, 16, 128), dict(physics="SCALAR", nu=2e-3, kappa=3e-3, dt=1e-3)),
+    ("scalar128z_fp32", (16, 16, 128), dict(physics="SCALAR", nu=2e-3, kappa=3e-3, dt=1e-3, precision="FP32")),
+    ("rb128z_fp64", (17, 16, 128), dict(basis="SCFT", physics="RB", Ra=1e4, Pr=1.0, kfactor=KF_RB, dt=1e-4)),
+    ("rb128z_fp32", (17, 16, 128), dict(basis="SCFT", physics="RB", Ra=1e4, Pr=1.0, kfactor=KF_RB, dt=1e-4,
+                                        precision="FP32")),
+]
+
+
+def test_eight_lane_z_network_n3_128_matches_warp_network(lib):
+    """N3 = 128 (M = 64): k_z_prod_oct64 against the 32-lane radix-2 network (TG_ZPASS_OCT=0)."""
+    compare(run("1", O64CASES, "TG_ZPASS_OCT"), run("0", O64CASES, "TG_ZPASS_OCT"), O64CASES)
 
 
 RCASES = [
