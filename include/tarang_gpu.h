@@ -446,6 +446,58 @@ int tg_debug_set(tg_ctx* ctx, int what, long long value);
  * ---------------------------------------------------------------------------------------- */
 typedef struct tg_server tg_server;
 
+/* ------------------------------------------------------------------ slab-sharded solve
+ * One solve split over `world` ranks (one process per GPU), the reference's MPI slab
+ * decomposition (basis_basicfn.cc:49-281): rank r's context holds compact kx rows
+ * [xs[r], xs[r] + xn[r]) of the stored modes (a near-equal split of the nkx stored rows), and
+ * between the two exchanges of an RHS evaluation the real y planes [ys[r], ys[r] + yn[r]).  The
+ * caller moves the data between the phases (an NCCL all-to-all, or device copies when several
+ * ranks share a GPU) and sums the reductions; per RK stage s = 1..4 of a step:
+ *   tg_slab_phase(ctx, 0, s)   y-inverse of the stage input, packed: TG_SLAB_INV_SEND field f
+ *                              holds world chunks [xn[r]][yn[d]][kzp], chunk d for rank d
+ *   all-to-all of each input field f: chunk r of every rank's INV_SEND, in rank order, into
+ *                              TG_SLAB_INV_RECV f = [nkx][yn[r]][kzp]
+ *   tg_slab_phase(ctx, 1, s)   x-inverse, fused z-pass, x-forward: TG_SLAB_FWD_SEND product q =
+ *                              [nkx][yn[r]][kzp], chunk d = the rows of rank d, [xn[d]][yn[r]][kzp]
+ *   all-to-all of each product q into TG_SLAB_FWD_RECV q = world chunks [xn[r]][yn[s]][kzp]
+ *   tg_slab_phase(ctx, 2, s)   unpack, y-forward, the RK stage on the rank's modes; after
+ *                              stage 4 the rank's 8 reduction sums are in TG_SLAB_SUMS
+ * then the element-wise sum of every rank's TG_SLAB_SUMS into TG_SLAB_GLOBAL_SUMS and
+ * tg_slab_phase(ctx, 3, 0): Get_dt (compute_dt.cc:47-55) and the time and step count.  Before
+ * the first step (after tg_slab_upload): phase 4 (the state's sums into TG_SLAB_SUMS), the same
+ * sum, and phase 5 (dt only).  Elements are complex values of elem_bytes (16 FP64, 8 FP32-mixed);
+ * every buffer is device memory on the context's stream.  Built for fluid, passive scalar and
+ * convection with forces local in K (none, buoyancy, Coriolis, liquid metal, fixed modes): the
+ * band forcings and MHD return TG_ERR_UNSUPPORTED.  A slab context answers only tg_slab_* calls,
+ * tg_ctx_destroy and tg_last_error. */
+#define TG_SLAB_MAX_RANKS 64
+#define TG_SLAB_INV_SEND 0
+#define TG_SLAB_INV_RECV 1
+#define TG_SLAB_FWD_SEND 2
+#define TG_SLAB_FWD_RECV 3
+#define TG_SLAB_SUMS 4        /* double[8] */
+#define TG_SLAB_GLOBAL_SUMS 5 /* double[8] */
+typedef struct tg_slab_info {
+  int world, rank;
+  int x0, nx, y0, ny;              /* this rank's kx rows and y planes */
+  int xs[TG_SLAB_MAX_RANKS], xn[TG_SLAB_MAX_RANKS];
+  int ys[TG_SLAB_MAX_RANKS], yn[TG_SLAB_MAX_RANKS];
+  int nkx, nky, nkz, kzp;          /* stored modes: the compact layout [nkx][nky][kzp] */
+  int nin, nprod;                  /* fields of the inverse and forward exchanges */
+  size_t elem_bytes;
+} tg_slab_info;
+int tg_slab_create(const tg_config* cfg, int world, int rank, tg_ctx** out);
+int tg_slab_info_get(const tg_ctx* ctx, tg_slab_info* info);
+int tg_slab_buffer(tg_ctx* ctx, int which, int field, void** ptr);
+int tg_slab_phase(tg_ctx* ctx, int phase, int stage);
+/* state field f (V1..V3, then T) in the reference layout [N1][N2][N3/2+1] complex: upload
+ * keeps the rank's stored rows, download writes them (other rows of host untouched) */
+int tg_slab_upload(tg_ctx* ctx, int field, const double* host);
+int tg_slab_download(tg_ctx* ctx, int field, double* host);
+/* the reductions after phase 3 or 5 (sums[0] energy of U, sums[1] sum mult K^2 |U|^2, [4], [5]
+ * the same of T) and scalars [0] dt, [1] time, [2] steps, [3] non-finite flag */
+int tg_slab_scalars(tg_ctx* ctx, double* sums, double* scalars);
+
 typedef struct tg_server_config {
   size_t hbm_budget_bytes; /* admission budget: device bytes of all resident batches */
   int max_batch;           /* most requests in one batch */

@@ -130,6 +130,23 @@ class tg_server_stats(C.Structure):
     ]
 
 
+TG_SLAB_MAX_RANKS = 64
+TG_SLAB_INV_SEND, TG_SLAB_INV_RECV, TG_SLAB_FWD_SEND, TG_SLAB_FWD_RECV = 0, 1, 2, 3
+TG_SLAB_SUMS, TG_SLAB_GLOBAL_SUMS = 4, 5
+
+
+class tg_slab_info(C.Structure):
+    _fields_ = [
+        ("world", C.c_int), ("rank", C.c_int),
+        ("x0", C.c_int), ("nx", C.c_int), ("y0", C.c_int), ("ny", C.c_int),
+        ("xs", C.c_int * TG_SLAB_MAX_RANKS), ("xn", C.c_int * TG_SLAB_MAX_RANKS),
+        ("ys", C.c_int * TG_SLAB_MAX_RANKS), ("yn", C.c_int * TG_SLAB_MAX_RANKS),
+        ("nkx", C.c_int), ("nky", C.c_int), ("nkz", C.c_int), ("kzp", C.c_int),
+        ("nin", C.c_int), ("nprod", C.c_int),
+        ("elem_bytes", C.c_size_t),
+    ]
+
+
 class tg_batch_stat(C.Structure):
     _fields_ = [
         ("N", C.c_int * 3),
@@ -222,6 +239,13 @@ SIGNATURES = {
     "tg_server_take_finished": (C.c_int, [_VP, C.POINTER(C.c_longlong), C.c_int, C.POINTER(C.c_int)]),
     "tg_server_stats_get": (C.c_int, [_VP, C.POINTER(tg_server_stats)]),
     "tg_server_batch_stats": (C.c_int, [_VP, C.POINTER(tg_batch_stat), C.c_int, C.POINTER(C.c_int)]),
+    "tg_slab_create": (C.c_int, [C.POINTER(tg_config), C.c_int, C.c_int, C.POINTER(_VP)]),
+    "tg_slab_info_get": (C.c_int, [_VP, C.POINTER(tg_slab_info)]),
+    "tg_slab_buffer": (C.c_int, [_VP, C.c_int, C.c_int, C.POINTER(_VP)]),
+    "tg_slab_phase": (C.c_int, [_VP, C.c_int, C.c_int]),
+    "tg_slab_upload": (C.c_int, [_VP, C.c_int, _DP]),
+    "tg_slab_download": (C.c_int, [_VP, C.c_int, _DP]),
+    "tg_slab_scalars": (C.c_int, [_VP, _DP, _DP]),
     "tg_server_clock": (C.c_double, [_VP]),
     "tg_request_bytes": (C.c_int, [C.POINTER(tg_config), C.c_int, C.POINTER(C.c_size_t)]),
 }

@@ -63,12 +63,6 @@ int ctx_sync(tg_ctx* c, const char* where) {
 
 }  // namespace tg
 
-#define TG_CK(call)                                        \
-  do {                                                     \
-    cudaError_t _e = (call);                               \
-    if (_e != cudaSuccess) return cuda_err(c, _e, #call);  \
-  } while (0)
-
 namespace {
 
 // Device table exp(-2 pi i m / L), m in [0, L), evaluated in long double and rounded.
@@ -192,6 +186,9 @@ int run_force(tg_ctx* c, const void* const* U, int uprec) {
   return TG_OK;
 }
 
+}  // namespace
+
+namespace tg {
 RKArgs rk_args(tg_ctx* c, int stage) {
   RKArgs a{};
   a.g = c->g;
@@ -223,7 +220,7 @@ RKArgs rk_args(tg_ctx* c, int stage) {
 }
 
 // reduce the partials of slots r0 .. r0+n-1 and apply the dt rule to each of them
-int run_finalize(tg_ctx* c, int dt_mode, bool ring, int r0 = 0, int n = -1) {
+int run_finalize(tg_ctx* c, int dt_mode, bool ring, int r0, int n) {
   if (n < 0) n = c->nact;
   FinalizeArgs f{};
   f.part = c->part + (size_t)r0 * 8 * c->npart_blocks;
@@ -248,7 +245,7 @@ int run_finalize(tg_ctx* c, int dt_mode, bool ring, int r0 = 0, int n = -1) {
   return TG_OK;
 }
 
-}  // namespace
+}  // namespace tg
 
 namespace tg {
 // energy partials of the master state of slots r0 .. r0+n-1 into reduction slots (U: 0,1;
@@ -450,7 +447,11 @@ void free_ctx(tg_ctx* c) {
     fr(c->PP[i]);
     fr(c->PY[i]);
     fr(c->PX[i]);
+    fr(c->SA[i]);
+    fr(c->SB[i]);
   }
+  for (int i = 0; i < 6; ++i) fr(c->SR[i]);
+  fr(c->gsum);
   fr(c->PR);
   fr(c->FB);
   fr(c->trigx);
@@ -531,8 +532,9 @@ const char* tg_last_error(const tg_ctx* ctx) { return ctx ? ctx->err.c_str() : "
 }  // extern "C"
 
 namespace tg {
-int ctx_create_batch(const tg_config* cfg, int B, tg_ctx** out) {
+int ctx_create_batch(const tg_config* cfg, int B, tg_ctx** out, int slab_W, int slab_r) {
   if (!cfg || !out || B < 1) return TG_ERR_ARG;
+  if (slab_W < 0 || (slab_W > 0 && (B != 1 || slab_r < 0 || slab_r >= slab_W))) return TG_ERR_ARG;
   *out = nullptr;
   {
     const int v = validate_config(cfg);
@@ -590,6 +592,27 @@ int ctx_create_batch(const tg_config* cfg, int B, tg_ctx** out) {
   g.kf1 = cfg->kfactor[1];
   g.kf2 = cfg->kfactor[2];
   g.basis = c->basis;
+  g.x0 = 0;
+  if (slab_W > 0) {
+    // rank slab_r's compact kx rows and real y planes (the reference's slab decomposition,
+    // basis_basicfn.cc:49-281: x slabs in spectral space, y slabs in real space)
+    if (g.nkx < slab_W || N2 < slab_W) {
+      delete c;
+      return TG_ERR_ARG;
+    }
+    c->slab_W = slab_W;
+    c->slab_r = slab_r;
+    c->slab_x.resize(slab_W);
+    c->slab_nx.resize(slab_W);
+    c->slab_y.resize(slab_W);
+    c->slab_ny.resize(slab_W);
+    for (int i = 0; i < slab_W; ++i) {
+      split_range(g.nkx, slab_W, i, c->slab_x[i], c->slab_nx[i]);
+      split_range(N2, slab_W, i, c->slab_y[i], c->slab_ny[i]);
+    }
+    g.x0 = c->slab_x[slab_r];
+    g.S = (long long)c->slab_nx[slab_r] * g.nky * g.kzp;
+  }
   c->S = g.S;
   c->D = (long long)N1 * N2 * c->M3;
 
@@ -705,8 +728,24 @@ int ctx_create_batch(const tg_config* cfg, int B, tg_ctx** out) {
   const size_t Sd1 = sizeof(cx<double>) * (size_t)g.S;
   const size_t Sd = Sd1 * B;
   const size_t St = c->tsz * (size_t)g.S * B;
-  const size_t WXb = c->tsz * (size_t)N1 * g.nky * g.kzp * B;
+  size_t WXb = c->tsz * (size_t)N1 * g.nky * g.kzp * B;
   const size_t WYb = c->tsz * (size_t)N1 * N2 * g.kzp * B;
+  size_t PPb = WYb, PYb = WXb;
+  if (slab_W > 0) {
+    // between the exchanges: [N1][ny][kzp] (x-inverse outputs, products), [nkx][ny][kzp]
+    // (x-forward outputs = forward send)
+    const size_t ny = (size_t)c->slab_ny[slab_r], nx = (size_t)c->slab_nx[slab_r];
+    WXb = PPb = c->tsz * (size_t)N1 * ny * g.kzp;
+    PYb = c->tsz * (size_t)g.nkx * ny * g.kzp;
+    const size_t Ab = c->tsz * nx * N2 * g.kzp;
+    for (int q = 0; q < c->nprod; ++q) {
+      if ((rc = dalloc(c, &c->SA[q], Ab))) return fail(rc);
+      if ((rc = dalloc(c, &c->SB[q], Ab))) return fail(rc);
+    }
+    for (int i = 0; i < c->nin; ++i)
+      if ((rc = dalloc(c, &c->SR[i], PYb))) return fail(rc);
+    if ((rc = dalloc(c, (void**)&c->gsum, sizeof(double) * 16))) return fail(rc);
+  }
   for (int i = 0; i < c->nstate; ++i) {
     if ((rc = dalloc(c, (void**)&c->U0[i], Sd))) return fail(rc);
     if ((rc = dalloc(c, (void**)&c->TOT[i], Sd))) return fail(rc);
@@ -716,11 +755,11 @@ int ctx_create_batch(const tg_config* cfg, int B, tg_ctx** out) {
   if ((rc = dalloc(c, (void**)&c->PR, Sd1))) return fail(rc);
   for (int i = 0; i < c->nin; ++i) {
     if ((rc = dalloc(c, &c->WX[i], WXb))) return fail(rc);
-    if ((rc = dalloc(c, &c->WY[i], WYb))) return fail(rc);
+    if (slab_W == 0 && (rc = dalloc(c, &c->WY[i], WYb))) return fail(rc);
   }
   for (int q = 0; q < c->nprod; ++q) {
-    if ((rc = dalloc(c, &c->PP[q], WYb))) return fail(rc);
-    if ((rc = dalloc(c, &c->PY[q], WXb))) return fail(rc);
+    if ((rc = dalloc(c, &c->PP[q], PPb))) return fail(rc);
+    if ((rc = dalloc(c, &c->PY[q], PYb))) return fail(rc);
     if ((rc = dalloc(c, &c->PX[q], St))) return fail(rc);
   }
   c->npart_blocks = reduction_blocks(g.S);
@@ -1023,6 +1062,7 @@ cudaError_t copy_stored(tg_ctx* c, cx<double>* compact, double* dense, bool to_d
 }  // namespace
 
 int tg_field_download_stored(tg_ctx* c, int field, double* host, size_t n) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c || !host || field < 0 || field >= TG_NFIELDS) return TG_ERR_ARG;
   if (n != 2 * (size_t)c->D) return set_err(c, TG_ERR_ARG, "download: n_doubles must be 2*N1*N2*(N3/2+1)");
   const int si = field_state_index(c, field);
@@ -1034,6 +1074,7 @@ int tg_field_download_stored(tg_ctx* c, int field, double* host, size_t n) {
 }
 
 int tg_field_upload(tg_ctx* c, int field, const double* host, size_t n) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c || !host || field < 0 || field >= TG_NFIELDS) return TG_ERR_ARG;
   if (n != 2 * (size_t)c->D) return set_err(c, TG_ERR_ARG, "upload: n_doubles must be 2*N1*N2*(N3/2+1)");
   cudaSetDevice(c->dev);
@@ -1071,6 +1112,7 @@ int tg_field_upload(tg_ctx* c, int field, const double* host, size_t n) {
 }
 
 int tg_field_download(tg_ctx* c, int field, double* host, size_t n) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c || !host || field < 0 || field >= TG_NFIELDS) return TG_ERR_ARG;
   if (n != 2 * (size_t)c->D) return set_err(c, TG_ERR_ARG, "download: n_doubles must be 2*N1*N2*(N3/2+1)");
   cudaSetDevice(c->dev);
@@ -1147,6 +1189,7 @@ int tg_field_download(tg_ctx* c, int field, double* host, size_t n) {
 }
 
 int tg_field_alloc(tg_ctx* c, int* field) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c || !field) return TG_ERR_ARG;
   *field = -1;
   cudaSetDevice(c->dev);
@@ -1164,6 +1207,7 @@ int tg_field_alloc(tg_ctx* c, int* field) {
 }
 
 int tg_field_free(tg_ctx* c, int field) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c || field < TG_WORK0 || field >= TG_WORK0 + TG_NWORK) return TG_ERR_ARG;
   const int i = field - TG_WORK0;
   if (!c->work_reserved[i]) return set_err(c, TG_ERR_STATE, "free: work field not reserved");
@@ -1179,6 +1223,7 @@ int tg_field_free(tg_ctx* c, int field) {
 }
 
 int tg_field_copy(tg_ctx* c, int dst, int src) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c || dst < 0 || dst >= TG_NFIELDS || src < 0 || src >= TG_NFIELDS) return TG_ERR_ARG;
   cudaSetDevice(c->dev);
   const bool dwork = dst >= TG_WORK0 && dst < TG_WORK0 + TG_NWORK;
@@ -1221,6 +1266,7 @@ int tg_field_copy(tg_ctx* c, int dst, int src) {
 }
 
 int tg_forward_transform(tg_ctx* c, int field, int parity) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c || field < TG_WORK0 || field >= TG_WORK0 + TG_NWORK) return TG_ERR_ARG;
   cudaSetDevice(c->dev);
   if (!c->dense[field]) return set_err(c, TG_ERR_STATE, "transform: work field never written");
@@ -1229,6 +1275,7 @@ int tg_forward_transform(tg_ctx* c, int field, int parity) {
 }
 
 int tg_inverse_transform(tg_ctx* c, int field, int parity) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c || field < TG_WORK0 || field >= TG_WORK0 + TG_NWORK) return TG_ERR_ARG;
   cudaSetDevice(c->dev);
   if (!c->dense[field]) return set_err(c, TG_ERR_STATE, "transform: work field never written");
@@ -1237,6 +1284,7 @@ int tg_inverse_transform(tg_ctx* c, int field, int parity) {
 }
 
 int tg_compute_force(tg_ctx* c) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c) return TG_ERR_ARG;
   cudaSetDevice(c->dev);
   if (c->force_on) {
@@ -1250,6 +1298,7 @@ int tg_compute_force(tg_ctx* c) {
 }
 
 int tg_set_force_modes(tg_ctx* c, int n, const int* k, const double* F) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c || n < 0 || (n > 0 && (!k || !F))) return TG_ERR_ARG;
   if (c->cfg.force_kind != TG_FORCE_MODES) return set_err(c, TG_ERR_STATE, "set_force_modes: force_kind is not TG_FORCE_MODES");
   cudaSetDevice(c->dev);
@@ -1310,6 +1359,7 @@ int tg_set_force_modes(tg_ctx* c, int n, const int* k, const double* F) {
 }
 
 int tg_compute_nlin(tg_ctx* c) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c) return TG_ERR_ARG;
   cudaSetDevice(c->dev);
   const void* in[6];
@@ -1323,6 +1373,7 @@ int tg_compute_nlin(tg_ctx* c) {
 }
 
 int tg_add_force(tg_ctx* c) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c) return TG_ERR_ARG;
   if (!c->have_nlin) return set_err(c, TG_ERR_STATE, "Add_force before Compute_nlin");
   cudaSetDevice(c->dev);
@@ -1344,6 +1395,7 @@ int tg_add_force(tg_ctx* c) {
 }
 
 int tg_compute_pressure(tg_ctx* c) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c) return TG_ERR_ARG;
   if (!c->have_nlin) return set_err(c, TG_ERR_STATE, "Compute_pressure before Compute_nlin");
   cudaSetDevice(c->dev);
@@ -1353,6 +1405,7 @@ int tg_compute_pressure(tg_ctx* c) {
 }
 
 int tg_compute_rhs(tg_ctx* c) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c) return TG_ERR_ARG;
   if (!c->have_nlin || !c->have_pressure) return set_err(c, TG_ERR_STATE, "Compute_rhs before Compute_pressure");
   cudaSetDevice(c->dev);
@@ -1361,6 +1414,7 @@ int tg_compute_rhs(tg_ctx* c) {
 }
 
 int tg_get_dt(tg_ctx* c, double* dt) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c) return TG_ERR_ARG;
   cudaSetDevice(c->dev);
   int rc = run_energy(c, 2);
@@ -1375,6 +1429,7 @@ int tg_get_dt(tg_ctx* c, double* dt) {
 }
 
 int tg_time_advance(tg_ctx* c) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c) return TG_ERR_ARG;
   if (!c->have_nlin || !c->have_pressure) return set_err(c, TG_ERR_STATE, "Time_advance needs Compute_nlin and Compute_pressure");
   cudaSetDevice(c->dev);
@@ -1391,6 +1446,7 @@ int tg_time_advance(tg_ctx* c) {
 }
 
 int tg_step(tg_ctx* c, int n, double* energies) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c || n < 0) return TG_ERR_ARG;
   if (n == 0) return TG_OK;
   cudaSetDevice(c->dev);
@@ -1449,6 +1505,7 @@ int tg_time(const tg_ctx* c, double* t, long long* steps) {
 }
 
 int tg_energy(tg_ctx* c, int group, double* energy, double* diss) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c) return TG_ERR_ARG;
   if (group < 0 || group > 2) return TG_ERR_ARG;
   if (group == 1 && c->phys != TG_MHD) return TG_ERR_ARG;
@@ -1466,6 +1523,7 @@ int tg_energy(tg_ctx* c, int group, double* energy, double* diss) {
 }
 
 int tg_shell_spectrum(tg_ctx* c, int group, double* ek, double* dissk, int n) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c || !ek) return TG_ERR_ARG;
   if (group < 0 || group > 2) return TG_ERR_ARG;
   if (group == 1 && c->phys != TG_MHD) return TG_ERR_ARG;
@@ -1549,12 +1607,14 @@ int tg_shell_spectrum(tg_ctx* c, int group, double* ek, double* dissk, int n) {
 }
 
 int tg_profile_enable(tg_ctx* c, int enable) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c) return TG_ERR_ARG;
   c->prof = enable != 0;
   return TG_OK;
 }
 
 int tg_profile_read(tg_ctx* c, tg_kernel_stat* out, int max, int* n) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c || (max > 0 && !out)) return TG_ERR_ARG;
   cudaSetDevice(c->dev);
   TG_SYNC(c, __func__);
@@ -1586,6 +1646,7 @@ int tg_profile_read(tg_ctx* c, tg_kernel_stat* out, int max, int* n) {
 }
 
 int tg_nusselt(tg_ctx* c, double* nu) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c || !nu) return TG_ERR_ARG;
   if (c->phys != TG_RB) return set_err(c, TG_ERR_ARG, "Nusselt number needs the RB physics");
   cudaSetDevice(c->dev);

@@ -123,6 +123,17 @@ struct tg_ctx {
   std::vector<ProfRec> prof_recs;
   std::vector<cudaEvent_t> ev_pool;
 
+  // slab-sharded single solve (tg_slab_*): this context is rank slab_r of slab_W; its spectral
+  // state holds compact kx rows [slab_x[r], slab_x[r] + slab_nx[r]) (g.x0, g.S local) and between
+  // the two exchanges of an RHS evaluation its pass buffers hold real y planes
+  // [slab_y[r], slab_y[r] + slab_ny[r]).  slab_W = 0: a whole-grid context.
+  int slab_W = 0, slab_r = 0;
+  std::vector<int> slab_x, slab_nx, slab_y, slab_ny;
+  void* SA[9] = {};   // [nx][N2][kzp]: y-inverse outputs of the inputs; unpacked products
+  void* SB[9] = {};   // [nx][N2][kzp] as W chunks [nx][ny_d][kzp]: inverse send, forward receive
+  void* SR[6] = {};   // [nkx][ny][kzp]: inverse receive (sources in rank order)
+  double* gsum = nullptr;  // [8] reductions summed over the ranks (written by the host's all-reduce)
+
   // graph of one fused step
   cudaGraphExec_t step_graph = nullptr;
   bool graphs = true;
@@ -139,6 +150,14 @@ void wait_args(const tg_ctx* c, AxisArgs& a);
 // its tile since the last check (TG_ERR_TIMEOUT: the results of that work are not valid; the
 // word is cleared, so the context stays usable) or a CUDA error
 int ctx_sync(tg_ctx* c, const char* where);
+// a slab context (tg_slab_create) answers only the tg_slab_* calls: TG_ERR_STATE with a message
+int slab_refuse(tg_ctx* c);
+// a CUDA call inside a function with a context `c` in scope: its error becomes the call's status
+#define TG_CK(call)                                        \
+  do {                                                     \
+    cudaError_t _e = (call);                               \
+    if (_e != cudaSuccess) return cuda_err(c, _e, #call);  \
+  } while (0)
 #define TG_SYNC(c, where)                      \
   do {                                         \
     const int _rs = tg::ctx_sync((c), (where)); \
@@ -165,8 +184,19 @@ int pipe_inverse_xy(tg_ctx* c, int nf, const void* const* in, const void* const*
 int pipe_products_forward(tg_ctx* c, int nin, const void* const* WY, int nprod, const ProdPairs& pp,
                           void* const* PP, void* const* PY, void* const* PX, const int* xkinds = nullptr);
 int dalloc_ctx(tg_ctx* c, void** p, size_t bytes);
-// a context holding B same-shape request slots (B = 1: tg_ctx_create)
-int ctx_create_batch(const tg_config* cfg, int B, tg_ctx** out);
+// a context holding B same-shape request slots (B = 1: tg_ctx_create); with slab_W > 0, rank
+// slab_r's share of a slab-sharded solve (B = 1)
+int ctx_create_batch(const tg_config* cfg, int B, tg_ctx** out, int slab_W = 0, int slab_r = 0);
+// arguments of the RK stage kernel for the context's current buffers
+RKArgs rk_args(tg_ctx* c, int stage);
+// reduce the partials of slots r0 .. r0+n-1 (n < 0: all active) and apply the dt rule
+int run_finalize(tg_ctx* c, int dt_mode, bool ring, int r0 = 0, int n = -1);
+// start and count of part i of n items split over W parts (the first n % W parts one larger)
+inline void split_range(int n, int W, int i, int& start, int& count) {
+  const int b = n / W, rem = n % W;
+  count = b + (i < rem ? 1 : 0);
+  start = i * b + (i < rem ? i : rem);
+}
 size_t ctx_bytes_estimate(const tg_config* cfg, int B, bool with_staging);
 int ensure_staging_ctx(tg_ctx* c);
 // TG_OK or the code tg_ctx_create returns for cfg before allocating anything

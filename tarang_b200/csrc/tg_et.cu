@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(TPB) k_et_contract(ContractArgs a) {
     int r1, r2, l3;
     compact_mode(g, idx, r1, r2, l3);
     if (l3 >= g.nkz) continue;
-    const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
+    const int l1 = geo_l1(g, r1), l2 = amap_index(g.ay, r2);
     const double kx = geo_kx(g, r1) * g.kf0, ky = geo_ky(g, r2) * g.kf1, kz = l3 * g.kf2;
     const double K = sqrt(kx * kx + ky * ky + kz * kz);
     int bin = 0;  // receiver annulus: first rho >= |K|
@@ -500,7 +500,7 @@ __global__ void __launch_bounds__(256) k_force_feed_lm(Geo g, const cx<double>* 
     const double bk = b0 * kx + b1 * ky + b2 * kz;
     const cx<double> a = u0[idx], b = u1[idx], d = u2[idx];
     const double v2 = a.x * a.x + a.y * a.y + b.x * b.x + b.y * b.y + d.x * d.x + d.y * d.y;
-    const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
+    const int l1 = geo_l1(g, r1), l2 = amap_index(g.ay, r2);
     atomicAdd(&sh[sh_i], -2 * mult_four(l1, l2, l3, g.N1, g.N2) * (bk * bk / K2) * v2);
   }
   __syncthreads();
@@ -585,6 +585,7 @@ int helicity_table(tg_ctx* c, int magnetic, const std::vector<double>& rho, std:
 // out has n >= S+1 entries) or the n x n shell-to-shell table (giver rows 1 .. S-1, receivers binned by Get_shell_index over
 // |K| <= R_in; Shell_mult_*_all four_ET.cc:181-256, 999-1090, 1094-1190) of a helicity table.
 int helicity_out(tg_ctx* c, int magnetic, int shells, double* out, int n) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c || !out) return TG_ERR_ARG;
   const int S = c->cfg.n_shells;
   if (S < 6 || n < S + 1) return TG_ERR_ARG;
@@ -617,6 +618,7 @@ int helicity_out(tg_ctx* c, int magnetic, int shells, double* out, int n) {
 extern "C" {
 
 int tg_et_radii(tg_ctx* c, double* radii, int n) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c || !radii) return TG_ERR_ARG;
   const int S = c->cfg.n_shells;
   if (S < 6) return set_err(c, TG_ERR_ARG, "energy transfer needs at least 6 shells");
@@ -627,6 +629,7 @@ int tg_et_radii(tg_ctx* c, double* radii, int n) {
 }
 
 int tg_flux(tg_ctx* c, int kind, double* flux, int n) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c || !flux) return TG_ERR_ARG;
   const int S = c->cfg.n_shells;
   if (S < 6 || n < S + 1) return TG_ERR_ARG;
@@ -665,6 +668,7 @@ int tg_helicity_shell_to_shell(tg_ctx* c, double* tr, int n) { return helicity_o
 int tg_magnetic_helicity_shell_to_shell(tg_ctx* c, double* tr, int n) { return helicity_out(c, 1, 1, tr, n); }
 
 int tg_shell_to_shell(tg_ctx* c, int kind, double* tr, int n) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c || !tr) return TG_ERR_ARG;
   const int S = c->cfg.n_shells;
   if (S < 6 || n < S + 1) return TG_ERR_ARG;
@@ -698,7 +702,7 @@ __global__ void __launch_bounds__(256) k_force_feed_rb(Geo g, const cx<double>* 
     int sh_i = 0;
     while (sh_i <= S && !(K <= R.r[sh_i])) ++sh_i;
     if (sh_i > S) continue;
-    const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
+    const int l1 = geo_l1(g, r1), l2 = amap_index(g.ay, r2);
     const double m = g.basis == 0 ? mult_four(l1, l2, l3, g.N1, g.N2) : mult_scft(l1, l2, l3, g.N2);
     const cx<double> a = u1[idx], b = th[idx];
     atomicAdd(&sh[sh_i], 2 * m * coef * (a.x * b.x + a.y * b.y));
@@ -712,6 +716,7 @@ __global__ void __launch_bounds__(256) k_force_feed_rb(Geo g, const cx<double>* 
 // Compute_force_feed_shell(W) (Re(F_B . B*), MHD); 2: forceSF_shell of
 // Compute_force_feed_shell_scalar (Re(F_T . T*), passive scalar) (compute_force_feed.cc:70-155)
 int tg_force_feed_group(tg_ctx* c, int group, double* feed, int n) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c || !feed) return TG_ERR_ARG;
   const int S = c->cfg.n_shells;
   if (S < 6 || S > kMaxShells || n < S + 1 || group < 0 || group > 2) return TG_ERR_ARG;

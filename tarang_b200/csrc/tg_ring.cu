@@ -90,7 +90,7 @@ __global__ void __launch_bounds__(TPB) k_ring(RingArgs a, int use_smem) {
     int r1, r2, l3;
     compact_mode(g, idx, r1, r2, l3);
     if (l3 >= g.nkz) continue;
-    const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
+    const int l1 = geo_l1(g, r1), l2 = amap_index(g.ay, r2);
     const double k[3] = {geo_kx(g, r1) * g.kf0, geo_ky(g, r2) * g.kf1, l3 * g.kf2};
     const int ax = a.axis - 1, p1 = (ax + 1) % 3, p2 = (ax + 2) % 3;
     const double kpll = k[ax];
@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(TPB) k_shell_helicity(Geo g, const cx<double>*
     int r1, r2, l3;
     compact_mode(g, idx, r1, r2, l3);
     if (l3 >= g.nkz) continue;
-    const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
+    const int l1 = geo_l1(g, r1), l2 = amap_index(g.ay, r2);
     const double kx = geo_kx(g, r1) * g.kf0, ky = geo_ky(g, r2) * g.kf1, kz = l3 * g.kf2;
     const int b = (int)ceil(sqrt(kx * kx + ky * ky + kz * kz));
     if (b >= nbins) continue;
@@ -385,7 +385,7 @@ __global__ void __launch_bounds__(TPB) k_ring_feed(RingFeedArgs a) {
     if (l3 >= g.nkz) continue;
     const int bin = ring_bin(a.b, K, th);
     if (bin < 0) continue;
-    const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
+    const int l1 = geo_l1(g, r1), l2 = amap_index(g.ay, r2);
     double re = 0;
     if (a.lm) {
       const double K2 = k[0] * k[0] + k[1] * k[1] + k[2] * k[2];
@@ -429,7 +429,7 @@ __global__ void __launch_bounds__(TPB) k_ring_contract(RingContractArgs a) {
     const int bin = ring_bin(a.b, K, th);
     if (bin < 0) continue;
     const int shell = bin / cols, sector = bin - shell * cols;
-    const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
+    const int l1 = geo_l1(g, r1), l2 = amap_index(g.ay, r2);
     double v = 0;
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
@@ -478,6 +478,7 @@ void ring_radii(const tg_ctx* c, int n, double* r) { ring_radii_from((double)rad
 extern "C" {
 
 int tg_ring_radii(tg_ctx* c, int n_ring_shells, double* radii, int n) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c || !radii || n_ring_shells < 5 || n_ring_shells > kMaxRingShells || n < n_ring_shells + 1) return TG_ERR_ARG;
   ring_radii(c, n_ring_shells, radii);
   return TG_OK;
@@ -594,6 +595,7 @@ int run_ring_tr(tg_ctx* c, int kind, int axis, int n_ring_shells, int n_sectors,
 extern "C" {
 
 int tg_ring_sizes(tg_ctx* c, int axis, int* ring_shells, int* cylinder_shells) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c || axis < 1 || axis > 3) return TG_ERR_ARG;
   if (ring_shells) *ring_shells = radius_inside(c) + 1;
   if (cylinder_shells) *cylinder_shells = krho_inside(c, axis) + 1;
@@ -601,27 +603,33 @@ int tg_ring_sizes(tg_ctx* c, int axis, int* ring_shells, int* cylinder_shells) {
 }
 
 int tg_ring_spectrum(tg_ctx* c, int group, int axis, int n_sectors, double* ek1, double* ek2, double* dissk, int n) {
+  if (c && c->slab_W) return slab_refuse(c);
   return run_ring(c, group, axis, n_sectors, 0, ek1, ek2, dissk, n);
 }
 
 int tg_cylinder_ring_spectrum(tg_ctx* c, int group, int axis, int n_slabs, double* ek1, double* ek2, double* dissk,
                               int n) {
+  if (c && c->slab_W) return slab_refuse(c);
   return run_ring(c, group, axis, n_slabs, 1, ek1, ek2, dissk, n);
 }
 
 int tg_ring_to_ring(tg_ctx* c, int kind, int axis, int n_ring_shells, int n_sectors, double* tr, int n) {
+  if (c && c->slab_W) return slab_refuse(c);
   return run_ring_tr(c, kind, axis, n_ring_shells, n_sectors, 0, tr, n);
 }
 
 int tg_ring_spectrum_helicity(tg_ctx* c, int group, int axis, int n_sectors, double* h, int n) {
+  if (c && c->slab_W) return slab_refuse(c);
   return run_ring(c, group, axis, n_sectors, 0, h, nullptr, nullptr, n, 1);
 }
 
 int tg_cylinder_ring_spectrum_helicity(tg_ctx* c, int group, int axis, int n_slabs, double* h, int n) {
+  if (c && c->slab_W) return slab_refuse(c);
   return run_ring(c, group, axis, n_slabs, 1, h, nullptr, nullptr, n, 1);
 }
 
 int tg_shell_spectrum_helicity(tg_ctx* c, int group, double* h1, double* h2, double* h3, int n) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c || !h1) return TG_ERR_ARG;
   if (c->basis != TG_FOUR) return set_err(c, TG_ERR_UNSUPPORTED, "helicity spectrum: FOUR basis only");
   if (group != 0 && !(group == 1 && c->phys == TG_MHD)) return TG_ERR_ARG;
@@ -682,6 +690,7 @@ int tg_shell_spectrum_helicity(tg_ctx* c, int group, double* h1, double* h2, dou
 // Compute_force_feed_ring / Compute_force_feed_cylinder_ring (compute_force_feed.cc:162-300)
 int tg_force_feed_ring(tg_ctx* c, int group, int cylinder, int axis, int n_ring_shells, int n_sectors, double* out,
                        int n) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c || !out) return TG_ERR_ARG;
   if (c->phys == TG_RB || (c->basis != TG_FOUR && !(c->force_on == 1 && c->phys != TG_MHD)))
     return set_err(c, TG_ERR_UNSUPPORTED, "ring force feed: FOUR or an SCFT band forcing, no convection");
@@ -728,10 +737,12 @@ int tg_force_feed_ring(tg_ctx* c, int group, int cylinder, int axis, int n_ring_
 }
 
 int tg_cylinder_ring_to_ring(tg_ctx* c, int kind, int axis, int n_cylinder_shells, int n_slabs, double* tr, int n) {
+  if (c && c->slab_W) return slab_refuse(c);
   return run_ring_tr(c, kind, axis, n_cylinder_shells, n_slabs, 1, tr, n);
 }
 
 int tg_cylinder_radii(tg_ctx* c, int axis, int n_cylinder_shells, double* radii, int n) {
+  if (c && c->slab_W) return slab_refuse(c);
   if (!c || !radii || axis < 1 || axis > 3 || n_cylinder_shells < 5 || n_cylinder_shells > kMaxRingShells ||
       n < n_cylinder_shells + 1)
     return TG_ERR_ARG;

@@ -58,7 +58,7 @@ __global__ void k_dense_to_compact(Geo g, const cx<double>* __restrict__ dense, 
   compact_mode(g, idx, r1, r2, l3);
   cx<double> v = mkc<double>(0, 0);
   if (l3 < g.nkz) {
-    const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
+    const int l1 = geo_l1(g, r1), l2 = amap_index(g.ay, r2);
     const int M3 = g.N3 / 2 + 1;
     v = dense[((long long)l1 * g.N2 + l2) * M3 + l3];
   }
@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(TPB, RKOcc<PHYS>::v) k_rk(RKArgs a) {
 #pragma unroll
       for (int c = 0; c < NS; ++c) r[c] = a.RHS[c][gi];
     }
-    const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
+    const int l1 = geo_l1(g, r1), l2 = amap_index(g.ay, r2);
     double eh = 0, e1 = 0;
 #pragma unroll
     for (int c = 0; c < NS; ++c) {
@@ -605,7 +605,7 @@ __global__ void __launch_bounds__(TPB) k_cross_partials(Geo g, const cx<double>*
     int r1, r2, l3;
     compact_mode(g, idx, r1, r2, l3);
     if (l3 >= g.nkz) continue;
-    const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
+    const int l1 = geo_l1(g, r1), l2 = amap_index(g.ay, r2);
     double w;
     if (g.basis == 0) {
       w = energy_weight_four(l1, l2, l3, g.N1, g.N2);
@@ -627,7 +627,7 @@ __global__ void __launch_bounds__(TPB) k_energy_partials(Geo g, PtrArr6 pa, int 
     int r1, r2, l3;
     compact_mode(g, idx, r1, r2, l3);
     if (l3 < g.nkz) {
-      const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
+      const int l1 = geo_l1(g, r1), l2 = amap_index(g.ay, r2);
       const double kx = geo_kx(g, r1) * g.kf0, ky = geo_ky(g, r2) * g.kf1, kz = l3 * g.kf2;
       const double K2 = kx * kx + ky * ky + kz * kz;
       double w, m;
@@ -707,7 +707,7 @@ __global__ void __launch_bounds__(TPB) k_shell_spectrum(Geo g, PtrArr6 pa, int n
     int r1, r2, l3;
     compact_mode(g, idx, r1, r2, l3);
     if (l3 >= g.nkz) continue;
-    const int l1 = amap_index(g.ax, r1), l2 = amap_index(g.ay, r2);
+    const int l1 = geo_l1(g, r1), l2 = amap_index(g.ay, r2);
     const double kx = geo_kx(g, r1) * g.kf0, ky = geo_ky(g, r2) * g.kf1, kz = l3 * g.kf2;
     const double K = sqrt(kx * kx + ky * ky + kz * kz);
     const int bin = (int)ceil(K);

@@ -15,9 +15,12 @@ struct Geo {
   int N1, N2, N3;
   AxisMap ax, ay;       // stored kx, ky (FFT index space)
   int nkx, nky, nkz, kzp;
-  long long S;          // compact elements per field
+  long long S;          // compact elements per field (of the context's kx rows)
   double kf0, kf1, kf2; // kfactor
   int basis;            // 0 FOUR, 1 SCFT
+  // a slab context holds compact kx rows x0 .. x0 + S / (nky kzp) - 1 of the nkx stored rows;
+  // a whole-grid context has x0 = 0
+  int x0;
 };
 
 __host__ __device__ __forceinline__ void compact_mode(const Geo& g, long long idx, int& r1, int& r2, int& l3) {
@@ -26,8 +29,10 @@ __host__ __device__ __forceinline__ void compact_mode(const Geo& g, long long id
   r2 = (int)(rr % g.nky);
   r1 = (int)(rr / g.nky);
 }
+// FFT index l1 of the context's compact kx row r1
+__host__ __device__ __forceinline__ int geo_l1(const Geo& g, int r1) { return amap_index(g.ax, r1 + g.x0); }
 __host__ __device__ __forceinline__ int geo_kx(const Geo& g, int r1) {
-  const int l1 = amap_index(g.ax, r1);
+  const int l1 = geo_l1(g, r1);
   if (g.basis == 1) return l1;
   return l1 <= g.N1 / 2 ? l1 : l1 - g.N1;
 }
