@@ -597,7 +597,7 @@ int ctx_create_batch(const tg_config* cfg, int B, tg_ctx** out, int slab_W, int 
     // rank slab_r's compact kx rows and real y planes (the reference's slab decomposition,
     // basis_basicfn.cc:49-281: x slabs in spectral space, y slabs in real space)
     if (g.nkx < slab_W || N2 < slab_W) {
-      delete c;
+      free_ctx(c);
       return TG_ERR_ARG;
     }
     c->slab_W = slab_W;
