@@ -11,6 +11,7 @@
 #include <cstring>
 
 #include "tg_fft_launch.h"
+#include "tg_fft_tc.cuh"
 #include "tg_tma.cuh"
 
 namespace tg {
@@ -324,8 +325,54 @@ cudaError_t run_r2r_gemm(const AxisLaunch& l, const R2RArgs& r, cudaStream_t s, 
   return run_r2r_gemm_rt<Ri, Ro, Rw, 22>(l, r, nout, nin, s);
 }
 
+// FP32 forms: the x-pass contraction on the tensor cores (k_axis_r2r_tc, 3xTF32) unless
+// TG_R2R_TC=0
+bool r2r_tc_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("TG_R2R_TC");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
+
+template <typename Ri>
+cudaError_t run_r2r_tc(const AxisLaunch& l, const R2RArgs& r, cudaStream_t s, bool* used) {
+  *used = false;
+  if (!r2r_tc_enabled()) return cudaSuccess;
+  const int nin = amap_count(l.a.in), nout = amap_count(l.a.out);
+  for (int f = 0; f < l.nfields; ++f) {
+    const int k = r.kind[f];
+    if (k < 0 || k > 3 || !r.mat[k] || r.mat_rows[k] != nout || r.mat_cols[k] != nin) return cudaSuccess;
+  }
+  // float4 column loads and stores need row starts on 16-byte boundaries
+  if (nin < 1 || nout < 1 || (l.a.sr % 2) || (l.a.sb % 2) || (l.a.dr % 2) || (l.a.db % 2)) return cudaSuccess;
+  TcArgs t{};
+  t.npad = (nout + 15) / 16 * 16;
+  t.kpad = (nin + 7) / 8 * 8;
+  if (t.npad > 256) return cudaSuccess;
+  t.tmem_cols = 32;
+  while (t.tmem_cols < t.npad) t.tmem_cols *= 2;
+  t.ntiles = (int)((2LL * l.a.ncols + 127) / 128);
+  const size_t smem = sizeof(float) * (2 * (size_t)t.npad * t.kpad + 4 * 128 * (size_t)kTcKC) + 32;
+  if (smem > 227 * 1024) return cudaSuccess;
+  auto kern = k_axis_r2r_tc<Ri>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int per = l.nbatch * l.nfields;
+  const int P = std::max(1, std::min(t.ntiles, (2 * 148 + per - 1) / per));
+  *used = true;
+  dim3 grid(P, l.nbatch, l.nfields);
+  kern<<<grid, 128, smem, s>>>(l.a, l.ps, r, t);
+  return cudaGetLastError();
+}
+
 template <typename Ri, typename Ro, typename Rw>
 cudaError_t run_r2r(const AxisLaunch& l, const R2RArgs& r, int N, cudaStream_t s) {
+  if constexpr (sizeof(Ro) == 4 && sizeof(Rw) == 4) {
+    bool used = false;
+    cudaError_t e = run_r2r_tc<Ri>(l, r, s, &used);
+    if (e != cudaSuccess || used) return e;
+  }
   {
     bool used = false;
     cudaError_t e = run_r2r_gemm<Ri, Ro, Rw>(l, r, s, &used);

@@ -142,3 +142,22 @@ def test_register_tiled_x_pass_matches_matrix_product(lib):
     """The SCFT x-pass as a register-tiled matrix product (default) equals the shared-memory
     matrix product (TG_R2R_GEMM=0): same sums in the same order."""
     compare(run("1", RCASES, "TG_R2R_GEMM"), run("0", RCASES, "TG_R2R_GEMM"), RCASES)
+
+
+TCASES = [
+    ("rb129_fp32", (129, 32, 32), dict(basis="SCFT", physics="RB", Ra=1e4, Pr=1.0, kfactor=KF_RB, dt=1e-4,
+                                       precision="FP32")),
+    ("rb65_fp32", (65, 32, 64), dict(basis="SCFT", physics="RB", Ra=1e4, Pr=1.0, kfactor=KF_RB, dt=1e-4,
+                                     precision="FP32")),
+    ("rb33_fp32", (33, 16, 16), dict(basis="SCFT", physics="RB", Ra=1e4, Pr=1.0, kfactor=KF_RB, dt=1e-4,
+                                     precision="FP32")),
+    ("scft_fluid_fp32", (24, 16, 32), dict(basis="SCFT", nu=2e-3, dt=1e-3, kfactor=KF_RB, precision="FP32")),
+    ("scft_fluid_full32", (24, 16, 32), dict(basis="SCFT", nu=2e-3, dt=1e-3, kfactor=KF_RB, dealias=False,
+                                             precision="FP32")),
+]
+
+
+def test_tensor_core_x_pass_matches_register_tiled(lib):
+    """FP32 forms: the SCFT x-pass on the tensor cores (3xTF32 tcgen05, TG_R2R_TC=1) against the
+    register-tiled FP32 matrix product (TG_R2R_TC=0), to FP32-mixed rounding."""
+    compare(run("1", TCASES, "TG_R2R_TC"), run("0", TCASES, "TG_R2R_TC"), TCASES)
