@@ -28,10 +28,12 @@ namespace tg {
 constexpr int kTcKC = 32;          // K rows per shared-memory chunk
 constexpr int kTcPolls = 1 << 22;  // bounded mbarrier waits
 
+// the TF32 part of x: rounded to the nearest 10-bit mantissa and the 13 lower bits cleared, so
+// that x - hi is exact (the tensor cores read only the upper 19 bits of each operand)
 __device__ __forceinline__ float tf32_hi(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return __uint_as_float(r);
+  uint32_t u = __float_as_uint(x);
+  if ((u & 0x7f800000u) != 0x7f800000u) u += 0x1000u;
+  return __uint_as_float(u & 0xffffe000u);
 }
 
 // shared-memory matrix descriptor, no swizzle (tcgen05 version 1): start, LBO, SBO in bytes
