@@ -325,27 +325,39 @@ cudaError_t run_r2r_gemm(const AxisLaunch& l, const R2RArgs& r, cudaStream_t s, 
   return run_r2r_gemm_rt<Ri, Ro, Rw, 22>(l, r, nout, nin, s);
 }
 
-// FP32 forms: the x-pass contraction on the tensor cores (k_axis_r2r_tc, 3xTF32) unless
-// TG_R2R_TC=0
-bool r2r_tc_enabled() {
-  static const bool on = [] {
+// FP32 forms: the x-pass contraction on the tensor cores (k_axis_r2r_tc, 3xTF32) when a field of
+// one request spans at least kTcMinTiles column tiles (the per-block set-up and the pipeline fill
+// amortise; measured: 352 tiles, the 129 x 256 x 256 convection step, 2.42 ms against 2.89 ms; 64
+// tiles, 65 x 128 x 128, 0.43 ms against 0.39 ms).  The rule looks at one request's geometry only,
+// so a request batched in the serving loop takes the same path as on a lone context.
+// TG_R2R_TC=0 never, =1 always.
+constexpr int kTcMinTiles = 128;
+int r2r_tc_mode() {
+  static const int m = [] {
     const char* e = std::getenv("TG_R2R_TC");
-    return e && e[0] == '1';
+    if (e && e[0] == '0') return 0;
+    if (e && e[0] == '1') return 1;
+    return 2;
   }();
-  return on;
+  return m;
 }
 
 template <typename Ri>
 cudaError_t run_r2r_tc(const AxisLaunch& l, const R2RArgs& r, cudaStream_t s, bool* used) {
   *used = false;
-  if (!r2r_tc_enabled()) return cudaSuccess;
+  const int mode = r2r_tc_mode();
+  if (mode == 0) return cudaSuccess;
+  if (mode == 2 && (2LL * l.a.ncols + 127) / 128 < kTcMinTiles) return cudaSuccess;
   const int nin = amap_count(l.a.in), nout = amap_count(l.a.out);
   for (int f = 0; f < l.nfields; ++f) {
     const int k = r.kind[f];
     if (k < 0 || k > 3 || !r.mat[k] || r.mat_rows[k] != nout || r.mat_cols[k] != nin) return cudaSuccess;
   }
-  // float4 column loads and stores need row starts on 16-byte boundaries
-  if (nin < 1 || nout < 1 || (l.a.sr % 2) || (l.a.sb % 2) || (l.a.dr % 2) || (l.a.db % 2)) return cudaSuccess;
+  // the bulk row copies need 16-byte aligned row starts and sizes: even strides (complex) and
+  // column counts that are multiples of 8
+  if (nin < 1 || nout < 1 || (l.a.sr % 2) || (l.a.sb % 2) || (l.a.ncols % 8)) return cudaSuccess;
+  for (int f = 0; f < l.nfields; ++f)
+    if (reinterpret_cast<uintptr_t>(l.ps.src[f]) % 16) return cudaSuccess;
   TcArgs t{};
   t.npad = (nout + 15) / 16 * 16;
   t.kpad = (nin + 7) / 8 * 8;
@@ -353,16 +365,25 @@ cudaError_t run_r2r_tc(const AxisLaunch& l, const R2RArgs& r, cudaStream_t s, bo
   t.tmem_cols = 32;
   while (t.tmem_cols < t.npad) t.tmem_cols *= 2;
   t.ntiles = (int)((2LL * l.a.ncols + 127) / 128);
-  const size_t smem = sizeof(float) * (2 * (size_t)t.npad * t.kpad + 4 * 128 * (size_t)kTcKC) + 32;
+  // B pairs, NAB operand pairs, two staging buffers of raw rows, three mbarriers, slot and flag;
+  // two operand buffers where they fit
+  auto bytes = [&](int nab) {
+    return sizeof(float) * (2 * (size_t)t.npad * t.kpad + 2 * (size_t)nab * 128 * kTcKC) +
+           sizeof(Ri) * 2 * 128 * (size_t)kTcKC + 80;
+  };
+  const int nab = bytes(2) <= 227 * 1024 ? 2 : 1;
+  const size_t smem = bytes(nab);
   if (smem > 227 * 1024) return cudaSuccess;
-  auto kern = k_axis_r2r_tc<Ri>;
+  auto kern = nab == 2 ? k_axis_r2r_tc<Ri, 2> : k_axis_r2r_tc<Ri, 1>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
+  // one block per SM fits (shared memory): one persistent wave of at most 148 blocks, or one block
+  // per (batch, field) when those alone exceed it
   const int per = l.nbatch * l.nfields;
-  const int P = std::max(1, std::min(t.ntiles, (2 * 148 + per - 1) / per));
+  const int P = std::max(1, std::min(t.ntiles, 148 / per));
   *used = true;
   dim3 grid(P, l.nbatch, l.nfields);
-  kern<<<grid, 128, smem, s>>>(l.a, l.ps, r, t);
+  kern<<<grid, kTcThreads, smem, s>>>(l.a, l.ps, r, t);
   return cudaGetLastError();
 }
 
