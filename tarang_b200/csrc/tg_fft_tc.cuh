@@ -11,14 +11,15 @@
 // at float offset (r % 8) 4 + k % 4 + (k / 4) 32 + (r / 8) (KW / 4) 32 (core matrices of 8 rows x 4
 // k, 128 bytes; the stride between k chunks of 4, LBO, is 128 bytes, between groups of 8 rows,
 // SBO, KW * 32 bytes).  (With tcgen05 kind::tf32 the MN-major no-swizzle form returned zeros on
-// B200; the K-major form is exact.)  One thread issues the MMAs (tcgen05.mma
-// cta_group::1 kind::tf32, M = 128, K = 8 per instruction) and commits them to an mbarrier; the
-// K dimension runs in chunks of 32 through two shared-memory buffers, so the threads fill one while
-// the tensor cores read the other.  The epilogue reads tensor memory with tcgen05.ld (warp w owns
-// lanes 32 w .. 32 w + 31, the columns of its quarter of the tile) and stores each output row's
-// 128 columns coalesced.  Every wait on an mbarrier is bounded: past the limit the block records
-// the failure in the context's status word (TG_ERR_TIMEOUT on the host), waits again (bounded) for
-// its committed MMAs, frees its tensor memory and returns.
+// B200; the K-major form is exact.)  The K dimension runs in chunks of 32: a chunk's rows arrive
+// by untiled bulk copies (cp.async.bulk, no multicast) two chunks ahead in two staging buffers,
+// the threads split them into one of two operand buffers, and one thread issues the chunk's MMAs
+// (tcgen05.mma cta_group::1 kind::tf32, M = 128, K = 8 per instruction) and commits them to that
+// buffer's mbarrier.  The epilogue reads tensor memory with tcgen05.ld (warps w and w + 4 own lanes
+// 32 (w % 4) .. + 31, alternate 16-column groups) and stores each output row's 128 columns
+// coalesced.  Every wait on an mbarrier is bounded: past the limit the block records the failure
+// in the context's status word (TG_ERR_TIMEOUT on the host), waits again (bounded) for its
+// committed MMAs and issued copies, frees its tensor memory and returns.
 #pragma once
 
 #include "tg_fft.cuh"
