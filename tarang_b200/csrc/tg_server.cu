@@ -57,6 +57,8 @@ struct Batch {
   double step_ms = 0;                // measured time of one step at the current active count
   int step_ms_nact = 0;
   double idle_since = -1;            // server clock when the batch last became empty
+  int sat_out = 0;                   // consecutive rounds the batch sat out (kLagShare)
+  bool run_now = false;              // this round's decision
 };
 
 // Page-locked host blocks, reused by size: initial fields on their way to the device and
@@ -425,6 +427,26 @@ int launch_batch(tg_server* s, Batch& b, int k) {
 // still needs.  Until a batch has a measured step time it runs one.
 constexpr int kMaxStepsPerRound = 16;
 
+// Device time a batch still needs: its longest request's remaining steps x its measured step time
+// (negative until the batch has a timing)
+double remaining_ms(const tg_server* s, const Batch& b) {
+  if (!(b.step_ms > 0)) return -1.0;
+  int rem = 0;
+  for (long long id : b.slot_req) {
+    const Req& q = s->reqs.at(id);
+    rem = std::max(rem, q.n_steps - q.st.steps_done);
+  }
+  return rem * b.step_ms;
+}
+
+// A timed batch whose remaining device time is below this share of the largest one sits the round
+// out, so the batches that lag (late arrivals, large shapes) get the device and all of them head
+// for the same finishing time; that is the least possible makespan for the work resident.  A
+// batch that sat out kMaxSitOut rounds in a row runs anyway (no starvation under a steady stream
+// of long requests).
+constexpr double kLagShare = 0.5;
+constexpr int kMaxSitOut = 8;
+
 int steps_this_round(const tg_server* s, const Batch& b, double slowest_ms) {
   int left = 1 << 30;
   for (long long id : b.slot_req) {
@@ -583,12 +605,23 @@ int tg_server_pump(tg_server* s, int* n_active) {
   // launch a step of every resident batch first, so that the host work of admission (copies
   // into pinned blocks, new contexts) overlaps the steps on the device
   std::map<long long, std::pair<int, int>> launched;  // batch -> (slots stepped, launch code)
-  double slowest = 0;
+  double most = 0;
   for (auto& kv : s->batches)
-    if (!kv.second.slot_req.empty()) slowest = std::max(slowest, kv.second.step_ms);
+    if (!kv.second.slot_req.empty()) most = std::max(most, remaining_ms(s, kv.second));
   for (auto& kv : s->batches) {
     Batch& b = kv.second;
+    b.run_now = false;
     if (b.slot_req.empty()) continue;
+    const double r = remaining_ms(s, b);
+    b.run_now = r < 0 || !s->cfg.use_graphs || r >= kLagShare * most || b.sat_out >= kMaxSitOut;
+    b.sat_out = b.run_now ? 0 : b.sat_out + 1;
+  }
+  double slowest = 0;
+  for (auto& kv : s->batches)
+    if (kv.second.run_now) slowest = std::max(slowest, kv.second.step_ms);
+  for (auto& kv : s->batches) {
+    Batch& b = kv.second;
+    if (!b.run_now) continue;
     const int nl = (int)b.slot_req.size();
     const int k = s->cfg.use_graphs ? steps_this_round(s, b, slowest) : 1;
     launched[kv.first] = {nl, launch_batch(s, b, k)};
