@@ -526,6 +526,7 @@ def run_configs(args, torch, stream):
 
 # --------------------------------------------------------------------------------- serving
 KF_RB = (math.pi, math.pi / math.sqrt(2.0), math.pi / math.sqrt(2.0))
+SERVE_MAX_BATCH = 128   # request slots per batch: every type of the ensemble fits one batch
 SERVE_TYPES = [  # name, configuration, initial condition kind
     ("fluid32", dict(N=(32, 32, 32)), "fluid"),
     ("fluid64", dict(N=(64, 64, 64)), "fluid"),
@@ -603,23 +604,33 @@ def serve_workload(args):
 
 def serve_loop(srv, reqs, arrivals, mine, steps, keep):
     """Submit requests `mine` at their arrival times, pump until all finish; returns
-    (finish records by request index, kept results, pump round times, clock origin)."""
+    (finish records by request index, kept results, pump round times, clock origin).  Each round
+    is launched first (pump_begin) and the requests that have arrived are submitted while its
+    steps run on the device; pump_end admits them and waits for the round."""
     ids, fin, results, round_ms = {}, {}, {}, []
     t_base = srv.clock()
     sub = 0
     active = 0
-    while True:
+
+    def submit_arrived():
+        nonlocal sub
         now = srv.clock() - t_base
         while sub < len(mine) and arrivals[mine[sub]] <= now:
             i = mine[sub]
             ids[srv.submit(reqs[i][1], reqs[i][2], steps)] = i
             sub += 1
-        if sub < len(mine) and active == 0 and arrivals[mine[sub]] > now:
-            time.sleep(min(arrivals[mine[sub]] - now, 0.05))
-            active = 1
-            continue
+        return now
+
+    while True:
+        if active == 0:
+            now = submit_arrived()
+            if len(ids) == len(fin):          # nothing in the server: wait for the next arrival
+                time.sleep(min(max(arrivals[mine[sub]] - now, 0.0), 0.05))
+                continue
         r0 = time.perf_counter()
-        active = srv.pump()
+        srv.pump_begin()
+        submit_arrived()
+        active = srv.pump_end()
         round_ms.append(1e3 * (time.perf_counter() - r0))
         for rid in srv.take_finished():
             i = ids[rid]
@@ -716,7 +727,7 @@ def run_serving(args, rank=0, world=1, dist=False):
     if dist:
         import torch
         torch.distributed.barrier()
-    srv = Server(hbm_budget=args.serve_budget, max_batch=64, keep_results=True)
+    srv = Server(hbm_budget=args.serve_budget, max_batch=SERVE_MAX_BATCH, keep_results=True)
     fin, results, round_ms, t_base = serve_loop(srv, reqs, arrivals, mine, steps, keep)
     st = srv.stats()
     srv.close()
@@ -770,7 +781,7 @@ def run_serving(args, rank=0, world=1, dist=False):
                     "types uniform over " + ", ".join(n for n, _, _ in SERVE_TYPES) +
                     "; nu log-uniform [1e-3, 1e-2] (convection: Ra = Pr/nu^2, Pr = 1)",
         "gpus": world, "placement": "request i on rank i mod n_gpus, one server per GPU",
-        "hbm_budget_bytes_per_gpu": args.serve_budget, "max_batch": 64,
+        "hbm_budget_bytes_per_gpu": args.serve_budget, "max_batch": SERVE_MAX_BATCH,
         "requests_done": int(len(comp)), "requests_failed": sum(p["failed"] for p in parts),
         "aggregate_request_steps_per_s": agg,
         "aggregate_grid_point_steps_per_s": points / makespan,

@@ -548,15 +548,21 @@ int tg_server_destroy(tg_server* srv);
  * tg_ctx_create rejects or an init of the wrong length (no id).  A request that cannot fit the
  * budget even alone gets an id and state TG_REQ_FAILED with TG_ERR_OOM. */
 int tg_server_submit(tg_server* srv, const tg_request* req, long long* id);
-/* one scheduling round: advance the resident batches (batches on their own streams,
- * overlapping) by one step, or with graphs on by as many steps as fit in the slowest running
- * batch's step (at most 16, never past a request's last step); with graphs on, a batch whose
- * remaining device time (its longest request's remaining steps x its measured step time) is under
- * half the largest sits the round out (at most 8 rounds in a row), so that the lagging batches get
- * the device and all finish together; meanwhile admit queued requests that fit
+/* one scheduling round: advance the resident batches (one after another on the device, each on
+ * its own stream) by one step, or with graphs on by as many steps as fit in the slowest running
+ * batch's step (at most 16, never past a request's last step); meanwhile admit queued requests
+ * that fit
  * (first come first served, later ones may pass one that waits for room); then retire finished
  * and failed requests.  *n_active = requests running or queued afterwards */
 int tg_server_pump(tg_server* srv, int* n_active);
+/* tg_server_pump in two halves, so that the caller's own host work overlaps the round's steps on
+ * the device: pump_begin launches the round (TG_ERR_STATE when a round is already open);
+ * submissions, polls and results may follow; pump_end admits queued requests (those submitted
+ * in between included), waits for the round and retires finished requests, as tg_server_pump.
+ * pump_end without an open round is an admission-only round.  tg_server_drain and
+ * tg_server_destroy close an open round first. */
+int tg_server_pump_begin(tg_server* srv);
+int tg_server_pump_end(tg_server* srv, int* n_active);
 /* pump until every submitted request is done or failed (bounded by max_rounds; 0 = no bound) */
 int tg_server_drain(tg_server* srv, long long max_rounds);
 int tg_server_poll(tg_server* srv, long long id, tg_request_status* st);

@@ -232,6 +232,8 @@ SIGNATURES = {
     "tg_server_destroy": (C.c_int, [_VP]),
     "tg_server_submit": (C.c_int, [_VP, C.POINTER(tg_request), C.POINTER(C.c_longlong)]),
     "tg_server_pump": (C.c_int, [_VP, C.POINTER(C.c_int)]),
+    "tg_server_pump_begin": (C.c_int, [_VP]),
+    "tg_server_pump_end": (C.c_int, [_VP, C.POINTER(C.c_int)]),
     "tg_server_drain": (C.c_int, [_VP, C.c_longlong]),
     "tg_server_poll": (C.c_int, [_VP, C.c_longlong, C.POINTER(tg_request_status)]),
     "tg_server_result": (C.c_int, [_VP, C.c_longlong, _DP, C.c_size_t]),

@@ -352,33 +352,32 @@ cudaError_t run_r2r_tc(const AxisLaunch& l, const R2RArgs& r, cudaStream_t s, bo
   for (int f = 0; f < l.nfields; ++f) {
     const int k = r.kind[f];
     if (k < 0 || k > 3 || !r.mat[k] || r.mat_rows[k] != nout || r.mat_cols[k] != nin) return cudaSuccess;
+    if (l.a.comb[f]) return cudaSuccess;
   }
-  // the bulk row copies need 16-byte aligned row starts and sizes: even strides (complex) and
-  // column counts that are multiples of 8
-  if (nin < 1 || nout < 1 || (l.a.sr % 2) || (l.a.sb % 2) || (l.a.ncols % 8)) return cudaSuccess;
-  for (int f = 0; f < l.nfields; ++f)
-    if (reinterpret_cast<uintptr_t>(l.ps.src[f]) % 16) return cudaSuccess;
+  if (nin < 1 || nout < 1) return cudaSuccess;
   TcArgs t{};
   t.npad = (nout + 15) / 16 * 16;
   t.kpad = (nin + 7) / 8 * 8;
   if (t.npad > 256) return cudaSuccess;
-  t.tmem_cols = 32;
+  t.tmem_cols = 32;  // per accumulator; two of them
   while (t.tmem_cols < t.npad) t.tmem_cols *= 2;
   t.ntiles = (int)((2LL * l.a.ncols + 127) / 128);
-  // B pairs, NAB operand pairs, two staging buffers of raw rows, three mbarriers, slot and flag;
-  // two operand buffers where they fit
+  // coefficient pairs, nab operand slots of [hi, lo] chunks, eleven mbarriers, slot and flag;
+  // three slots where they fit
   auto bytes = [&](int nab) {
     return sizeof(float) * (2 * (size_t)t.npad * t.kpad + 2 * (size_t)nab * 128 * kTcKC) +
-           sizeof(Ri) * 2 * 128 * (size_t)kTcKC + 80;
+           sizeof(uint64_t) * (2 * kTcMaxNab + 5) + 16;
   };
-  const int nab = bytes(2) <= 227 * 1024 ? 2 : 1;
+  int nab = kTcMaxNab;
+  while (nab > 1 && bytes(nab) > 227 * 1024) --nab;
   const size_t smem = bytes(nab);
   if (smem > 227 * 1024) return cudaSuccess;
-  auto kern = nab == 2 ? k_axis_r2r_tc<Ri, 2> : k_axis_r2r_tc<Ri, 1>;
+  t.nab = nab;
+  auto kern = k_axis_r2r_tc<Ri>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  // one block per SM fits (shared memory): one persistent wave of at most 148 blocks, or one block
-  // per (batch, field) when those alone exceed it
+  // one block per SM (shared memory, tensor memory): one persistent wave of at most 148 blocks,
+  // or one block per (batch, field) when those alone exceed it
   const int per = l.nbatch * l.nfields;
   const int P = std::max(1, std::min(t.ntiles, 148 / per));
   *used = true;

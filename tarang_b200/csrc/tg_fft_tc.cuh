@@ -11,15 +11,25 @@
 // at float offset (r % 8) 4 + k % 4 + (k / 4) 32 + (r / 8) (KW / 4) 32 (core matrices of 8 rows x 4
 // k, 128 bytes; the stride between k chunks of 4, LBO, is 128 bytes, between groups of 8 rows,
 // SBO, KW * 32 bytes).  (With tcgen05 kind::tf32 the MN-major no-swizzle form returned zeros on
-// B200; the K-major form is exact.)  The K dimension runs in chunks of 32: a chunk's rows arrive
-// by untiled bulk copies (cp.async.bulk, no multicast) two chunks ahead in two staging buffers,
-// the threads split them into one of two operand buffers, and one thread issues the chunk's MMAs
-// (tcgen05.mma cta_group::1 kind::tf32, M = 128, K = 8 per instruction) and commits them to that
-// buffer's mbarrier.  The epilogue reads tensor memory with tcgen05.ld (warps w and w + 4 own lanes
-// 32 (w % 4) .. + 31, alternate 16-column groups) and stores each output row's 128 columns
-// coalesced.  Every wait on an mbarrier is bounded: past the limit the block records the failure
-// in the context's status word (TG_ERR_TIMEOUT on the host), waits again (bounded) for its
-// committed MMAs and issued copies, frees its tensor memory and returns.
+// B200; the K-major form is exact.)
+//
+// The block is warp-specialised and every hand-off is an mbarrier:
+//   converter warps (8)  read each K chunk (32 rows x 128 columns) straight from global memory
+//                        into registers several chunks ahead (coalesced: a warp reads 32
+//                        consecutive columns of a row), split them into TF32 pairs and write the
+//                        operand ring (NA slots), one arrival per thread -> op_full[slot]
+//   MMA warp (1 thread)  waits op_full, issues the chunk's MMAs (tcgen05.mma cta_group::1
+//                        kind::tf32, M = 128, K = 8 each) into one of two accumulators and commits
+//                        them to op_empty[slot]; after a tile's last chunk it commits acc_full
+//   epilogue warps (4)   wait acc_full, read the accumulator with tcgen05.ld (warp w: lanes
+//                        32 w .. 32 w + 31, one column each) and store each output row's 128
+//                        columns coalesced, then release the accumulator (acc_empty)
+// so the loads of later chunks, the MMAs of the current one and the stores of the previous tile
+// overlap; the bytes in flight per SM are the converters' register ring, not shared memory,
+// which the coefficient pairs and the operand ring fill.  Every wait is bounded: past the limit
+// the thread records the failure in the context's status word (TG_ERR_TIMEOUT on the host) and a
+// block-wide abort flag that ends the other roles' waits; the MMA thread then waits (bounded) for
+// its issued MMAs before the tensor memory is freed.
 #pragma once
 
 #include "tg_fft.cuh"
@@ -109,47 +119,80 @@ __device__ __forceinline__ int tc_off(int r, int k, int KW) {
   return (r & 7) * 4 + (k & 3) + (k >> 2) * 32 + (r >> 3) * (KW >> 2) * 32;
 }
 
+
 struct TcArgs {
   int npad;        // output rows padded to a multiple of 16 (MMA N)
   int kpad;        // input rows padded to a multiple of 8
-  int tmem_cols;   // tensor-memory columns allocated (a power of two >= 32, >= npad)
+  int tmem_cols;   // tensor-memory columns of one accumulator (a power of two >= 32, >= npad)
   int ntiles;      // 128-real-column tiles per batch row (ceil(2 ncols / 128))
+  int nab;         // operand ring slots
 };
 
-// one contiguous row segment global -> shared, completion counted in bytes on an mbarrier
-__device__ __forceinline__ void bulk_row(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_u32(dst)),
-               "l"(src), "r"(bytes), "r"(smem_u32(bar))
-               : "memory");
+constexpr int kTcEpiWarps = 4;   // warps 0-3: epilogue
+constexpr int kTcMmaWarp = 4;    // warp 4: tensor-memory allocation and the MMA thread
+constexpr int kTcCvtWarps = 8;   // warps 5-12: converters
+constexpr int kTcThreads = 32 * (kTcEpiWarps + 1 + kTcCvtWarps);
+constexpr int kTcMaxNab = 3;
+// the first converter warp asks L2 for the rows of the chunk this many chunks ahead of the one it
+// loads into registers (0: no prefetch)
+#ifndef TG_TC_PREFETCH
+#define TG_TC_PREFETCH 8
+#endif
+constexpr int kTcPrefetch = TG_TC_PREFETCH;
+// chunks each converter thread holds in registers ahead of the one it splits (16 values per chunk)
+template <typename Ri>
+struct TcRing {
+#ifndef TG_TC_RING32
+#define TG_TC_RING32 5
+#define TG_TC_RING64 3
+#endif
+  static constexpr int D = sizeof(Ri) == 4 ? TG_TC_RING32 : TG_TC_RING64;
+};
+
+// bounded wait that also ends when another role has aborted the block; false on either
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, int* wait_flag) {
+  for (int i = 0; i <= kTcPolls; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if ((i & 31) == 31 && *abort_flag) return false;
+  }
+  *abort_flag = 1;
+  if (wait_flag) atomicExch(wait_flag, 1);
+  return false;
+}
+
+__device__ __forceinline__ void tc_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
 // grid (P, nbatch, nfields): block (x, b, f) takes the tiles x, x + P, ... of batch b, field f.
-// Chunk i of the block (tile i / nkc, k rows (i % nkc) kTcKC ..) moves in three steps: its rows
-// arrive in staging buffer i % 2 by bulk copies issued two chunks ahead; the threads split them
-// into the K-major TF32 pairs of the operand buffer; one thread issues the chunk's MMAs.
-// NAB operand buffers (2: the split of chunk i + 1 overlaps the MMAs of chunk i; 1 where shared
-// memory is short); 256 threads: thread t splits column t % 128, k half t / 128 of each chunk, and
-// warps w and w + 4 read the same tensor-memory lanes, alternate 16-column groups of the accumulator
-constexpr int kTcThreads = 256;
-template <typename Ri, int NAB>
+template <typename Ri>
 __global__ void __launch_bounds__(kTcThreads, 1) k_axis_r2r_tc(AxisArgs a, PtrSet ps, R2RArgs r, TcArgs t) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int D = TcRing<Ri>::D;
+  constexpr int ACH = 128 * kTcKC;  // floats of one operand (hi or lo) chunk
   const int f = blockIdx.z, b = blockIdx.y;
   const int kind = r.kind[f];
   const int nrows = r.mat_rows[kind], nin = r.mat_cols[kind];
   const double* M = r.mat[kind];
-  const int NP = t.npad, KP = t.kpad;
-  constexpr int ACH = 128 * kTcKC;
+  const int NP = t.npad, KP = t.kpad, NA = t.nab, TC = t.tmem_cols;
   float* Bh = reinterpret_cast<float*>(smem_raw);
   float* Bl = Bh + NP * KP;
-  float* Abase = Bl + NP * KP;  // NAB operand chunks [hi, lo], K-major TF32 pairs
-  Ri* stg = reinterpret_cast<Ri*>(Abase + 2 * NAB * ACH);  // [2][kTcKC][128] raw rows
-  uint64_t* sbar = reinterpret_cast<uint64_t*>(stg + 2 * ACH);  // staging buffers
-  uint64_t* mbar = sbar + 2;  // MMA completion, one per operand buffer (commits of chunks i % NAB)
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 2);
-  int* flag = reinterpret_cast<int*>(tmem_slot + 1);
-  const int tid = threadIdx.x, warp = tid >> 5;
+  float* Abase = Bl + NP * KP;  // NA slots of [hi, lo] chunks
+  uint64_t* op_full = reinterpret_cast<uint64_t*>(Abase + 2 * (size_t)NA * ACH);
+  uint64_t* op_empty = op_full + kTcMaxNab;
+  uint64_t* acc_full = op_empty + kTcMaxNab;
+  uint64_t* acc_empty = acc_full + 2;
+  uint64_t* done_bar = acc_empty + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done_bar + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   for (int i = tid; i < NP * KP; i += kTcThreads) {
     const int k = i / NP, m = i - k * NP;
@@ -160,16 +203,21 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_axis_r2r_tc(AxisArgs a, PtrSe
     Bl[o] = v - h;
   }
   if (tid == 0) {
-    tc_mbar_init(smem_u32(&sbar[0]), 1);
-    tc_mbar_init(smem_u32(&sbar[1]), 1);
-    tc_mbar_init(smem_u32(&mbar[0]), 1);
-    tc_mbar_init(smem_u32(&mbar[1]), 1);
+    for (int s = 0; s < kTcMaxNab; ++s) {
+      tc_mbar_init(smem_u32(&op_full[s]), 32 * kTcCvtWarps);
+      tc_mbar_init(smem_u32(&op_empty[s]), 1);
+    }
+    for (int s = 0; s < 2; ++s) {
+      tc_mbar_init(smem_u32(&acc_full[s]), 1);
+      tc_mbar_init(smem_u32(&acc_empty[s]), 32 * kTcEpiWarps);
+    }
+    tc_mbar_init(smem_u32(done_bar), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    *flag = 1;
+    *abort_flag = 0;
   }
-  if (warp == 0) {
+  if (warp == kTcMmaWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(t.tmem_cols)
+                 "r"(2 * TC)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -178,150 +226,169 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_axis_r2r_tc(AxisArgs a, PtrSe
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  const uint32_t idesc = tc_idesc(NP);
-  const uint32_t bh = smem_u32(Bh), bl = smem_u32(Bl);
-  const uint32_t sbo_b = (uint32_t)KP * 32, sbo_a = kTcKC * 32;  // bytes between 8-row groups
-  const long long ncr = 2LL * a.ncols;                             // real columns
-  const Ri* src = reinterpret_cast<const Ri*>(ps.src[f]) + (long long)b * a.sb * 2;
-  float* dst = reinterpret_cast<float*>(ps.dst[f]) + (long long)b * a.db * 2;
-  const long long srr = 2 * a.sr, drr = 2 * a.dr;  // real strides of the rows
-  const float sc = (float)a.scale;
+  const long long ncr = 2LL * a.ncols;  // real columns
   const int nkc = (KP + kTcKC - 1) / kTcKC;
-  const int my_tiles = (t.ntiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+  const int P = (int)gridDim.x;
+  const int my_tiles = (t.ntiles - (int)blockIdx.x + P - 1) / P;
   const int nchunks = my_tiles * nkc;
+  int* wflag = a.wait_flag;
 
-  // thread 0: the bulk copies of chunk i into staging buffer i % 2 (rows k < nin only)
-  auto issue = [&](int i) {
-    const int tile = (int)blockIdx.x + (i / nkc) * (int)gridDim.x, k0 = (i % nkc) * kTcKC;
-    const long long c0 = (long long)tile * 128;
-    const int ncol = (int)min(128LL, ncr - c0);
-    const int k1 = min(min(k0 + kTcKC, KP), nin);
-    const unsigned row_bytes = (unsigned)ncol * sizeof(Ri);
-    const unsigned total = k1 > k0 ? (unsigned)(k1 - k0) * row_bytes : 0u;
-    uint64_t* bar = &sbar[i & 1];
-    if (total == 0) {
-      // no stored rows in this chunk: complete the phase by a plain arrival
-      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-      return;
-    }
-    mbar_arrive_expect_tx(bar, total);
-    Ri* sb = stg + (size_t)(i & 1) * ACH;
-    for (int k = k0; k < k1; ++k) bulk_row(sb + (size_t)(k - k0) * 128, src + (long long)k * srr + c0, row_bytes, bar);
-  };
-  int issued = 0, landed = 0, committed = 0;  // chunks (thread 0's counts)
-  // chunk j's MMAs: the (j / NAB)-th completion of mbar[j % NAB], waited before that barrier is
-  // committed again, so no barrier runs two phases ahead of its waiter
-  if (tid == 0) {
-    if (nchunks > 0) issue(0);
-    if (nchunks > 1) issue(1);
-    issued = min(nchunks, 2);
-  }
-  bool ok = true;
-  for (int i = 0; i < nchunks && ok; ++i) {
-    const int tile = (int)blockIdx.x + (i / nkc) * (int)gridDim.x, kc = i % nkc;
-    const int k0 = kc * kTcKC, kn = min(kTcKC, KP - k0);
-    const long long c0 = (long long)tile * 128;
-    // staging i has landed, and the MMAs of chunk i - NAB have read operand buffer i % NAB
-    if (tid == 0) {
-      if (!tc_mbar_wait(smem_u32(&sbar[i & 1]), (uint32_t)((i >> 1) & 1), kTcPolls)) *flag = 0;
-      else landed = i + 1;
-      if (*flag && i >= NAB &&
-          !tc_mbar_wait(smem_u32(&mbar[i % NAB]), (uint32_t)(((i - NAB) / NAB) & 1), kTcPolls))
-        *flag = 0;
-    }
-    __syncthreads();
-    ok = *flag != 0;
-    if (!ok) break;
-    float* Ah = Abase + (size_t)(i % NAB) * 2 * ACH;
-    float* Al = Ah + ACH;
-    // split: column c0 + (tid % 128), k quads of half tid / 128, 4 k per float4 of the K-major operand
-    {
-      const Ri* sb = stg + (size_t)(i & 1) * ACH;
-      const int cl = tid & 127, half = tid >> 7;
-      const bool cin = c0 + cl < ncr;
-      const int nq = kn >> 2, q0 = half * ((nq + 1) >> 1), q1 = min(nq, q0 + ((nq + 1) >> 1));
-      for (int kq = q0; kq < q1; ++kq) {
-        float v[4];
+  if (warp >= kTcMmaWarp + 1) {
+    // ---- converters: thread (column cl, k half kh) of each chunk, D chunks in registers
+    const int ct = tid - 32 * (kTcMmaWarp + 1);
+    const int cl = ct & 127, kh = ct >> 7;
+    const Ri* src = reinterpret_cast<const Ri*>(ps.src[f]) + (long long)b * a.sb * 2;
+    const long long srr = 2 * a.sr;
+    Ri v[D][16];
+    // chunk i's 16 values of this thread into v[slot]
+#define TC_LOAD(i, slot)                                                                    \
+  do {                                                                                      \
+    const int tile_ = (int)blockIdx.x + ((i) / nkc) * P;                                    \
+    const long long col_ = (long long)tile_ * 128 + cl;                                     \
+    const int k0_ = ((i) % nkc) * kTcKC + kh * 16;                                          \
+    const bool cin_ = col_ < ncr;                                                           \
+    const Ri* p_ = src + (long long)k0_ * srr + col_;                                       \
+    _Pragma("unroll") for (int j = 0; j < 16; ++j) v[slot][j] =                             \
+        (cin_ && k0_ + j < nin) ? p_[(long long)j * srr] : (Ri)0;                           \
+  } while (0)
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const int kk = kq * 4 + e;
-          v[e] = (cin && k0 + kk < nin) ? (float)sb[(size_t)kk * 128 + cl] : 0.0f;
+    for (int d = 0; d < D - 1; ++d)
+      if (d < nchunks) TC_LOAD(d, d);
+    bool ok = true;
+    for (int i0 = 0; i0 < nchunks && ok; i0 += D) {
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        const int i = i0 + d;
+        if (i < nchunks && ok) {
+          if (i + D - 1 < nchunks) TC_LOAD(i + D - 1, (d + D - 1) % D);
+          if (kTcPrefetch > 0 && ct < 32 && i + D - 1 + kTcPrefetch < nchunks) {
+            // lane j: row j of that chunk, its 128 columns (four 128-byte lines at most)
+            const int ip = i + D - 1 + kTcPrefetch;
+            const int tile_p = (int)blockIdx.x + (ip / nkc) * P;
+            const int kp = (ip % nkc) * kTcKC + ct;
+            const long long c0p = (long long)tile_p * 128;
+            if (kp < nin && c0p < ncr) {
+              const char* rp = reinterpret_cast<const char*>(src + (long long)kp * srr + c0p);
+              const long long nb = min(128LL, ncr - c0p) * (long long)sizeof(Ri);
+              for (long long o = 0; o < nb; o += 128) asm volatile("prefetch.global.L2 [%0];" ::"l"(rp + o));
+              asm volatile("prefetch.global.L2 [%0];" ::"l"(rp + nb - 1));
+            }
+          }
+          const int s = i % NA;
+          // the whole warp takes one decision (the split ends in warp-wide steps)
+          const bool free_slot =
+              __all_sync(0xffffffffu, i < NA || tc_wait(smem_u32(&op_empty[s]), (uint32_t)(((i / NA) - 1) & 1),
+                                                         abort_flag, wflag));
+          if (!free_slot) {
+            ok = false;
+          } else {
+            float* Ah = Abase + (size_t)s * 2 * ACH;
+            float* Al = Ah + ACH;
+            const int kq0 = (i % nkc) * kTcKC + kh * 16;  // first k of this thread's 16
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              if (kq0 + 4 * q < KP) {
+                const int o = tc_off(cl, kh * 16 + 4 * q, kTcKC);
+                float4 h, l;
+                const float x0 = (float)v[d][4 * q], x1 = (float)v[d][4 * q + 1];
+                const float x2 = (float)v[d][4 * q + 2], x3 = (float)v[d][4 * q + 3];
+                h.x = tf32_hi(x0);
+                h.y = tf32_hi(x1);
+                h.z = tf32_hi(x2);
+                h.w = tf32_hi(x3);
+                l.x = x0 - h.x;
+                l.y = x1 - h.y;
+                l.z = x2 - h.z;
+                l.w = x3 - h.w;
+                *reinterpret_cast<float4*>(Ah + o) = h;
+                *reinterpret_cast<float4*>(Al + o) = l;
+              }
+            }
+            // each thread's writes reach the tensor cores' (async) proxy before its arrival
+            proxy_fence();
+            tc_arrive(smem_u32(&op_full[s]));
+          }
         }
-        const int o = tc_off(cl, kq * 4, kTcKC);
-        float4 h, l;
-        h.x = tf32_hi(v[0]);
-        h.y = tf32_hi(v[1]);
-        h.z = tf32_hi(v[2]);
-        h.w = tf32_hi(v[3]);
-        l.x = v[0] - h.x;
-        l.y = v[1] - h.y;
-        l.z = v[2] - h.z;
-        l.w = v[3] - h.w;
-        *reinterpret_cast<float4*>(Ah + o) = h;
-        *reinterpret_cast<float4*>(Al + o) = l;
       }
     }
-    proxy_fence();
-    __syncthreads();
-    if (tid == 0) {
-      // staging buffer i % 2 is free again: chunk i + 2 goes there
-      if (i + 2 < nchunks) {
-        issue(i + 2);
-        issued = i + 3;
+#undef TC_LOAD
+  } else if (warp == kTcMmaWarp) {
+    // ---- the MMA thread
+    if (lane == 0) {
+      const uint32_t idesc = tc_idesc(NP);
+      const uint32_t bh = smem_u32(Bh), bl = smem_u32(Bl);
+      const uint32_t sbo_b = (uint32_t)KP * 32, sbo_a = kTcKC * 32;  // bytes between 8-row groups
+      int i = 0;
+      bool ok = true;
+      for (int lt = 0; lt < my_tiles && ok; ++lt) {
+        const int acc = lt & 1;
+        if (lt >= 2 && !tc_wait(smem_u32(&acc_empty[acc]), (uint32_t)(((lt >> 1) - 1) & 1), abort_flag, wflag)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t dt = tmem + (uint32_t)(acc * TC);
+        for (int kc = 0; kc < nkc; ++kc, ++i) {
+          const int s = i % NA;
+          if (!tc_wait(smem_u32(&op_full[s]), (uint32_t)((i / NA) & 1), abort_flag, wflag)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const int k0 = kc * kTcKC, kn = min(kTcKC, KP - k0);
+          const uint32_t ah = smem_u32(Abase + (size_t)s * 2 * ACH), al = ah + (uint32_t)(ACH * sizeof(float));
+          for (int sg = 0; sg < (kn >> 3); ++sg) {
+            const int kg = (k0 >> 3) + sg;  // k group of 8 of B
+            // two k chunks of 4 per MMA: start at chunk 2 sg (A) / 2 kg (B), 128 bytes each
+            const uint64_t dah = tc_desc(ah + (uint32_t)sg * 256, 128, sbo_a);
+            const uint64_t dal = tc_desc(al + (uint32_t)sg * 256, 128, sbo_a);
+            const uint64_t dbh = tc_desc(bh + (uint32_t)kg * 256, 128, sbo_b);
+            const uint64_t dbl = tc_desc(bl + (uint32_t)kg * 256, 128, sbo_b);
+            tc_mma(dt, dal, dbh, idesc, (kc == 0 && sg == 0) ? 0 : 1);
+            tc_mma(dt, dah, dbl, idesc, 1);
+            tc_mma(dt, dah, dbh, idesc, 1);
+          }
+          tc_commit(smem_u32(&op_empty[s]));
+        }
+        if (ok) tc_commit(smem_u32(&acc_full[acc]));
       }
-      tc_fence_after();
-      const uint32_t ah = smem_u32(Ah), al = smem_u32(Al);
-      for (int s = 0; s < (kn >> 3); ++s) {
-        const int kg = (k0 >> 3) + s;  // k group of 8 of B
-        // two k chunks of 4 per MMA: start at chunk 2 s (A) / 2 kg (B), 128 bytes each
-        const uint64_t dah = tc_desc(ah + (uint32_t)s * 256, 128, sbo_a);
-        const uint64_t dal = tc_desc(al + (uint32_t)s * 256, 128, sbo_a);
-        const uint64_t dbh = tc_desc(bh + (uint32_t)kg * 256, 128, sbo_b);
-        const uint64_t dbl = tc_desc(bl + (uint32_t)kg * 256, 128, sbo_b);
-        const int first = (kc == 0 && s == 0) ? 0 : 1;
-        tc_mma(tmem, dal, dbh, idesc, first);
-        tc_mma(tmem, dah, dbl, idesc, 1);
-        tc_mma(tmem, dah, dbh, idesc, 1);
-      }
-      tc_commit(smem_u32(&mbar[i % NAB]));
-      committed = i + 1;
+      // every MMA issued has completed before the block goes on to free the tensor memory
+      tc_commit(smem_u32(done_bar));
+      tc_mbar_wait(smem_u32(done_bar), 0, kTcPolls);
     }
-    if (kc == nkc - 1) {
-      // the tile's last chunk: its MMAs done, the accumulator out
-      if (tid == 0 && !tc_mbar_wait(smem_u32(&mbar[i % NAB]), (uint32_t)((i / NAB) & 1), kTcPolls)) *flag = 0;
-      __syncthreads();
-      ok = *flag != 0;
-      if (!ok) break;
+    __syncwarp();
+  } else {
+    // ---- epilogue: warp w reads lanes 32 w .. 32 w + 31 (columns c0 + 32 w + lane)
+    float* dst = reinterpret_cast<float*>(ps.dst[f]) + (long long)b * a.db * 2;
+    const long long drr = 2 * a.dr;
+    const float sc = (float)a.scale;
+    for (int lt = 0; lt < my_tiles; ++lt) {
+      const int acc = lt & 1;
+      // one decision per warp: tcgen05.ld is warp-wide
+      if (!__all_sync(0xffffffffu, tc_wait(smem_u32(&acc_full[acc]), (uint32_t)((lt >> 1) & 1), abort_flag, wflag)))
+        break;
       tc_fence_after();
-      const long long col = c0 + (warp & 3) * 32 + (tid & 31);
-      const uint32_t trow = tmem + ((uint32_t)((warp & 3) * 32) << 16);
-      for (int j0 = (warp >> 2) * 16; j0 < NP; j0 += 32) {
-        float v[16];
-        tc_ld16(trow + (uint32_t)j0, v);
+      const int tile = (int)blockIdx.x + lt * P;
+      const long long col = (long long)tile * 128 + warp * 32 + lane;
+      const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(acc * TC);
+      for (int j0 = 0; j0 < NP; j0 += 16) {
+        float w[16];
+        tc_ld16(trow + (uint32_t)j0, w);
+        if (col < ncr) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int m = j0 + j;
-          if (m < nrows && col < ncr) dst[(long long)m * drr + col] = sc * v[j];
+          for (int j = 0; j < 16; ++j)
+            if (j0 + j < nrows) dst[(long long)(j0 + j) * drr + col] = sc * w[j];
         }
       }
       tc_fence_before();
-      __syncthreads();
-      // the wait at the top of chunk i + 1 for this chunk's MMAs passes at once: phase i done
+      tc_arrive(smem_u32(&acc_empty[acc]));
     }
   }
-  if (!ok) {
-    if (tid == 0) {
-      if (a.wait_flag) atomicExch(a.wait_flag, 1);
-      // let the committed MMAs and the issued copies finish before the block's memory goes away
-      for (int j = max(0, committed - NAB); j < committed; ++j)
-        tc_mbar_wait(smem_u32(&mbar[j % NAB]), (uint32_t)((j / NAB) & 1), kTcPolls);
-      for (int j = landed; j < issued; ++j) tc_mbar_wait(smem_u32(&sbar[j & 1]), (uint32_t)((j >> 1) & 1), kTcPolls);
-    }
-    __syncthreads();
-  }
+  tc_fence_before();
+  __syncthreads();
   tc_fence_after();
-  if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(t.tmem_cols) : "memory");
+  if (warp == kTcMmaWarp)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TC) : "memory");
 }
 
 }  // namespace tg

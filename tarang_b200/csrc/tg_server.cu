@@ -57,8 +57,6 @@ struct Batch {
   double step_ms = 0;                // measured time of one step at the current active count
   int step_ms_nact = 0;
   double idle_since = -1;            // server clock when the batch last became empty
-  int sat_out = 0;                   // consecutive rounds the batch sat out (kLagShare)
-  bool run_now = false;              // this round's decision
 };
 
 // Page-locked host blocks, reused by size: initial fields on their way to the device and
@@ -109,6 +107,9 @@ struct tg_server {
   size_t bytes = 0, bytes_peak = 0;
   long long rounds = 0, request_steps = 0, graph_launches = 0, eager_steps = 0;
   std::string err;
+  bool round_open = false;                                // between pump_begin and pump_end
+  cudaEvent_t chain = nullptr;                            // end of the last batch launched
+  std::map<long long, std::pair<int, int>> launched;      // batch -> (slots stepped, launch code)
 };
 
 namespace {
@@ -380,29 +381,34 @@ int launch_batch(tg_server* s, Batch& b, int k) {
     if (cudaEventCreate(&b.ev0) != cudaSuccess || cudaEventCreate(&b.ev1) != cudaSuccess)
       return cuda_err(c, cudaGetLastError(), "cudaEventCreate");
   }
+  // the graph of this active count first, so that a capture stays outside the timed steps
+  cudaGraphExec_t ex = nullptr;
+  if (s->cfg.use_graphs && b.warmed) {
+    auto it = b.graphs.find(nact);
+    if (it == b.graphs.end()) {
+      cudaGraph_t gr = nullptr;
+      e = cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal);
+      if (e != cudaSuccess) return cuda_err(c, e, "cudaStreamBeginCapture");
+      int rc = enqueue_step(c, false);
+      cudaError_t e2 = cudaStreamEndCapture(c->st, &gr);
+      if (rc) {
+        if (gr) cudaGraphDestroy(gr);
+        return rc;
+      }
+      if (e2 != cudaSuccess) return cuda_err(c, e2, "cudaStreamEndCapture");
+      cudaGraphExec_t g = nullptr;
+      e = cudaGraphInstantiate(&g, gr, 0);
+      cudaGraphDestroy(gr);
+      if (e != cudaSuccess) return cuda_err(c, e, "cudaGraphInstantiate");
+      it = b.graphs.emplace(nact, g).first;
+    }
+    ex = it->second;
+  }
   e = cudaEventRecord(b.ev0, c->st);
   if (e != cudaSuccess) return cuda_err(c, e, "cudaEventRecord");
   for (int step = 0; step < k; ++step) {
-    if (s->cfg.use_graphs && b.warmed) {
-      auto it = b.graphs.find(nact);
-      if (it == b.graphs.end()) {
-        cudaGraph_t gr = nullptr;
-        e = cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal);
-        if (e != cudaSuccess) return cuda_err(c, e, "cudaStreamBeginCapture");
-        int rc = enqueue_step(c, false);
-        cudaError_t e2 = cudaStreamEndCapture(c->st, &gr);
-        if (rc) {
-          if (gr) cudaGraphDestroy(gr);
-          return rc;
-        }
-        if (e2 != cudaSuccess) return cuda_err(c, e2, "cudaStreamEndCapture");
-        cudaGraphExec_t ex = nullptr;
-        e = cudaGraphInstantiate(&ex, gr, 0);
-        cudaGraphDestroy(gr);
-        if (e != cudaSuccess) return cuda_err(c, e, "cudaGraphInstantiate");
-        it = b.graphs.emplace(nact, ex).first;
-      }
-      e = cudaGraphLaunch(it->second, c->st);
+    if (ex) {
+      e = cudaGraphLaunch(ex, c->st);
       if (e != cudaSuccess) return cuda_err(c, e, "cudaGraphLaunch");
       s->graph_launches++;
     } else {
@@ -426,26 +432,6 @@ int launch_batch(tg_server* s, Batch& b, int k) {
 // in that time (at most kMaxStepsPerRound), never past the fewest steps any of its requests
 // still needs.  Until a batch has a measured step time it runs one.
 constexpr int kMaxStepsPerRound = 16;
-
-// Device time a batch still needs: its longest request's remaining steps x its measured step time
-// (negative until the batch has a timing)
-double remaining_ms(const tg_server* s, const Batch& b) {
-  if (!(b.step_ms > 0)) return -1.0;
-  int rem = 0;
-  for (long long id : b.slot_req) {
-    const Req& q = s->reqs.at(id);
-    rem = std::max(rem, q.n_steps - q.st.steps_done);
-  }
-  return rem * b.step_ms;
-}
-
-// A timed batch whose remaining device time is below this share of the largest one sits the round
-// out, so the batches that lag (late arrivals, large shapes) get the device and all of them head
-// for the same finishing time; that is the least possible makespan for the work resident.  A
-// batch that sat out kMaxSitOut rounds in a row runs anyway (no starvation under a steady stream
-// of long requests).
-constexpr double kLagShare = 0.5;
-constexpr int kMaxSitOut = 8;
 
 int steps_this_round(const tg_server* s, const Batch& b, double slowest_ms) {
   int left = 1 << 30;
@@ -549,7 +535,9 @@ int tg_server_create(const tg_server_config* cfg, tg_server** out) {
 int tg_server_destroy(tg_server* s) {
   if (!s) return TG_ERR_ARG;
   cudaSetDevice(s->dev);
+  if (s->round_open) tg_server_pump_end(s, nullptr);
   for (auto& kv : s->batches) destroy_batch(s, kv.second);
+  if (s->chain) cudaEventDestroy(s->chain);
   for (auto& kv : s->reqs)
     if (kv.second.result) cudaFreeHost(kv.second.result);
   for (auto& kv : s->reqs)
@@ -599,33 +587,50 @@ int tg_server_submit(tg_server* s, const tg_request* rq, long long* id) {
   return TG_OK;
 }
 
-int tg_server_pump(tg_server* s, int* n_active) {
+// The round's launches: the steps of every running batch go to the device first, so that the
+// host work that follows (submissions between pump_begin and pump_end, then admission: copies
+// into pinned blocks, new contexts) overlaps them.  The batches run one after another on the
+// device (each batch's stream waits for the previous batch's steps): a batch of requests
+// saturates the device alone, and batches overlapping on their streams measured slower in sum
+// (L2 shared by unrelated working sets) than the same batches in sequence.  Each batch's step
+// time (events on its stream, after the wait) is then its own, which steps_this_round needs.
+int tg_server_pump_begin(tg_server* s) {
   if (!s) return TG_ERR_ARG;
+  if (s->round_open) return TG_ERR_STATE;
   cudaSetDevice(s->dev);
-  // launch a step of every resident batch first, so that the host work of admission (copies
-  // into pinned blocks, new contexts) overlaps the steps on the device
-  std::map<long long, std::pair<int, int>> launched;  // batch -> (slots stepped, launch code)
-  double most = 0;
-  for (auto& kv : s->batches)
-    if (!kv.second.slot_req.empty()) most = std::max(most, remaining_ms(s, kv.second));
-  for (auto& kv : s->batches) {
-    Batch& b = kv.second;
-    b.run_now = false;
-    if (b.slot_req.empty()) continue;
-    const double r = remaining_ms(s, b);
-    b.run_now = r < 0 || !s->cfg.use_graphs || r >= kLagShare * most || b.sat_out >= kMaxSitOut;
-    b.sat_out = b.run_now ? 0 : b.sat_out + 1;
+  auto& launched = s->launched;
+  launched.clear();
+  if (!s->chain && cudaEventCreateWithFlags(&s->chain, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    s->chain = nullptr;
+    return TG_ERR_CUDA;
   }
   double slowest = 0;
   for (auto& kv : s->batches)
-    if (kv.second.run_now) slowest = std::max(slowest, kv.second.step_ms);
+    if (!kv.second.slot_req.empty()) slowest = std::max(slowest, kv.second.step_ms);
+  // (the chain orders independent work only: where a wait or record fails the batches overlap)
+  bool chained = false;
   for (auto& kv : s->batches) {
     Batch& b = kv.second;
-    if (!b.run_now) continue;
+    if (b.slot_req.empty()) continue;
+    if (chained && cudaStreamWaitEvent(b.c->st, s->chain, 0) != cudaSuccess) cudaGetLastError();
     const int nl = (int)b.slot_req.size();
     const int k = s->cfg.use_graphs ? steps_this_round(s, b, slowest) : 1;
     launched[kv.first] = {nl, launch_batch(s, b, k)};
+    chained = cudaEventRecord(s->chain, b.c->st) == cudaSuccess;
+    if (!chained) cudaGetLastError();
   }
+  s->round_open = true;
+  return TG_OK;
+}
+
+// admission, then the wait for the round's steps and the retirement of finished requests
+int tg_server_pump_end(tg_server* s, int* n_active) {
+  if (!s) return TG_ERR_ARG;
+  cudaSetDevice(s->dev);
+  if (!s->round_open) s->launched.clear();  // a round without launches: admission only
+  s->round_open = false;
+  const auto& launched = s->launched;
   int first_err = admit(s);
   for (auto& kv : s->batches) {
     Batch& b = kv.second;
@@ -651,6 +656,7 @@ int tg_server_pump(tg_server* s, int* n_active) {
       ++it;
     }
   }
+  s->launched.clear();
   if (n_active) {
     int n = (int)s->queue.size();
     for (auto& kv : s->batches) n += (int)kv.second.slot_req.size();
@@ -659,9 +665,20 @@ int tg_server_pump(tg_server* s, int* n_active) {
   return first_err;
 }
 
+int tg_server_pump(tg_server* s, int* n_active) {
+  const int rc = tg_server_pump_begin(s);
+  if (rc) return rc;
+  return tg_server_pump_end(s, n_active);
+}
+
 int tg_server_drain(tg_server* s, long long max_rounds) {
   if (!s) return TG_ERR_ARG;
   int first_err = TG_OK;
+  if (s->round_open) {
+    int n = 0;
+    first_err = tg_server_pump_end(s, &n);
+    if (n == 0) return first_err;
+  }
   for (long long i = 0; max_rounds <= 0 || i < max_rounds; ++i) {
     int n = 0;
     const int rc = tg_server_pump(s, &n);

@@ -113,6 +113,21 @@ class Server:
             raise L.TarangError(rc, "tg_server_pump")
         return n.value
 
+    def pump_begin(self):
+        """Launch one round's steps and return at once; submissions made before pump_end
+        overlap the round on the device."""
+        rc = self.lib.tg_server_pump_begin(self.h)
+        if rc != L.TG_OK:
+            raise L.TarangError(rc, "tg_server_pump_begin")
+
+    def pump_end(self) -> int:
+        """Admit, wait for the round opened by pump_begin, retire; requests running or queued."""
+        n = C.c_int()
+        rc = self.lib.tg_server_pump_end(self.h, C.byref(n))
+        if rc != L.TG_OK:
+            raise L.TarangError(rc, "tg_server_pump_end")
+        return n.value
+
     def drain(self, max_rounds: int = 0):
         rc = self.lib.tg_server_drain(self.h, int(max_rounds))
         if rc != L.TG_OK:

@@ -154,6 +154,9 @@ TCASES = [
     ("scft_fluid_fp32", (24, 16, 32), dict(basis="SCFT", nu=2e-3, dt=1e-3, kfactor=KF_RB, precision="FP32")),
     ("scft_fluid_full32", (24, 16, 32), dict(basis="SCFT", nu=2e-3, dt=1e-3, kfactor=KF_RB, dealias=False,
                                              precision="FP32")),
+    # several tiles per block: both accumulators, the operand ring and the register ring wrap
+    ("rb65x128_fp32", (65, 128, 128), dict(basis="SCFT", physics="RB", Ra=1e4, Pr=1.0, kfactor=KF_RB, dt=1e-4,
+                                           precision="FP32")),
 ]
 
 
@@ -161,3 +164,45 @@ def test_tensor_core_x_pass_matches_register_tiled(lib):
     """FP32 forms: the SCFT x-pass on the tensor cores (3xTF32 tcgen05, TG_R2R_TC=1) against the
     register-tiled FP32 matrix product (TG_R2R_TC=0), to FP32-mixed rounding."""
     compare(run("1", TCASES, "TG_R2R_TC"), run("0", TCASES, "TG_R2R_TC"), TCASES)
+
+
+SERVE_SCRIPT = r"""
+import json, sys
+import numpy as np
+sys.path.insert(0, %r)
+from tarang_b200 import ic
+from tarang_b200.serving import Server
+from tarang_b200.solver import IncFluid
+KF = (3.141592653589793, 2.221441469079183, 2.221441469079183)
+N = (33, 32, 64)
+out = {}
+reqs = []
+for j in range(3):
+    cfg = dict(N=N, basis="SCFT", physics="RB", Ra=1e4 * (1 + j), Pr=1.0, kfactor=KF, dt=1e-4, precision="FP32")
+    f = np.stack(ic.random_phase_field(N, seed=40 + j) + [ic.random_phase_field(N, seed=50 + j)[0]])
+    reqs.append((cfg, f, 3 + j))
+same = []
+with Server(hbm_budget=8e9, max_batch=4) as srv:
+    ids = [srv.submit(c, f, k) for c, f, k in reqs]
+    srv.drain()
+    for rid, (c, f, k) in zip(ids, reqs):
+        c = dict(c)
+        s = IncFluid(c.pop("N"), **c)
+        s.set_V(list(f[:3]))
+        s.set_T(f[3])
+        s.step(k)
+        want = s.get_V() + [s.get_T()]
+        s.close()
+        got = srv.result(rid)
+        same.append(all(np.array_equal(a.view(np.float64), b.view(np.float64)) for a, b in zip(got, want)))
+print(json.dumps(same))
+""" % ROOT
+
+
+def test_tensor_core_x_pass_batched_equals_lone(lib):
+    """With the tensor-core x-pass forced on (TG_R2R_TC=1), requests served in one batch equal
+    their lone-context runs bit for bit (a tile's result does not depend on the launch shape)."""
+    env = dict(os.environ, TG_R2R_TC="1")
+    r = subprocess.run([sys.executable, "-c", SERVE_SCRIPT], capture_output=True, text=True, env=env, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert json.loads(r.stdout.strip().splitlines()[-1]) == [True, True, True]

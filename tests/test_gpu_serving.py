@@ -137,6 +137,34 @@ def test_late_arrivals_join_running_batch(lib):
             assert same_bits(srv.result(rid), want)
 
 
+def test_split_pump_submits_during_round(lib):
+    """pump_begin / submit / pump_end: requests submitted while a round runs on the device are
+    admitted at its end and join the running batch; a second pump_begin on an open round is
+    TG_ERR_STATE; drain closes an open round; every result equals its lone run."""
+    from tarang_b200.serving import Server
+    N = (32, 32, 32)
+    reqs = [(dict(N=N, nu=1e-3 * (1 + j), dt=1e-3), fluid_fields(N, 800 + j), 3 + 2 * (j % 3)) for j in range(6)]
+    with Server(hbm_budget=8e9, max_batch=4) as srv:
+        ids = [srv.submit(*reqs[0])]
+        srv.pump()
+        for j in range(1, len(reqs)):
+            srv.pump_begin()
+            if j == 1:
+                with pytest.raises(L.TarangError) as e:
+                    srv.pump_begin()
+                assert e.value.code == L.TG_ERR_STATE
+            ids.append(srv.submit(*reqs[j]))
+            assert srv.poll(ids[-1])["state"] == "queued"
+            srv.pump_end()
+            assert srv.poll(ids[-1])["state"] in ("running", "done")
+        srv.pump_begin()
+        srv.drain()
+        assert srv.pump_end() == 0          # admission-only round on an empty server
+        for rid, (c, f, k) in zip(ids, reqs):
+            want, _, _ = lone(c, f, k)
+            assert same_bits(srv.result(rid), want)
+
+
 def test_budget_admission(lib):
     from tarang_b200.serving import Server, request_bytes
     cfg = dict(N=(32, 32, 32), nu=2e-3, dt=1e-3)
