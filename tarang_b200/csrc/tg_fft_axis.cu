@@ -29,13 +29,17 @@ struct TmaSet {
   CUtensorMap dst[kMaxPtr];
 };
 
-// One block: W = 256/R1 columns of one batch of one field.  Tile rows in shared memory are
+// One block: W columns (TmaW) of one batch of one field.  Tile rows in shared memory are
 // row-major [row][W]; the same buffer holds the loaded input tile, then the transposed
 // intermediate, then the output tile.
 // Tile width of the TMA axis kernel: 8 columns (64 or 128 contiguous bytes per row), so the
 // solver's column counts (kzp, a multiple of 8, and nky * kzp) split into whole tiles; the block
-// has W * R1 threads (128 at L = 256).
-constexpr int kTmaW = 8;
+// has W * R1 threads (128 at L = 256).  (16-column FP32 tiles, 128-byte row segments at 256
+// threads a block, measured no faster: 256^3 FP32-mixed step 1.85 ms against 1.81 ms.)
+template <typename Rw>
+struct TmaW {
+  static constexpr int v = 8;
+};
 // resident blocks per SM the kernel is built for: 64 registers (FP32 arithmetic) or 80 (FP64)
 template <typename Rw, int NT>
 struct AxisOcc {
@@ -43,10 +47,10 @@ struct AxisOcc {
 };
 
 template <typename Ri, typename Ro, typename Rw, int R1, int R2, int DIR, bool COMB>
-__global__ void __launch_bounds__(kTmaW * R1, AxisOcc<Rw, kTmaW * R1>::v)
+__global__ void __launch_bounds__(TmaW<Rw>::v * R1, AxisOcc<Rw, TmaW<Rw>::v * R1>::v)
     k_axis_tma(AxisArgs a, const __grid_constant__ TmaSet tm, int nin_rows, int nout_rows, unsigned tile_bytes) {
   constexpr int L = R1 * R2;
-  constexpr int W = kTmaW;
+  constexpr int W = TmaW<Rw>::v;
   constexpr int NT = W * R1;
   constexpr int CEi = (int)(sizeof(cx<Ri>) / 8), CEo = (int)(sizeof(cx<Ro>) / 8);
   extern __shared__ unsigned char smem_raw[];
@@ -147,7 +151,7 @@ template <typename Ri, typename Ro, typename Rw, int R1, int R2, int DIR>
 cudaError_t run_axis_tma(const AxisLaunch& l, cudaStream_t s, bool* used) {
   *used = false;
   constexpr int L = R1 * R2;
-  constexpr int W = kTmaW;
+  constexpr int W = TmaW<Rw>::v;
   constexpr int NT = W * R1;
   constexpr int CEi = (int)(sizeof(cx<Ri>) / 8), CEo = (int)(sizeof(cx<Ro>) / 8);
   const int nin_rows = amap_count(l.a.in), nout_rows = amap_count(l.a.out);
@@ -326,12 +330,12 @@ cudaError_t run_r2r_gemm(const AxisLaunch& l, const R2RArgs& r, cudaStream_t s, 
 }
 
 // FP32 forms: the x-pass contraction on the tensor cores (k_axis_r2r_tc, 3xTF32) when a field of
-// one request spans at least kTcMinTiles column tiles (the per-block set-up and the pipeline fill
-// amortise; measured: 352 tiles, the 129 x 256 x 256 convection step, 2.42 ms against 2.89 ms; 64
-// tiles, 65 x 128 x 128, 0.43 ms against 0.39 ms).  The rule looks at one request's geometry only,
-// so a request batched in the serving loop takes the same path as on a lone context.
-// TG_R2R_TC=0 never, =1 always.
-constexpr int kTcMinTiles = 128;
+// one request spans at least kTcMinTiles column tiles (the per-block set-up, coefficient pairs and
+// tensor memory, amortises; measured FP32-mixed steps against the register-tiled form: 129 x 256
+// x 256 1.89 against 2.92 ms, 65 x 128 x 128 0.342 against 0.397 ms).  The rule looks at one
+// request's geometry only, so a request batched in the serving loop takes the same path as on a
+// lone context.  TG_R2R_TC=0 never, =1 always.
+constexpr int kTcMinTiles = 16;
 int r2r_tc_mode() {
   static const int m = [] {
     const char* e = std::getenv("TG_R2R_TC");
