@@ -316,8 +316,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_axis_r2r_tc(AxisArgs a, PtrSe
     // ---- the MMA thread
     if (lane == 0) {
       const uint32_t idesc = tc_idesc(NP);
-      const uint32_t bh = smem_u32(Bh), bl = smem_u32(Bl);
       const uint32_t sbo_b = (uint32_t)KP * 32, sbo_a = kTcKC * 32;  // bytes between 8-row groups
+      // descriptors of k group 0; a step of 256 bytes (8 k) adds 16 to the start-address field
+      // (address / 16, 14 bits: shared-memory addresses stay below 256 KB, so no carry)
+      const uint64_t dbh0 = tc_desc(smem_u32(Bh), 128, sbo_b), dbl0 = tc_desc(smem_u32(Bl), 128, sbo_b);
+      const uint64_t da0 = tc_desc(smem_u32(Abase), 128, sbo_a);
+      constexpr uint64_t kSlotStep = (uint64_t)(2 * ACH * sizeof(float)) >> 4, kLoStep = (uint64_t)(ACH * sizeof(float)) >> 4;
       int i = 0;
       bool ok = true;
       for (int lt = 0; lt < my_tiles && ok; ++lt) {
@@ -336,14 +340,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_axis_r2r_tc(AxisArgs a, PtrSe
           }
           tc_fence_after();
           const int k0 = kc * kTcKC, kn = min(kTcKC, KP - k0);
-          const uint32_t ah = smem_u32(Abase + (size_t)s * 2 * ACH), al = ah + (uint32_t)(ACH * sizeof(float));
+          const uint64_t dah0 = da0 + (uint64_t)s * kSlotStep;
           for (int sg = 0; sg < (kn >> 3); ++sg) {
             const int kg = (k0 >> 3) + sg;  // k group of 8 of B
             // two k chunks of 4 per MMA: start at chunk 2 sg (A) / 2 kg (B), 128 bytes each
-            const uint64_t dah = tc_desc(ah + (uint32_t)sg * 256, 128, sbo_a);
-            const uint64_t dal = tc_desc(al + (uint32_t)sg * 256, 128, sbo_a);
-            const uint64_t dbh = tc_desc(bh + (uint32_t)kg * 256, 128, sbo_b);
-            const uint64_t dbl = tc_desc(bl + (uint32_t)kg * 256, 128, sbo_b);
+            const uint64_t dah = dah0 + (uint64_t)sg * 16, dal = dah + kLoStep;
+            const uint64_t dbh = dbh0 + (uint64_t)kg * 16, dbl = dbl0 + (uint64_t)kg * 16;
             tc_mma(dt, dal, dbh, idesc, (kc == 0 && sg == 0) ? 0 : 1);
             tc_mma(dt, dah, dbl, idesc, 1);
             tc_mma(dt, dah, dbh, idesc, 1);
