@@ -11,6 +11,11 @@ this image, so the oracle restates its algorithms and is pinned by
     (``trunk/test/test-fftw/out1.d``: an unnormalised C2R->R2C round trip of a
     unit delta at (0,0,2) on a 4^3 grid returns 64 = N^3,
     produced by ``trunk/test/test-fftw/main_mpi.cc:93-118``), and
+  * the reference's own inline wavenumber code (``lib/four/four_inline.h``,
+    ``lib/scft/scft_inline.h``) compiled from the reference tree with
+    declaration-only stand-ins for the MPI, FFTW and blitz++ headers
+    (``oracle/ref_pin``): wavenumbers, |K|, multiplicity factors, radii and
+    anisotropic extents, stored as ``tests/golden/ref_inline.json``, and
   * analytic known answers (single modes, Taylor-Green, Beltrami flow,
     exact viscous decay, energy conservation of the inviscid nonlinear term,
     antisymmetry of the shell-to-shell transfer),
