@@ -52,7 +52,10 @@ extern "C" {
 /* arithmetic form */
 #define TG_FP64 0
 #define TG_FP32_MIXED 1 /* FP32 transforms and products, FP64 RK state/projection/reductions */
-/* integ_scheme */
+/* integ_scheme (IncFluid::Time_advance time_advance.cc:60-163): integrating-factor Euler, the
+ * integrating-factor midpoint rule and the integrating-factor RK4 (Lawson) */
+#define TG_EULER 1
+#define TG_RK2 2
 #define TG_RK4 4
 /* force_field_proc (compute_force_main.cc:43-124) */
 #define TG_FORCE_DECAY 0
@@ -119,7 +122,7 @@ typedef struct tg_config {
   int physics;        /* TG_FLUID / TG_MHD / TG_SCALAR / TG_RB */
   int precision;      /* TG_FP64 / TG_FP32_MIXED */
   int dealias;        /* 1: alias_switch "DEALIAS" (2/3 rule), 0: "ALIAS" */
-  int scheme;         /* TG_RK4 */
+  int scheme;         /* TG_EULER / TG_RK2 / TG_RK4 */
   double kfactor[3];  /* 2 pi / L per axis (Ifluid_main.cc:159-161) */
   double nu;          /* dissipation_coefficient of U */
   double eta;         /* dissipation_coefficient of B (MHD) */
@@ -137,6 +140,11 @@ typedef struct tg_config {
   int rb_pr_switch;
   int rb_u_scaling;
   double rb_temp_grad;
+  /* hyper_dissipation_coefficient of U and B, hyper_diffusion_coefficient of T: the viscous
+   * factor exp(-nu K^2 dt) becomes exp(-(nu + nu_h K^2) K^2 dt) (Mult_field_exp_ksqr_dt
+   * mult_exp_visc.cc:56-165, Array_exp_ksqr_FOUR four_basic.cc:377-403); 0: off (the
+   * hyper_dissipation_switch / hyper_diffusion_switch of the reference) */
+  double hyper_nu, hyper_eta, hyper_kappa;
 } tg_config;
 
 typedef struct tg_ctx tg_ctx;

@@ -422,6 +422,51 @@ def exp_ksqr(A, factor, kfactor, basis="FOUR"):
     return A * np.exp(factor * ksqr(N, kfactor, basis))
 
 
+def exp_ksqr_hyper(A, factor, hyper_factor, kfactor, basis="FOUR"):
+    """Array_exp_ksqr_FOUR with the hyper term  four_basic.cc:377-403 (Array_exp_ksqr_SCFT
+    scft_basic.cc:370-395): A *= exp((factor + hyper_factor K^2) K^2)."""
+    if hyper_factor == 0:
+        return exp_ksqr(A, factor, kfactor, basis)
+    N = (A.shape[0], A.shape[1], 2 * (A.shape[2] - 1))
+    K2 = ksqr(N, kfactor, basis)
+    return A * np.exp((factor + hyper_factor * K2) * K2)
+
+
+def if_time_advance(u0, coefs, rhs, dt, scheme, kfactor, basis="FOUR"):
+    """IncFluid::Time_advance  time_advance.cc:60-163 on a list of fields: EULER, RK2 or RK4 with
+    Single_time_step(dt, a, b, c) = E(b)(E(a - b) u + c dt N)  single_time_step.cc:54-86 and
+    E(a) = exp(-(nu + nu_h K^2) a dt K^2) per field (Mult_field_exp_ksqr_dt mult_exp_visc.cc:
+    56-165); coefs[i] = (nu, nu_h); rhs(fields) -> right-hand sides (Compute_rhs)."""
+    n = len(u0)
+
+    def E(A, i, a):
+        nu, nh = coefs[i]
+        return exp_ksqr_hyper(A, -nu * a * dt, -nh * a * dt, kfactor, basis)
+
+    if scheme == "EULER":                       # Single_time_step(dt, 1, 1, 1)
+        r = rhs(u0)
+        return [E(u0[i] + dt * r[i], i, 1.0) for i in range(n)]
+    if scheme == "RK2":
+        r = rhs(u0)                             # Single_time_step(dt, 1/2, 1/2, 1/2)
+        um = [E(u0[i] + (dt / 2) * r[i], i, 0.5) for i in range(n)]
+        r = rhs(um)                             # Single_time_step(dt, 1, 1/2, 1) from u0
+        return [E(E(u0[i], i, 0.5) + dt * r[i], i, 0.5) for i in range(n)]
+    if scheme != "RK4":
+        raise ValueError(scheme)
+    r = rhs(u0)
+    u = [E(u0[i] + (dt / 2) * r[i], i, 0.5) for i in range(n)]
+    tot = [(dt / 6) * E(r[i], i, 1.0) for i in range(n)]
+    r = rhs(u)
+    u = [E(u0[i], i, 0.5) + (dt / 2) * r[i] for i in range(n)]
+    tot = [tot[i] + (dt / 3) * E(r[i], i, 0.5) for i in range(n)]
+    r = rhs(u)
+    u = [E(E(u0[i], i, 0.5) + dt * r[i], i, 0.5) for i in range(n)]
+    tot = [tot[i] + (dt / 3) * E(r[i], i, 0.5) for i in range(n)]
+    r = rhs(u)
+    tot = [tot[i] + (dt / 6) * r[i] for i in range(n)]
+    return [E(u0[i], i, 1.0) + tot[i] for i in range(n)]
+
+
 # --------------------------------------------------------------------------------------
 # Nonlinear terms  (lib/IncFlow/nlin_calc)
 # --------------------------------------------------------------------------------------
@@ -937,7 +982,7 @@ class FluidSolver:
     time_advance.cc:100-155, Single_time_step single_time_step.cc:54-86 and Compute_RK4_parts
     single_time_step.cc:440-444, Compute_force_TO_rhs single_time_step.cc:351-365."""
 
-    def __init__(self, N, kfactor, nu, Tdt, basis="FOUR", alias="DEALIAS", force=None):
+    def __init__(self, N, kfactor, nu, Tdt, basis="FOUR", alias="DEALIAS", force=None, scheme="RK4", nu_h=0.0):
         self.N = tuple(N)
         self.kfactor = tuple(kfactor)
         self.nu = nu
@@ -945,6 +990,8 @@ class FluidSolver:
         self.basis = basis
         self.alias = alias
         self.force = force   # see fluid_force
+        self.scheme = scheme  # integ_scheme EULER / RK2 / RK4
+        self.nu_h = nu_h      # hyper_dissipation_coefficient (0: hyper_dissipation_switch off)
 
     # Compute_force(); Compute_nlin(); Add_force(); Compute_pressure(); Compute_rhs()
     def rhs(self, V):
@@ -963,6 +1010,12 @@ class FluidSolver:
         E0 = sum(total_energy(v, self.basis) for v in V)
         dt = get_dt(E0, self.N, self.kfactor, self.Tdt, self.alias, self.basis)
         u0 = [v.copy() for v in V]
+        if self.scheme != "RK4" or self.nu_h != 0:
+            u = if_time_advance(u0, [(self.nu, self.nu_h)] * 3, lambda f: self.rhs(f)[0], dt, self.scheme,
+                                self.kfactor, self.basis)
+            if self.alias == "DEALIAS":
+                u = [dealias(a, self.basis) for a in u]
+            return u, dt
         # stage 1: Single_time_step(dt, 1/2, 1/2, 1/2): V += dt/2 N; V *= E(1/2)
         r, _ = self.rhs(u0)
         u = [u0[i] + (dt / 2) * r[i] for i in range(3)]
@@ -997,9 +1050,11 @@ class MHDSolver(FluidSolver):
     time_advance_VF_MHD.cc:59-182: the same IF-RK4 with nu for U and eta for B; only U.nlin is
     projected (Compute_pressure uses U's nlin), W.nlin -> -W.nlin (compute_rhs.cc:111-119)."""
 
-    def __init__(self, N, kfactor, nu, eta, Tdt, basis="FOUR", alias="DEALIAS", force=None):
-        super().__init__(N, kfactor, nu, Tdt, basis, alias, force)
+    def __init__(self, N, kfactor, nu, eta, Tdt, basis="FOUR", alias="DEALIAS", force=None, scheme="RK4", nu_h=0.0,
+                 eta_h=0.0):
+        super().__init__(N, kfactor, nu, Tdt, basis, alias, force, scheme, nu_h)
         self.eta = eta
+        self.eta_h = eta_h
 
     def rhs2(self, V, W):
         """Compute_force(W), Compute_nlin(W), Add_force(W) (add_force.cc:58-66): U.nlin -= F,
@@ -1040,6 +1095,15 @@ class MHDSolver(FluidSolver):
         dt = min(dt, self.Tdt)
         u0 = [v.copy() for v in V]
         b0 = [w.copy() for w in W]
+        if self.scheme != "RK4" or self.nu_h != 0 or self.eta_h != 0:
+            f = if_time_advance(u0 + b0, [(self.nu, self.nu_h)] * 3 + [(self.eta, self.eta_h)] * 3,
+                                lambda x: list(sum(self.rhs2(x[:3], x[3:]), [])), dt, self.scheme, self.kfactor,
+                                self.basis)
+            u, b = f[:3], f[3:]
+            if self.alias == "DEALIAS":
+                u = [dealias(a, self.basis) for a in u]
+                b = [dealias(a, self.basis) for a in b]
+            return u, b, dt
         ru, rb = self.rhs2(u0, b0)
         u = self.E([u0[i] + (dt / 2) * ru[i] for i in range(3)], 0.5, dt)
         b = self.Eb([b0[i] + (dt / 2) * rb[i] for i in range(3)], 0.5, dt)
@@ -1092,7 +1156,8 @@ class RBSolver:
     Fields: V = [u1 (sin), u2 (cos), u3 (cos)], T = theta (sin) in the SCFT basis."""
 
     def __init__(self, N, kfactor, Ra, Pr, Tdt, basis="SCFT", alias="DEALIAS", temperature_grad=1.0,
-                 pr_switch="PRLARGE", u_scaling="ULARGE", omega=None):
+                 pr_switch="PRLARGE", u_scaling="ULARGE", omega=None, scheme="RK4", nu_h=0.0, kappa_h=0.0):
+        self.scheme, self.nu_h, self.kappa_h = scheme, nu_h, kappa_h
         self.N = tuple(N)
         self.kfactor = tuple(kfactor)
         self.nu, self.kappa, self.fu, self.ft, self.nuf = rb_coefficients(Ra, Pr, pr_switch, u_scaling,
@@ -1135,6 +1200,17 @@ class RBSolver:
         u0 = [v.copy() for v in V]
         t0 = T.copy()
         nu, ka = self.nu, self.kappa
+        if self.scheme != "RK4" or self.nu_h != 0 or self.kappa_h != 0:
+            def rhs(f):
+                ru, rt = self.rhs(f[:3], f[3])
+                return ru + [rt]
+            f = if_time_advance(u0 + [t0], [(nu, self.nu_h)] * 3 + [(ka, self.kappa_h)], rhs, dt, self.scheme,
+                                self.kfactor, self.basis)
+            u, t = f[:3], f[3]
+            if self.alias == "DEALIAS":
+                u = [dealias(a, self.basis) for a in u]
+                t = dealias(t, self.basis)
+            return u, t, dt
         ru, rt = self.rhs(u0, t0)
         u = self.E([u0[i] + (dt / 2) * ru[i] for i in range(3)], nu, 0.5, dt)
         t = self.E([t0 + (dt / 2) * rt], ka, 0.5, dt)[0]
@@ -1175,7 +1251,9 @@ class ScalarSolver(RBSolver):
     eps, eps_h, eps_T) (procs 1, 2 with the scalar variants compute_force_ek_hk_supply.cc:164-289,
     compute_force_const_ek_hk.cc:167-293)."""
 
-    def __init__(self, N, kfactor, nu, kappa, Tdt, basis="FOUR", alias="DEALIAS", force=None):
+    def __init__(self, N, kfactor, nu, kappa, Tdt, basis="FOUR", alias="DEALIAS", force=None, scheme="RK4",
+                 nu_h=0.0, kappa_h=0.0):
+        self.scheme, self.nu_h, self.kappa_h = scheme, nu_h, kappa_h
         self.N = tuple(N)
         self.kfactor = tuple(kfactor)
         self.nu, self.kappa = nu, kappa

@@ -25,7 +25,7 @@ TG_ERR_BUSY = -8
 TG_FOUR, TG_SCFT = 0, 1
 TG_FLUID, TG_MHD, TG_SCALAR, TG_RB = 0, 1, 2, 3
 TG_FP64, TG_FP32_MIXED = 0, 1
-TG_RK4 = 4
+TG_EULER, TG_RK2, TG_RK4 = 1, 2, 4
 TG_FORCE_DECAY, TG_FORCE_ENERGY_SUPPLY, TG_FORCE_MODES, TG_FORCE_CORIOLIS, TG_FORCE_RB = 0, 1, 5, 21, 51
 TG_FORCE_ENERGY_HELICITY = 2
 TG_FORCE_LIQUID_METAL = 101
@@ -81,6 +81,9 @@ class tg_config(C.Structure):
         ("rb_pr_switch", C.c_int),
         ("rb_u_scaling", C.c_int),
         ("rb_temp_grad", C.c_double),
+        ("hyper_nu", C.c_double),
+        ("hyper_eta", C.c_double),
+        ("hyper_kappa", C.c_double),
     ]
 
 

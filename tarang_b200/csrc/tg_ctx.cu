@@ -196,6 +196,7 @@ RKArgs rk_args(tg_ctx* c, int stage) {
   a.nstate = c->nstate;
   for (int i = 0; i < 6; ++i) {
     a.nu[i] = c->nu_of[i];
+    a.nuh[i] = c->nuh_of[i];
     a.U0[i] = c->U0[i];
     a.TOT[i] = c->TOT[i];
     a.US[i] = c->US[i];
@@ -207,7 +208,7 @@ RKArgs rk_args(tg_ctx* c, int stage) {
   a.fx = c->fx;
   a.fy = c->fy;
   a.fz = c->fz;
-  a.part = (stage == 4) ? c->part : nullptr;
+  a.part = stage_is_final(stage) ? c->part : nullptr;
   a.rb_buoy_u = c->rb_fu;
   a.rb_buoy_t = c->rb_ft;
   a.nact = c->nact;
@@ -277,12 +278,31 @@ int ensure_dt(tg_ctx* c) {
   return TG_OK;
 }
 
-// stages 2..4 (or 1..4) of the RK4 step on the fused path; `ring` records the step's energy
-int run_stages(tg_ctx* c, int first_stage, bool ring) {
-  for (int stage = first_stage; stage <= 4; ++stage) {
+int scheme_stages(int scheme, int out[4]) {
+  if (scheme == TG_EULER) {
+    out[0] = 5;
+    return 1;
+  }
+  if (scheme == TG_RK2) {
+    out[0] = 7;
+    out[1] = 6;
+    return 2;
+  }
+  for (int i = 0; i < 4; ++i) out[i] = i + 1;
+  return 4;
+}
+
+// the stages first..last of the configured scheme's step on the fused path (first = 1: the
+// whole step; 2: after a first stage from precomputed right-hand sides); `ring` records the
+// step's energy
+int run_stages(tg_ctx* c, int first, bool ring) {
+  int st[4];
+  const int ns_stages = scheme_stages(c->cfg.scheme, st);
+  for (int si = first - 1; si < ns_stages; ++si) {
+    const int stage = st[si];
     const void* in[6];
     int inprec;
-    if (stage == 1) {
+    if (si == 0) {
       for (int i = 0; i < c->nstate; ++i) in[i] = c->U0[i];
       inprec = F64;
     } else {
@@ -297,9 +317,12 @@ int run_stages(tg_ctx* c, int first_stage, bool ring) {
     for (int i = 0; i < c->nstate; ++i) a.IN[i] = in[i];
     a.inprec = (inprec == F64) ? 0 : 1;
     {
+      // bytes: products and U0 read; TOT read (RK4 stages 2-4) and written (1-3); the stage
+      // field written (1-3, 7) or U0 (final stages)
       const double ns = c->nstate, e = el_compact(c);
-      const double rd = c->nprod * e * c->tsz + ns * e * 16 + (stage > 1 ? ns * e * 16 : 0);
-      const double wr = (stage < 4) ? ns * e * (c->tsz + 16) : ns * e * 16;
+      const bool tot_rd = stage >= 2 && stage <= 4, tot_wr = stage >= 1 && stage <= 3;
+      const double rd = c->nprod * e * c->tsz + ns * e * 16 + (tot_rd ? ns * e * 16 : 0);
+      const double wr = (stage_is_final(stage) ? ns * e * 16 : ns * e * c->tsz) + (tot_wr ? ns * e * 16 : 0);
       ProfScope pr(c, "rk_stage", rd + wr);
       TG_CK(launch_rk(a, c->phys, c->tprec, c->tprec, 0, c->st, nullptr));
     }
@@ -655,6 +678,7 @@ int ctx_create_batch(const tg_config* cfg, int B, tg_ctx** out, int slab_W, int 
   }
 
   state_viscosities(cfg, c->nu_of);
+  state_hyper(cfg, c->nuh_of);
 
   int rc = TG_OK;
   auto fail = [&](int code) {
@@ -840,7 +864,10 @@ int validate_config(const tg_config* cfg) {
        (cfg->rb_u_scaling != TG_RB_ULARGE && cfg->rb_u_scaling != TG_RB_USMALL) || !std::isfinite(cfg->rb_temp_grad)))
     return TG_ERR_ARG;
   if (cfg->precision != TG_FP64 && cfg->precision != TG_FP32_MIXED) return TG_ERR_ARG;
-  if (cfg->scheme != TG_RK4) return TG_ERR_UNSUPPORTED;
+  if (cfg->scheme != TG_RK4 && cfg->scheme != TG_RK2 && cfg->scheme != TG_EULER) return TG_ERR_UNSUPPORTED;
+  if (!(cfg->hyper_nu >= 0 && cfg->hyper_eta >= 0 && cfg->hyper_kappa >= 0) || !std::isfinite(cfg->hyper_nu) ||
+      !std::isfinite(cfg->hyper_eta) || !std::isfinite(cfg->hyper_kappa))
+    return TG_ERR_ARG;
   if (cfg->force_kind != TG_FORCE_DECAY && cfg->force_kind != TG_FORCE_ENERGY_SUPPLY &&
       cfg->force_kind != TG_FORCE_ENERGY_HELICITY && cfg->force_kind != TG_FORCE_RB &&
       cfg->force_kind != TG_FORCE_LIQUID_METAL &&
@@ -895,6 +922,16 @@ RBCoef rb_coefficients(const tg_config* cfg) {
     r.nuf = small_u ? 2.0 : 2 * std::sqrt(Ra * Pr);
   }
   return r;
+}
+
+void state_hyper(const tg_config* cfg, double nuh[6]) {
+  for (int i = 0; i < 6; ++i) nuh[i] = 0.0;
+  for (int i = 0; i < 3; ++i) nuh[i] = cfg->hyper_nu;
+  if (cfg->physics == TG_MHD) {
+    for (int i = 0; i < 3; ++i) nuh[3 + i] = cfg->hyper_eta;
+  } else if (cfg->physics == TG_SCALAR || cfg->physics == TG_RB) {
+    nuh[3] = cfg->hyper_kappa;
+  }
 }
 
 void state_viscosities(const tg_config* cfg, double nu[6]) {
@@ -1435,11 +1472,18 @@ int tg_time_advance(tg_ctx* c) {
   cudaSetDevice(c->dev);
   int rc = ensure_dt(c);
   if (rc) return rc;
-  // stage 1 from the caller's nlin and pressure (Compute_rhs inside Time_advance)
+  // the scheme's first stage from the caller's nlin and pressure (Compute_rhs inside
+  // Time_advance), then the rest of the step
   TG_CK(launch_rhs_from_nlin(c->g, c->phys, c->NL, c->PR, c->st));
-  RKArgs a = rk_args(c, 1);
+  int st[4];
+  const int nst = scheme_stages(c->cfg.scheme, st);
+  RKArgs a = rk_args(c, st[0]);
   TG_CK(launch_rk(a, c->phys, c->tprec, c->tprec, 1, c->st, nullptr));
-  rc = run_stages(c, 2, false);
+  if (nst == 1) {
+    rc = run_finalize(c, 1, false);
+  } else {
+    rc = run_stages(c, 2, false);
+  }
   if (rc) return rc;
   c->have_nlin = c->have_pressure = c->have_force = false;
   return TG_OK;

@@ -28,6 +28,7 @@ struct tg_ctx {
   int nstate = 3, nin = 3, nprod = 6;
   tg::ProdPairs pairs{};
   double nu_of[6] = {0, 0, 0, 0, 0, 0};
+  double nuh_of[6] = {0, 0, 0, 0, 0, 0};  // hyper coefficients per state field (0: off)
   // batch of same-shape requests (serving): B slots, the first nact of them advanced by a step;
   // slot r of every state and pipeline buffer at offset r * S (or r * stage size)
   int B = 1;
@@ -203,6 +204,12 @@ int ensure_staging_ctx(tg_ctx* c);
 int validate_config(const tg_config* cfg);
 // viscosity of each state field (nu, eta, kappa; RB: from Ra and Pr)
 void state_viscosities(const tg_config* cfg, double nu[6]);
+void state_hyper(const tg_config* cfg, double nuh[6]);
+// the RK kernel's stages of one step of the configured scheme, in order (k_rk STAGE codes):
+// RK4 1, 2, 3, 4; EULER 5; RK2 7, 6
+int scheme_stages(int scheme, int out[4]);
+// the stage that ends a step (energy partials, U0 written)
+inline bool stage_is_final(int stage) { return stage == 4 || stage == 5 || stage == 6; }
 struct RBCoef {
   double nu, kappa, fu, ft, nuf;
 };

@@ -128,9 +128,9 @@ int state_fields(int physics) {
 // from the context; the per-slot coefficients (viscosities, dt) may differ.
 std::string batch_key(const tg_config& c, long long id) {
   char buf[512];
-  std::snprintf(buf, sizeof(buf), "%d,%d,%d|b%d|p%d|x%d|d%d|s%d|k%a,%a,%a|f%d", c.N[0], c.N[1], c.N[2], c.basis,
-                c.physics, c.precision, c.dealias, c.scheme, c.kfactor[0], c.kfactor[1], c.kfactor[2],
-                c.force_kind);
+  std::snprintf(buf, sizeof(buf), "%d,%d,%d|b%d|p%d|x%d|d%d|s%d|k%a,%a,%a|f%d|h%a,%a,%a", c.N[0], c.N[1], c.N[2],
+                c.basis, c.physics, c.precision, c.dealias, c.scheme, c.kfactor[0], c.kfactor[1], c.kfactor[2],
+                c.force_kind, c.hyper_nu, c.hyper_eta, c.hyper_kappa);
   std::string k(buf);
   if (c.force_kind == TG_FORCE_ENERGY_SUPPLY || c.force_kind == TG_FORCE_ENERGY_HELICITY)
     k += "|solo" + std::to_string(id);

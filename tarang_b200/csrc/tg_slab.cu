@@ -295,6 +295,8 @@ int tg_slab_create(const tg_config* cfg, int world, int rank, tg_ctx** out) {
   if (cfg->physics == TG_MHD || cfg->force_kind == TG_FORCE_ENERGY_SUPPLY ||
       cfg->force_kind == TG_FORCE_ENERGY_HELICITY)
     return TG_ERR_UNSUPPORTED;
+  // the phases run the four RK4 stages (tg_slab_phase stage 1..4)
+  if (cfg->scheme != TG_RK4) return TG_ERR_UNSUPPORTED;
   const int Mz = cfg->N[2] / 2;
   if (Mz < 4 || Mz > 256 || (Mz & (Mz - 1))) return TG_ERR_UNSUPPORTED;
   return ctx_create_batch(cfg, 1, out, world, rank);

@@ -161,12 +161,18 @@ __device__ __forceinline__ void project_rhs(cx<double>* r, int ns, const XDer& d
   for (int c = 3; c < ns; ++c) r[c] = mkc<double>(-r[c].x, -r[c].y);
 }
 
-// ------------------------------------------------------------------ RK4 stage kernel
-// IncFluid::Time_advance RK4 (time_advance.cc:100-155) with E(a) = exp(-nu a dt K^2):
-//  stage 1: u1 = E(1/2)(u0 + dt/2 N0),        tot  = dt/6 E(1) N0
-//  stage 2: u2 = E(1/2) u0 + dt/2 N1,         tot += dt/3 E(1/2) N1
-//  stage 3: u3 = E(1/2)(E(1/2) u0 + dt N2),   tot += dt/3 E(1/2) N2
-//  stage 4: u  = E(1) u0 + tot + dt/6 N3   (then the energy of u for the NaN check / Get_dt)
+// ------------------------------------------------------------------ RK stage kernel
+// IncFluid::Time_advance (time_advance.cc:60-163) with E(a) = exp(-(nu + nu_h K^2) a dt K^2)
+// (the hyper term when on, mult_exp_visc.cc:56-165) and Single_time_step(dt, a, b, c) =
+// E(b)(E(a - b) u + c dt N) (single_time_step.cc:54-86):
+//  RK4 stage 1: u1 = E(1/2)(u0 + dt/2 N0),        tot  = dt/6 E(1) N0
+//      stage 2: u2 = E(1/2) u0 + dt/2 N1,         tot += dt/3 E(1/2) N1
+//      stage 3: u3 = E(1/2)(E(1/2) u0 + dt N2),   tot += dt/3 E(1/2) N2
+//      stage 4: u  = E(1) u0 + tot + dt/6 N3
+//  EULER (5):   u  = E(1)(u0 + dt N0)                       Single_time_step(dt, 1, 1, 1)
+//  RK2   (7):   u1 = E(1/2)(u0 + dt/2 N0)                   Single_time_step(dt, 1/2, 1/2, 1/2)
+//        (6):   u  = E(1/2)(E(1/2) u0 + dt N1)              Single_time_step(dt, 1, 1/2, 1)
+// after a final stage (4, 5, 6) the energy of u for the NaN check / Get_dt
 // Resident blocks per SM the RK kernel is built for (fluid/scalar: 3 at 80 registers, MHD: 2).
 template <int PHYS>
 struct RKOcc {
@@ -184,9 +190,13 @@ __global__ void __launch_bounds__(TPB, RKOcc<PHYS>::v) k_rk(RKArgs a) {
   const int slot = blockIdx.y;
   const long long base = (long long)slot * g.S;
   const double dt = a.dt[(long long)slot * 8];
-  double nus[NS];
+  constexpr bool FINAL = STAGE == 4 || STAGE == 5 || STAGE == 6;
+  double nus[NS], nuh[NS];
 #pragma unroll
-  for (int c = 0; c < NS; ++c) nus[c] = a.nu_tab ? a.nu_tab[slot * 6 + c] : a.nu[c];
+  for (int c = 0; c < NS; ++c) {
+    nus[c] = a.nu_tab ? a.nu_tab[slot * 6 + c] : a.nu[c];
+    nuh[c] = a.nuh[c];
+  }
   const unsigned S = (unsigned)g.S, kzp = (unsigned)g.kzp, nky = (unsigned)g.nky;
   const unsigned stride = gridDim.x * TPB;
   for (unsigned i = blockIdx.x * TPB + threadIdx.x; i < S; i += stride) {
@@ -198,7 +208,7 @@ __global__ void __launch_bounds__(TPB, RKOcc<PHYS>::v) k_rk(RKArgs a) {
     cx<double> u0[NS], tot[NS];
 #pragma unroll
     for (int c = 0; c < NS; ++c) u0[c] = a.U0[c][gi];
-    if constexpr (STAGE > 1) {
+    if constexpr (STAGE >= 2 && STAGE <= 4) {
 #pragma unroll
       for (int c = 0; c < NS; ++c) tot[c] = a.TOT[c][gi];
     }
@@ -253,9 +263,11 @@ __global__ void __launch_bounds__(TPB, RKOcc<PHYS>::v) k_rk(RKArgs a) {
     double eh = 0, e1 = 0;
 #pragma unroll
     for (int c = 0; c < NS; ++c) {
-      if (c == 0 || nus[c] != nus[c - 1]) {
-        eh = exp(-nus[c] * 0.5 * dt * K2);
-        if constexpr (STAGE == 1 || STAGE == 4) e1 = exp(-nus[c] * dt * K2);
+      if (c == 0 || nus[c] != nus[c - 1] || nuh[c] != nuh[c - 1]) {
+        // nu + nu_h K^2 (nu exactly when the hyper term is off)
+        const double nuk = nuh[c] != 0.0 ? nus[c] + nuh[c] * K2 : nus[c];
+        eh = exp(-nuk * 0.5 * dt * K2);
+        if constexpr (STAGE == 1 || STAGE == 4 || STAGE == 5) e1 = exp(-nuk * dt * K2);
       }
       const cx<double> rc = r[c];
       if constexpr (STAGE == 1) {
@@ -267,8 +279,13 @@ __global__ void __launch_bounds__(TPB, RKOcc<PHYS>::v) k_rk(RKArgs a) {
       } else if constexpr (STAGE == 3) {
         stc<Rs>(a.US[c], gi, eh * (eh * u0[c] + dt * rc));
         a.TOT[c][gi] = tot[c] + (dt / 3.0) * (eh * rc);
+      } else if constexpr (STAGE == 7) {
+        stc<Rs>(a.US[c], gi, eh * (u0[c] + (0.5 * dt) * rc));
       } else {
-        const cx<double> u = e1 * u0[c] + (tot[c] + (dt / 6.0) * rc);
+        cx<double> u;
+        if constexpr (STAGE == 4) u = e1 * u0[c] + (tot[c] + (dt / 6.0) * rc);
+        else if constexpr (STAGE == 5) u = e1 * (u0[c] + dt * rc);
+        else u = eh * (eh * u0[c] + dt * rc);
         a.U0[c][gi] = u;
         const double m2 = u.x * u.x + u.y * u.y;
         const int grp = (PHYS == PH_MHD) ? (c / 3) * 2 : (c < 3 ? 0 : 4);
@@ -286,7 +303,7 @@ __global__ void __launch_bounds__(TPB, RKOcc<PHYS>::v) k_rk(RKArgs a) {
       }
     }
   }
-  if constexpr (STAGE == 4) {
+  if constexpr (FINAL) {
     if (a.part != nullptr) {
       block_sum<6>(acc);
       if (threadIdx.x == 0) {
@@ -301,15 +318,23 @@ template <typename Rp, typename Rs, int PHYS>
 cudaError_t run_rk_src(const RKArgs& a, int src, cudaStream_t s, int nblk) {
   const dim3 grid(nblk, a.nact > 0 ? a.nact : 1);
   if (src == 1) {
-    // precomputed right-hand sides enter at stage 1 only (Time_advance after Compute_rhs)
-    if (a.stage != 1) return cudaErrorInvalidValue;
-    k_rk<Rp, Rs, PHYS, 1, 1><<<grid, TPB, 0, s>>>(a);
+    // precomputed right-hand sides enter at a scheme's first stage only (Time_advance after
+    // Compute_rhs): RK4 1, EULER 5, RK2 7
+    switch (a.stage) {
+      case 1: k_rk<Rp, Rs, PHYS, 1, 1><<<grid, TPB, 0, s>>>(a); break;
+      case 5: k_rk<Rp, Rs, PHYS, 1, 5><<<grid, TPB, 0, s>>>(a); break;
+      case 7: k_rk<Rp, Rs, PHYS, 1, 7><<<grid, TPB, 0, s>>>(a); break;
+      default: return cudaErrorInvalidValue;
+    }
   } else {
     switch (a.stage) {
       case 1: k_rk<Rp, Rs, PHYS, 0, 1><<<grid, TPB, 0, s>>>(a); break;
       case 2: k_rk<Rp, Rs, PHYS, 0, 2><<<grid, TPB, 0, s>>>(a); break;
       case 3: k_rk<Rp, Rs, PHYS, 0, 3><<<grid, TPB, 0, s>>>(a); break;
       case 4: k_rk<Rp, Rs, PHYS, 0, 4><<<grid, TPB, 0, s>>>(a); break;
+      case 5: k_rk<Rp, Rs, PHYS, 0, 5><<<grid, TPB, 0, s>>>(a); break;
+      case 6: k_rk<Rp, Rs, PHYS, 0, 6><<<grid, TPB, 0, s>>>(a); break;
+      case 7: k_rk<Rp, Rs, PHYS, 0, 7><<<grid, TPB, 0, s>>>(a); break;
       default: return cudaErrorInvalidValue;
     }
   }

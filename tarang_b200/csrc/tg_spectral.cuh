@@ -65,9 +65,10 @@ __host__ __device__ __forceinline__ double mult_scft(int m, int l2, int l3, int 
 
 struct RKArgs {
   Geo g;
-  int stage;               // 1..4
+  int stage;               // RK4 1..4, EULER 5, RK2 7 then 6
   int nstate;              // state fields
   double nu[6];            // per state field
+  double nuh[6];           // hyper coefficients per state field (0: off)
   const double* dt;        // device scalar
   cx<double>* U0[6];       // FP64 master state
   cx<double>* TOT[6];      // FP64 RK accumulator
@@ -76,7 +77,7 @@ struct RKArgs {
   const cx<double>* RHS[6];// precomputed right-hand sides (SRC = 1)
   const cx<double>* FB;    // force box [nstate][box] or null
   int fx, fy, fz;          // force box half widths (kx, ky in [-f, f], kz in [0, fz])
-  double* part;            // stage 4: per-block partial sums [blocks][8]
+  double* part;            // final stage (4, 5, 6): per-block partial sums [blocks][8]
   double rb_buoy_u, rb_buoy_t;  // RB forces: Force1 = rb_buoy_u * theta, T.Force = rb_buoy_t * u1
   const void* IN[6];       // the stage's input fields (the forces are computed from them)
   int inprec;              // 0 FP64, 1 FP32

@@ -147,15 +147,16 @@ def config_from_para(p: dict, kind: str = "FLUID") -> dict:
     """Keyword arguments of solver.make_config (N, basis, physics, dealias, kfactor,
     coefficients, dt, forcing, shells) for a parsed para.d, plus 'run' with the time span, the
     field I/O switches and the initial-condition procedure.  Raises ValueError for what the GPU
-    solver does not run (hyperdissipation, schemes other than RK4, other forcings)."""
+    solver does not run (other schemes, other forcings).  The integration scheme (EULER, RK2,
+    RK4) and, with hyper_dissipation_switch (switches(1)) on, the hyper coefficients of U and of
+    W or T (IncVF.cc:70-83, IncSF.cc:62-65) carry over."""
     kind = kind.upper()
     if kind not in _N_FIELDS:
         raise ValueError(f"kind {kind}")
     basis, alias, scheme = p["string_switches"][1], p["string_switches"][2], p["string_switches"][3]
-    if scheme != "RK4":
-        raise ValueError(f"integration scheme {scheme}: only RK4 runs on the GPU")
-    if p["switches"][1] != 0:
-        raise ValueError("hyperdissipation is not supported")
+    if scheme not in ("EULER", "RK2", "RK4"):
+        raise ValueError(f"integration scheme {scheme}: EULER, RK2 and RK4 run on the GPU")
+    hyper = p["switches"][1] != 0
     sd, si = p["solver_double"], p["solver_int"]
     if kind == "RB":
         # RB_slip_main.cc:150-240: kfactor given or scaled by (pi, pi/sqrt 2, pi/sqrt 2); Ra
@@ -177,13 +178,17 @@ def config_from_para(p: dict, kind: str = "FLUID") -> dict:
     else:
         kf = (sd[1], sd[2], sd[3])
     cfg = dict(N=tuple(p["N"][1:4]), basis=basis, physics=kind, dealias=(alias == "DEALIAS"),
-               kfactor=kf, nu=p["diss"][0], dt=p["time_para"][3], n_shells=p["ET"][3])
+               kfactor=kf, nu=p["diss"][0], dt=p["time_para"][3], n_shells=p["ET"][3], scheme=scheme,
+               hyper_nu=p["hyper_diss"][0] if hyper else 0.0)
     if kind == "MHD":
         cfg["eta"] = p["diss"][1]
+        cfg["hyper_eta"] = p["hyper_diss"][1] if hyper else 0.0
     elif kind == "SCALAR":
         cfg["kappa"] = p["diss"][1]
     elif kind == "RB":
         cfg.update(Ra=ra, Pr=pr, Pr_switch=pr_switch, RB_Uscaling=u_scaling, temperature_grad=temp_grad)
+    if kind in ("SCALAR", "RB"):
+        cfg["hyper_kappa"] = p["hyper_diss"][1] if hyper else 0.0
     proc = p["force_int"][1] if len(p["force_int"]) > 1 else 0
     fd = p["force_double"] + [0.0] * 7
     run_force = None

@@ -26,6 +26,7 @@ _BASIS = {"FOUR": L.TG_FOUR, "SCFT": L.TG_SCFT}
 _PHYS = {"FLUID": L.TG_FLUID, "INC_FLUID": L.TG_FLUID, "MHD": L.TG_MHD, "INC_MHD": L.TG_MHD,
          "SCALAR": L.TG_SCALAR, "INC_SCALAR": L.TG_SCALAR, "RB": L.TG_RB, "RB_SLIP": L.TG_RB}
 _PREC = {"FP64": L.TG_FP64, "FP32": L.TG_FP32_MIXED, "FP32_MIXED": L.TG_FP32_MIXED}
+_SCHEME = {"EULER": L.TG_EULER, "RK2": L.TG_RK2, "RK4": L.TG_RK4}
 
 
 _DP_T = C.POINTER(C.c_double)
@@ -38,7 +39,8 @@ def _dptr(a: np.ndarray):
 def make_config(N, basis="FOUR", physics="FLUID", precision="FP64", dealias=True,
                 kfactor=(1.0, 1.0, 1.0), nu=0.01, eta=None, kappa=None, dt=1e-3,
                 force=None, n_shells=12, device=0, Ra=0.0, Pr=0.0, stream=None,
-                Pr_switch="PRLARGE", RB_Uscaling="ULARGE", temperature_grad=1.0) -> L.tg_config:
+                Pr_switch="PRLARGE", RB_Uscaling="ULARGE", temperature_grad=1.0, scheme="RK4",
+                hyper_nu=0.0, hyper_eta=None, hyper_kappa=None) -> L.tg_config:
     lib = L.load()
     cfg = L.tg_config()
     lib.tg_config_default(C.byref(cfg))
@@ -47,7 +49,10 @@ def make_config(N, basis="FOUR", physics="FLUID", precision="FP64", dealias=True
     cfg.physics = _PHYS[physics] if isinstance(physics, str) else int(physics)
     cfg.precision = _PREC[precision] if isinstance(precision, str) else int(precision)
     cfg.dealias = 1 if dealias else 0
-    cfg.scheme = L.TG_RK4
+    cfg.scheme = _SCHEME[scheme] if isinstance(scheme, str) else int(scheme)
+    cfg.hyper_nu = float(hyper_nu)
+    cfg.hyper_eta = float(hyper_nu if hyper_eta is None else hyper_eta)
+    cfg.hyper_kappa = float(hyper_nu if hyper_kappa is None else hyper_kappa)
     cfg.kfactor[:] = [float(k) for k in kfactor]
     cfg.nu = float(nu)
     cfg.eta = float(nu if eta is None else eta)

@@ -47,7 +47,8 @@ def test_config_default_without_gpu(lib):
     cfg = _lib.tg_config()
     lib.tg_config_default(ctypes.byref(cfg))
     assert list(cfg.N) == [64, 64, 64] and cfg.scheme == 4 and cfg.dealias == 1
-    assert ctypes.sizeof(_lib.tg_config) == 200 and cfg.rb_temp_grad == 1.0
+    assert ctypes.sizeof(_lib.tg_config) == 224 and cfg.rb_temp_grad == 1.0
+    assert cfg.hyper_nu == 0.0 and cfg.hyper_eta == 0.0 and cfg.hyper_kappa == 0.0   # hyper terms off
 
 
 def test_struct_layouts_match_header(tmp_path):

@@ -308,6 +308,27 @@ def test_read_para_fluid(lib):
     assert cs.force_kind == L.TG_FORCE_ENERGY_SUPPLY and list(cs.force_para) == [1.0, 2.0, 0.3, 0.0, 0.5, 0.0]
 
 
+def test_read_para_scheme_and_hyper(lib):
+    """integ_scheme and, with hyper_dissipation_switch (switches(1)) on, the hyper coefficients of
+    U and of the scalar reach the configuration."""
+    from tarang_b200.para import config_from_para, read_para
+    from tarang_b200.solver import make_config
+    text = PARA.format(N1=16, N2=16, N3=16, Ra=0, Pr=0, basis="FOUR", nu=0.003, kappa=0.002, dt=0.0005, S=8, proc=1)
+    text = text.replace("(3)scheme\tRK4", "(3)scheme\tRK2").replace("(1)a 0", "(1)a 1")
+    text = text.replace("#hyper\n0\t0", "#hyper\n1e-6\t2e-6")
+    c = config_from_para(read_para(text, n_fields=2), "SCALAR")
+    assert c["scheme"] == "RK2" and c["hyper_nu"] == 1e-6 and c["hyper_kappa"] == 2e-6
+    kw = dict(c)
+    kw.pop("run")
+    cfg = make_config(**kw)
+    assert cfg.scheme == L.TG_RK2 and cfg.hyper_nu == 1e-6 and cfg.hyper_kappa == 2e-6
+    # switch off: the coefficients are ignored, as the reference ignores them
+    c0 = config_from_para(read_para(text.replace("(1)a 1", "(1)a 0"), n_fields=2), "SCALAR")
+    assert c0["hyper_nu"] == 0.0 and c0["hyper_kappa"] == 0.0
+    with pytest.raises(ValueError):
+        config_from_para(read_para(text.replace("(3)scheme\tRK2", "(3)scheme\tAB2"), n_fields=2), "SCALAR")
+
+
 def test_read_para_convection(lib):
     import math
     from tarang_b200.para import config_from_para, read_para
