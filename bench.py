@@ -727,7 +727,9 @@ def run_serving(args, rank=0, world=1, dist=False):
     if dist:
         import torch
         torch.distributed.barrier()
-    srv = Server(hbm_budget=args.serve_budget, max_batch=SERVE_MAX_BATCH, keep_results=True)
+    # the request fields are the workload's own arrays, alive for the whole run: the server reads
+    # them at admission instead of copying them at submission
+    srv = Server(hbm_budget=args.serve_budget, max_batch=SERVE_MAX_BATCH, keep_results=True, borrow_inputs=True)
     fin, results, round_ms, t_base = serve_loop(srv, reqs, arrivals, mine, steps, keep)
     st = srv.stats()
     srv.close()

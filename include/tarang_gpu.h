@@ -512,6 +512,11 @@ typedef struct tg_server_config {
   int device;
   int use_graphs;          /* 1: replay one captured CUDA graph per batch and active count */
   int keep_results;        /* 1: keep each finished request's fields for tg_server_result */
+  /* 1: tg_server_submit keeps the caller's init pointer instead of copying the fields; the
+   * caller keeps that memory valid and unchanged until the request leaves TG_REQ_QUEUED (its
+   * admission copies straight from it to the device).  0: submit copies (into page-locked
+   * memory when the pool has room). */
+  int borrow_inputs;
 } tg_server_config;
 
 typedef struct tg_request {
@@ -593,6 +598,8 @@ typedef struct tg_batch_stat {
   int n_active;          /* requests running in it now */
   int step_ms_n_active;  /* active requests during the timed steps (0: none timed yet) */
   double step_ms;        /* device ms of one step of the whole batch */
+  double device_ms;      /* device ms of all the batch's steps so far (CUDA events) */
+  long long steps;       /* batch steps run so far */
 } tg_batch_stat;
 int tg_server_batch_stats(tg_server* srv, tg_batch_stat* out, int max, int* n);
 double tg_server_clock(tg_server* srv);

@@ -94,6 +94,7 @@ class tg_server_config(C.Structure):
         ("device", C.c_int),
         ("use_graphs", C.c_int),
         ("keep_results", C.c_int),
+        ("borrow_inputs", C.c_int),
     ]
 
 
@@ -160,6 +161,8 @@ class tg_batch_stat(C.Structure):
         ("n_active", C.c_int),
         ("step_ms_n_active", C.c_int),
         ("step_ms", C.c_double),
+        ("device_ms", C.c_double),
+        ("steps", C.c_longlong),
     ]
 
 

@@ -32,6 +32,7 @@ struct Req {
   int nstate = 3;
   std::vector<double> init;    // dropped at admission (when the pinned pool was full at submit)
   double* init_pin = nullptr;  // pinned block of the pool holding the fields (usual case)
+  const double* init_borrow = nullptr;  // the caller's fields (borrow_inputs), until admission
   size_t n_init = 0;
   double* result = nullptr;    // pinned block of the pool, kept when keep_results
   size_t n_result = 0;
@@ -54,6 +55,9 @@ struct Batch {
   size_t bytes = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // around the steps of the current round
   int launched_steps = 0;
+  bool launched_graph = false;       // the round's steps were graph replays (their timing counts)
+  double device_ms = 0;              // all timed steps so far
+  long long steps_run = 0;
   double step_ms = 0;                // measured time of one step at the current active count
   int step_ms_nact = 0;
   double idle_since = -1;            // server clock when the batch last became empty
@@ -178,6 +182,7 @@ void finish_req(tg_server* s, Req& r, int state, int error) {
   std::vector<double>().swap(r.init);
   if (r.init_pin) s->pinned.put(r.init_pin, r.n_init);
   r.init_pin = nullptr;
+  r.init_borrow = nullptr;
 }
 
 // Enqueue, on the batch stream, the copy of a request's fields into slot `slot` and the set-up
@@ -187,19 +192,27 @@ int load_slot(tg_server* s, Batch& b, int slot, Req& r) {
   tg_ctx* c = b.c;
   const size_t D2 = 2 * (size_t)c->D;
   const size_t n = D2 * c->nstate;
-  double* pin = r.init_pin;
-  if (pin) {
-    r.init_pin = nullptr;  // from here on the batch releases it (after the copies ran)
+  const double* src = r.init_borrow;
+  if (src) {
+    // the caller's (pageable) memory: each copy returns once the driver has staged it, so the
+    // caller's buffer is free again when this function returns
+    r.init_borrow = nullptr;
   } else {
-    pin = s->pinned.get(n);
-    if (!pin) return set_err(c, TG_ERR_OOM, "pinned host block for a request's fields");
-    std::memcpy(pin, r.init.data(), sizeof(double) * n);
-    std::vector<double>().swap(r.init);
+    double* pin = r.init_pin;
+    if (pin) {
+      r.init_pin = nullptr;  // from here on the batch releases it (after the copies ran)
+    } else {
+      pin = s->pinned.get(n);
+      if (!pin) return set_err(c, TG_ERR_OOM, "pinned host block for a request's fields");
+      std::memcpy(pin, r.init.data(), sizeof(double) * n);
+      std::vector<double>().swap(r.init);
+    }
+    b.loading.emplace_back(pin, n);
+    src = pin;
   }
-  b.loading.emplace_back(pin, n);
   cudaError_t e;
   for (int i = 0; i < c->nstate; ++i) {
-    e = cudaMemcpyAsync(c->staging, pin + (size_t)i * D2, sizeof(double) * D2, cudaMemcpyHostToDevice, c->st);
+    e = cudaMemcpyAsync(c->staging, src + (size_t)i * D2, sizeof(double) * D2, cudaMemcpyHostToDevice, c->st);
     if (e != cudaSuccess) return cuda_err(c, e, "slot upload");
     e = launch_dense_to_compact(c->g, c->staging, c->U0[i] + (size_t)slot * c->S, 0, c->st);
     if (e != cudaSuccess) return cuda_err(c, e, "slot upload");
@@ -421,6 +434,7 @@ int launch_batch(tg_server* s, Batch& b, int k) {
   e = cudaEventRecord(b.ev1, c->st);
   if (e != cudaSuccess) return cuda_err(c, e, "cudaEventRecord");
   b.launched_steps = k;
+  b.launched_graph = ex != nullptr;
   e = cudaMemcpyAsync(b.h, c->scal, sizeof(double) * 8 * nact, cudaMemcpyDeviceToHost, c->st);
   if (e != cudaSuccess) return cuda_err(c, e, "slot scalars");
   e = cudaMemcpyAsync(b.h + 8 * (size_t)b.B, c->red_out, sizeof(double) * 8 * nact, cudaMemcpyDeviceToHost, c->st);
@@ -461,7 +475,16 @@ int collect_batch(tg_server* s, Batch& b, int nl, int launch_rc) {
     b.slot_req.clear();
     return code;
   }
+  // only graph replays time a step: an eager step's events also span its host-side launches
+  // (module loading, first-use set-up) and would make the batch look far slower than it is
   if (nl > 0 && b.launched_steps > 0) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, b.ev0, b.ev1) == cudaSuccess) {
+      b.device_ms += ms;
+      b.steps_run += b.launched_steps;
+    }
+  }
+  if (nl > 0 && b.launched_steps > 0 && b.launched_graph) {
     float ms = 0;
     if (cudaEventElapsedTime(&ms, b.ev0, b.ev1) == cudaSuccess) {
       const double per = ms / b.launched_steps;
@@ -573,6 +596,11 @@ int tg_server_submit(tg_server* s, const tg_request* rq, long long* id) {
     r.st.error = TG_ERR_OOM;
     r.st.finish_s = r.st.submit_s;
     s->finished.push_back(r.id);
+  } else if (s->cfg.borrow_inputs) {
+    // no copy: admission uploads from the caller's memory (valid until the request runs)
+    r.n_init = rq->n_doubles;
+    r.init_borrow = rq->init;
+    s->queue.push_back(r.id);
   } else {
     // into a reused page-locked block when the pool has room (no page faults, and the upload
     // at admission is a plain asynchronous copy), else into ordinary memory
@@ -758,6 +786,8 @@ int tg_server_batch_stats(tg_server* s, tg_batch_stat* out, int max, int* n) {
     o.n_active = (int)b.slot_req.size();
     o.step_ms_n_active = b.step_ms > 0 ? b.step_ms_nact : 0;
     o.step_ms = b.step_ms;
+    o.device_ms = b.device_ms;
+    o.steps = b.steps_run;
   }
   *n = k;
   return TG_OK;

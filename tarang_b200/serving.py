@@ -42,7 +42,9 @@ def request_bytes(config: dict, batch: int = 1) -> int:
 
 class Server:
     def __init__(self, hbm_budget: float = 150e9, max_batch: int = 64, device: int = 0,
-                 use_graphs: bool = True, keep_results: bool = True):
+                 use_graphs: bool = True, keep_results: bool = True, borrow_inputs: bool = False):
+        """borrow_inputs: submit keeps a reference to the fields array instead of copying it;
+        the array must not change until the request has left the queue."""
         self.lib = L.load()
         sc = L.tg_server_config()
         sc.hbm_budget_bytes = int(hbm_budget)
@@ -50,6 +52,9 @@ class Server:
         sc.device = int(device)
         sc.use_graphs = 1 if use_graphs else 0
         sc.keep_results = 1 if keep_results else 0
+        sc.borrow_inputs = 1 if borrow_inputs else 0
+        self.borrow = bool(borrow_inputs)
+        self._held: dict[int, np.ndarray] = {}   # borrowed fields, kept alive until admission
         h = C.c_void_p()
         rc = self.lib.tg_server_create(C.byref(sc), C.byref(h))
         if rc != L.TG_OK:
@@ -104,6 +109,8 @@ class Server:
         if rc != L.TG_OK:
             raise L.TarangError(rc, "tg_server_submit")
         self.shapes[rid.value] = (ns,) + shape
+        if self.borrow:
+            self._held[rid.value] = flat
         return rid.value
 
     def pump(self) -> int:
@@ -111,6 +118,7 @@ class Server:
         rc = self.lib.tg_server_pump(self.h, C.byref(n))
         if rc != L.TG_OK:
             raise L.TarangError(rc, "tg_server_pump")
+        self._drop_admitted()
         return n.value
 
     def pump_begin(self):
@@ -126,10 +134,18 @@ class Server:
         rc = self.lib.tg_server_pump_end(self.h, C.byref(n))
         if rc != L.TG_OK:
             raise L.TarangError(rc, "tg_server_pump_end")
+        self._drop_admitted()
         return n.value
+
+    def _drop_admitted(self):
+        # borrowed fields of requests that have left the queue are no longer read
+        if self._held:
+            for rid in [r for r in self._held if self.poll(r)["state"] != "queued"]:
+                del self._held[rid]
 
     def drain(self, max_rounds: int = 0):
         rc = self.lib.tg_server_drain(self.h, int(max_rounds))
+        self._drop_admitted()
         if rc != L.TG_OK:
             raise L.TarangError(rc, "tg_server_drain")
 
@@ -176,7 +192,8 @@ class Server:
 
     def batch_stats(self) -> list:
         """Per resident batch: shape N, physics, precision, capacity, n_active and step_ms, the
-        device time of one step of the whole batch at step_ms_n_active running requests."""
+        device time of one step of the whole batch at step_ms_n_active running requests; device_ms
+        and steps, the device time and number of all its batch steps so far."""
         buf = (L.tg_batch_stat * 64)()
         n = C.c_int()
         rc = self.lib.tg_server_batch_stats(self.h, buf, 64, C.byref(n))

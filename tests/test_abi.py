@@ -55,7 +55,7 @@ def test_struct_layouts_match_header(tmp_path):
     """The ctypes mirrors have the sizes and field offsets that a C compiler gives the header."""
     from tarang_b200 import _lib
     structs = [_lib.tg_config, _lib.tg_server_config, _lib.tg_request, _lib.tg_request_status,
-               _lib.tg_server_stats, _lib.tg_kernel_stat]
+               _lib.tg_server_stats, _lib.tg_kernel_stat, _lib.tg_batch_stat, _lib.tg_slab_info]
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "tarang_gpu.h"', 'int main(void) {']
     for s in structs:
         n = s.__name__

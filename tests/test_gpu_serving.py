@@ -165,6 +165,31 @@ def test_split_pump_submits_during_round(lib):
             assert same_bits(srv.result(rid), want)
 
 
+def test_borrowed_inputs(lib):
+    """borrow_inputs: submit keeps the caller's arrays (no copy) and admission reads them; the
+    results equal those of copied inputs bit for bit, and the caller may reuse an array once its
+    request runs."""
+    from tarang_b200.serving import Server
+    N = (32, 32, 32)
+    cfgs = [dict(N=N, nu=1e-3 * (1 + j), dt=1e-3) for j in range(4)]
+    fields = [np.ascontiguousarray(np.stack(fluid_fields(N, 900 + j))) for j in range(4)]
+    with Server(hbm_budget=8e9, max_batch=4) as a, Server(hbm_budget=8e9, max_batch=4, borrow_inputs=True) as b:
+        ia = [a.submit(c, f, 5) for c, f in zip(cfgs, fields)]
+        ib = [b.submit(c, f, 5) for c, f in zip(cfgs, fields)]
+        assert len(b._held) == 4
+        b.pump()
+        assert not b._held and all(b.poll(i)["state"] != "queued" for i in ib)
+        kept = [f.copy() for f in fields]
+        for f in fields:
+            f[...] = 0          # the requests run: their inputs are no longer read
+        a.drain()
+        b.drain()
+        for x, y, f in zip(ia, ib, kept):
+            assert same_bits(a.result(x), b.result(y))
+            want, _, _ = lone(cfgs[0] if x == ia[0] else cfgs[ia.index(x)], list(f), 5)
+            assert same_bits(b.result(y), want)
+
+
 def test_budget_admission(lib):
     from tarang_b200.serving import Server, request_bytes
     cfg = dict(N=(32, 32, 32), nu=2e-3, dt=1e-3)
