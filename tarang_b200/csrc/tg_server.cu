@@ -36,6 +36,7 @@ struct Req {
   size_t n_init = 0;
   double* result = nullptr;    // pinned block of the pool, kept when keep_results
   size_t n_result = 0;
+  cudaEvent_t result_ev = nullptr;  // the result's copies into `result` are done past this event
   tg_request_status st{};
   std::string key;
   long long batch = -1;        // batch id while running
@@ -112,6 +113,13 @@ struct tg_server {
   long long rounds = 0, request_steps = 0, graph_launches = 0, eager_steps = 0;
   std::string err;
   bool round_open = false;                                // between pump_begin and pump_end
+  // released result blocks whose copies may still run: back to the pool once their event passed
+  struct PendingBlock {
+    double* p;
+    size_t n;
+    cudaEvent_t ev;
+  };
+  std::vector<PendingBlock> pending_free;
   cudaEvent_t chain = nullptr;                            // end of the last batch launched
   std::map<long long, std::pair<int, int>> launched;      // batch -> (slots stepped, launch code)
 };
@@ -230,8 +238,9 @@ int load_slot(tg_server* s, Batch& b, int slot, Req& r) {
   return run_energy_slots(c, 2, slot, 1);
 }
 
-// fields of slot `slot` into a pinned block held by the request (reference layout); the batch
-// stream is idle when this runs, so the wait covers these copies only
+// fields of slot `slot` into a pinned block held by the request (reference layout), queued on
+// the batch stream ahead of anything that reuses the slot or the staging buffer; the copies
+// overlap the next round, and reading the result (tg_server_result) waits for their event
 int store_slot(tg_server* s, Batch& b, int slot, Req& r) {
   tg_ctx* c = b.c;
   if (!s->cfg.keep_results) return TG_OK;
@@ -239,23 +248,34 @@ int store_slot(tg_server* s, Batch& b, int slot, Req& r) {
   const size_t n = D2 * c->nstate;
   double* pin = s->pinned.get(n);
   if (!pin) return set_err(c, TG_ERR_OOM, "pinned host block for a result");
-  for (int i = 0; i < c->nstate; ++i) {
-    cudaError_t e = launch_compact_to_dense(c->g, c->U0[i] + (size_t)slot * c->S, 0, c->staging, c->st);
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < c->nstate && e == cudaSuccess; ++i) {
+    e = launch_compact_to_dense(c->g, c->U0[i] + (size_t)slot * c->S, 0, c->staging, c->st);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(pin + (size_t)i * D2, c->staging, sizeof(double) * D2, cudaMemcpyDeviceToHost, c->st);
-    if (e != cudaSuccess) {
-      s->pinned.put(pin, n);
-      return cuda_err(c, e, "slot download");
-    }
   }
-  cudaError_t e = cudaStreamSynchronize(c->st);
+  cudaEvent_t ev = nullptr;
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventRecord(ev, c->st);
   if (e != cudaSuccess) {
+    cudaStreamSynchronize(c->st);  // no copy into the block may still be running
+    if (ev) cudaEventDestroy(ev);
     s->pinned.put(pin, n);
     return cuda_err(c, e, "slot download");
   }
   r.result = pin;
   r.n_result = n;
+  r.result_ev = ev;
   return TG_OK;
+}
+
+// the request's result copies have landed (a no-op once waited for)
+void wait_result(Req& r) {
+  if (r.result_ev) {
+    cudaEventSynchronize(r.result_ev);
+    cudaEventDestroy(r.result_ev);
+    r.result_ev = nullptr;
+  }
 }
 
 // slot `to` takes the request in slot `from` (device copies on the batch stream)
@@ -559,6 +579,13 @@ int tg_server_destroy(tg_server* s) {
   if (!s) return TG_ERR_ARG;
   cudaSetDevice(s->dev);
   if (s->round_open) tg_server_pump_end(s, nullptr);
+  for (auto& kv : s->reqs) wait_result(kv.second);
+  for (auto& pb : s->pending_free) {
+    cudaEventSynchronize(pb.ev);
+    cudaEventDestroy(pb.ev);
+    cudaFreeHost(pb.p);
+  }
+  s->pending_free.clear();
   for (auto& kv : s->batches) destroy_batch(s, kv.second);
   if (s->chain) cudaEventDestroy(s->chain);
   for (auto& kv : s->reqs)
@@ -656,6 +683,19 @@ int tg_server_pump_begin(tg_server* s) {
 int tg_server_pump_end(tg_server* s, int* n_active) {
   if (!s) return TG_ERR_ARG;
   cudaSetDevice(s->dev);
+  {
+    std::vector<tg_server::PendingBlock> keep;
+    for (auto& pb : s->pending_free) {
+      if (cudaEventQuery(pb.ev) == cudaSuccess) {
+        cudaEventDestroy(pb.ev);
+        s->pinned.put(pb.p, pb.n);
+      } else {
+        cudaGetLastError();  // cudaErrorNotReady is no error
+        keep.push_back(pb);
+      }
+    }
+    s->pending_free.swap(keep);
+  }
   if (!s->round_open) s->launched.clear();  // a round without launches: admission only
   s->round_open = false;
   const auto& launched = s->launched;
@@ -728,9 +768,11 @@ int tg_server_result(tg_server* s, long long id, double* host, size_t n) {
   if (!s || !host) return TG_ERR_ARG;
   auto it = s->reqs.find(id);
   if (it == s->reqs.end()) return TG_ERR_ARG;
-  const Req& r = it->second;
+  Req& r = it->second;
   if (r.st.state != TG_REQ_DONE || !r.result) return TG_ERR_STATE;
   if (n != r.n_result) return TG_ERR_ARG;
+  cudaSetDevice(s->dev);
+  wait_result(r);
   std::memcpy(host, r.result, sizeof(double) * n);
   return TG_OK;
 }
@@ -740,7 +782,15 @@ int tg_server_release(tg_server* s, long long id) {
   auto it = s->reqs.find(id);
   if (it == s->reqs.end()) return TG_ERR_ARG;
   Req& r = it->second;
-  s->pinned.put(r.result, r.n_result);
+  cudaSetDevice(s->dev);
+  if (r.result && r.result_ev) {
+    // the block goes back to the pool once no copy writes it (checked at each pump_end)
+    s->pending_free.push_back({r.result, r.n_result, r.result_ev});
+    r.result_ev = nullptr;
+  } else {
+    wait_result(r);
+    s->pinned.put(r.result, r.n_result);
+  }
   r.result = nullptr;
   r.n_result = 0;
   return TG_OK;
