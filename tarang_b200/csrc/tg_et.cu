@@ -139,6 +139,7 @@ struct ContractArgs {
   int nrec;
   Radii rad;
   double* hist;           // [nrec][S+1]
+  double* part;           // [blocks][nrec][S+1]: each block's sums, reduced in block order
   int cross;              // 1: N = F(H x G) (EnergyTr_Compute_nlin_UcrossB) instead of D_j F(H_j G_i)
 };
 
@@ -146,63 +147,101 @@ struct ContractArgs {
 // of the cosine series P(0, 0) is -kx P and of the sine series P(1, 0), P(2, 0) is +kx P, y and z
 // as FOUR.  hist[r][shell(|K|)] += 2 mult Re(sum_i N_i conj(R_i)) (Multiplicity_factor_FOUR or
 // _SCFT).
+// v of every active lane into row[bin], the same sum whatever the warp's timing: the lanes of a
+// bin (__match_any_sync) add their values in lane order and the lowest of them adds the total to
+// the warp's own row
+__device__ __forceinline__ void warp_bin_add(double* row, int bin, double v, bool active) {
+  const int lane = threadIdx.x & 31;
+  const unsigned peers = __match_any_sync(0xffffffffu, active ? bin : -1 - lane);
+  double sum = 0;
+  for (unsigned m = peers; m; m &= m - 1) sum += __shfl_sync(peers, v, __ffs(m) - 1);
+  if (active && lane == __ffs(peers) - 1) row[bin] += sum;
+}
+
 template <typename Rp>
 __global__ void __launch_bounds__(TPB) k_et_contract(ContractArgs a) {
-  __shared__ double sh[2 * (kMaxShells + 1)];
+  constexpr int W = TPB / 32;
+  constexpr int ROW = 2 * (kMaxShells + 1);
+  __shared__ double sh[W][ROW];  // one row of bins per warp: no two warps add to one word
   const int nb = a.rad.S + 1;
-  for (int i = threadIdx.x; i < a.nrec * nb; i += TPB) sh[i] = 0;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int i = threadIdx.x; i < W * ROW; i += TPB) sh[i / ROW][i % ROW] = 0;
   __syncthreads();
   const Geo& g = a.g;
   const long long stride = (long long)gridDim.x * TPB;
-  for (long long idx = (long long)blockIdx.x * TPB + threadIdx.x; idx < g.S; idx += stride) {
-    int r1, r2, l3;
-    compact_mode(g, idx, r1, r2, l3);
-    if (l3 >= g.nkz) continue;
-    const int l1 = geo_l1(g, r1), l2 = amap_index(g.ay, r2);
-    const double kx = geo_kx(g, r1) * g.kf0, ky = geo_ky(g, r2) * g.kf1, kz = l3 * g.kf2;
-    const double K = sqrt(kx * kx + ky * ky + kz * kz);
-    int bin = 0;  // receiver annulus: first rho >= |K|
-    while (bin < a.rad.S && K > a.rad.r[bin]) ++bin;
-    cx<double> N[3];
-    if (a.cross) {
-      // (H x G)_i from P(i, j) = F(H_j G_i): x = P(2,1) - P(1,2), y = P(0,2) - P(2,0), z = P(1,0) - P(0,1)
-      auto P = [&](int i, int j) { return cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + j])[idx]); };
-      N[0] = P(2, 1) - P(1, 2);
-      N[1] = P(0, 2) - P(2, 0);
-      N[2] = P(1, 0) - P(0, 1);
-    } else if (g.basis == 0) {
-#pragma unroll
-      for (int i = 0; i < 3; ++i) {
-        const cx<double> p0 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 0])[idx]);
-        const cx<double> p1 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 1])[idx]);
-        const cx<double> p2 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 2])[idx]);
-        const cx<double> s = mkc<double>(kx * p0.x + ky * p1.x + kz * p2.x, kx * p0.y + ky * p1.y + kz * p2.y);
-        N[i] = ione(s);
-      }
-    } else {
-#pragma unroll
-      for (int i = 0; i < 3; ++i) {
-        const cx<double> p0 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 0])[idx]);
-        const cx<double> p1 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 1])[idx]);
-        const cx<double> p2 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 2])[idx]);
-        const double dx = (i == 0) ? -kx : kx;
-        N[i] = mkc<double>(dx * p0.x - (ky * p1.y + kz * p2.y), dx * p0.y + (ky * p1.x + kz * p2.x));
-      }
+  // warp-uniform trip count: every lane of a warp takes part in the warp's bin sums
+  for (long long w0 = (long long)blockIdx.x * TPB + warp * 32; w0 < g.S; w0 += stride) {
+    const long long idx = w0 + lane;
+    bool active = idx < g.S;
+    int r1 = 0, r2 = 0, l3 = 0;
+    if (active) {
+      compact_mode(g, idx, r1, r2, l3);
+      active = l3 < g.nkz;
     }
-    const double m = g.basis == 0 ? mult_four(l1, l2, l3, g.N1, g.N2) : mult_scft(l1, l2, l3, g.N2);
+    int bin = 0;  // receiver annulus: first rho >= |K|
+    double m = 0;
+    cx<double> N[3] = {mkc<double>(0, 0), mkc<double>(0, 0), mkc<double>(0, 0)};
+    if (active) {
+      const int l1 = geo_l1(g, r1), l2 = amap_index(g.ay, r2);
+      const double kx = geo_kx(g, r1) * g.kf0, ky = geo_ky(g, r2) * g.kf1, kz = l3 * g.kf2;
+      const double K = sqrt(kx * kx + ky * ky + kz * kz);
+      while (bin < a.rad.S && K > a.rad.r[bin]) ++bin;
+      if (a.cross) {
+        // (H x G)_i from P(i, j) = F(H_j G_i): x = P(2,1) - P(1,2), y = P(0,2) - P(2,0), z = P(1,0) - P(0,1)
+        auto P = [&](int i, int j) { return cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + j])[idx]); };
+        N[0] = P(2, 1) - P(1, 2);
+        N[1] = P(0, 2) - P(2, 0);
+        N[2] = P(1, 0) - P(0, 1);
+      } else if (g.basis == 0) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          const cx<double> p0 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 0])[idx]);
+          const cx<double> p1 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 1])[idx]);
+          const cx<double> p2 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 2])[idx]);
+          const cx<double> s = mkc<double>(kx * p0.x + ky * p1.x + kz * p2.x, kx * p0.y + ky * p1.y + kz * p2.y);
+          N[i] = ione(s);
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          const cx<double> p0 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 0])[idx]);
+          const cx<double> p1 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 1])[idx]);
+          const cx<double> p2 = cvt<double>(reinterpret_cast<const cx<Rp>*>(a.PX[3 * i + 2])[idx]);
+          const double dx = (i == 0) ? -kx : kx;
+          N[i] = mkc<double>(dx * p0.x - (ky * p1.y + kz * p2.y), dx * p0.y + (ky * p1.x + kz * p2.x));
+        }
+      }
+      m = g.basis == 0 ? mult_four(l1, l2, l3, g.N1, g.N2) : mult_scft(l1, l2, l3, g.N2);
+    }
     for (int r = 0; r < a.nrec; ++r) {
       double v = 0;
+      if (active) {
 #pragma unroll
-      for (int i = 0; i < 3; ++i) {
-        const cx<double> b = a.R[r][i][idx];
-        v += N[i].x * b.x + N[i].y * b.y;
+        for (int i = 0; i < 3; ++i) {
+          const cx<double> b = a.R[r][i][idx];
+          v += N[i].x * b.x + N[i].y * b.y;
+        }
       }
-      atomicAdd(&sh[r * nb + bin], 2.0 * m * v);
+      warp_bin_add(sh[warp] + r * nb, bin, 2.0 * m * v, active);
     }
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < a.nrec * nb; i += TPB)
-    if (sh[i] != 0) atomicAdd(&a.hist[i], sh[i]);
+  // the block's sums, warps in order
+  for (int i = threadIdx.x; i < a.nrec * nb; i += TPB) {
+    double t = 0;
+#pragma unroll
+    for (int w = 0; w < W; ++w) t += sh[w][i];
+    a.part[(size_t)blockIdx.x * a.nrec * nb + i] = t;
+  }
+}
+
+// hist[i] = the blocks' sums of bin i in block order (one thread per bin)
+__global__ void k_et_reduce(const double* __restrict__ part, int nblocks, int nbins, double* hist) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nbins) return;
+  double t = 0;
+  for (int b = 0; b < nblocks; ++b) t += part[(size_t)b * nbins + i];
+  hist[i] = t;
 }
 
 struct KindSpec {
@@ -254,7 +293,9 @@ int et_tables_ptr(tg_ctx* c, const cx<double>* const* Hp, const cx<double>* cons
   for (int i = 0; i <= A; ++i) rad.r[i] = rho[i];
   const int nb = A + 1;
   const size_t need = (size_t)nrec * (A + 1) * nb;
-  rc = ensure_diag(c, need);
+  const int nblk = (int)std::min<long long>((g.S + TPB - 1) / TPB, 148LL * 8);
+  // the tables, then the per-block sums of one contraction (reduced in block order)
+  rc = ensure_diag(c, need + (size_t)nblk * nrec * nb);
   if (rc) return rc;
   cudaError_t e = cudaMemsetAsync(c->diag, 0, sizeof(double) * need, c->st);
   if (e != cudaSuccess) return cuda_err(c, e, "memset");
@@ -268,7 +309,6 @@ int et_tables_ptr(tg_ctx* c, const cx<double>* const* Hp, const cx<double>* cons
       pp.a[3 * i + j] = (signed char)(3 + i);  // G_i
       pp.b[3 * i + j] = (signed char)j;        // H_j
     }
-  const int nblk = (int)std::min<long long>((g.S + TPB - 1) / TPB, 148LL * 8);
   for (int n = 1; n <= A; ++n) {
     k_fill_shell<<<(int)((g.S + TPB - 1) / TPB), TPB, 0, c->st>>>(
         g, Fp[0], Fp[1], Fp[2], c->etG[0], c->etG[1], c->etG[2], rho[n - 1], rho[n]);
@@ -288,10 +328,12 @@ int et_tables_ptr(tg_ctx* c, const cx<double>* const* Hp, const cx<double>* cons
     a.rad = rad;
     a.cross = cross;
     a.hist = c->diag + (size_t)n * nrec * nb;  // layout [g][r][a]
+    a.part = c->diag + need;
     {
       ProfScope pr(c, "et_contract", 0.0);
       if (c->tprec == F64) k_et_contract<double><<<nblk, TPB, 0, c->st>>>(a);
       else k_et_contract<float><<<nblk, TPB, 0, c->st>>>(a);
+      k_et_reduce<<<(nrec * nb + 127) / 128, 128, 0, c->st>>>(a.part, nblk, nrec * nb, a.hist);
     }
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_err(c, e, "et contract");
