@@ -511,7 +511,9 @@ typedef struct tg_server_config {
   int max_batch;           /* most requests in one batch */
   int device;
   int use_graphs;          /* 1: replay one captured CUDA graph per batch and active count */
-  int keep_results;        /* 1: keep each finished request's fields for tg_server_result */
+  int keep_results;        /* 1: keep each finished request's fields for tg_server_result, in
+                              device memory outside the batch budget (page-locked host memory
+                              where the device has no room) until tg_server_release */
   /* 1: tg_server_submit keeps the caller's init pointer instead of copying the fields; the
    * caller keeps that memory valid and unchanged until the request leaves TG_REQ_QUEUED (its
    * admission copies straight from it to the device).  0: submit copies (into page-locked
@@ -579,9 +581,11 @@ int tg_server_pump_end(tg_server* srv, int* n_active);
 /* pump until every submitted request is done or failed (bounded by max_rounds; 0 = no bound) */
 int tg_server_drain(tg_server* srv, long long max_rounds);
 int tg_server_poll(tg_server* srv, long long id, tg_request_status* st);
-/* final fields of a finished request (keep_results = 1), same packing as tg_request.init */
+/* final fields of a finished request (keep_results = 1), same packing as tg_request.init: copied
+ * from the device when called (the batches' streams go on meanwhile) */
 int tg_server_result(tg_server* srv, long long id, double* host, size_t n_doubles);
-/* drop a finished request's kept fields */
+/* drop a finished request's kept fields (their device memory is freed once any copy of them
+ * has run; no host wait) */
 int tg_server_release(tg_server* srv, long long id);
 /* ids of requests that finished (done or failed) since the last call, oldest first: up to max
  * of them into ids, *n = how many were written */

@@ -34,8 +34,9 @@ struct Req {
   double* init_pin = nullptr;  // pinned block of the pool holding the fields (usual case)
   const double* init_borrow = nullptr;  // the caller's fields (borrow_inputs), until admission
   size_t n_init = 0;
-  double* result = nullptr;    // pinned block of the pool, kept when keep_results
-  size_t n_result = 0;
+  double* result = nullptr;    // kept fields (reference layout): a device block, or a pinned host
+  size_t n_result = 0;         // block when the device had no room
+  bool result_host = false;
   cudaEvent_t result_ev = nullptr;  // the result's copies into `result` are done past this event
   tg_request_status st{};
   std::string key;
@@ -113,13 +114,8 @@ struct tg_server {
   long long rounds = 0, request_steps = 0, graph_launches = 0, eager_steps = 0;
   std::string err;
   bool round_open = false;                                // between pump_begin and pump_end
-  // released result blocks whose copies may still run: back to the pool once their event passed
-  struct PendingBlock {
-    double* p;
-    size_t n;
-    cudaEvent_t ev;
-  };
-  std::vector<PendingBlock> pending_free;
+  cudaStream_t aux = nullptr;  // result downloads and frees (non-blocking)
+  cudaMemPool_t pool = nullptr;  // device blocks of kept results: freed blocks stay for reuse
   cudaEvent_t chain = nullptr;                            // end of the last batch launched
   std::map<long long, std::pair<int, int>> launched;      // batch -> (slots stepped, launch code)
 };
@@ -238,21 +234,29 @@ int load_slot(tg_server* s, Batch& b, int slot, Req& r) {
   return run_energy_slots(c, 2, slot, 1);
 }
 
-// fields of slot `slot` into a pinned block held by the request (reference layout), queued on
-// the batch stream ahead of anything that reuses the slot or the staging buffer; the copies
-// overlap the next round, and reading the result (tg_server_result) waits for their event
+// fields of slot `slot` into a device block held by the request (reference layout), queued on
+// the batch stream ahead of anything that reuses the slot or the staging buffer; no host work and
+// no page-locking: the block goes to the host only when tg_server_result asks for it
 int store_slot(tg_server* s, Batch& b, int slot, Req& r) {
   tg_ctx* c = b.c;
   if (!s->cfg.keep_results) return TG_OK;
   const size_t D2 = 2 * (size_t)c->D;
   const size_t n = D2 * c->nstate;
-  double* pin = s->pinned.get(n);
-  if (!pin) return set_err(c, TG_ERR_OOM, "pinned host block for a result");
+  // kept results are outside the batch budget (the caller releases them); a pinned host block
+  // where the device has no room
+  double* res = nullptr;
+  bool on_host = false;
+  if (cudaMallocFromPoolAsync(reinterpret_cast<void**>(&res), sizeof(double) * n, s->pool, c->st) != cudaSuccess) {
+    cudaGetLastError();
+    res = s->pinned.get(n);
+    if (!res) return set_err(c, TG_ERR_OOM, "block for a result");
+    on_host = true;
+  }
+  const cudaMemcpyKind kind = on_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
   cudaError_t e = cudaSuccess;
   for (int i = 0; i < c->nstate && e == cudaSuccess; ++i) {
     e = launch_compact_to_dense(c->g, c->U0[i] + (size_t)slot * c->S, 0, c->staging, c->st);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(pin + (size_t)i * D2, c->staging, sizeof(double) * D2, cudaMemcpyDeviceToHost, c->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(res + (size_t)i * D2, c->staging, sizeof(double) * D2, kind, c->st);
   }
   cudaEvent_t ev = nullptr;
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
@@ -260,11 +264,13 @@ int store_slot(tg_server* s, Batch& b, int slot, Req& r) {
   if (e != cudaSuccess) {
     cudaStreamSynchronize(c->st);  // no copy into the block may still be running
     if (ev) cudaEventDestroy(ev);
-    s->pinned.put(pin, n);
-    return cuda_err(c, e, "slot download");
+    if (on_host) s->pinned.put(res, n);
+    else cudaFree(res);
+    return cuda_err(c, e, "slot result");
   }
-  r.result = pin;
+  r.result = res;
   r.n_result = n;
+  r.result_host = on_host;
   r.result_ev = ev;
   return TG_OK;
 }
@@ -570,6 +576,25 @@ int tg_server_create(const tg_server_config* cfg, tg_server** out) {
   tg_server* s = new tg_server();
   s->cfg = *cfg;
   s->dev = cfg->device;
+  if (cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    delete s;
+    return TG_ERR_CUDA;
+  }
+  // the kept results' pool keeps freed memory mapped (a pool that hands memory back at every
+  // synchronisation maps it again for the next result)
+  cudaMemPoolProps pp{};
+  pp.allocType = cudaMemAllocationTypePinned;
+  pp.location.type = cudaMemLocationTypeDevice;
+  pp.location.id = s->dev;
+  if (cudaMemPoolCreate(&s->pool, &pp) != cudaSuccess) {
+    cudaGetLastError();
+    cudaStreamDestroy(s->aux);
+    delete s;
+    return TG_ERR_CUDA;
+  }
+  unsigned long long keep = ~0ull;
+  cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
   s->t0 = std::chrono::steady_clock::now();
   *out = s;
   return TG_OK;
@@ -580,16 +605,16 @@ int tg_server_destroy(tg_server* s) {
   cudaSetDevice(s->dev);
   if (s->round_open) tg_server_pump_end(s, nullptr);
   for (auto& kv : s->reqs) wait_result(kv.second);
-  for (auto& pb : s->pending_free) {
-    cudaEventSynchronize(pb.ev);
-    cudaEventDestroy(pb.ev);
-    cudaFreeHost(pb.p);
-  }
-  s->pending_free.clear();
   for (auto& kv : s->batches) destroy_batch(s, kv.second);
   if (s->chain) cudaEventDestroy(s->chain);
-  for (auto& kv : s->reqs)
-    if (kv.second.result) cudaFreeHost(kv.second.result);
+  if (s->aux) cudaStreamSynchronize(s->aux);  // frees and downloads of results queued there
+  for (auto& kv : s->reqs) {
+    if (!kv.second.result) continue;
+    if (kv.second.result_host) cudaFreeHost(kv.second.result);
+    else cudaFree(kv.second.result);
+  }
+  if (s->aux) cudaStreamDestroy(s->aux);
+  if (s->pool) cudaMemPoolDestroy(s->pool);
   for (auto& kv : s->reqs)
     if (kv.second.init_pin) cudaFreeHost(kv.second.init_pin);
   s->pinned.clear();
@@ -683,19 +708,7 @@ int tg_server_pump_begin(tg_server* s) {
 int tg_server_pump_end(tg_server* s, int* n_active) {
   if (!s) return TG_ERR_ARG;
   cudaSetDevice(s->dev);
-  {
-    std::vector<tg_server::PendingBlock> keep;
-    for (auto& pb : s->pending_free) {
-      if (cudaEventQuery(pb.ev) == cudaSuccess) {
-        cudaEventDestroy(pb.ev);
-        s->pinned.put(pb.p, pb.n);
-      } else {
-        cudaGetLastError();  // cudaErrorNotReady is no error
-        keep.push_back(pb);
-      }
-    }
-    s->pending_free.swap(keep);
-  }
+
   if (!s->round_open) s->launched.clear();  // a round without launches: admission only
   s->round_open = false;
   const auto& launched = s->launched;
@@ -772,8 +785,20 @@ int tg_server_result(tg_server* s, long long id, double* host, size_t n) {
   if (r.st.state != TG_REQ_DONE || !r.result) return TG_ERR_STATE;
   if (n != r.n_result) return TG_ERR_ARG;
   cudaSetDevice(s->dev);
-  wait_result(r);
-  std::memcpy(host, r.result, sizeof(double) * n);
+  if (r.result_host) {
+    wait_result(r);
+    std::memcpy(host, r.result, sizeof(double) * n);
+    return TG_OK;
+  }
+  // on the server's own non-blocking stream, after the result's copies, so that the batches'
+  // streams go on
+  cudaError_t e = r.result_ev ? cudaStreamWaitEvent(s->aux, r.result_ev, 0) : cudaSuccess;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(host, r.result, sizeof(double) * n, cudaMemcpyDeviceToHost, s->aux);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->aux);
+  if (e != cudaSuccess) {
+    s->err = std::string("result download: ") + cudaGetErrorString(e);
+    return TG_ERR_CUDA;
+  }
   return TG_OK;
 }
 
@@ -783,13 +808,17 @@ int tg_server_release(tg_server* s, long long id) {
   if (it == s->reqs.end()) return TG_ERR_ARG;
   Req& r = it->second;
   cudaSetDevice(s->dev);
-  if (r.result && r.result_ev) {
-    // the block goes back to the pool once no copy writes it (checked at each pump_end)
-    s->pending_free.push_back({r.result, r.n_result, r.result_ev});
-    r.result_ev = nullptr;
-  } else {
+  if (r.result && r.result_host) {
     wait_result(r);
     s->pinned.put(r.result, r.n_result);
+  } else if (r.result) {
+    // freed on the server's stream once the result's copies have run (no host wait)
+    if (r.result_ev) cudaStreamWaitEvent(s->aux, r.result_ev, 0);
+    cudaFreeAsync(r.result, s->aux);
+  }
+  if (r.result_ev) {
+    cudaEventDestroy(r.result_ev);
+    r.result_ev = nullptr;
   }
   r.result = nullptr;
   r.n_result = 0;
