@@ -79,4 +79,15 @@ __host__ __device__ __forceinline__ int amap_index(const AxisMap& m, int r) {
 }
 __host__ __device__ __forceinline__ int amap_count(const AxisMap& m) { return m.lo + m.hi; }
 
+// v of every active lane into row[bin], the same sum whatever the warp's timing: the lanes of a
+// bin (__match_any_sync) add their values in lane order and the lowest of them adds the total to
+// the warp's own row
+__device__ __forceinline__ void warp_bin_add(double* row, int bin, double v, bool active) {
+  const int lane = threadIdx.x & 31;
+  const unsigned peers = __match_any_sync(0xffffffffu, active ? bin : -1 - lane);
+  double sum = 0;
+  for (unsigned m = peers; m; m &= m - 1) sum += __shfl_sync(peers, v, __ffs(m) - 1);
+  if (active && lane == __ffs(peers) - 1) row[bin] += sum;
+}
+
 }  // namespace tg

@@ -1586,22 +1586,24 @@ int tg_shell_spectrum(tg_ctx* c, int group, double* ek, double* dissk, int n) {
   const int nf = (group == 2) ? 1 : 3;
   const cx<double>* F[3];
   for (int i = 0; i < nf; ++i) F[i] = c->U0[(group == 0 ? 0 : 3) + i];
-  // scratch: [nf*nbins] ek, [nbins] cnt, [nbins] diss, [nbins] cnt2
+  // scratch: [nf*nbins] ek, [nbins] cnt, [nbins] diss, [nbins] cnt2, then the kernels' block sums
   const size_t need = (size_t)(nf + 3) * nbins;
-  if (c->diag_cap < need) {
+  const size_t part_n = (size_t)shell_spectrum_blocks(c->g) * (nf + 1) * nbins;
+  if (c->diag_cap < need + part_n) {
     if (c->diag) {
       cudaFree(c->diag);
       c->bytes -= sizeof(double) * c->diag_cap;
     }
     c->diag = nullptr;
     c->diag_cap = 0;
-    int rc = dalloc(c, (void**)&c->diag, sizeof(double) * need);
+    int rc = dalloc(c, (void**)&c->diag, sizeof(double) * (need + part_n));
     if (rc) return rc;
-    c->diag_cap = need;
+    c->diag_cap = need + part_n;
   }
   double* dbuf = c->diag;
+  double* part = c->diag + need;
   TG_CK(cudaMemsetAsync(dbuf, 0, sizeof(double) * need, c->st));
-  TG_CK(launch_shell_spectrum(c->g, F, nf, 0.0, dbuf, dbuf + (size_t)nf * nbins, nbins, c->st));
+  TG_CK(launch_shell_spectrum(c->g, F, nf, 0.0, dbuf, dbuf + (size_t)nf * nbins, nbins, part, c->st));
   // dissipation spectrum: sum over components of K^2-weighted, times 2 (Cvf.cc:430-448)
   double* dk = dbuf + (size_t)(nf + 1) * nbins;
   double* dcnt = dk + nbins;
@@ -1609,7 +1611,7 @@ int tg_shell_spectrum(tg_ctx* c, int group, double* ek, double* dissk, int n) {
     // accumulate all components into one row by summing separate passes
     for (int i = 0; i < nf; ++i) {
       const cx<double>* Fi[1] = {F[i]};
-      TG_CK(launch_shell_spectrum(c->g, Fi, 1, 2.0, dk, dcnt, nbins, c->st));
+      TG_CK(launch_shell_spectrum(c->g, Fi, 1, 2.0, dk, dcnt, nbins, part, c->st));
     }
   }
   std::vector<double> h(need);

@@ -147,17 +147,6 @@ struct ContractArgs {
 // of the cosine series P(0, 0) is -kx P and of the sine series P(1, 0), P(2, 0) is +kx P, y and z
 // as FOUR.  hist[r][shell(|K|)] += 2 mult Re(sum_i N_i conj(R_i)) (Multiplicity_factor_FOUR or
 // _SCFT).
-// v of every active lane into row[bin], the same sum whatever the warp's timing: the lanes of a
-// bin (__match_any_sync) add their values in lane order and the lowest of them adds the total to
-// the warp's own row
-__device__ __forceinline__ void warp_bin_add(double* row, int bin, double v, bool active) {
-  const int lane = threadIdx.x & 31;
-  const unsigned peers = __match_any_sync(0xffffffffu, active ? bin : -1 - lane);
-  double sum = 0;
-  for (unsigned m = peers; m; m &= m - 1) sum += __shfl_sync(peers, v, __ffs(m) - 1);
-  if (active && lane == __ffs(peers) - 1) row[bin] += sum;
-}
-
 template <typename Rp>
 __global__ void __launch_bounds__(TPB) k_et_contract(ContractArgs a) {
   constexpr int W = TPB / 32;

@@ -723,33 +723,65 @@ __global__ void __launch_bounds__(TPB) k_finalize(FinalizeArgs a) {
   scal[0] = fmin(dt, Tdt);
 }
 
-__global__ void __launch_bounds__(TPB) k_shell_spectrum(Geo g, PtrArr6 pa, int nf, double n_pow, double* ek, double* cnt, int nbins) {
-  extern __shared__ double sh[];  // [(nf + 1) * nbins]
-  for (int i = threadIdx.x; i < (nf + 1) * nbins; i += TPB) sh[i] = 0;
+// Shell sums of the fields' energies (and the mode counts) in a fixed order: per warp a row of
+// bins (warp_bin_add: the lanes of a shell in lane order), the block's rows in warp order into
+// part[block], then k_bins_accumulate adds the blocks in block order to ek / cnt -- the same bits
+// on every run
+__global__ void __launch_bounds__(TPB) k_shell_spectrum(Geo g, PtrArr6 pa, int nf, double n_pow, double* part,
+                                                        int nbins) {
+  constexpr int W = TPB / 32;
+  extern __shared__ double sh[];  // [W][(nf + 1) * nbins]
+  const int row = (nf + 1) * nbins;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int i = threadIdx.x; i < W * row; i += TPB) sh[i] = 0;
   __syncthreads();
+  double* mine = sh + (size_t)warp * row;
   const long long stride = (long long)gridDim.x * TPB;
-  for (long long idx = (long long)blockIdx.x * TPB + threadIdx.x; idx < g.S; idx += stride) {
-    int r1, r2, l3;
-    compact_mode(g, idx, r1, r2, l3);
-    if (l3 >= g.nkz) continue;
-    const int l1 = geo_l1(g, r1), l2 = amap_index(g.ay, r2);
-    const double kx = geo_kx(g, r1) * g.kf0, ky = geo_ky(g, r2) * g.kf1, kz = l3 * g.kf2;
-    const double K = sqrt(kx * kx + ky * ky + kz * kz);
-    const int bin = (int)ceil(K);
-    if (bin >= nbins) continue;
-    const double m = (g.basis == 0) ? mult_four(l1, l2, l3, g.N1, g.N2) : mult_scft(l1, l2, l3, g.N2);
-    const double kp = (n_pow == 0.0) ? 1.0 : pow(K, n_pow);
-    for (int c = 0; c < nf; ++c) {
-      const cx<double> u = pa.p[c][idx];
-      atomicAdd(&sh[c * nbins + bin], m * kp * (u.x * u.x + u.y * u.y));
+  for (long long w0 = (long long)blockIdx.x * TPB + warp * 32; w0 < g.S; w0 += stride) {
+    const long long idx = w0 + lane;
+    bool active = idx < g.S;
+    int r1 = 0, r2 = 0, l3 = 0, bin = 0;
+    double m = 0, kp = 0;
+    if (active) {
+      compact_mode(g, idx, r1, r2, l3);
+      active = l3 < g.nkz;
     }
-    atomicAdd(&sh[nf * nbins + bin], g.basis == 0 ? m : 0.5 * m);  // SCFT counts factor/2 (scft_energy.cc:279)
+    if (active) {
+      const int l1 = geo_l1(g, r1), l2 = amap_index(g.ay, r2);
+      const double kx = geo_kx(g, r1) * g.kf0, ky = geo_ky(g, r2) * g.kf1, kz = l3 * g.kf2;
+      const double K = sqrt(kx * kx + ky * ky + kz * kz);
+      bin = (int)ceil(K);
+      active = bin < nbins;
+      m = (g.basis == 0) ? mult_four(l1, l2, l3, g.N1, g.N2) : mult_scft(l1, l2, l3, g.N2);
+      kp = (n_pow == 0.0) ? 1.0 : pow(K, n_pow);
+    }
+    for (int c = 0; c < nf; ++c) {
+      double v = 0;
+      if (active) {
+        const cx<double> u = pa.p[c][idx];
+        v = m * kp * (u.x * u.x + u.y * u.y);
+      }
+      warp_bin_add(mine + c * nbins, bin, v, active);
+    }
+    warp_bin_add(mine + nf * nbins, bin, g.basis == 0 ? m : 0.5 * m, active);  // SCFT counts factor/2 (scft_energy.cc:279)
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < nf * nbins; i += TPB)
-    if (sh[i] != 0) atomicAdd(&ek[i], sh[i]);
-  for (int i = threadIdx.x; i < nbins; i += TPB)
-    if (sh[nf * nbins + i] != 0) atomicAdd(&cnt[i], sh[nf * nbins + i]);
+  for (int i = threadIdx.x; i < row; i += TPB) {
+    double t = 0;
+    for (int w = 0; w < W; ++w) t += sh[(size_t)w * row + i];
+    part[(size_t)blockIdx.x * row + i] = t;
+  }
+}
+
+// out[i] += the blocks' part[b][i] in block order (i < n), one thread per bin
+__global__ void k_bins_accumulate(const double* __restrict__ part, int nblocks, int n, double* out0, int n0,
+                                  double* out1) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double t = 0;
+  for (int b = 0; b < nblocks; ++b) t += part[(size_t)b * n + i];
+  if (i < n0) out0[i] += t;
+  else out1[i - n0] += t;
 }
 
 inline int nblk(long long n) { return (int)((n + TPB - 1) / TPB); }
@@ -884,18 +916,25 @@ cudaError_t launch_finalize(const FinalizeArgs& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_shell_spectrum(const Geo& g, const cx<double>* const* F, int nf, double n_pow, double* ek, double* cnt, int nbins, cudaStream_t s) {
+int shell_spectrum_blocks(const Geo& g) {
+  int nb = nblk(g.S);
+  return nb > 148 * 8 ? 148 * 8 : nb;
+}
+
+cudaError_t launch_shell_spectrum(const Geo& g, const cx<double>* const* F, int nf, double n_pow, double* ek, double* cnt,
+                                  int nbins, double* part, cudaStream_t s) {
   PtrArr6 pa{};
   for (int c = 0; c < nf; ++c) pa.p[c] = const_cast<cx<double>*>(F[c]);
-  const size_t smem = (size_t)(nf + 1) * nbins * sizeof(double);
+  const int row = (nf + 1) * nbins;
+  const size_t smem = (size_t)(TPB / 32) * row * sizeof(double);
   if (smem > 200 * 1024) return cudaErrorInvalidValue;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(k_shell_spectrum, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  int nb = nblk(g.S);
-  if (nb > 148 * 8) nb = 148 * 8;
-  k_shell_spectrum<<<nb, TPB, smem, s>>>(g, pa, nf, n_pow, ek, cnt, nbins);
+  const int nb = shell_spectrum_blocks(g);
+  k_shell_spectrum<<<nb, TPB, smem, s>>>(g, pa, nf, n_pow, part, nbins);
+  k_bins_accumulate<<<(row + 127) / 128, 128, 0, s>>>(part, nb, row, ek, nf * nbins, cnt);
   return cudaGetLastError();
 }
 

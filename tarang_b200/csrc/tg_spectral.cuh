@@ -147,6 +147,9 @@ struct FinalizeArgs {
 };
 cudaError_t launch_finalize(const FinalizeArgs& a, cudaStream_t s);
 // shell spectrum: ek[c][bin] += mult K^n |A|^2, counts
-cudaError_t launch_shell_spectrum(const Geo& g, const cx<double>* const* F, int nf, double n_pow, double* ek, double* cnt, int nbins, cudaStream_t s);
+// part: scratch of shell_spectrum_blocks(g) x (nf + 1) x nbins doubles; ek and cnt are added to
+int shell_spectrum_blocks(const Geo& g);
+cudaError_t launch_shell_spectrum(const Geo& g, const cx<double>* const* F, int nf, double n_pow, double* ek, double* cnt,
+                                  int nbins, double* part, cudaStream_t s);
 
 }  // namespace tg

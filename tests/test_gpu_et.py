@@ -87,8 +87,8 @@ def test_force_feed_shell(lib, N, S):
 
 
 def test_tables_are_deterministic(lib):
-    """The flux and shell-to-shell tables are the same bits on a second call and on a second
-    context (the contraction's shell sums run in a fixed order)."""
+    """The flux and shell-to-shell tables and the shell spectrum are the same bits on a second
+    call and on a second context (their shell sums run in a fixed order)."""
     from tarang_b200.solver import IncFluid
     N, S = (32, 32, 32), 10
     V = ic.random_phase_field(N, seed=7)
@@ -96,7 +96,10 @@ def test_tables_are_deterministic(lib):
     for _ in range(2):
         s = IncFluid(N, nu=1e-3, dt=1e-3, n_shells=S)
         s.set_V(V)
-        out.append((s.Compute_flux(), s.Compute_shell_tr(), s.Compute_flux()))
+        out.append((s.Compute_flux(), s.Compute_shell_tr(), s.Compute_flux(), s.CV_Compute_shell_spectrum()))
         s.close()
-    (f0, t0, f1), (g0, u0, _) = out
+    (f0, t0, f1, e0), (g0, u0, _, e1) = out
     assert np.array_equal(f0, f1) and np.array_equal(f0, g0) and np.array_equal(t0, u0)
+    # and the shell spectrum (energy, dissipation) likewise
+    for a, b in zip(e0, e1):
+        assert np.array_equal(a, b)
